@@ -1,0 +1,434 @@
+"""Panel meshes: geometry arrays consumed by the assembly kernels, and the
+generators used by the benchmark workloads.
+
+Face geometry restates capytaine ``meshes/geometry.py:35-118`` (normals from
+the diagonals of quads, areas and centres from the two triangles (a, b, c) and
+(a, c, d), radius = distance from the first vertex to the centre) and
+``meshes/meshes.py:454-486`` (triangles stored as quads whose last vertex is
+repeated; default quadrature = one point at the centre weighted by the area).
+Generators follow ``meshes/predefined/spheres.py:26-66``,
+``rectangles.py:26-213`` and ``cylinders.py:108-205``; clipping follows
+``meshes/clip.py`` and the cleaning rules of ``meshes/clean.py``.
+"""
+from __future__ import annotations
+
+import hashlib
+from functools import cached_property
+from itertools import product
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+__all__ = [
+    "Mesh",
+    "mesh_sphere",
+    "mesh_ellipsoid",
+    "mesh_rectangle",
+    "mesh_parallelepiped",
+    "mesh_vertical_cylinder",
+]
+
+
+def _as_face_lists(faces) -> List[List[int]]:
+    out = []
+    for f in faces:
+        f = [int(v) for v in f]
+        if len(f) == 4 and f[2] == f[3]:
+            f = f[:3]
+        out.append(f)
+    return out
+
+
+class Mesh:
+    """A surface mesh of triangles and quadrilaterals.
+
+    Parameters
+    ----------
+    vertices: array (V, 3)
+    faces: sequence of 3- or 4-vertex index lists (0-based); a 4-index face whose
+        last two indices are equal is a triangle, as in capytaine.
+    quadrature_method: None (one point at the centre) or "Gauss-Legendre 2".
+    clean: merge near-duplicate vertices and drop degenerate faces
+        (capytaine ``meshes/clean.py``).
+    """
+
+    def __init__(self, vertices, faces, *, quadrature_method: Optional[str] = None,
+                 name: Optional[str] = None, clean: bool = True):
+        self.vertices = np.array(vertices, dtype=np.float64).reshape(-1, 3)
+        self._faces = _as_face_lists(faces)
+        if clean and len(self._faces) > 0:
+            self.vertices, self._faces = _clean_mesh(self.vertices, self._faces)
+        self.quadrature_method = quadrature_method
+        self.name = name
+
+    # -- sizes ---------------------------------------------------------------
+    @property
+    def nb_faces(self) -> int:
+        return len(self._faces)
+
+    @property
+    def nb_vertices(self) -> int:
+        return self.vertices.shape[0]
+
+    def __repr__(self):
+        return f"Mesh(nb_faces={self.nb_faces}, nb_vertices={self.nb_vertices}, name={self.name!r})"
+
+    # -- geometry (capytaine meshes/geometry.py:35-85) -------------------------
+    @cached_property
+    def faces(self) -> np.ndarray:
+        """(N, 4) int array, triangles padded by repeating their last vertex."""
+        arr = np.array([f if len(f) == 4 else f + [f[-1]] for f in self._faces], dtype=np.int64)
+        return arr.reshape(-1, 4)
+
+    @cached_property
+    def _is_quad(self) -> np.ndarray:
+        f = self.faces
+        return f[:, 2] != f[:, 3]
+
+    @cached_property
+    def faces_normals(self) -> np.ndarray:
+        v, f, q = self.vertices, self.faces, self._is_quad
+        ac = v[f[:, 2]] - v[f[:, 0]]
+        bd = v[f[:, 3]] - v[f[:, 1]]
+        quad_n = np.cross(ac, bd)
+        tri_n = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+        n = np.where(q[:, None], quad_n, tri_n)
+        return n / np.linalg.norm(n, axis=1)[:, None]
+
+    @cached_property
+    def _triangle_parts(self):
+        v, f = self.vertices, self.faces
+        a, b, c, d = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]], v[f[:, 3]]
+        area1 = 0.5 * np.linalg.norm(np.cross(b - a, c - a), axis=1)
+        area2 = np.where(self._is_quad, 0.5 * np.linalg.norm(np.cross(c - a, d - a), axis=1), 0.0)
+        return a, b, c, d, area1, area2
+
+    @cached_property
+    def faces_areas(self) -> np.ndarray:
+        _, _, _, _, area1, area2 = self._triangle_parts
+        return np.where(self._is_quad, area1 + area2, area1)
+
+    @cached_property
+    def faces_centers(self) -> np.ndarray:
+        a, b, c, d, area1, area2 = self._triangle_parts
+        c1 = (a + b + c) / 3
+        c2 = (a + c + d) / 3
+        quad_c = (c1 * area1[:, None] + c2 * area2[:, None]) / (area1 + area2)[:, None]
+        return np.where(self._is_quad[:, None], quad_c, c1)
+
+    @cached_property
+    def faces_radiuses(self) -> np.ndarray:
+        return np.linalg.norm(self.faces_centers - self.vertices[self.faces[:, 0]], axis=1)
+
+    @cached_property
+    def quadrature_points(self):
+        """(points (N, Q, 3), weights (N, Q)); capytaine meshes/meshes.py:472-486."""
+        if self.quadrature_method is None:
+            return self.faces_centers.reshape((-1, 1, 3)), self.faces_areas.reshape(-1, 1)
+        if self.quadrature_method == "Gauss-Legendre 2":
+            return _gauss_legendre_2(self.vertices, self.faces)
+        raise ValueError(f"Unknown quadrature_method: {self.quadrature_method}")
+
+    @cached_property
+    def z_span(self):
+        return float(self.vertices[:, 2].min()), float(self.vertices[:, 2].max())
+
+    @cached_property
+    def content_hash(self) -> str:
+        """Digest of the vertex and face arrays (cache key for device-resident data)."""
+        h = hashlib.sha1()
+        h.update(np.ascontiguousarray(self.vertices).tobytes())
+        h.update(np.ascontiguousarray(self.faces).tobytes())
+        h.update(repr(self.quadrature_method).encode())
+        return h.hexdigest()
+
+    def __eq__(self, other):
+        return isinstance(other, Mesh) and self.content_hash == other.content_hash
+
+    def __hash__(self):
+        return hash(self.content_hash)
+
+    # -- transformations ------------------------------------------------------
+    def translated(self, shift, name=None) -> "Mesh":
+        return Mesh(self.vertices + np.asarray(shift, dtype=float), self._faces,
+                    quadrature_method=self.quadrature_method, name=name or self.name, clean=False)
+
+    def scaled(self, factors, name=None) -> "Mesh":
+        return Mesh(self.vertices * np.asarray(factors, dtype=float), self._faces,
+                    quadrature_method=self.quadrature_method, name=name or self.name, clean=False)
+
+    def with_quadrature(self, quadrature_method) -> "Mesh":
+        return Mesh(self.vertices, self._faces, quadrature_method=quadrature_method, name=self.name, clean=False)
+
+    def merged(self) -> "Mesh":
+        return self
+
+    def clipped(self, *, origin, normal, name=None) -> "Mesh":
+        v, f = _clip_faces(self.vertices, self._faces, np.asarray(normal, float), np.asarray(origin, float))
+        return Mesh(v, f, quadrature_method=self.quadrature_method, name=name or self.name, clean=True)
+
+    def immersed_part(self, free_surface=0.0) -> "Mesh":
+        """Part below z = free_surface; capytaine abstract_meshes.py:383-407 (infinite depth)."""
+        if self.z_span[1] <= free_surface:
+            return self
+        return self.clipped(origin=(0, 0, free_surface), normal=(0, 0, 1))
+
+    @staticmethod
+    def join_meshes(*meshes, name=None) -> "Mesh":
+        verts, faces, off = [], [], 0
+        for m in meshes:
+            verts.append(m.vertices)
+            faces.extend([[i + off for i in f] for f in m._faces])
+            off += m.nb_vertices
+        return Mesh(np.concatenate(verts), faces, name=name, clean=True)
+
+
+# ---------------------------------------------------------------------------
+def _gauss_legendre_2(vertices, faces):
+    """capytaine meshes/geometry.py:88-118."""
+    s = 1 / np.sqrt(3)
+    local_points = np.array([(s, s), (s, -s), (-s, s), (-s, -s)])
+    local_weights = np.array([0.25, 0.25, 0.25, 0.25])
+    fv = vertices[faces]
+    nb_faces = fv.shape[0]
+    points = np.empty((nb_faces, 4, 3))
+    weights = np.empty((nb_faces, 4))
+    for k, (xk, yk) in enumerate(local_points):
+        points[:, k, :] = ((1 + xk) * (1 + yk) * fv[:, 0] + (1 + xk) * (1 - yk) * fv[:, 1]
+                           + (1 - xk) * (1 - yk) * fv[:, 2] + (1 - xk) * (1 + yk) * fv[:, 3]) / 4
+        dxidx = ((1 + yk) * fv[:, 0] + (1 - yk) * fv[:, 1] - (1 - yk) * fv[:, 2] - (1 + yk) * fv[:, 3]) / 4
+        dxidy = ((1 + xk) * fv[:, 0] - (1 + xk) * fv[:, 1] - (1 - xk) * fv[:, 2] + (1 - xk) * fv[:, 3]) / 4
+        detJ = np.linalg.norm(np.cross(dxidx, dxidy), axis=1)
+        weights[:, k] = local_weights[k] * 4 * detJ
+    return points, weights
+
+
+def _clean_mesh(vertices, faces, tol=1e-8, max_iter=5):
+    """Merge near-duplicate vertices, drop repeated indices, degenerate, duplicate
+    and small faces, and unused vertices (capytaine meshes/clean.py)."""
+    from scipy.spatial import cKDTree
+
+    for _ in range(max_iter):
+        nv0, nf0 = len(vertices), len(faces)
+        # 1) near-duplicate vertices -> smallest index of each group
+        tree = cKDTree(vertices)
+        groups = tree.query_ball_tree(tree, r=tol)
+        rep_new = {}
+        new_vertices = []
+        mapping = np.empty(len(vertices), dtype=np.int64)
+        for i, group in enumerate(groups):
+            rep = min(group)
+            if rep not in rep_new:
+                rep_new[rep] = len(new_vertices)
+                new_vertices.append(vertices[rep])
+            mapping[i] = rep_new[rep]
+        vertices = np.array(new_vertices)
+        faces = [[int(mapping[i]) for i in f] for f in faces]
+        # 2) repeated indices inside faces
+        new_faces = []
+        for f in faces:
+            seen, uniq = set(), []
+            for vi in f:
+                if vi not in seen:
+                    seen.add(vi)
+                    uniq.append(vi)
+            if len(uniq) in (3, 4):
+                new_faces.append(uniq)
+            elif len(uniq) > 4:
+                raise ValueError(f"Face with {len(uniq)} unique vertices: only 3 or 4 supported.")
+        faces = new_faces
+        # 3) duplicate faces
+        seen_f, uniq_faces = set(), []
+        for f in faces:
+            key = tuple(sorted(f))
+            if key not in seen_f:
+                seen_f.add(key)
+                uniq_faces.append(f)
+        faces = uniq_faces
+        # 4) small faces
+        def area(f):
+            p = vertices[f]
+            a = 0.5 * np.linalg.norm(np.cross(p[1] - p[0], p[2] - p[0]))
+            if len(f) == 4:
+                a += 0.5 * np.linalg.norm(np.cross(p[2] - p[0], p[3] - p[0]))
+            return a
+        faces = [f for f in faces if area(f) > tol]
+        # 5) unused vertices
+        used = sorted({i for f in faces for i in f})
+        remap = {old: new for new, old in enumerate(used)}
+        vertices = vertices[used] if used else np.empty((0, 3))
+        faces = [[remap[i] for i in f] for f in faces]
+        if len(vertices) == nv0 and len(faces) == nf0:
+            break
+    return vertices, faces
+
+
+def _clip_faces(vertices, faces, normal, origin, tol=1e-8):
+    """Keep the half-space (origin - v)·normal >= -tol; capytaine meshes/clip.py."""
+    verts = vertices.astype(float).tolist()
+    new_faces = []
+    for face in faces:
+        pts = np.asarray([verts[i] for i in face], dtype=float)
+        s = (origin - pts) @ normal
+        keep = [face[i] for i in range(len(face)) if s[i] >= -tol]
+        if len(keep) == 0:
+            continue
+        if len(keep) == len(face):
+            new_faces.append(list(face))
+            continue
+        keep_set = set(keep)
+        edges = list(zip(face, face[1:] + face[:1]))
+        inters = {}
+        for (i, j) in edges:
+            if (i in keep_set) ^ (j in keep_set):
+                v1, v2 = np.array(verts[i]), np.array(verts[j])
+                u = v2 - v1
+                denom = float(np.dot(normal, u))
+                if abs(denom) < tol:
+                    raise ValueError("Segment is parallel to the plane (no unique intersection).")
+                t = float(np.dot(normal, origin - v1) / denom)
+                t = max(0.0, min(1.0, t))
+                inters[(i, j)] = len(verts)
+                verts.append((v1 + t * u).tolist())
+        boundary = []
+        for (i, j) in edges:
+            if i in keep_set:
+                boundary.append(i)
+            if (i, j) in inters:
+                boundary.append(inters[(i, j)])
+        if len(boundary) == 3:
+            new_faces.append(boundary)
+        elif len(boundary) == 4:
+            new_faces.append([boundary[0], boundary[1], boundary[2]])
+            new_faces.append([boundary[0], boundary[2], boundary[3]])
+        elif len(boundary) == 5:
+            new_faces.append([boundary[0], boundary[1], boundary[2]])
+            new_faces.append([boundary[0], boundary[2], boundary[3], boundary[4]])
+        else:
+            for k in range(1, len(boundary) - 1):
+                new_faces.append([boundary[0], boundary[k], boundary[k + 1]])
+    return np.asarray(verts, dtype=float), new_faces
+
+
+# ---------------------------------------------------------------------------
+# Generators
+def _surface_of_revolution(profile_points, n):
+    """Profile (m, 3) in the xOz half plane, sorted by increasing z, swept n times
+    around Oz: faces (i, i+m, i+m+1, i+1) per wedge as in capytaine
+    symmetric_meshes.py:410-423, wedges concatenated in order of rotation angle."""
+    pts = np.asarray(sorted(list(np.asarray(profile_points, float)), key=lambda p: p[2]))
+    m = len(pts)
+    verts = []
+    for j in range(n):
+        t = 2 * np.pi * j / n
+        c, s = np.cos(t), np.sin(t)
+        rot = np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+        verts.append(pts @ rot.T)
+    verts = np.concatenate(verts)  # ring j occupies rows [j*m, (j+1)*m)
+    faces = []
+    for j in range(n):
+        jn = (j + 1) % n
+        for i in range(m - 1):
+            faces.append([j * m + i, jn * m + i, jn * m + i + 1, j * m + i + 1])
+    return verts, faces
+
+
+def mesh_sphere(*, radius=1.0, center=(0.0, 0.0, 0.0), resolution=(10, 10), name=None) -> Mesh:
+    """Sphere from a meridian of ntheta+1 points swept nphi times (capytaine spheres.py:26-66)."""
+    ntheta, nphi = resolution
+    theta = np.linspace(0.0, np.pi, ntheta + 1)
+    meridian = radius * np.stack([np.sin(theta), np.zeros_like(theta), -np.cos(theta)], axis=1)
+    verts, faces = _surface_of_revolution(meridian, nphi)
+    return Mesh(verts, faces, name=name).translated(center)
+
+
+def mesh_ellipsoid(*, semi_axes=(1.0, 1.0, 1.0), center=(0.0, 0.0, 0.0), resolution=(10, 10), name=None) -> Mesh:
+    """Unit sphere scaled along each axis (capytaine has no ellipsoid generator)."""
+    return mesh_sphere(radius=1.0, resolution=resolution, name=name).scaled(semi_axes).translated(center)
+
+
+def mesh_rectangle(*, size=(5.0, 5.0), center=(0.0, 0.0, 0.0), resolution=(5, 5),
+                   normal=(0.0, 0.0, 1.0), name=None) -> Mesh:
+    """One-sided rectangle (capytaine rectangles.py:26-100), built directly in the
+    plane orthogonal to ``normal`` with panels oriented along ``normal``."""
+    width, height = size
+    nw, nh = resolution
+    normal = np.asarray(normal, float)
+    normal = normal / np.linalg.norm(normal)
+    # In-plane axes: the reference builds the panel in x=0 with normal -x, then rotates.
+    a = np.array([-1.0, 0.0, 0.0])
+    R = _rotation_aligning(a, normal)
+    y_range = np.linspace(-width / 2, width / 2, nw + 1)
+    z_range = np.linspace(-height / 2, height / 2, nh + 1)
+    nodes = np.array(list(product([0.0], y_range, z_range)), dtype=float)
+    panels = [(j + i * (nh + 1), j + 1 + i * (nh + 1), j + 1 + (i + 1) * (nh + 1), j + (i + 1) * (nh + 1))
+              for (i, j) in product(range(nw), range(nh))]
+    nodes = nodes @ R.T
+    return Mesh(nodes, panels, name=name, clean=False).translated(center)
+
+
+def _rotation_aligning(a, b, eps=1e-8):
+    """Rotation matrix taking unit vector a onto unit vector b
+    (capytaine abstract_meshes.py:129-175)."""
+    a = a / np.linalg.norm(a)
+    b = b / np.linalg.norm(b)
+    v = np.cross(a, b)
+    c = float(np.dot(a, b))
+    s = float(np.linalg.norm(v))
+    if s < eps and c > 0:
+        return np.eye(3)
+    if s < eps and c < 0:
+        axis = np.eye(3)[int(np.argmin(np.abs(a)))]
+        v = np.cross(a, axis)
+        v = v / np.linalg.norm(v)
+        return 2 * np.outer(v, v) - np.eye(3)
+    vx = np.array([[0, -v[2], v[1]], [v[2], 0, -v[0]], [-v[1], v[0], 0]])
+    return np.eye(3) + vx + vx @ vx * ((1 - c) / s ** 2)
+
+
+def mesh_parallelepiped(size=(1.0, 1.0, 1.0), center=(0, 0, 0), resolution=(4, 4, 4),
+                        missing_sides=frozenset(), name=None) -> Mesh:
+    """Six rectangles with outward normals (capytaine rectangles.py:103-213)."""
+    width, thickness, height = size
+    nw, nth, nh = resolution
+    sides = []
+    if "left" not in missing_sides:
+        sides.append(mesh_rectangle(size=(thickness, height), resolution=(nth, nh), center=(-width / 2, 0, 0),
+                                    normal=(-1, 0, 0)))
+    if "right" not in missing_sides:
+        sides.append(mesh_rectangle(size=(thickness, height), resolution=(nth, nh), center=(width / 2, 0, 0),
+                                    normal=(1, 0, 0)))
+    if "front" not in missing_sides:
+        sides.append(mesh_rectangle(size=(width, height), resolution=(nw, nh), center=(0, -thickness / 2, 0),
+                                    normal=(0, -1, 0)))
+    if "back" not in missing_sides:
+        sides.append(mesh_rectangle(size=(width, height), resolution=(nw, nh), center=(0, thickness / 2, 0),
+                                    normal=(0, 1, 0)))
+    if "top" not in missing_sides:
+        sides.append(mesh_rectangle(size=(thickness, width), resolution=(nth, nw), center=(0, 0, height / 2),
+                                    normal=(0, 0, 1)))
+    if "bottom" not in missing_sides:
+        sides.append(mesh_rectangle(size=(thickness, width), resolution=(nth, nw), center=(0, 0, -height / 2),
+                                    normal=(0, 0, -1)))
+    return Mesh.join_meshes(*sides, name=name).translated(center)
+
+
+def mesh_vertical_cylinder(*, length=10.0, radius=1.0, center=(0, 0, 0), resolution=(2, 8, 10), name=None) -> Mesh:
+    """Closed vertical cylinder: bottom disc, lateral surface, top disc
+    (capytaine cylinders.py:108-205, full circle)."""
+    nr, ntheta, nz = resolution
+    theta_range = np.linspace(0, 2 * np.pi, ntheta + 1)
+    z_range = np.linspace(-length / 2, length / 2, nz + 1)
+    if nr > 0:
+        r_range = np.linspace(0.0, radius, nr + 1)
+        nodes = np.concatenate([
+            np.array([(r * np.sin(t), r * np.cos(t), -length / 2) for (r, t) in product(r_range, theta_range)]),
+            np.array([(radius * np.sin(t), radius * np.cos(t), z) for (z, t) in product(z_range, theta_range)]),
+            np.array([(r * np.sin(t), r * np.cos(t), length / 2) for (r, t) in product(r_range[::-1], theta_range)]),
+        ])
+    else:
+        r_range = np.array([])
+        nodes = np.array([(radius * np.sin(t), radius * np.cos(t), z) for (z, t) in product(z_range, theta_range)])
+    panels = [(j + i * (ntheta + 1), j + (i + 1) * (ntheta + 1), j + 1 + (i + 1) * (ntheta + 1), j + 1 + i * (ntheta + 1))
+              for (i, j) in product(range(nz + 2 * len(r_range)), range(ntheta))]
+    return Mesh(nodes, panels, name=name, clean=True).translated(center)

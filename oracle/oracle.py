@@ -1,0 +1,360 @@
+"""ORACLE — test infrastructure only.
+
+CPU restatement of capytaine's Delhommeau Green function and of the indirect
+BEM solve for one frequency.  Only ``tests/``, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` import this module; the product package
+never does.
+
+* Green function: ctypes bindings to ``liboracle_delhommeau.so`` (C++
+  restatement of libs/libDelhommeau/src, built by ``oracle/Makefile``), wrapped
+  the way capytaine ``green_functions/delhommeau.py:116-261, 336-520`` and
+  ``green_functions/abstract_green_function.py:30-72`` wrap the Fortran core.
+* Solver glue: ``bem/solver.py:145-215`` (indirect method), boundary conditions
+  ``bem/problems_and_results.py:373-381, 440-449``, Airy waves
+  ``bem/airy_waves.py:19-102``, force integration ``bodies/bodies.py:238-250``,
+  coefficients ``bem/problems_and_results.py:583-592``; the linear algebra is
+  SciPy's ``lu_factor``/``lu_solve``, which is what the reference calls
+  (``tools/block_circulant_matrices.py:361-385``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle_delhommeau.so")
+
+LEGACY_GRID, SCALED_NEMOH3_GRID = 0, 1
+HIGH_FREQ, LOW_FREQ, LOW_FREQ_WITH_RANKINE_PART = 0, 1, 2
+GRID_ENUM = {"legacy": LEGACY_GRID, "scaled_nemoh3": SCALED_NEMOH3_GRID}
+SING_ENUM = {"high_freq": HIGH_FREQ, "low_freq": LOW_FREQ, "low_freq_with_rankine_part": LOW_FREQ_WITH_RANKINE_PART}
+
+
+def build_oracle():
+    """Compile the C++ restatement with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _load():
+    if not os.path.exists(_LIB_PATH):
+        build_oracle()
+    lib = ctypes.CDLL(_LIB_PATH)
+    d, i, p = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
+    lib.oracle_exp_e1.argtypes = [d, d, p]
+    lib.oracle_numerical_integration.argtypes = [d, d, i, p]
+    lib.oracle_asymptotic_approximations.argtypes = [d, d, p]
+    lib.oracle_default_r_spacing.argtypes = [i, d, i, p]
+    lib.oracle_default_z_spacing.argtypes = [i, d, i, p]
+    lib.oracle_nearest_r_index.argtypes = [d, p, i, i]
+    lib.oracle_nearest_r_index.restype = i
+    lib.oracle_nearest_z_index.argtypes = [d, p, i, i]
+    lib.oracle_nearest_z_index.restype = i
+    lib.oracle_construct_tabulation.argtypes = [p, i, p, i, i, p, i]
+    lib.oracle_pick_in_default_tabulation.argtypes = [d, d, i, p, i, p, i, p, p]
+    lib.oracle_wave_part_infinite_depth.argtypes = [i, p, p, d, i, i, p, i, p, i, p, i, p, p]
+    lib.oracle_integral_of_rankine.argtypes = [i, p, p, p, p, p, p, i, i, p, p]
+    lib.oracle_build_matrices.argtypes = [i, p, p, i, p, p, p, p, p, p, i, p, p, d, d, i, i, p, i, p, i, p, i, i,
+                                          i, p, p, i]
+    lib.oracle_build_matrices.restype = i
+    lib.oracle_add_diagonal_term.argtypes = [i, i, p, p, d, i, p]
+    lib.oracle_add_rankine_term_only.argtypes = [i, p, p, i, p, p, p, p, p, p, i, i, p, p, i]
+    lib.oracle_pi.restype = d
+    return lib
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _c(a, dtype=np.float64):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+# ---------------------------------------------------------------------------
+# Delhommeau_integrals.f90 entry points
+def exp_e1(z: complex) -> complex:
+    out = np.zeros(2)
+    lib().oracle_exp_e1(float(np.real(z)), float(np.imag(z)), _ptr(out))
+    return complex(out[0], out[1])
+
+
+def numerical_integration(r, z, npts) -> np.ndarray:
+    out = np.zeros(5)
+    lib().oracle_numerical_integration(float(r), float(z), int(npts), _ptr(out))
+    return out
+
+
+def asymptotic_approximations(r, z) -> np.ndarray:
+    out = np.zeros(5)
+    lib().oracle_asymptotic_approximations(float(r), float(z), _ptr(out))
+    return out
+
+
+def default_r_spacing(nr, rmax, method) -> np.ndarray:
+    out = np.zeros(max(nr, 0))
+    lib().oracle_default_r_spacing(int(nr), float(rmax), int(method), _ptr(out))
+    return out
+
+
+def default_z_spacing(nz, zmin, method) -> np.ndarray:
+    out = np.zeros(max(nz, 0))
+    lib().oracle_default_z_spacing(int(nz), float(zmin), int(method), _ptr(out))
+    return out
+
+
+def nearest_r_index(r, r_range, method) -> int:
+    r_range = _c(r_range)
+    return lib().oracle_nearest_r_index(float(r), _ptr(r_range), len(r_range), int(method))
+
+
+def nearest_z_index(z, z_range, method) -> int:
+    z_range = _c(z_range)
+    return lib().oracle_nearest_z_index(float(z), _ptr(z_range), len(z_range), int(method))
+
+
+def construct_tabulation(r_range, z_range, npts, nthreads=0) -> np.ndarray:
+    r_range, z_range = _c(r_range), _c(z_range)
+    out = np.zeros((len(r_range), len(z_range), 5))
+    lib().oracle_construct_tabulation(_ptr(r_range), len(r_range), _ptr(z_range), len(z_range), int(npts),
+                                      _ptr(out), int(nthreads))
+    return out
+
+
+# ---------------------------------------------------------------------------
+class OracleDelhommeau:
+    """CPU Delhommeau Green function with the reference's constructor defaults
+    (capytaine green_functions/delhommeau.py:30-41)."""
+
+    def __init__(self, *, tabulation_nr=676, tabulation_rmax=100.0, tabulation_nz=372, tabulation_zmin=-251.0,
+                 tabulation_nb_integration_points=1001, tabulation_grid_shape="scaled_nemoh3",
+                 gf_singularities="low_freq", nthreads=0, tabulation=None):
+        self.tabulation_nb_integration_points = int(tabulation_nb_integration_points)
+        self.tabulation_grid_shape = tabulation_grid_shape
+        self.tabulation_grid_shape_index = GRID_ENUM[tabulation_grid_shape]
+        self.gf_singularities = gf_singularities
+        self.floating_point_precision = "float64"
+        self.nthreads = nthreads
+        if tabulation is not None:
+            r, z, v = tabulation
+            self.tabulated_r_range, self.tabulated_z_range = _c(r), _c(z)
+            self.tabulated_integrals = _c(v)
+        else:
+            self.tabulated_r_range = default_r_spacing(tabulation_nr, tabulation_rmax, self.tabulation_grid_shape_index)
+            self.tabulated_z_range = default_z_spacing(tabulation_nz, tabulation_zmin, self.tabulation_grid_shape_index)
+            self.tabulated_integrals = construct_tabulation(self.tabulated_r_range, self.tabulated_z_range,
+                                                            self.tabulation_nb_integration_points, nthreads)
+
+    @property
+    def tabulation(self):
+        return self.tabulated_r_range, self.tabulated_z_range, self.tabulated_integrals
+
+    def _tab_args(self):
+        t = self.tabulated_integrals if self.tabulated_integrals.size else np.zeros(5)
+        return (self.tabulation_nb_integration_points, self.tabulation_grid_shape_index,
+                _ptr(self.tabulated_r_range), len(self.tabulated_r_range),
+                _ptr(self.tabulated_z_range), len(self.tabulated_z_range), _ptr(t))
+
+    def wave_part_infinite_depth(self, x0i, x0j, k, gf_singularities=None):
+        sing = SING_ENUM[gf_singularities or self.gf_singularities]
+        x0i = _c(np.atleast_2d(x0i))
+        x0j = _c(np.atleast_2d(x0j))
+        n = x0i.shape[0]
+        G = np.zeros((n, 2))
+        nG = np.zeros((n, 3, 2))
+        lib().oracle_wave_part_infinite_depth(n, _ptr(x0i), _ptr(x0j), float(k), *self._tab_args(), sing,
+                                              _ptr(G), _ptr(nG))
+        return G[:, 0] + 1j * G[:, 1], nG[..., 0] + 1j * nG[..., 1]
+
+    @staticmethod
+    def _colloc_and_normals(mesh1, mesh2, adjoint):
+        """abstract_green_function.py:30-57"""
+        if hasattr(mesh1, "faces_centers"):
+            pts = mesh1.faces_centers
+            nrm = mesh1.faces_normals if adjoint else mesh2.faces_normals
+            return _c(pts), _c(nrm)
+        pts = np.asarray(mesh1, dtype=float)
+        if pts.ndim == 2 and pts.shape[1] == 3:
+            nrm = np.zeros((pts.shape[0], 3)) if adjoint else mesh2.faces_normals
+            return _c(pts), _c(nrm)
+        raise ValueError(f"Unrecognized first input: {mesh1}")
+
+    @staticmethod
+    def _mesh_args(mesh2):
+        qp, qw = mesh2.quadrature_points
+        return (_c(mesh2.vertices), _c(mesh2.faces, np.int32), _c(mesh2.faces_centers), _c(mesh2.faces_normals),
+                _c(mesh2.faces_areas), _c(mesh2.faces_radiuses), qp.shape[1], _c(qp), _c(qw))
+
+    def evaluate_rankine_only(self, mesh1, mesh2, *, adjoint_double_layer=True, early_dot_product=True,
+                              diagonal_term_in_double_layer=True):
+        """delhommeau.py:336-402"""
+        pts, nrm = self._colloc_and_normals(mesh1, mesh2, adjoint_double_layer)
+        n, N = pts.shape[0], mesh2.nb_faces
+        kdim = 1 if early_dot_product else 3
+        S = np.zeros((n, N), order="F")
+        K = np.zeros((kdim, n, N), order="F")
+        v, f, c, nn, a, r, nq, qp, qw = self._mesh_args(mesh2)
+        lib().oracle_add_rankine_term_only(n, _ptr(pts), _ptr(nrm), N, _ptr(v), _ptr(f), _ptr(c), _ptr(nn), _ptr(a),
+                                           _ptr(r), int(adjoint_double_layer), kdim, _ptr(S), _ptr(K),
+                                           self.nthreads)
+        if diagonal_term_in_double_layer:
+            Kc = K.astype(np.complex128, order="F")
+            centers = _c(mesh2.faces_centers[:min(n, N)])
+            lib().oracle_add_diagonal_term(n, N, _ptr(centers), _ptr(nrm), np.inf, kdim, _ptr(Kc))
+            K = np.real(Kc).copy(order="F")
+        if np.any(np.isnan(S)) or np.any(np.isnan(K)):
+            raise FloatingPointError("Green function returned a NaN in the interaction matrix.")
+        if early_dot_product:
+            K = K.reshape((n, N), order="F")
+        return S, K
+
+    def evaluate(self, mesh1, mesh2, *, free_surface=0.0, water_depth=np.inf, wavenumber=1.0,
+                 adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True):
+        """delhommeau.py:405-520 (infinite depth)."""
+        if free_surface == np.inf:
+            if water_depth != np.inf:
+                raise ValueError("When setting free_surface=inf, the water depth should also be infinite")
+            return self.evaluate_rankine_only(mesh1, mesh2, adjoint_double_layer=adjoint_double_layer,
+                                              early_dot_product=early_dot_product)
+        if water_depth != np.inf:
+            raise NotImplementedError("finite depth is outside the oracle")
+        pts, nrm = self._colloc_and_normals(mesh1, mesh2, adjoint_double_layer)
+        n, N = pts.shape[0], mesh2.nb_faces
+        kdim = 1 if early_dot_product else 3
+        S = np.zeros((n, N), order="F", dtype=np.complex128)
+        K = np.zeros((kdim, n, N), order="F", dtype=np.complex128)
+        wavenumber = float(wavenumber)
+        if wavenumber == 0.0 and self.gf_singularities != "low_freq":
+            sing = "low_freq"
+        elif wavenumber == np.inf and self.gf_singularities != "high_freq":
+            sing = "high_freq"
+        elif np.any(abs(mesh2.faces_centers[:, 2]) < 1e-6) and self.gf_singularities != "low_freq":
+            sing = "low_freq"
+        else:
+            sing = self.gf_singularities
+        v, f, c, nn, a, r, nq, qp, qw = self._mesh_args(mesh2)
+        status = lib().oracle_build_matrices(n, _ptr(pts), _ptr(nrm), N, _ptr(v), _ptr(f), _ptr(c), _ptr(nn), _ptr(a),
+                                             _ptr(r), nq, _ptr(qp), _ptr(qw), wavenumber, float(water_depth),
+                                             *self._tab_args(), SING_ENUM[sing], int(adjoint_double_layer), kdim,
+                                             _ptr(S), _ptr(K), self.nthreads)
+        if status != 0:
+            raise RuntimeError(f"oracle_build_matrices failed with status {status}")
+        if diagonal_term_in_double_layer:
+            centers = _c(mesh2.faces_centers[:min(n, N)])
+            lib().oracle_add_diagonal_term(n, N, _ptr(centers), _ptr(nrm), float(free_surface), kdim, _ptr(K))
+        if early_dot_product:
+            K = K.reshape((n, N), order="F")
+        return S, K
+
+
+# ---------------------------------------------------------------------------
+# Solver glue
+@dataclass
+class Dof:
+    """Rigid-body dof: translation along ``direction`` or rotation about
+    ``direction`` through ``center`` (capytaine bodies/dofs.py:60-98)."""
+    kind: str
+    direction: Sequence[float]
+    center: Sequence[float] = (0.0, 0.0, 0.0)
+
+    def motion(self, points: np.ndarray) -> np.ndarray:
+        d = np.asarray(self.direction, float)
+        if self.kind == "translation":
+            return np.tile(d, (points.shape[0], 1))
+        return np.cross(d, points - np.asarray(self.center, float))
+
+
+def rigid_body_dofs(rotation_center=(0.0, 0.0, 0.0), only=None) -> Dict[str, Dof]:
+    """capytaine bodies/dofs.py:139-172"""
+    dofs = {
+        "Surge": Dof("translation", (1, 0, 0)),
+        "Sway": Dof("translation", (0, 1, 0)),
+        "Heave": Dof("translation", (0, 0, 1)),
+        "Roll": Dof("rotation", (1, 0, 0), rotation_center),
+        "Pitch": Dof("rotation", (0, 1, 0), rotation_center),
+        "Yaw": Dof("rotation", (0, 0, 1), rotation_center),
+    }
+    if only is not None:
+        dofs = {k: v for k, v in dofs.items() if k in only}
+    return dofs
+
+
+def airy_waves_velocity(points, omega, k, g, beta):
+    """airy_waves.py:56-95, infinite depth (k*h >= 20 branch)."""
+    x, y, z = points.T
+    wbar = x * np.cos(beta) + y * np.sin(beta)
+    cih = np.exp(k * z)
+    sih = np.exp(k * z)
+    v = g * k / omega * np.exp(1j * k * wbar) * np.array([np.cos(beta) * cih, np.sin(beta) * cih, -1j * sih])
+    return v.T
+
+
+def airy_waves_pressure(points, omega, k, g, rho, beta):
+    """airy_waves.py:19-53 and 98-99, infinite depth."""
+    x, y, z = points.T
+    wbar = x * np.cos(beta) + y * np.sin(beta)
+    phi = -1j * g / omega * np.exp(k * z) * np.exp(1j * k * wbar)
+    return 1j * omega * rho * phi
+
+
+def integrate_pressure(mesh, dofs: Dict[str, Dof], pressure):
+    """bodies/bodies.py:238-250"""
+    forces = {}
+    for name, dof in dofs.items():
+        m = dof.motion(mesh.faces_centers)
+        ndof = -np.sum(m * mesh.faces_normals, axis=1)
+        forces[name] = np.sum(pressure * ndof * mesh.faces_areas)
+    return forces
+
+
+def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: float, *, rho=1000.0, g=9.81,
+                    wave_directions=(0.0,), free_surface=0.0, linear_solver="lu"):
+    """One frequency-solve, indirect method (solver.py:188-207): assemble S and K at
+    k = omega^2/g, factor K once, solve every radiation and diffraction RHS, take
+    S @ sigma, integrate pressures.  Returns added mass, damping (dict of dict) and
+    excitation forces (dict heading -> dict dof -> complex)."""
+    import scipy.linalg as sl
+
+    k = omega ** 2 / g if free_surface != np.inf else 0.0
+    S, K = gf.evaluate(mesh, mesh, free_surface=free_surface, water_depth=np.inf, wavenumber=k,
+                       adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True)
+    lu = sl.lu_factor(K) if linear_solver == "lu" else None
+    normals = mesh.faces_normals
+    results = {"added_mass": {}, "radiation_damping": {}, "excitation": {}, "diffraction": {}, "froude_krylov": {}}
+    rhs_list = []
+    for name, dof in dofs.items():
+        disp = np.sum(dof.motion(mesh.faces_centers) * normals, axis=1)
+        rhs_list.append(("rad", name, -1j * omega * disp))
+    if free_surface != np.inf:
+        for beta in wave_directions:
+            bc = -(airy_waves_velocity(mesh.faces_centers, omega, k, g, beta) * normals).sum(axis=1)
+            rhs_list.append(("dif", beta, bc))
+    for kind, key, bc in rhs_list:
+        rhs = bc.astype(np.complex128)
+        sigma = sl.lu_solve(lu, rhs) if lu is not None else np.linalg.solve(K, rhs)
+        potential = S @ sigma
+        pressure = 1j * omega * rho * potential
+        forces = integrate_pressure(mesh, dofs, pressure)
+        if kind == "rad":
+            results["added_mass"][key] = {d: float(np.real(f) / omega ** 2) for d, f in forces.items()}
+            results["radiation_damping"][key] = {d: float(np.imag(f) / omega) for d, f in forces.items()}
+        else:
+            fk = integrate_pressure(mesh, dofs, airy_waves_pressure(mesh.faces_centers, omega, k, g, rho, key))
+            results["diffraction"][key] = forces
+            results["froude_krylov"][key] = fk
+            results["excitation"][key] = {d: forces[d] + fk[d] for d in forces}
+    return results
