@@ -1,0 +1,146 @@
+"""ctypes binding of ``libcapytaine_b200.so`` (declared in include/capytaine_b200.h).
+
+The product path always goes through this library.  There is no CPU fallback:
+importing works without a GPU (so the library and its symbols can be
+inspected), but every compute call raises when the library or a CUDA device is
+missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcapytaine_b200.so")
+
+BEM_OK = 0
+BEM_ERR_INVALID_ARGUMENT = 1
+BEM_ERR_CUDA = 2
+BEM_ERR_NAN = 3
+BEM_ERR_SINGULAR = 4
+BEM_ERR_NOT_CONVERGED = 5
+BEM_ERR_OUT_OF_MEMORY = 6
+BEM_ERR_UNSUPPORTED = 7
+BEM_ERR_TIMEOUT = 8
+
+BEM_GRID_LEGACY, BEM_GRID_SCALED_NEMOH3 = 0, 1
+BEM_GF_HIGH_FREQ, BEM_GF_LOW_FREQ, BEM_GF_LOW_FREQ_WITH_RANKINE_PART = 0, 1, 2
+BEM_DTYPE_C128, BEM_DTYPE_C64 = 0, 1
+BEM_PREC_FP64, BEM_PREC_MIXED = 0, 1
+
+
+class BemError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"[bem status {code}] {message}")
+        self.code = code
+
+
+class GreenFunctionEvaluationError(BemError):
+    """Same meaning as capytaine's GreenFunctionEvaluationError (NaN in a matrix)."""
+
+
+class SingularMatrixError(BemError):
+    pass
+
+
+class NotConvergedError(BemError):
+    pass
+
+
+c_int, c_i64, c_double, c_void_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+
+
+class AssemblyArgs(ctypes.Structure):
+    """Mirror of ``bem_assembly_args`` (include/capytaine_b200.h)."""
+    _fields_ = [
+        ("n", c_int), ("points_dev", c_void_p), ("dot_normals_dev", c_void_p),
+        ("nb_faces", c_int), ("nb_vertices", c_int), ("vertices_dev", c_void_p), ("faces_dev", c_void_p),
+        ("centers_dev", c_void_p), ("normals_dev", c_void_p), ("areas_dev", c_void_p), ("radii_dev", c_void_p),
+        ("nb_quad_points", c_int), ("quad_points_dev", c_void_p), ("quad_weights_dev", c_void_p),
+        ("tabulation_nb_integration_points", c_int), ("tabulation_grid_shape", c_int), ("nr", c_int), ("nz", c_int),
+        ("r_range_dev", c_void_p), ("z_range_dev", c_void_p), ("table_dev", c_void_p), ("table32_dev", c_void_p),
+        ("wavenumber", c_double), ("free_surface", c_double), ("gf_singularities", c_int),
+        ("adjoint_double_layer", c_int), ("early_dot_product", c_int), ("diagonal_term", c_int), ("precision", c_int),
+        ("out_dtype", c_int), ("S_dev", c_void_p), ("K_dev", c_void_p), ("lds", c_i64), ("ldk", c_i64),
+        ("k_plane_stride", c_i64), ("nan_flag_dev", c_void_p),
+    ]
+
+
+_SIGNATURES = {
+    "bem_last_error": ([], ctypes.c_char_p),
+    "bem_version": ([], c_int),
+    "bem_default_r_spacing": ([c_int, c_double, c_int, c_void_p], c_int),
+    "bem_default_z_spacing": ([c_int, c_double, c_int, c_void_p], c_int),
+    "bem_construct_tabulation": ([c_void_p, c_int, c_void_p, c_int, c_int, c_void_p, c_void_p], c_int),
+    "bem_assemble": ([ctypes.POINTER(AssemblyArgs), c_void_p], c_int),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def exported_symbols():
+    """Names of the C-ABI entry points this binding declares."""
+    return sorted(_SIGNATURES)
+
+
+def load(build_if_missing: bool = False):
+    """Load the shared library (optionally building it first)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            if build_if_missing:
+                from . import build as _build
+                _build.build()
+            else:
+                raise BemError(BEM_ERR_UNSUPPORTED,
+                               f"{LIB_PATH} is missing: build it with `python -m capytaine_b200.build`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+        return lib
+
+
+def check(status: int):
+    """Raise the exception matching a bem status code."""
+    if status == BEM_OK:
+        return
+    msg = load().bem_last_error().decode(errors="replace")
+    if status == BEM_ERR_NAN:
+        raise GreenFunctionEvaluationError(status, msg or "Green function returned a NaN in the interaction matrix.")
+    if status == BEM_ERR_SINGULAR:
+        raise SingularMatrixError(status, msg or "singular matrix")
+    if status == BEM_ERR_NOT_CONVERGED:
+        raise NotConvergedError(status, msg or "iterative refinement did not converge")
+    if status == BEM_ERR_OUT_OF_MEMORY:
+        raise MemoryError(msg)
+    raise BemError(status, msg)
+
+
+def call(name, *args):
+    check(getattr(load(), name)(*args))
+
+
+def require_cuda(device=None):
+    """Fail loudly when no CUDA device is usable: there is no CPU path."""
+    import torch
+    if not torch.cuda.is_available():
+        raise BemError(BEM_ERR_UNSUPPORTED, "capytaine_b200 needs a CUDA device (sm_100a); none is available")
+    load()
+    return torch.device(device if device is not None else "cuda")
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)

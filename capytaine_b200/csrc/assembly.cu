@@ -1,0 +1,511 @@
+// Assembly of the Delhommeau influence matrices S and K (or D, or the full
+// gradient) for one wavenumber in infinite depth.
+//
+// Replaces matrices::build_matrices, add_diagonal_term and add_rankine_term_only
+// (libs/libDelhommeau/src/matrices.f90:28-432) with the callees
+// Green_Rankine.f90:28-338 (exact and one-point Rankine integrals, reflected
+// through the free surface), Green_wave.f90:50-271 (wave term, free-surface
+// self-panel term) and Delhommeau_integrals.f90:157-402 (tabulation lookup,
+// asymptotic branch).
+//
+// Work decomposition: a CTA owns 128 consecutive collocation points (rows I) and
+// a tile of kTileJ source panels (columns J) staged in shared memory.  Each
+// thread walks its row across the tile, so each column store of a warp is 32
+// consecutive complex entries of the column-major output.
+//
+// Precision: BEM_PREC_FP64 evaluates every term in float64.  BEM_PREC_MIXED
+// evaluates the one-point (far-field) Rankine terms and the tabulated wave term
+// in float32 and keeps float64 for the exact near-field Rankine integrals
+// (panel pairs closer than 7 panel radii), whose log/atan terms are singular.
+#include <cmath>
+#include "integrals.cuh"
+
+namespace bem {
+namespace {
+
+constexpr int kRows = 128;   // threads per CTA = rows per CTA
+constexpr int kTileJ = 32;   // panels per CTA
+
+struct FaceRec {
+  double v[12];  // 4 vertices
+  double c[3];
+  double n[3];
+  double area;
+  double radius;
+  double q0[3];  // first quadrature point
+  double w0;     // its weight
+};
+
+// gfortran-compatible enough: plain Euclidean norms (last-ulp differences only).
+__device__ __forceinline__ double dnorm3(double x, double y, double z) { return sqrt(x * x + y * y + z * z); }
+
+// Green_Rankine.f90:68-157
+__device__ void exact_rankine(const double M[3], const FaceRec& f, bool deriv_first, double& G, double dG[3]) {
+  const double* c = f.c;
+  const double* n = f.n;
+  const double GZ = (M[0] - c[0]) * n[0] + (M[1] - c[1]) * n[1] + (M[2] - c[2]) * n[2];
+  double RR[4], DRX[4][3];
+#pragma unroll
+  for (int L = 0; L < 4; ++L) {
+    const double d0 = M[0] - f.v[3 * L], d1 = M[1] - f.v[3 * L + 1], d2 = M[2] - f.v[3 * L + 2];
+    RR[L] = dnorm3(d0, d1, d2);
+    const double inv = 1.0 / RR[L];
+    DRX[L][0] = d0 * inv;
+    DRX[L][1] = d1 * inv;
+    DRX[L][2] = d2 * inv;
+  }
+  G = 0.0;
+  dG[0] = dG[1] = dG[2] = 0.0;
+  const double sgn = copysign(1.0, GZ);
+  const double aGZ = fabs(GZ);
+  const bool use_atan = aGZ >= kLit1em4 * f.radius;
+#pragma unroll
+  for (int L = 0; L < 4; ++L) {
+    const int Ln = (L + 1) & 3;
+    const double e0 = f.v[3 * Ln] - f.v[3 * L], e1 = f.v[3 * Ln + 1] - f.v[3 * L + 1],
+                 e2 = f.v[3 * Ln + 2] - f.v[3 * L + 2];
+    const double DK = dnorm3(e0, e1, e2);
+    if (DK >= kLit1em3 * f.radius) {
+      const double PJ0 = e0 / DK, PJ1 = e1 / DK, PJ2 = e2 / DK;
+      const double GYX0 = n[1] * PJ2 - n[2] * PJ1;
+      const double GYX1 = n[2] * PJ0 - n[0] * PJ2;
+      const double GYX2 = n[0] * PJ1 - n[1] * PJ0;
+      const double GY = (M[0] - f.v[3 * L]) * GYX0 + (M[1] - f.v[3 * L + 1]) * GYX1 + (M[2] - f.v[3 * L + 2]) * GYX2;
+      const double S = RR[Ln] + RR[L];
+      const double ANT = 2 * GY * DK;
+      const double DNT = S * S - DK * DK + 2 * aGZ * S;
+      const double ANL = S + DK;
+      const double DNL = S - DK;
+      const double ALDEN = log(ANL / DNL);
+      const double AT = use_atan ? atan(ANT / DNT) : 0.0;
+      const double ANLX0 = DRX[Ln][0] + DRX[L][0], ANLX1 = DRX[Ln][1] + DRX[L][1], ANLX2 = DRX[Ln][2] + DRX[L][2];
+      const double two_dk = 2 * DK;
+      const double a1 = 2 * (S + aGZ), a2 = 2 * sgn * S;
+      const double DNTX0 = a1 * ANLX0 + a2 * n[0];
+      const double DNTX1 = a1 * ANLX1 + a2 * n[1];
+      const double DNTX2 = a1 * ANLX2 + a2 * n[2];
+      if (fabs(GY) < kLit1em5) {
+        G = G - 2 * AT * aGZ;
+      } else {
+        G = G + GY * ALDEN - 2 * AT * aGZ;
+      }
+      const double c1 = GY * (DNL - ANL) / (ANL * DNL);
+      const double cA = 2 * sgn * AT;
+      const double cB = 2 * aGZ / (ANT * ANT + DNT * DNT);
+      dG[0] = dG[0] + ALDEN * GYX0 - cA * n[0] + c1 * ANLX0 - cB * (two_dk * GYX0 * DNT - DNTX0 * ANT);
+      dG[1] = dG[1] + ALDEN * GYX1 - cA * n[1] + c1 * ANLX1 - cB * (two_dk * GYX1 * DNT - DNTX1 * ANT);
+      dG[2] = dG[2] + ALDEN * GYX2 - cA * n[2] + c1 * ANLX2 - cB * (two_dk * GYX2 * DNT - DNTX2 * ANT);
+    }
+  }
+  if (!deriv_first) {
+    dG[0] = -dG[0];
+    dG[1] = -dG[1];
+    dG[2] = -dG[2];
+  }
+}
+
+// Green_Rankine.f90:161-198 (derivative with respect to the first variable)
+// v = face centre - point, computed in float64 by the caller.
+template <class R>
+__device__ __forceinline__ void one_point_rankine(R v0, R v1, R v2, R area, R& G, R dG[3]) {
+  const R ro2 = v0 * v0 + v1 * v1 + v2 * v2;
+  const R ro = sqrt(ro2);
+  if (ro > (R)kLit1em7) {
+    G = area / ro;
+    const R s = G / ro2;
+    dG[0] = v0 * s;
+    dG[1] = v1 * s;
+    dG[2] = v2 * s;
+  } else {
+    G = 0;
+    dG[0] = dG[1] = dG[2] = 0;
+  }
+}
+
+__device__ __forceinline__ int f_nint(double x) {
+  if (!(fabs(x) < 2.0e9)) return (x > 0) ? 2000000000 : -2000000000;  // also NaN
+  return (int)round(x);
+}
+__device__ __forceinline__ int f_int(double x) {
+  if (!(fabs(x) < 2.0e9)) return (x > 0) ? 2000000000 : -2000000000;
+  return (int)trunc(x);
+}
+
+// Delhommeau_integrals.f90:301-363 (1-based indices)
+__device__ __forceinline__ int nearest_r_index(double r, int nr, double rmax, int grid) {
+  if (grid == kLegacyGrid) {
+    if (r < kLit1em6) return 1;
+    if (r < 1.0) return f_int(5 * (log10(r) + 6) + 1);
+    return f_int(3 * r + 28);
+  }
+  const int index_of_1 = (int)lroundf((float)(nr * 81) / 676.0f);
+  if (r < kLit1em10) return 1;
+  if (r < 1.0) return f_nint((log10(r) / 10.0 + 1.0) * (double)(index_of_1 - 1) + 1);
+  return f_nint((r - 1) * (double)(nr - index_of_1) / (rmax - 1) + (double)index_of_1);
+}
+__device__ __forceinline__ int nearest_z_index(double z, int nz, double zlast, int grid) {
+  const double absz = fabs(z);
+  if (grid == kLegacyGrid) {
+    if (absz > kLit1em2) return f_int(8 * (log10(absz) + 4.5));
+    return f_int(5 * (log10(absz) + 6));
+  }
+  const double dz = (log10(fabs(zlast)) + 10.0) / (double)nz;
+  return f_nint((log10(absz) + 10) / dz);
+}
+
+__device__ __forceinline__ double pl2(double u1, double u2, double u3, double x) {
+  return ((x - u1) * (x - u2)) / ((u3 - u1) * (u3 - u2));
+}
+
+// Delhommeau_integrals.f90:157-186
+template <class R>
+__device__ void asymptotic(R r, R z, R out[5]) {
+  const R one_over_r = (R)1 / fmax(r, (R)kLit1em10);
+  const R one_over_r1 = (R)1 / hypot(r, z);
+  const R expz_sqr = exp(z) * sqrt((R)(2 * kPI) * one_over_r);
+  R s, c;
+  sincos(r - (R)(kPI / 4), &s, &c);
+  const R r13 = one_over_r1 * one_over_r1 * one_over_r1;
+  out[0] = 2 * (-expz_sqr * s + z * r13 - one_over_r1);
+  out[1] = 2 * (-expz_sqr * s + z * r13);
+  out[2] = 2 * (expz_sqr * c);
+  out[3] = 2 * (-expz_sqr * (c - s * one_over_r / 2) + r * r13);
+  out[4] = 2 * (-expz_sqr * (s + c * one_over_r / 2));
+}
+
+struct TabView {
+  int npts, grid, nr, nz;
+  const double* r_range;
+  const double* z_range;
+  const double* tab;
+  const float* tab32;
+  double rmax, zlast;
+};
+
+// The five integrals at (r, z): table (3x3 Lagrange), asymptotic form or
+// direct integration (Green_wave.f90:226-240).
+template <class R>
+__device__ void integrals_at(double r, double z, const TabView& T, R out[5]) {
+  if (T.nz <= 1 || T.nr <= 1) {
+    double o[5];
+    numerical_integration_device(r, z, T.npts, o);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = (R)o[k];
+    return;
+  }
+  if (fabs(z) < fabs(T.zlast) && r < T.rmax) {
+    int i = nearest_r_index(r, T.nr, T.rmax, T.grid);
+    i = max(2, min(T.nr - 1, i));
+    int j = nearest_z_index(z, T.nz, T.zlast, T.grid);
+    j = max(2, min(T.nz - 1, j));
+    const int ic = i - 1, jc = j - 1;
+    const double r1 = __ldg(T.r_range + ic - 1), r2 = __ldg(T.r_range + ic), r3 = __ldg(T.r_range + ic + 1);
+    const double z1 = __ldg(T.z_range + jc - 1), z2 = __ldg(T.z_range + jc), z3 = __ldg(T.z_range + jc + 1);
+    const R xl0 = (R)pl2(r2, r3, r1, r), xl1 = (R)pl2(r3, r1, r2, r), xl2 = (R)pl2(r1, r2, r3, r);
+    const R zl0 = (R)pl2(z2, z3, z1, z), zl1 = (R)pl2(z3, z1, z2, z), zl2 = (R)pl2(z1, z2, z3, z);
+    R acc[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) acc[k] = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const size_t base = ((size_t)(ic - 1 + a) * T.nz + (jc - 1)) * kNbTab;
+      const R xa = (a == 0) ? xl0 : (a == 1) ? xl1 : xl2;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        R t0, t1, t2;
+        if constexpr (sizeof(R) == 8) {
+          t0 = __ldg(T.tab + base + k);
+          t1 = __ldg(T.tab + base + kNbTab + k);
+          t2 = __ldg(T.tab + base + 2 * kNbTab + k);
+        } else {
+          t0 = __ldg(T.tab32 + base + k);
+          t1 = __ldg(T.tab32 + base + kNbTab + k);
+          t2 = __ldg(T.tab32 + base + 2 * kNbTab + k);
+        }
+        acc[k] += xa * (t0 * zl0 + t1 * zl1 + t2 * zl2);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = acc[k];
+    return;
+  }
+  asymptotic<R>((R)r, (R)z, out);
+}
+
+// Green_wave.f90:162-271 at one quadrature point, multiplied by weight w.
+template <class R>
+__device__ void wave_part(const double x[3], const double xj[3], double k, const TabView& T, int sing, R w,
+                          R& Gre, R& Gim, R dGre[3], R dGim[3]) {
+  const double dx = x[0] - xj[0], dy = x[1] - xj[1];
+  const double r = k * sqrt(dx * dx + dy * dy);
+  const double z = k * (x[2] + xj[2]);
+  const R r1 = (R)hypot(r, z);
+  R drdx1 = 0, drdx2 = 0;
+  if (fabs(r) > 16 * kEpsilon) {
+    drdx1 = (R)(k * k * dx / r);
+    drdx2 = (R)(k * k * dy / r);
+  }
+  const R dzdx3 = (R)k;
+  R I[5];
+  integrals_at<R>(r, z, T, I);
+  R gre, gim = I[2];
+  R d0r, d1r, d2r;
+  const R d0i = drdx1 * I[4], d1i = drdx2 * I[4], d2i = dzdx3 * I[2];
+  if (sing == kHighFreq) {
+    gre = I[1];
+    const R r13 = r1 * r1 * r1;
+    d0r = drdx1 * I[3] - 2 * drdx1 * (R)r / r13;
+    d1r = drdx2 * I[3] - 2 * drdx2 * (R)r / r13;
+    d2r = dzdx3 * gre - 2 * dzdx3 * (R)z / r13;
+  } else {
+    gre = I[0];
+    d0r = drdx1 * I[3];
+    d1r = drdx2 * I[3];
+    d2r = (sing == kLowFreq) ? dzdx3 * (gre + 2 / r1) : dzdx3 * gre;
+  }
+  const R kw = (R)k * w;
+  Gre += kw * gre;
+  Gim += kw * gim;
+  dGre[0] += kw * d0r;
+  dGre[1] += kw * d1r;
+  dGre[2] += kw * d2r;
+  dGim[0] += kw * d0i;
+  dGim[1] += kw * d1i;
+  dGim[2] += kw * d2i;
+}
+
+template <class Out>
+struct OutT;
+template <>
+struct OutT<double2> {
+  __device__ static double2 make(double re, double im) { return make_double2(re, im); }
+};
+template <>
+struct OutT<float2> {
+  __device__ static float2 make(double re, double im) { return make_float2((float)re, (float)im); }
+};
+
+template <class Out, bool MIXED>
+__global__ void __launch_bounds__(kRows) assemble_kernel(const bem_assembly_args a, TabView T, double k_wave,
+                                                         int gf_sing, bool finite_k, double sign_refl) {
+  __shared__ FaceRec faces[kTileJ];
+  if (T.nr > 1 && T.nz > 1) {
+    // Grid bounds of the tabulation (last r and z values).
+    T.rmax = __ldg(T.r_range + T.nr - 1);
+    T.zlast = __ldg(T.z_range + T.nz - 1);
+  }
+  const int J0 = blockIdx.y * kTileJ;
+  const int nJ = min(kTileJ, a.nb_faces - J0);
+  // Stage the tile's panels: thread t fills face t (<= kTileJ faces).
+  if ((int)threadIdx.x < nJ) {
+    const int J = J0 + threadIdx.x;
+    FaceRec& f = faces[threadIdx.x];
+#pragma unroll
+    for (int L = 0; L < 4; ++L) {
+      const int v = a.faces_dev[4 * J + L];
+      f.v[3 * L] = a.vertices_dev[3 * v];
+      f.v[3 * L + 1] = a.vertices_dev[3 * v + 1];
+      f.v[3 * L + 2] = a.vertices_dev[3 * v + 2];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      f.c[d] = a.centers_dev[3 * J + d];
+      f.n[d] = a.normals_dev[3 * J + d];
+      f.q0[d] = a.quad_points_dev[(size_t)3 * a.nb_quad_points * J + d];
+    }
+    f.area = a.areas_dev[J];
+    f.radius = a.radii_dev[J];
+    f.w0 = a.quad_weights_dev[(size_t)a.nb_quad_points * J];
+  }
+  __syncthreads();
+  const int I = blockIdx.x * kRows + threadIdx.x;
+  if (I >= a.n) return;
+  const double M[3] = {a.points_dev[3 * I], a.points_dev[3 * I + 1], a.points_dev[3 * I + 2]};
+  const bool adjoint = a.adjoint_double_layer != 0;
+  double nI[3] = {0, 0, 0};
+  if (adjoint) {
+    nI[0] = a.dot_normals_dev[3 * I];
+    nI[1] = a.dot_normals_dev[3 * I + 1];
+    nI[2] = a.dot_normals_dev[3 * I + 2];
+  }
+  const bool rankine_only = isinf(a.free_surface);
+  const int diag_limit = min(a.n, a.nb_faces);
+  double diag_coef = 0.5;
+  if (a.diagonal_term && I < diag_limit) {
+    // matrices.f90:348 uses the centre of face i of mesh2
+    diag_coef = (fabs(a.centers_dev[3 * I + 2] - a.free_surface) < kLit1em8) ? 1.0 : 0.5;
+  }
+  Out* S = reinterpret_cast<Out*>(a.S_dev);
+  Out* K = reinterpret_cast<Out*>(a.K_dev);
+  bool nan_seen = false;
+  using R = typename std::conditional<MIXED, float, double>::type;
+
+  for (int jj = 0; jj < nJ; ++jj) {
+    const FaceRec& f = faces[jj];
+    const int J = J0 + jj;
+    // ---- Rankine term (exact near field, one point far field) ------------
+    double Gr = 0, dGr[3] = {0, 0, 0};
+    {
+      const double d0 = M[0] - f.c[0], d1 = M[1] - f.c[1], d2 = M[2] - f.c[2];
+      const double r0 = dnorm3(d0, d1, d2);
+      if (r0 > 7 * f.radius) {
+        R g, dg[3];
+        one_point_rankine<R>((R)-d0, (R)-d1, (R)-d2, (R)f.area, g, dg);
+        Gr = g;
+        dGr[0] = dg[0];
+        dGr[1] = dg[1];
+        dGr[2] = dg[2];
+      } else {
+        exact_rankine(M, f, true, Gr, dGr);
+      }
+    }
+    double Gre = Gr;
+    double dGre[3] = {dGr[0], dGr[1], dGr[2]};
+    double Gim = 0, dGim[3] = {0, 0, 0};
+    if (!rankine_only) {
+      // ---- reflected Rankine term, mirror z -> -z ---------------------------
+      double Gf, dGf[3];
+      {
+        const double dh = sqrt((M[0] - f.c[0]) * (M[0] - f.c[0]) + (M[1] - f.c[1]) * (M[1] - f.c[1]));
+        const double r1 = hypot(dh, -M[2] - f.c[2]);
+        const double Mr[3] = {M[0], M[1], -M[2]};
+        if (r1 > 7 * f.radius) {
+          R g, dg[3];
+          one_point_rankine<R>((R)(f.c[0] - Mr[0]), (R)(f.c[1] - Mr[1]), (R)(f.c[2] - Mr[2]), (R)f.area, g, dg);
+          Gf = g;
+          dGf[0] = dg[0];
+          dGf[1] = dg[1];
+          dGf[2] = dg[2];
+        } else {
+          exact_rankine(Mr, f, true, Gf, dGf);
+        }
+        dGf[2] = -dGf[2];  // reflection coefficient c0 = -1
+      }
+      Gre += sign_refl * Gf;
+      dGre[0] += sign_refl * dGf[0];
+      dGre[1] += sign_refl * dGf[1];
+      dGre[2] += sign_refl * dGf[2];
+      if (gf_sing == kLowFreqWithRankinePart) dGre[2] += 2 * k_wave * Gf;
+      // ---- wave term --------------------------------------------------------
+      if (finite_k) {
+        const double dxh = M[0] - f.c[0], dyh = M[1] - f.c[1];
+        const double rr = k_wave * sqrt(dxh * dxh + dyh * dyh);
+        const double zz = k_wave * (M[2] + f.c[2]);
+        if (fabs(rr) < kLit1em10 && fabs(zz) < kLit1em10) {
+          // Green_wave.f90:128-158, panel on the free surface with itself
+          const double re = (1 - log(k_wave * k_wave * f.area / kPI)) + 2 * (kEulerGamma - kLog2);
+          const double ka = k_wave * f.area;
+          const double gre = ka * re, gim = ka * (-2 * kPI);
+          Gre += gre;
+          Gim += gim;
+          dGre[2] += k_wave * (gre + 4 * sqrt(kPI * f.area));
+          dGim[2] += k_wave * gim;
+        } else {
+          R wr = 0, wi = 0, wdr[3] = {0, 0, 0}, wdi[3] = {0, 0, 0};
+          wave_part<R>(M, f.q0, k_wave, T, gf_sing, (R)f.w0, wr, wi, wdr, wdi);
+          for (int q = 1; q < a.nb_quad_points; ++q) {
+            const double* qp = a.quad_points_dev + ((size_t)a.nb_quad_points * J + q) * 3;
+            const double xq[3] = {qp[0], qp[1], qp[2]};
+            wave_part<R>(M, xq, k_wave, T, gf_sing, (R)a.quad_weights_dev[(size_t)a.nb_quad_points * J + q], wr, wi,
+                         wdr, wdi);
+          }
+          Gre += wr;
+          Gim += wi;
+          dGre[0] += wdr[0];
+          dGre[1] += wdr[1];
+          dGre[2] += wdr[2];
+          dGim[0] += wdi[0];
+          dGim[1] += wdi[1];
+          dGim[2] += wdi[2];
+        }
+      }
+    }
+    if (!adjoint) {
+      // Derivative with respect to the source point: Rankine gradient flips,
+      // the reflected and wave gradients flip horizontally only
+      // (Green_Rankine.f90:154-156, 289-294; Green_wave.f90:120-122).
+      // Recombine from the parts: the direct Rankine part flips fully.
+      dGre[0] = -dGre[0];
+      dGre[1] = -dGre[1];
+      dGim[0] = -dGim[0];
+      dGim[1] = -dGim[1];
+      dGre[2] = dGre[2] - 2 * dGr[2];
+    }
+    const double sre = kMinusOneOverFourPi * Gre, sim = kMinusOneOverFourPi * Gim;
+    const size_t sidx = (size_t)I + (size_t)a.lds * J;
+    S[sidx] = OutT<Out>::make(sre, sim);
+    nan_seen |= isnan(sre) || isnan(sim);
+    const bool on_diag = a.diagonal_term && I == J && I < diag_limit;
+    const size_t kidx = (size_t)I + (size_t)a.ldk * J;
+    if (a.early_dot_product) {
+      const double* dn = adjoint ? nI : (a.dot_normals_dev + 3 * J);
+      double kre = kMinusOneOverFourPi * (dn[0] * dGre[0] + dn[1] * dGre[1] + dn[2] * dGre[2]);
+      const double kim = kMinusOneOverFourPi * (dn[0] * dGim[0] + dn[1] * dGim[1] + dn[2] * dGim[2]);
+      if (on_diag) kre += diag_coef;
+      K[kidx] = OutT<Out>::make(kre, kim);
+      nan_seen |= isnan(kre) || isnan(kim);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double kre = kMinusOneOverFourPi * dGre[c];
+        const double kim = kMinusOneOverFourPi * dGim[c];
+        if (on_diag) kre += diag_coef * a.dot_normals_dev[3 * I + c];
+        K[kidx + (size_t)c * a.k_plane_stride] = OutT<Out>::make(kre, kim);
+        nan_seen |= isnan(kre) || isnan(kim);
+      }
+    }
+  }
+  if (nan_seen && a.nan_flag_dev) atomicOr(a.nan_flag_dev, 1);
+}
+
+}  // namespace
+}  // namespace bem
+
+extern "C" int bem_assemble(const bem_assembly_args* args, void* stream) {
+  using namespace bem;
+  if (!args) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: null args");
+  const bem_assembly_args& a = *args;
+  if (a.n < 0 || a.nb_faces < 0) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: negative size");
+  if (a.n == 0 || a.nb_faces == 0) return BEM_OK;
+  if (!a.points_dev || !a.vertices_dev || !a.faces_dev || !a.centers_dev || !a.normals_dev || !a.areas_dev ||
+      !a.radii_dev || !a.quad_points_dev || !a.quad_weights_dev || !a.S_dev || !a.K_dev)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: null pointer");
+  if (a.nb_quad_points < 1) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: nb_quad_points < 1");
+  if (a.lds < a.n || a.ldk < a.n) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: leading dimension < n");
+  if (!a.early_dot_product && a.k_plane_stride < a.ldk * (int64_t)a.nb_faces)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: gradient planes overlap");
+  if ((a.early_dot_product || a.diagonal_term) && !a.dot_normals_dev)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: dot_normals required");
+  const bool rankine_only = std::isinf(a.free_surface);
+  const bool finite_k = (a.wavenumber > 0.0) && std::isfinite(a.wavenumber);
+  const bool tabulated = a.nr > 1 && a.nz > 1;
+  if (!rankine_only && finite_k) {
+    if (tabulated && (!a.r_range_dev || !a.z_range_dev || !a.table_dev))
+      return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: tabulation pointers missing");
+    if (!tabulated && a.tabulation_nb_integration_points <= 0)
+      return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: nb_integration_points <= 0");
+    if (a.precision == BEM_PREC_MIXED && tabulated && !a.table32_dev)
+      return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: mixed precision needs the float32 table");
+  }
+  const TabView T{a.tabulation_nb_integration_points, a.tabulation_grid_shape, a.nr, a.nz, a.r_range_dev,
+                  a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0};
+  int gf_sing = a.gf_singularities;
+  // Singularity variant overrides of delhommeau.py:472-487.
+  if (a.wavenumber == 0.0) gf_sing = kLowFreq;
+  else if (std::isinf(a.wavenumber)) gf_sing = kHighFreq;
+  const double sign_refl = (gf_sing == kHighFreq) ? -1.0 : 1.0;
+  dim3 grid(ceil_div(a.n, kRows), ceil_div(a.nb_faces, kTileJ));
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool mixed = a.precision == BEM_PREC_MIXED;
+  if (a.out_dtype == BEM_DTYPE_C128) {
+    if (mixed) assemble_kernel<double2, true><<<grid, kRows, 0, s>>>(a, T, a.wavenumber, gf_sing, finite_k, sign_refl);
+    else assemble_kernel<double2, false><<<grid, kRows, 0, s>>>(a, T, a.wavenumber, gf_sing, finite_k, sign_refl);
+  } else if (a.out_dtype == BEM_DTYPE_C64) {
+    if (mixed) assemble_kernel<float2, true><<<grid, kRows, 0, s>>>(a, T, a.wavenumber, gf_sing, finite_k, sign_refl);
+    else assemble_kernel<float2, false><<<grid, kRows, 0, s>>>(a, T, a.wavenumber, gf_sing, finite_k, sign_refl);
+  } else {
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: unknown out_dtype");
+  }
+  BEM_CUDA_CHECK(cudaGetLastError());
+  return BEM_OK;
+}

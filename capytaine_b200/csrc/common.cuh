@@ -1,0 +1,51 @@
+// Shared device definitions for the capytaine_b200 kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/capytaine_b200.h"
+
+namespace bem {
+
+// Constants of libDelhommeau constants.f90:22-32.  The Fortran literals carry no
+// kind suffix, so they are single precision values promoted to double.
+constexpr double kPI = (double)(float)3.141592653588979;
+constexpr double kMinusOneOverFourPi = -1.0 / (4.0 * kPI);
+constexpr double kEulerGamma = (double)(float)0.5772156649;
+constexpr double kLog2 = 0.69314718055994530942;
+constexpr double kEpsilon = 2.220446049250313e-16;  // EPSILON(1d0)
+// Default-real thresholds of Green_Rankine.f90 / Green_wave.f90 / matrices.f90.
+constexpr double kLit1em3 = (double)1e-3f;
+constexpr double kLit1em4 = (double)1e-4f;
+constexpr double kLit1em5 = (double)1e-5f;
+constexpr double kLit1em6 = (double)1e-6f;
+constexpr double kLit1em7 = (double)1e-7f;
+constexpr double kLit1em8 = (double)1e-8f;
+constexpr double kLit1em10 = (double)1e-10f;
+constexpr double kLit1em2 = (double)1e-2f;
+
+constexpr int kNbTab = 5;
+constexpr int kLegacyGrid = 0;
+constexpr int kScaledNemoh3Grid = 1;
+constexpr int kHighFreq = 0;
+constexpr int kLowFreq = 1;
+constexpr int kLowFreqWithRankinePart = 2;
+
+struct c64d {
+  double re, im;
+};
+
+__host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Error recording shared by all entry points.
+int set_cuda_error(cudaError_t e, const char* where);
+int set_error(int code, const char* msg);
+
+}  // namespace bem
+
+#define BEM_CUDA_CHECK(call)                                  \
+  do {                                                        \
+    cudaError_t _e = (call);                                  \
+    if (_e != cudaSuccess) return bem::set_cuda_error(_e, #call); \
+  } while (0)

@@ -1,0 +1,122 @@
+/* capytaine_b200 — C ABI of the B200 (sm_100a) Delhommeau BEM hot path.
+ *
+ * Every entry point takes plain pointers and sizes.  Pointers named *_dev are
+ * CUDA device pointers (any allocator: torch, cudaMalloc, cupy); pointers named
+ * *_host are host pointers.  `stream` is a cudaStream_t passed as void* (NULL =
+ * legacy default stream).  Work is enqueued on the stream; functions return
+ * before it completes unless stated otherwise.  Every function returns a
+ * status code (BEM_OK = 0); bem_last_error() gives a message for the calling
+ * thread.
+ *
+ * Array conventions follow capytaine: points and vectors are (n, 3) row-major
+ * float64; faces are (N, 4) int32, 0-based, triangles stored with their last
+ * vertex repeated (capytaine meshes/meshes.py:454-469); influence matrices are
+ * column-major (Fortran order) complex arrays, entry (I, J) at I + J*ld.
+ */
+#ifndef CAPYTAINE_B200_H
+#define CAPYTAINE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------- */
+#define BEM_OK 0
+#define BEM_ERR_INVALID_ARGUMENT 1
+#define BEM_ERR_CUDA 2
+#define BEM_ERR_NAN 3             /* NaN in an influence matrix (engines.py:400-405)   */
+#define BEM_ERR_SINGULAR 4        /* zero pivot in the LU factorisation                */
+#define BEM_ERR_NOT_CONVERGED 5   /* iterative refinement / GMRES did not converge    */
+#define BEM_ERR_OUT_OF_MEMORY 6
+#define BEM_ERR_UNSUPPORTED 7     /* option outside the implemented path (finite depth) */
+#define BEM_ERR_TIMEOUT 8         /* a bounded device-side wait gave up                */
+
+/* ---- enums (values of libDelhommeau constants.f90:40-52) ------------------ */
+#define BEM_GRID_LEGACY 0
+#define BEM_GRID_SCALED_NEMOH3 1
+#define BEM_GF_HIGH_FREQ 0
+#define BEM_GF_LOW_FREQ 1
+#define BEM_GF_LOW_FREQ_WITH_RANKINE_PART 2
+
+#define BEM_DTYPE_C128 0          /* complex128 outputs                               */
+#define BEM_DTYPE_C64 1           /* complex64 outputs                                */
+
+#define BEM_PREC_FP64 0           /* every term in float64                            */
+#define BEM_PREC_MIXED 1          /* float32 far field and wave term, float64 near field */
+
+/* Message describing the last error raised on the calling thread. */
+const char* bem_last_error(void);
+/* Library version, major*10000 + minor*100 + patch. */
+int bem_version(void);
+
+/* ---- tabulation of the Delhommeau integrals ------------------------------- */
+/* Grid of the tabulation.  Replace delhommeau_integrals::default_r_spacing and
+ * default_z_spacing (libs/libDelhommeau/src/Delhommeau_integrals.f90:208-270),
+ * called from capytaine green_functions/delhommeau.py:253-258.  Host output. */
+int bem_default_r_spacing(int nr, double rmax, int grid_shape, double* r_range_host);
+int bem_default_z_spacing(int nz, double zmin, int grid_shape, double* z_range_host);
+
+/* Five tabulated integrals on the (r, z) grid by Simpson integration over theta.
+ * Replaces delhommeau_integrals::construct_tabulation
+ * (Delhommeau_integrals.f90:43-153,190-204), called from delhommeau.py:259-261.
+ * table_dev: float64, C-order (nr, nz, 5). */
+int bem_construct_tabulation(const double* r_range_dev, int nr, const double* z_range_dev, int nz,
+                             int nb_integration_points, double* table_dev, void* stream);
+
+/* ---- assembly of the influence matrices ----------------------------------- */
+typedef struct {
+  /* collocation side (mesh1 or a raw list of points) */
+  int32_t n;                       /* number of collocation points (rows)                      */
+  const double* points_dev;        /* (n, 3)                                                   */
+  const double* dot_normals_dev;   /* (n, 3) if adjoint_double_layer else (nb_faces, 3)        */
+  /* source side (mesh2) */
+  int32_t nb_faces;                /* columns                                                  */
+  int32_t nb_vertices;
+  const double* vertices_dev;      /* (nb_vertices, 3)                                         */
+  const int32_t* faces_dev;        /* (nb_faces, 4), 0-based                                   */
+  const double* centers_dev;       /* (nb_faces, 3)                                            */
+  const double* normals_dev;       /* (nb_faces, 3)                                            */
+  const double* areas_dev;         /* (nb_faces)                                               */
+  const double* radii_dev;         /* (nb_faces)                                               */
+  int32_t nb_quad_points;
+  const double* quad_points_dev;   /* (nb_faces, nb_quad_points, 3)                            */
+  const double* quad_weights_dev;  /* (nb_faces, nb_quad_points)                               */
+  /* tabulation (nr or nz <= 1 selects direct integration, as the reference) */
+  int32_t tabulation_nb_integration_points;
+  int32_t tabulation_grid_shape;
+  int32_t nr;
+  int32_t nz;
+  const double* r_range_dev;
+  const double* z_range_dev;
+  const double* table_dev;         /* (nr, nz, 5) C-order float64                              */
+  const float* table32_dev;        /* optional float32 copy for BEM_PREC_MIXED (may be NULL)   */
+  /* problem */
+  double wavenumber;               /* 0 and +inf are allowed (no wave term)                    */
+  double free_surface;             /* +inf: Rankine kernel only (no free surface)              */
+  int32_t gf_singularities;        /* BEM_GF_*                                                 */
+  int32_t adjoint_double_layer;    /* 1: K (derivative w.r.t. collocation point), 0: D          */
+  int32_t early_dot_product;       /* 1: K (n, N); 0: three gradient planes                    */
+  int32_t diagonal_term;           /* add 1/2 (1 on free-surface panels) on the diagonal       */
+  int32_t precision;               /* BEM_PREC_*                                               */
+  /* outputs */
+  int32_t out_dtype;               /* BEM_DTYPE_*                                              */
+  void* S_dev;                     /* (n, N) column-major, leading dimension lds               */
+  void* K_dev;                     /* (n, N) column-major (ldk), or 3 planes ldk*N apart       */
+  int64_t lds;
+  int64_t ldk;
+  int64_t k_plane_stride;          /* elements between gradient planes when !early_dot_product */
+  int32_t* nan_flag_dev;           /* optional: set to 1 if a NaN was produced                  */
+} bem_assembly_args;
+
+/* S and K (or D, or the full gradient) for one wavenumber, infinite depth.
+ * Replaces matrices::build_matrices, add_diagonal_term and add_rankine_term_only
+ * (libs/libDelhommeau/src/matrices.f90:28-432), called from capytaine
+ * green_functions/delhommeau.py:377-390 and 498-515. */
+int bem_assemble(const bem_assembly_args* args, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CAPYTAINE_B200_H */
