@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Frequency-solves per second of the B200 BEM engines on the 6084-panel barge.
+
+Workload (one frequency-solve): assemble S and K of the Delhommeau Green
+function at k = omega^2/g, factor K, solve the 6 rigid-body radiation problems
+and the diffraction problem (heading 0), potentials S @ sigma, pressure
+integration -> added mass, damping, excitation.  Barge 80 x 20 m, draft 10 m,
+6084 panels, omega in linspace(0.05, 3, 60), infinite depth, rho 1000, g 9.81.
+A step is one batch of `--batch` frequencies taken in order from the sweep.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--engine fp64|mixed]
+    python bench.py --impl reference     # CPU reference (oracle port) arm
+
+Multi-GPU (torchrun, one process per GPU): frequencies are independent units,
+each rank solves its own share with no data-path collective (weak scaling);
+the only collectives are the timing barrier and the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "freq solves/sec at N=6000, refined-mixed vs FP64 LU at 1e-5 err; p50/p99 latency"
+UNIT = "freq-solves/s"
+OMEGAS = np.linspace(0.05, 3.0, 60)
+RHO, G = 1000.0, 9.81
+
+
+def barge_body():
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.meshes import mesh_parallelepiped
+    mesh = mesh_parallelepiped(size=(80, 20, 20), resolution=(104, 26, 26)).immersed_part()
+    return FloatingBody(mesh, rigid_body_dofs(rotation_center=(0.0, 0.0, 0.0)), name="barge")
+
+
+def workload_config(args, n):
+    return {"workload": "barge 80x20x10m, 6 dofs + diffraction (heading 0), omega linspace(0.05,3,60)",
+            "nb_panels": int(n), "frequencies_per_step": int(args.batch), "engine": args.engine,
+            "depth": "infinite", "l2": "inputs larger than L2 (K: 604 MB complex128 per frequency)",
+            "parallelism": f"frequency shards x{args.world}"}
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device_index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        out["samples"] = len(rows)
+        out["sm_mhz"] = float(np.median(sm)) if sm else None
+        out["sm_max_mhz"] = float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        out["reasons"] = sorted(reasons)
+        out["power_w_max"] = max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit()) \
+            if any(r[3].replace(".", "").isdigit() for r in rows) else None
+        return out
+
+
+def measured_peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def fp64_tensor_peak_tflops():
+    """cuBLAS DGEMM 8192^3 best of 5 in this run: FP64 has no entry in the
+    measured-peaks file, so the float64 roofline denominator is measured here."""
+    import torch
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    best = 0.0
+    for _ in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_solve(body, omega, gf_oracle):
+    """One frequency-solve with the oracle port (C++ OpenMP assembly + SciPy LU)."""
+    from oracle import oracle as O
+    odofs = {name: O.Dof("translation" if type(d).__name__ == "TranslationDof" else "rotation", d.direction,
+                         getattr(d, "rotation_center", (0.0, 0.0, 0.0))) for name, d in body.dofs.items()}
+    return O.solve_frequency(gf_oracle, body.mesh, odofs, omega, rho=RHO, g=G, wave_directions=(0.0,))
+
+
+def oracle_gf():
+    from oracle import oracle as O
+    O.build_oracle()
+    return O.OracleDelhommeau(nthreads=0)
+
+
+def coefficient_error(res, idx, ref):
+    """Max over A, B, F_exc of |c - c_ref| / max(|c_ref|, 1e-3 max|C_ref|)."""
+    dofs = list(res.dofs)
+    A = np.array([[ref["added_mass"][i][j] for j in dofs] for i in dofs])
+    B = np.array([[ref["radiation_damping"][i][j] for j in dofs] for i in dofs])
+    E = np.array([[ref["excitation"][0.0][j] for j in dofs]])
+    errs = {}
+    for name, got, r in (("added_mass", res.added_mass[idx], A), ("radiation_damping", res.radiation_damping[idx], B),
+                         ("excitation", res.excitation[idx], E)):
+        floor = 1e-3 * np.abs(r).max()
+        errs[name] = float(np.max(np.abs(got - r) / np.maximum(np.abs(r), floor)))
+    return errs
+
+
+def run_reference(args):
+    """--impl reference: the oracle port on the host cores, one frequency per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = len(os.sched_getaffinity(0))
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    body = barge_body()
+    gf = oracle_gf()
+    times = []
+    for step in range(args.warmup + args.steps):
+        w = float(OMEGAS[step % len(OMEGAS)])
+        t0 = time.perf_counter()
+        cpu_reference_solve(body, w, gf)
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = len(times) / total
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": workload_config(args, body.mesh.nb_faces) | {"engine": "oracle port (C++ OpenMP + SciPy LU)",
+                                                                    "frequencies_per_step": 1},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{len(times)} frequency-solves of the 6084-panel barge, one per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=15)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--engine", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    world = args.world
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    from capytaine_b200 import _lib
+    from capytaine_b200.engine import B200Engine
+    from capytaine_b200.green_function import Delhommeau
+
+    body = barge_body()
+    n = body.mesh_including_lid.nb_faces
+    gf = Delhommeau(tabulation_cache_dir=None, precision=args.engine)
+    engine = B200Engine(green_function=gf, precision=args.engine, max_batch=args.batch)
+    # this rank's share of the sweep: frequencies rank, rank + world, ...
+    my_omegas = OMEGAS[rank::world]
+    nb = args.batch
+    batches = [my_omegas[(s * nb + np.arange(nb)) % len(my_omegas)] for s in range(args.warmup + args.steps)]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-resident timing (value) ----------------------------------
+    lib = _lib.load()
+    for s in range(args.warmup):
+        engine.solve_frequencies(body, batches[s])
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.bem_launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    step_ms = []
+    ev0.record()
+    for s in range(args.warmup, args.warmup + args.steps):
+        e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_a.record()
+        res = engine.solve_frequencies(body, batches[s])
+        e_b.record()
+        step_ms.append((e_a, e_b))
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = lib.bem_launch_count() - launches0
+    barrier()
+    clocks = sampler.stop()
+    t_ms = ev0.elapsed_time(ev1)
+    lat = np.array([a.elapsed_time(b) for a, b in step_ms])
+    if dist is not None:
+        t = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    total_solves = args.steps * nb * world
+    value = total_solves / (t_ms * 1e-3)
+
+    # ---- per-stage times and the roofline of the dominant kernel ----------
+    st = engine.solve_frequencies(body, batches[0], sync_stats=True).stats
+    stage = max(("assembly_ms", "lu_ms", "solve_ms", "post_ms"), key=lambda k: st[k])
+    npad = -(-n // 64) * 64
+    peaks, peak_src = measured_peaks()
+    if stage == "lu_ms":
+        p64 = fp64_tensor_peak_tflops()
+        flops = 8 * npad ** 3 / 3 * nb
+        achieved = flops / (st["lu_ms"] * 1e-3) / 1e12
+        roofline = {"kernel": "zgemm_dmma_kernel (LU trailing updates, float64 tensor-core MMA)", "bound": "tensor",
+                    "achieved": achieved, "peak": p64, "unit": "TFLOP/s", "frac": achieved / p64, "traffic": None,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (float64 has no entry in "
+                                   "MEASURED_PEAKS.json)",
+                    "algorithmic": "8 n^3 / 3 real flops per complex LU, n = 6144 (padded)"}
+    else:
+        bytes_ = 32.0 * n * n * nb
+        achieved = bytes_ / (st["assembly_ms"] * 1e-3) / 1e9
+        roofline = {"kernel": "assemble_kernel (S and K of one frequency)", "bound": "hbm", "achieved": achieved,
+                    "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                    "peak_source": f"{peak_src} hbm_gbs", "algorithmic": "32 bytes (complex128 S and K) per panel pair"}
+
+    # ---- end to end through the public API with host buffers --------------
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for s in range(args.warmup, args.warmup + args.steps):
+        gf._mesh_cache.clear()  # mesh arrays come from host memory every step
+        r = engine.solve_frequencies(body, batches[s])
+        m = body.mesh_including_lid
+        h2d += 8 * (m.vertices.size + 3 * 3 * m.nb_faces + 2 * m.nb_faces + 4 * m.nb_faces) + 4 * m.faces.size
+        h2d += 8 * (2 * len(body.dofs) * m.nb_faces) + 4 * m.nb_faces + 8 * (2 * nb + 1)
+        d2h += 16 * nb * (len(body.dofs) + 1) * len(body.dofs) * 2 + 4 * (nb + 2)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": total_solves / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d / args.steps),
+           "d2h_bytes_per_step": int(d2h / args.steps)}
+
+    # ---- CPU baseline (oracle port on the host cores) and accuracy --------
+    cpu = None
+    accuracy = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = len(os.sched_getaffinity(0))
+        gfo = oracle_gf()
+        w = float(OMEGAS[20])
+        t0 = time.perf_counter()
+        ref = cpu_reference_solve(body, w, gfo)
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": 1.0 / cpu_s, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"1 frequency-solve (omega={w:.3f}) of the 6084-panel barge"}
+        got = engine.solve_frequencies(body, [w])
+        accuracy = {"omega": w, "max_rel_err_vs_oracle": coefficient_error(got, 0, ref),
+                    "note": "GPU-built tabulation vs oracle-built tabulation"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c128" if args.engine == "fp64" else "c128/f32",
+                "data": "synthetic", "config": workload_config(args, n), "roofline": roofline,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+                "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                               "unit": f"ms per step of {nb} frequencies"},
+                "stages_ms_per_step": {k: round(v, 3) for k, v in st.items()}, "accuracy": accuracy}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -70,10 +70,27 @@ class AssemblyArgs(ctypes.Structure):
 _SIGNATURES = {
     "bem_last_error": ([], ctypes.c_char_p),
     "bem_version": ([], c_int),
+    "bem_launch_count": ([], ctypes.c_longlong),
     "bem_default_r_spacing": ([c_int, c_double, c_int, c_void_p], c_int),
     "bem_default_z_spacing": ([c_int, c_double, c_int, c_void_p], c_int),
     "bem_construct_tabulation": ([c_void_p, c_int, c_void_p, c_int, c_int, c_void_p, c_void_p], c_int),
     "bem_assemble": ([ctypes.POINTER(AssemblyArgs), c_void_p], c_int),
+    "bem_zpad_identity": ([c_void_p, c_i64, c_i64, c_int, c_int, c_int, c_void_p], c_int),
+    "bem_zgemm": ([c_int, c_int, c_int, c_double, c_void_p, c_i64, c_i64, c_void_p, c_i64, c_i64, c_double,
+                   c_void_p, c_i64, c_i64, c_int, c_void_p], c_int),
+    "bem_zlu_workspace_bytes": ([c_int, c_int], c_i64),
+    "bem_zlu_factor": ([c_void_p, c_int, c_i64, c_i64, c_int, c_void_p, c_void_p, c_void_p, c_void_p], c_int),
+    "bem_zlu_solve": ([c_void_p, c_int, c_i64, c_i64, c_int, c_void_p, c_void_p, c_void_p, c_i64, c_i64, c_int,
+                       c_void_p, c_void_p], c_int),
+    "bem_build_rhs": ([c_int, c_int, c_void_p, c_void_p, c_double, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                       c_void_p, c_void_p, c_void_p, c_i64, c_i64, c_void_p], c_int),
+    "bem_zgemm_ts_workspace_bytes": ([c_int, c_int, c_int, c_int], c_i64),
+    "bem_zgemm_ts": ([c_int, c_int, c_int, c_double, c_double, c_void_p, c_i64, c_i64, c_void_p, c_i64, c_i64,
+                      c_double, c_double, c_void_p, c_i64, c_i64, c_int, c_void_p, c_void_p], c_int),
+    "bem_integrate_pressure": ([c_int, c_int, c_int, c_int, c_void_p, c_i64, c_i64, c_void_p, c_double, c_void_p,
+                                c_void_p, c_void_p], c_int),
+    "bem_froude_krylov": ([c_int, c_int, c_int, c_int, c_void_p, c_double, c_double, c_void_p, c_void_p,
+                           c_void_p, c_void_p, c_void_p], c_int),
 }
 
 _lock = threading.Lock()

@@ -36,8 +36,38 @@ struct FaceRec {
   double w0;     // its weight
 };
 
-// gfortran-compatible enough: plain Euclidean norms (last-ulp differences only).
+// Plain Euclidean norm, used inside the exact integrals (last-ulp differences only).
 __device__ __forceinline__ double dnorm3(double x, double y, double z) { return sqrt(x * x + y * y + z * z); }
+
+// Fortran NORM2 with gfortran's scaled accumulation, every operation rounded
+// on its own.  The near/far switch `r0 > 7*radius` (Green_Rankine.f90:50,227)
+// meets exact ties on regular meshes (panel pairs exactly 7 radii apart); this
+// norm makes the tie resolve the same way as in the CPU restatement.
+__device__ __forceinline__ double norm2_scaled(const double* x, int n) {
+  double scale = 0.0, result = 1.0;
+  for (int i = 0; i < n; ++i) {
+    if (x[i] != 0.0) {
+      const double ax = fabs(x[i]);
+      if (scale < ax) {
+        const double v = __ddiv_rn(scale, ax);
+        result = __dadd_rn(1.0, __dmul_rn(__dmul_rn(result, v), v));
+        scale = ax;
+      } else {
+        const double v = __ddiv_rn(ax, scale);
+        result = __dadd_rn(result, __dmul_rn(v, v));
+      }
+    }
+  }
+  return __dmul_rn(scale, __dsqrt_rn(result));
+}
+__device__ __forceinline__ double norm2_3(double a, double b, double c) {
+  const double v[3] = {a, b, c};
+  return norm2_scaled(v, 3);
+}
+__device__ __forceinline__ double norm2_2(double a, double b) {
+  const double v[2] = {a, b};
+  return norm2_scaled(v, 2);
+}
 
 // Green_Rankine.f90:68-157
 __device__ void exact_rankine(const double M[3], const FaceRec& f, bool deriv_first, double& G, double dG[3]) {
@@ -237,7 +267,7 @@ template <class R>
 __device__ void wave_part(const double x[3], const double xj[3], double k, const TabView& T, int sing, R w,
                           R& Gre, R& Gim, R dGre[3], R dGim[3]) {
   const double dx = x[0] - xj[0], dy = x[1] - xj[1];
-  const double r = k * sqrt(dx * dx + dy * dy);
+  const double r = k * norm2_2(dx, dy);
   const double z = k * (x[2] + xj[2]);
   const R r1 = (R)hypot(r, z);
   R drdx1 = 0, drdx2 = 0;
@@ -347,7 +377,7 @@ __global__ void __launch_bounds__(kRows) assemble_kernel(const bem_assembly_args
     double Gr = 0, dGr[3] = {0, 0, 0};
     {
       const double d0 = M[0] - f.c[0], d1 = M[1] - f.c[1], d2 = M[2] - f.c[2];
-      const double r0 = dnorm3(d0, d1, d2);
+      const double r0 = norm2_3(d0, d1, d2);
       if (r0 > 7 * f.radius) {
         R g, dg[3];
         one_point_rankine<R>((R)-d0, (R)-d1, (R)-d2, (R)f.area, g, dg);
@@ -366,7 +396,7 @@ __global__ void __launch_bounds__(kRows) assemble_kernel(const bem_assembly_args
       // ---- reflected Rankine term, mirror z -> -z ---------------------------
       double Gf, dGf[3];
       {
-        const double dh = sqrt((M[0] - f.c[0]) * (M[0] - f.c[0]) + (M[1] - f.c[1]) * (M[1] - f.c[1]));
+        const double dh = norm2_2(M[0] - f.c[0], M[1] - f.c[1]);
         const double r1 = hypot(dh, -M[2] - f.c[2]);
         const double Mr[3] = {M[0], M[1], -M[2]};
         if (r1 > 7 * f.radius) {
@@ -389,7 +419,7 @@ __global__ void __launch_bounds__(kRows) assemble_kernel(const bem_assembly_args
       // ---- wave term --------------------------------------------------------
       if (finite_k) {
         const double dxh = M[0] - f.c[0], dyh = M[1] - f.c[1];
-        const double rr = k_wave * sqrt(dxh * dxh + dyh * dyh);
+        const double rr = k_wave * norm2_2(dxh, dyh);
         const double zz = k_wave * (M[2] + f.c[2]);
         if (fabs(rr) < kLit1em10 && fabs(zz) < kLit1em10) {
           // Green_wave.f90:128-158, panel on the free surface with itself
@@ -506,6 +536,7 @@ extern "C" int bem_assemble(const bem_assembly_args* args, void* stream) {
   } else {
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: unknown out_dtype");
   }
+  count_launches(1);
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
 }

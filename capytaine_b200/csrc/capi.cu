@@ -2,12 +2,15 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <atomic>
 #include "common.cuh"
 
 namespace bem {
 namespace {
 thread_local std::string g_last_error;
 }
+std::atomic<long long> g_launches{0};
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int set_error(int code, const char* msg) {
   g_last_error = msg ? msg : "";
@@ -27,3 +30,5 @@ int set_cuda_error(cudaError_t e, const char* where) {
 extern "C" const char* bem_last_error(void) { return bem::g_last_error.c_str(); }
 
 extern "C" int bem_version(void) { return 100; }
+
+extern "C" long long bem_launch_count(void) { return bem::g_launches.load(std::memory_order_relaxed); }

@@ -41,6 +41,8 @@ __host__ __device__ inline int ceil_div(long long a, long long b) { return (int)
 // Error recording shared by all entry points.
 int set_cuda_error(cudaError_t e, const char* where);
 int set_error(int code, const char* msg);
+// Running count of kernels this library has launched (bem_launch_count).
+void count_launches(int n);
 
 }  // namespace bem
 

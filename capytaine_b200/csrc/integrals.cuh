@@ -77,7 +77,12 @@ __device__ inline c64d exp_e1(double zr, double zi) {
     q = cf_mul(z, cf_radd(0.28388363e+00f, q));
     q = cf_mul(z, cf_radd(-0.76273617e+00f, q));
     q = cf_radd(0.1e+01f, q);
-    cf lz{logf(hypotf(z.re, z.im)), atan2f(z.im, z.re)};
+    // Complex logarithm of a float value: modulus rounded to float, then the
+    // float-rounded log and argument evaluated in double precision.  This
+    // tracks the host C library's clogf (what gfortran calls for LOG of a
+    // COMPLEX(4)) to a few 1e-9 over the whole default tabulation.
+    const float modulus = (float)sqrt((double)z.re * (double)z.re + (double)z.im * (double)z.im);
+    cf lz{(float)log((double)modulus), (float)atan2((double)z.im, (double)z.re)};
     cf num = cf_add(cf_mul(lz, p1), cf_rmul(0.5772156649e+00f, p2));
     cf r = cf_div(num, q);
     g = cf{-r.re, -r.im};

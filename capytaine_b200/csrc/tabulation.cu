@@ -80,6 +80,7 @@ extern "C" int bem_construct_tabulation(const double* r_range_dev, int nr, const
   const int threads = 128;
   bem::tabulation_kernel<<<bem::ceil_div(cells, threads), threads, 0, (cudaStream_t)stream>>>(
       r_range_dev, nr, z_range_dev, nz, npts, table_dev);
+  bem::count_launches(1);
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
 }

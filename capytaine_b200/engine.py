@@ -1,0 +1,377 @@
+"""Matrix engine on the B200: device-resident S/K, batched LU, frequency solves.
+
+Two entry points:
+
+* ``B200Engine.solve_frequencies(body, omegas, ...)``: the whole indirect
+  solve of many frequencies of one body, batched on the device (assembly of S
+  and K at k = omega^2/g, LU of K, every radiation and diffraction RHS, S @ sigma,
+  pressure integration) with only the coefficients coming back to the host.
+  One frequency-solve is what capytaine does for one (body, omega) group in
+  ``BEMSolver.solve_all`` (bem/solver.py:268-372, problems grouped by
+  bem/problems_and_results.py:267-275).
+* the ``MatrixEngine`` interface of capytaine (bem/engines.py:46-59, 142-176,
+  273-346, 348-398): ``build_matrices`` returns device-backed matrices whose
+  ``@`` and whose LU (``linear_solver``) run on the GPU, so capytaine's own
+  ``BEMSolver`` can use this engine unchanged.
+"""
+from __future__ import annotations
+
+import ctypes
+import logging
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .green_function import Delhommeau
+
+LOG = logging.getLogger(__name__)
+
+NB = 64  # LU block size; matrices are padded to a multiple of it
+
+
+def padded_size(n: int) -> int:
+    return int(math.ceil(n / NB) * NB)
+
+
+def _vp(x):
+    return ctypes.c_void_p(x.data_ptr() if hasattr(x, "data_ptr") else int(x))
+
+
+@dataclass
+class FrequencyResults:
+    """Coefficients of a frequency sweep.  Arrays are indexed [omega, ...]:
+    added_mass / radiation_damping [omega, radiating_dof, influenced_dof],
+    diffraction / froude_krylov / excitation [omega, heading, influenced_dof]."""
+    omegas: np.ndarray
+    dofs: List[str]
+    wave_directions: np.ndarray
+    added_mass: np.ndarray
+    radiation_damping: np.ndarray
+    diffraction: np.ndarray
+    froude_krylov: np.ndarray
+    excitation: np.ndarray
+    stats: Dict[str, float] = field(default_factory=dict)
+
+    def coefficients(self) -> Dict[str, np.ndarray]:
+        return dict(added_mass=self.added_mass, radiation_damping=self.radiation_damping,
+                    excitation=self.excitation)
+
+
+class _Workspace:
+    """Device buffers of one (n, batch, nrhs) shape, reused across batches."""
+
+    def __init__(self, n, batch, nrhs, device, precision):
+        import torch
+        self.n, self.batch, self.nrhs = n, batch, nrhs
+        self.npad = padded_size(n)
+        npad = self.npad
+        c128 = dict(dtype=torch.complex128, device=device)
+        self.K = torch.empty((batch, npad * npad), **c128)
+        self.S = torch.empty((batch, n * n), **c128)
+        self.B = torch.zeros((batch, npad * nrhs), **c128)
+        self.phi = torch.empty((batch, n * nrhs), **c128)
+        self.piv = torch.empty((batch, npad), dtype=torch.int32, device=device)
+        self.info = torch.zeros(batch, dtype=torch.int32, device=device)
+        self.err = torch.zeros(1, dtype=torch.int32, device=device)
+        self.nan = torch.zeros(1, dtype=torch.int32, device=device)
+        lib = _lib.load()
+        self.lu_work = torch.empty(int(lib.bem_zlu_workspace_bytes(npad, batch)), dtype=torch.uint8, device=device)
+        self.ts_work = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, min(nrhs, 16), batch)),
+                                   dtype=torch.uint8, device=device)
+
+    @property
+    def nbytes(self):
+        return sum(t.numel() * t.element_size() for t in (self.K, self.S, self.B, self.phi, self.lu_work,
+                                                           self.ts_work))
+
+
+class B200Engine:
+    """capytaine-compatible matrix engine running the Delhommeau assembly and the
+    dense solves on one B200.
+
+    precision: "fp64" (float64 assembly, float64 LU) or "mixed" (float32 far
+    field / wave term with float64 near field, low-precision tensor-core LU,
+    float64-residual GMRES iterative refinement).
+    """
+
+    def __init__(self, *, green_function: Optional[Delhommeau] = None, precision: str = "fp64",
+                 linear_solver: str = "lu_decomposition", max_batch: int = 8, device=None):
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.precision = precision
+        self.green_function = green_function if green_function is not None else Delhommeau(precision=precision)
+        self._linear_solver = linear_solver
+        self.max_batch = int(max_batch)
+        self._device = device
+        self._ws: Dict[tuple, _Workspace] = {}
+        self.last_computed_inputs = None
+        self.last_computed_matrices = None
+        self.exportable_settings = {
+            "engine": "B200Engine",
+            "linear_solver": str(linear_solver),
+            "precision": precision,
+            **self.green_function.exportable_settings,
+        }
+
+    def __str__(self):
+        return f"B200Engine(green_function={self.green_function}, precision={self.precision!r})"
+
+    __repr__ = __str__
+
+    @property
+    def device(self):
+        return _lib.require_cuda(self._device)
+
+    def workspace(self, n, batch, nrhs) -> _Workspace:
+        key = (n, batch, nrhs)
+        ws = self._ws.get(key)
+        if ws is None:
+            self._ws.clear()  # one resident shape at a time (memory)
+            ws = _Workspace(n, batch, nrhs, self.device, self.precision)
+            self._ws[key] = ws
+        return ws
+
+    # ------------------------------------------------------------------------
+    # Batched frequency solves
+    def solve_frequencies(self, body, omegas: Sequence[float], *, wave_directions: Sequence[float] = (0.0,),
+                          rho: float = 1000.0, g: float = 9.81, batch: Optional[int] = None,
+                          sync_stats: bool = False) -> FrequencyResults:
+        import torch
+        dev = self.device
+        mesh = body.mesh_including_lid
+        n = mesh.nb_faces
+        omegas = np.asarray(omegas, dtype=float)
+        heads = np.asarray(wave_directions, dtype=float)
+        ndof, nhead = len(body.dofs), len(heads)
+        nrhs = ndof + nhead
+        if nrhs > 16:
+            raise ValueError("at most 16 right-hand sides per frequency (dofs + headings)")
+        B = min(self.max_batch if batch is None else batch, len(omegas))
+        ws = self.workspace(n, B, nrhs)
+        npad = ws.npad
+        lib = _lib.load()
+        stream = _lib.stream_ptr()
+        gf = self.green_function
+        dm = gf.device_mesh(mesh)
+        dofn = torch.as_tensor(body.dof_normal_components(), dtype=torch.float64, device=dev).contiguous()
+        wdof = torch.as_tensor(body.pressure_weights(), dtype=torch.float64, device=dev).contiguous()
+        hull = torch.as_tensor(body.hull_mask.astype(np.int32), device=dev)
+        heads_t = torch.as_tensor(heads, dtype=torch.float64, device=dev)
+        F_all = np.zeros((len(omegas), nrhs, ndof), dtype=np.complex128)
+        FK_all = np.zeros((len(omegas), max(nhead, 1), ndof), dtype=np.complex128)
+        stats = {"assembly_ms": 0.0, "lu_ms": 0.0, "solve_ms": 0.0, "post_ms": 0.0}
+        for start in range(0, len(omegas), B):
+            om = omegas[start:start + B]
+            nb = len(om)
+            ks = om ** 2 / g
+            om_t = torch.as_tensor(om, dtype=torch.float64, device=dev)
+            k_t = torch.as_tensor(ks, dtype=torch.float64, device=dev)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)] if sync_stats else None
+            if ev:
+                ev[0].record()
+            ws.nan.zero_()
+            for b in range(nb):
+                gf.assemble_into(mesh, mesh, ws.S[b], ws.K[b], wavenumber=float(ks[b]), lds=n, ldk=npad,
+                                 nan_flag=ws.nan, precision="fp64")
+            _lib.check(lib.bem_zpad_identity(_vp(ws.K), npad, npad * npad, nb, n, npad, stream))
+            if ev:
+                ev[1].record()
+            _lib.check(lib.bem_zlu_factor(_vp(ws.K), npad, npad, npad * npad, nb, _vp(ws.piv), _vp(ws.info),
+                                          _vp(ws.lu_work), stream))
+            if ev:
+                ev[2].record()
+            ws.B.zero_()
+            ws.err.zero_()
+            _lib.check(lib.bem_build_rhs(n, nb, _vp(om_t), _vp(k_t), g, ndof, _vp(dofn), nhead, _vp(heads_t),
+                                         _vp(dm.centers), _vp(dm.normals), _vp(hull), _vp(ws.B), npad, npad * nrhs,
+                                         stream))
+            _lib.check(lib.bem_zlu_solve(_vp(ws.K), npad, npad, npad * npad, nb, _vp(ws.piv), _vp(ws.lu_work),
+                                         _vp(ws.B), npad, npad * nrhs, nrhs, _vp(ws.err), stream))
+            if ev:
+                ev[3].record()
+            _lib.check(lib.bem_zgemm_ts(n, n, nrhs, 1.0, 0.0, _vp(ws.S), n, n * n, _vp(ws.B), npad, npad * nrhs,
+                                        0.0, 0.0, _vp(ws.phi), n, n * nrhs, nb, _vp(ws.ts_work), stream))
+            F = torch.empty((nb, nrhs, ndof), dtype=torch.complex128, device=dev)
+            _lib.check(lib.bem_integrate_pressure(n, nb, nrhs, ndof, _vp(ws.phi), n, n * nrhs, _vp(om_t), rho,
+                                                  _vp(wdof), _vp(F), stream))
+            if nhead > 0:
+                FK = torch.empty((nb, nhead, ndof), dtype=torch.complex128, device=dev)
+                _lib.check(lib.bem_froude_krylov(n, nb, ndof, nhead, _vp(k_t), rho, g, _vp(heads_t),
+                                                 _vp(dm.centers), _vp(wdof), _vp(FK), stream))
+                FK_all[start:start + nb, :nhead] = FK.cpu().numpy()
+            if ev:
+                ev[4].record()
+            F_all[start:start + nb] = F.cpu().numpy()
+            flags = torch.cat([ws.info, ws.err, ws.nan]).cpu().numpy()
+            if ev:
+                torch.cuda.synchronize()
+                stats["assembly_ms"] += ev[0].elapsed_time(ev[1])
+                stats["lu_ms"] += ev[1].elapsed_time(ev[2])
+                stats["solve_ms"] += ev[2].elapsed_time(ev[3])
+                stats["post_ms"] += ev[3].elapsed_time(ev[4])
+            if flags[nb + 1] != 0:
+                raise _lib.GreenFunctionEvaluationError(_lib.BEM_ERR_NAN, "Green function returned a NaN in the "
+                                                        "interaction matrix.\nIt could be due to overlapping panels.")
+            if np.any(flags[:nb] != 0):
+                raise _lib.SingularMatrixError(_lib.BEM_ERR_SINGULAR,
+                                               f"zero pivot in the LU factorisation (info={flags[:nb].tolist()})")
+            if flags[nb] != 0:
+                raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
+        return self._coefficients(body, omegas, heads, F_all, FK_all, stats)
+
+    @staticmethod
+    def _coefficients(body, omegas, heads, F_all, FK_all, stats):
+        ndof = len(body.dofs)
+        w = omegas[:, None, None]
+        rad = F_all[:, :ndof, :]
+        added_mass = np.real(rad) / w ** 2
+        damping = np.imag(rad) / w
+        diffraction = F_all[:, ndof:, :]
+        fk = FK_all[:, : len(heads), :]
+        return FrequencyResults(omegas=omegas, dofs=list(body.dofs), wave_directions=heads, added_mass=added_mass,
+                                radiation_damping=damping, diffraction=diffraction, froude_krylov=fk,
+                                excitation=diffraction + fk, stats=stats)
+
+    # ------------------------------------------------------------------------
+    # capytaine MatrixEngine interface
+    def build_matrices(self, mesh1, mesh2, **gf_params):
+        """bem/engines.py:273-298 with a single-entry cache (:258-270)."""
+        key = (mesh1, mesh2, dict(gf_params))
+        if key == self.last_computed_inputs:
+            return self.last_computed_matrices
+        self.last_computed_matrices = None
+        params = dict(gf_params)
+        params.setdefault("early_dot_product", True)
+        S, K = self.green_function.evaluate_device(mesh1, mesh2, **params)
+        self.last_computed_inputs = key
+        self.last_computed_matrices = (DeviceMatrix(S, self), DeviceMatrix(K, self))
+        return self.last_computed_matrices
+
+    def build_S_matrix(self, points, mesh, **gf_params):
+        S, _ = self.green_function.evaluate_device(points, mesh, **gf_params)
+        return DeviceMatrix(S, self)
+
+    def build_fullK_matrix(self, mesh1, mesh2, **gf_params):
+        gf_params.setdefault("diagonal_term_in_double_layer", True)
+        gf_params.setdefault("adjoint_double_layer", True)
+        gf_params["early_dot_product"] = False
+        _, K = self.green_function.evaluate_device(mesh1, mesh2, **gf_params)
+        return K.cpu().numpy()
+
+    def linear_solver(self, A, b):
+        """bem/engines.py:300-346: LU of A on the device, cached on A (the cache
+        entry replaces K, as the reference does), one RHS per call."""
+        if not isinstance(A, DeviceMatrix):
+            A = DeviceMatrix(_to_device(np.asarray(A), self.device), self)
+        x = A.solve(np.asarray(b))
+        if x.shape != np.asarray(b).shape:
+            raise ValueError("linear solver output shape mismatch")
+        return x
+
+    def compute_ram_estimation(self, problem):
+        """Device memory (GB) of S, K and the LU (bem/engines.py:348-398, no symmetry)."""
+        n = problem.body.mesh_including_lid.nb_faces if hasattr(problem.body, "mesh_including_lid") \
+            else problem.body.mesh.nb_faces
+        return 3 * 16 * padded_size(n) ** 2 / 1e9
+
+
+def _to_device(a: np.ndarray, device):
+    import torch
+    t = torch.as_tensor(np.asfortranarray(a), device=device)
+    return t
+
+
+class DeviceMatrix:
+    """A device-resident influence matrix usable where capytaine expects an
+    ndarray: ``M @ x`` and ``engine.linear_solver(M, b)`` run on the GPU."""
+
+    def __init__(self, t, engine: B200Engine):
+        self.t = t  # (n, N) view, column-major
+        self.engine = engine
+        self._lu = None
+
+    @property
+    def shape(self):
+        return tuple(self.t.shape)
+
+    @property
+    def dtype(self):
+        return np.dtype(str(self.t.dtype).replace("torch.", ""))
+
+    def __array__(self, dtype=None, copy=None):
+        a = self.t.cpu().numpy()
+        return a.astype(dtype) if dtype is not None else a
+
+    def __matmul__(self, x):
+        import torch
+        x = np.asarray(x)
+        vec = x.ndim == 1
+        X = x.reshape(x.shape[0], -1).astype(np.complex128)
+        n, K = self.t.shape
+        nrhs = X.shape[1]
+        # Explicit column-major buffers: element (i, c) at i + c*ld (reported strides
+        # of size-1 dimensions are not reliable leading dimensions).
+        Acm = torch.empty((K, n), dtype=torch.complex128, device=self.t.device)  # Acm[j, i] = A[i, j]
+        Acm.copy_(self.t.T)
+        Xcm = torch.as_tensor(np.ascontiguousarray(X.T), device=Acm.device)   # Xcm[c, k] = X[k, c]
+        Ycm = torch.empty((nrhs, n), dtype=torch.complex128, device=Acm.device)
+        lib = _lib.load()
+        for c0 in range(0, nrhs, 16):
+            c1 = min(nrhs, c0 + 16)
+            work = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, K, c1 - c0, 1)), dtype=torch.uint8,
+                               device=Acm.device)
+            _lib.check(lib.bem_zgemm_ts(n, K, c1 - c0, 1.0, 0.0, _vp(Acm), n, 0, _vp(Xcm[c0:c1]), K, 0, 0.0, 0.0,
+                                        _vp(Ycm[c0:c1]), n, 0, 1, _vp(work), _lib.stream_ptr()))
+        res = Ycm.T.cpu().numpy()
+        if self.t.dtype == torch.complex64:
+            res = res.astype(np.complex64)
+        return res[:, 0] if vec else res.reshape((n,) + x.shape[1:])
+
+    def _factor(self):
+        import torch
+        if self._lu is not None:
+            return self._lu
+        n = self.t.shape[0]
+        npad = padded_size(n)
+        dev = self.t.device
+        lib = _lib.load()
+        # Column-major npad x npad buffer: element (r, c) at r + c*npad, i.e. Kf.T[r, c].
+        Kf = torch.zeros((npad, npad), dtype=torch.complex128, device=dev)
+        Kf.T[:n, :n] = self.t.to(torch.complex128)
+        _lib.check(lib.bem_zpad_identity(_vp(Kf), npad, npad * npad, 1, n, npad, _lib.stream_ptr()))
+        piv = torch.empty(npad, dtype=torch.int32, device=dev)
+        info = torch.zeros(1, dtype=torch.int32, device=dev)
+        work = torch.empty(int(lib.bem_zlu_workspace_bytes(npad, 1)), dtype=torch.uint8, device=dev)
+        _lib.check(lib.bem_zlu_factor(_vp(Kf), npad, npad, npad * npad, 1, _vp(piv), _vp(info), _vp(work),
+                                      _lib.stream_ptr()))
+        if int(info.item()) != 0:
+            raise _lib.SingularMatrixError(_lib.BEM_ERR_SINGULAR, f"zero pivot at column {int(info.item())}")
+        self._lu = (Kf, piv, work, npad)
+        return self._lu
+
+    def solve(self, b: np.ndarray) -> np.ndarray:
+        import torch
+        Kf, piv, work, npad = self._factor()
+        b = np.asarray(b)
+        vec = b.ndim == 1
+        Bm = b.reshape(b.shape[0], -1).astype(np.complex128)
+        n, nrhs = Bm.shape
+        dev = Kf.device
+        lib = _lib.load()
+        out = np.empty_like(Bm)
+        for c0 in range(0, nrhs, 64):
+            c1 = min(nrhs, c0 + 64)
+            Bd = torch.zeros((c1 - c0, npad), dtype=torch.complex128, device=dev)  # column-major npad x nrhs
+            Bd[:, :n] = torch.as_tensor(Bm[:, c0:c1].T.copy(), device=dev)
+            err = torch.zeros(1, dtype=torch.int32, device=dev)
+            _lib.check(lib.bem_zlu_solve(_vp(Kf), npad, npad, npad * npad, 1, _vp(piv), _vp(work), _vp(Bd), npad,
+                                         npad * (c1 - c0), c1 - c0, _vp(err), _lib.stream_ptr()))
+            if int(err.item()) != 0:
+                raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
+            out[:, c0:c1] = Bd[:, :n].T.cpu().numpy()
+        x = out[:, 0] if vec else out.reshape(b.shape)
+        return x.astype(np.complex64) if self.t.dtype == torch.complex64 else x

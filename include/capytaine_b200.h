@@ -50,6 +50,9 @@ extern "C" {
 const char* bem_last_error(void);
 /* Library version, major*10000 + minor*100 + patch. */
 int bem_version(void);
+/* Number of kernels this library has launched since it was loaded (all devices,
+ * all threads): instrumentation for benchmarks. */
+long long bem_launch_count(void);
 
 /* ---- tabulation of the Delhommeau integrals ------------------------------- */
 /* Grid of the tabulation.  Replace delhommeau_integrals::default_r_spacing and
@@ -115,6 +118,70 @@ typedef struct {
  * (libs/libDelhommeau/src/matrices.f90:28-432), called from capytaine
  * green_functions/delhommeau.py:377-390 and 498-515. */
 int bem_assemble(const bem_assembly_args* args, void* stream);
+
+/* ---- dense complex128 linear algebra (batched) ---------------------------- */
+/* Matrices are column-major complex128 (interleaved re, im), `batch` of them
+ * `stride` elements apart.  n must be a multiple of 64: pad the system with the
+ * identity (bem_zpad_identity) and the right-hand sides with zeros. */
+
+/* Zero rows and columns n..npad-1 and put ones on their diagonal. */
+int bem_zpad_identity(void* A_dev, int64_t lda, int64_t stride, int batch, int n, int npad, void* stream);
+
+/* C = alpha A B + beta C (alpha, beta real), float64 tensor-core MMAs. */
+int bem_zgemm(int M, int N, int K, double alpha, const void* A_dev, int64_t lda, int64_t strideA,
+              const void* B_dev, int64_t ldb, int64_t strideB, double beta, void* C_dev, int64_t ldc,
+              int64_t strideC, int batch, void* stream);
+
+/* Workspace of bem_zlu_factor / bem_zlu_solve in bytes (inverted diagonal
+ * blocks and completion flags). */
+int64_t bem_zlu_workspace_bytes(int n, int batch);
+
+/* In-place LU factorisation P A = L U, partial pivoting within each 64-row
+ * diagonal block.  Replaces LAPACK zgetrf behind scipy.linalg.lu_factor
+ * (capytaine tools/block_circulant_matrices.py:361-378, bem/engines.py:326-338).
+ * piv_dev: batch x n ints (row permutation inside each block); info_dev: batch
+ * ints, 0 or the 1-based column of the first zero pivot (as LAPACK's info). */
+int bem_zlu_factor(void* A_dev, int n, int64_t lda, int64_t stride, int batch, int* piv_dev, int* info_dev,
+                   void* work_dev, void* stream);
+
+/* Solve A X = B in place for nrhs <= 64 columns with the factors of
+ * bem_zlu_factor.  Replaces LAPACK zgetrs behind scipy.linalg.lu_solve
+ * (tools/block_circulant_matrices.py:382-385).  err_dev: one int set to 1 when
+ * a bounded wait of the persistent kernel timed out (result invalid). */
+int bem_zlu_solve(const void* A_dev, int n, int64_t lda, int64_t stride, int batch, const int* piv_dev,
+                  const void* work_dev, void* B_dev, int64_t ldb, int64_t strideB, int nrhs, int* err_dev,
+                  void* stream);
+
+/* ---- right-hand sides, potentials, forces --------------------------------- */
+/* Columns 0..ndof-1: radiation BC -1j*omega*(dof . n) (dofn_dev: ndof x n);
+ * columns ndof..ndof+nhead-1: diffraction BC -(u_Airy . n), infinite depth.
+ * Zero where hull_dev[i] == 0 (lid panels; hull_dev may be NULL).  One batch
+ * entry per frequency (omega_dev, wavenumber_dev: batch doubles).
+ * Replaces bem/problems_and_results.py:373-381, 440-449 and
+ * bem/airy_waves.py:56-95. */
+int bem_build_rhs(int n, int batch, const double* omega_dev, const double* wavenumber_dev, double g, int ndof,
+                  const double* dofn_dev, int nhead, const double* headings_dev, const double* centers_dev,
+                  const double* normals_dev, const int32_t* hull_dev, void* B_dev, int64_t ldb, int64_t strideB,
+                  void* stream);
+
+/* Y = alpha A X + beta Y, A (M x K) complex128, X (K x nrhs), nrhs <= 16:
+ * the potential S @ sigma (bem/solver.py:197-198) and residuals. */
+int64_t bem_zgemm_ts_workspace_bytes(int M, int K, int nrhs, int batch);
+int bem_zgemm_ts(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
+                 int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re, double beta_im,
+                 void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev, void* stream);
+
+/* F[b][c][d] = i omega_b rho sum_i phi[b][i][c] wdof[d][i] with
+ * wdof[d][i] = -(dof_d . n_i) area_i on hull panels (0 on lid panels).
+ * Replaces bodies/bodies.py:238-250 applied to bem/solver.py:199-207. */
+int bem_integrate_pressure(int n, int batch, int nrhs, int ndof, const void* phi_dev, int64_t ldp, int64_t strideP,
+                           const double* omega_dev, double rho, const double* wdof_dev, void* F_dev, void* stream);
+
+/* Froude-Krylov force of each heading: F[b][h][d] = sum_i p0_i wdof[d][i],
+ * p0 = rho g exp(k z) exp(i k (x cos beta + y sin beta)) (airy_waves.py:19-53,98-102). */
+int bem_froude_krylov(int n, int batch, int ndof, int nhead, const double* wavenumber_dev, double rho, double g,
+                      const double* headings_dev, const double* centers_dev, const double* wdof_dev, void* F_dev,
+                      void* stream);
 
 #ifdef __cplusplus
 }

@@ -22,6 +22,7 @@
 #include <cstring>
 #include <climits>
 #include <omp.h>
+#include <complex>
 
 namespace {
 
@@ -74,8 +75,9 @@ inline C smith_div(T a, T b, T c, T d) {
 inline c32 cdiv(c32 x, c32 y) { return smith_div<f32, c32>(x.re, x.im, y.re, y.im); }
 inline c64 cdiv64(c64 x, c64 y) { return smith_div<f64, c64>(x.re, x.im, y.re, y.im); }
 inline c32 clog32(c32 z) {
-  // Principal complex logarithm in single precision.
-  return {std::log(std::hypot(z.re, z.im)), std::atan2(z.im, z.re)};
+  // LOG of a COMPLEX(4) value: gfortran calls the C library's clogf.
+  std::complex<float> w = std::log(std::complex<float>(z.re, z.im));
+  return {w.real(), w.imag()};
 }
 
 // gfortran NORM2: scaled sum of squares.
