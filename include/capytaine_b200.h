@@ -183,6 +183,21 @@ int bem_froude_krylov(int n, int batch, int ndof, int nhead, const double* waven
                       const double* headings_dev, const double* centers_dev, const double* wdof_dev, void* F_dev,
                       void* stream);
 
+/* ---- allocation-free variant ---------------------------------------------- */
+/* No counterpart in the reference.  Same operation and arguments as
+ * bem_zgemm_ts without the workspace: for callers that can only pass buffers
+ * they already own (a fixed device pool that allows no further allocation, or
+ * a loop where a cudaMalloc is unacceptable).  The split-K partial sums live in
+ * a static device array of bem_zgemm_ts_static_capacity() = 524288 complex128
+ * entries (8 MiB, held on every GPU that loads the library until exit);
+ * M * nrhs * batch must not exceed it (else BEM_ERR_INVALID_ARGUMENT).  The
+ * first call on a device looks the array up (make it before any stream
+ * capture); calls that overlap on the GPU share the array and race. */
+int64_t bem_zgemm_ts_static_capacity(void);
+int bem_zgemm_ts_static(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
+                        int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,
+                        double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
