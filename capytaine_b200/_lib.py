@@ -89,6 +89,8 @@ _SIGNATURES = {
                       c_double, c_double, c_void_p, c_i64, c_i64, c_int, c_void_p, c_void_p], c_int),
     "bem_integrate_pressure": ([c_int, c_int, c_int, c_int, c_void_p, c_i64, c_i64, c_void_p, c_double, c_void_p,
                                 c_void_p, c_void_p], c_int),
+    "bem_cgemm_tf32_update": ([c_void_p, c_i64, c_int, c_void_p, c_i64, c_int, c_int, c_void_p, c_void_p, c_i64,
+                               c_i64, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p], c_int),
     "bem_zgemm_ts_static_capacity": ([], c_i64),
     "bem_zgemm_ts_static": ([c_int, c_int, c_int, c_double, c_double, c_void_p, c_i64, c_i64, c_void_p, c_i64, c_i64,
                              c_double, c_double, c_void_p, c_i64, c_i64, c_int, c_void_p], c_int),

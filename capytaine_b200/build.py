@@ -83,7 +83,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     with cf.ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
         list(ex.map(run, jobs))
     if force or jobs or not os.path.exists(LIB):
-        link = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-lcuda"]
+        link = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
         run(link)
     return LIB
 

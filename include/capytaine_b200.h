@@ -183,6 +183,22 @@ int bem_froude_krylov(int n, int batch, int ndof, int nhead, const double* waven
                       const double* headings_dev, const double* centers_dev, const double* wdof_dev, void* F_dev,
                       void* stream);
 
+/* ---- tensor-core complex update (mixed precision) ------------------------- */
+/* C -= A B for complex A (m x k) and B (k x n) on the tcgen05 tensor cores with
+ * TF32 inputs and FP32 accumulation, C stored as two float32 planes (Cr, Ci),
+ * column-major with leading dimension ldc, trailing block starting at
+ * (c_row0, c_col0), m and n multiples of 128.  Operands are packed K-major with
+ * K' = kp = 2k (multiple of 32):
+ *   Aop[b][a_row0 + i][:] = [Re A(i, :), Im A(i, :)]
+ *   Bop[b][b_row0 + 2*j0 + t][:]       = [Re B(:, j0+t); -Im B(:, j0+t)]
+ *   Bop[b][b_row0 + 2*j0 + 128 + t][:] = [Im B(:, j0+t);  Re B(:, j0+t)]
+ * for each group of 128 columns j0 and t < 128.  err_dev is set to 1 when a
+ * bounded wait inside the kernel gave up.  This is the trailing update of the
+ * mixed-precision LU that replaces zgetrf's (tools/block_circulant_matrices.py:378). */
+int bem_cgemm_tf32_update(const float* Aop_dev, int64_t a_rows, int a_row0, const float* Bop_dev, int64_t b_rows,
+                          int b_row0, int kp, float* Cr_dev, float* Ci_dev, int64_t ldc, int64_t c_stride,
+                          int c_row0, int c_col0, int m, int n, int batch, int* err_dev, void* stream);
+
 /* ---- allocation-free variant ---------------------------------------------- */
 /* No counterpart in the reference.  Same operation and arguments as
  * bem_zgemm_ts without the workspace: for callers that can only pass buffers
