@@ -114,6 +114,27 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
+def tf32_tensor_peak_tflops():
+    """cuBLAS TF32 GEMM 8192^3 best of 5 in this run (TF32 has no entry in the
+    measured-peaks file)."""
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    a = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
+    best = 0.0
+    for _ in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    return best
+
+
 def fp64_tensor_peak_tflops():
     """cuBLAS DGEMM 8192^3 best of 5 in this run: FP64 has no entry in the
     measured-peaks file, so the float64 roofline denominator is measured here."""
@@ -225,7 +246,7 @@ def main():
 
     body = barge_body()
     n = body.mesh_including_lid.nb_faces
-    gf = Delhommeau(tabulation_cache_dir=None, precision=args.engine)
+    gf = Delhommeau(tabulation_cache_dir=None)
     engine = B200Engine(green_function=gf, precision=args.engine, max_batch=args.batch)
     # this rank's share of the sweep: frequencies rank, rank + world, ...
     my_omegas = OMEGAS[rank::world]
@@ -275,7 +296,7 @@ def main():
     stage = max(("assembly_ms", "lu_ms", "solve_ms", "post_ms"), key=lambda k: st[k])
     npad = -(-n // 64) * 64
     peaks, peak_src = measured_peaks()
-    if stage == "lu_ms":
+    if stage == "lu_ms" and args.engine == "fp64":
         p64 = fp64_tensor_peak_tflops()
         flops = 8 * npad ** 3 / 3 * nb
         achieved = flops / (st["lu_ms"] * 1e-3) / 1e12
@@ -284,6 +305,16 @@ def main():
                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (float64 has no entry in "
                                    "MEASURED_PEAKS.json)",
                     "algorithmic": "8 n^3 / 3 real flops per complex LU, n = 6144 (padded)"}
+    elif stage == "lu_ms":
+        npad128 = -(-n // 128) * 128
+        ptf = tf32_tensor_peak_tflops()
+        flops = 8 * npad128 ** 3 / 3 * nb
+        achieved = flops / (st["lu_ms"] * 1e-3) / 1e12
+        roofline = {"kernel": "cgemm_tf32_update_kernel (LU trailing updates, tcgen05 TF32)", "bound": "tensor",
+                    "achieved": achieved, "peak": ptf, "unit": "TFLOP/s", "frac": achieved / ptf, "traffic": None,
+                    "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run (TF32 has no entry in "
+                                   "MEASURED_PEAKS.json)",
+                    "algorithmic": "8 n^3 / 3 real flops per complex LU (complex count), n = 6144 (padded)"}
     else:
         bytes_ = 32.0 * n * n * nb
         achieved = bytes_ / (st["assembly_ms"] * 1e-3) / 1e9
@@ -336,7 +367,8 @@ def main():
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                                "unit": f"ms per step of {nb} frequencies"},
-                "stages_ms_per_step": {k: round(v, 3) for k, v in st.items()}, "accuracy": accuracy}
+                "stages_ms_per_step": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()},
+                "accuracy": accuracy}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

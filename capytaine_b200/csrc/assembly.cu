@@ -14,9 +14,12 @@
 // consecutive complex entries of the column-major output.
 //
 // Precision: BEM_PREC_FP64 evaluates every term in float64.  BEM_PREC_MIXED
-// evaluates the one-point (far-field) Rankine terms and the tabulated wave term
-// in float32 and keeps float64 for the exact near-field Rankine integrals
-// (panel pairs closer than 7 panel radii), whose log/atan terms are singular.
+// evaluates the tabulated wave term (table values, Lagrange interpolation,
+// gradient assembly) in float32 and keeps the Rankine terms in float64: the
+// exact near-field integrals are singular (log/atan), and the one-point far
+// field dominates the real part of K, whose float32 rounding would perturb the
+// O(k)-small imaginary part of the source strengths (radiation damping at low
+// frequency) beyond 1e-5 relative.
 #include <cmath>
 #include "integrals.cuh"
 
@@ -379,8 +382,8 @@ __global__ void __launch_bounds__(kRows) assemble_kernel(const bem_assembly_args
       const double d0 = M[0] - f.c[0], d1 = M[1] - f.c[1], d2 = M[2] - f.c[2];
       const double r0 = norm2_3(d0, d1, d2);
       if (r0 > 7 * f.radius) {
-        R g, dg[3];
-        one_point_rankine<R>((R)-d0, (R)-d1, (R)-d2, (R)f.area, g, dg);
+        double g, dg[3];
+        one_point_rankine<double>(-d0, -d1, -d2, f.area, g, dg);
         Gr = g;
         dGr[0] = dg[0];
         dGr[1] = dg[1];
@@ -400,8 +403,8 @@ __global__ void __launch_bounds__(kRows) assemble_kernel(const bem_assembly_args
         const double r1 = hypot(dh, -M[2] - f.c[2]);
         const double Mr[3] = {M[0], M[1], -M[2]};
         if (r1 > 7 * f.radius) {
-          R g, dg[3];
-          one_point_rankine<R>((R)(f.c[0] - Mr[0]), (R)(f.c[1] - Mr[1]), (R)(f.c[2] - Mr[2]), (R)f.area, g, dg);
+          double g, dg[3];
+          one_point_rankine<double>(f.c[0] - Mr[0], f.c[1] - Mr[1], f.c[2] - Mr[2], f.area, g, dg);
           Gf = g;
           dGf[0] = dg[0];
           dGf[1] = dg[1];

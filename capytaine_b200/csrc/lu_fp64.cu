@@ -105,10 +105,10 @@ __global__ void __launch_bounds__(256) zlu_diag_kernel(double2* __restrict__ A, 
       for (int r = j + 1 + tid; r < kNB; r += blockDim.x) T[j * kLd + r] = cdiv(T[j * kLd + r], pivot);
     }
     __syncthreads();
-    const int cnt = kNB - 1 - j;
-    for (int idx = tid; idx < cnt * cnt; idx += blockDim.x) {
-      const int r = j + 1 + idx % cnt, c = j + 1 + idx / cnt;
-      T[c * kLd + r] = cfms(T[c * kLd + r], T[j * kLd + r], T[c * kLd + j]);
+    // rank-1 update: warp w takes columns j+1+w, j+1+w+8, ...
+    for (int c = j + 1 + warp; c < kNB; c += 8) {
+      const double2 tcj = T[c * kLd + j];
+      for (int r = j + 1 + lane; r < kNB; r += 32) T[c * kLd + r] = cfms(T[c * kLd + r], T[j * kLd + r], tcj);
     }
     __syncthreads();
   }
@@ -163,11 +163,11 @@ __global__ void __launch_bounds__(256) zlu_panel_kernel(double2* __restrict__ A,
     __syncthreads();
     if (kind == 1) {
       // X <- L11^{-1} X, column sweep over the unit lower factor
+      const int warp = tid >> 5, lane = tid & 31;
       for (int i = 0; i < kNB - 1; ++i) {
-        const int cnt = kNB - 1 - i;
-        for (int idx = tid; idx < cnt * kNB; idx += blockDim.x) {
-          const int r = i + 1 + idx % cnt, c = idx / cnt;
-          X[c * kLd + r] = cfms(X[c * kLd + r], D[i * kLd + r], X[c * kLd + i]);
+        for (int c = warp; c < kNB; c += 8) {
+          const double2 xi = X[c * kLd + i];
+          for (int r = i + 1 + lane; r < kNB; r += 32) X[c * kLd + r] = cfms(X[c * kLd + r], D[i * kLd + r], xi);
         }
         __syncthreads();
       }
@@ -183,15 +183,13 @@ __global__ void __launch_bounds__(256) zlu_panel_kernel(double2* __restrict__ A,
       X[c * kLd + r] = Ab[(size_t)(r0 + r) + (size_t)(kk + c) * lda];
     }
     __syncthreads();
+    const int rr = tid & (kNB - 1), cs = tid >> 6;  // 64 rows x 4 column phases
     for (int j = 0; j < kNB; ++j) {
       const double2 ujj = D[j * kLd + j];
       if (tid < kNB && cabs1(ujj) > 0.0) X[j * kLd + tid] = cdiv(X[j * kLd + tid], ujj);
       __syncthreads();
-      const int cnt = kNB - 1 - j;
-      for (int idx = tid; idx < cnt * kNB; idx += blockDim.x) {
-        const int r = idx % kNB, c = j + 1 + idx / kNB;
-        X[c * kLd + r] = cfms(X[c * kLd + r], X[j * kLd + r], D[c * kLd + j]);
-      }
+      const double2 xj = X[j * kLd + rr];
+      for (int c = j + 1 + cs; c < kNB; c += 4) X[c * kLd + rr] = cfms(X[c * kLd + rr], xj, D[c * kLd + j]);
       __syncthreads();
     }
     for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {

@@ -1,0 +1,641 @@
+// Mixed-precision complex LU with float64-residual iterative refinement.
+//
+// Replaces the complex128 zgetrf/zgetrs solve of capytaine
+// (tools/block_circulant_matrices.py:361-385, bem/engines.py:300-346) by:
+//   * a float32 copy of K in two planes (real, imaginary), column-major, padded
+//     to a multiple of 128 with the identity;
+//   * a blocked right-looking block LU with 128-wide blocks, A = L U with L
+//     unit block lower (L_ik = A_ik A_kk^{-1}) and U block upper (the updated
+//     block rows): each diagonal block is inverted by Gauss-Jordan elimination
+//     with partial pivoting among its rows, held in registers; the panel is the
+//     product A21 A_kk^{-1}; the trailing update C -= L21 U12 runs on the
+//     tcgen05 tensor cores (TF32 inputs, FP32 accumulation; tc_gemm.cu) from
+//     operands the panel kernel packs.  No row permutation leaves the diagonal
+//     blocks, so the solves need none;
+//   * block substitutions with these factors (persistent kernel, diagonal
+//     inverses applied in the backward sweep);
+//   * iterative refinement: x += LU^{-1} (b - K x) with the residual computed
+//     in float64 against the float64 matrix until the relative residual of
+//     every right-hand side is below the requested tolerance.
+#include <algorithm>
+#include <vector>
+#include "common.cuh"
+
+namespace bem {
+
+int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
+                      int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
+                      int n, int batch, int* err, cudaStream_t stream);
+
+namespace {
+
+constexpr int kB = 128;        // LU block
+constexpr int kLdB = kB + 1;   // shared leading dimension of a 128-row tile
+constexpr int kPT = 64;        // panel tile width
+constexpr int kLdP = kPT + 1;
+constexpr int kRhs = 16;       // right-hand sides per solve launch
+constexpr int kLdR = kRhs + 1;
+constexpr long long kSpin = 4000000;
+
+__device__ __forceinline__ float2 fmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ float2 ffms(float2 acc, float2 a, float2 b) {
+  return make_float2(acc.x - (a.x * b.x - a.y * b.y), acc.y - (a.x * b.y + a.y * b.x));
+}
+__device__ __forceinline__ float2 fdiv(float2 a, float2 b) {
+  const float d = b.x * b.x + b.y * b.y;
+  return make_float2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__device__ __forceinline__ float fabs1(float2 a) { return fabsf(a.x) + fabsf(a.y); }
+
+struct Planes {
+  float* re;
+  float* im;
+  int64_t ld;      // = npad
+  int64_t stride;  // floats between matrices (re and im planes of one matrix are plane apart)
+};
+__device__ __forceinline__ float2 ldp(const Planes& W, int b, int r, int c) {
+  const size_t o = (size_t)b * W.stride + (size_t)r + (size_t)c * W.ld;
+  return make_float2(W.re[o], W.im[o]);
+}
+__device__ __forceinline__ void stp(const Planes& W, int b, int r, int c, float2 v) {
+  const size_t o = (size_t)b * W.stride + (size_t)r + (size_t)c * W.ld;
+  W.re[o] = v.x;
+  W.im[o] = v.y;
+}
+
+// K (complex128, n x n, leading dimension ldk) -> planes (npad x npad) with the
+// identity on the padding.
+__global__ void convert_pad_kernel(const double2* __restrict__ K, int64_t ldk, int64_t strideK, int n, int npad,
+                                   Planes W) {
+  const int b = blockIdx.z;
+  const int c = blockIdx.y;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < npad; r += gridDim.x * blockDim.x) {
+    float2 v;
+    if (r < n && c < n) {
+      const double2 z = K[(size_t)b * strideK + (size_t)r + (size_t)c * ldk];
+      v = make_float2((float)z.x, (float)z.y);
+    } else {
+      v = make_float2(r == c ? 1.0f : 0.0f, 0.0f);
+    }
+    stp(W, b, r, c, v);
+  }
+}
+
+// Inverse of the diagonal block A_kk by Gauss-Jordan elimination with partial
+// pivoting among its rows.  The 128 x 128 block lives in registers: thread
+// (warp w, lane l) owns rows l + 32 a (a < 4) and columns w + 16 m (m < 8).
+// Per column: the owning warp picks the pivot and publishes the column, all
+// warps swap the two rows with shuffles and publish the pivot row, then every
+// thread updates its 32 entries.  Two barriers per column; the published
+// column/row alternate between two buffers.  Output: inv (128 x 128,
+// column-major) = A_kk^{-1}; info flags an exactly zero pivot.
+// One Gauss-Jordan column step with the owner slot JM of column j known at
+// compile time (j = 16 JM + jw).
+template <int JM>
+__device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b, int lane, int w, int tid,
+                                        float2 (*colbuf)[kB], float2 (*rowbuf)[kB], int* s_piv, int* perm,
+                                        int* __restrict__ info) {
+  constexpr int SJ = JM >> 1;  // register slot of row j (j >> 5)
+  const int j = 16 * JM + jw;
+  const int buf = j & 1;
+  if (w == jw) {
+    float best = -1.0f;
+    int bi = j;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = lane + 32 * i;
+      const float av = fabs1(a[i][JM]);
+      if (r >= j && (av > best || (av == best && r < bi))) {
+        best = av;
+        bi = r;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = lane + 32 * i;
+      const int dst = (r == j) ? bi : ((r == bi) ? j : r);
+      colbuf[buf][dst] = a[i][JM];
+    }
+    if (lane == 0) {
+      s_piv[buf] = bi;
+      if (!(best > 0.0f) && info[b] == 0) info[b] = kk + j + 1;
+    }
+  }
+  __syncthreads();
+  const int p = s_piv[buf];
+  const int lj = j & 31;
+  if (p != j) {
+    const int lp = p & 31, sp = p >> 5;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      float2 vp = a[0][m];
+#pragma unroll
+      for (int i = 1; i < 4; ++i)
+        if (i == sp) vp = a[i][m];
+      const float2 vj = a[SJ][m];
+      const float2 from_p = make_float2(__shfl_sync(0xffffffffu, vp.x, lp), __shfl_sync(0xffffffffu, vp.y, lp));
+      const float2 from_j = make_float2(__shfl_sync(0xffffffffu, vj.x, lj), __shfl_sync(0xffffffffu, vj.y, lj));
+      if (lane == lj) a[SJ][m] = from_p;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (i == sp && lane == lp) a[i][m] = from_j;
+    }
+    if (tid == 0) {
+      const int t = perm[j];
+      perm[j] = perm[p];
+      perm[p] = t;
+    }
+  }
+  if (lane == lj) {
+#pragma unroll
+    for (int m = 0; m < 8; ++m) rowbuf[buf][w + 16 * m] = a[SJ][m];
+  }
+  __syncthreads();
+  const float2 piv = rowbuf[buf][j];
+  const float2 dinv = fabs1(piv) > 0.0f ? fdiv(make_float2(1.0f, 0.0f), piv) : make_float2(0.0f, 0.0f);
+  float2 u[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) u[m] = (m == JM && w == jw) ? dinv : fmul(rowbuf[buf][w + 16 * m], dinv);
+  const float2 mdinv = make_float2(-dinv.x, -dinv.y);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (i == SJ && lane == lj) {
+#pragma unroll
+      for (int m = 0; m < 8; ++m) a[i][m] = u[m];
+    } else {
+      const float2 f = colbuf[buf][lane + 32 * i];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        if (m == JM && w == jw) a[i][m] = fmul(f, mdinv);
+        else a[i][m] = ffms(a[i][m], f, u[m]);
+      }
+    }
+  }
+}
+
+// Inverse of the diagonal block A_kk by Gauss-Jordan elimination with partial
+// pivoting among its rows.  The 128 x 128 block lives in registers: thread
+// (warp w, lane l) owns rows l + 32 a (a < 4) and columns w + 16 m (m < 8).
+// Per column: the owning warp picks the pivot and publishes the column, all
+// warps swap the two rows with shuffles and publish the pivot row, then every
+// thread updates its 32 entries.  Two barriers per column; the published
+// column/row alternate between two buffers.  Columns are visited slot by slot
+// so that register indices are compile-time constants.  Output: inv (128 x 128,
+// column-major) = A_kk^{-1}; info flags an exactly zero pivot.
+__global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* __restrict__ info,
+                                                        float2* __restrict__ inv, int nblk) {
+  __shared__ float2 colbuf[2][kB];
+  __shared__ float2 rowbuf[2][kB];
+  __shared__ int s_piv[2];
+  __shared__ int perm[kB];
+  const int b = blockIdx.x, tid = threadIdx.x;
+  const int lane = tid & 31, w = tid >> 5;
+  float2 a[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int m = 0; m < 8; ++m) a[i][m] = ldp(W, b, kk + lane + 32 * i, kk + w + 16 * m);
+  if (tid < kB) perm[tid] = tid;
+  __syncthreads();
+#define BEM_GJ_SLOT(JM) \
+  for (int jw = 0; jw < 16; ++jw) gj_step<JM>(a, jw, kk, b, lane, w, tid, colbuf, rowbuf, s_piv, perm, info);
+  BEM_GJ_SLOT(0)
+  BEM_GJ_SLOT(1)
+  BEM_GJ_SLOT(2)
+  BEM_GJ_SLOT(3)
+  BEM_GJ_SLOT(4)
+  BEM_GJ_SLOT(5)
+  BEM_GJ_SLOT(6)
+  BEM_GJ_SLOT(7)
+#undef BEM_GJ_SLOT
+  __syncthreads();
+  // inverse of A_kk = (P A_kk)^{-1} P: column c of the result goes to column perm[c]
+  float2* out = inv + ((size_t)b * nblk + kk / kB) * kB * kB;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int r = lane + 32 * i, c = w + 16 * m;
+      out[r + (size_t)perm[c] * kB] = a[i][m];
+    }
+}
+
+// Panels of step kk of the block LU.  Tiles [0, nrest): the block row to the
+// right of the diagonal, packed unchanged as the B operand (U12 = A12);
+// tiles [nrest, 2 nrest): 64 rows below the diagonal, L21 = A21 A_kk^{-1},
+// written back and packed as the A operand.
+// Aop: [batch][npad][2*kB]; Bop: [batch][2*npad][2*kB].
+__global__ void __launch_bounds__(256) clu_panel_kernel(Planes W, int npad, int kk, const float2* __restrict__ inv,
+                                                        int nblk, float* __restrict__ Aop, float* __restrict__ Bop) {
+  extern __shared__ float2 fsm[];
+  float2* D = fsm;               // A_kk^{-1}, D[c*kLdB + r]
+  float2* X = fsm + kB * kLdB;   // 64 x 128 rows of A21, X[c*kLdP + r]
+  const int b = blockIdx.y, tid = threadIdx.x;
+  const int nrest = (npad - kk - kB) / kPT;
+  const int t = blockIdx.x;
+  const size_t kp = 2 * kB;
+  if (t < nrest) {
+    // pack 128 x 64 of A12: B operand rows of the complex columns c0 .. c0+63
+    const int c0 = kk + kB + t * kPT;
+    const int j0 = c0 & ~(kB - 1);
+    float* Bb = Bop + (size_t)b * 2 * npad * kp;
+    for (int idx = tid; idx < kB * kPT; idx += blockDim.x) {
+      const int r = idx & (kB - 1), c = idx >> 7;
+      const float2 u = ldp(W, b, kk + r, c0 + c);
+      const int jj = c0 - j0 + c;
+      float* rowR = Bb + (size_t)(2 * j0 + jj) * kp;
+      float* rowI = Bb + (size_t)(2 * j0 + kB + jj) * kp;
+      rowR[r] = u.x;
+      rowR[kB + r] = -u.y;
+      rowI[r] = u.y;
+      rowI[kB + r] = u.x;
+    }
+    return;
+  }
+  const float2* invb = inv + ((size_t)b * nblk + kk / kB) * kB * kB;
+  for (int idx = tid; idx < kB * kB; idx += blockDim.x) D[(idx >> 7) * kLdB + (idx & (kB - 1))] = invb[idx];
+  const int r0 = kk + kB + (t - nrest) * kPT;
+  for (int idx = tid; idx < kPT * kB; idx += blockDim.x) {
+    const int r = idx & (kPT - 1), c = idx >> 6;
+    X[c * kLdP + r] = ldp(W, b, r0 + r, kk + c);
+  }
+  __syncthreads();
+  // thread: one row r, 32 columns
+  const int r = tid & (kPT - 1), cq = (tid >> 6) * 32;
+  float2 acc[32];
+#pragma unroll
+  for (int u = 0; u < 32; ++u) acc[u] = make_float2(0.0f, 0.0f);
+  for (int m = 0; m < kB; ++m) {
+    const float2 x = X[m * kLdP + r];
+#pragma unroll
+    for (int u = 0; u < 32; ++u) {
+      const float2 a = D[(cq + u) * kLdB + m];
+      acc[u].x += x.x * a.x - x.y * a.y;
+      acc[u].y += x.x * a.y + x.y * a.x;
+    }
+  }
+  float* row = Aop + (size_t)b * npad * kp + (size_t)(r0 + r) * kp;
+#pragma unroll
+  for (int u = 0; u < 32; ++u) {
+    const int c = cq + u;
+    stp(W, b, r0 + r, kk + c, acc[u]);
+    row[c] = acc[u].x;
+    row[kB + c] = acc[u].y;
+  }
+}
+
+// 16-byte asynchronous global -> shared copy and its completion wait.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst))),
+               "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__device__ __forceinline__ int ld_acquire_i(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_i(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+// Persistent block substitution with the block LU factors; B complex128 in
+// place.  Forward: y_i = b_i - sum_{j<i} L_ij y_j (unit block lower).  Backward:
+// x_i = A_ii^{-1} (y_i - sum_{j>i} U_ij x_j).  Each CTA owns one 128-row block;
+// the off-diagonal block of a dependency is copied to shared memory
+// asynchronously (real and imaginary planes, 16-byte copies) before waiting for
+// that dependency; the diagonal inverse is staged through the same buffer.
+__global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nblk, int batch,
+                                                               const float2* __restrict__ inv, double2* B,
+                                                               int64_t ldb, int64_t strideB, int nrhs, int forward,
+                                                               int* flags, int* ticket, int* err) {
+  extern __shared__ __align__(16) float fsmf[];
+  float* Lre = fsmf;                       // Lre[m*kB + r], 128 x 128
+  float* Lim = Lre + kB * kB;
+  float2* X = reinterpret_cast<float2*>(Lim + kB * kB);  // X[r*kLdR + c]
+  float2* Y = X + kB * kLdR;                               // Y[m*kLdR + c]
+  __shared__ int s_t;
+  const int tid = threadIdx.x;
+  if (tid == 0) s_t = atomicAdd(ticket, 1);
+  __syncthreads();
+  const int t = s_t;
+  const int b = t % batch, step = t / batch;
+  const int i = forward ? step : (nblk - 1 - step);
+  double2* Bb = B + (size_t)b * strideB;
+  const int r0 = i * kB;
+  for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
+    const int r = idx & (kB - 1), c = idx >> 7;
+    const double2 v = __ldcg(Bb + (size_t)(r0 + r) + (size_t)c * ldb);
+    X[r * kLdR + c] = make_float2((float)v.x, (float)v.y);
+  }
+  const int ndep = forward ? i : (nblk - 1 - i);
+  const float* Wre = W.re + (size_t)b * W.stride;
+  const float* Wim = W.im + (size_t)b * W.stride;
+  for (int q = 0; q < ndep; ++q) {
+    const int j = forward ? q : (nblk - 1 - q);
+    // off-diagonal block (does not depend on the flag): 128 columns x 128 rows,
+    // 32 sixteen-byte pieces per column and plane
+    for (int idx = tid; idx < kB * 32; idx += blockDim.x) {
+      const int m = idx >> 5, piece = idx & 31;
+      const size_t g = (size_t)(r0 + piece * 4) + (size_t)(j * kB + m) * W.ld;
+      cp_async16(Lre + m * kB + piece * 4, Wre + g);
+      cp_async16(Lim + m * kB + piece * 4, Wim + g);
+    }
+    if (tid == 0) {
+      long long it = 0;
+      while (ld_acquire_i(flags + (size_t)b * nblk + j) == 0) {
+        if (++it > kSpin) {
+          atomicExch(err, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
+      const int m = idx & (kB - 1), c = idx >> 7;
+      const double2 v = __ldcg(Bb + (size_t)(j * kB + m) + (size_t)c * ldb);
+      Y[m * kLdR + c] = make_float2((float)v.x, (float)v.y);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
+      const int r = idx & (kB - 1), c = idx >> 7;
+      float2 acc = X[r * kLdR + c];
+#pragma unroll 8
+      for (int m = 0; m < kB; ++m) {
+        const float ar = Lre[m * kB + r], ai = Lim[m * kB + r];
+        const float2 y = Y[m * kLdR + c];
+        acc.x -= ar * y.x - ai * y.y;
+        acc.y -= ar * y.y + ai * y.x;
+      }
+      X[r * kLdR + c] = acc;
+    }
+    __syncthreads();
+  }
+  if (forward) {
+    // unit block lower factor: y_i = X
+    for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
+      const int r = idx & (kB - 1), c = idx >> 7;
+      const float2 v = X[r * kLdR + c];
+      Bb[(size_t)(r0 + r) + (size_t)c * ldb] = make_double2((double)v.x, (double)v.y);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) st_release_i(flags + (size_t)b * nblk + i, 1);
+    return;
+  }
+  // backward: x_i = A_ii^{-1} X; the inverse (interleaved complex) through the planes
+  const float2* Inv = inv + ((size_t)b * nblk + i) * kB * kB;
+  for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
+    const float2 v = __ldg(Inv + idx);  // element (idx % 128, idx / 128)
+    Lre[idx] = v.x;
+    Lim[idx] = v.y;
+  }
+  __syncthreads();
+  float2 res[8];  // kB * kRhs / blockDim.x
+  int cnt = 0;
+  for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
+    const int r = idx & (kB - 1), c = idx >> 7;
+    float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll 8
+    for (int m = 0; m < kB; ++m) {
+      const float ar = Lre[m * kB + r], ai = Lim[m * kB + r];
+      const float2 x = X[m * kLdR + c];
+      acc.x += ar * x.x - ai * x.y;
+      acc.y += ar * x.y + ai * x.x;
+    }
+    res[cnt++] = acc;
+  }
+  cnt = 0;
+  for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
+    const int r = idx & (kB - 1), c = idx >> 7;
+    const float2 v = res[cnt++];
+    Bb[(size_t)(r0 + r) + (size_t)c * ldb] = make_double2((double)v.x, (double)v.y);
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) st_release_i(flags + (size_t)b * nblk + i, 1);
+}
+
+// x += d; r = b (copies for the residual), over (batch, n, nrhs) with leading dimension ld.
+__global__ void ir_update_kernel(double2* __restrict__ X, const double2* __restrict__ D, double2* __restrict__ R,
+                                 const double2* __restrict__ Bv, int n, int nrhs, int64_t ld, int64_t stride) {
+  const int b = blockIdx.z, c = blockIdx.y;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const size_t o = (size_t)b * stride + (size_t)c * ld + r;
+    const double2 x = X[o], d = D[o];
+    X[o] = make_double2(x.x + d.x, x.y + d.y);
+    R[o] = Bv[o];
+  }
+}
+
+// Squared norms of columns: out[(b*nrhs + c)] = sum |V(:, c)|^2 over n rows.
+__global__ void colnorm2_kernel(const double2* __restrict__ V, int n, int64_t ld, int64_t stride,
+                                double* __restrict__ out) {
+  const int c = blockIdx.x, b = blockIdx.y, nrhs = gridDim.x;
+  const double2* v = V + (size_t)b * stride + (size_t)c * ld;
+  double s = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) s += v[r].x * v[r].x + v[r].y * v[r].y;
+  __shared__ double red[256];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[(size_t)b * nrhs + c] = red[0];
+}
+
+bool g_mixed_configured = false;
+int configure_mixed() {
+  if (g_mixed_configured) return BEM_OK;
+  const int panel = (kB * kLdB + kB * kLdP) * (int)sizeof(float2);
+  const int trsm = 2 * kB * kB * (int)sizeof(float) + 2 * kB * kLdR * (int)sizeof(float2);
+  BEM_CUDA_CHECK(cudaFuncSetAttribute(clu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, panel));
+  BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, trsm));
+  g_mixed_configured = true;
+  return BEM_OK;
+}
+
+// Workspace layout (bytes): [planes 2*npad^2 floats][Aop npad*2kB floats][Bop 2*npad*2kB floats]
+// [diagonal inverses nblk*kB*kB float2][flags batch*nblk + 1 ints], each per matrix except flags.
+struct MixedWork {
+  float* W;
+  float* Aop;
+  float* Bop;
+  float2* inv;
+  int* flags;
+};
+MixedWork carve(void* work, int npad, int batch) {
+  char* p = (char*)work;
+  const int nblk = npad / kB;
+  MixedWork w;
+  w.W = (float*)p;
+  p += (size_t)batch * 2 * npad * npad * sizeof(float);
+  w.Aop = (float*)p;
+  p += (size_t)batch * npad * 2 * kB * sizeof(float);
+  w.Bop = (float*)p;
+  p += (size_t)batch * 2 * npad * 2 * kB * sizeof(float);
+  w.inv = (float2*)p;
+  p += (size_t)batch * nblk * kB * kB * sizeof(float2);
+  w.flags = (int*)p;
+  return w;
+}
+Planes planes_of(const MixedWork& w, int npad) {
+  return Planes{w.W, w.W + (size_t)npad * npad, npad, 2 * (int64_t)npad * npad};
+}
+
+}  // namespace
+}  // namespace bem
+
+using namespace bem;
+
+extern "C" int64_t bem_clu_workspace_bytes(int npad, int batch) {
+  if (npad <= 0 || npad % kB || batch <= 0) return -1;
+  const int64_t nblk = npad / kB;
+  return (int64_t)batch * 2 * npad * (int64_t)npad * 4 + (int64_t)batch * npad * 2 * kB * 4 +
+         (int64_t)batch * 2 * npad * 2 * kB * 4 + (int64_t)batch * nblk * kB * kB * 8 +
+         ((int64_t)batch * nblk + 1) * 4 + 1024;
+}
+
+extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
+                              int* piv_dev, int* info_dev, void* work_dev, int* err_dev, void* stream) {
+  if (!K_dev || !piv_dev || !info_dev || !work_dev || !err_dev || n <= 0 || npad < n || npad % kB || batch <= 0 ||
+      ldk < n)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_clu_factor: bad arguments (npad multiple of 128, >= n)");
+  if (reinterpret_cast<uintptr_t>(work_dev) & 1023)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_clu_factor: workspace must be 1024-byte aligned");
+  int st = configure_mixed();
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  MixedWork w = carve(work_dev, npad, batch);
+  Planes W = planes_of(w, npad);
+  const int nblk = npad / kB;
+  int launches = 0;
+  BEM_CUDA_CHECK(cudaMemsetAsync(info_dev, 0, sizeof(int) * batch, s));
+  convert_pad_kernel<<<dim3(ceil_div(npad, 256), npad, batch), 256, 0, s>>>((const double2*)K_dev, ldk, strideK, n,
+                                                                           npad, W);
+  ++launches;
+  const int panel_smem = (kB * kLdB + kB * kLdP) * (int)sizeof(float2);
+  for (int kk = 0; kk < npad; kk += kB) {
+    clu_gj_kernel<<<batch, 512, 0, s>>>(W, kk, info_dev, w.inv, nblk);
+    ++launches;
+    const int nrest = (npad - kk - kB) / kPT;
+    if (nrest > 0) {
+      clu_panel_kernel<<<dim3(2 * nrest, batch), 256, panel_smem, s>>>(W, npad, kk, w.inv, nblk, w.Aop, w.Bop);
+      ++launches;
+    }
+    const int m = npad - kk - kB;
+    if (m > 0) {
+      st = cgemm_tf32_update(w.Aop, npad, kk + kB, w.Bop, 2 * (int64_t)npad, 2 * (kk + kB), 2 * kB, W.re, W.im,
+                             npad, W.stride, kk + kB, kk + kB, m, m, batch, err_dev, s);
+      if (st) return st;
+    }
+  }
+  count_launches(launches);
+  BEM_CUDA_CHECK(cudaGetLastError());
+  return BEM_OK;
+}
+
+extern "C" int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv_dev, void* B_dev, int64_t ldb,
+                             int64_t strideB, int nrhs, int* err_dev, void* stream) {
+  if (!work_dev || !piv_dev || !B_dev || !err_dev || npad <= 0 || npad % kB || batch <= 0 || nrhs <= 0 ||
+      ldb < npad)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_clu_solve: bad arguments");
+  int st = configure_mixed();
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  MixedWork w = carve(work_dev, npad, batch);
+  Planes W = planes_of(w, npad);
+  const int nblk = npad / kB;
+  const int smem = 2 * kB * kB * (int)sizeof(float) + 2 * kB * kLdR * (int)sizeof(float2);
+  int* ticket = w.flags + (size_t)batch * nblk;
+  int launches = 0;
+  for (int c0 = 0; c0 < nrhs; c0 += kRhs) {
+    const int nc = std::min(kRhs, nrhs - c0);
+    double2* Bc = (double2*)B_dev + (size_t)c0 * ldb;
+    for (int forward = 1; forward >= 0; --forward) {
+      BEM_CUDA_CHECK(cudaMemsetAsync(w.flags, 0, sizeof(int) * ((size_t)batch * nblk + 1), s));
+      ctrsm_persistent_kernel<<<nblk * batch, 256, smem, s>>>(W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward,
+                                                             w.flags, ticket, err_dev);
+      ++launches;
+    }
+  }
+  count_launches(launches);
+  BEM_CUDA_CHECK(cudaGetLastError());
+  return BEM_OK;
+}
+
+extern "C" int bem_zgemm_ts(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
+                            int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,
+                            double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev,
+                            void* stream);
+
+extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
+                                void* work_dev, const int* piv_dev, const void* B_dev, void* X_dev, void* R_dev,
+                                void* D_dev, int64_t ldb, int64_t strideB, int nrhs, double tol, int max_iter,
+                                void* ts_work_dev, double* norms_dev, int* err_dev, int* iters_out,
+                                double* resid_out, void* stream) {
+  if (!K_dev || !work_dev || !piv_dev || !B_dev || !X_dev || !R_dev || !D_dev || !ts_work_dev || !norms_dev ||
+      !err_dev || !iters_out || !resid_out || nrhs <= 0 || nrhs > 16 || max_iter <= 0 || ldb < npad)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_refine_solve: bad arguments (nrhs <= 16)");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t bytes = sizeof(double2) * ((size_t)(batch - 1) * strideB + (size_t)(nrhs - 1) * ldb + npad);
+  const int nvec = batch * nrhs;
+  std::vector<double> bn(nvec), rn(nvec);
+  // |b| per column
+  colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)B_dev, n, ldb, strideB, norms_dev);
+  BEM_CUDA_CHECK(cudaMemcpyAsync(bn.data(), norms_dev, sizeof(double) * nvec, cudaMemcpyDeviceToHost, s));
+  // x = 0, r = b
+  BEM_CUDA_CHECK(cudaMemsetAsync(X_dev, 0, bytes, s));
+  BEM_CUDA_CHECK(cudaMemcpyAsync(R_dev, B_dev, bytes, cudaMemcpyDeviceToDevice, s));
+  int launches = 1;
+  double worst = 0.0;
+  int it = 0;
+  for (it = 1; it <= max_iter; ++it) {
+    // d = LU^{-1} r (float32 factors); the padded rows of r stay zero
+    BEM_CUDA_CHECK(cudaMemcpyAsync(D_dev, R_dev, bytes, cudaMemcpyDeviceToDevice, s));
+    int st = bem_clu_solve(work_dev, npad, batch, piv_dev, D_dev, ldb, strideB, nrhs, err_dev, stream);
+    if (st) return st;
+    // x += d ; r = b ; r = b - K x (float64)
+    ir_update_kernel<<<dim3(ceil_div(n, 256), nrhs, batch), 256, 0, s>>>((double2*)X_dev, (const double2*)D_dev,
+                                                                         (double2*)R_dev, (const double2*)B_dev, n,
+                                                                         nrhs, ldb, strideB);
+    st = bem_zgemm_ts(n, n, nrhs, -1.0, 0.0, K_dev, ldk, strideK, X_dev, ldb, strideB, 1.0, 0.0, R_dev, ldb, strideB,
+                      batch, ts_work_dev, stream);
+    if (st) return st;
+    colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)R_dev, n, ldb, strideB, norms_dev);
+    launches += 2;
+    BEM_CUDA_CHECK(cudaMemcpyAsync(rn.data(), norms_dev, sizeof(double) * nvec, cudaMemcpyDeviceToHost, s));
+    BEM_CUDA_CHECK(cudaStreamSynchronize(s));
+    worst = 0.0;
+    for (int v = 0; v < nvec; ++v) {
+      const double rel = bn[v] > 0.0 ? std::sqrt(rn[v] / bn[v]) : std::sqrt(rn[v]);
+      worst = std::max(worst, rel);
+    }
+    if (worst <= tol) break;
+  }
+  count_launches(launches);
+  *iters_out = std::min(it, max_iter);
+  *resid_out = worst;
+  BEM_CUDA_CHECK(cudaGetLastError());
+  if (!(worst <= tol)) {
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "iterative refinement stopped at relative residual %.3e after %d iterations",
+                  worst, max_iter);
+    return set_error(BEM_ERR_NOT_CONVERGED, msg);
+  }
+  return BEM_OK;
+}

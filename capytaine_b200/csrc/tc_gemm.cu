@@ -219,17 +219,18 @@ __global__ void __launch_bounds__(192, 1) cgemm_tf32_update_kernel(const __grid_
       float* Cr = p.Cr + (size_t)b * p.c_stride + row;
       float* Ci = p.Ci + (size_t)b * p.c_stride + row;
       const int col0 = p.c_col0 + tn * kTNc;
+      // Per chunk of 32 accumulator columns: the 32 loads of C are issued before
+      // any store so that they are in flight together (a load after a store to
+      // a possibly aliasing address would otherwise wait for it).
 #pragma unroll 1
       for (int chunk = 0; chunk < kTN / 32; ++chunk) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(chunk * 32), v);
-        float* base = (chunk < kTNc / 32) ? Cr : Ci;
-        const int cc = (chunk % (kTNc / 32)) * 32;
+        float v[32], c[32];
+        float* __restrict__ base = ((chunk < kTNc / 32) ? Cr : Ci) + (size_t)(col0 + (chunk % (kTNc / 32)) * 32) * p.ldc;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          float* ptr = base + (size_t)(col0 + cc + j) * p.ldc;
-          *ptr = *ptr - v[j];
-        }
+        for (int j = 0; j < 32; ++j) c[j] = __ldcs(base + (size_t)j * p.ldc);
+        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(chunk * 32), v);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) __stcs(base + (size_t)j * p.ldc, c[j] - v[j]);
       }
     }
   }

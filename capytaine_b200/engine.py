@@ -62,48 +62,84 @@ class FrequencyResults:
 
 
 class _Workspace:
-    """Device buffers of one (n, batch, nrhs) shape, reused across batches."""
+    """Device buffers of one (n, batch, nrhs, precision) shape, reused across batches.
+
+    fp64:  K padded to a multiple of 64 (LU in place), S, right-hand sides B.
+    mixed: K unpadded (float64 residuals), float32 LU workspace padded to a
+           multiple of 128, B / X / R / D vectors of the refinement."""
 
     def __init__(self, n, batch, nrhs, device, precision):
         import torch
-        self.n, self.batch, self.nrhs = n, batch, nrhs
-        self.npad = padded_size(n)
-        npad = self.npad
+        self.n, self.batch, self.nrhs, self.precision = n, batch, nrhs, precision
+        lib = _lib.load()
         c128 = dict(dtype=torch.complex128, device=device)
-        self.K = torch.empty((batch, npad * npad), **c128)
         self.S = torch.empty((batch, n * n), **c128)
-        self.B = torch.zeros((batch, npad * nrhs), **c128)
         self.phi = torch.empty((batch, n * nrhs), **c128)
-        self.piv = torch.empty((batch, npad), dtype=torch.int32, device=device)
         self.info = torch.zeros(batch, dtype=torch.int32, device=device)
         self.err = torch.zeros(1, dtype=torch.int32, device=device)
         self.nan = torch.zeros(1, dtype=torch.int32, device=device)
-        lib = _lib.load()
-        self.lu_work = torch.empty(int(lib.bem_zlu_workspace_bytes(npad, batch)), dtype=torch.uint8, device=device)
         self.ts_work = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, min(nrhs, 16), batch)),
                                    dtype=torch.uint8, device=device)
+        if precision == "fp64":
+            self.npad = padded_size(n)
+            npad = self.npad
+            self.K = torch.empty((batch, npad * npad), **c128)
+            self.ldk = npad
+            self.B = torch.zeros((batch, npad * nrhs), **c128)
+            self.lu_work = torch.empty(int(lib.bem_zlu_workspace_bytes(npad, batch)), dtype=torch.uint8,
+                                       device=device)
+            self._aligned = None
+        else:
+            self.npad = int(math.ceil(n / 128) * 128)
+            npad = self.npad
+            self.K = torch.empty((batch, n * n), **c128)
+            self.ldk = n
+            self.B = torch.zeros((batch, npad * nrhs), **c128)
+            self.X = torch.zeros((batch, npad * nrhs), **c128)
+            self.R = torch.zeros((batch, npad * nrhs), **c128)
+            self.D = torch.zeros((batch, npad * nrhs), **c128)
+            self.norms = torch.zeros(batch * nrhs, dtype=torch.float64, device=device)
+            nbytes = int(lib.bem_clu_workspace_bytes(npad, batch))
+            self.lu_work = torch.empty(nbytes + 1024, dtype=torch.uint8, device=device)
+            base = self.lu_work.data_ptr()
+            self._aligned = (base + 1023) // 1024 * 1024  # 1024-byte aligned start
+        self.piv = torch.empty((batch, self.npad), dtype=torch.int32, device=device)
+
+    @property
+    def lu_work_ptr(self):
+        return self._aligned if self._aligned is not None else self.lu_work.data_ptr()
 
     @property
     def nbytes(self):
-        return sum(t.numel() * t.element_size() for t in (self.K, self.S, self.B, self.phi, self.lu_work,
-                                                           self.ts_work))
+        ts = [t for t in (self.K, self.S, self.B, self.phi, self.lu_work, self.ts_work)]
+        ts += [getattr(self, k) for k in ("X", "R", "D") if hasattr(self, k)]
+        return sum(t.numel() * t.element_size() for t in ts)
 
 
 class B200Engine:
     """capytaine-compatible matrix engine running the Delhommeau assembly and the
     dense solves on one B200.
 
-    precision: "fp64" (float64 assembly, float64 LU) or "mixed" (float32 far
-    field / wave term with float64 near field, low-precision tensor-core LU,
-    float64-residual GMRES iterative refinement).
+    precision: "fp64" (float64 LU) or "mixed" (float32 LU with TF32
+    tensor-core trailing updates, float64-residual iterative refinement to
+    refine_tol).  assembly_precision: "fp64" (default) or "mixed" (float32
+    tabulated wave term, float64 Rankine terms).
     """
 
     def __init__(self, *, green_function: Optional[Delhommeau] = None, precision: str = "fp64",
-                 linear_solver: str = "lu_decomposition", max_batch: int = 8, device=None):
+                 linear_solver: str = "lu_decomposition", max_batch: int = 8, device=None,
+                 refine_tol: float = 1e-10, refine_max_iter: int = 30, assembly_precision: str = "fp64"):
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
+        if assembly_precision not in ("fp64", "mixed"):
+            raise ValueError("assembly_precision must be 'fp64' or 'mixed'")
         self.precision = precision
-        self.green_function = green_function if green_function is not None else Delhommeau(precision=precision)
+        # float32 wave terms perturb the O(k)-small imaginary parts that carry the
+        # radiation damping at low frequency beyond 1e-5: float64 assembly by default.
+        self.assembly_precision = assembly_precision
+        self.refine_tol = float(refine_tol)
+        self.refine_max_iter = int(refine_max_iter)
+        self.green_function = green_function if green_function is not None else Delhommeau()
         self._linear_solver = linear_solver
         self.max_batch = int(max_batch)
         self._device = device
@@ -114,6 +150,7 @@ class B200Engine:
             "engine": "B200Engine",
             "linear_solver": str(linear_solver),
             "precision": precision,
+            "assembly_precision": assembly_precision,
             **self.green_function.exportable_settings,
         }
 
@@ -127,7 +164,7 @@ class B200Engine:
         return _lib.require_cuda(self._device)
 
     def workspace(self, n, batch, nrhs) -> _Workspace:
-        key = (n, batch, nrhs)
+        key = (n, batch, nrhs, self.precision)
         ws = self._ws.get(key)
         if ws is None:
             self._ws.clear()  # one resident shape at a time (memory)
@@ -174,26 +211,49 @@ class B200Engine:
             if ev:
                 ev[0].record()
             ws.nan.zero_()
+            ws.err.zero_()
+            mixed = self.precision == "mixed"
             for b in range(nb):
-                gf.assemble_into(mesh, mesh, ws.S[b], ws.K[b], wavenumber=float(ks[b]), lds=n, ldk=npad,
-                                 nan_flag=ws.nan, precision="fp64")
-            _lib.check(lib.bem_zpad_identity(_vp(ws.K), npad, npad * npad, nb, n, npad, stream))
+                gf.assemble_into(mesh, mesh, ws.S[b], ws.K[b], wavenumber=float(ks[b]), lds=n, ldk=ws.ldk,
+                                 nan_flag=ws.nan, precision=self.assembly_precision)
+            if not mixed:
+                _lib.check(lib.bem_zpad_identity(_vp(ws.K), npad, npad * npad, nb, n, npad, stream))
             if ev:
                 ev[1].record()
-            _lib.check(lib.bem_zlu_factor(_vp(ws.K), npad, npad, npad * npad, nb, _vp(ws.piv), _vp(ws.info),
-                                          _vp(ws.lu_work), stream))
+            if mixed:
+                _lib.check(lib.bem_clu_factor(_vp(ws.K), n, n * n, n, npad, nb, _vp(ws.piv), _vp(ws.info),
+                                              _vp(ws.lu_work_ptr), _vp(ws.err), stream))
+            else:
+                _lib.check(lib.bem_zlu_factor(_vp(ws.K), npad, npad, npad * npad, nb, _vp(ws.piv), _vp(ws.info),
+                                              _vp(ws.lu_work), stream))
             if ev:
                 ev[2].record()
             ws.B.zero_()
-            ws.err.zero_()
             _lib.check(lib.bem_build_rhs(n, nb, _vp(om_t), _vp(k_t), g, ndof, _vp(dofn), nhead, _vp(heads_t),
                                          _vp(dm.centers), _vp(dm.normals), _vp(hull), _vp(ws.B), npad, npad * nrhs,
                                          stream))
-            _lib.check(lib.bem_zlu_solve(_vp(ws.K), npad, npad, npad * npad, nb, _vp(ws.piv), _vp(ws.lu_work),
-                                         _vp(ws.B), npad, npad * nrhs, nrhs, _vp(ws.err), stream))
+            if mixed:
+                iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
+                status = lib.bem_refine_solve(_vp(ws.K), n, n * n, n, npad, nb, _vp(ws.lu_work_ptr), _vp(ws.piv),
+                                              _vp(ws.B), _vp(ws.X), _vp(ws.R), _vp(ws.D), npad, npad * nrhs, nrhs,
+                                              self.refine_tol, self.refine_max_iter, _vp(ws.ts_work),
+                                              _vp(ws.norms), _vp(ws.err), ctypes.byref(iters),
+                                              ctypes.byref(resid), stream)
+                stats["refine_iters"] = max(stats.get("refine_iters", 0), iters.value)
+                stats["refine_residual"] = max(stats.get("refine_residual", 0.0), resid.value)
+                if status != _lib.BEM_OK and status != _lib.BEM_ERR_NOT_CONVERGED:
+                    _lib.check(status)
+                if status == _lib.BEM_ERR_NOT_CONVERGED:
+                    stats["not_converged"] = stats.get("not_converged", 0) + 1
+                    raise _lib.NotConvergedError(status, lib.bem_last_error().decode())
+                sol = ws.X
+            else:
+                _lib.check(lib.bem_zlu_solve(_vp(ws.K), npad, npad, npad * npad, nb, _vp(ws.piv), _vp(ws.lu_work),
+                                             _vp(ws.B), npad, npad * nrhs, nrhs, _vp(ws.err), stream))
+                sol = ws.B
             if ev:
                 ev[3].record()
-            _lib.check(lib.bem_zgemm_ts(n, n, nrhs, 1.0, 0.0, _vp(ws.S), n, n * n, _vp(ws.B), npad, npad * nrhs,
+            _lib.check(lib.bem_zgemm_ts(n, n, nrhs, 1.0, 0.0, _vp(ws.S), n, n * n, _vp(sol), npad, npad * nrhs,
                                         0.0, 0.0, _vp(ws.phi), n, n * nrhs, nb, _vp(ws.ts_work), stream))
             F = torch.empty((nb, nrhs, ndof), dtype=torch.complex128, device=dev)
             _lib.check(lib.bem_integrate_pressure(n, nb, nrhs, ndof, _vp(ws.phi), n, n * nrhs, _vp(om_t), rho,

@@ -44,7 +44,7 @@ extern "C" {
 #define BEM_DTYPE_C64 1           /* complex64 outputs                                */
 
 #define BEM_PREC_FP64 0           /* every term in float64                            */
-#define BEM_PREC_MIXED 1          /* float32 far field and wave term, float64 near field */
+#define BEM_PREC_MIXED 1          /* float32 wave term, float64 Rankine terms             */
 
 /* Message describing the last error raised on the calling thread. */
 const char* bem_last_error(void);
@@ -198,6 +198,42 @@ int bem_froude_krylov(int n, int batch, int ndof, int nhead, const double* waven
 int bem_cgemm_tf32_update(const float* Aop_dev, int64_t a_rows, int a_row0, const float* Bop_dev, int64_t b_rows,
                           int b_row0, int kp, float* Cr_dev, float* Ci_dev, int64_t ldc, int64_t c_stride,
                           int c_row0, int c_col0, int m, int n, int batch, int* err_dev, void* stream);
+
+/* ---- mixed-precision solve ------------------------------------------------- */
+/* Workspace of bem_clu_factor / bem_clu_solve (float32 planes of K, packed
+ * tensor-core operands, inverted diagonal blocks, flags); 1024-byte aligned. */
+int64_t bem_clu_workspace_bytes(int npad, int batch);
+
+/* Float32 block LU of the complex128 matrices K (n x n, leading dimension ldk,
+ * `batch` of them strideK apart): copy to float32 planes padded to npad
+ * (multiple of 128) with the identity, then K = L U with L unit block lower
+ * (L_ik = K_ik K_kk^{-1}) and U block upper, 128-wide blocks; each diagonal
+ * block is inverted by Gauss-Jordan elimination with partial pivoting among
+ * its rows, trailing updates run on the tcgen05 tensor cores (TF32 inputs,
+ * FP32 accumulation).  piv_dev (batch x npad ints) is reserved: no row
+ * permutation leaves the diagonal blocks.  info_dev: batch ints, 0 or the
+ * 1-based column of the first zero pivot; err_dev: bounded-wait timeout flag.
+ * Replaces the LU of tools/block_circulant_matrices.py:361-378 in the
+ * mixed-precision engine. */
+int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch, int* piv_dev,
+                   int* info_dev, void* work_dev, int* err_dev, void* stream);
+
+/* B <- (LU)^{-1} B with the float32 block factors; B complex128 (npad x nrhs, ldb); piv_dev reserved. */
+int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv_dev, void* B_dev, int64_t ldb,
+                  int64_t strideB, int nrhs, int* err_dev, void* stream);
+
+/* Iterative refinement: X solves K X = B to a relative residual below tol in
+ * every column (residual r = b - K x evaluated in float64 against the float64
+ * K, correction from the float32 LU).  B, X, R, D: complex128 npad x nrhs
+ * (rows n..npad-1 of B zero), nrhs <= 16; ts_work_dev sized by
+ * bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch); norms_dev: batch*nrhs
+ * doubles.  Synchronises the stream once per iteration (convergence test).
+ * Returns BEM_ERR_NOT_CONVERGED (X holds the last iterate) when max_iter is
+ * reached.  Replaces the lu_solve of tools/block_circulant_matrices.py:382-385. */
+int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch, void* work_dev,
+                     const int* piv_dev, const void* B_dev, void* X_dev, void* R_dev, void* D_dev, int64_t ldb,
+                     int64_t strideB, int nrhs, double tol, int max_iter, void* ts_work_dev, double* norms_dev,
+                     int* err_dev, int* iters_out, double* resid_out, void* stream);
 
 /* ---- allocation-free variant ---------------------------------------------- */
 /* No counterpart in the reference.  Same operation and arguments as
