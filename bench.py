@@ -18,6 +18,7 @@ the only collectives are the timing barrier and the max over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -153,6 +154,63 @@ def fp64_tensor_peak_tflops():
     return best
 
 
+def lu_update_flops(npad, block):
+    """Real flops of the trailing updates of one blocked complex LU: sum over
+    the block steps of 8 m^2 b for an m x m update of depth b."""
+    return sum(8.0 * (npad - kk - block) ** 2 * block for kk in range(0, npad - block, block))
+
+
+def kernel_roofline(kernels, n, frequencies, engine, peaks, peak_src):
+    """Roofline of the kernel class with the largest device time in the timed
+    region: algorithmic work per launch / average launch duration."""
+    name, k = max(kernels.items(), key=lambda kv: kv[1]["ms_total"])
+    avg_s = k["ms_total"] / k["launches"] * 1e-3
+    total_ms = sum(v["ms_total"] for v in kernels.values())
+    base = {"kernel": name, "launches": k["launches"], "avg_launch_ms": avg_s * 1e3,
+            "share_of_timed_kernels": k["ms_total"] / total_ms, "traffic": None}
+    if name == "cgemm_tf32_update_kernel":
+        npad = -(-n // 128) * 128
+        flops = lu_update_flops(npad, 128) * frequencies / k["launches"]
+        peak = tf32_tensor_peak_tflops()
+        ach = flops / avg_s / 1e12
+        return base | {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                       "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run (TF32 has no entry in "
+                                      "MEASURED_PEAKS.json)",
+                       "algorithmic": "8 m^2 128 real flops per complex update of m x m by depth 128"}
+    if name == "zgemm_dmma_kernel":
+        npad = -(-n // 64) * 64
+        flops = lu_update_flops(npad, 64) * frequencies / k["launches"]
+        peak = fp64_tensor_peak_tflops()
+        ach = flops / avg_s / 1e12
+        return base | {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                       "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (float64 has no entry in "
+                                      "MEASURED_PEAKS.json)",
+                       "algorithmic": "8 m^2 64 real flops per complex update of m x m by depth 64"}
+    if name == "ctrsm_persistent_kernel":
+        npad = -(-n // 128) * 128
+        # one forward and one backward sweep read the float32 planes once (8 bytes per entry)
+        bytes_ = 8.0 * npad * npad / 2
+        ach = bytes_ / avg_s / 1e9
+        return base | {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                       "frac": ach / peaks["hbm_gbs"], "peak_source": f"{peak_src} hbm_gbs",
+                       "algorithmic": "8 bytes per entry of one triangle of the float32 factors per sweep"}
+    if name == "assemble_kernel":
+        bytes_ = 32.0 * n * n
+        ach = bytes_ / avg_s / 1e9
+        return base | {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                       "frac": ach / peaks["hbm_gbs"], "peak_source": f"{peak_src} hbm_gbs",
+                       "algorithmic": "32 bytes (complex128 S and K entries) per panel pair"}
+    # latency-bound kernels: report the bytes they move against HBM
+    if name == "clu_gj_kernel":
+        bytes_ = 2 * 8.0 * 128 * 128
+    else:
+        bytes_ = 0.0
+    ach = bytes_ / avg_s / 1e9
+    return base | {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                   "frac": ach / peaks["hbm_gbs"], "peak_source": f"{peak_src} hbm_gbs",
+                   "algorithmic": "bytes read and written per launch"}
+
+
 # ---------------------------------------------------------------------------
 def cpu_reference_solve(body, omega, gf_oracle):
     """One frequency-solve with the oracle port (C++ OpenMP assembly + SciPy LU)."""
@@ -220,7 +278,9 @@ def main():
     ap.add_argument("--steps", type=int, default=15)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--engine", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--engine", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--fp64-steps", type=int, default=4,
+                    help="timed steps of the float64 engine for the refined-mixed vs float64 comparison (0: skip)")
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -267,6 +327,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     launches0 = lib.bem_launch_count()
+    _lib.check(lib.bem_kernel_timer_enable(1))
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     step_ms = []
@@ -292,35 +353,17 @@ def main():
     value = total_solves / (t_ms * 1e-3)
 
     # ---- per-stage times and the roofline of the dominant kernel ----------
+    kernels = {}
+    for c in range(10):
+        tot, cnt = ctypes.c_double(0.0), ctypes.c_longlong(0)
+        _lib.check(lib.bem_kernel_timer_read(c, ctypes.byref(tot), ctypes.byref(cnt)))
+        if cnt.value:
+            kernels[lib.bem_kernel_class_name(c).decode()] = {"class": c, "ms_total": tot.value,
+                                                              "launches": int(cnt.value)}
+    _lib.check(lib.bem_kernel_timer_enable(0))
     st = engine.solve_frequencies(body, batches[0], sync_stats=True).stats
-    stage = max(("assembly_ms", "lu_ms", "solve_ms", "post_ms"), key=lambda k: st[k])
-    npad = -(-n // 64) * 64
     peaks, peak_src = measured_peaks()
-    if stage == "lu_ms" and args.engine == "fp64":
-        p64 = fp64_tensor_peak_tflops()
-        flops = 8 * npad ** 3 / 3 * nb
-        achieved = flops / (st["lu_ms"] * 1e-3) / 1e12
-        roofline = {"kernel": "zgemm_dmma_kernel (LU trailing updates, float64 tensor-core MMA)", "bound": "tensor",
-                    "achieved": achieved, "peak": p64, "unit": "TFLOP/s", "frac": achieved / p64, "traffic": None,
-                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (float64 has no entry in "
-                                   "MEASURED_PEAKS.json)",
-                    "algorithmic": "8 n^3 / 3 real flops per complex LU, n = 6144 (padded)"}
-    elif stage == "lu_ms":
-        npad128 = -(-n // 128) * 128
-        ptf = tf32_tensor_peak_tflops()
-        flops = 8 * npad128 ** 3 / 3 * nb
-        achieved = flops / (st["lu_ms"] * 1e-3) / 1e12
-        roofline = {"kernel": "cgemm_tf32_update_kernel (LU trailing updates, tcgen05 TF32)", "bound": "tensor",
-                    "achieved": achieved, "peak": ptf, "unit": "TFLOP/s", "frac": achieved / ptf, "traffic": None,
-                    "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run (TF32 has no entry in "
-                                   "MEASURED_PEAKS.json)",
-                    "algorithmic": "8 n^3 / 3 real flops per complex LU (complex count), n = 6144 (padded)"}
-    else:
-        bytes_ = 32.0 * n * n * nb
-        achieved = bytes_ / (st["assembly_ms"] * 1e-3) / 1e9
-        roofline = {"kernel": "assemble_kernel (S and K of one frequency)", "bound": "hbm", "achieved": achieved,
-                    "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-                    "peak_source": f"{peak_src} hbm_gbs", "algorithmic": "32 bytes (complex128 S and K) per panel pair"}
+    roofline = kernel_roofline(kernels, n, nb * args.steps, args.engine, peaks, peak_src)
 
     # ---- end to end through the public API with host buffers --------------
     barrier()
@@ -343,6 +386,29 @@ def main():
     e2e = {"value": total_solves / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d / args.steps),
            "d2h_bytes_per_step": int(d2h / args.steps)}
 
+    # ---- the float64 engine on the same batches (refined-mixed vs FP64 LU) -
+    fp64 = None
+    if args.engine == "mixed" and args.fp64_steps > 0:
+        eng64 = B200Engine(green_function=gf, precision="fp64", max_batch=args.batch)
+        eng64.solve_frequencies(body, batches[0])
+        barrier()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for s in range(args.warmup, args.warmup + args.fp64_steps):
+            eng64.solve_frequencies(body, batches[s])
+        f1.record()
+        torch.cuda.synchronize()
+        f_ms = f0.elapsed_time(f1)
+        if dist is not None:
+            t = torch.tensor([f_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            f_ms = float(t.item())
+        fp64 = {"value": args.fp64_steps * nb * world / (f_ms * 1e-3), "unit": UNIT, "steps": args.fp64_steps,
+                "ms_per_step": f_ms / args.fp64_steps}
+        fp64["mixed_over_fp64"] = value / fp64["value"]
+        del eng64
+
     # ---- CPU baseline (oracle port on the host cores) and accuracy --------
     cpu = None
     accuracy = None
@@ -357,18 +423,24 @@ def main():
                "sample": f"1 frequency-solve (omega={w:.3f}) of the 6084-panel barge"}
         got = engine.solve_frequencies(body, [w])
         accuracy = {"omega": w, "max_rel_err_vs_oracle": coefficient_error(got, 0, ref),
+                    "refine_iters": got.stats.get("refine_iters"), "refine_residual": got.stats.get("refine_residual"),
                     "note": "GPU-built tabulation vs oracle-built tabulation"}
+        if args.engine == "mixed":
+            g64 = B200Engine(green_function=gf, precision="fp64", max_batch=1).solve_frequencies(body, [w])
+            accuracy["fp64_engine_max_rel_err_vs_oracle"] = coefficient_error(g64, 0, ref)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "c128" if args.engine == "fp64" else "c128/f32",
+                "scaling": "weak", "vs_baseline": None, "dtype": "c128" if args.engine == "fp64" else "c128 (assembly, residuals) / f32-tf32 (LU)",
                 "data": "synthetic", "config": workload_config(args, n), "roofline": roofline,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                                "unit": f"ms per step of {nb} frequencies"},
                 "stages_ms_per_step": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()},
-                "accuracy": accuracy}
+                "kernels_timed_region": {k: {"ms_total": round(v["ms_total"], 3), "launches": v["launches"]}
+                                         for k, v in kernels.items()},
+                "fp64_engine": fp64, "accuracy": accuracy}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

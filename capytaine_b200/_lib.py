@@ -71,6 +71,10 @@ _SIGNATURES = {
     "bem_last_error": ([], ctypes.c_char_p),
     "bem_version": ([], c_int),
     "bem_launch_count": ([], ctypes.c_longlong),
+    "bem_kernel_timer_enable": ([ctypes.c_int], ctypes.c_int),
+    "bem_kernel_timer_read": ([ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)],
+                              ctypes.c_int),
+    "bem_kernel_class_name": ([ctypes.c_int], ctypes.c_char_p),
     "bem_default_r_spacing": ([c_int, c_double, c_int, c_void_p], c_int),
     "bem_default_z_spacing": ([c_int, c_double, c_int, c_void_p], c_int),
     "bem_construct_tabulation": ([c_void_p, c_int, c_void_p, c_int, c_int, c_void_p, c_void_p], c_int),

@@ -531,9 +531,11 @@ extern "C" int bem_assemble(const bem_assembly_args* args, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   const bool mixed = a.precision == BEM_PREC_MIXED;
   if (a.out_dtype == BEM_DTYPE_C128) {
+    TimedLaunch tl(kKAssemble, s);
     if (mixed) assemble_kernel<double2, true><<<grid, kRows, 0, s>>>(a, T, a.wavenumber, gf_sing, finite_k, sign_refl);
     else assemble_kernel<double2, false><<<grid, kRows, 0, s>>>(a, T, a.wavenumber, gf_sing, finite_k, sign_refl);
   } else if (a.out_dtype == BEM_DTYPE_C64) {
+    TimedLaunch tl(kKAssemble, s);
     if (mixed) assemble_kernel<float2, true><<<grid, kRows, 0, s>>>(a, T, a.wavenumber, gf_sing, finite_k, sign_refl);
     else assemble_kernel<float2, false><<<grid, kRows, 0, s>>>(a, T, a.wavenumber, gf_sing, finite_k, sign_refl);
   } else {

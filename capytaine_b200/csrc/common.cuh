@@ -44,6 +44,30 @@ int set_error(int code, const char* msg);
 // Running count of kernels this library has launched (bem_launch_count).
 void count_launches(int n);
 
+// Optional per-kernel device timing (bem_kernel_timer_*): while enabled, a
+// TimedLaunch scope records a CUDA event pair on the launch stream around the
+// launches it encloses, attributed to one of these kernel classes.
+enum KernelClass {
+  kKAssemble = 0,
+  kKZgemmDmma,
+  kKCgemmTf32,
+  kKCluGj,
+  kKCluPanel,
+  kKCtrsm,
+  kKZluDiag,
+  kKZluPanel,
+  kKZtrsm,
+  kKZgemmTs,
+  kKClassCount
+};
+struct TimedLaunch {
+  TimedLaunch(int kernel_class, cudaStream_t stream);
+  ~TimedLaunch();
+  int cls;
+  cudaStream_t s;
+  cudaEvent_t e0;
+};
+
 }  // namespace bem
 
 #define BEM_CUDA_CHECK(call)                                  \

@@ -545,17 +545,22 @@ extern "C" int bem_zlu_factor(void* A_dev, int n, int64_t lda, int64_t stride, i
   const int smem = 2 * kNB * kLd * (int)sizeof(double2);
   BEM_CUDA_CHECK(cudaMemsetAsync(info_dev, 0, sizeof(int) * batch, s));
   for (int kk = 0; kk < n; kk += kNB) {
-    zlu_diag_kernel<<<batch, 256, kNB * kLd * sizeof(double2), s>>>(A, lda, stride, kk, piv_dev, n, info_dev);
+    {
+      TimedLaunch tl(kKZluDiag, s);
+      zlu_diag_kernel<<<batch, 256, kNB * kLd * sizeof(double2), s>>>(A, lda, stride, kk, piv_dev, n, info_dev);
+    }
     count_launches(1);
     const int nleft = kk / kNB, nrest = (n - kk - kNB) / kNB;
     const int ntiles = nleft + 2 * nrest;
     if (ntiles > 0) {
+      TimedLaunch tl(kKZluPanel, s);
       zlu_panel_kernel<<<dim3(ntiles, batch), 256, smem, s>>>(A, lda, stride, n, kk, piv_dev, n);
       count_launches(1);
     }
     if (nrest > 0) {
       const int m = n - kk - kNB;
       dim3 grid(ceil_div(m, kBM), ceil_div(m, kBN), batch);
+      TimedLaunch tl(kKZgemmDmma, s);
       zgemm_dmma_kernel<<<grid, 128, 0, s>>>(m, m, kNB, -1.0, A + (size_t)(kk + kNB) + (size_t)kk * lda, lda, stride,
                                              A + (size_t)kk + (size_t)(kk + kNB) * lda, lda, stride, 1.0,
                                              A + (size_t)(kk + kNB) + (size_t)(kk + kNB) * lda, lda, stride);
@@ -590,6 +595,7 @@ extern "C" int bem_zlu_solve(const void* A_dev, int n, int64_t lda, int64_t stri
     double2* Bc = (double2*)B_dev + (size_t)c0 * ldb;
     for (int forward = 1; forward >= 0; --forward) {
       BEM_CUDA_CHECK(cudaMemsetAsync(flags, 0, sizeof(int) * ((size_t)batch * nblk + 1), s));
+      TimedLaunch tl(kKZtrsm, s);
       ztrsm_persistent_kernel<<<nblk * batch, 256, smem, s>>>((const double2*)A_dev, lda, stride, nblk, batch,
                                                              piv_dev, n, inv, Bc, ldb, strideB, nc, forward, flags,
                                                              ticket, err_dev);

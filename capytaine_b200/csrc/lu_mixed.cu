@@ -18,6 +18,9 @@
 //     in float64 against the float64 matrix until the relative residual of
 //     every right-hand side is below the requested tolerance.
 #include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <vector>
 #include "common.cuh"
 
@@ -34,7 +37,6 @@ constexpr int kLdB = kB + 1;   // shared leading dimension of a 128-row tile
 constexpr int kPT = 64;        // panel tile width
 constexpr int kLdP = kPT + 1;
 constexpr int kRhs = 16;       // right-hand sides per solve launch
-constexpr int kLdR = kRhs + 1;
 constexpr long long kSpin = 4000000;
 
 __device__ __forceinline__ float2 fmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
@@ -316,17 +318,43 @@ __device__ __forceinline__ void st_release_i(int* p, int v) {
 // the off-diagonal block of a dependency is copied to shared memory
 // asynchronously (real and imaginary planes, 16-byte copies) before waiting for
 // that dependency; the diagonal inverse is staged through the same buffer.
+// Thread (r, h) accumulates row r over the half h of the 128-long inner
+// dimension for all NC columns (one float pair per entry of the tile, NC/2
+// 16-byte broadcast reads of the right-hand sides); the halves meet in P.
+template <int NC>
+__device__ __forceinline__ void tile_times_rhs(const float* __restrict__ Tre, const float* __restrict__ Tim,
+                                               const float2* __restrict__ Y, int r, int h, float2 (&acc)[NC]) {
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.0f, 0.0f);
+#pragma unroll 4
+  for (int m = 64 * h; m < 64 * h + 64; ++m) {
+    const float ar = Tre[m * kB + r], ai = Tim[m * kB + r];
+    const float4* y4 = reinterpret_cast<const float4*>(Y + m * NC);
+#pragma unroll
+    for (int c2 = 0; c2 < NC / 2; ++c2) {
+      const float4 y = y4[c2];
+      acc[2 * c2].x = fmaf(ar, y.x, fmaf(-ai, y.y, acc[2 * c2].x));
+      acc[2 * c2].y = fmaf(ar, y.y, fmaf(ai, y.x, acc[2 * c2].y));
+      acc[2 * c2 + 1].x = fmaf(ar, y.z, fmaf(-ai, y.w, acc[2 * c2 + 1].x));
+      acc[2 * c2 + 1].y = fmaf(ar, y.w, fmaf(ai, y.z, acc[2 * c2 + 1].y));
+    }
+  }
+}
+
+template <int NC>
 __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nblk, int batch,
                                                                const float2* __restrict__ inv, double2* B,
                                                                int64_t ldb, int64_t strideB, int nrhs, int forward,
                                                                int* flags, int* ticket, int* err) {
   extern __shared__ __align__(16) float fsmf[];
-  float* Lre = fsmf;                       // Lre[m*kB + r], 128 x 128
+  float* Lre = fsmf;  // Lre[m*kB + r], 128 x 128
   float* Lim = Lre + kB * kB;
-  float2* X = reinterpret_cast<float2*>(Lim + kB * kB);  // X[r*kLdR + c]
-  float2* Y = X + kB * kLdR;                               // Y[m*kLdR + c]
+  float2* X = reinterpret_cast<float2*>(Lim + kB * kB);  // X[r*NC + c]
+  float2* Y = X + kB * NC;                                 // Y[m*NC + c]
+  float2* P = Y + kB * NC;                                 // P[r*NC + c]
   __shared__ int s_t;
   const int tid = threadIdx.x;
+  const int r = tid & (kB - 1), h = tid >> 7;
   if (tid == 0) s_t = atomicAdd(ticket, 1);
   __syncthreads();
   const int t = s_t;
@@ -334,14 +362,19 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   const int i = forward ? step : (nblk - 1 - step);
   double2* Bb = B + (size_t)b * strideB;
   const int r0 = i * kB;
-  for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
-    const int r = idx & (kB - 1), c = idx >> 7;
-    const double2 v = __ldcg(Bb + (size_t)(r0 + r) + (size_t)c * ldb);
-    X[r * kLdR + c] = make_float2((float)v.x, (float)v.y);
+  for (int idx = tid; idx < kB * NC; idx += blockDim.x) {
+    const int rr = idx & (kB - 1), c = idx >> 7;
+    float2 v = make_float2(0.0f, 0.0f);
+    if (c < nrhs) {
+      const double2 d = __ldcg(Bb + (size_t)(r0 + rr) + (size_t)c * ldb);
+      v = make_float2((float)d.x, (float)d.y);
+    }
+    X[rr * NC + c] = v;
   }
   const int ndep = forward ? i : (nblk - 1 - i);
   const float* Wre = W.re + (size_t)b * W.stride;
   const float* Wim = W.im + (size_t)b * W.stride;
+  float2 acc[NC];
   for (int q = 0; q < ndep; ++q) {
     const int j = forward ? q : (nblk - 1 - q);
     // off-diagonal block (does not depend on the flag): 128 columns x 128 rows,
@@ -363,33 +396,43 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
       }
     }
     __syncthreads();
-    for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
+    for (int idx = tid; idx < kB * NC; idx += blockDim.x) {
       const int m = idx & (kB - 1), c = idx >> 7;
-      const double2 v = __ldcg(Bb + (size_t)(j * kB + m) + (size_t)c * ldb);
-      Y[m * kLdR + c] = make_float2((float)v.x, (float)v.y);
+      float2 v = make_float2(0.0f, 0.0f);
+      if (c < nrhs) {
+        const double2 d = __ldcg(Bb + (size_t)(j * kB + m) + (size_t)c * ldb);
+        v = make_float2((float)d.x, (float)d.y);
+      }
+      Y[m * NC + c] = v;
     }
     cp_async_wait_all();
     __syncthreads();
-    for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
-      const int r = idx & (kB - 1), c = idx >> 7;
-      float2 acc = X[r * kLdR + c];
-#pragma unroll 8
-      for (int m = 0; m < kB; ++m) {
-        const float ar = Lre[m * kB + r], ai = Lim[m * kB + r];
-        const float2 y = Y[m * kLdR + c];
-        acc.x -= ar * y.x - ai * y.y;
-        acc.y -= ar * y.y + ai * y.x;
-      }
-      X[r * kLdR + c] = acc;
+    tile_times_rhs<NC>(Lre, Lim, Y, r, h, acc);
+    if (h == 1) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
     }
     __syncthreads();
+    if (h == 0) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float2 o = P[r * NC + c];
+        float2 x = X[r * NC + c];
+        x.x -= acc[c].x + o.x;
+        x.y -= acc[c].y + o.y;
+        X[r * NC + c] = x;
+      }
+    }
   }
   if (forward) {
     // unit block lower factor: y_i = X
-    for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
-      const int r = idx & (kB - 1), c = idx >> 7;
-      const float2 v = X[r * kLdR + c];
-      Bb[(size_t)(r0 + r) + (size_t)c * ldb] = make_double2((double)v.x, (double)v.y);
+    __syncthreads();
+    for (int idx = tid; idx < kB * NC; idx += blockDim.x) {
+      const int rr = idx & (kB - 1), c = idx >> 7;
+      if (c < nrhs) {
+        const float2 v = X[rr * NC + c];
+        Bb[(size_t)(r0 + rr) + (size_t)c * ldb] = make_double2((double)v.x, (double)v.y);
+      }
     }
     __threadfence();
     __syncthreads();
@@ -404,30 +447,27 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
     Lim[idx] = v.y;
   }
   __syncthreads();
-  float2 res[8];  // kB * kRhs / blockDim.x
-  int cnt = 0;
-  for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
-    const int r = idx & (kB - 1), c = idx >> 7;
-    float2 acc = make_float2(0.0f, 0.0f);
-#pragma unroll 8
-    for (int m = 0; m < kB; ++m) {
-      const float ar = Lre[m * kB + r], ai = Lim[m * kB + r];
-      const float2 x = X[m * kLdR + c];
-      acc.x += ar * x.x - ai * x.y;
-      acc.y += ar * x.y + ai * x.x;
-    }
-    res[cnt++] = acc;
+  tile_times_rhs<NC>(Lre, Lim, X, r, h, acc);
+  if (h == 1) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
   }
-  cnt = 0;
-  for (int idx = tid; idx < kB * nrhs; idx += blockDim.x) {
-    const int r = idx & (kB - 1), c = idx >> 7;
-    const float2 v = res[cnt++];
-    Bb[(size_t)(r0 + r) + (size_t)c * ldb] = make_double2((double)v.x, (double)v.y);
+  __syncthreads();
+  if (h == 0) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      if (c < nrhs) {
+        const float2 o = P[r * NC + c];
+        Bb[(size_t)(r0 + r) + (size_t)c * ldb] = make_double2((double)(acc[c].x + o.x), (double)(acc[c].y + o.y));
+      }
+    }
   }
   __threadfence();
   __syncthreads();
   if (tid == 0) st_release_i(flags + (size_t)b * nblk + i, 1);
 }
+
+constexpr int trsm_smem_bytes(int nc) { return 2 * kB * kB * (int)sizeof(float) + 3 * kB * nc * (int)sizeof(float2); }
 
 // x += d; r = b (copies for the residual), over (batch, n, nrhs) with leading dimension ld.
 __global__ void ir_update_kernel(double2* __restrict__ X, const double2* __restrict__ D, double2* __restrict__ R,
@@ -462,9 +502,11 @@ bool g_mixed_configured = false;
 int configure_mixed() {
   if (g_mixed_configured) return BEM_OK;
   const int panel = (kB * kLdB + kB * kLdP) * (int)sizeof(float2);
-  const int trsm = 2 * kB * kB * (int)sizeof(float) + 2 * kB * kLdR * (int)sizeof(float2);
   BEM_CUDA_CHECK(cudaFuncSetAttribute(clu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, panel));
-  BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, trsm));
+  BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      trsm_smem_bytes(8)));
+  BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      trsm_smem_bytes(16)));
   g_mixed_configured = true;
   return BEM_OK;
 }
@@ -484,10 +526,10 @@ MixedWork carve(void* work, int npad, int batch) {
   MixedWork w;
   w.W = (float*)p;
   p += (size_t)batch * 2 * npad * npad * sizeof(float);
-  w.Aop = (float*)p;
-  p += (size_t)batch * npad * 2 * kB * sizeof(float);
-  w.Bop = (float*)p;
-  p += (size_t)batch * 2 * npad * 2 * kB * sizeof(float);
+  w.Aop = (float*)p;  // two buffers of batch x npad x 256
+  p += 2 * (size_t)batch * npad * 2 * kB * sizeof(float);
+  w.Bop = (float*)p;  // two buffers of batch x 2 npad x 256
+  p += 2 * (size_t)batch * 2 * npad * 2 * kB * sizeof(float);
   w.inv = (float2*)p;
   p += (size_t)batch * nblk * kB * kB * sizeof(float2);
   w.flags = (int*)p;
@@ -495,6 +537,35 @@ MixedWork carve(void* work, int npad, int batch) {
 }
 Planes planes_of(const MixedWork& w, int npad) {
   return Planes{w.W, w.W + (size_t)npad * npad, npad, 2 * (int64_t)npad * npad};
+}
+
+// Per-device side stream (highest priority) and the two events of the lookahead
+// in the block LU.  The mutex is held while a factorisation is enqueued, so the
+// events are never re-recorded by another caller in between.
+struct Lookahead {
+  std::mutex mu;
+  cudaStream_t side = nullptr;
+  cudaEvent_t strips = nullptr;
+  cudaEvent_t panel = nullptr;
+};
+std::mutex g_lookahead_mu;
+std::map<int, std::unique_ptr<Lookahead>> g_lookahead;
+int lookahead_for_current_device(Lookahead** out) {
+  int dev = 0;
+  BEM_CUDA_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_lookahead_mu);
+  std::unique_ptr<Lookahead>& la = g_lookahead[dev];
+  if (!la) {
+    auto fresh = std::make_unique<Lookahead>();
+    int least = 0, greatest = 0;
+    BEM_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    BEM_CUDA_CHECK(cudaStreamCreateWithPriority(&fresh->side, cudaStreamNonBlocking, greatest));
+    BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->strips, cudaEventDisableTiming));
+    BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->panel, cudaEventDisableTiming));
+    la = std::move(fresh);
+  }
+  *out = la.get();
+  return BEM_OK;
 }
 
 }  // namespace
@@ -505,8 +576,8 @@ using namespace bem;
 extern "C" int64_t bem_clu_workspace_bytes(int npad, int batch) {
   if (npad <= 0 || npad % kB || batch <= 0) return -1;
   const int64_t nblk = npad / kB;
-  return (int64_t)batch * 2 * npad * (int64_t)npad * 4 + (int64_t)batch * npad * 2 * kB * 4 +
-         (int64_t)batch * 2 * npad * 2 * kB * 4 + (int64_t)batch * nblk * kB * kB * 8 +
+  return (int64_t)batch * 2 * npad * (int64_t)npad * 4 + 2 * (int64_t)batch * npad * 2 * kB * 4 +
+         2 * (int64_t)batch * 2 * npad * 2 * kB * 4 + (int64_t)batch * nblk * kB * kB * 8 +
          ((int64_t)batch * nblk + 1) * 4 + 1024;
 }
 
@@ -529,20 +600,49 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
                                                                            npad, W);
   ++launches;
   const int panel_smem = (kB * kLdB + kB * kLdP) * (int)sizeof(float2);
-  for (int kk = 0; kk < npad; kk += kB) {
-    clu_gj_kernel<<<batch, 512, 0, s>>>(W, kk, info_dev, w.inv, nblk);
+  const size_t abuf = (size_t)batch * npad * 2 * kB, bbuf = (size_t)batch * 2 * npad * 2 * kB;
+  float* Aop[2] = {w.Aop, w.Aop + abuf};
+  float* Bop[2] = {w.Bop, w.Bop + bbuf};
+  auto diag_and_panel = [&](int kk, int buf, cudaStream_t on) -> int {
+    {
+      TimedLaunch tl(kKCluGj, on);
+      clu_gj_kernel<<<batch, 512, 0, on>>>(W, kk, info_dev, w.inv, nblk);
+    }
     ++launches;
     const int nrest = (npad - kk - kB) / kPT;
     if (nrest > 0) {
-      clu_panel_kernel<<<dim3(2 * nrest, batch), 256, panel_smem, s>>>(W, npad, kk, w.inv, nblk, w.Aop, w.Bop);
+      TimedLaunch tl(kKCluPanel, on);
+      clu_panel_kernel<<<dim3(2 * nrest, batch), 256, panel_smem, on>>>(W, npad, kk, w.inv, nblk, Aop[buf],
+                                                                       Bop[buf]);
       ++launches;
     }
-    const int m = npad - kk - kB;
-    if (m > 0) {
-      st = cgemm_tf32_update(w.Aop, npad, kk + kB, w.Bop, 2 * (int64_t)npad, 2 * (kk + kB), 2 * kB, W.re, W.im,
-                             npad, W.stride, kk + kB, kk + kB, m, m, batch, err_dev, s);
-      if (st) return st;
-    }
+    return BEM_OK;
+  };
+  // C rows r0.. (m), complex columns c0.. (nc) -= L21 U12 of the block step whose
+  // packed operands are in buffer buf.
+  auto update = [&](int buf, int r0, int c0, int m, int nc) -> int {
+    if (m <= 0 || nc <= 0) return BEM_OK;
+    return cgemm_tf32_update(Aop[buf], npad, r0, Bop[buf], 2 * (int64_t)npad, 2 * c0, 2 * kB, W.re, W.im, npad,
+                             W.stride, r0, c0, m, nc, batch, err_dev, s);
+  };
+  Lookahead* la = nullptr;
+  if ((st = lookahead_for_current_device(&la))) return st;
+  std::lock_guard<std::mutex> lock(la->mu);
+  // Right-looking block LU with a lookahead of one block: after the strips of
+  // step k that block k+1 needs (its block row and block column), the inverse
+  // and panel of block k+1 run on the side stream while the rest of the
+  // trailing update of step k runs on the caller's stream.
+  diag_and_panel(0, 0, s);
+  for (int kk = 0, step = 0; kk + kB < npad; kk += kB, ++step) {
+    const int cur = step & 1, kn = kk + kB, rest = npad - kn - kB;
+    if ((st = update(cur, kn, kn, kB, npad - kn))) return st;  // block row kn
+    if ((st = update(cur, kn + kB, kn, rest, kB))) return st;  // block column kn below the diagonal
+    BEM_CUDA_CHECK(cudaEventRecord(la->strips, s));
+    BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->strips, 0));
+    diag_and_panel(kn, cur ^ 1, la->side);
+    BEM_CUDA_CHECK(cudaEventRecord(la->panel, la->side));
+    if ((st = update(cur, kn + kB, kn + kB, rest, rest))) return st;
+    BEM_CUDA_CHECK(cudaStreamWaitEvent(s, la->panel, 0));
   }
   count_launches(launches);
   BEM_CUDA_CHECK(cudaGetLastError());
@@ -560,7 +660,6 @@ extern "C" int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv
   MixedWork w = carve(work_dev, npad, batch);
   Planes W = planes_of(w, npad);
   const int nblk = npad / kB;
-  const int smem = 2 * kB * kB * (int)sizeof(float) + 2 * kB * kLdR * (int)sizeof(float2);
   int* ticket = w.flags + (size_t)batch * nblk;
   int launches = 0;
   for (int c0 = 0; c0 < nrhs; c0 += kRhs) {
@@ -568,8 +667,13 @@ extern "C" int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv
     double2* Bc = (double2*)B_dev + (size_t)c0 * ldb;
     for (int forward = 1; forward >= 0; --forward) {
       BEM_CUDA_CHECK(cudaMemsetAsync(w.flags, 0, sizeof(int) * ((size_t)batch * nblk + 1), s));
-      ctrsm_persistent_kernel<<<nblk * batch, 256, smem, s>>>(W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward,
-                                                             w.flags, ticket, err_dev);
+      TimedLaunch tl(kKCtrsm, s);
+      if (nc <= 8)
+        ctrsm_persistent_kernel<8><<<nblk * batch, 256, trsm_smem_bytes(8), s>>>(
+            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev);
+      else
+        ctrsm_persistent_kernel<16><<<nblk * batch, 256, trsm_smem_bytes(16), s>>>(
+            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev);
       ++launches;
     }
   }

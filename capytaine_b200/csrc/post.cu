@@ -56,46 +56,58 @@ __global__ void build_rhs_kernel(int n, int64_t ldb, int64_t strideB, int batch,
   }
 }
 
-constexpr int kTsRows = 128;
+constexpr int kTsRows = 256;
 constexpr int kTsMaxRhs = 16;
+constexpr int kTsUnroll = 8;
 
+// Partial products of the split-K tall GEMM: one thread per row of A, the
+// CTA's column chunk of X in shared memory (row kk holds NC right-hand sides,
+// zero beyond nrhs), kTsUnroll streamed 16-byte loads of A in flight per
+// thread before their FMAs.
+template <int NC>
 __global__ void __launch_bounds__(kTsRows) zgemm_ts_partial_kernel(int M, int K, int nrhs, int kchunk,
                                                                   const double2* __restrict__ A, int64_t lda,
                                                                   int64_t strideA, const double2* __restrict__ X,
                                                                   int64_t ldx, int64_t strideX,
                                                                   double2* __restrict__ part) {
-  extern __shared__ double2 xs[];  // kchunk x nrhs
+  extern __shared__ double2 xs[];  // xs[kk * NC + c]
   const int b = blockIdx.z;
   const int split = blockIdx.y;
   const int k0 = split * kchunk;
-  const int k1 = min(K, k0 + kchunk);
+  const int kc = min(K, k0 + kchunk) - k0;
   A += (size_t)b * strideA;
   X += (size_t)b * strideX;
-  for (int idx = threadIdx.x; idx < (k1 - k0) * nrhs; idx += blockDim.x) {
-    const int kk = idx % (k1 - k0), c = idx / (k1 - k0);
-    xs[c * kchunk + kk] = X[(size_t)(k0 + kk) + (size_t)c * ldx];
-  }
+  for (int c = 0; c < NC; ++c)
+    for (int kk = threadIdx.x; kk < kc; kk += blockDim.x)
+      xs[kk * NC + c] = (c < nrhs) ? X[(size_t)(k0 + kk) + (size_t)c * ldx] : make_double2(0.0, 0.0);
   __syncthreads();
   const int row = blockIdx.x * kTsRows + threadIdx.x;
   if (row >= M) return;
-  double2 acc[kTsMaxRhs];
+  double2 acc[NC];
 #pragma unroll
-  for (int c = 0; c < kTsMaxRhs; ++c) acc[c] = make_double2(0.0, 0.0);
+  for (int c = 0; c < NC; ++c) acc[c] = make_double2(0.0, 0.0);
   const double2* a = A + row + (size_t)k0 * lda;
-  for (int kk = 0; kk < k1 - k0; ++kk) {
-    const double2 v = __ldcs(a + (size_t)kk * lda);  // streamed once
+  for (int kk = 0; kk < kc; kk += kTsUnroll) {
+    double2 v[kTsUnroll];
 #pragma unroll
-    for (int c = 0; c < kTsMaxRhs; ++c) {
-      if (c < nrhs) {
-        const double2 x = xs[c * kchunk + kk];
-        acc[c].x += v.x * x.x - v.y * x.y;
-        acc[c].y += v.x * x.y + v.y * x.x;
+    for (int u = 0; u < kTsUnroll; ++u)
+      v[u] = (kk + u < kc) ? __ldcs(a + (size_t)(kk + u) * lda) : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int u = 0; u < kTsUnroll; ++u) {
+      if (kk + u < kc) {
+        const double2* xr = xs + (kk + u) * NC;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const double2 x = xr[c];
+          acc[c].x = fma(v[u].x, x.x, fma(-v[u].y, x.y, acc[c].x));
+          acc[c].y = fma(v[u].x, x.y, fma(v[u].y, x.x, acc[c].y));
+        }
       }
     }
   }
   double2* p = part + ((size_t)b * gridDim.y + split) * (size_t)M * nrhs;
 #pragma unroll
-  for (int c = 0; c < kTsMaxRhs; ++c)
+  for (int c = 0; c < NC; ++c)
     if (c < nrhs) p[(size_t)c * M + row] = acc[c];
 }
 
@@ -205,7 +217,7 @@ extern "C" int bem_build_rhs(int n, int batch, const double* omega_dev, const do
   return BEM_OK;
 }
 
-static int ts_nsplit(int K) { return std::max(1, std::min(64, K / 96)); }
+static int ts_nsplit(int K) { return std::max(1, std::min(24, K / 256)); }
 
 extern "C" int64_t bem_zgemm_ts_workspace_bytes(int M, int K, int nrhs, int batch) {
   return (int64_t)batch * ts_nsplit(K) * (int64_t)M * nrhs * (int64_t)sizeof(double2);
@@ -220,18 +232,26 @@ extern "C" int bem_zgemm_ts(int M, int K, int nrhs, double alpha_re, double alph
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zgemm_ts: bad arguments (nrhs must be <= 16)");
   const int nsplit = ts_nsplit(K);
   const int kchunk = ceil_div(K, nsplit);
-  const size_t smem = (size_t)kchunk * nrhs * sizeof(double2);
+  const int nc = nrhs <= 8 ? 8 : 16;
+  const size_t smem = (size_t)kchunk * nc * sizeof(double2);
   if (smem > 200 * 1024) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zgemm_ts: chunk too large");
   cudaStream_t s = (cudaStream_t)stream;
   static bool configured = false;
   if (!configured) {
-    BEM_CUDA_CHECK(cudaFuncSetAttribute(zgemm_ts_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    BEM_CUDA_CHECK(cudaFuncSetAttribute(zgemm_ts_partial_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024));
+    BEM_CUDA_CHECK(cudaFuncSetAttribute(zgemm_ts_partial_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         200 * 1024));
     configured = true;
   }
-  zgemm_ts_partial_kernel<<<dim3(ceil_div(M, kTsRows), nsplit, batch), kTsRows, smem, s>>>(
-      M, K, nrhs, kchunk, (const double2*)A_dev, lda, strideA, (const double2*)X_dev, ldx, strideX,
-      (double2*)work_dev);
+  TimedLaunch tl(kKZgemmTs, s);
+  const dim3 grid(ceil_div(M, kTsRows), nsplit, batch);
+  if (nc == 8)
+    zgemm_ts_partial_kernel<8><<<grid, kTsRows, smem, s>>>(M, K, nrhs, kchunk, (const double2*)A_dev, lda, strideA,
+                                                           (const double2*)X_dev, ldx, strideX, (double2*)work_dev);
+  else
+    zgemm_ts_partial_kernel<16><<<grid, kTsRows, smem, s>>>(M, K, nrhs, kchunk, (const double2*)A_dev, lda, strideA,
+                                                            (const double2*)X_dev, ldx, strideX, (double2*)work_dev);
   zgemm_ts_reduce_kernel<<<dim3(ceil_div(M, 256), nrhs, batch), 256, 0, s>>>(
       M, nrhs, nsplit, make_double2(alpha_re, alpha_im), make_double2(beta_re, beta_im), (const double2*)work_dev,
       (double2*)Y_dev, ldy, strideY);

@@ -13,7 +13,8 @@
 //                     2*j0 + 128 + t     : [ Im B(:, j0+t);  Re B(:, j0+t)]
 // A CTA owns a 128 x 128 complex tile of C (accumulator 128 lanes x 256 fp32
 // columns: real parts then imaginary parts).  Warp 0 streams operand slices
-// with TMA (128-byte swizzle) through a 4-stage shared-memory ring, one thread
+// with TMA (128-byte swizzle) through a 2-stage shared-memory ring (two CTAs
+// per SM, so that one CTA's epilogue overlaps the other's MMAs), one thread
 // of warp 1 issues tcgen05.mma (M=128, N=256, K=8 per instruction), warps 2-5
 // read the accumulator back with tcgen05.ld and apply C -= acc in place.
 // Every mbarrier wait is bounded; on timeout the kernel records an error and
@@ -29,7 +30,7 @@ constexpr int kTM = 128;            // tile rows
 constexpr int kTNc = 128;           // tile complex columns
 constexpr int kTN = 2 * kTNc;       // accumulator columns (MMA N)
 constexpr int kKC = 32;             // K' values per stage (128 bytes of fp32)
-constexpr int kStages = 4;
+constexpr int kStages = 2;
 constexpr int kABytes = kTM * kKC * 4;   // 16 KiB
 constexpr int kBBytes = kTN * kKC * 4;   // 32 KiB
 constexpr int kStageBytes = kABytes + kBBytes;
@@ -134,7 +135,7 @@ struct UpdateArgs {
   int* err;
 };
 
-__global__ void __launch_bounds__(192, 1) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
+__global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
                                                                    const __grid_constant__ CUtensorMap mapB,
                                                                    UpdateArgs p) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -295,7 +296,10 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
   }
   UpdateArgs p{a_row0, b_row0, c_row0, c_col0, kp / kKC, Cr, Ci, ldc, c_stride, err};
   dim3 grid(m / kTM, n / kTNc, batch);
-  cgemm_tf32_update_kernel<<<grid, 192, smem, stream>>>(mapA, mapB, p);
+  {
+    TimedLaunch tl(kKCgemmTf32, stream);
+    cgemm_tf32_update_kernel<<<grid, 192, smem, stream>>>(mapA, mapB, p);
+  }
   count_launches(1);
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;

@@ -53,6 +53,17 @@ int bem_version(void);
 /* Number of kernels this library has launched since it was loaded (all devices,
  * all threads): instrumentation for benchmarks. */
 long long bem_launch_count(void);
+/* Optional device timing per kernel class (no counterpart in the reference:
+ * benchmark instrumentation).  While enabled, launches of the classes below
+ * are bracketed by CUDA events recorded on their launch stream.  enable(0/1)
+ * discards what was recorded; read() waits for the recorded events and returns
+ * the summed duration and the number of bracketed launches of one class.
+ * Classes: 0 assemble, 1 float64 DMMA GEMM, 2 tcgen05 TF32 update, 3 Gauss-
+ * Jordan diagonal inverse, 4 mixed panel, 5 mixed block substitution, 6 float64
+ * diagonal LU, 7 float64 panel, 8 float64 triangular solve, 9 tall GEMM. */
+int bem_kernel_timer_enable(int on);
+int bem_kernel_timer_read(int kernel_class, double* total_ms_host, long long* launches_host);
+const char* bem_kernel_class_name(int kernel_class);
 
 /* ---- tabulation of the Delhommeau integrals ------------------------------- */
 /* Grid of the tabulation.  Replace delhommeau_integrals::default_r_spacing and
