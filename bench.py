@@ -48,7 +48,8 @@ def workload_config(args, n):
     return {"workload": "barge 80x20x10m, 6 dofs + diffraction (heading 0), omega linspace(0.05,3,60)",
             "nb_panels": int(n), "frequencies_per_step": int(args.batch), "engine": args.engine,
             "depth": "infinite", "l2": "inputs larger than L2 (K: 604 MB complex128 per frequency)",
-            "parallelism": f"frequency shards x{args.world}"}
+            "parallelism": f"frequency shards x{args.world}",
+            "rankine_part": "computed once per sweep of the 60 frequencies (cache cleared at each sweep start)"}
 
 
 # ---------------------------------------------------------------------------
@@ -313,6 +314,9 @@ def main():
     nb = args.batch
     batches = [my_omegas[(s * nb + np.arange(nb)) % len(my_omegas)] for s in range(args.warmup + args.steps)]
 
+    def sweep_start(s):
+        return (s * nb) % len(my_omegas) < nb
+
     def barrier():
         if dist is not None:
             dist.barrier()
@@ -335,6 +339,8 @@ def main():
     for s in range(args.warmup, args.warmup + args.steps):
         e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e_a.record()
+        if sweep_start(s):
+            gf.clear_rankine_cache()  # the Rankine part is computed once per sweep of the body
         res = engine.solve_frequencies(body, batches[s])
         e_b.record()
         step_ms.append((e_a, e_b))
@@ -372,6 +378,8 @@ def main():
     h2d = d2h = 0
     for s in range(args.warmup, args.warmup + args.steps):
         gf._mesh_cache.clear()  # mesh arrays come from host memory every step
+        if sweep_start(s):
+            gf.clear_rankine_cache()
         r = engine.solve_frequencies(body, batches[s])
         m = body.mesh_including_lid
         h2d += 8 * (m.vertices.size + 3 * 3 * m.nb_faces + 2 * m.nb_faces + 4 * m.nb_faces) + 4 * m.faces.size

@@ -318,9 +318,14 @@ struct OutT<float2> {
   __device__ static float2 make(double re, double im) { return make_float2((float)re, (float)im); }
 };
 
-template <class Out, bool MIXED>
+// RANKINE_PART: write only the wavenumber-independent Rankine part of each
+// entry, unscaled, to rank_out(I, J) = (sum of the direct and reflected Rankine
+// G, dot normal . their gradient) with the same arithmetic as the full entry.
+template <class Out, bool MIXED, bool RANKINE_PART = false>
 __global__ void __launch_bounds__(kRows) assemble_kernel(const bem_assembly_args a, TabView T, double k_wave,
-                                                         int gf_sing, bool finite_k, double sign_refl) {
+                                                         int gf_sing, bool finite_k, double sign_refl,
+                                                         double2* __restrict__ rank_out = nullptr,
+                                                         int64_t rank_ld = 0) {
   __shared__ FaceRec faces[kTileJ];
   if (T.nr > 1 && T.nz > 1) {
     // Grid bounds of the tabulation (last r and z values).
@@ -420,7 +425,7 @@ __global__ void __launch_bounds__(kRows) assemble_kernel(const bem_assembly_args
       dGre[2] += sign_refl * dGf[2];
       if (gf_sing == kLowFreqWithRankinePart) dGre[2] += 2 * k_wave * Gf;
       // ---- wave term --------------------------------------------------------
-      if (finite_k) {
+      if (finite_k && !RANKINE_PART) {
         const double dxh = M[0] - f.c[0], dyh = M[1] - f.c[1];
         const double rr = k_wave * norm2_2(dxh, dyh);
         const double zz = k_wave * (M[2] + f.c[2]);
@@ -464,6 +469,13 @@ __global__ void __launch_bounds__(kRows) assemble_kernel(const bem_assembly_args
       dGim[1] = -dGim[1];
       dGre[2] = dGre[2] - 2 * dGr[2];
     }
+    if constexpr (RANKINE_PART) {
+      const double* dn = adjoint ? nI : (a.dot_normals_dev + 3 * J);
+      const double kdot = dn[0] * dGre[0] + dn[1] * dGre[1] + dn[2] * dGre[2];
+      rank_out[(size_t)I + (size_t)rank_ld * J] = make_double2(Gre, kdot);
+      nan_seen |= isnan(Gre) || isnan(kdot);
+      continue;
+    }
     const double sre = kMinusOneOverFourPi * Gre, sim = kMinusOneOverFourPi * Gim;
     const size_t sidx = (size_t)I + (size_t)a.lds * J;
     S[sidx] = OutT<Out>::make(sre, sim);
@@ -486,6 +498,192 @@ __global__ void __launch_bounds__(kRows) assemble_kernel(const bem_assembly_args
         K[kidx + (size_t)c * a.k_plane_stride] = OutT<Out>::make(kre, kim);
         nan_seen |= isnan(kre) || isnan(kim);
       }
+    }
+  }
+  if (nan_seen && a.nan_flag_dev) atomicOr(a.nan_flag_dev, 1);
+}
+
+// Wave term of Green_wave.f90:162-271 at one point pair for a unit weight:
+// (g, gradient) with the arithmetic of wave_part<double> before its final
+// multiplication by k w.  Swapping the two points leaves g and the vertical
+// derivative unchanged and negates the horizontal derivatives exactly (they
+// are linear in x - xj), which the symmetric assembly below relies on.
+__device__ __forceinline__ void wave_core(const double x[3], const double xj[3], double k, const TabView& T,
+                                          int sing, double& gre, double& gim, double dr[3], double di[3]) {
+  const double dx = x[0] - xj[0], dy = x[1] - xj[1];
+  const double r = k * norm2_2(dx, dy);
+  const double z = k * (x[2] + xj[2]);
+  const double r1 = hypot(r, z);
+  double drdx1 = 0, drdx2 = 0;
+  if (fabs(r) > 16 * kEpsilon) {
+    drdx1 = k * k * dx / r;
+    drdx2 = k * k * dy / r;
+  }
+  const double dzdx3 = k;
+  double I[5];
+  integrals_at<double>(r, z, T, I);
+  gim = I[2];
+  di[0] = drdx1 * I[4];
+  di[1] = drdx2 * I[4];
+  di[2] = dzdx3 * I[2];
+  if (sing == kHighFreq) {
+    gre = I[1];
+    const double r13 = r1 * r1 * r1;
+    dr[0] = drdx1 * I[3] - 2 * drdx1 * r / r13;
+    dr[1] = drdx2 * I[3] - 2 * drdx2 * r / r13;
+    dr[2] = dzdx3 * gre - 2 * dzdx3 * z / r13;
+  } else {
+    gre = I[0];
+    dr[0] = drdx1 * I[3];
+    dr[1] = drdx2 * I[3];
+    dr[2] = (sing == kLowFreq) ? dzdx3 * (gre + 2 / r1) : dzdx3 * gre;
+  }
+}
+
+constexpr int kSymT = 128;    // square tile: 128 rows x 128 columns, one thread per row
+constexpr int kSymChunk = 8;  // columns per mirrored write-back
+
+struct SymFace {
+  double x[3];   // collocation point = quadrature point = centre
+  double dn[3];  // dot normal of the face
+  double area, w, zc;
+};
+
+// S and K of a mesh with itself from a cached Rankine part: the CTA of tile
+// (bi, bj), bi <= bj, evaluates the wave term once per pair (I, J) and writes
+// both (I, J) and, off the diagonal tiles, (J, I) (through shared memory, so
+// that the mirrored stores stay coalesced).  FP64, complex128 outputs, K with
+// the dot product taken.
+__global__ void __launch_bounds__(kSymT) wave_symmetric_kernel(const bem_assembly_args a, TabView T, double k,
+                                                               int gf_sing, const double2* __restrict__ rank,
+                                                               int64_t rank_ld) {
+  const int bi = blockIdx.x, bj = blockIdx.y;
+  if (bi > bj) return;
+  __shared__ SymFace faces[kSymT];
+  __shared__ double4 mir[kSymChunk][kSymT];  // (S_w re, S_w im, K_w re, K_w im) of entries (J, I)
+  if (T.nr > 1 && T.nz > 1) {
+    T.rmax = __ldg(T.r_range + T.nr - 1);
+    T.zlast = __ldg(T.z_range + T.nz - 1);
+  }
+  const int tid = threadIdx.x;
+  const int N = a.n;
+  const int I0 = bi * kSymT, J0 = bj * kSymT;
+  {
+    const int J = J0 + tid;
+    if (J < N) {
+      SymFace& f = faces[tid];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        f.x[d] = a.points_dev[3 * J + d];
+        f.dn[d] = a.dot_normals_dev[3 * J + d];
+      }
+      f.area = a.areas_dev[J];
+      f.w = a.quad_weights_dev[J];
+      f.zc = a.centers_dev[3 * J + 2];
+    }
+  }
+  __syncthreads();
+  const int I = I0 + tid;
+  const bool row_ok = I < N;
+  const bool diag_tile = bi == bj;
+  const bool adjoint = a.adjoint_double_layer != 0;
+  double M[3] = {0, 0, 0}, nI[3] = {0, 0, 0}, wI = 0, zcI = 0;
+  if (row_ok) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      M[d] = a.points_dev[3 * I + d];
+      nI[d] = a.dot_normals_dev[3 * I + d];
+    }
+    wI = a.quad_weights_dev[I];
+    zcI = a.centers_dev[3 * I + 2];
+  }
+  const double kwI = k * wI;
+  double2* S = reinterpret_cast<double2*>(a.S_dev);
+  double2* K = reinterpret_cast<double2*>(a.K_dev);
+  bool nan_seen = false;
+  const int nJ = min(kSymT, N - J0);
+  for (int jc = 0; jc < nJ; jc += kSymChunk) {
+#pragma unroll 1
+    for (int u = 0; u < kSymChunk; ++u) {
+      const int jj = jc + u;
+      if (!row_ok || jj >= nJ) continue;
+      const SymFace& f = faces[jj];
+      const int J = J0 + jj;
+      double gre, gim, dr[3], di[3];
+      bool self_fs = false;
+      {
+        const double rr = k * norm2_2(M[0] - f.x[0], M[1] - f.x[1]);
+        const double zz = k * (M[2] + f.x[2]);
+        self_fs = fabs(rr) < kLit1em10 && fabs(zz) < kLit1em10;
+      }
+      const double2 rk = rank[(size_t)I + (size_t)rank_ld * J];
+      double sre, sim, kre, kim;
+      if (self_fs) {
+        // Green_wave.f90:128-158, panel on the free surface with itself (I == J)
+        const double re = (1 - log(k * k * f.area / kPI)) + 2 * (kEulerGamma - kLog2);
+        const double ka = k * f.area;
+        const double g_re = ka * re, g_im = ka * (-2 * kPI);
+        const double dz_re = k * (g_re + 4 * sqrt(kPI * f.area)), dz_im = k * g_im;
+        const double* dn = adjoint ? nI : f.dn;
+        sre = kMinusOneOverFourPi * (rk.x + g_re);
+        sim = kMinusOneOverFourPi * g_im;
+        kre = kMinusOneOverFourPi * (rk.y + dn[2] * dz_re);
+        kim = kMinusOneOverFourPi * (dn[2] * dz_im);
+      } else {
+        wave_core(M, f.x, k, T, gf_sing, gre, gim, dr, di);
+        const double kwJ = k * f.w;
+        double vr[3] = {kwJ * dr[0], kwJ * dr[1], kwJ * dr[2]};
+        double vi[3] = {kwJ * di[0], kwJ * di[1], kwJ * di[2]};
+        if (!adjoint) {
+          vr[0] = -vr[0];
+          vr[1] = -vr[1];
+          vi[0] = -vi[0];
+          vi[1] = -vi[1];
+        }
+        const double* dn = adjoint ? nI : f.dn;
+        sre = kMinusOneOverFourPi * (rk.x + kwJ * gre);
+        sim = kMinusOneOverFourPi * (kwJ * gim);
+        kre = kMinusOneOverFourPi * (rk.y + (dn[0] * vr[0] + dn[1] * vr[1] + dn[2] * vr[2]));
+        kim = kMinusOneOverFourPi * (dn[0] * vi[0] + dn[1] * vi[1] + dn[2] * vi[2]);
+        if (!diag_tile) {
+          // entry (J, I): horizontal derivatives change sign
+          double wr[3] = {-kwI * dr[0], -kwI * dr[1], kwI * dr[2]};
+          double wi[3] = {-kwI * di[0], -kwI * di[1], kwI * di[2]};
+          if (!adjoint) {
+            wr[0] = -wr[0];
+            wr[1] = -wr[1];
+            wi[0] = -wi[0];
+            wi[1] = -wi[1];
+          }
+          const double* dm = adjoint ? f.dn : nI;
+          mir[u][tid] = make_double4(kwI * gre, kwI * gim, dm[0] * wr[0] + dm[1] * wr[1] + dm[2] * wr[2],
+                                     dm[0] * wi[0] + dm[1] * wi[1] + dm[2] * wi[2]);
+        }
+      }
+      if (a.diagonal_term && I == J) kre += (fabs(zcI - a.free_surface) < kLit1em8) ? 1.0 : 0.5;
+      S[(size_t)I + (size_t)a.lds * J] = make_double2(sre, sim);
+      K[(size_t)I + (size_t)a.ldk * J] = make_double2(kre, kim);
+      nan_seen |= isnan(sre) || isnan(sim) || isnan(kre) || isnan(kim);
+    }
+    if (!diag_tile) {
+      __syncthreads();
+      // mirrored entries: rows J0 + jc + u, columns I0 + c; 8 threads per column
+      const int u = tid & (kSymChunk - 1);
+      const int J = J0 + jc + u;
+#pragma unroll 1
+      for (int c = tid >> 3; c < kSymT; c += kSymT / kSymChunk) {
+        const int Ic = I0 + c;
+        if (jc + u < nJ && Ic < N) {
+          const double4 m = mir[u][c];
+          const double2 rk = rank[(size_t)J + (size_t)rank_ld * Ic];
+          const double sre = kMinusOneOverFourPi * (rk.x + m.x), sim = kMinusOneOverFourPi * m.y;
+          const double kre = kMinusOneOverFourPi * (rk.y + m.z), kim = kMinusOneOverFourPi * m.w;
+          S[(size_t)J + (size_t)a.lds * Ic] = make_double2(sre, sim);
+          K[(size_t)J + (size_t)a.ldk * Ic] = make_double2(kre, kim);
+          nan_seen |= isnan(sre) || isnan(sim) || isnan(kre) || isnan(kim);
+        }
+      }
+      __syncthreads();
     }
   }
   if (nan_seen && a.nan_flag_dev) atomicOr(a.nan_flag_dev, 1);
@@ -540,6 +738,91 @@ extern "C" int bem_assemble(const bem_assembly_args* args, void* stream) {
     else assemble_kernel<float2, false><<<grid, kRows, 0, s>>>(a, T, a.wavenumber, gf_sing, finite_k, sign_refl);
   } else {
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: unknown out_dtype");
+  }
+  count_launches(1);
+  BEM_CUDA_CHECK(cudaGetLastError());
+  return BEM_OK;
+}
+
+namespace {
+int check_common(const bem_assembly_args& a, const char* who) {
+  using namespace bem;
+  char msg[200];
+  if (a.n <= 0 || a.nb_faces <= 0) {
+    std::snprintf(msg, sizeof(msg), "%s: empty mesh", who);
+    return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+  }
+  if (!a.points_dev || !a.vertices_dev || !a.faces_dev || !a.centers_dev || !a.normals_dev || !a.areas_dev ||
+      !a.radii_dev || !a.quad_points_dev || !a.quad_weights_dev || !a.dot_normals_dev) {
+    std::snprintf(msg, sizeof(msg), "%s: null pointer", who);
+    return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+  }
+  if (std::isinf(a.free_surface) || a.gf_singularities == BEM_GF_LOW_FREQ_WITH_RANKINE_PART || !a.early_dot_product) {
+    std::snprintf(msg, sizeof(msg),
+                  "%s: needs a free surface, early dot product and gf_singularities high_freq or low_freq", who);
+    return set_error(BEM_ERR_UNSUPPORTED, msg);
+  }
+  return BEM_OK;
+}
+}  // namespace
+
+extern "C" int bem_assemble_rankine_part(const bem_assembly_args* args, void* out_dev, int64_t ld, void* stream) {
+  using namespace bem;
+  if (!args || !out_dev) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_rankine_part: null pointer");
+  const bem_assembly_args& a = *args;
+  int st = check_common(a, "bem_assemble_rankine_part");
+  if (st) return st;
+  if (ld < a.n) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_rankine_part: ld < n");
+  // the reflected-term sign of the variant used at this wavenumber (delhommeau.py:472-487)
+  int gf_sing = a.gf_singularities;
+  if (a.wavenumber == 0.0) gf_sing = kLowFreq;
+  else if (std::isinf(a.wavenumber)) gf_sing = kHighFreq;
+  const double sign_refl = (gf_sing == kHighFreq) ? -1.0 : 1.0;
+  const TabView T{0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0};
+  dim3 grid(ceil_div(a.n, kRows), ceil_div(a.nb_faces, kTileJ));
+  cudaStream_t s = (cudaStream_t)stream;
+  {
+    TimedLaunch tl(kKAssemble, s);
+    assemble_kernel<double2, false, true><<<grid, kRows, 0, s>>>(a, T, a.wavenumber, gf_sing, false, sign_refl,
+                                                                 (double2*)out_dev, ld);
+  }
+  count_launches(1);
+  BEM_CUDA_CHECK(cudaGetLastError());
+  return BEM_OK;
+}
+
+extern "C" int bem_assemble_wave_symmetric(const bem_assembly_args* args, const void* rankine_dev, int64_t ld,
+                                           void* stream) {
+  using namespace bem;
+  if (!args || !rankine_dev) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_wave_symmetric: null pointer");
+  const bem_assembly_args& a = *args;
+  int st = check_common(a, "bem_assemble_wave_symmetric");
+  if (st) return st;
+  if (!a.S_dev || !a.K_dev) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_wave_symmetric: null output");
+  if (a.n != a.nb_faces || a.nb_quad_points != 1 || a.points_dev != a.quad_points_dev ||
+      a.centers_dev != a.quad_points_dev)
+    return set_error(BEM_ERR_INVALID_ARGUMENT,
+                     "bem_assemble_wave_symmetric: needs one mesh, one quadrature point per face, and the same "
+                     "array for points, centres and quadrature points");
+  if (!(a.wavenumber > 0.0) || !std::isfinite(a.wavenumber))
+    return set_error(BEM_ERR_UNSUPPORTED, "bem_assemble_wave_symmetric: wavenumber must be finite and > 0");
+  if (a.out_dtype != BEM_DTYPE_C128 || a.precision != BEM_PREC_FP64)
+    return set_error(BEM_ERR_UNSUPPORTED, "bem_assemble_wave_symmetric: complex128 outputs, float64 only");
+  if (a.lds < a.n || a.ldk < a.n || ld < a.n)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_wave_symmetric: leading dimension < n");
+  const bool tabulated = a.nr > 1 && a.nz > 1;
+  if (tabulated && (!a.r_range_dev || !a.z_range_dev || !a.table_dev))
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_wave_symmetric: tabulation pointers missing");
+  if (!tabulated && a.tabulation_nb_integration_points <= 0)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_wave_symmetric: nb_integration_points <= 0");
+  const TabView T{a.tabulation_nb_integration_points, a.tabulation_grid_shape, a.nr, a.nz, a.r_range_dev,
+                  a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0};
+  const int nb = ceil_div(a.n, kSymT);
+  cudaStream_t s = (cudaStream_t)stream;
+  {
+    TimedLaunch tl(kKAssemble, s);
+    wave_symmetric_kernel<<<dim3(nb, nb), kSymT, 0, s>>>(a, T, a.wavenumber, a.gf_singularities,
+                                                         (const double2*)rankine_dev, ld);
   }
   count_launches(1);
   BEM_CUDA_CHECK(cudaGetLastError());

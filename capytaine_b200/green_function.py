@@ -66,6 +66,8 @@ class DeviceMesh:
         self.quad_points = torch.as_tensor(np.ascontiguousarray(qp), **f64)
         self.quad_weights = torch.as_tensor(np.ascontiguousarray(qw), **f64)
         self.centers_z = np.asarray(mesh.faces_centers[:, 2])
+        # one quadrature point per face, at the face centre (collocation point)
+        self.collocation_at_quadrature = bool(qp.shape[1] == 1 and np.array_equal(qp[:, 0, :], mesh.faces_centers))
         self.nbytes = sum(t.numel() * t.element_size() for t in
                           (self.vertices, self.faces, self.centers, self.normals, self.areas, self.radii,
                            self.quad_points, self.quad_weights))
@@ -119,6 +121,10 @@ class Delhommeau:
         self._tab_host = None
         self._dev_tab = None
         self._mesh_cache: "OrderedDict[str, DeviceMesh]" = OrderedDict()
+        # Rankine parts of mesh-with-itself assemblies, reused across wavenumbers
+        # (device memory budget in bytes; 0 disables the reuse).
+        self.rankine_cache_bytes = 4 << 30
+        self._rankine_cache: "OrderedDict[tuple, object]" = OrderedDict()
         self.exportable_settings = {
             "green_function": self.__class__.__name__,
             "tabulation_nr": tabulation_nr,
@@ -316,7 +322,41 @@ class Delhommeau:
             k_plane_stride=k_plane_stride if k_plane_stride is not None else 0,
             nan_flag_dev=nan_flag.data_ptr() if nan_flag is not None else 0,
         )
-        _lib.check(_lib.load().bem_assemble(a, _lib.stream_ptr(stream)))
+        lib = _lib.load()
+        same_mesh = hasattr(mesh1, "faces_centers") and mesh1.content_hash == mesh2.content_hash
+        if (same_mesh and dm2.collocation_at_quadrature and need_wave and sing in ("low_freq", "high_freq")
+                and prec == "fp64" and dtype == _lib.BEM_DTYPE_C128 and early_dot_product
+                and 16 * n * n <= self.rankine_cache_bytes):
+            # Rankine part reused across wavenumbers; wave term once per pair of faces.
+            q = dm2.quad_points.data_ptr()
+            a.points_dev = a.centers_dev = a.quad_points_dev = q
+            rank = self._rankine_part(mesh2.content_hash, dm2, a, bool(adjoint_double_layer), sing,
+                                      float(free_surface), stream)
+            _lib.check(lib.bem_assemble_wave_symmetric(a, rank.data_ptr(), n, _lib.stream_ptr(stream)))
+            return
+        _lib.check(lib.bem_assemble(a, _lib.stream_ptr(stream)))
+
+    def _rankine_part(self, mesh_key, dm, args, adjoint, sing, free_surface, stream):
+        """Device array of the wavenumber-independent Rankine part of a mesh with
+        itself (bem_assemble_rankine_part), cached per mesh and variant."""
+        import torch
+        key = (mesh_key, adjoint, sing == "high_freq", free_surface)
+        rank = self._rankine_cache.get(key)
+        if rank is not None:
+            self._rankine_cache.move_to_end(key)
+            return rank
+        n = dm.nb_faces
+        while self._rankine_cache and (sum(t.numel() * 16 for t in self._rankine_cache.values()) + 16 * n * n
+                                       > self.rankine_cache_bytes):
+            self._rankine_cache.popitem(last=False)
+        rank = torch.empty((n, n), dtype=torch.complex128, device=self.device)
+        _lib.check(_lib.load().bem_assemble_rankine_part(args, rank.data_ptr(), n, _lib.stream_ptr(stream)))
+        self._rankine_cache[key] = rank
+        return rank
+
+    def clear_rankine_cache(self):
+        """Release the cached Rankine parts."""
+        self._rankine_cache.clear()
 
     def evaluate_device(self, mesh1, mesh2, *, free_surface=0.0, water_depth=np.inf, wavenumber=1.0,
                         adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True,

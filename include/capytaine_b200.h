@@ -130,6 +130,26 @@ typedef struct {
  * green_functions/delhommeau.py:377-390 and 498-515. */
 int bem_assemble(const bem_assembly_args* args, void* stream);
 
+/* Wavenumber-independent part of the assembly, kept for reuse across
+ * frequencies (no counterpart in the reference, which recomputes it for every
+ * frequency in matrices.f90:28-432): out(I, J) = (direct + reflected Rankine G,
+ * dot normal . their gradient), unscaled, column-major complex128 with leading
+ * dimension ld, the diagonal term excluded.  Same arguments as bem_assemble
+ * (S/K unused); the reflected-term sign follows the variant in force at
+ * args->wavenumber.  Needs a free surface, early_dot_product and
+ * gf_singularities high_freq or low_freq. */
+int bem_assemble_rankine_part(const bem_assembly_args* args, void* out_dev, int64_t ld, void* stream);
+
+/* S and K of a mesh with itself at args->wavenumber (finite, > 0) from a Rankine
+ * part made by bem_assemble_rankine_part with the same arguments: the wave term
+ * (Green_wave.f90:50-271) is evaluated once per unordered pair of faces and
+ * written to both entries (it is symmetric, its horizontal gradient changes
+ * sign).  Same results as bem_assemble up to rounding.  Needs n == nb_faces, one
+ * quadrature point per face, the same device array for points_dev, centers_dev
+ * and quad_points_dev (collocation at the quadrature points), float64
+ * precision and complex128 outputs. */
+int bem_assemble_wave_symmetric(const bem_assembly_args* args, const void* rankine_dev, int64_t ld, void* stream);
+
 /* ---- dense complex128 linear algebra (batched) ---------------------------- */
 /* Matrices are column-major complex128 (interleaved re, im), `batch` of them
  * `stride` elements apart.  n must be a multiple of 64: pad the system with the

@@ -1,0 +1,94 @@
+"""The mesh-with-itself fast path of the assembly (Rankine part computed once
+and reused across wavenumbers; wave term evaluated once per unordered pair of
+faces and mirrored) against the general kernel that evaluates every entry on
+its own.  Both are float64; they differ only in rounding order, so the bar is
+1e-13 relative to the largest entry.  Parity of the fast path with the oracle
+is covered by test_gpu_assembly.py, whose mesh-with-itself cases take it."""
+import os
+
+import numpy as np
+import pytest
+
+from capytaine_b200.meshes import Mesh, mesh_sphere, mesh_rectangle, mesh_parallelepiped
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-13
+
+
+def _gf(default_oracle_gf, tmp_path, **kw):
+    from capytaine_b200.green_function import Delhommeau
+    gf = Delhommeau(tabulation_cache_dir=str(tmp_path), **kw)
+    np.savez(os.path.join(str(tmp_path), gf._cache_filename), r_range=default_oracle_gf.tabulated_r_range,
+             z_range=default_oracle_gf.tabulated_z_range, values=default_oracle_gf.tabulated_integrals)
+    return gf
+
+
+def _close(a, b, rtol=RTOL):
+    err = np.abs(a - b).max() / np.abs(b).max()
+    assert err <= rtol, err
+
+
+def _lid_mesh():
+    hull = mesh_sphere(radius=2.0, resolution=(10, 16)).immersed_part()
+    lid = mesh_rectangle(size=(1.6, 1.6), resolution=(4, 4), center=(0, 0, 0), normal=(0, 0, 1))
+    return Mesh.join_meshes(hull, lid)
+
+
+MESHES = {
+    "hemisphere_lid": _lid_mesh,  # free-surface panels: self term of Green_wave.f90:128-158
+    "barge_300": lambda: mesh_parallelepiped(size=(10, 3, 3), resolution=(20, 6, 6)).immersed_part(),
+}
+
+
+@pytest.mark.parametrize("mesh_name", sorted(MESHES))
+@pytest.mark.parametrize("sing", ["low_freq", "high_freq"])
+@pytest.mark.parametrize("adjoint", [True, False])
+def test_symmetric_path_matches_general_kernel(default_oracle_gf, tmp_path, mesh_name, sing, adjoint):
+    mesh = MESHES[mesh_name]()
+    fast = _gf(default_oracle_gf, tmp_path, gf_singularities=sing)
+    general = _gf(default_oracle_gf, tmp_path, gf_singularities=sing)
+    general.rankine_cache_bytes = 0
+    # small, medium and large k (the last one reaches the asymptotic branch)
+    for k in (0.05, 1.3, 40.0):
+        S, K = fast.evaluate(mesh, mesh, wavenumber=k, adjoint_double_layer=adjoint)
+        S0, K0 = general.evaluate(mesh, mesh, wavenumber=k, adjoint_double_layer=adjoint)
+        _close(S, S0)
+        _close(K, K0)
+    assert len(fast._rankine_cache) == 1 and len(general._rankine_cache) == 0
+
+
+def test_rankine_cache_keys_and_budget(default_oracle_gf, tmp_path):
+    mesh = MESHES["barge_300"]()
+    gf = _gf(default_oracle_gf, tmp_path)
+    n = mesh.nb_faces
+    gf.evaluate(mesh, mesh, wavenumber=1.0)
+    gf.evaluate(mesh, mesh, wavenumber=2.0)
+    assert len(gf._rankine_cache) == 1
+    gf.evaluate(mesh, mesh, wavenumber=2.0, adjoint_double_layer=False)
+    assert len(gf._rankine_cache) == 2
+    gf.evaluate(mesh, mesh, wavenumber=0.5)  # a hit
+    assert len(gf._rankine_cache) == 2
+    gf.rankine_cache_bytes = 16 * n * n  # room for one: a new mesh evicts both
+    small = mesh_sphere(resolution=(6, 8)).immersed_part()
+    gf.evaluate(small, small, wavenumber=0.5)
+    assert len(gf._rankine_cache) == 1
+    gf.clear_rankine_cache()
+    assert len(gf._rankine_cache) == 0
+
+
+def test_padded_leading_dimensions(default_oracle_gf, tmp_path):
+    """The engine's padded layout (lds, ldk > n) through the fast path."""
+    import torch
+    mesh = MESHES["barge_300"]()
+    gf = _gf(default_oracle_gf, tmp_path)
+    n = mesh.nb_faces
+    ld = n + 37
+    S = torch.full((n, ld), complex(7, 7), dtype=torch.complex128, device="cuda")
+    K = torch.full((n, ld), complex(7, 7), dtype=torch.complex128, device="cuda")
+    gf.assemble_into(mesh, mesh, S, K, wavenumber=0.8, lds=ld, ldk=ld)
+    S_ref, K_ref = gf.evaluate(mesh, mesh, wavenumber=0.8)
+    # column-major (n x n) with leading dimension ld: column J at S[J, :n]
+    _close(S[:, :n].cpu().numpy().T, S_ref)
+    _close(K[:, :n].cpu().numpy().T, K_ref)
+    assert torch.all(S[:, n:] == complex(7, 7)) and torch.all(K[:, n:] == complex(7, 7))

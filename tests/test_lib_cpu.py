@@ -47,6 +47,37 @@ def test_invalid_arguments_are_rejected_without_gpu(lib):
     assert lib.bem_default_r_spacing(-1, 100.0, 1, None) == _lib.BEM_ERR_INVALID_ARGUMENT
 
 
+def test_symmetric_assembly_preconditions_checked_on_host(lib):
+    """The mesh-with-itself fast path refuses, before any launch, inputs it
+    does not cover (the host falls back to bem_assemble for those)."""
+    fake = 4096  # never dereferenced: every call below fails its host checks
+    a = _lib.AssemblyArgs(n=10, points_dev=fake, dot_normals_dev=fake, nb_faces=12, nb_vertices=4,
+                          vertices_dev=fake, faces_dev=fake, centers_dev=fake, normals_dev=fake, areas_dev=fake,
+                          radii_dev=fake, nb_quad_points=1, quad_points_dev=fake, quad_weights_dev=fake,
+                          wavenumber=1.0, free_surface=0.0, gf_singularities=_lib.BEM_GF_LOW_FREQ,
+                          adjoint_double_layer=1, early_dot_product=1, diagonal_term=1,
+                          precision=_lib.BEM_PREC_FP64, out_dtype=_lib.BEM_DTYPE_C128, S_dev=fake, K_dev=fake,
+                          lds=12, ldk=12)
+    assert lib.bem_assemble_wave_symmetric(a, fake, 12, None) == _lib.BEM_ERR_INVALID_ARGUMENT  # n != nb_faces
+    assert b"one mesh" in lib.bem_last_error()
+    a.n = 12
+    a.points_dev = 8192  # collocation points not the quadrature points
+    assert lib.bem_assemble_wave_symmetric(a, fake, 12, None) == _lib.BEM_ERR_INVALID_ARGUMENT
+    a.points_dev = fake
+    a.wavenumber = float("inf")
+    assert lib.bem_assemble_wave_symmetric(a, fake, 12, None) == _lib.BEM_ERR_UNSUPPORTED
+    a.wavenumber = 1.0
+    a.gf_singularities = _lib.BEM_GF_LOW_FREQ_WITH_RANKINE_PART
+    assert lib.bem_assemble_rankine_part(a, fake, 12, None) == _lib.BEM_ERR_UNSUPPORTED
+    assert lib.bem_assemble_wave_symmetric(a, fake, 12, None) == _lib.BEM_ERR_UNSUPPORTED
+    a.gf_singularities = _lib.BEM_GF_LOW_FREQ
+    a.free_surface = float("inf")
+    assert lib.bem_assemble_rankine_part(a, fake, 12, None) == _lib.BEM_ERR_UNSUPPORTED
+    a.free_surface = 0.0
+    assert lib.bem_assemble_rankine_part(a, fake, 11, None) == _lib.BEM_ERR_INVALID_ARGUMENT  # ld < n
+    assert lib.bem_assemble_rankine_part(a, None, 12, None) == _lib.BEM_ERR_INVALID_ARGUMENT
+
+
 _STRUCTS = {"bem_assembly_args": _lib.AssemblyArgs}
 
 
