@@ -155,6 +155,13 @@ def fp64_tensor_peak_tflops():
     return best
 
 
+# DRAM bytes per algorithmic flop of the trailing-update GEMM, from one ncu
+# capture of a full-size launch (m = 5632: 466.0 MB read + written for 32.5 GFLOP;
+# profiles/cgemm_tf32_update_kernel_barge6084.md); the traffic of the average
+# launch is scaled from it by its flops.
+CGEMM_DRAM_BYTES_PER_FLOP = 466.0e6 / (8 * 5632 ** 2 * 128)
+
+
 def lu_update_flops(npad, block):
     """Real flops of the trailing updates of one blocked complex LU: sum over
     the block steps of 8 m^2 b for an m x m update of depth b."""
@@ -177,7 +184,10 @@ def kernel_roofline(kernels, n, frequencies, engine, peaks, peak_src):
         return base | {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
                        "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run (TF32 has no entry in "
                                       "MEASURED_PEAKS.json)",
-                       "algorithmic": "8 m^2 128 real flops per complex update of m x m by depth 128"}
+                       "algorithmic": "8 m^2 128 real flops per complex update of m x m by depth 128",
+                       "traffic": flops * CGEMM_DRAM_BYTES_PER_FLOP,
+                       "traffic_note": "DRAM bytes per launch, ncu capture of an m=5632 launch scaled by flops",
+                       "hbm_bound_frac": (flops * CGEMM_DRAM_BYTES_PER_FLOP / avg_s / 1e9) / peaks["hbm_gbs"]}
     if name == "zgemm_dmma_kernel":
         npad = -(-n // 64) * 64
         flops = lu_update_flops(npad, 64) * frequencies / k["launches"]
@@ -282,7 +292,7 @@ def main():
     ap.add_argument("--engine", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--fp64-steps", type=int, default=4,
                     help="timed steps of the float64 engine for the refined-mixed vs float64 comparison (0: skip)")
-    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -29,6 +29,10 @@ namespace bem {
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream);
+int zgemm_ts_enqueue(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
+                     int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,
+                     double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev,
+                     void* stream, const int* skip);
 
 namespace {
 
@@ -345,7 +349,8 @@ template <int NC>
 __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nblk, int batch,
                                                                const float2* __restrict__ inv, double2* B,
                                                                int64_t ldb, int64_t strideB, int nrhs, int forward,
-                                                               int* flags, int* ticket, int* err) {
+                                                               int* flags, int* ticket, int* err, const int* skip) {
+  if (skip && *skip) return;  // refinement already converged
   extern __shared__ __align__(16) float fsmf[];
   float* Lre = fsmf;  // Lre[m*kB + r], 128 x 128
   float* Lim = Lre + kB * kB;
@@ -469,13 +474,14 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
 
 constexpr int trsm_smem_bytes(int nc) { return 2 * kB * kB * (int)sizeof(float) + 3 * kB * nc * (int)sizeof(float2); }
 
-// x += d; r = b (copies for the residual), over (batch, n, nrhs) with leading dimension ld.
-__global__ void ir_update_kernel(double2* __restrict__ X, const double2* __restrict__ D, double2* __restrict__ R,
-                                 const double2* __restrict__ Bv, int n, int nrhs, int64_t ld, int64_t stride) {
+// x += r (the correction solved in place in r), then r = b for the residual.
+__global__ void ir_update_kernel(double2* __restrict__ X, double2* __restrict__ R, const double2* __restrict__ Bv,
+                                 int n, int nrhs, int64_t ld, int64_t stride, const int* skip) {
+  if (skip && *skip) return;
   const int b = blockIdx.z, c = blockIdx.y;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const size_t o = (size_t)b * stride + (size_t)c * ld + r;
-    const double2 x = X[o], d = D[o];
+    const double2 x = X[o], d = R[o];
     X[o] = make_double2(x.x + d.x, x.y + d.y);
     R[o] = Bv[o];
   }
@@ -483,7 +489,8 @@ __global__ void ir_update_kernel(double2* __restrict__ X, const double2* __restr
 
 // Squared norms of columns: out[(b*nrhs + c)] = sum |V(:, c)|^2 over n rows.
 __global__ void colnorm2_kernel(const double2* __restrict__ V, int n, int64_t ld, int64_t stride,
-                                double* __restrict__ out) {
+                                double* __restrict__ out, const int* skip) {
+  if (skip && *skip) return;
   const int c = blockIdx.x, b = blockIdx.y, nrhs = gridDim.x;
   const double2* v = V + (size_t)b * stride + (size_t)c * ld;
   double s = 0.0;
@@ -496,6 +503,28 @@ __global__ void colnorm2_kernel(const double2* __restrict__ V, int n, int64_t ld
     __syncthreads();
   }
   if (threadIdx.x == 0) out[(size_t)b * nrhs + c] = red[0];
+}
+
+// Convergence test of one refinement iteration on the device: worst relative
+// residual max_v sqrt(|r_v|^2 / |b_v|^2) (absolute where b_v = 0), iteration
+// count; sets *done when worst <= tol so that the iterations enqueued after
+// this one return at once.  state: [worst, iterations].
+__global__ void refine_check_kernel(const double* __restrict__ bn, const double* __restrict__ rn, int nvec,
+                                    double tol, int* done, double* state) {
+  if (*done) return;
+  __shared__ double red[32];
+  double worst = 0.0;
+  for (int v = threadIdx.x; v < nvec; v += blockDim.x)
+    worst = fmax(worst, bn[v] > 0.0 ? sqrt(rn[v] / bn[v]) : sqrt(rn[v]));
+  for (int off = 16; off > 0; off >>= 1) worst = fmax(worst, __shfl_xor_sync(0xffffffffu, worst, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = worst;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) worst = fmax(worst, red[w]);
+    state[0] = worst;
+    state[1] += 1.0;
+    if (worst <= tol) *done = 1;
+  }
 }
 
 bool g_mixed_configured = false;
@@ -578,7 +607,7 @@ extern "C" int64_t bem_clu_workspace_bytes(int npad, int batch) {
   const int64_t nblk = npad / kB;
   return (int64_t)batch * 2 * npad * (int64_t)npad * 4 + 2 * (int64_t)batch * npad * 2 * kB * 4 +
          2 * (int64_t)batch * 2 * npad * 2 * kB * 4 + (int64_t)batch * nblk * kB * kB * 8 +
-         ((int64_t)batch * nblk + 1) * 4 + 1024;
+         ((int64_t)batch * nblk + 2) * 4 + 1024;
 }
 
 extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
@@ -649,14 +678,12 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
   return BEM_OK;
 }
 
-extern "C" int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv_dev, void* B_dev, int64_t ldb,
-                             int64_t strideB, int nrhs, int* err_dev, void* stream) {
-  if (!work_dev || !piv_dev || !B_dev || !err_dev || npad <= 0 || npad % kB || batch <= 0 || nrhs <= 0 ||
-      ldb < npad)
-    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_clu_solve: bad arguments");
+namespace bem {
+namespace {
+int clu_solve_enqueue(void* work_dev, int npad, int batch, void* B_dev, int64_t ldb, int64_t strideB, int nrhs,
+                      int* err_dev, cudaStream_t s, const int* skip) {
   int st = configure_mixed();
   if (st) return st;
-  cudaStream_t s = (cudaStream_t)stream;
   MixedWork w = carve(work_dev, npad, batch);
   Planes W = planes_of(w, npad);
   const int nblk = npad / kB;
@@ -670,16 +697,27 @@ extern "C" int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv
       TimedLaunch tl(kKCtrsm, s);
       if (nc <= 8)
         ctrsm_persistent_kernel<8><<<nblk * batch, 256, trsm_smem_bytes(8), s>>>(
-            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev);
+            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip);
       else
         ctrsm_persistent_kernel<16><<<nblk * batch, 256, trsm_smem_bytes(16), s>>>(
-            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev);
+            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip);
       ++launches;
     }
   }
   count_launches(launches);
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
+}
+}  // namespace
+}  // namespace bem
+
+extern "C" int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv_dev, void* B_dev, int64_t ldb,
+                             int64_t strideB, int nrhs, int* err_dev, void* stream) {
+  if (!work_dev || !piv_dev || !B_dev || !err_dev || npad <= 0 || npad % kB || batch <= 0 || nrhs <= 0 ||
+      ldb < npad)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_clu_solve: bad arguments");
+  return clu_solve_enqueue(work_dev, npad, batch, B_dev, ldb, strideB, nrhs, err_dev, (cudaStream_t)stream,
+                           nullptr);
 }
 
 extern "C" int bem_zgemm_ts(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
@@ -689,56 +727,61 @@ extern "C" int bem_zgemm_ts(int M, int K, int nrhs, double alpha_re, double alph
 
 extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
                                 void* work_dev, const int* piv_dev, const void* B_dev, void* X_dev, void* R_dev,
-                                void* D_dev, int64_t ldb, int64_t strideB, int nrhs, double tol, int max_iter,
-                                void* ts_work_dev, double* norms_dev, int* err_dev, int* iters_out,
-                                double* resid_out, void* stream) {
-  if (!K_dev || !work_dev || !piv_dev || !B_dev || !X_dev || !R_dev || !D_dev || !ts_work_dev || !norms_dev ||
-      !err_dev || !iters_out || !resid_out || nrhs <= 0 || nrhs > 16 || max_iter <= 0 || ldb < npad)
+                                int64_t ldb, int64_t strideB, int nrhs, double tol, int max_iter, void* ts_work_dev,
+                                double* norms_dev, int* err_dev, int* iters_out, double* resid_out, void* stream) {
+  if (!K_dev || !work_dev || !piv_dev || !B_dev || !X_dev || !R_dev || !ts_work_dev || !norms_dev || !err_dev ||
+      !iters_out || !resid_out || nrhs <= 0 || nrhs > 16 || max_iter <= 0 || ldb < npad || npad % kB || n > npad ||
+      batch <= 0)
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_refine_solve: bad arguments (nrhs <= 16)");
   cudaStream_t s = (cudaStream_t)stream;
   const size_t bytes = sizeof(double2) * ((size_t)(batch - 1) * strideB + (size_t)(nrhs - 1) * ldb + npad);
   const int nvec = batch * nrhs;
-  std::vector<double> bn(nvec), rn(nvec);
-  // |b| per column
-  colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)B_dev, n, ldb, strideB, norms_dev);
-  BEM_CUDA_CHECK(cudaMemcpyAsync(bn.data(), norms_dev, sizeof(double) * nvec, cudaMemcpyDeviceToHost, s));
-  // x = 0, r = b
+  double* bn = norms_dev;
+  double* rn = norms_dev + nvec;
+  double* state = norms_dev + 2 * nvec;  // [worst, iterations]
+  MixedWork w = carve(work_dev, npad, batch);
+  int* done = w.flags + (size_t)batch * (npad / kB) + 1;
+  int launches = 1;
+  // |b|^2 per column; x = 0, r = b, not converged
+  colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)B_dev, n, ldb, strideB, bn, nullptr);
   BEM_CUDA_CHECK(cudaMemsetAsync(X_dev, 0, bytes, s));
   BEM_CUDA_CHECK(cudaMemcpyAsync(R_dev, B_dev, bytes, cudaMemcpyDeviceToDevice, s));
-  int launches = 1;
-  double worst = 0.0;
-  int it = 0;
-  for (it = 1; it <= max_iter; ++it) {
-    // d = LU^{-1} r (float32 factors); the padded rows of r stay zero
-    BEM_CUDA_CHECK(cudaMemcpyAsync(D_dev, R_dev, bytes, cudaMemcpyDeviceToDevice, s));
-    int st = bem_clu_solve(work_dev, npad, batch, piv_dev, D_dev, ldb, strideB, nrhs, err_dev, stream);
-    if (st) return st;
-    // x += d ; r = b ; r = b - K x (float64)
-    ir_update_kernel<<<dim3(ceil_div(n, 256), nrhs, batch), 256, 0, s>>>((double2*)X_dev, (const double2*)D_dev,
-                                                                         (double2*)R_dev, (const double2*)B_dev, n,
-                                                                         nrhs, ldb, strideB);
-    st = bem_zgemm_ts(n, n, nrhs, -1.0, 0.0, K_dev, ldk, strideK, X_dev, ldb, strideB, 1.0, 0.0, R_dev, ldb, strideB,
-                      batch, ts_work_dev, stream);
-    if (st) return st;
-    colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)R_dev, n, ldb, strideB, norms_dev);
-    launches += 2;
-    BEM_CUDA_CHECK(cudaMemcpyAsync(rn.data(), norms_dev, sizeof(double) * nvec, cudaMemcpyDeviceToHost, s));
-    BEM_CUDA_CHECK(cudaStreamSynchronize(s));
-    worst = 0.0;
-    for (int v = 0; v < nvec; ++v) {
-      const double rel = bn[v] > 0.0 ? std::sqrt(rn[v] / bn[v]) : std::sqrt(rn[v]);
-      worst = std::max(worst, rel);
+  BEM_CUDA_CHECK(cudaMemsetAsync(done, 0, sizeof(int), s));
+  BEM_CUDA_CHECK(cudaMemsetAsync(state, 0, 2 * sizeof(double), s));
+  // Iterations are enqueued in groups without host synchronisation; once the
+  // device-side test has converged the rest of the group returns at once.
+  constexpr int kGroup = 4;
+  double host_state[2] = {0.0, 0.0};
+  int enqueued = 0;
+  while (enqueued < max_iter) {
+    const int group = std::min(kGroup, max_iter - enqueued);
+    for (int g = 0; g < group; ++g) {
+      // r <- (LU)^{-1} r in place (float32 factors; the padded rows of r stay zero)
+      int st = clu_solve_enqueue(work_dev, npad, batch, R_dev, ldb, strideB, nrhs, err_dev, s, done);
+      if (st) return st;
+      // x += r ; r = b ; r -= K x (float64)
+      ir_update_kernel<<<dim3(ceil_div(n, 256), nrhs, batch), 256, 0, s>>>(
+          (double2*)X_dev, (double2*)R_dev, (const double2*)B_dev, n, nrhs, ldb, strideB, done);
+      st = zgemm_ts_enqueue(n, n, nrhs, -1.0, 0.0, K_dev, ldk, strideK, X_dev, ldb, strideB, 1.0, 0.0, R_dev, ldb,
+                            strideB, batch, ts_work_dev, stream, done);
+      if (st) return st;
+      colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)R_dev, n, ldb, strideB, rn, done);
+      refine_check_kernel<<<1, 256, 0, s>>>(bn, rn, nvec, tol, done, state);
+      launches += 3;
     }
-    if (worst <= tol) break;
+    enqueued += group;
+    BEM_CUDA_CHECK(cudaMemcpyAsync(host_state, state, sizeof(host_state), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (host_state[0] <= tol && host_state[1] > 0.0) break;
   }
   count_launches(launches);
-  *iters_out = std::min(it, max_iter);
-  *resid_out = worst;
+  *iters_out = (int)host_state[1];
+  *resid_out = host_state[0];
   BEM_CUDA_CHECK(cudaGetLastError());
-  if (!(worst <= tol)) {
+  if (!(host_state[0] <= tol)) {
     char msg[160];
     std::snprintf(msg, sizeof(msg), "iterative refinement stopped at relative residual %.3e after %d iterations",
-                  worst, max_iter);
+                  host_state[0], max_iter);
     return set_error(BEM_ERR_NOT_CONVERGED, msg);
   }
   return BEM_OK;

@@ -16,7 +16,8 @@
 // with TMA (128-byte swizzle) through a 2-stage shared-memory ring (two CTAs
 // per SM, so that one CTA's epilogue overlaps the other's MMAs), one thread
 // of warp 1 issues tcgen05.mma (M=128, N=256, K=8 per instruction), warps 2-5
-// read the accumulator back with tcgen05.ld and apply C -= acc in place.
+// read the accumulator back with tcgen05.ld and apply C -= acc in place, the
+// loads of C running ahead of the accumulator reads.
 // Every mbarrier wait is bounded; on timeout the kernel records an error and
 // still drains its own copies before freeing tensor memory.
 #include <cuda.h>
@@ -122,6 +123,18 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 struct UpdateArgs {
   int a_row0;        // first operand row of the trailing block (Aop)
   int b_row0;        // first operand row of the trailing block (Bop), = 2 * first complex column
@@ -210,28 +223,58 @@ __global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_
       mma_commit(accf);
     }
   } else {
-    // epilogue warps 2..5: TMEM lanes 32*(warp % 4) .. +31
+    // epilogue warps 2..5: TMEM lanes 32*(warp % 4) .. +31.  The C tile is read
+    // in 16 chunks of 16 columns through a register double buffer: chunk 0 is
+    // loaded while the MMAs run, chunk i+1 while chunk i is applied.
+    constexpr int kCW = 16;                // columns per chunk
+    constexpr int kChunks = kTN / kCW;     // 16 (8 real, 8 imaginary)
+    constexpr int kPlaneChunks = kTNc / kCW;
     const int q = warp & 3;
+    const int row = p.c_row0 + tm * kTM + 32 * q + lane;
+    float* Cr = p.Cr + (size_t)b * p.c_stride + row;
+    float* Ci = p.Ci + (size_t)b * p.c_stride + row;
+    const int col0 = p.c_col0 + tn * kTNc;
+    const int64_t ldc = p.ldc;
+    auto at = [&](int chunk) -> float* {
+      return (chunk < kPlaneChunks ? Cr : Ci) + (size_t)(col0 + (chunk % kPlaneChunks) * kCW) * ldc;
+    };
+    float cb0[kCW], cb1[kCW];
+    {
+      const float* src = at(0);
+#pragma unroll
+      for (int j = 0; j < kCW; ++j) cb0[j] = __ldcs(src + j * ldc);
+    }
     const bool ok = __all_sync(0xffffffffu, mbar_wait(accf, 0, p.err));
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     __syncwarp();
     if (ok) {
-      const int row = p.c_row0 + tm * kTM + 32 * q + lane;
-      float* Cr = p.Cr + (size_t)b * p.c_stride + row;
-      float* Ci = p.Ci + (size_t)b * p.c_stride + row;
-      const int col0 = p.c_col0 + tn * kTNc;
-      // Per chunk of 32 accumulator columns: the 32 loads of C are issued before
-      // any store so that they are in flight together (a load after a store to
-      // a possibly aliasing address would otherwise wait for it).
+      const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16);
 #pragma unroll 1
-      for (int chunk = 0; chunk < kTN / 32; ++chunk) {
-        float v[32], c[32];
-        float* __restrict__ base = ((chunk < kTNc / 32) ? Cr : Ci) + (size_t)(col0 + (chunk % (kTNc / 32)) * 32) * p.ldc;
+      for (int chunk = 0; chunk < kChunks; chunk += 2) {
+        {
+          const float* src = at(chunk + 1);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) c[j] = __ldcs(base + (size_t)j * p.ldc);
-        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(chunk * 32), v);
+          for (int j = 0; j < kCW; ++j) cb1[j] = __ldcs(src + j * ldc);
+        }
+        {
+          float v[kCW];
+          tmem_ld16(tbase + (uint32_t)(chunk * kCW), v);
+          float* dst = at(chunk);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) __stcs(base + (size_t)j * p.ldc, c[j] - v[j]);
+          for (int j = 0; j < kCW; ++j) __stcs(dst + j * ldc, cb0[j] - v[j]);
+        }
+        if (chunk + 2 < kChunks) {
+          const float* src = at(chunk + 2);
+#pragma unroll
+          for (int j = 0; j < kCW; ++j) cb0[j] = __ldcs(src + j * ldc);
+        }
+        {
+          float v[kCW];
+          tmem_ld16(tbase + (uint32_t)((chunk + 1) * kCW), v);
+          float* dst = at(chunk + 1);
+#pragma unroll
+          for (int j = 0; j < kCW; ++j) __stcs(dst + j * ldc, cb1[j] - v[j]);
+        }
       }
     }
   }

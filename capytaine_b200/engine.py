@@ -20,6 +20,8 @@ import ctypes
 import logging
 import math
 import time
+import weakref
+from collections import OrderedDict
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Sequence
 
@@ -97,8 +99,7 @@ class _Workspace:
             self.B = torch.zeros((batch, npad * nrhs), **c128)
             self.X = torch.zeros((batch, npad * nrhs), **c128)
             self.R = torch.zeros((batch, npad * nrhs), **c128)
-            self.D = torch.zeros((batch, npad * nrhs), **c128)
-            self.norms = torch.zeros(batch * nrhs, dtype=torch.float64, device=device)
+            self.norms = torch.zeros(2 * batch * nrhs + 2, dtype=torch.float64, device=device)
             nbytes = int(lib.bem_clu_workspace_bytes(npad, batch))
             self.lu_work = torch.empty(nbytes + 1024, dtype=torch.uint8, device=device)
             base = self.lu_work.data_ptr()
@@ -112,7 +113,7 @@ class _Workspace:
     @property
     def nbytes(self):
         ts = [t for t in (self.K, self.S, self.B, self.phi, self.lu_work, self.ts_work)]
-        ts += [getattr(self, k) for k in ("X", "R", "D") if hasattr(self, k)]
+        ts += [getattr(self, k) for k in ("X", "R") if hasattr(self, k)]
         return sum(t.numel() * t.element_size() for t in ts)
 
 
@@ -144,6 +145,7 @@ class B200Engine:
         self.max_batch = int(max_batch)
         self._device = device
         self._ws: Dict[tuple, _Workspace] = {}
+        self._body_cache: "OrderedDict[tuple, tuple]" = OrderedDict()
         self.last_computed_inputs = None
         self.last_computed_matrices = None
         self.exportable_settings = {
@@ -174,6 +176,23 @@ class B200Engine:
 
     # ------------------------------------------------------------------------
     # Batched frequency solves
+    def _body_arrays(self, body, mesh):
+        """Device copies of the dof normal components, pressure weights and
+        hull mask of a body, kept for the body's next call."""
+        import torch
+        key = (id(body), mesh.content_hash, tuple(body.dofs))
+        hit = self._body_cache.get(key)
+        if hit is not None and hit[0]() is body:
+            return hit[1]
+        dev = self.device
+        arrays = (torch.as_tensor(body.dof_normal_components(), dtype=torch.float64, device=dev).contiguous(),
+                  torch.as_tensor(body.pressure_weights(), dtype=torch.float64, device=dev).contiguous(),
+                  torch.as_tensor(body.hull_mask.astype(np.int32), device=dev))
+        self._body_cache[key] = (weakref.ref(body), arrays)
+        while len(self._body_cache) > 8:
+            self._body_cache.popitem(last=False)
+        return arrays
+
     def solve_frequencies(self, body, omegas: Sequence[float], *, wave_directions: Sequence[float] = (0.0,),
                           rho: float = 1000.0, g: float = 9.81, batch: Optional[int] = None,
                           sync_stats: bool = False) -> FrequencyResults:
@@ -194,9 +213,7 @@ class B200Engine:
         stream = _lib.stream_ptr()
         gf = self.green_function
         dm = gf.device_mesh(mesh)
-        dofn = torch.as_tensor(body.dof_normal_components(), dtype=torch.float64, device=dev).contiguous()
-        wdof = torch.as_tensor(body.pressure_weights(), dtype=torch.float64, device=dev).contiguous()
-        hull = torch.as_tensor(body.hull_mask.astype(np.int32), device=dev)
+        dofn, wdof, hull = self._body_arrays(body, mesh)
         heads_t = torch.as_tensor(heads, dtype=torch.float64, device=dev)
         F_all = np.zeros((len(omegas), nrhs, ndof), dtype=np.complex128)
         FK_all = np.zeros((len(omegas), max(nhead, 1), ndof), dtype=np.complex128)
@@ -235,7 +252,7 @@ class B200Engine:
             if mixed:
                 iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
                 status = lib.bem_refine_solve(_vp(ws.K), n, n * n, n, npad, nb, _vp(ws.lu_work_ptr), _vp(ws.piv),
-                                              _vp(ws.B), _vp(ws.X), _vp(ws.R), _vp(ws.D), npad, npad * nrhs, nrhs,
+                                              _vp(ws.B), _vp(ws.X), _vp(ws.R), npad, npad * nrhs, nrhs,
                                               self.refine_tol, self.refine_max_iter, _vp(ws.ts_work),
                                               _vp(ws.norms), _vp(ws.err), ctypes.byref(iters),
                                               ctypes.byref(resid), stream)

@@ -255,16 +255,19 @@ int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv_dev, void*
 
 /* Iterative refinement: X solves K X = B to a relative residual below tol in
  * every column (residual r = b - K x evaluated in float64 against the float64
- * K, correction from the float32 LU).  B, X, R, D: complex128 npad x nrhs
- * (rows n..npad-1 of B zero), nrhs <= 16; ts_work_dev sized by
- * bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch); norms_dev: batch*nrhs
- * doubles.  Synchronises the stream once per iteration (convergence test).
- * Returns BEM_ERR_NOT_CONVERGED (X holds the last iterate) when max_iter is
- * reached.  Replaces the lu_solve of tools/block_circulant_matrices.py:382-385. */
+ * K, correction from the float32 LU, solved in place in R).  B, X, R:
+ * complex128 npad x nrhs (rows n..npad-1 of B zero), nrhs <= 16; work_dev the
+ * factorisation of bem_clu_factor; ts_work_dev sized by
+ * bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch); norms_dev: 2*batch*nrhs + 2
+ * doubles.  The convergence test runs on the device: iterations are enqueued
+ * in groups of four and those after convergence return at once, so the stream
+ * is synchronised once per group.  Returns BEM_ERR_NOT_CONVERGED (X holds the
+ * last iterate) when max_iter is reached.  Replaces the lu_solve of
+ * tools/block_circulant_matrices.py:382-385. */
 int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch, void* work_dev,
-                     const int* piv_dev, const void* B_dev, void* X_dev, void* R_dev, void* D_dev, int64_t ldb,
-                     int64_t strideB, int nrhs, double tol, int max_iter, void* ts_work_dev, double* norms_dev,
-                     int* err_dev, int* iters_out, double* resid_out, void* stream);
+                     const int* piv_dev, const void* B_dev, void* X_dev, void* R_dev, int64_t ldb, int64_t strideB,
+                     int nrhs, double tol, int max_iter, void* ts_work_dev, double* norms_dev, int* err_dev,
+                     int* iters_out, double* resid_out, void* stream);
 
 /* ---- allocation-free variant ---------------------------------------------- */
 /* No counterpart in the reference.  Same operation and arguments as

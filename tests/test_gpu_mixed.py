@@ -66,14 +66,15 @@ def test_refinement_reaches_1e10(n, batch, nrhs):
     lib, npad, mats, rhs, K, B, work, wptr, piv, info, err = _setup(n, batch, nrhs, n + 1)
     X = torch.zeros_like(B)
     R = torch.zeros_like(B)
-    D = torch.zeros_like(B)
     ts = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch)), dtype=torch.uint8, device="cuda")
-    norms = torch.zeros(batch * nrhs, dtype=torch.float64, device="cuda")
+    norms = torch.zeros(2 * batch * nrhs + 2, dtype=torch.float64, device="cuda")
     iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
     _lib.check(lib.bem_refine_solve(_vp(K), n, n * n, n, npad, batch, _vp(wptr), _vp(piv), _vp(B), _vp(X), _vp(R),
-                                    _vp(D), npad, npad * nrhs, nrhs, 1e-10, 30, _vp(ts), _vp(norms), _vp(err),
+                                    npad, npad * nrhs, nrhs, 1e-10, 30, _vp(ts), _vp(norms), _vp(err),
                                     ctypes.byref(iters), ctypes.byref(resid), _lib.stream_ptr()))
     assert resid.value <= 1e-10 and 1 <= iters.value <= 10
+    for b in range(batch):  # B is read only
+        np.testing.assert_array_equal(B[b, :, :n].T.cpu().numpy(), rhs[b])
     for b in range(batch):
         x = X[b, :, :n].T.cpu().numpy()
         ref = np.linalg.solve(mats[b], rhs[b])
@@ -126,3 +127,20 @@ def test_float32_wave_term_keeps_added_mass_and_excitation(oracle_mod, default_o
     ref = [oracle_mod.solve_frequency(default_oracle_gf, mesh, oracle_mod.rigid_body_dofs(), w) for w in omegas]
     errs = coefficient_errors(res, ref, body.dofs)
     assert errs["added_mass"] < MIXED_GATE and errs["excitation"] < MIXED_GATE, errs
+
+
+def test_refinement_reports_non_convergence():
+    """max_iter reached above tol: BEM_ERR_NOT_CONVERGED with the iteration
+    count and the residual of the last iterate."""
+    import torch
+    n, batch, nrhs = 300, 1, 3
+    lib, npad, mats, rhs, K, B, work, wptr, piv, info, err = _setup(n, batch, nrhs, 7)
+    X, R = torch.zeros_like(B), torch.zeros_like(B)
+    ts = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch)), dtype=torch.uint8, device="cuda")
+    norms = torch.zeros(2 * batch * nrhs + 2, dtype=torch.float64, device="cuda")
+    iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
+    st = lib.bem_refine_solve(_vp(K), n, n * n, n, npad, batch, _vp(wptr), _vp(piv), _vp(B), _vp(X), _vp(R), npad,
+                              npad * nrhs, nrhs, 1e-300, 2, _vp(ts), _vp(norms), _vp(err), ctypes.byref(iters),
+                              ctypes.byref(resid), _lib.stream_ptr())
+    assert st == _lib.BEM_ERR_NOT_CONVERGED and iters.value == 2 and 0.0 < resid.value < 1e-5
+    assert b"iterative refinement stopped" in lib.bem_last_error()
