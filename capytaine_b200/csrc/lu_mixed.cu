@@ -28,7 +28,7 @@ namespace bem {
 
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
-                      int n, int batch, int* err, cudaStream_t stream);
+                      int n, int batch, int* err, cudaStream_t stream, int store = 0);
 int zgemm_ts_enqueue(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
                      int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,
                      double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev,
@@ -37,9 +37,8 @@ int zgemm_ts_enqueue(int M, int K, int nrhs, double alpha_re, double alpha_im, c
 namespace {
 
 constexpr int kB = 128;        // LU block
-constexpr int kLdB = kB + 1;   // shared leading dimension of a 128-row tile
 constexpr int kPT = 64;        // panel tile width
-constexpr int kLdP = kPT + 1;
+constexpr int kSplitK = 6 * kB;  // K' of the split-TF32 panel product: (hi, lo, hi) x (re, im) x 128
 constexpr int kRhs = 16;       // right-hand sides per solve launch
 constexpr long long kSpin = 4000000;
 
@@ -59,6 +58,10 @@ struct Planes {
   int64_t ld;      // = npad
   int64_t stride;  // floats between matrices (re and im planes of one matrix are plane apart)
 };
+// The part of x that TF32 keeps (the low 13 mantissa bits cleared); x - hi is
+// exact in float32 and is the "lo" part of the split product.
+__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xffffe000u); }
+
 __device__ __forceinline__ float2 ldp(const Planes& W, int b, int r, int c) {
   const size_t o = (size_t)b * W.stride + (size_t)r + (size_t)c * W.ld;
   return make_float2(W.re[o], W.im[o]);
@@ -198,7 +201,8 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
 // so that register indices are compile-time constants.  Output: inv (128 x 128,
 // column-major) = A_kk^{-1}; info flags an exactly zero pivot.
 __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* __restrict__ info,
-                                                        float2* __restrict__ inv, int nblk) {
+                                                        float2* __restrict__ inv, int nblk,
+                                                        float* __restrict__ binv) {
   __shared__ float2 colbuf[2][kB];
   __shared__ float2 rowbuf[2][kB];
   __shared__ int s_piv[2];
@@ -225,32 +229,55 @@ __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* _
 #undef BEM_GJ_SLOT
   __syncthreads();
   // inverse of A_kk = (P A_kk)^{-1} P: column c of the result goes to column perm[c]
+  // and packed as the B operand of the split-TF32 product L21 = A21 A_kk^{-1}
+  // (three K-blocks of 256: hi, hi, lo; see clu_pack_kernel for the A side):
+  // row t: [Re X(:, t) | -Im X(:, t)] per block, row 128 + t: [Im X(:, t) | Re X(:, t)]
   float2* out = inv + ((size_t)b * nblk + kk / kB) * kB * kB;
+  float* bo = binv + (size_t)b * (2 * kB) * kSplitK;
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const int r = lane + 32 * i, c = w + 16 * m;
-      out[r + (size_t)perm[c] * kB] = a[i][m];
+      const int pc = perm[c];
+      const float2 v = a[i][m];
+      out[r + (size_t)pc * kB] = v;
+      const float2 hi = make_float2(tf32_hi(v.x), tf32_hi(v.y));
+      const float2 lo = make_float2(v.x - hi.x, v.y - hi.y);
+      float* rr = bo + (size_t)pc * kSplitK + r;
+      float* ri = bo + (size_t)(kB + pc) * kSplitK + r;
+      rr[0] = hi.x;
+      rr[kB] = -hi.y;
+      rr[2 * kB] = hi.x;
+      rr[3 * kB] = -hi.y;
+      rr[4 * kB] = lo.x;
+      rr[5 * kB] = -lo.y;
+      ri[0] = hi.y;
+      ri[kB] = hi.x;
+      ri[2 * kB] = hi.y;
+      ri[3 * kB] = hi.x;
+      ri[4 * kB] = lo.y;
+      ri[5 * kB] = lo.x;
     }
 }
 
-// Panels of step kk of the block LU.  Tiles [0, nrest): the block row to the
-// right of the diagonal, packed unchanged as the B operand (U12 = A12);
-// tiles [nrest, 2 nrest): 64 rows below the diagonal, L21 = A21 A_kk^{-1},
-// written back and packed as the A operand.
+// Operand packing of step kk of the block LU (A_kk^{-1} comes packed from the
+// Gauss-Jordan kernel).  Blocks [0, nrest): the block row to the right of the
+// diagonal, 64 columns each, packed as the B operand (U12 = A12).  Blocks
+// [nrest, nrest + nrows/32): 32 rows of the block column [col0, col0 + 128)
+// from row row0 on, packed K-major: into A3 as the split-TF32 operand of the
+// panel product (A21), or into Aop as [Re(128) | Im(128)] (L21, the A operand
+// of the trailing update).
 // Aop: [batch][npad][2*kB]; Bop: [batch][2*npad][2*kB].
-__global__ void __launch_bounds__(256) clu_panel_kernel(Planes W, int npad, int kk, const float2* __restrict__ inv,
-                                                        int nblk, float* __restrict__ Aop, float* __restrict__ Bop) {
-  extern __shared__ float2 fsm[];
-  float2* D = fsm;               // A_kk^{-1}, D[c*kLdB + r]
-  float2* X = fsm + kB * kLdB;   // 64 x 128 rows of A21, X[c*kLdP + r]
+__global__ void __launch_bounds__(256) clu_pack_kernel(Planes W, int npad, int kk, int nrest, int row0, int col0,
+                                                       float* __restrict__ Aop, float* __restrict__ Bop,
+                                                       float* __restrict__ A3) {
+  __shared__ float tre[kB][33], tim[kB][33];  // [column][row] of a 32 x 128 tile
   const int b = blockIdx.y, tid = threadIdx.x;
-  const int nrest = (npad - kk - kB) / kPT;
-  const int t = blockIdx.x;
   const size_t kp = 2 * kB;
+  const int t = blockIdx.x;
   if (t < nrest) {
-    // pack 128 x 64 of A12: B operand rows of the complex columns c0 .. c0+63
+    // 128 x 64 of A12: B operand rows of the complex columns c0 .. c0+63
     const int c0 = kk + kB + t * kPT;
     const int j0 = c0 & ~(kB - 1);
     float* Bb = Bop + (size_t)b * 2 * npad * kp;
@@ -267,35 +294,31 @@ __global__ void __launch_bounds__(256) clu_panel_kernel(Planes W, int npad, int 
     }
     return;
   }
-  const float2* invb = inv + ((size_t)b * nblk + kk / kB) * kB * kB;
-  for (int idx = tid; idx < kB * kB; idx += blockDim.x) D[(idx >> 7) * kLdB + (idx & (kB - 1))] = invb[idx];
-  const int r0 = kk + kB + (t - nrest) * kPT;
-  for (int idx = tid; idx < kPT * kB; idx += blockDim.x) {
-    const int r = idx & (kPT - 1), c = idx >> 6;
-    X[c * kLdP + r] = ldp(W, b, r0 + r, kk + c);
+  const int r0 = row0 + (t - nrest) * 32;
+  const int lane = tid & 31, w = tid >> 5;
+  const float* re = W.re + (size_t)b * W.stride;
+  const float* im = W.im + (size_t)b * W.stride;
+  for (int c = w; c < kB; c += 8) {
+    const size_t g = (size_t)(col0 + c) * W.ld + r0 + lane;
+    tre[c][lane] = re[g];
+    tim[c][lane] = im[g];
   }
   __syncthreads();
-  // thread: one row r, 32 columns
-  const int r = tid & (kPT - 1), cq = (tid >> 6) * 32;
-  float2 acc[32];
-#pragma unroll
-  for (int u = 0; u < 32; ++u) acc[u] = make_float2(0.0f, 0.0f);
-  for (int m = 0; m < kB; ++m) {
-    const float2 x = X[m * kLdP + r];
-#pragma unroll
-    for (int u = 0; u < 32; ++u) {
-      const float2 a = D[(cq + u) * kLdB + m];
-      acc[u].x += x.x * a.x - x.y * a.y;
-      acc[u].y += x.x * a.y + x.y * a.x;
-    }
+  const int c = tid & (kB - 1);
+  if (!A3) {
+    float* dst = Aop + (size_t)b * npad * kp + (size_t)r0 * kp;
+    for (int i = 0; i < 32; ++i) dst[(size_t)i * kp + tid] = (tid < kB) ? tre[c][i] : tim[c][i];
+    return;
   }
-  float* row = Aop + (size_t)b * npad * kp + (size_t)(r0 + r) * kp;
-#pragma unroll
-  for (int u = 0; u < 32; ++u) {
-    const int c = cq + u;
-    stp(W, b, r0 + r, kk + c, acc[u]);
-    row[c] = acc[u].x;
-    row[kB + c] = acc[u].y;
+  // split rows [hi | lo | hi], each [Re(128) | Im(128)], for the panel product
+  float* dst = A3 + (size_t)b * npad * kSplitK + (size_t)r0 * kSplitK;
+  for (int i = 0; i < 32; ++i) {
+    const float x = (tid < kB) ? tre[c][i] : tim[c][i];
+    const float hi = tf32_hi(x);
+    float* row = dst + (size_t)i * kSplitK;
+    row[tid] = hi;
+    row[2 * kB + tid] = x - hi;
+    row[4 * kB + tid] = hi;
   }
 }
 
@@ -530,8 +553,6 @@ __global__ void refine_check_kernel(const double* __restrict__ bn, const double*
 bool g_mixed_configured = false;
 int configure_mixed() {
   if (g_mixed_configured) return BEM_OK;
-  const int panel = (kB * kLdB + kB * kLdP) * (int)sizeof(float2);
-  BEM_CUDA_CHECK(cudaFuncSetAttribute(clu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, panel));
   BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       trsm_smem_bytes(8)));
   BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -547,6 +568,8 @@ struct MixedWork {
   float* Aop;
   float* Bop;
   float2* inv;
+  float* binv;  // batch x 256 x kSplitK: packed A_kk^{-1} of the current block
+  float* a3;    // batch x npad x kSplitK: split A21 of the current block
   int* flags;
 };
 MixedWork carve(void* work, int npad, int batch) {
@@ -561,6 +584,10 @@ MixedWork carve(void* work, int npad, int batch) {
   p += 2 * (size_t)batch * 2 * npad * 2 * kB * sizeof(float);
   w.inv = (float2*)p;
   p += (size_t)batch * nblk * kB * kB * sizeof(float2);
+  w.binv = (float*)p;
+  p += (size_t)batch * (2 * kB) * kSplitK * sizeof(float);
+  w.a3 = (float*)p;
+  p += (size_t)batch * npad * kSplitK * sizeof(float);
   w.flags = (int*)p;
   return w;
 }
@@ -607,6 +634,7 @@ extern "C" int64_t bem_clu_workspace_bytes(int npad, int batch) {
   const int64_t nblk = npad / kB;
   return (int64_t)batch * 2 * npad * (int64_t)npad * 4 + 2 * (int64_t)batch * npad * 2 * kB * 4 +
          2 * (int64_t)batch * 2 * npad * 2 * kB * 4 + (int64_t)batch * nblk * kB * kB * 8 +
+         (int64_t)batch * (2 * kB) * kSplitK * 4 + (int64_t)batch * npad * kSplitK * 4 +
          ((int64_t)batch * nblk + 2) * 4 + 1024;
 }
 
@@ -628,23 +656,32 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
   convert_pad_kernel<<<dim3(ceil_div(npad, 256), npad, batch), 256, 0, s>>>((const double2*)K_dev, ldk, strideK, n,
                                                                            npad, W);
   ++launches;
-  const int panel_smem = (kB * kLdB + kB * kLdP) * (int)sizeof(float2);
   const size_t abuf = (size_t)batch * npad * 2 * kB, bbuf = (size_t)batch * 2 * npad * 2 * kB;
   float* Aop[2] = {w.Aop, w.Aop + abuf};
   float* Bop[2] = {w.Bop, w.Bop + bbuf};
+  // Inverse of the diagonal block, then the panel: A12 and A21 packed, L21 =
+  // A21 A_kk^{-1} on the tensor cores into the working matrix, L21 packed.
   auto diag_and_panel = [&](int kk, int buf, cudaStream_t on) -> int {
     {
       TimedLaunch tl(kKCluGj, on);
-      clu_gj_kernel<<<batch, 512, 0, on>>>(W, kk, info_dev, w.inv, nblk);
+      clu_gj_kernel<<<batch, 512, 0, on>>>(W, kk, info_dev, w.inv, nblk, w.binv);
     }
     ++launches;
-    const int nrest = (npad - kk - kB) / kPT;
-    if (nrest > 0) {
+    const int m = npad - kk - kB;
+    if (m <= 0) return BEM_OK;
+    const int nrest = m / kPT;
+    {
       TimedLaunch tl(kKCluPanel, on);
-      clu_panel_kernel<<<dim3(2 * nrest, batch), 256, panel_smem, on>>>(W, npad, kk, w.inv, nblk, Aop[buf],
-                                                                       Bop[buf]);
-      ++launches;
+      clu_pack_kernel<<<dim3(nrest + m / 32, batch), 256, 0, on>>>(W, npad, kk, nrest, kk + kB, kk, Aop[buf],
+                                                                    Bop[buf], w.a3);
+      // split TF32: A_hi B_hi + A_lo B_hi + A_hi B_lo, float32-level multipliers
+      int st2 = cgemm_tf32_update(w.a3, npad, kk + kB, w.binv, 2 * kB, 0, kSplitK, W.re, W.im, npad, W.stride,
+                                  kk + kB, kk, m, kB, batch, err_dev, on, 1);
+      if (st2) return st2;
+      clu_pack_kernel<<<dim3(m / 32, batch), 256, 0, on>>>(W, npad, kk, 0, kk + kB, kk, Aop[buf], Bop[buf],
+                                                           nullptr);
     }
+    launches += 2;
     return BEM_OK;
   };
   // C rows r0.. (m), complex columns c0.. (nc) -= L21 U12 of the block step whose
@@ -661,14 +698,14 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
   // step k that block k+1 needs (its block row and block column), the inverse
   // and panel of block k+1 run on the side stream while the rest of the
   // trailing update of step k runs on the caller's stream.
-  diag_and_panel(0, 0, s);
+  if ((st = diag_and_panel(0, 0, s))) return st;
   for (int kk = 0, step = 0; kk + kB < npad; kk += kB, ++step) {
     const int cur = step & 1, kn = kk + kB, rest = npad - kn - kB;
     if ((st = update(cur, kn, kn, kB, npad - kn))) return st;  // block row kn
     if ((st = update(cur, kn + kB, kn, rest, kB))) return st;  // block column kn below the diagonal
     BEM_CUDA_CHECK(cudaEventRecord(la->strips, s));
     BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->strips, 0));
-    diag_and_panel(kn, cur ^ 1, la->side);
+    if ((st = diag_and_panel(kn, cur ^ 1, la->side))) return st;
     BEM_CUDA_CHECK(cudaEventRecord(la->panel, la->side));
     if ((st = update(cur, kn + kB, kn + kB, rest, rest))) return st;
     BEM_CUDA_CHECK(cudaStreamWaitEvent(s, la->panel, 0));

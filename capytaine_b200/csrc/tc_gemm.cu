@@ -146,6 +146,7 @@ struct UpdateArgs {
   int64_t ldc;
   int64_t c_stride;  // elements between matrices
   int* err;
+  int store;         // 0: C -= A B;  1: C = A B (C is not read)
 };
 
 __global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
@@ -238,8 +239,11 @@ __global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_
     auto at = [&](int chunk) -> float* {
       return (chunk < kPlaneChunks ? Cr : Ci) + (size_t)(col0 + (chunk % kPlaneChunks) * kCW) * ldc;
     };
+    const bool rd = p.store == 0;
     float cb0[kCW], cb1[kCW];
-    {
+#pragma unroll
+    for (int j = 0; j < kCW; ++j) cb0[j] = cb1[j] = 0.0f;
+    if (rd) {
       const float* src = at(0);
 #pragma unroll
       for (int j = 0; j < kCW; ++j) cb0[j] = __ldcs(src + j * ldc);
@@ -251,7 +255,7 @@ __global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_
       const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16);
 #pragma unroll 1
       for (int chunk = 0; chunk < kChunks; chunk += 2) {
-        {
+        if (rd) {
           const float* src = at(chunk + 1);
 #pragma unroll
           for (int j = 0; j < kCW; ++j) cb1[j] = __ldcs(src + j * ldc);
@@ -261,9 +265,9 @@ __global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_
           tmem_ld16(tbase + (uint32_t)(chunk * kCW), v);
           float* dst = at(chunk);
 #pragma unroll
-          for (int j = 0; j < kCW; ++j) __stcs(dst + j * ldc, cb0[j] - v[j]);
+          for (int j = 0; j < kCW; ++j) __stcs(dst + j * ldc, rd ? cb0[j] - v[j] : v[j]);
         }
-        if (chunk + 2 < kChunks) {
+        if (rd && chunk + 2 < kChunks) {
           const float* src = at(chunk + 2);
 #pragma unroll
           for (int j = 0; j < kCW; ++j) cb0[j] = __ldcs(src + j * ldc);
@@ -273,7 +277,7 @@ __global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_
           tmem_ld16(tbase + (uint32_t)((chunk + 1) * kCW), v);
           float* dst = at(chunk + 1);
 #pragma unroll
-          for (int j = 0; j < kCW; ++j) __stcs(dst + j * ldc, cb1[j] - v[j]);
+          for (int j = 0; j < kCW; ++j) __stcs(dst + j * ldc, rd ? cb1[j] - v[j] : v[j]);
         }
       }
     }
@@ -323,7 +327,7 @@ bool g_tc_configured = false;
 // of 128) -= A' B' for `batch` matrices.
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
-                      int n, int batch, int* err, cudaStream_t stream) {
+                      int n, int batch, int* err, cudaStream_t stream, int store) {
   if (m <= 0 || n <= 0) return BEM_OK;
   if (m % kTM || n % kTNc || kp % kKC || (a_row0 % 8) || (b_row0 % 8))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: sizes must be multiples of 128 (K' of 32)");
@@ -337,7 +341,7 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
     BEM_CUDA_CHECK(cudaFuncSetAttribute(cgemm_tf32_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     g_tc_configured = true;
   }
-  UpdateArgs p{a_row0, b_row0, c_row0, c_col0, kp / kKC, Cr, Ci, ldc, c_stride, err};
+  UpdateArgs p{a_row0, b_row0, c_row0, c_col0, kp / kKC, Cr, Ci, ldc, c_stride, err, store};
   dim3 grid(m / kTM, n / kTNc, batch);
   {
     TimedLaunch tl(kKCgemmTf32, stream);
@@ -361,5 +365,5 @@ extern "C" int bem_cgemm_tf32_update(const float* Aop_dev, int64_t a_rows, int a
   if ((reinterpret_cast<uintptr_t>(Aop_dev) | reinterpret_cast<uintptr_t>(Bop_dev)) & 15)
     return bem::set_error(BEM_ERR_INVALID_ARGUMENT, "bem_cgemm_tf32_update: operands must be 16-byte aligned");
   return bem::cgemm_tf32_update(Aop_dev, a_rows, a_row0, Bop_dev, b_rows, b_row0, kp, Cr_dev, Ci_dev, ldc, c_stride,
-                                c_row0, c_col0, m, n, batch, err_dev, (cudaStream_t)stream);
+                                c_row0, c_col0, m, n, batch, err_dev, (cudaStream_t)stream, 0);
 }
