@@ -47,6 +47,9 @@ def barge_body():
 def workload_config(args, n):
     return {"workload": "barge 80x20x10m, 6 dofs + diffraction (heading 0), omega linspace(0.05,3,60)",
             "nb_panels": int(n), "frequencies_per_step": int(args.batch), "engine": args.engine,
+            "solver": (f"float32 tcgen05 LU + {args.refinement} refinement to 1e-10" if args.engine == "mixed"
+                       else {"gmres": "float64 GMRES (atol 1e-6, rtol 1e-5, restart 20)",
+                             "lu_decomposition": "float64 DMMA LU"}[args.linear_solver]),
             "depth": "infinite", "l2": "inputs larger than L2 (K: 604 MB complex128 per frequency)",
             "parallelism": f"frequency shards x{args.world}",
             "rankine_part": "computed once per sweep of the 60 frequencies (cache cleared at each sweep start)"}
@@ -293,6 +296,10 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=4,
                     help="timed steps of the float64 engine for the refined-mixed vs float64 comparison (0: skip)")
     ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--refinement", default="classical", choices=["classical", "gmres"],
+                    help="refinement of the mixed engine: x += (LU)^-1 r, or GMRES preconditioned by the LU")
+    ap.add_argument("--linear-solver", default="lu_decomposition", choices=["lu_decomposition", "gmres"],
+                    help="solver of the float64 engine (--engine fp64)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -318,7 +325,11 @@ def main():
     body = barge_body()
     n = body.mesh_including_lid.nb_faces
     gf = Delhommeau(tabulation_cache_dir=None)
-    engine = B200Engine(green_function=gf, precision=args.engine, max_batch=args.batch)
+    if args.engine == "mixed":
+        engine = B200Engine(green_function=gf, precision="mixed", max_batch=args.batch, refinement=args.refinement)
+    else:
+        engine = B200Engine(green_function=gf, precision="fp64", max_batch=args.batch,
+                            linear_solver=args.linear_solver)
     # this rank's share of the sweep: frequencies rank, rank + world, ...
     my_omegas = OMEGAS[rank::world]
     nb = args.batch

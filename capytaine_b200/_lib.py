@@ -104,6 +104,10 @@ _SIGNATURES = {
     "bem_refine_solve": ([c_void_p, c_i64, c_i64, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                           c_void_p, c_i64, c_i64, c_int, c_double, c_int, c_void_p, c_void_p, c_void_p,
                           ctypes.POINTER(c_int), ctypes.POINTER(c_double), c_void_p], c_int),
+    "bem_gmres_workspace_bytes": ([c_int, c_int, c_int, c_int, c_int], c_i64),
+    "bem_gmres_solve": ([c_void_p, c_i64, c_i64, c_int, c_int, c_int, c_void_p, c_void_p, c_i64, c_i64, c_int,
+                         c_double, c_double, c_int, c_int, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_int),
+                         ctypes.POINTER(c_double), c_void_p], c_int),
     "bem_zgemm_ts_static_capacity": ([], c_i64),
     "bem_zgemm_ts_static": ([c_int, c_int, c_int, c_double, c_double, c_void_p, c_i64, c_i64, c_void_p, c_i64, c_i64,
                              c_double, c_double, c_void_p, c_i64, c_i64, c_int, c_void_p], c_int),

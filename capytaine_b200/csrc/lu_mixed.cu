@@ -716,7 +716,9 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
 }
 
 namespace bem {
-namespace {
+// Forward and backward block substitution with the float32 factors, in place on
+// B (npad x nrhs complex128 per matrix); returns at once while *skip != 0.  Also
+// the preconditioner of the GMRES solver.
 int clu_solve_enqueue(void* work_dev, int npad, int batch, void* B_dev, int64_t ldb, int64_t strideB, int nrhs,
                       int* err_dev, cudaStream_t s, const int* skip) {
   int st = configure_mixed();
@@ -745,7 +747,6 @@ int clu_solve_enqueue(void* work_dev, int npad, int batch, void* B_dev, int64_t 
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
 }
-}  // namespace
 }  // namespace bem
 
 extern "C" int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv_dev, void* B_dev, int64_t ldb,

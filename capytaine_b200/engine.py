@@ -82,12 +82,14 @@ class _Workspace:
         self.nan = torch.zeros(1, dtype=torch.int32, device=device)
         self.ts_work = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, min(nrhs, 16), batch)),
                                    dtype=torch.uint8, device=device)
+        self._gmres = None
         if precision == "fp64":
             self.npad = padded_size(n)
             npad = self.npad
             self.K = torch.empty((batch, npad * npad), **c128)
             self.ldk = npad
             self.B = torch.zeros((batch, npad * nrhs), **c128)
+            self.X = torch.zeros((batch, npad * nrhs), **c128)
             self.lu_work = torch.empty(int(lib.bem_zlu_workspace_bytes(npad, batch)), dtype=torch.uint8,
                                        device=device)
             self._aligned = None
@@ -106,6 +108,17 @@ class _Workspace:
             self._aligned = (base + 1023) // 1024 * 1024  # 1024-byte aligned start
         self.piv = torch.empty((batch, self.npad), dtype=torch.int32, device=device)
 
+    def gmres_work(self, restart):
+        """256-byte aligned workspace of bem_gmres_solve for this shape."""
+        import torch
+        if self._gmres is None or self._gmres[0] != restart:
+            nbytes = int(_lib.load().bem_gmres_workspace_bytes(self.n, self.npad, self.nrhs, self.batch, restart))
+            if nbytes < 0:
+                raise ValueError("bad GMRES workspace shape")
+            buf = torch.empty(nbytes + 256, dtype=torch.uint8, device=self.K.device)
+            self._gmres = (restart, buf, (buf.data_ptr() + 255) // 256 * 256)
+        return self._gmres[2]
+
     @property
     def lu_work_ptr(self):
         return self._aligned if self._aligned is not None else self.lu_work.data_ptr()
@@ -114,6 +127,8 @@ class _Workspace:
     def nbytes(self):
         ts = [t for t in (self.K, self.S, self.B, self.phi, self.lu_work, self.ts_work)]
         ts += [getattr(self, k) for k in ("X", "R") if hasattr(self, k)]
+        if self._gmres is not None:
+            ts.append(self._gmres[1])
         return sum(t.numel() * t.element_size() for t in ts)
 
 
@@ -125,16 +140,38 @@ class B200Engine:
     tensor-core trailing updates, float64-residual iterative refinement to
     refine_tol).  assembly_precision: "fp64" (default) or "mixed" (float32
     tabulated wave term, float64 Rankine terms).
+
+    linear_solver (as capytaine's DefaultMatrixEngine, bem/engines.py:300-346):
+    "lu_decomposition" (default), "lu_decomposition_with_overwrite" (the same
+    here: K is always factored in place on the device), "gmres" (restarted
+    GMRES on the float64 K with SciPy's settings as capytaine's solve_gmres,
+    bem/engines.py:74-89: atol 1e-6, rtol 1e-5, restart 20; with precision
+    "fp64" only), or a callable ``(A, b) -> x`` used by ``linear_solver``.
+
+    refinement (precision "mixed"): "classical" (x += (LU)^-1 r) or "gmres"
+    (GMRES on the float64 K left-preconditioned by the float32 LU), both to
+    refine_tol relative residual.
     """
 
     def __init__(self, *, green_function: Optional[Delhommeau] = None, precision: str = "fp64",
-                 linear_solver: str = "lu_decomposition", max_batch: int = 8, device=None,
-                 refine_tol: float = 1e-10, refine_max_iter: int = 30, assembly_precision: str = "fp64"):
+                 linear_solver="lu_decomposition", max_batch: int = 8, device=None,
+                 refine_tol: float = 1e-10, refine_max_iter: int = 30, assembly_precision: str = "fp64",
+                 refinement: str = "classical", gmres_restart: int = 20, gmres_maxiter: Optional[int] = None):
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         if assembly_precision not in ("fp64", "mixed"):
             raise ValueError("assembly_precision must be 'fp64' or 'mixed'")
+        if not callable(linear_solver) and linear_solver not in ("lu_decomposition",
+                                                                 "lu_decomposition_with_overwrite", "gmres"):
+            raise NotImplementedError(f"Unknown `linear_solver` in B200Engine: {linear_solver}")
+        if linear_solver == "gmres" and precision != "fp64":
+            raise ValueError("linear_solver='gmres' is the float64 solver; use refinement='gmres' with 'mixed'")
+        if refinement not in ("classical", "gmres"):
+            raise ValueError("refinement must be 'classical' or 'gmres'")
         self.precision = precision
+        self.refinement = refinement
+        self.gmres_restart = int(gmres_restart)
+        self.gmres_maxiter = gmres_maxiter
         # float32 wave terms perturb the O(k)-small imaginary parts that carry the
         # radiation damping at low frequency beyond 1e-5: float64 assembly by default.
         self.assembly_precision = assembly_precision
@@ -153,6 +190,7 @@ class B200Engine:
             "linear_solver": str(linear_solver),
             "precision": precision,
             "assembly_precision": assembly_precision,
+            **({"refinement": refinement} if precision == "mixed" else {}),
             **self.green_function.exportable_settings,
         }
 
@@ -230,17 +268,18 @@ class B200Engine:
             ws.nan.zero_()
             ws.err.zero_()
             mixed = self.precision == "mixed"
+            plain_gmres = (not mixed) and self._linear_solver == "gmres"
             for b in range(nb):
                 gf.assemble_into(mesh, mesh, ws.S[b], ws.K[b], wavenumber=float(ks[b]), lds=n, ldk=ws.ldk,
                                  nan_flag=ws.nan, precision=self.assembly_precision)
-            if not mixed:
+            if not mixed and not plain_gmres:
                 _lib.check(lib.bem_zpad_identity(_vp(ws.K), npad, npad * npad, nb, n, npad, stream))
             if ev:
                 ev[1].record()
             if mixed:
                 _lib.check(lib.bem_clu_factor(_vp(ws.K), n, n * n, n, npad, nb, _vp(ws.piv), _vp(ws.info),
                                               _vp(ws.lu_work_ptr), _vp(ws.err), stream))
-            else:
+            elif not plain_gmres:
                 _lib.check(lib.bem_zlu_factor(_vp(ws.K), npad, npad, npad * npad, nb, _vp(ws.piv), _vp(ws.info),
                                               _vp(ws.lu_work), stream))
             if ev:
@@ -249,13 +288,23 @@ class B200Engine:
             _lib.check(lib.bem_build_rhs(n, nb, _vp(om_t), _vp(k_t), g, ndof, _vp(dofn), nhead, _vp(heads_t),
                                          _vp(dm.centers), _vp(dm.normals), _vp(hull), _vp(ws.B), npad, npad * nrhs,
                                          stream))
-            if mixed:
+            if plain_gmres:
+                sol = self._gmres_solve(ws, n, nb, nrhs, 1e-6, 1e-5, None, stats, stream)
+            elif mixed:
                 iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
-                status = lib.bem_refine_solve(_vp(ws.K), n, n * n, n, npad, nb, _vp(ws.lu_work_ptr), _vp(ws.piv),
-                                              _vp(ws.B), _vp(ws.X), _vp(ws.R), npad, npad * nrhs, nrhs,
-                                              self.refine_tol, self.refine_max_iter, _vp(ws.ts_work),
-                                              _vp(ws.norms), _vp(ws.err), ctypes.byref(iters),
-                                              ctypes.byref(resid), stream)
+                if self.refinement == "gmres":
+                    # relative residual refine_tol in every column: atol 0, rtol refine_tol
+                    maxc = max(1, -(-self.refine_max_iter // self.gmres_restart))
+                    status = lib.bem_gmres_solve(_vp(ws.K), n, n * n, n, npad, nb, _vp(ws.B), _vp(ws.X), npad,
+                                                 npad * nrhs, nrhs, 0.0, self.refine_tol, self.gmres_restart, maxc,
+                                                 _vp(ws.lu_work_ptr), _vp(ws.gmres_work(self.gmres_restart)),
+                                                 _vp(ws.err), ctypes.byref(iters), ctypes.byref(resid), stream)
+                else:
+                    status = lib.bem_refine_solve(_vp(ws.K), n, n * n, n, npad, nb, _vp(ws.lu_work_ptr),
+                                                  _vp(ws.piv), _vp(ws.B), _vp(ws.X), _vp(ws.R), npad, npad * nrhs,
+                                                  nrhs, self.refine_tol, self.refine_max_iter, _vp(ws.ts_work),
+                                                  _vp(ws.norms), _vp(ws.err), ctypes.byref(iters),
+                                                  ctypes.byref(resid), stream)
                 stats["refine_iters"] = max(stats.get("refine_iters", 0), iters.value)
                 stats["refine_residual"] = max(stats.get("refine_residual", 0.0), resid.value)
                 if status != _lib.BEM_OK and status != _lib.BEM_ERR_NOT_CONVERGED:
@@ -300,6 +349,25 @@ class B200Engine:
                 raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
         return self._coefficients(body, omegas, heads, F_all, FK_all, stats)
 
+    def _gmres_solve(self, ws, n, nb, nrhs, atol, rtol, precond_ptr, stats, stream):
+        """Plain float64 GMRES of every RHS column in ws.B into ws.X (SciPy's
+        settings: restart 20, at most 10 n cycles by default)."""
+        lib = _lib.load()
+        npad = ws.npad
+        maxc = self.gmres_maxiter if self.gmres_maxiter is not None else 10 * n
+        iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
+        status = lib.bem_gmres_solve(_vp(ws.K), ws.ldk, ws.ldk * ws.ldk if ws.ldk == npad else n * n, n, npad, nb,
+                                     _vp(ws.B), _vp(ws.X), npad, npad * nrhs, nrhs, atol, rtol, self.gmres_restart,
+                                     int(maxc), precond_ptr, _vp(ws.gmres_work(self.gmres_restart)), _vp(ws.err),
+                                     ctypes.byref(iters), ctypes.byref(resid), stream)
+        stats["gmres_iters"] = max(stats.get("gmres_iters", 0), iters.value)
+        stats["gmres_residual"] = max(stats.get("gmres_residual", 0.0), resid.value)
+        if status == _lib.BEM_ERR_NOT_CONVERGED:
+            raise _lib.NotConvergedError(status, lib.bem_last_error().decode() +
+                                         "\nThis can be due to overlapping panels or irregular frequencies.")
+        _lib.check(status)
+        return ws.X
+
     @staticmethod
     def _coefficients(body, omegas, heads, F_all, FK_all, stats):
         ndof = len(body.dofs)
@@ -341,10 +409,20 @@ class B200Engine:
 
     def linear_solver(self, A, b):
         """bem/engines.py:300-346: LU of A on the device, cached on A (the cache
-        entry replaces K, as the reference does), one RHS per call."""
+        entry replaces K, as the reference does), one RHS per call; or GMRES
+        (bem/engines.py:74-89); or the user's callable."""
+        if callable(self._linear_solver):
+            x = self._linear_solver(A, b)
+            if np.asarray(x).shape != np.asarray(b).shape:
+                raise ValueError(f"Error in linear solver of {self}: the shape of the output is not the same "
+                                 "as the shape of the RHS")
+            return x
         if not isinstance(A, DeviceMatrix):
             A = DeviceMatrix(_to_device(np.asarray(A), self.device), self)
-        x = A.solve(np.asarray(b))
+        if self._linear_solver == "gmres":
+            x = A.gmres(np.asarray(b), atol=1e-6, rtol=1e-5, restart=self.gmres_restart, maxiter=self.gmres_maxiter)
+        else:
+            x = A.solve(np.asarray(b))
         if x.shape != np.asarray(b).shape:
             raise ValueError("linear solver output shape mismatch")
         return x
@@ -429,6 +507,42 @@ class DeviceMatrix:
             raise _lib.SingularMatrixError(_lib.BEM_ERR_SINGULAR, f"zero pivot at column {int(info.item())}")
         self._lu = (Kf, piv, work, npad)
         return self._lu
+
+    def gmres(self, b: np.ndarray, *, atol=1e-6, rtol=1e-5, restart=20, maxiter=None) -> np.ndarray:
+        """Restarted GMRES on the device (x0 = 0), SciPy's criterion
+        |b - A x| <= max(atol, rtol |b|) per column; NotConvergedError (a
+        RuntimeError) otherwise, as capytaine's solve_gmres (bem/engines.py:74-89)."""
+        import torch
+        b = np.asarray(b)
+        vec = b.ndim == 1
+        Bm = b.reshape(b.shape[0], -1).astype(np.complex128)
+        n, nrhs = Bm.shape
+        dev = self.t.device
+        lib = _lib.load()
+        A = self.t.to(torch.complex128)
+        Acm = torch.empty((n, n), dtype=torch.complex128, device=dev)  # Acm[j, i] = A[i, j]: column-major
+        Acm.copy_(A.T)
+        maxc = int(maxiter) if maxiter is not None else 10 * n
+        out = np.empty_like(Bm)
+        for c0 in range(0, nrhs, 16):
+            c1 = min(nrhs, c0 + 16)
+            nc = c1 - c0
+            Bd = torch.as_tensor(np.ascontiguousarray(Bm[:, c0:c1].T), device=dev)  # column-major n x nc
+            Xd = torch.empty_like(Bd)
+            nbytes = int(lib.bem_gmres_workspace_bytes(n, n, nc, 1, restart))
+            work = torch.empty(nbytes + 256, dtype=torch.uint8, device=dev)
+            wptr = (work.data_ptr() + 255) // 256 * 256
+            iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
+            st = lib.bem_gmres_solve(_vp(Acm), n, 0, n, n, 1, _vp(Bd), _vp(Xd), n, 0, nc, float(atol), float(rtol),
+                                     int(restart), maxc, None, _vp(wptr), None, ctypes.byref(iters),
+                                     ctypes.byref(resid), _lib.stream_ptr())
+            if st == _lib.BEM_ERR_NOT_CONVERGED:
+                raise _lib.NotConvergedError(st, lib.bem_last_error().decode() +
+                                             "\nThis can be due to overlapping panels or irregular frequencies.")
+            _lib.check(st)
+            out[:, c0:c1] = Xd.T.cpu().numpy()
+        x = out[:, 0] if vec else out.reshape(b.shape)
+        return x.astype(np.complex64) if self.t.dtype == torch.complex64 else x
 
     def solve(self, b: np.ndarray) -> np.ndarray:
         import torch

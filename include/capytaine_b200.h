@@ -269,6 +269,33 @@ int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, int
                      int nrhs, double tol, int max_iter, void* ts_work_dev, double* norms_dev, int* err_dev,
                      int* iters_out, double* resid_out, void* stream);
 
+/* ---- GMRES ------------------------------------------------------------------ */
+/* Workspace of bem_gmres_solve in bytes (Krylov bases, Hessenberg matrices,
+ * rotations, per-system state, tall-GEMM partial sums); -1 for bad sizes. */
+int64_t bem_gmres_workspace_bytes(int n, int npad, int nrhs, int batch, int restart);
+
+/* Restarted GMRES, x0 = 0, for each of the nrhs columns of each of the `batch`
+ * matrices A (n x n complex128, column-major, lda, strideA apart).  Column c of
+ * B (ldb, strideB; rows < n read) converges when |b - A x| <= max(atol, rtol |b|);
+ * inner iterations stop when the (preconditioned) Arnoldi residual meets the
+ * adaptive inner tolerance, as scipy.sparse.linalg.gmres does.  restart <= 64
+ * (capytaine/SciPy: 20), at most max_cycles restart cycles.
+ * precond_work_dev: NULL for plain GMRES, or the factorisation of
+ * bem_clu_factor (npad multiple of 128, err_dev required) used as the left
+ * preconditioner M^-1 = (LU)^-1 with float32 factors and float64 products:
+ * GMRES-based iterative refinement of the mixed-precision LU.  X (ldb,
+ * strideB): rows < n written.  work_dev: bem_gmres_workspace_bytes, 256-byte
+ * aligned.  iters_out: largest number of inner iterations over the systems;
+ * resid_out: largest |b - A x| / |b|.  Synchronises the stream once per group
+ * of four inner iterations and once per cycle.  Returns BEM_ERR_NOT_CONVERGED
+ * when a system breaks down or max_cycles is reached.  Replaces
+ * scipy.sparse.linalg.gmres behind capytaine's solve_gmres
+ * (bem/engines.py:74-89). */
+int bem_gmres_solve(const void* A_dev, int64_t lda, int64_t strideA, int n, int npad, int batch, const void* B_dev,
+                    void* X_dev, int64_t ldb, int64_t strideB, int nrhs, double atol, double rtol, int restart,
+                    int max_cycles, void* precond_work_dev, void* work_dev, int* err_dev, int* iters_out,
+                    double* resid_out, void* stream);
+
 /* ---- allocation-free variant ---------------------------------------------- */
 /* No counterpart in the reference.  Same operation and arguments as
  * bem_zgemm_ts without the workspace: for callers that can only pass buffers

@@ -321,6 +321,16 @@ def integrate_pressure(mesh, dofs: Dict[str, Dof], pressure):
     return forces
 
 
+def solve_gmres(A, b):
+    """capytaine bem/engines.py:74-89: SciPy GMRES with atol=1e-6 (rtol 1e-5,
+    restart 20 by default); RuntimeError when it does not converge."""
+    import scipy.sparse.linalg as ssl
+    x, info = ssl.gmres(A, b, atol=1e-6)
+    if info > 0:
+        raise RuntimeError(f"No convergence of the GMRES after {info} iterations.")
+    return x
+
+
 def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: float, *, rho=1000.0, g=9.81,
                     wave_directions=(0.0,), free_surface=0.0, linear_solver="lu"):
     """One frequency-solve, indirect method (solver.py:188-207): assemble S and K at
@@ -345,7 +355,12 @@ def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: flo
             rhs_list.append(("dif", beta, bc))
     for kind, key, bc in rhs_list:
         rhs = bc.astype(np.complex128)
-        sigma = sl.lu_solve(lu, rhs) if lu is not None else np.linalg.solve(K, rhs)
+        if lu is not None:
+            sigma = sl.lu_solve(lu, rhs)
+        elif linear_solver == "gmres":
+            sigma = solve_gmres(K, rhs)
+        else:
+            sigma = np.linalg.solve(K, rhs)
         potential = S @ sigma
         pressure = 1j * omega * rho * potential
         forces = integrate_pressure(mesh, dofs, pressure)
