@@ -55,6 +55,84 @@ def workload_config(args, n):
             "rankine_part": "computed once per sweep of the 60 frequencies (cache cleared at each sweep start)"}
 
 
+RIGID_DOFS = ("Surge", "Sway", "Heave", "Roll", "Pitch", "Yaw")
+
+
+def seeded_bodies(seed, count, panels=(500, 8000)):
+    """Seeded floating bodies with panel counts uniform in `panels`: even
+    indices ellipsoids (semi-axes U[1, 10] m, centred on the free surface),
+    odd indices vertical cylinders (radius U[1, 8] m, draft U[2, 15] m), the
+    resolution chosen for the panel target; 1 to 6 rigid dofs about the origin."""
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.meshes import mesh_ellipsoid, mesh_vertical_cylinder
+    rng = np.random.default_rng(seed)
+    bodies = []
+    for i in range(count):
+        target = rng.uniform(*panels)
+        if i % 2 == 0:
+            axes = rng.uniform(1.0, 10.0, 3)
+            a = max(4, int(round(np.sqrt(target))))
+            mesh = mesh_ellipsoid(semi_axes=tuple(axes), resolution=(a, 2 * a)).immersed_part()
+        else:
+            r, d = rng.uniform(1.0, 8.0), rng.uniform(2.0, 15.0)
+            h = np.sqrt((2 * np.pi * r * d + 2 * np.pi * r * r) / target)  # side + bottom rings of nr x nth
+            nth = max(8, int(round(2 * np.pi * r / h)))
+            nz = max(1, int(round(d / h)))
+            nr = max(1, int(round(r / h)))
+            mesh = mesh_vertical_cylinder(length=2 * d, radius=r, resolution=(nr, nth, 2 * nz)).immersed_part()
+        ndof = int(rng.integers(1, 7))
+        dofs = [RIGID_DOFS[j] for j in sorted(rng.permutation(6)[:ndof])]
+        bodies.append(FloatingBody(mesh, rigid_body_dofs(only=dofs), name=f"body{i}"))
+    return bodies
+
+
+def run_serving(engine, bodies, *, rate, n_requests, seed, slots, repeat_frac=0.2):
+    """Poisson arrivals (mean `rate` per second, seeded) of frequency-solve
+    requests on the SolveServer: each request a body of the pool and omega ~
+    U[0.1, 4], or with probability repeat_frac a repeat of one of the 16 most
+    recent (body, omega) pairs, whose resident factors are reused.  Latency =
+    completion - arrival on the host clock."""
+    from capytaine_b200.serving import SolveServer
+    rng = np.random.default_rng(seed)
+    plan, recent = [], []
+    for _ in range(n_requests):
+        if recent and rng.random() < repeat_frac:
+            plan.append(recent[int(rng.integers(len(recent)))])
+        else:
+            pair = (bodies[int(rng.integers(len(bodies)))], float(rng.uniform(0.1, 4.0)))
+            plan.append(pair)
+            recent = (recent + [pair])[-16:]
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    with SolveServer(engine, slots=slots) as srv:
+        for b in bodies[:4]:  # warm-up: kernels loaded, tabulation resident
+            srv.solve(b, 1.0)
+        srv.release_resident()
+        futs = []
+        t0 = time.perf_counter()
+        for (b, w), ta in zip(plan, arrivals):
+            delay = t0 + ta - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            futs.append(srv.submit(b, w))
+        res = [f.result() for f in futs]
+        counters = dict(srv.counters)
+    lat = np.array([r.latency for r in res]) * 1e3
+    first = min(r.arrival for r in res)
+    last = max(r.finished for r in res)
+    panels = np.array([b.mesh_including_lid.nb_faces for b, _ in plan])
+    return {"arrival_rate_per_s": rate, "requests": n_requests, "slots": slots,
+            "solves_per_s": n_requests / (last - first), "offered_s": float(arrivals[-1]),
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(lat.max())},
+            "reused_factors": int(sum(r.reused_factors for r in res)),
+            "panels": {"min": int(panels.min()), "mean": float(panels.mean()), "max": int(panels.max())},
+            "max_inflight_requests": counters["max_inflight_requests"],
+            "max_reserved_gb": counters["max_reserved_bytes"] / 1e9, "evicted": counters["evicted"],
+            "body_pool": len(bodies), "seed": seed,
+            "workload": "Poisson arrivals; seeded ellipsoids / vertical cylinders of 500-8000 panels, 1-6 dofs, "
+                        "omega ~ U[0.1, 4], 20% repeats of resident (mesh, omega) pairs"}
+
+
 # ---------------------------------------------------------------------------
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
@@ -301,6 +379,10 @@ def main():
     ap.add_argument("--linear-solver", default="lu_decomposition", choices=["lu_decomposition", "gmres"],
                     help="solver of the float64 engine (--engine fp64)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=1000,
+                    help="requests of the serving run (Poisson arrivals); 0 skips it")
+    ap.add_argument("--arrival-rate", type=float, default=200.0)
+    ap.add_argument("--slots", type=int, default=6)
     args = ap.parse_args()
     args.world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
@@ -438,6 +520,15 @@ def main():
         fp64["mixed_over_fp64"] = value / fp64["value"]
         del eng64
 
+    # ---- serving: Poisson request stream, p50 / p99 latency ---------------
+    serving = None
+    if args.serving_requests > 0:
+        pool = seeded_bodies(1000 + rank, 32)
+        serving = run_serving(B200Engine(green_function=gf, precision=args.engine, refinement=args.refinement)
+                              if args.engine == "mixed" else B200Engine(green_function=gf, precision="fp64"),
+                              pool, rate=args.arrival_rate, n_requests=args.serving_requests, seed=7 + rank,
+                              slots=args.slots)
+
     # ---- CPU baseline (oracle port on the host cores) and accuracy --------
     cpu = None
     accuracy = None
@@ -469,7 +560,7 @@ def main():
                 "stages_ms_per_step": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()},
                 "kernels_timed_region": {k: {"ms_total": round(v["ms_total"], 3), "launches": v["launches"]}
                                          for k, v in kernels.items()},
-                "fp64_engine": fp64, "accuracy": accuracy}
+                "fp64_engine": fp64, "accuracy": accuracy, "serving": serving}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -181,5 +181,28 @@ def stream_ptr(stream=None):
     return ctypes.c_void_p(s.cuda_stream)
 
 
+class StreamShared:
+    """Device tensors written on one CUDA stream and read from others (caches
+    shared by the threads of a request server): a reader's stream waits for the
+    writer's event, and the tensors are marked as in use by the reader's stream
+    so that the caching allocator does not hand their memory out under it."""
+
+    def __init__(self, *tensors):
+        import torch
+        self.tensors = tensors
+        self.stream = torch.cuda.current_stream()
+        self.event = torch.cuda.Event()
+        self.event.record(self.stream)
+
+    def acquire(self):
+        import torch
+        cur = torch.cuda.current_stream()
+        if cur != self.stream:
+            cur.wait_event(self.event)
+            for t in self.tensors:
+                t.record_stream(cur)
+        return self
+
+
 def ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)

@@ -595,9 +595,11 @@ Planes planes_of(const MixedWork& w, int npad) {
   return Planes{w.W, w.W + (size_t)npad * npad, npad, 2 * (int64_t)npad * npad};
 }
 
-// Per-device side stream (highest priority) and the two events of the lookahead
-// in the block LU.  The mutex is held while a factorisation is enqueued, so the
-// events are never re-recorded by another caller in between.
+// Side stream (highest priority) and the two events of the lookahead in the
+// block LU, one set per (device, caller stream): factorisations enqueued on
+// different streams (concurrent requests of a server) overlap on the device
+// without sharing a side stream.  The mutex is held while a factorisation is
+// enqueued, so the events are never re-recorded by another caller in between.
 struct Lookahead {
   std::mutex mu;
   cudaStream_t side = nullptr;
@@ -605,12 +607,12 @@ struct Lookahead {
   cudaEvent_t panel = nullptr;
 };
 std::mutex g_lookahead_mu;
-std::map<int, std::unique_ptr<Lookahead>> g_lookahead;
-int lookahead_for_current_device(Lookahead** out) {
+std::map<std::pair<int, cudaStream_t>, std::unique_ptr<Lookahead>> g_lookahead;
+int lookahead_for(cudaStream_t caller, Lookahead** out) {
   int dev = 0;
   BEM_CUDA_CHECK(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(g_lookahead_mu);
-  std::unique_ptr<Lookahead>& la = g_lookahead[dev];
+  std::unique_ptr<Lookahead>& la = g_lookahead[std::make_pair(dev, caller)];
   if (!la) {
     auto fresh = std::make_unique<Lookahead>();
     int least = 0, greatest = 0;
@@ -692,7 +694,7 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
                              W.stride, r0, c0, m, nc, batch, err_dev, s);
   };
   Lookahead* la = nullptr;
-  if ((st = lookahead_for_current_device(&la))) return st;
+  if ((st = lookahead_for(s, &la))) return st;
   std::lock_guard<std::mutex> lock(la->mu);
   // Right-looking block LU with a lookahead of one block: after the strips of
   // step k that block k+1 needs (its block row and block column), the inverse

@@ -19,6 +19,7 @@ from __future__ import annotations
 import ctypes
 import logging
 import math
+import threading
 import time
 import weakref
 from collections import OrderedDict
@@ -63,50 +64,80 @@ class FrequencyResults:
                     excitation=self.excitation)
 
 
-class _Workspace:
-    """Device buffers of one (n, batch, nrhs, precision) shape, reused across batches.
+class _Factors:
+    """Device storage of the matrices of `batch` frequency-solves of one mesh
+    (n panels): S, K and the factorisation of K.
 
-    fp64:  K padded to a multiple of 64 (LU in place), S, right-hand sides B.
-    mixed: K unpadded (float64 residuals), float32 LU workspace padded to a
-           multiple of 128, B / X / R / D vectors of the refinement."""
+    fp64:  K padded to a multiple of 64 (LU in place, identity padding).
+    mixed: K unpadded (float64 residuals) and the float32 LU workspace padded
+           to a multiple of 128."""
 
-    def __init__(self, n, batch, nrhs, device, precision):
+    def __init__(self, n, batch, device, precision):
         import torch
-        self.n, self.batch, self.nrhs, self.precision = n, batch, nrhs, precision
+        self.n, self.batch, self.precision = n, batch, precision
         lib = _lib.load()
         c128 = dict(dtype=torch.complex128, device=device)
         self.S = torch.empty((batch, n * n), **c128)
-        self.phi = torch.empty((batch, n * nrhs), **c128)
         self.info = torch.zeros(batch, dtype=torch.int32, device=device)
-        self.err = torch.zeros(1, dtype=torch.int32, device=device)
-        self.nan = torch.zeros(1, dtype=torch.int32, device=device)
-        self.ts_work = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, min(nrhs, 16), batch)),
-                                   dtype=torch.uint8, device=device)
-        self._gmres = None
         if precision == "fp64":
             self.npad = padded_size(n)
-            npad = self.npad
-            self.K = torch.empty((batch, npad * npad), **c128)
-            self.ldk = npad
-            self.B = torch.zeros((batch, npad * nrhs), **c128)
-            self.X = torch.zeros((batch, npad * nrhs), **c128)
-            self.lu_work = torch.empty(int(lib.bem_zlu_workspace_bytes(npad, batch)), dtype=torch.uint8,
+            self.K = torch.empty((batch, self.npad * self.npad), **c128)
+            self.ldk = self.npad
+            self.strideK = self.npad * self.npad
+            self.lu_work = torch.empty(int(lib.bem_zlu_workspace_bytes(self.npad, batch)), dtype=torch.uint8,
                                        device=device)
-            self._aligned = None
+            self.lu_work_ptr = self.lu_work.data_ptr()
         else:
             self.npad = int(math.ceil(n / 128) * 128)
-            npad = self.npad
             self.K = torch.empty((batch, n * n), **c128)
             self.ldk = n
-            self.B = torch.zeros((batch, npad * nrhs), **c128)
-            self.X = torch.zeros((batch, npad * nrhs), **c128)
-            self.R = torch.zeros((batch, npad * nrhs), **c128)
-            self.norms = torch.zeros(2 * batch * nrhs + 2, dtype=torch.float64, device=device)
-            nbytes = int(lib.bem_clu_workspace_bytes(npad, batch))
+            self.strideK = n * n
+            nbytes = int(lib.bem_clu_workspace_bytes(self.npad, batch))
             self.lu_work = torch.empty(nbytes + 1024, dtype=torch.uint8, device=device)
-            base = self.lu_work.data_ptr()
-            self._aligned = (base + 1023) // 1024 * 1024  # 1024-byte aligned start
+            self.lu_work_ptr = (self.lu_work.data_ptr() + 1023) // 1024 * 1024  # 1024-byte aligned start
         self.piv = torch.empty((batch, self.npad), dtype=torch.int32, device=device)
+
+    @staticmethod
+    def estimate_bytes(n, batch, precision):
+        """Device bytes of a _Factors of this shape (admission by footprint)."""
+        lib = _lib.load()
+        if precision == "fp64":
+            npad = padded_size(n)
+            return batch * (16 * n * n + 16 * npad * npad) + int(lib.bem_zlu_workspace_bytes(npad, batch))
+        npad = int(math.ceil(n / 128) * 128)
+        return batch * 32 * n * n + int(lib.bem_clu_workspace_bytes(npad, batch)) + 1024
+
+    @property
+    def nbytes(self):
+        return sum(t.numel() * t.element_size() for t in (self.S, self.K, self.lu_work, self.piv, self.info))
+
+
+class _Rhs:
+    """Right-hand sides, solutions, potentials and the small work buffers of
+    `batch` frequency-solves with nrhs columns each (padded rows zero)."""
+
+    def __init__(self, n, npad, batch, nrhs, device, precision):
+        import torch
+        self.n, self.npad, self.batch, self.nrhs, self.precision = n, npad, batch, nrhs, precision
+        lib = _lib.load()
+        c128 = dict(dtype=torch.complex128, device=device)
+        self.B = torch.zeros((batch, npad * nrhs), **c128)
+        self.X = torch.zeros((batch, npad * nrhs), **c128)
+        self.R = torch.zeros((batch, npad * nrhs), **c128)
+        self.phi = torch.empty((batch, n * nrhs), **c128)
+        self.norms = torch.zeros(2 * batch * nrhs + 2, dtype=torch.float64, device=device)
+        self.ts_work = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch)), dtype=torch.uint8,
+                                   device=device)
+        self.flags = torch.zeros(2, dtype=torch.int32, device=device)  # [err, nan]
+        self._gmres = None
+
+    @property
+    def err(self):
+        return self.flags[0:1]
+
+    @property
+    def nan(self):
+        return self.flags[1:2]
 
     def gmres_work(self, restart):
         """256-byte aligned workspace of bem_gmres_solve for this shape."""
@@ -115,21 +146,35 @@ class _Workspace:
             nbytes = int(_lib.load().bem_gmres_workspace_bytes(self.n, self.npad, self.nrhs, self.batch, restart))
             if nbytes < 0:
                 raise ValueError("bad GMRES workspace shape")
-            buf = torch.empty(nbytes + 256, dtype=torch.uint8, device=self.K.device)
+            buf = torch.empty(nbytes + 256, dtype=torch.uint8, device=self.B.device)
             self._gmres = (restart, buf, (buf.data_ptr() + 255) // 256 * 256)
         return self._gmres[2]
 
-    @property
-    def lu_work_ptr(self):
-        return self._aligned if self._aligned is not None else self.lu_work.data_ptr()
+    @staticmethod
+    def estimate_bytes(n, npad, batch, nrhs):
+        lib = _lib.load()
+        return 16 * batch * nrhs * (3 * npad + n) + int(lib.bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch)) + 4096
 
     @property
     def nbytes(self):
-        ts = [t for t in (self.K, self.S, self.B, self.phi, self.lu_work, self.ts_work)]
-        ts += [getattr(self, k) for k in ("X", "R") if hasattr(self, k)]
+        ts = [self.B, self.X, self.R, self.phi, self.norms, self.ts_work, self.flags]
         if self._gmres is not None:
             ts.append(self._gmres[1])
         return sum(t.numel() * t.element_size() for t in ts)
+
+
+class _Workspace:
+    """Factor storage and RHS buffers of one (n, batch, nrhs, precision) shape,
+    reused across the batches of a sweep."""
+
+    def __init__(self, n, batch, nrhs, device, precision):
+        self.n, self.batch, self.nrhs, self.precision = n, batch, nrhs, precision
+        self.f = _Factors(n, batch, device, precision)
+        self.r = _Rhs(n, self.f.npad, batch, nrhs, device, precision)
+
+    @property
+    def nbytes(self):
+        return self.f.nbytes + self.r.nbytes
 
 
 class B200Engine:
@@ -183,6 +228,7 @@ class B200Engine:
         self._device = device
         self._ws: Dict[tuple, _Workspace] = {}
         self._body_cache: "OrderedDict[tuple, tuple]" = OrderedDict()
+        self._lock = threading.RLock()
         self.last_computed_inputs = None
         self.last_computed_matrices = None
         self.exportable_settings = {
@@ -219,23 +265,24 @@ class B200Engine:
         hull mask of a body, kept for the body's next call."""
         import torch
         key = (id(body), mesh.content_hash, tuple(body.dofs))
-        hit = self._body_cache.get(key)
-        if hit is not None and hit[0]() is body:
-            return hit[1]
-        dev = self.device
-        arrays = (torch.as_tensor(body.dof_normal_components(), dtype=torch.float64, device=dev).contiguous(),
-                  torch.as_tensor(body.pressure_weights(), dtype=torch.float64, device=dev).contiguous(),
-                  torch.as_tensor(body.hull_mask.astype(np.int32), device=dev))
-        self._body_cache[key] = (weakref.ref(body), arrays)
-        while len(self._body_cache) > 8:
-            self._body_cache.popitem(last=False)
-        return arrays
+        with self._lock:
+            hit = self._body_cache.get(key)
+            if hit is not None and hit[0]() is body:
+                hit[1].acquire()
+                return hit[1].tensors
+            dev = self.device
+            arrays = (torch.as_tensor(body.dof_normal_components(), dtype=torch.float64, device=dev).contiguous(),
+                      torch.as_tensor(body.pressure_weights(), dtype=torch.float64, device=dev).contiguous(),
+                      torch.as_tensor(body.hull_mask.astype(np.int32), device=dev))
+            self._body_cache[key] = (weakref.ref(body), _lib.StreamShared(*arrays))
+            while len(self._body_cache) > 32:
+                self._body_cache.popitem(last=False)
+            return arrays
 
     def solve_frequencies(self, body, omegas: Sequence[float], *, wave_directions: Sequence[float] = (0.0,),
                           rho: float = 1000.0, g: float = 9.81, batch: Optional[int] = None,
                           sync_stats: bool = False) -> FrequencyResults:
         import torch
-        dev = self.device
         mesh = body.mesh_including_lid
         n = mesh.nb_faces
         omegas = np.asarray(omegas, dtype=float)
@@ -246,127 +293,163 @@ class B200Engine:
             raise ValueError("at most 16 right-hand sides per frequency (dofs + headings)")
         B = min(self.max_batch if batch is None else batch, len(omegas))
         ws = self.workspace(n, B, nrhs)
-        npad = ws.npad
-        lib = _lib.load()
-        stream = _lib.stream_ptr()
-        gf = self.green_function
-        dm = gf.device_mesh(mesh)
-        dofn, wdof, hull = self._body_arrays(body, mesh)
-        heads_t = torch.as_tensor(heads, dtype=torch.float64, device=dev)
         F_all = np.zeros((len(omegas), nrhs, ndof), dtype=np.complex128)
         FK_all = np.zeros((len(omegas), max(nhead, 1), ndof), dtype=np.complex128)
         stats = {"assembly_ms": 0.0, "lu_ms": 0.0, "solve_ms": 0.0, "post_ms": 0.0}
         for start in range(0, len(omegas), B):
             om = omegas[start:start + B]
             nb = len(om)
-            ks = om ** 2 / g
-            om_t = torch.as_tensor(om, dtype=torch.float64, device=dev)
-            k_t = torch.as_tensor(ks, dtype=torch.float64, device=dev)
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)] if sync_stats else None
             if ev:
                 ev[0].record()
-            ws.nan.zero_()
-            ws.err.zero_()
-            mixed = self.precision == "mixed"
-            plain_gmres = (not mixed) and self._linear_solver == "gmres"
-            for b in range(nb):
-                gf.assemble_into(mesh, mesh, ws.S[b], ws.K[b], wavenumber=float(ks[b]), lds=n, ldk=ws.ldk,
-                                 nan_flag=ws.nan, precision=self.assembly_precision)
-            if not mixed and not plain_gmres:
-                _lib.check(lib.bem_zpad_identity(_vp(ws.K), npad, npad * npad, nb, n, npad, stream))
+            ws.r.flags.zero_()
+            self.assemble_stage(ws.f, mesh, om ** 2 / g, nan_flag=ws.r.nan)
             if ev:
                 ev[1].record()
-            if mixed:
-                _lib.check(lib.bem_clu_factor(_vp(ws.K), n, n * n, n, npad, nb, _vp(ws.piv), _vp(ws.info),
-                                              _vp(ws.lu_work_ptr), _vp(ws.err), stream))
-            elif not plain_gmres:
-                _lib.check(lib.bem_zlu_factor(_vp(ws.K), npad, npad, npad * npad, nb, _vp(ws.piv), _vp(ws.info),
-                                              _vp(ws.lu_work), stream))
+            self.factor_stage(ws.f, nb, ws.r.err)
             if ev:
                 ev[2].record()
-            ws.B.zero_()
-            _lib.check(lib.bem_build_rhs(n, nb, _vp(om_t), _vp(k_t), g, ndof, _vp(dofn), nhead, _vp(heads_t),
-                                         _vp(dm.centers), _vp(dm.normals), _vp(hull), _vp(ws.B), npad, npad * nrhs,
-                                         stream))
-            if plain_gmres:
-                sol = self._gmres_solve(ws, n, nb, nrhs, 1e-6, 1e-5, None, stats, stream)
-            elif mixed:
-                iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
-                if self.refinement == "gmres":
-                    # relative residual refine_tol in every column: atol 0, rtol refine_tol
-                    maxc = max(1, -(-self.refine_max_iter // self.gmres_restart))
-                    status = lib.bem_gmres_solve(_vp(ws.K), n, n * n, n, npad, nb, _vp(ws.B), _vp(ws.X), npad,
-                                                 npad * nrhs, nrhs, 0.0, self.refine_tol, self.gmres_restart, maxc,
-                                                 _vp(ws.lu_work_ptr), _vp(ws.gmres_work(self.gmres_restart)),
-                                                 _vp(ws.err), ctypes.byref(iters), ctypes.byref(resid), stream)
-                else:
-                    status = lib.bem_refine_solve(_vp(ws.K), n, n * n, n, npad, nb, _vp(ws.lu_work_ptr),
-                                                  _vp(ws.piv), _vp(ws.B), _vp(ws.X), _vp(ws.R), npad, npad * nrhs,
-                                                  nrhs, self.refine_tol, self.refine_max_iter, _vp(ws.ts_work),
-                                                  _vp(ws.norms), _vp(ws.err), ctypes.byref(iters),
-                                                  ctypes.byref(resid), stream)
-                stats["refine_iters"] = max(stats.get("refine_iters", 0), iters.value)
-                stats["refine_residual"] = max(stats.get("refine_residual", 0.0), resid.value)
-                if status != _lib.BEM_OK and status != _lib.BEM_ERR_NOT_CONVERGED:
-                    _lib.check(status)
-                if status == _lib.BEM_ERR_NOT_CONVERGED:
-                    stats["not_converged"] = stats.get("not_converged", 0) + 1
-                    raise _lib.NotConvergedError(status, lib.bem_last_error().decode())
-                sol = ws.X
-            else:
-                _lib.check(lib.bem_zlu_solve(_vp(ws.K), npad, npad, npad * npad, nb, _vp(ws.piv), _vp(ws.lu_work),
-                                             _vp(ws.B), npad, npad * nrhs, nrhs, _vp(ws.err), stream))
-                sol = ws.B
-            if ev:
-                ev[3].record()
-            _lib.check(lib.bem_zgemm_ts(n, n, nrhs, 1.0, 0.0, _vp(ws.S), n, n * n, _vp(sol), npad, npad * nrhs,
-                                        0.0, 0.0, _vp(ws.phi), n, n * nrhs, nb, _vp(ws.ts_work), stream))
-            F = torch.empty((nb, nrhs, ndof), dtype=torch.complex128, device=dev)
-            _lib.check(lib.bem_integrate_pressure(n, nb, nrhs, ndof, _vp(ws.phi), n, n * nrhs, _vp(om_t), rho,
-                                                  _vp(wdof), _vp(F), stream))
-            if nhead > 0:
-                FK = torch.empty((nb, nhead, ndof), dtype=torch.complex128, device=dev)
-                _lib.check(lib.bem_froude_krylov(n, nb, ndof, nhead, _vp(k_t), rho, g, _vp(heads_t),
-                                                 _vp(dm.centers), _vp(wdof), _vp(FK), stream))
-                FK_all[start:start + nb, :nhead] = FK.cpu().numpy()
-            if ev:
-                ev[4].record()
-            F_all[start:start + nb] = F.cpu().numpy()
-            flags = torch.cat([ws.info, ws.err, ws.nan]).cpu().numpy()
+            F, FK = self.solve_stage(ws.f, ws.r, body, om, heads, rho=rho, g=g, stats=stats, events=ev)
+            F_all[start:start + nb] = F
+            FK_all[start:start + nb, :nhead] = FK
             if ev:
                 torch.cuda.synchronize()
                 stats["assembly_ms"] += ev[0].elapsed_time(ev[1])
                 stats["lu_ms"] += ev[1].elapsed_time(ev[2])
                 stats["solve_ms"] += ev[2].elapsed_time(ev[3])
                 stats["post_ms"] += ev[3].elapsed_time(ev[4])
-            if flags[nb + 1] != 0:
-                raise _lib.GreenFunctionEvaluationError(_lib.BEM_ERR_NAN, "Green function returned a NaN in the "
-                                                        "interaction matrix.\nIt could be due to overlapping panels.")
-            if np.any(flags[:nb] != 0):
-                raise _lib.SingularMatrixError(_lib.BEM_ERR_SINGULAR,
-                                               f"zero pivot in the LU factorisation (info={flags[:nb].tolist()})")
-            if flags[nb] != 0:
-                raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
         return self._coefficients(body, omegas, heads, F_all, FK_all, stats)
 
-    def _gmres_solve(self, ws, n, nb, nrhs, atol, rtol, precond_ptr, stats, stream):
-        """Plain float64 GMRES of every RHS column in ws.B into ws.X (SciPy's
+    # ---- stages of a frequency-solve, on the caller's current stream -------
+    # (solve_frequencies chains them; the request server of serving.py runs
+    # them on one stream per slot and keeps factors resident between requests)
+    @property
+    def _plain_gmres(self):
+        return self.precision == "fp64" and self._linear_solver == "gmres"
+
+    def assemble_stage(self, f: "_Factors", mesh, ks, *, nan_flag=None, reuse_rankine=True):
+        """S and K of the mesh with itself at the wavenumbers ks into f[0:len(ks)]."""
+        gf = self.green_function
+        n = mesh.nb_faces
+        for b, k in enumerate(ks):
+            gf.assemble_into(mesh, mesh, f.S[b], f.K[b], wavenumber=float(k), lds=n, ldk=f.ldk, nan_flag=nan_flag,
+                             precision=self.assembly_precision, reuse_rankine=reuse_rankine)
+
+    def factor_stage(self, f: "_Factors", nb, err):
+        """LU of K (float64 DMMA, or float32 tcgen05 for the mixed engine); none for plain GMRES."""
+        lib = _lib.load()
+        stream = _lib.stream_ptr()
+        n, npad = f.n, f.npad
+        if self.precision == "mixed":
+            _lib.check(lib.bem_clu_factor(_vp(f.K), n, n * n, n, npad, nb, _vp(f.piv), _vp(f.info),
+                                          _vp(f.lu_work_ptr), _vp(err), stream))
+        elif not self._plain_gmres:
+            _lib.check(lib.bem_zpad_identity(_vp(f.K), npad, npad * npad, nb, n, npad, stream))
+            _lib.check(lib.bem_zlu_factor(_vp(f.K), npad, npad, npad * npad, nb, _vp(f.piv), _vp(f.info),
+                                          _vp(f.lu_work), stream))
+
+    def solve_stage(self, f: "_Factors", r: "_Rhs", body, om, heads, *, rho=1000.0, g=9.81, stats=None,
+                    events=None):
+        """Right-hand sides, solve with the factors, S @ sigma and the force
+        integrals for the frequencies om (f[0:len(om)]); returns host arrays
+        F (nb, nrhs, ndof) and FK (nb, nhead, ndof).  Raises the reference's
+        exceptions on NaN, zero pivot or non-convergence."""
+        import torch
+        lib = _lib.load()
+        stream = _lib.stream_ptr()
+        dev = f.K.device
+        stats = {} if stats is None else stats
+        mesh = body.mesh_including_lid
+        n, npad = f.n, f.npad
+        om = np.asarray(om, dtype=float)
+        nb = len(om)
+        ks = om ** 2 / g
+        heads = np.asarray(heads, dtype=float)
+        ndof, nhead = len(body.dofs), len(heads)
+        nrhs = ndof + nhead
+        if r.nrhs != nrhs or r.batch < nb:
+            raise ValueError("right-hand side buffers of the wrong shape")
+        dm = self.green_function.device_mesh(mesh)
+        dofn, wdof, hull = self._body_arrays(body, mesh)
+        small = torch.as_tensor(np.concatenate([om, ks, heads]), dtype=torch.float64, device=dev)
+        om_t, k_t, heads_t = small[:nb], small[nb:2 * nb], small[2 * nb:]
+        r.B.zero_()
+        _lib.check(lib.bem_build_rhs(n, nb, _vp(om_t), _vp(k_t), g, ndof, _vp(dofn), nhead, _vp(heads_t),
+                                     _vp(dm.centers), _vp(dm.normals), _vp(hull), _vp(r.B), npad, npad * nrhs,
+                                     stream))
+        if self._plain_gmres:
+            sol = self._gmres_solve(f, r, nb, 1e-6, 1e-5, None, stats, stream)
+        elif self.precision == "mixed":
+            iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
+            if self.refinement == "gmres":
+                # relative residual refine_tol in every column: atol 0, rtol refine_tol
+                maxc = max(1, -(-self.refine_max_iter // self.gmres_restart))
+                status = lib.bem_gmres_solve(_vp(f.K), n, n * n, n, npad, nb, _vp(r.B), _vp(r.X), npad, npad * nrhs,
+                                             nrhs, 0.0, self.refine_tol, self.gmres_restart, maxc,
+                                             _vp(f.lu_work_ptr), _vp(r.gmres_work(self.gmres_restart)), _vp(r.err),
+                                             ctypes.byref(iters), ctypes.byref(resid), stream)
+            else:
+                status = lib.bem_refine_solve(_vp(f.K), n, n * n, n, npad, nb, _vp(f.lu_work_ptr), _vp(f.piv),
+                                              _vp(r.B), _vp(r.X), _vp(r.R), npad, npad * nrhs, nrhs, self.refine_tol,
+                                              self.refine_max_iter, _vp(r.ts_work), _vp(r.norms), _vp(r.err),
+                                              ctypes.byref(iters), ctypes.byref(resid), stream)
+            stats["refine_iters"] = max(stats.get("refine_iters", 0), iters.value)
+            stats["refine_residual"] = max(stats.get("refine_residual", 0.0), resid.value)
+            if status == _lib.BEM_ERR_NOT_CONVERGED:
+                stats["not_converged"] = stats.get("not_converged", 0) + 1
+                raise _lib.NotConvergedError(status, lib.bem_last_error().decode())
+            _lib.check(status)
+            sol = r.X
+        else:
+            _lib.check(lib.bem_zlu_solve(_vp(f.K), npad, npad, npad * npad, nb, _vp(f.piv), _vp(f.lu_work),
+                                         _vp(r.B), npad, npad * nrhs, nrhs, _vp(r.err), stream))
+            sol = r.B
+        if events:
+            events[3].record()
+        _lib.check(lib.bem_zgemm_ts(n, n, nrhs, 1.0, 0.0, _vp(f.S), n, n * n, _vp(sol), npad, npad * nrhs,
+                                    0.0, 0.0, _vp(r.phi), n, n * nrhs, nb, _vp(r.ts_work), stream))
+        out = torch.empty((nb * nrhs * ndof + nb * max(nhead, 1) * ndof,), dtype=torch.complex128, device=dev)
+        F = out[:nb * nrhs * ndof]
+        FK = out[nb * nrhs * ndof:]
+        _lib.check(lib.bem_integrate_pressure(n, nb, nrhs, ndof, _vp(r.phi), n, n * nrhs, _vp(om_t), rho,
+                                              _vp(wdof), _vp(F), stream))
+        if nhead > 0:
+            _lib.check(lib.bem_froude_krylov(n, nb, ndof, nhead, _vp(k_t), rho, g, _vp(heads_t), _vp(dm.centers),
+                                             _vp(wdof), _vp(FK), stream))
+        if events:
+            events[4].record()
+        host = out.cpu().numpy()
+        flags = torch.cat([f.info[:nb], r.flags]).cpu().numpy()
+        if flags[nb + 1] != 0:
+            raise _lib.GreenFunctionEvaluationError(_lib.BEM_ERR_NAN, "Green function returned a NaN in the "
+                                                    "interaction matrix.\nIt could be due to overlapping panels.")
+        if np.any(flags[:nb] != 0):
+            raise _lib.SingularMatrixError(_lib.BEM_ERR_SINGULAR,
+                                           f"zero pivot in the LU factorisation (info={flags[:nb].tolist()})")
+        if flags[nb] != 0:
+            raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
+        F_h = host[:nb * nrhs * ndof].reshape(nb, nrhs, ndof)
+        FK_h = host[nb * nrhs * ndof:].reshape(nb, max(nhead, 1), ndof)[:, :nhead]
+        return F_h, FK_h
+
+    def _gmres_solve(self, f, r, nb, atol, rtol, precond_ptr, stats, stream):
+        """Plain float64 GMRES of every RHS column in r.B into r.X (SciPy's
         settings: restart 20, at most 10 n cycles by default)."""
         lib = _lib.load()
-        npad = ws.npad
+        n, npad, nrhs = f.n, f.npad, r.nrhs
         maxc = self.gmres_maxiter if self.gmres_maxiter is not None else 10 * n
         iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
-        status = lib.bem_gmres_solve(_vp(ws.K), ws.ldk, ws.ldk * ws.ldk if ws.ldk == npad else n * n, n, npad, nb,
-                                     _vp(ws.B), _vp(ws.X), npad, npad * nrhs, nrhs, atol, rtol, self.gmres_restart,
-                                     int(maxc), precond_ptr, _vp(ws.gmres_work(self.gmres_restart)), _vp(ws.err),
-                                     ctypes.byref(iters), ctypes.byref(resid), stream)
+        status = lib.bem_gmres_solve(_vp(f.K), f.ldk, f.strideK, n, npad, nb, _vp(r.B), _vp(r.X), npad, npad * nrhs,
+                                     nrhs, atol, rtol, self.gmres_restart, int(maxc), precond_ptr,
+                                     _vp(r.gmres_work(self.gmres_restart)), _vp(r.err), ctypes.byref(iters),
+                                     ctypes.byref(resid), stream)
         stats["gmres_iters"] = max(stats.get("gmres_iters", 0), iters.value)
         stats["gmres_residual"] = max(stats.get("gmres_residual", 0.0), resid.value)
         if status == _lib.BEM_ERR_NOT_CONVERGED:
             raise _lib.NotConvergedError(status, lib.bem_last_error().decode() +
                                          "\nThis can be due to overlapping panels or irregular frequencies.")
         _lib.check(status)
-        return ws.X
+        return r.X
 
     @staticmethod
     def _coefficients(body, omegas, heads, F_all, FK_all, stats):

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import logging
 import os
+import threading
 from collections import OrderedDict
 from typing import Optional
 
@@ -71,6 +72,8 @@ class DeviceMesh:
         self.nbytes = sum(t.numel() * t.element_size() for t in
                           (self.vertices, self.faces, self.centers, self.normals, self.areas, self.radii,
                            self.quad_points, self.quad_weights))
+        self.shared = _lib.StreamShared(self.vertices, self.faces, self.centers, self.normals, self.areas,
+                                        self.radii, self.quad_points, self.quad_weights)
 
 
 class Delhommeau:
@@ -121,6 +124,10 @@ class Delhommeau:
         self._tab_host = None
         self._dev_tab = None
         self._mesh_cache: "OrderedDict[str, DeviceMesh]" = OrderedDict()
+        # The caches are shared by the threads (and CUDA streams) of a request
+        # server: dictionary updates under this lock, device readiness through
+        # StreamShared events.
+        self._lock = threading.RLock()
         # Rankine parts of mesh-with-itself assemblies, reused across wavenumbers
         # (device memory budget in bytes; 0 disables the reuse).
         self.rankine_cache_bytes = 4 << 30
@@ -181,8 +188,13 @@ class Delhommeau:
     def _device_tabulation(self):
         """Device table (float64 and float32 copies), built on the GPU or loaded
         from the tabulation cache (capytaine delhommeau.py:208-261)."""
-        if self._dev_tab is not None:
+        with self._lock:
+            if self._dev_tab is None:
+                self._build_device_tabulation()
+            self._dev_tab_shared.acquire()
             return self._dev_tab
+
+    def _build_device_tabulation(self):
         import torch
         dev = self.device
         r = torch.as_tensor(self.tabulated_r_range, dtype=torch.float64, device=dev)
@@ -217,7 +229,7 @@ class Delhommeau:
                     except OSError:
                         LOG.warning("Could not save tabulation to %s", path)
         self._dev_tab = (r, z, table, table.to(torch.float32))
-        return self._dev_tab
+        self._dev_tab_shared = _lib.StreamShared(*self._dev_tab)
 
     @property
     def tabulated_integrals(self) -> np.ndarray:
@@ -232,14 +244,16 @@ class Delhommeau:
     # ---- meshes -------------------------------------------------------------
     def device_mesh(self, mesh) -> DeviceMesh:
         key = mesh.content_hash
-        dm = self._mesh_cache.get(key)
-        if dm is None:
-            dm = DeviceMesh(mesh, self.device)
-            self._mesh_cache[key] = dm
-            while len(self._mesh_cache) > 8:
-                self._mesh_cache.popitem(last=False)
-        else:
-            self._mesh_cache.move_to_end(key)
+        with self._lock:
+            dm = self._mesh_cache.get(key)
+            if dm is None:
+                dm = DeviceMesh(mesh, self.device)
+                self._mesh_cache[key] = dm
+                while len(self._mesh_cache) > 8:
+                    self._mesh_cache.popitem(last=False)
+            else:
+                self._mesh_cache.move_to_end(key)
+            dm.shared.acquire()
         return dm
 
     def _collocation(self, mesh1, mesh2, adjoint):
@@ -272,9 +286,12 @@ class Delhommeau:
 
     def assemble_into(self, mesh1, mesh2, S, K, *, free_surface=0.0, water_depth=np.inf, wavenumber=1.0,
                       adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True,
-                      lds=None, ldk=None, k_plane_stride=None, precision=None, stream=None, nan_flag=None):
+                      lds=None, ldk=None, k_plane_stride=None, precision=None, stream=None, nan_flag=None,
+                      reuse_rankine=True):
         """Write S and K into caller-owned device buffers (column-major with
-        leading dimensions lds/ldk) through ``bem_assemble``."""
+        leading dimensions lds/ldk) through ``bem_assemble``.  For a mesh with
+        itself the wavenumber-independent Rankine part is kept and reused
+        across calls unless reuse_rankine is False."""
         import torch
         if water_depth != np.inf:
             raise NotImplementedError("finite water depth is outside the B200 path (infinite depth only)")
@@ -324,7 +341,8 @@ class Delhommeau:
         )
         lib = _lib.load()
         same_mesh = hasattr(mesh1, "faces_centers") and mesh1.content_hash == mesh2.content_hash
-        if (same_mesh and dm2.collocation_at_quadrature and need_wave and sing in ("low_freq", "high_freq")
+        if (reuse_rankine and same_mesh and dm2.collocation_at_quadrature and need_wave
+                and sing in ("low_freq", "high_freq")
                 and prec == "fp64" and dtype == _lib.BEM_DTYPE_C128 and early_dot_product
                 and 16 * n * n <= self.rankine_cache_bytes):
             # Rankine part reused across wavenumbers; wave term once per pair of faces.
@@ -341,22 +359,25 @@ class Delhommeau:
         itself (bem_assemble_rankine_part), cached per mesh and variant."""
         import torch
         key = (mesh_key, adjoint, sing == "high_freq", free_surface)
-        rank = self._rankine_cache.get(key)
-        if rank is not None:
-            self._rankine_cache.move_to_end(key)
+        with self._lock:
+            hit = self._rankine_cache.get(key)
+            if hit is not None:
+                self._rankine_cache.move_to_end(key)
+                hit.acquire()
+                return hit.tensors[0]
+            n = dm.nb_faces
+            while self._rankine_cache and (sum(e.tensors[0].numel() * 16 for e in self._rankine_cache.values())
+                                           + 16 * n * n > self.rankine_cache_bytes):
+                self._rankine_cache.popitem(last=False)
+            rank = torch.empty((n, n), dtype=torch.complex128, device=self.device)
+            _lib.check(_lib.load().bem_assemble_rankine_part(args, rank.data_ptr(), n, _lib.stream_ptr(stream)))
+            self._rankine_cache[key] = _lib.StreamShared(rank)
             return rank
-        n = dm.nb_faces
-        while self._rankine_cache and (sum(t.numel() * 16 for t in self._rankine_cache.values()) + 16 * n * n
-                                       > self.rankine_cache_bytes):
-            self._rankine_cache.popitem(last=False)
-        rank = torch.empty((n, n), dtype=torch.complex128, device=self.device)
-        _lib.check(_lib.load().bem_assemble_rankine_part(args, rank.data_ptr(), n, _lib.stream_ptr(stream)))
-        self._rankine_cache[key] = rank
-        return rank
 
     def clear_rankine_cache(self):
         """Release the cached Rankine parts."""
-        self._rankine_cache.clear()
+        with self._lock:
+            self._rankine_cache.clear()
 
     def evaluate_device(self, mesh1, mesh2, *, free_surface=0.0, water_depth=np.inf, wavenumber=1.0,
                         adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True,

@@ -245,14 +245,12 @@ def _clean_mesh(vertices, faces, tol=1e-8, max_iter=5):
                 seen_f.add(key)
                 uniq_faces.append(f)
         faces = uniq_faces
-        # 4) small faces
-        def area(f):
-            p = vertices[f]
-            a = 0.5 * np.linalg.norm(np.cross(p[1] - p[0], p[2] - p[0]))
-            if len(f) == 4:
-                a += 0.5 * np.linalg.norm(np.cross(p[2] - p[0], p[3] - p[0]))
-            return a
-        faces = [f for f in faces if area(f) > tol]
+        # 4) small faces (a triangle padded with its last vertex adds a zero second half)
+        if faces:
+            fv = vertices[np.array([f if len(f) == 4 else f + [f[-1]] for f in faces])]
+            areas = 0.5 * (np.linalg.norm(np.cross(fv[:, 1] - fv[:, 0], fv[:, 2] - fv[:, 0]), axis=1)
+                           + np.linalg.norm(np.cross(fv[:, 2] - fv[:, 0], fv[:, 3] - fv[:, 0]), axis=1))
+            faces = [f for f, a in zip(faces, areas) if a > tol]
         # 5) unused vertices
         used = sorted({i for f in faces for i in f})
         remap = {old: new for new, old in enumerate(used)}

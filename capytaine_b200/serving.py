@@ -1,0 +1,337 @@
+"""Request server for frequency-solves on one B200: continuous batching.
+
+A request is one frequency-solve of one body: assemble S and K at
+k = omega^2/g, factor K, solve every radiation and diffraction problem, S @
+sigma, forces -> added mass, radiation damping, excitation (what capytaine's
+``BEMSolver.solve_all`` does for one (body, omega) group, bem/solver.py:268-372).
+capytaine itself has no server; this is the request loop around the same
+engine stages (``B200Engine.assemble_stage`` / ``factor_stage`` /
+``solve_stage``).
+
+Scheduling
+* ``submit`` queues a request and returns a ``concurrent.futures.Future``.
+* ``slots`` worker threads, each with its own CUDA stream: requests admitted
+  while others run are enqueued on their own stream, so their kernels overlap
+  on the device (different mesh sizes run side by side).
+* Admission by device-memory footprint: a request is admitted (in arrival
+  order) when a slot is free and the bytes of its matrices, factors and
+  right-hand sides fit in ``memory_budget`` next to what is in flight and what
+  is resident; resident factors not in use are evicted (least recently used)
+  to make room.  A request that alone exceeds the budget fails with
+  MemoryError.
+* Residency: the factors of every solved (mesh, omega) stay on the device
+  (with S and K) until evicted; a later request for the same mesh and omega
+  only solves its right-hand sides with them.  Device meshes and the
+  tabulation are resident in the Green function's caches.
+
+Results do not depend on what else runs: every kernel is deterministic and
+requests share no mutable device memory.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import logging
+import threading
+import time
+from collections import OrderedDict, deque
+from dataclasses import dataclass, field
+from typing import Deque, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .engine import B200Engine, _Factors, _Rhs
+
+LOG = logging.getLogger(__name__)
+
+
+@dataclass
+class SolveResult:
+    """Coefficients of one frequency-solve: added_mass / radiation_damping
+    [radiating_dof, influenced_dof], diffraction / froude_krylov / excitation
+    [heading, influenced_dof]; host clock times (time.perf_counter) of arrival,
+    admission and completion; whether resident factors were reused."""
+    request_id: int
+    omega: float
+    dofs: List[str]
+    wave_directions: np.ndarray
+    added_mass: np.ndarray
+    radiation_damping: np.ndarray
+    diffraction: np.ndarray
+    froude_krylov: np.ndarray
+    excitation: np.ndarray
+    arrival: float
+    admitted: float
+    finished: float
+    reused_factors: bool
+    stats: Dict[str, float] = field(default_factory=dict)
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+@dataclass
+class _Request:
+    rid: int
+    body: object
+    omega: float
+    heads: np.ndarray
+    rho: float
+    g: float
+    arrival: float
+    future: cf.Future
+    key: tuple = ()
+    n: int = 0
+    nrhs: int = 0
+
+
+class _Resident:
+    """S, K and the factors of one (mesh, omega) kept on the device between requests."""
+
+    def __init__(self, f: _Factors, nbytes: int):
+        self.f = f
+        self.nbytes = nbytes
+        self.users = 0
+        self.lock = threading.Lock()
+
+
+class SolveServer:
+    """Continuous-batching request loop (see the module docstring).
+
+    engine: a B200Engine (its precision, refinement and Green function are
+    used; default: the refined mixed-precision engine).  memory_budget: device
+    bytes for in-flight requests plus resident factors (default 60% of the
+    device memory).  slots: concurrent requests on the device.  keep_factors:
+    keep the factors of solved (mesh, omega) pairs resident for reuse.
+    """
+
+    def __init__(self, engine: Optional[B200Engine] = None, *, slots: int = 4, memory_budget: Optional[int] = None,
+                 keep_factors: bool = True):
+        import torch
+        self.engine = engine if engine is not None else B200Engine(precision="mixed")
+        dev = torch.device(self.engine.device)
+        if dev.type == "cuda" and dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        if memory_budget is None:
+            total = torch.cuda.get_device_properties(self.device).total_memory
+            memory_budget = int(0.6 * total)
+        self.memory_budget = int(memory_budget)
+        self.keep_factors = bool(keep_factors)
+        self._cv = threading.Condition()
+        self._pending: Deque[_Request] = deque()
+        self._resident: "OrderedDict[tuple, _Resident]" = OrderedDict()
+        self._resident_bytes = 0
+        self._inflight_bytes = 0
+        self._next_id = 0
+        self._closed = False
+        self._failure: Optional[BaseException] = None
+        self.counters = {"submitted": 0, "completed": 0, "failed": 0, "reused": 0, "evicted": 0,
+                         "max_reserved_bytes": 0, "max_inflight_requests": 0}
+        self._inflight = 0
+        self._workers = [threading.Thread(target=self._worker, name=f"bem-slot-{i}", daemon=True)
+                         for i in range(int(slots))]
+        for t in self._workers:
+            t.start()
+
+    # ---- public API ---------------------------------------------------------
+    def submit(self, body, omega: float, *, wave_directions: Sequence[float] = (0.0,), rho: float = 1000.0,
+               g: float = 9.81) -> cf.Future:
+        heads = np.asarray(wave_directions, dtype=float)
+        mesh = body.mesh_including_lid
+        nrhs = len(body.dofs) + len(heads)
+        if nrhs > 16:
+            raise ValueError("at most 16 right-hand sides per frequency (dofs + headings)")
+        fut: cf.Future = cf.Future()
+        with self._cv:
+            if self._failure is not None:
+                raise RuntimeError(f"request server slot failed: {self._failure!r}")
+            if self._closed:
+                raise RuntimeError("server is shut down")
+            rid = self._next_id
+            self._next_id += 1
+            req = _Request(rid, body, float(omega), heads, float(rho), float(g), time.perf_counter(), fut)
+            req.key = (mesh.content_hash, float(omega), float(g))
+            req.n = mesh.nb_faces
+            req.nrhs = nrhs
+            self._pending.append(req)
+            self.counters["submitted"] += 1
+            self._cv.notify_all()
+        return fut
+
+    def solve(self, body, omega: float, *, timeout: Optional[float] = None, **kw) -> SolveResult:
+        """Submit and wait (at most `timeout` seconds when given)."""
+        return self.submit(body, omega, **kw).result(timeout=timeout)
+
+    def shutdown(self, wait: bool = True):
+        with self._cv:
+            self._closed = True
+            self._cv.notify_all()
+        if wait:
+            for t in self._workers:
+                t.join()
+
+    def release_resident(self):
+        """Drop every resident factorisation not in use."""
+        with self._cv:
+            for key in [k for k, e in self._resident.items() if e.users == 0]:
+                self._drop_locked(key)
+
+    @property
+    def resident_bytes(self) -> int:
+        return self._resident_bytes
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.shutdown()
+
+    # ---- admission ----------------------------------------------------------
+    def _footprint(self, req: _Request, reuse: bool) -> int:
+        """Device bytes a request holds while it runs: its S, K and factors
+        (unless resident factors are reused) and its right-hand sides."""
+        prec = self.engine.precision
+        blk = 128 if prec == "mixed" else 64
+        npad = -(-req.n // blk) * blk
+        f_bytes = 0 if reuse else _Factors.estimate_bytes(req.n, 1, prec)
+        return f_bytes + _Rhs.estimate_bytes(req.n, npad, 1, req.nrhs)
+
+    def _drop_locked(self, key):
+        e = self._resident.pop(key)
+        self._resident_bytes -= e.nbytes
+        self.counters["evicted"] += 1
+
+    def _make_room_locked(self, need: int) -> bool:
+        while self._inflight_bytes + self._resident_bytes + need > self.memory_budget:
+            victim = next((k for k, e in self._resident.items() if e.users == 0), None)
+            if victim is None:
+                return False
+            self._drop_locked(victim)
+        return True
+
+    def _take_locked(self):
+        """Admission in arrival order: the head of the queue when it fits."""
+        if not self._pending:
+            return None
+        head = self._pending[0]
+        res = self._resident.get(head.key)
+        need = self._footprint(head, res is not None)
+        if need > self.memory_budget:
+            self._pending.popleft()
+            head.future.set_exception(MemoryError(
+                f"request of {head.n} panels needs {need / 1e9:.2f} GB, above the server budget "
+                f"{self.memory_budget / 1e9:.2f} GB"))
+            self.counters["failed"] += 1
+            return "retry"
+        if res is not None:
+            res.users += 1  # pinned before making room, so it is not evicted
+            self._resident.move_to_end(head.key)
+        if not self._make_room_locked(need):
+            if res is not None:
+                res.users -= 1
+            return None
+        self._pending.popleft()
+        return head, res, need
+
+    def _slot_stream(self):
+        """Context placing the calling thread's work on its own CUDA stream."""
+        import contextlib
+        import torch
+        dev = torch.device(self.device)
+        if dev.type != "cuda":  # host-side tests of the scheduler with a stand-in engine
+            return contextlib.nullcontext()
+        torch.cuda.set_device(dev.index)
+        return torch.cuda.stream(torch.cuda.Stream(device=dev))
+
+    def _worker(self):
+        try:
+            self._serve()
+        except BaseException as exc:  # a slot that cannot run fails the queue instead of hanging it
+            with self._cv:
+                self._closed = True
+                self._failure = exc
+                while self._pending:
+                    req = self._pending.popleft()
+                    if not req.future.done():
+                        req.future.set_exception(RuntimeError(f"request server slot failed: {exc!r}"))
+                self._cv.notify_all()
+            LOG.error("request server slot failed: %r", exc)
+
+    def _serve(self):
+        slot = self._slot_stream()
+        while True:
+            with self._cv:
+                while True:
+                    if self._closed and not self._pending:
+                        return
+                    got = self._take_locked()
+                    if got == "retry":
+                        continue
+                    if got is not None:
+                        break
+                    self._cv.wait()
+                req, res, need = got
+                self._inflight_bytes += need
+                self._inflight += 1
+                self.counters["max_inflight_requests"] = max(self.counters["max_inflight_requests"], self._inflight)
+                self.counters["max_reserved_bytes"] = max(self.counters["max_reserved_bytes"],
+                                                          self._inflight_bytes + self._resident_bytes)
+            admitted = time.perf_counter()
+            keep = None
+            try:
+                with slot:
+                    keep = self._run(req, res, admitted)
+            except BaseException as exc:  # the request fails, the server goes on
+                if not req.future.done():
+                    req.future.set_exception(exc)
+            finally:
+                with self._cv:
+                    self._inflight_bytes -= need
+                    self._inflight -= 1
+                    if res is not None:
+                        res.users -= 1
+                    if keep is not None and req.key not in self._resident and self._make_room_locked(keep.nbytes):
+                        self._resident[req.key] = _Resident(keep, keep.nbytes)
+                        self._resident_bytes += keep.nbytes
+                    if req.future.exception() is None:
+                        self.counters["completed"] += 1
+                    else:
+                        self.counters["failed"] += 1
+                    self._cv.notify_all()
+
+    def _run(self, req: _Request, res: Optional[_Resident], admitted: float):
+        """Enqueue the request's work on the current (slot) stream and wait
+        for it; returns the factors to keep resident, if any."""
+        eng = self.engine
+        body = req.body
+        mesh = body.mesh_including_lid
+        om = np.array([req.omega])
+        stats: Dict[str, float] = {}
+        if res is not None:
+            with res.lock:  # repeats of one entry take turns on its buffers
+                r = _Rhs(res.f.n, res.f.npad, 1, req.nrhs, self.device, eng.precision)
+                F, FK = eng.solve_stage(res.f, r, body, om, req.heads, rho=req.rho, g=req.g, stats=stats)
+            keep = None
+        else:
+            f = _Factors(req.n, 1, self.device, eng.precision)
+            r = _Rhs(f.n, f.npad, 1, req.nrhs, self.device, eng.precision)
+            r.flags.zero_()
+            eng.assemble_stage(f, mesh, om ** 2 / req.g, nan_flag=r.nan, reuse_rankine=False)
+            eng.factor_stage(f, 1, r.err)
+            F, FK = eng.solve_stage(f, r, body, om, req.heads, rho=req.rho, g=req.g, stats=stats)
+            keep = f if self.keep_factors else None
+        finished = time.perf_counter()
+        ndof = len(body.dofs)
+        w = req.omega
+        rad, dif, fk = F[0, :ndof, :], F[0, ndof:, :], FK[0]
+        req.future.set_result(SolveResult(
+            request_id=req.rid, omega=w, dofs=list(body.dofs), wave_directions=req.heads,
+            added_mass=np.real(rad) / w ** 2, radiation_damping=np.imag(rad) / w, diffraction=dif,
+            froude_krylov=fk, excitation=dif + fk, arrival=req.arrival, admitted=admitted, finished=finished,
+            reused_factors=res is not None, stats=dict(stats)))
+        if res is not None:
+            with self._cv:
+                self.counters["reused"] += 1
+        return keep

@@ -14,6 +14,18 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "slow: long-running case")
 
 
+def pytest_collection_modifyitems(config, items):
+    """A GPU test that stops making progress fails after 15 minutes instead of
+    holding the device (pytest-timeout, when installed)."""
+    try:
+        import pytest_timeout  # noqa: F401
+    except ImportError:
+        return
+    for item in items:
+        if item.get_closest_marker("gpu") and not item.get_closest_marker("timeout"):
+            item.add_marker(pytest.mark.timeout(900))
+
+
 @pytest.fixture(scope="session")
 def golden():
     import json
