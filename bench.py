@@ -86,27 +86,42 @@ def seeded_bodies(seed, count, panels=(500, 8000)):
     return bodies
 
 
+def scaled_body(body, factors, name):
+    """A distinct body: the mesh of `body` stretched by `factors` along x, y, z
+    (same topology, new geometry), same dofs; its host-side geometry computed."""
+    from capytaine_b200.bodies import FloatingBody
+    m = body.mesh.scaled(factors)
+    for prop in ("faces_centers", "faces_normals", "faces_areas", "faces_radiuses", "quadrature_points",
+                 "content_hash"):
+        getattr(m, prop)
+    return FloatingBody(m, body.dofs, name=name)
+
+
 def run_serving(engine, bodies, *, rate, n_requests, seed, slots, repeat_frac=0.2):
     """Poisson arrivals (mean `rate` per second, seeded) of frequency-solve
-    requests on the SolveServer: each request a body of the pool and omega ~
-    U[0.1, 4], or with probability repeat_frac a repeat of one of the 16 most
-    recent (body, omega) pairs, whose resident factors are reused.  Latency =
-    completion - arrival on the host clock."""
+    requests on the SolveServer: each new request a distinct body (a body of
+    the pool stretched by U[0.8, 1.25] along each axis) at omega ~ U[0.1, 4];
+    with probability repeat_frac a repeat of one of the 16 most recent (body,
+    omega) pairs, whose resident factors are reused.  Latency = completion -
+    arrival on the host clock."""
     from capytaine_b200.serving import SolveServer
     rng = np.random.default_rng(seed)
     plan, recent = [], []
-    for _ in range(n_requests):
+    for i in range(n_requests):
         if recent and rng.random() < repeat_frac:
             plan.append(recent[int(rng.integers(len(recent)))])
         else:
-            pair = (bodies[int(rng.integers(len(bodies)))], float(rng.uniform(0.1, 4.0)))
+            base = bodies[int(rng.integers(len(bodies)))]
+            pair = (scaled_body(base, rng.uniform(0.8, 1.25, 3), f"request{i}"), float(rng.uniform(0.1, 4.0)))
             plan.append(pair)
             recent = (recent + [pair])[-16:]
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
     with SolveServer(engine, slots=slots) as srv:
-        for b in bodies[:4]:  # warm-up: kernels loaded, tabulation resident
-            srv.solve(b, 1.0)
+        warm = [srv.submit(b, 1.0) for b in bodies[:2 * slots]]  # kernels loaded, every slot used
+        for f in warm:
+            f.result()
         srv.release_resident()
+        srv.counters.update(evicted=0, reused=0, max_inflight_requests=0, max_reserved_bytes=0)
         futs = []
         t0 = time.perf_counter()
         for (b, w), ta in zip(plan, arrivals):
@@ -114,23 +129,33 @@ def run_serving(engine, bodies, *, rate, n_requests, seed, slots, repeat_frac=0.
             if delay > 0:
                 time.sleep(delay)
             futs.append(srv.submit(b, w))
-        res = [f.result() for f in futs]
+        res, errors = [], []
+        for f in futs:
+            try:
+                res.append(f.result())
+            except Exception as exc:  # reported in the line, not fatal to the run
+                errors.append(repr(exc)[:200])
         counters = dict(srv.counters)
+        arena_peak = srv._arena.peak
     lat = np.array([r.latency for r in res]) * 1e3
     first = min(r.arrival for r in res)
     last = max(r.finished for r in res)
+    escalated = sum(1 for r in res if r.stats.get("escalated_to_gmres"))
     panels = np.array([b.mesh_including_lid.nb_faces for b, _ in plan])
     return {"arrival_rate_per_s": rate, "requests": n_requests, "slots": slots,
-            "solves_per_s": n_requests / (last - first), "offered_s": float(arrivals[-1]),
+            "completed": len(res), "failed": len(errors), "first_error": errors[0] if errors else None,
+            "escalated_to_gmres": escalated,
+            "solves_per_s": len(res) / (last - first), "offered_s": float(arrivals[-1]),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "max": float(lat.max())},
             "reused_factors": int(sum(r.reused_factors for r in res)),
             "panels": {"min": int(panels.min()), "mean": float(panels.mean()), "max": int(panels.max())},
             "max_inflight_requests": counters["max_inflight_requests"],
             "max_reserved_gb": counters["max_reserved_bytes"] / 1e9, "evicted": counters["evicted"],
-            "body_pool": len(bodies), "seed": seed,
-            "workload": "Poisson arrivals; seeded ellipsoids / vertical cylinders of 500-8000 panels, 1-6 dofs, "
-                        "omega ~ U[0.1, 4], 20% repeats of resident (mesh, omega) pairs"}
+            "arena_peak_gb": arena_peak / 1e9, "body_pool": len(bodies), "seed": seed,
+            "workload": "Poisson arrivals; distinct seeded bodies (ellipsoids / vertical cylinders of 500-8000 "
+                        "panels stretched per request), 1-6 dofs, omega ~ U[0.1, 4], 20% repeats of resident "
+                        "(mesh, omega) pairs"}
 
 
 # ---------------------------------------------------------------------------

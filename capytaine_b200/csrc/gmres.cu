@@ -1,5 +1,5 @@
 // Restarted GMRES for the dense complex128 BEM systems, batched over matrices and
-// right-hand sides, optionally left-preconditioned by the float32 block LU.
+// right-hand sides, optionally right-preconditioned by the float32 block LU.
 //
 // Without a preconditioner this is the iteration of scipy.sparse.linalg.gmres
 // (SciPy 1.18 `_isolve/iterative.py`) as capytaine calls it in solve_gmres
@@ -8,9 +8,12 @@
 // rotations, back substitution of the Hessenberg system at the end of each
 // restart cycle, the true residual b - A x checked after each cycle and the
 // inner tolerance adapted as SciPy does (gh-8400 rule).  With the float32 LU
-// factors of bem_clu_factor as M^-1 it is GMRES on M^-1 A x = M^-1 b with a
-// float64 matrix-vector product: GMRES-based iterative refinement of the
-// mixed-precision LU.
+// factors of bem_clu_factor as M^-1 it is right-preconditioned GMRES,
+// A M^-1 u = b, x = M^-1 u, with float64 products: the Arnoldi residual is the
+// true residual, so a preconditioner that is poor in a few directions (K close
+// to singular near an irregular frequency) costs a few iterations, not the
+// convergence test.  This is GMRES-based iterative refinement of the
+// mixed-precision LU (capytaine calls SciPy's GMRES without a preconditioner).
 //
 // Every column of every matrix is an independent system ("system" below).  All
 // systems advance in lockstep: one matrix-vector product serves the current
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(kThreads) gmres_setup_kernel(Layout L, const d
   }
 }
 
-// W = R for the systems still running (start of a cycle, before M^-1).
+// W = R for the systems still running (start of a cycle).
 __global__ void gmres_copy_kernel(Layout L, const double2* __restrict__ R, double2* __restrict__ W,
                                   const GmresSystem* sys, const Flags* flags) {
   if (flags->skip_all) return;
@@ -185,8 +188,9 @@ __global__ void gmres_copy_kernel(Layout L, const double2* __restrict__ R, doubl
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) W[o + i] = R[o + i];
 }
 
-// Start of a cycle: v0 = z / |z| with z = M^-1 r in W, S = (|z|, 0, ...).  On the
-// first cycle also ptol = |M^-1 b| min(1, atol / |b|).
+// Start of a cycle: v0 = r / |r| (r in W), S = (|r|, 0, ...).  On the first
+// cycle also ptol = |b| min(1, atol / |b|) (SciPy's rule without a left
+// preconditioner).
 __global__ void __launch_bounds__(kThreads) gmres_start_kernel(Layout L, const double2* __restrict__ W,
                                                                double2* __restrict__ V, double2* __restrict__ Svec,
                                                                GmresSystem* sys, int first, Flags* flags) {
@@ -216,7 +220,7 @@ __global__ void __launch_bounds__(kThreads) gmres_start_kernel(Layout L, const d
       if (tmp > 0.0) {
         g.active = 1;
         g.ran = 1;
-      } else {  // M^-1 r = 0 with M nonsingular: r = 0, x is exact
+      } else {  // r = 0: x is exact
         g.active = 0;
         g.ran = 0;
         g.done = 1;
@@ -352,16 +356,23 @@ __global__ void __launch_bounds__(kThreads) gmres_arnoldi_kernel(Layout L, int c
 
 // End of a cycle: y = H^-1 S by back substitution (SciPy's pseudo-solve of
 // singular cases), x += V y; R = b for the residual.
+// With right preconditioning (Z != NULL) the combination z = V y goes to Z
+// (zero for systems that did not run) and x += M^-1 z follows.
 __global__ void __launch_bounds__(kThreads) gmres_update_kernel(Layout L, const double2* __restrict__ V,
                                                                 const double2* __restrict__ H,
                                                                 double2* __restrict__ Svec, const double2* __restrict__ Bv,
                                                                 double2* __restrict__ X, double2* __restrict__ R,
-                                                                const GmresSystem* sys, const Flags* flags) {
+                                                                double2* __restrict__ Z, const GmresSystem* sys,
+                                                                const Flags* flags) {
   __shared__ double2 y[kMaxRestart];
   if (flags->skip_all) return;
   const int s = blockIdx.x;
   const GmresSystem g = sys[s];
-  if (!g.ran || g.col_end < 0) return;
+  if (!g.ran || g.col_end < 0) {
+    if (Z)
+      for (int i = threadIdx.x; i < L.npad; i += blockDim.x) Z[L.vec_off(s) + i] = make_double2(0.0, 0.0);
+    return;
+  }
   const int col = g.col_end;
   if (threadIdx.x == 0) {
     const double2* h = H + (int64_t)s * L.m * (L.m + 1);  // h[c][r] at c*(m+1) + r
@@ -386,6 +397,20 @@ __global__ void __launch_bounds__(kThreads) gmres_update_kernel(Layout L, const 
   double2* x = X + L.x_off(s);
   const double2* b = Bv + L.x_off(s);
   double2* r = R + L.vec_off(s);
+  if (Z) {
+    double2* z = Z + L.vec_off(s);
+    for (int i = threadIdx.x; i < L.npad; i += blockDim.x) {
+      double2 zi = make_double2(0.0, 0.0);
+      for (int k = 0; k <= col; ++k) {
+        const double2 p = cmul(y[k], V[L.v_off(s, k) + i]);
+        zi.x += p.x;
+        zi.y += p.y;
+      }
+      z[i] = zi;
+      if (i < L.n) r[i] = b[i];
+    }
+    return;
+  }
   for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
     double2 xi = x[i];
     for (int k = 0; k <= col; ++k) {
@@ -396,6 +421,31 @@ __global__ void __launch_bounds__(kThreads) gmres_update_kernel(Layout L, const 
     x[i] = xi;
     r[i] = b[i];
   }
+}
+
+// x += z for the systems of the cycle (right preconditioning: z = M^-1 V y).
+__global__ void gmres_add_kernel(Layout L, const double2* __restrict__ Z, double2* __restrict__ X,
+                                 const GmresSystem* sys, const Flags* flags) {
+  if (flags->skip_all) return;
+  const int s = blockIdx.y;
+  if (!sys[s].ran || sys[s].col_end < 0) return;
+  const double2* z = Z + L.vec_off(s);
+  double2* x = X + L.x_off(s);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
+    const double2 zi = z[i], xi = x[i];
+    x[i] = make_double2(xi.x + zi.x, xi.y + zi.y);
+  }
+}
+
+// Z = v_col of the systems in the inner loop (right preconditioning: M^-1 v_col next).
+__global__ void gmres_gather_kernel(Layout L, const double2* __restrict__ V, int col, double2* __restrict__ Z,
+                                    const GmresSystem* sys, const Flags* flags) {
+  if (flags->skip_inner) return;
+  const int s = blockIdx.y;
+  if (!sys[s].active) return;
+  const double2* v = V + L.v_off(s, col);
+  double2* z = Z + L.vec_off(s);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.npad; i += gridDim.x * blockDim.x) z[i] = v[i];
 }
 
 // After r = b - A x: convergence (|r| <= atol), breakdown failure, SciPy's
@@ -452,6 +502,7 @@ __global__ void __launch_bounds__(kThreads) gmres_check_kernel(Layout L, const d
 struct GmresWork {
   double2* V;
   double2* W;
+  double2* Z;
   double2* R;
   double2* H;
   double2* Gs;
@@ -475,6 +526,7 @@ size_t carve_gmres(void* base, int n, int npad, int nrhs, int batch, int m, Gmre
   };
   const size_t oV = take(sizeof(double2) * nsys * (m + 1) * npad);
   const size_t oW = take(sizeof(double2) * nsys * npad);
+  const size_t oZ = take(sizeof(double2) * nsys * npad);
   const size_t oR = take(sizeof(double2) * nsys * npad);
   const size_t oH = take(sizeof(double2) * nsys * m * (m + 1));
   const size_t oGs = take(sizeof(double2) * nsys * m);
@@ -488,6 +540,7 @@ size_t carve_gmres(void* base, int n, int npad, int nrhs, int batch, int m, Gmre
     char* p = (char*)base;
     w->V = (double2*)(p + oV);
     w->W = (double2*)(p + oW);
+    w->Z = (double2*)(p + oZ);
     w->R = (double2*)(p + oR);
     w->H = (double2*)(p + oH);
     w->Gs = (double2*)(p + oGs);
@@ -537,6 +590,7 @@ extern "C" int bem_gmres_solve(const void* A_dev, int64_t lda, int64_t strideA, 
   BEM_CUDA_CHECK(cudaMemsetAsync(w.V, 0, sizeof(double2) * (size_t)nsys * (m + 1) * npad, s));
   BEM_CUDA_CHECK(cudaMemsetAsync(w.W, 0, sizeof(double2) * (size_t)nsys * npad, s));
   BEM_CUDA_CHECK(cudaMemsetAsync(w.R, 0, sizeof(double2) * (size_t)nsys * npad, s));
+  BEM_CUDA_CHECK(cudaMemsetAsync(w.Z, 0, sizeof(double2) * (size_t)nsys * npad, s));
   BEM_CUDA_CHECK(cudaMemsetAsync(w.flags, 0, sizeof(Flags), s));
   for (int b = 0; b < batch; ++b)
     BEM_CUDA_CHECK(cudaMemset2DAsync((double2*)X_dev + (size_t)b * strideB, ldb * sizeof(double2), 0,
@@ -547,28 +601,29 @@ extern "C" int bem_gmres_solve(const void* A_dev, int64_t lda, int64_t strideA, 
   bool converged = false;
   int cycle = 0;
   for (; cycle < max_cycles; ++cycle) {
-    // v0 = M^-1 r / |M^-1 r|
+    // v0 = r / |r|
     gmres_copy_kernel<<<dim3(ceil_div(n, 256), nsys), 256, 0, s>>>(L, w.R, w.W, w.sys, w.flags);
     ++launches;
-    if (precond_work_dev) {
-      int st = clu_solve_enqueue(precond_work_dev, npad, batch, w.W, npad, strideW, nrhs, err_dev, s,
-                                 &w.flags->skip_all);
-      if (st) return st;
-    }
     gmres_start_kernel<<<nsys, kThreads, 0, s>>>(L, w.W, w.V, w.S, w.sys, cycle == 0, w.flags);
     ++launches;
     for (int col = 0; col < m;) {
       const int group = std::min(kGroup, m - col);
       for (int g = 0; g < group; ++g, ++col) {
-        // w = M^-1 A v_col for all systems (one read of each A)
-        int st = zgemm_ts_enqueue(n, n, nrhs, 1.0, 0.0, A_dev, lda, strideA, w.V + (size_t)col * nrhs * npad, ldv,
-                                  strideV, 0.0, 0.0, w.W, npad, strideW, batch, w.ts, stream, &w.flags->skip_inner);
-        if (st) return st;
+        // w = A v_col, or w = A M^-1 v_col, for all systems (one read of each A)
+        int st;
         if (precond_work_dev) {
-          st = clu_solve_enqueue(precond_work_dev, npad, batch, w.W, npad, strideW, nrhs, err_dev, s,
+          gmres_gather_kernel<<<dim3(ceil_div(npad, 256), nsys), 256, 0, s>>>(L, w.V, col, w.Z, w.sys, w.flags);
+          ++launches;
+          st = clu_solve_enqueue(precond_work_dev, npad, batch, w.Z, npad, strideW, nrhs, err_dev, s,
                                  &w.flags->skip_inner);
           if (st) return st;
+          st = zgemm_ts_enqueue(n, n, nrhs, 1.0, 0.0, A_dev, lda, strideA, w.Z, npad, strideW, 0.0, 0.0, w.W, npad,
+                                strideW, batch, w.ts, stream, &w.flags->skip_inner);
+        } else {
+          st = zgemm_ts_enqueue(n, n, nrhs, 1.0, 0.0, A_dev, lda, strideA, w.V + (size_t)col * nrhs * npad, ldv,
+                                strideV, 0.0, 0.0, w.W, npad, strideW, batch, w.ts, stream, &w.flags->skip_inner);
         }
+        if (st) return st;
         gmres_arnoldi_kernel<<<nsys, kThreads, 0, s>>>(L, col, w.W, w.V, w.H, w.Gs, w.Gc, w.S, w.sys, w.flags);
         ++launches;
       }
@@ -580,8 +635,15 @@ extern "C" int bem_gmres_solve(const void* A_dev, int64_t lda, int64_t strideA, 
       }
     }
     gmres_update_kernel<<<nsys, kThreads, 0, s>>>(L, w.V, w.H, w.S, (const double2*)B_dev, (double2*)X_dev, w.R,
-                                                  w.sys, w.flags);
+                                                  precond_work_dev ? w.Z : nullptr, w.sys, w.flags);
     ++launches;
+    if (precond_work_dev) {  // x += M^-1 (V y)
+      int st = clu_solve_enqueue(precond_work_dev, npad, batch, w.Z, npad, strideW, nrhs, err_dev, s,
+                                 &w.flags->skip_all);
+      if (st) return st;
+      gmres_add_kernel<<<dim3(ceil_div(n, 256), nsys), 256, 0, s>>>(L, w.Z, (double2*)X_dev, w.sys, w.flags);
+      ++launches;
+    }
     // r = b - A x
     int st = zgemm_ts_enqueue(n, n, nrhs, -1.0, 0.0, A_dev, lda, strideA, X_dev, ldb, strideB, 1.0, 0.0, w.R, npad,
                               strideW, batch, w.ts, stream, &w.flags->skip_all);

@@ -810,9 +810,14 @@ extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK,
       launches += 3;
     }
     enqueued += group;
+    const double before = host_state[0];
     BEM_CUDA_CHECK(cudaMemcpyAsync(host_state, state, sizeof(host_state), cudaMemcpyDeviceToHost, s));
     BEM_CUDA_CHECK(cudaStreamSynchronize(s));
     if (host_state[0] <= tol && host_state[1] > 0.0) break;
+    // A contracting iteration gains far more than a factor 2 per group; one
+    // that does not (the float32 factors too far from K, e.g. near an
+    // irregular frequency) stops here and reports non-convergence.
+    if (enqueued > group && !(host_state[0] < 0.5 * before)) break;
   }
   count_launches(launches);
   *iters_out = (int)host_state[1];
@@ -821,7 +826,7 @@ extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK,
   if (!(host_state[0] <= tol)) {
     char msg[160];
     std::snprintf(msg, sizeof(msg), "iterative refinement stopped at relative residual %.3e after %d iterations",
-                  host_state[0], max_iter);
+                  host_state[0], (int)host_state[1]);
     return set_error(BEM_ERR_NOT_CONVERGED, msg);
   }
   return BEM_OK;

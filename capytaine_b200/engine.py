@@ -64,6 +64,18 @@ class FrequencyResults:
                     excitation=self.excitation)
 
 
+def _allocator(device, alloc):
+    """(shape, dtype, zero) -> tensor: torch's allocator, or the caller's
+    (views of a preallocated arena, see serving.DeviceArena)."""
+    if alloc is not None:
+        return alloc
+    import torch
+
+    def torch_alloc(shape, dtype, zero=False):
+        return (torch.zeros if zero else torch.empty)(shape, dtype=dtype, device=device)
+    return torch_alloc
+
+
 class _Factors:
     """Device storage of the matrices of `batch` frequency-solves of one mesh
     (n panels): S, K and the factorisation of K.
@@ -72,30 +84,29 @@ class _Factors:
     mixed: K unpadded (float64 residuals) and the float32 LU workspace padded
            to a multiple of 128."""
 
-    def __init__(self, n, batch, device, precision):
+    def __init__(self, n, batch, device, precision, alloc=None):
         import torch
         self.n, self.batch, self.precision = n, batch, precision
         lib = _lib.load()
-        c128 = dict(dtype=torch.complex128, device=device)
-        self.S = torch.empty((batch, n * n), **c128)
-        self.info = torch.zeros(batch, dtype=torch.int32, device=device)
+        mk = _allocator(device, alloc)
+        self.S = mk((batch, n * n), torch.complex128)
+        self.info = mk((batch,), torch.int32, True)
         if precision == "fp64":
             self.npad = padded_size(n)
-            self.K = torch.empty((batch, self.npad * self.npad), **c128)
+            self.K = mk((batch, self.npad * self.npad), torch.complex128)
             self.ldk = self.npad
             self.strideK = self.npad * self.npad
-            self.lu_work = torch.empty(int(lib.bem_zlu_workspace_bytes(self.npad, batch)), dtype=torch.uint8,
-                                       device=device)
+            self.lu_work = mk((int(lib.bem_zlu_workspace_bytes(self.npad, batch)),), torch.uint8)
             self.lu_work_ptr = self.lu_work.data_ptr()
         else:
             self.npad = int(math.ceil(n / 128) * 128)
-            self.K = torch.empty((batch, n * n), **c128)
+            self.K = mk((batch, n * n), torch.complex128)
             self.ldk = n
             self.strideK = n * n
             nbytes = int(lib.bem_clu_workspace_bytes(self.npad, batch))
-            self.lu_work = torch.empty(nbytes + 1024, dtype=torch.uint8, device=device)
+            self.lu_work = mk((nbytes + 1024,), torch.uint8)
             self.lu_work_ptr = (self.lu_work.data_ptr() + 1023) // 1024 * 1024  # 1024-byte aligned start
-        self.piv = torch.empty((batch, self.npad), dtype=torch.int32, device=device)
+        self.piv = mk((batch, self.npad), torch.int32)
 
     @staticmethod
     def estimate_bytes(n, batch, precision):
@@ -116,19 +127,19 @@ class _Rhs:
     """Right-hand sides, solutions, potentials and the small work buffers of
     `batch` frequency-solves with nrhs columns each (padded rows zero)."""
 
-    def __init__(self, n, npad, batch, nrhs, device, precision):
+    def __init__(self, n, npad, batch, nrhs, device, precision, alloc=None):
         import torch
         self.n, self.npad, self.batch, self.nrhs, self.precision = n, npad, batch, nrhs, precision
         lib = _lib.load()
-        c128 = dict(dtype=torch.complex128, device=device)
-        self.B = torch.zeros((batch, npad * nrhs), **c128)
-        self.X = torch.zeros((batch, npad * nrhs), **c128)
-        self.R = torch.zeros((batch, npad * nrhs), **c128)
-        self.phi = torch.empty((batch, n * nrhs), **c128)
-        self.norms = torch.zeros(2 * batch * nrhs + 2, dtype=torch.float64, device=device)
-        self.ts_work = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch)), dtype=torch.uint8,
-                                   device=device)
-        self.flags = torch.zeros(2, dtype=torch.int32, device=device)  # [err, nan]
+        mk = _allocator(device, alloc)
+        self._mk = mk
+        self.B = mk((batch, npad * nrhs), torch.complex128, True)
+        self.X = mk((batch, npad * nrhs), torch.complex128, True)
+        self.R = mk((batch, npad * nrhs), torch.complex128, True)
+        self.phi = mk((batch, n * nrhs), torch.complex128)
+        self.norms = mk((2 * batch * nrhs + 2,), torch.float64, True)
+        self.ts_work = mk((int(lib.bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch)),), torch.uint8)
+        self.flags = mk((2,), torch.int32, True)  # [err, nan]
         self._gmres = None
 
     @property
@@ -146,7 +157,7 @@ class _Rhs:
             nbytes = int(_lib.load().bem_gmres_workspace_bytes(self.n, self.npad, self.nrhs, self.batch, restart))
             if nbytes < 0:
                 raise ValueError("bad GMRES workspace shape")
-            buf = torch.empty(nbytes + 256, dtype=torch.uint8, device=self.B.device)
+            buf = self._mk((nbytes + 256,), torch.uint8)
             self._gmres = (restart, buf, (buf.data_ptr() + 255) // 256 * 256)
         return self._gmres[2]
 
@@ -194,8 +205,10 @@ class B200Engine:
     "fp64" only), or a callable ``(A, b) -> x`` used by ``linear_solver``.
 
     refinement (precision "mixed"): "classical" (x += (LU)^-1 r) or "gmres"
-    (GMRES on the float64 K left-preconditioned by the float32 LU), both to
-    refine_tol relative residual.
+    (GMRES on the float64 K right-preconditioned by the float32 LU), both to
+    refine_tol relative residual.  When the classical iteration stops
+    contracting (K nearly singular, e.g. near an irregular frequency) the
+    solve continues with the preconditioned GMRES (stats["escalated_to_gmres"]).
     """
 
     def __init__(self, *, green_function: Optional[Delhommeau] = None, precision: str = "fp64",
@@ -217,6 +230,7 @@ class B200Engine:
         self.refinement = refinement
         self.gmres_restart = int(gmres_restart)
         self.gmres_maxiter = gmres_maxiter
+        self.gmres_escalation_cycles = 10
         # float32 wave terms perturb the O(k)-small imaginary parts that carry the
         # radiation damping at low frequency beyond 1e-5: float64 assembly by default.
         self.assembly_precision = assembly_precision
@@ -393,6 +407,16 @@ class B200Engine:
                                               _vp(r.B), _vp(r.X), _vp(r.R), npad, npad * nrhs, nrhs, self.refine_tol,
                                               self.refine_max_iter, _vp(r.ts_work), _vp(r.norms), _vp(r.err),
                                               ctypes.byref(iters), ctypes.byref(resid), stream)
+                if status == _lib.BEM_ERR_NOT_CONVERGED:
+                    # x += (LU)^-1 r does not contract (K close to singular, e.g. near an
+                    # irregular frequency): GMRES on K, preconditioned by the same float32
+                    # factors, from x = 0 to the same tolerance.
+                    stats["escalated_to_gmres"] = stats.get("escalated_to_gmres", 0) + 1
+                    status = lib.bem_gmres_solve(_vp(f.K), n, n * n, n, npad, nb, _vp(r.B), _vp(r.X), npad,
+                                                 npad * nrhs, nrhs, 0.0, self.refine_tol, self.gmres_restart,
+                                                 max(1, self.gmres_escalation_cycles), _vp(f.lu_work_ptr),
+                                                 _vp(r.gmres_work(self.gmres_restart)), _vp(r.err),
+                                                 ctypes.byref(iters), ctypes.byref(resid), stream)
             stats["refine_iters"] = max(stats.get("refine_iters", 0), iters.value)
             stats["refine_residual"] = max(stats.get("refine_residual", 0.0), resid.value)
             if status == _lib.BEM_ERR_NOT_CONVERGED:

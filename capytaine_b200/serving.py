@@ -19,6 +19,10 @@ Scheduling
   is resident; resident factors not in use are evicted (least recently used)
   to make room.  A request that alone exceeds the budget fails with
   MemoryError.
+* Device memory: one arena of ``memory_budget`` bytes is allocated when the
+  server starts and every buffer of a request is a view of it, so serving
+  never calls the CUDA allocator (whose frees synchronise the whole device)
+  between requests.
 * Residency: the factors of every solved (mesh, omega) stay on the device
   (with S and K) until evicted; a later request for the same mesh and omega
   only solves its right-hand sides with them.  Device meshes and the
@@ -43,6 +47,88 @@ from . import _lib
 from .engine import B200Engine, _Factors, _Rhs
 
 LOG = logging.getLogger(__name__)
+
+
+class ArenaFull(MemoryError):
+    """No free block of the requested size in the arena (retry after frees)."""
+
+
+class DeviceArena:
+    """One device allocation carved into `granule`-aligned blocks, first fit
+    with coalescing of free neighbours.  ``allocator()`` returns an
+    (alloc, release) pair: alloc(shape, dtype, zero=False) hands out tensor
+    views (zeroed on the caller's current stream when asked), release() frees
+    every block handed out by that pair."""
+
+    def __init__(self, nbytes: int, device, granule: int = 1 << 16):
+        import torch
+        self.granule = int(granule)
+        self.size = int(nbytes) // self.granule * self.granule
+        self.buf = torch.empty(self.size, dtype=torch.uint8, device=device)
+        self._free = [(0, self.size)]  # (offset, size), sorted by offset
+        self._lock = threading.Lock()
+        self.used = 0
+        self.peak = 0
+
+    def allocate(self, nbytes: int) -> int:
+        size = max(self.granule, -(-int(nbytes) // self.granule) * self.granule)
+        with self._lock:
+            for i, (off, sz) in enumerate(self._free):
+                if sz >= size:
+                    if sz == size:
+                        self._free.pop(i)
+                    else:
+                        self._free[i] = (off + size, sz - size)
+                    self.used += size
+                    self.peak = max(self.peak, self.used)
+                    return off
+        raise ArenaFull(f"no free block of {size} bytes in the device arena")
+
+    def release(self, off: int, nbytes: int):
+        size = max(self.granule, -(-int(nbytes) // self.granule) * self.granule)
+        with self._lock:
+            self.used -= size
+            fl = self._free
+            lo, hi = 0, len(fl)
+            while lo < hi:  # insertion point by offset
+                mid = (lo + hi) // 2
+                if fl[mid][0] < off:
+                    lo = mid + 1
+                else:
+                    hi = mid
+            fl.insert(lo, (off, size))
+            if lo + 1 < len(fl) and fl[lo][0] + fl[lo][1] == fl[lo + 1][0]:
+                fl[lo] = (fl[lo][0], fl[lo][1] + fl[lo + 1][1])
+                fl.pop(lo + 1)
+            if lo > 0 and fl[lo - 1][0] + fl[lo - 1][1] == fl[lo][0]:
+                fl[lo - 1] = (fl[lo - 1][0], fl[lo - 1][1] + fl[lo][1])
+                fl.pop(lo)
+
+    @property
+    def largest_free(self) -> int:
+        with self._lock:
+            return max((sz for _, sz in self._free), default=0)
+
+    def allocator(self):
+        import torch
+        blocks = []
+
+        def alloc(shape, dtype, zero=False):
+            count = 1
+            for d in shape:
+                count *= int(d)
+            nbytes = count * torch.empty((), dtype=dtype).element_size()
+            off = self.allocate(nbytes)
+            blocks.append((off, nbytes))
+            t = self.buf[off:off + nbytes].view(dtype).view(tuple(shape))
+            if zero:
+                t.zero_()
+            return t
+
+        def release():
+            while blocks:
+                self.release(*blocks.pop())
+        return alloc, release
 
 
 @dataclass
@@ -89,9 +175,10 @@ class _Request:
 class _Resident:
     """S, K and the factors of one (mesh, omega) kept on the device between requests."""
 
-    def __init__(self, f: _Factors, nbytes: int):
+    def __init__(self, f: _Factors, nbytes: int, release):
         self.f = f
         self.nbytes = nbytes
+        self.release = release  # frees the arena blocks of f
         self.users = 0
         self.lock = threading.Lock()
 
@@ -119,6 +206,7 @@ class SolveServer:
             memory_budget = int(0.6 * total)
         self.memory_budget = int(memory_budget)
         self.keep_factors = bool(keep_factors)
+        self._arena = DeviceArena(self.memory_budget, self.device)
         self._cv = threading.Condition()
         self._pending: Deque[_Request] = deque()
         self._resident: "OrderedDict[tuple, _Resident]" = OrderedDict()
@@ -171,6 +259,8 @@ class SolveServer:
         if wait:
             for t in self._workers:
                 t.join()
+            self.release_resident()
+            self._arena = None  # the device memory goes back to torch's allocator
 
     def release_resident(self):
         """Drop every resident factorisation not in use."""
@@ -196,11 +286,16 @@ class SolveServer:
         blk = 128 if prec == "mixed" else 64
         npad = -(-req.n // blk) * blk
         f_bytes = 0 if reuse else _Factors.estimate_bytes(req.n, 1, prec)
-        return f_bytes + _Rhs.estimate_bytes(req.n, npad, 1, req.nrhs)
+        g_bytes = 0
+        if prec == "mixed":
+            g_bytes = int(_lib.load().bem_gmres_workspace_bytes(req.n, npad, req.nrhs, 1,
+                                                                self.engine.gmres_restart)) + 256
+        return f_bytes + g_bytes + _Rhs.estimate_bytes(req.n, npad, 1, req.nrhs)
 
     def _drop_locked(self, key):
         e = self._resident.pop(key)
         self._resident_bytes -= e.nbytes
+        e.release()
         self.counters["evicted"] += 1
 
     def _make_room_locked(self, need: int) -> bool:
@@ -292,36 +387,79 @@ class SolveServer:
                     self._inflight -= 1
                     if res is not None:
                         res.users -= 1
-                    if keep is not None and req.key not in self._resident and self._make_room_locked(keep.nbytes):
-                        self._resident[req.key] = _Resident(keep, keep.nbytes)
-                        self._resident_bytes += keep.nbytes
+                    if keep is not None:
+                        f, release = keep
+                        if req.key not in self._resident and self._make_room_locked(f.nbytes):
+                            self._resident[req.key] = _Resident(f, f.nbytes, release)
+                            self._resident_bytes += f.nbytes
+                        else:
+                            release()
                     if req.future.exception() is None:
                         self.counters["completed"] += 1
                     else:
                         self.counters["failed"] += 1
                     self._cv.notify_all()
 
+    def _buffers(self, build):
+        """build(alloc) with arena views, all or nothing: when the arena has no
+        block large enough, evict an unused resident factorisation, or wait
+        for a running request to free its buffers, and retry."""
+        while True:
+            arena = self._arena
+            if arena is None:
+                raise RuntimeError("server is shut down")
+            alloc, release = arena.allocator()
+            try:
+                return build(alloc), release
+            except ArenaFull:
+                release()
+                with self._cv:
+                    victim = next((k for k, e in self._resident.items() if e.users == 0), None)
+                    if victim is not None:
+                        self._drop_locked(victim)
+                    else:
+                        self._cv.wait(timeout=0.05)
+
     def _run(self, req: _Request, res: Optional[_Resident], admitted: float):
         """Enqueue the request's work on the current (slot) stream and wait
-        for it; returns the factors to keep resident, if any."""
+        for it; returns (factors, release) to keep resident, if any."""
         eng = self.engine
         body = req.body
         mesh = body.mesh_including_lid
         om = np.array([req.omega])
         stats: Dict[str, float] = {}
+        # GMRES workspace up front: the refined solve may escalate to it
+        gmres = eng.precision == "mixed"
+
+        def rhs(alloc, n, npad):
+            r = _Rhs(n, npad, 1, req.nrhs, self.device, eng.precision, alloc=alloc)
+            if gmres:
+                r.gmres_work(eng.gmres_restart)
+            return r
         if res is not None:
             with res.lock:  # repeats of one entry take turns on its buffers
-                r = _Rhs(res.f.n, res.f.npad, 1, req.nrhs, self.device, eng.precision)
-                F, FK = eng.solve_stage(res.f, r, body, om, req.heads, rho=req.rho, g=req.g, stats=stats)
+                r, release_r = self._buffers(lambda a: rhs(a, res.f.n, res.f.npad))
+                try:
+                    F, FK = eng.solve_stage(res.f, r, body, om, req.heads, rho=req.rho, g=req.g, stats=stats)
+                finally:
+                    release_r()
             keep = None
         else:
-            f = _Factors(req.n, 1, self.device, eng.precision)
-            r = _Rhs(f.n, f.npad, 1, req.nrhs, self.device, eng.precision)
-            r.flags.zero_()
-            eng.assemble_stage(f, mesh, om ** 2 / req.g, nan_flag=r.nan, reuse_rankine=False)
-            eng.factor_stage(f, 1, r.err)
-            F, FK = eng.solve_stage(f, r, body, om, req.heads, rho=req.rho, g=req.g, stats=stats)
-            keep = f if self.keep_factors else None
+            f, release = self._buffers(lambda a: _Factors(req.n, 1, self.device, eng.precision, alloc=a))
+            try:
+                r, release_r = self._buffers(lambda a: rhs(a, f.n, f.npad))
+                try:
+                    eng.assemble_stage(f, mesh, om ** 2 / req.g, nan_flag=r.nan, reuse_rankine=False)
+                    eng.factor_stage(f, 1, r.err)
+                    F, FK = eng.solve_stage(f, r, body, om, req.heads, rho=req.rho, g=req.g, stats=stats)
+                finally:
+                    release_r()
+            except BaseException:
+                release()
+                raise
+            keep = (f, release) if self.keep_factors else None  # S, K and factors stay with `release`
+            if keep is None:
+                release()
         finished = time.perf_counter()
         ndof = len(body.dofs)
         w = req.omega

@@ -262,7 +262,9 @@ int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv_dev, void*
  * doubles.  The convergence test runs on the device: iterations are enqueued
  * in groups of four and those after convergence return at once, so the stream
  * is synchronised once per group.  Returns BEM_ERR_NOT_CONVERGED (X holds the
- * last iterate) when max_iter is reached.  Replaces the lu_solve of
+ * last iterate) when max_iter is reached or when a group of iterations does
+ * not halve the residual (the float32 factors are too far from K for the
+ * iteration to contract).  Replaces the lu_solve of
  * tools/block_circulant_matrices.py:382-385. */
 int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch, void* work_dev,
                      const int* piv_dev, const void* B_dev, void* X_dev, void* R_dev, int64_t ldb, int64_t strideB,
@@ -281,9 +283,10 @@ int64_t bem_gmres_workspace_bytes(int n, int npad, int nrhs, int batch, int rest
  * adaptive inner tolerance, as scipy.sparse.linalg.gmres does.  restart <= 64
  * (capytaine/SciPy: 20), at most max_cycles restart cycles.
  * precond_work_dev: NULL for plain GMRES, or the factorisation of
- * bem_clu_factor (npad multiple of 128, err_dev required) used as the left
- * preconditioner M^-1 = (LU)^-1 with float32 factors and float64 products:
- * GMRES-based iterative refinement of the mixed-precision LU.  X (ldb,
+ * bem_clu_factor (npad multiple of 128, err_dev required) used as the right
+ * preconditioner M^-1 = (LU)^-1 (A M^-1 u = b, x = M^-1 u) with float32
+ * factors and float64 products: GMRES-based iterative refinement of the
+ * mixed-precision LU.  X (ldb,
  * strideB): rows < n written.  work_dev: bem_gmres_workspace_bytes, 256-byte
  * aligned.  iters_out: largest number of inner iterations over the systems;
  * resid_out: largest |b - A x| / |b|.  Synchronises the stream once per group

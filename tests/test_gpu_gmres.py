@@ -156,3 +156,44 @@ def test_engines_with_gmres_against_oracle(oracle_mod, default_oracle_gf, tmp_pa
     assert res.stats["refine_residual"] <= 1e-10
     errs = coefficient_errors(res, ref_lu, body.dofs)
     assert max(errs.values()) < 1e-7, errs
+
+
+def test_refinement_stops_and_gmres_recovers_near_a_singular_matrix():
+    """K with one eigenvalue 1e-7 (what an irregular frequency does to the BEM
+    system): the float32 LU is wrong in that direction, the classical iteration
+    x += (LU)^-1 r no longer contracts and stops early as non-converged; GMRES
+    right-preconditioned by the same factors removes the outlier in a few
+    iterations.  The tolerance is 1e-8: with |x| ~ 1e7 |b| the float64 residual
+    b - K x cannot be resolved much below ~1e-10 |b|."""
+    import torch
+    rng = np.random.default_rng(21)
+    n, nrhs = 256, 3
+    npad = 256
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    lam = rng.uniform(0.5, 1.5, n) * np.exp(1j * rng.uniform(-0.3, 0.3, n))
+    lam[0] = 1e-7 * (1 + 1j)
+    A = (Q * lam) @ Q.conj().T
+    b = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
+    lib = _lib.load()
+    K = torch.as_tensor(np.ascontiguousarray(A.T)).cuda().reshape(1, -1)
+    work = torch.empty(int(lib.bem_clu_workspace_bytes(npad, 1)) + 1024, dtype=torch.uint8, device="cuda")
+    wptr = (work.data_ptr() + 1023) // 1024 * 1024
+    piv = torch.empty((1, npad), dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.check(lib.bem_clu_factor(_vp(K), n, n * n, n, npad, 1, _vp(piv), _vp(info), _vp(wptr), _vp(err),
+                                  _lib.stream_ptr()))
+    B = torch.zeros((1, nrhs, npad), dtype=torch.complex128, device="cuda")
+    B[0, :, :n] = torch.as_tensor(b.T)
+    X, R = torch.zeros_like(B), torch.zeros_like(B)
+    ts = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, nrhs, 1)), dtype=torch.uint8, device="cuda")
+    norms = torch.zeros(2 * nrhs + 2, dtype=torch.float64, device="cuda")
+    iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
+    st = lib.bem_refine_solve(_vp(K), n, n * n, n, npad, 1, _vp(wptr), _vp(piv), _vp(B), _vp(X), _vp(R), npad,
+                              npad * nrhs, nrhs, 1e-8, 30, _vp(ts), _vp(norms), _vp(err), ctypes.byref(iters),
+                              ctypes.byref(resid), _lib.stream_ptr())
+    assert st == _lib.BEM_ERR_NOT_CONVERGED and iters.value < 30, (st, iters.value, resid.value)
+    xs, st, it, res, *_ = _gmres_device([A], [b], atol=0.0, rtol=1e-8, precond=_vp(wptr), npad=npad)
+    assert st == _lib.BEM_OK and res <= 1e-8 and it <= 20, (st, it, res, _lib.load().bem_last_error())
+    for c in range(nrhs):
+        assert np.linalg.norm(b[:, c] - A @ xs[0][:, c]) <= 2e-8 * np.linalg.norm(b[:, c])

@@ -18,6 +18,7 @@ class _StandInEngine:
     """Engine stages that only record calls: F depends on the mesh and omega."""
     precision = "mixed"
     device = "cpu"
+    gmres_restart = 20
 
     def __init__(self, delay=0.0):
         self.delay = delay
@@ -59,9 +60,30 @@ def _server(engine, **kw):
     return SolveServer(engine, **kw)
 
 
+def test_device_arena_first_fit_and_coalescing():
+    import torch
+    from capytaine_b200.serving import ArenaFull, DeviceArena
+    ar = DeviceArena(1 << 20, "cpu", granule=1 << 12)
+    a1, r1 = ar.allocator()
+    a2, r2 = ar.allocator()
+    x = a1((100,), torch.complex128, True)
+    y = a2((1000,), torch.float32)
+    z = a1((10, 10), torch.int32, True)
+    assert x.dtype == torch.complex128 and float(x.abs().sum()) == 0.0 and z.shape == (10, 10)
+    base = ar.buf.data_ptr()
+    assert (x.data_ptr() - base) % 4096 == 0 and (y.data_ptr() - base) % 4096 == 0
+    assert ar.used == 3 * 4096
+    with pytest.raises(ArenaFull):
+        a2(((1 << 20),), torch.uint8)
+    r1()
+    assert ar.used == 4096 and ar.largest_free == (1 << 20) - 2 * 4096
+    r2()
+    assert ar.used == 0 and ar.largest_free == 1 << 20 and ar.peak == 3 * 4096
+
+
 def test_scheduler_reuses_resident_factors_and_counts():
     eng = _StandInEngine()
-    with _server(eng, slots=2, memory_budget=1 << 30) as srv:
+    with _server(eng, slots=2, memory_budget=1 << 28) as srv:
         b = _body(4)
         r1 = srv.solve(b, 1.0, timeout=60)
         r2 = srv.solve(b, 1.0, timeout=60)
@@ -92,7 +114,7 @@ def test_scheduler_keeps_the_memory_budget_and_evicts():
 
 def test_scheduler_overlaps_requests_in_slots():
     eng = _StandInEngine(delay=0.02)
-    with _server(eng, slots=4, memory_budget=1 << 32) as srv:
+    with _server(eng, slots=4, memory_budget=1 << 28) as srv:
         futs = [srv.submit(_body(4 + (i % 3)), 0.3 + 0.1 * i) for i in range(8)]
         for f in futs:
             f.result(timeout=60)
@@ -115,7 +137,7 @@ def test_a_failing_slot_fails_the_queue_instead_of_hanging():
         def _slot_stream(self):
             raise ValueError("no device")
     with pytest.raises(RuntimeError, match="slot failed"):
-        srv = Broken(_StandInEngine(), slots=1, memory_budget=1 << 30)
+        srv = Broken(_StandInEngine(), slots=1, memory_budget=1 << 28)
         try:
             srv.submit(_body(4), 1.0).result(timeout=30)
         finally:
@@ -124,7 +146,7 @@ def test_a_failing_slot_fails_the_queue_instead_of_hanging():
 
 def test_scheduler_admits_in_arrival_order():
     eng = _StandInEngine(delay=0.005)
-    with _server(eng, slots=1, memory_budget=1 << 32) as srv:
+    with _server(eng, slots=1, memory_budget=1 << 28) as srv:
         bodies = [_body(4 + i) for i in range(5)]
         futs = [srv.submit(b, 1.0) for b in bodies]
         order = [f.result(timeout=60).request_id for f in futs]
@@ -151,9 +173,9 @@ def test_results_same_alone_and_in_the_mix(oracle_mod, default_oracle_gf, tmp_pa
     ]
     reqs = [(b, w) for w in (0.4, 1.3, 2.6) for b in bodies]
     eng = B200Engine(green_function=gf, precision="mixed")
-    with SolveServer(eng, slots=1) as alone:
+    with SolveServer(eng, slots=1, memory_budget=4 << 30) as alone:
         solo = [alone.solve(b, w, timeout=300) for b, w in reqs]
-    with SolveServer(eng, slots=4) as mix:
+    with SolveServer(eng, slots=4, memory_budget=4 << 30) as mix:
         futs = [mix.submit(b, w) for b, w in reqs + reqs[::-1]]
         got = [f.result(timeout=600) for f in futs]
         assert mix.counters["max_inflight_requests"] >= 2
@@ -183,7 +205,7 @@ def test_server_against_the_oracle(oracle_mod, default_oracle_gf, tmp_path):
     mesh = mesh_sphere(radius=1.0, resolution=(12, 24)).immersed_part()
     body = FloatingBody(mesh, rigid_body_dofs())
     omegas = [0.5, 2.0]
-    with SolveServer(B200Engine(green_function=gf, precision="mixed"), slots=2) as srv:
+    with SolveServer(B200Engine(green_function=gf, precision="mixed"), slots=2, memory_budget=2 << 30) as srv:
         res = [f.result(timeout=600) for f in [srv.submit(body, w) for w in omegas]]
     for w, r in zip(omegas, res):
         ref = oracle_mod.solve_frequency(default_oracle_gf, mesh, oracle_mod.rigid_body_dofs(), w)
