@@ -158,6 +158,84 @@ def run_serving(engine, bodies, *, rate, n_requests, seed, slots, repeat_frac=0.
                         "(mesh, omega) pairs"}
 
 
+def cylinder_array_body():
+    """3 x 3 vertical cylinders (radius 5 m, draft 20 m, spacing 30 m), each
+    with rigid-body dofs about its own axis at the free surface and an interior
+    lid for the removal of irregular frequencies: about 20000 panels."""
+    from capytaine_b200.bodies import FloatingBody, join_bodies, rigid_body_dofs
+    from capytaine_b200.meshes import mesh_vertical_cylinder
+    hull0 = mesh_vertical_cylinder(length=40.0, radius=5.0, resolution=(8, 52, 64)).immersed_part()
+    lid0 = hull0.generate_lid()
+    bodies = []
+    for i in range(3):
+        for j in range(3):
+            x, y = 30.0 * (i - 1), 30.0 * (j - 1)
+            bodies.append(FloatingBody(hull0.translated((x, y, 0.0)), rigid_body_dofs(rotation_center=(x, y, 0.0)),
+                                       lid_mesh=lid0.translated((x, y, 0.0)), name=f"cyl{3 * i + j}"))
+    return join_bodies(*bodies, name="array3x3")
+
+
+def run_array(args):
+    """--workload array: frequency-solves/s of the 3 x 3 cylinder array (54
+    dofs + diffraction heading 0, omega in linspace(0.1, 2, 40)), the refined
+    mixed engine against the float64 GMRES engine (SciPy's settings), both on
+    the device; coefficients of the two compared."""
+    import torch
+    from capytaine_b200.engine import B200Engine
+    from capytaine_b200.green_function import Delhommeau
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    body = cylinder_array_body()
+    n = body.mesh_including_lid.nb_faces
+    omegas = np.linspace(0.1, 2.0, 40)[::max(1, 40 // args.array_frequencies)][:args.array_frequencies]
+    gf = Delhommeau(tabulation_cache_dir=None)
+    out = {}
+    results = {}
+    for name, eng in (("mixed", B200Engine(green_function=gf, precision="mixed", max_batch=args.array_batch)),
+                      ("gmres_fp64", B200Engine(green_function=gf, precision="fp64", linear_solver="gmres",
+                                                max_batch=args.array_batch))):
+        eng.solve_frequencies(body, omegas[:1])  # warm-up
+        gf.clear_rankine_cache()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = eng.solve_frequencies(body, omegas)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        results[name] = res
+        out[name] = {"value": len(omegas) / (ms * 1e-3), "unit": UNIT, "ms_per_frequency": ms / len(omegas),
+                     "stats": {k: v for k, v in res.stats.items() if not k.endswith("_ms")}}
+        del eng
+        torch.cuda.empty_cache()
+    # float64 LU (DMMA) reference at the lowest and a middle frequency
+    ref_omegas = [float(omegas[0]), float(omegas[len(omegas) // 2])]
+    ref = B200Engine(green_function=gf, precision="fp64", max_batch=1).solve_frequencies(body, ref_omegas)
+    torch.cuda.empty_cache()
+    idx = [0, len(omegas) // 2]
+
+    def rel(a, b):
+        floor = 1e-3 * np.abs(b).max(axis=tuple(range(1, b.ndim)), keepdims=True)
+        return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
+    diff = {}
+    for name in ("mixed", "gmres_fp64"):
+        diff[name] = {c: rel(getattr(results[name], c)[idx], getattr(ref, c))
+                      for c in ("added_mass", "radiation_damping", "excitation")}
+    line = {"metric": "freq solves/sec at N=20000 (3x3 cylinder array with lids), refined-mixed vs complex128 GMRES",
+            "value": out["mixed"]["value"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "dtype": "c128 (assembly, residuals) / f32-tf32 (LU)", "data": "synthetic",
+            "config": {"workload": "3x3 vertical cylinders r=5 m, draft 20 m, spacing 30 m, interior lids, "
+                                   "9x6 dofs + diffraction heading 0, omega linspace(0.1, 2, 40)",
+                       "nb_panels": int(n), "nb_lid_panels": int(body.lid_mesh.nb_faces),
+                       "frequencies": len(omegas), "batch": args.array_batch},
+            "mixed": out["mixed"], "gmres_fp64": out["gmres_fp64"],
+            "mixed_over_gmres": out["mixed"]["value"] / out["gmres_fp64"]["value"],
+            "max_rel_err_vs_fp64_lu": diff, "reference_omegas": ref_omegas,
+            "note": "errors against the float64 LU engine at two frequencies; GMRES stops at SciPy's tolerance "
+                    "(|r| <= max(1e-6, 1e-5 |b|)), the mixed engine refines to 1e-10"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------------------
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
@@ -407,11 +485,17 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=1000,
                     help="requests of the serving run (Poisson arrivals); 0 skips it")
     ap.add_argument("--arrival-rate", type=float, default=200.0)
-    ap.add_argument("--slots", type=int, default=6)
+    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--workload", default="barge", choices=["barge", "array"],
+                    help="array: the 3x3 cylinder array with lids (20000 panels), mixed vs float64 GMRES")
+    ap.add_argument("--array-frequencies", type=int, default=40)
+    ap.add_argument("--array-batch", type=int, default=4)
     args = ap.parse_args()
     args.world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "array":
+        return run_array(args)
 
     import torch
     rank = int(os.environ.get("RANK", "0"))

@@ -34,6 +34,21 @@ class RotationDof:
         return np.cross(np.asarray(self.direction, float), points - np.asarray(self.rotation_center, float))
 
 
+@dataclass(frozen=True, eq=False)
+class DofOnSubmesh:
+    """A dof that is zero everywhere except on some faces, where another dof
+    defines the motion (capytaine bodies/dofs.py:100-127): the dofs of one body
+    inside a joined multibody.  `faces`: boolean mask over the faces of the
+    joined hull, whose face centres are the points the motion is evaluated at."""
+    dof: object
+    faces: np.ndarray
+
+    def evaluate_motion(self, points: np.ndarray) -> np.ndarray:
+        motion = np.zeros((points.shape[0], 3))
+        motion[self.faces, :] = self.dof.evaluate_motion(points[self.faces, :])
+        return motion
+
+
 def rigid_body_dofs(only=None, rotation_center=(0.0, 0.0, 0.0)) -> Dict[str, object]:
     """Surge, Sway, Heave, Roll, Pitch, Yaw (capytaine bodies/dofs.py:139-172)."""
     dofs = {
@@ -58,6 +73,9 @@ class FloatingBody:
         self.lid_mesh = lid_mesh
         self.dofs = dict(dofs) if dofs is not None else {}
         self.name = name or (mesh.name if mesh.name else "body")
+
+    def __add__(self, other: "FloatingBody") -> "FloatingBody":
+        return join_bodies(self, other)
 
     @property
     def mesh_including_lid(self) -> Mesh:
@@ -98,3 +116,34 @@ class FloatingBody:
         """Host version of bodies.py:238-250 on hull pressures."""
         w = self.pressure_weights()[:, : self.mesh.nb_faces]
         return {name: complex(np.sum(pressure * w[d])) for d, name in enumerate(self.dofs)}
+
+
+def join_bodies(*bodies, name: Optional[str] = None) -> "FloatingBody":
+    """Several bodies as one (capytaine bodies/multibodies.py:34-122): the
+    hull meshes joined in order, each dof restricted to the faces of its body
+    and named "<body name>__<dof name>" (kept as is when it already holds
+    "__"), the lids joined after all hulls."""
+    names = [b.name for b in bodies]
+    if len(set(names)) < len(names):
+        raise ValueError(f"In Multibody, all component bodies must have a distinct name.\nGot: {names}")
+    counts = [b.mesh.nb_faces for b in bodies]
+    total = sum(counts)
+    hull = Mesh(np.concatenate([b.mesh.vertices for b in bodies]),
+                [[i + off for i in f] for b, off in zip(bodies, np.cumsum([0] + [b.mesh.nb_vertices
+                                                                               for b in bodies[:-1]]))
+                 for f in b.mesh._faces], name=name, clean=False)
+    dofs = {}
+    start = 0
+    for b, cnt in zip(bodies, counts):
+        mask = np.zeros(total, dtype=bool)
+        mask[start:start + cnt] = True
+        start += cnt
+        for dname, dof in b.dofs.items():
+            dofs[dname if "__" in dname else f"{b.name}__{dname}"] = DofOnSubmesh(dof, mask)
+    lids = [b.lid_mesh for b in bodies if b.lid_mesh is not None and b.lid_mesh.nb_faces > 0]
+    lid = None
+    if lids:
+        lid = Mesh(np.concatenate([m.vertices for m in lids]),
+                   [[i + off for i in f] for m, off in zip(lids, np.cumsum([0] + [m.nb_vertices for m in lids[:-1]]))
+                    for f in m._faces], clean=False)
+    return FloatingBody(hull, dofs, lid_mesh=lid, name=name or "+".join(names))

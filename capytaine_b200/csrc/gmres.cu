@@ -487,7 +487,8 @@ __global__ void __launch_bounds__(kThreads) gmres_check_kernel(Layout L, const d
       all &= q.done;
       nf += q.failed;
       it = max(it, q.iters);
-      worst = fmax(worst, q.bnrm2 > 0.0 ? q.rnorm / q.bnrm2 : 0.0);
+      // systems whose |b| was below atol were solved by x = 0 at the start
+      if (q.bnrm2 > 0.0 && q.bnrm2 >= q.atol) worst = fmax(worst, q.rnorm / q.bnrm2);
     }
     flags->skip_all = all;
     flags->skip_inner = all;

@@ -774,7 +774,6 @@ extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK,
       batch <= 0)
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_refine_solve: bad arguments (nrhs <= 16)");
   cudaStream_t s = (cudaStream_t)stream;
-  const size_t bytes = sizeof(double2) * ((size_t)(batch - 1) * strideB + (size_t)(nrhs - 1) * ldb + npad);
   const int nvec = batch * nrhs;
   double* bn = norms_dev;
   double* rn = norms_dev + nvec;
@@ -784,8 +783,15 @@ extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK,
   int launches = 1;
   // |b|^2 per column; x = 0, r = b, not converged
   colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)B_dev, n, ldb, strideB, bn, nullptr);
-  BEM_CUDA_CHECK(cudaMemsetAsync(X_dev, 0, bytes, s));
-  BEM_CUDA_CHECK(cudaMemcpyAsync(R_dev, B_dev, bytes, cudaMemcpyDeviceToDevice, s));
+  // Only the nrhs columns of each matrix: the caller may interleave other
+  // columns (a wider right-hand-side block solved in chunks) between them.
+  for (int b = 0; b < batch; ++b) {
+    const size_t o = (size_t)b * strideB;
+    BEM_CUDA_CHECK(cudaMemset2DAsync((double2*)X_dev + o, ldb * sizeof(double2), 0, npad * sizeof(double2), nrhs, s));
+    BEM_CUDA_CHECK(cudaMemcpy2DAsync((double2*)R_dev + o, ldb * sizeof(double2), (const double2*)B_dev + o,
+                                     ldb * sizeof(double2), npad * sizeof(double2), nrhs, cudaMemcpyDeviceToDevice,
+                                     s));
+  }
   BEM_CUDA_CHECK(cudaMemsetAsync(done, 0, sizeof(int), s));
   BEM_CUDA_CHECK(cudaMemsetAsync(state, 0, 2 * sizeof(double), s));
   // Iterations are enqueued in groups without host synchronisation; once the

@@ -219,7 +219,9 @@ extern "C" int bem_build_rhs(int n, int batch, const double* omega_dev, const do
   return BEM_OK;
 }
 
-static int ts_nsplit(int K) { return std::max(1, std::min(24, K / 256)); }
+// Splits of the K dimension: up to 24 for parallelism, more when a chunk of
+// X would not fit in shared memory (768 rows x 16 columns x 16 bytes = 192 KiB).
+static int ts_nsplit(int K) { return std::max(std::max(1, std::min(24, K / 256)), ceil_div(K, 768)); }
 
 extern "C" int64_t bem_zgemm_ts_workspace_bytes(int M, int K, int nrhs, int batch) {
   return (int64_t)batch * ts_nsplit(K) * (int64_t)M * nrhs * (int64_t)sizeof(double2);

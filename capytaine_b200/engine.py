@@ -34,6 +34,7 @@ from .green_function import Delhommeau
 LOG = logging.getLogger(__name__)
 
 NB = 64  # LU block size; matrices are padded to a multiple of it
+RHS_CHUNK = 16  # right-hand sides per refinement / GMRES / tall-GEMM call
 
 
 def padded_size(n: int) -> int:
@@ -133,12 +134,13 @@ class _Rhs:
         lib = _lib.load()
         mk = _allocator(device, alloc)
         self._mk = mk
+        self.chunk = min(nrhs, RHS_CHUNK)  # columns per solve call
         self.B = mk((batch, npad * nrhs), torch.complex128, True)
         self.X = mk((batch, npad * nrhs), torch.complex128, True)
         self.R = mk((batch, npad * nrhs), torch.complex128, True)
         self.phi = mk((batch, n * nrhs), torch.complex128)
-        self.norms = mk((2 * batch * nrhs + 2,), torch.float64, True)
-        self.ts_work = mk((int(lib.bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch)),), torch.uint8)
+        self.norms = mk((2 * batch * self.chunk + 2,), torch.float64, True)
+        self.ts_work = mk((int(lib.bem_zgemm_ts_workspace_bytes(n, n, self.chunk, batch)),), torch.uint8)
         self.flags = mk((2,), torch.int32, True)  # [err, nan]
         self._gmres = None
 
@@ -154,7 +156,7 @@ class _Rhs:
         """256-byte aligned workspace of bem_gmres_solve for this shape."""
         import torch
         if self._gmres is None or self._gmres[0] != restart:
-            nbytes = int(_lib.load().bem_gmres_workspace_bytes(self.n, self.npad, self.nrhs, self.batch, restart))
+            nbytes = int(_lib.load().bem_gmres_workspace_bytes(self.n, self.npad, self.chunk, self.batch, restart))
             if nbytes < 0:
                 raise ValueError("bad GMRES workspace shape")
             buf = self._mk((nbytes + 256,), torch.uint8)
@@ -164,7 +166,8 @@ class _Rhs:
     @staticmethod
     def estimate_bytes(n, npad, batch, nrhs):
         lib = _lib.load()
-        return 16 * batch * nrhs * (3 * npad + n) + int(lib.bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch)) + 4096
+        chunk = min(nrhs, RHS_CHUNK)
+        return 16 * batch * nrhs * (3 * npad + n) + int(lib.bem_zgemm_ts_workspace_bytes(n, n, chunk, batch)) + 4096
 
     @property
     def nbytes(self):
@@ -303,8 +306,6 @@ class B200Engine:
         heads = np.asarray(wave_directions, dtype=float)
         ndof, nhead = len(body.dofs), len(heads)
         nrhs = ndof + nhead
-        if nrhs > 16:
-            raise ValueError("at most 16 right-hand sides per frequency (dofs + headings)")
         B = min(self.max_batch if batch is None else batch, len(omegas))
         ws = self.workspace(n, B, nrhs)
         F_all = np.zeros((len(omegas), nrhs, ndof), dtype=np.complex128)
@@ -391,47 +392,26 @@ class B200Engine:
         _lib.check(lib.bem_build_rhs(n, nb, _vp(om_t), _vp(k_t), g, ndof, _vp(dofn), nhead, _vp(heads_t),
                                      _vp(dm.centers), _vp(dm.normals), _vp(hull), _vp(r.B), npad, npad * nrhs,
                                      stream))
-        if self._plain_gmres:
-            sol = self._gmres_solve(f, r, nb, 1e-6, 1e-5, None, stats, stream)
-        elif self.precision == "mixed":
-            iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
-            if self.refinement == "gmres":
-                # relative residual refine_tol in every column: atol 0, rtol refine_tol
-                maxc = max(1, -(-self.refine_max_iter // self.gmres_restart))
-                status = lib.bem_gmres_solve(_vp(f.K), n, n * n, n, npad, nb, _vp(r.B), _vp(r.X), npad, npad * nrhs,
-                                             nrhs, 0.0, self.refine_tol, self.gmres_restart, maxc,
-                                             _vp(f.lu_work_ptr), _vp(r.gmres_work(self.gmres_restart)), _vp(r.err),
-                                             ctypes.byref(iters), ctypes.byref(resid), stream)
+        ld = npad * nrhs  # batch stride of B, X, R
+        sol = r.B if (self.precision == "fp64" and not self._plain_gmres) else r.X
+        for c0 in range(0, nrhs, RHS_CHUNK):
+            nc = min(RHS_CHUNK, nrhs - c0)
+            off = 16 * npad * c0  # byte offset of column c0
+            Bc, Xc, Rc = (_vp(t.data_ptr() + off) for t in (r.B, r.X, r.R))
+            if self._plain_gmres:
+                self._gmres_solve(f, r, nb, 1e-6, 1e-5, None, stats, stream, Bc, Xc, nc)
+            elif self.precision == "mixed":
+                self._refine(f, r, nb, Bc, Xc, Rc, nc, stats, stream)
             else:
-                status = lib.bem_refine_solve(_vp(f.K), n, n * n, n, npad, nb, _vp(f.lu_work_ptr), _vp(f.piv),
-                                              _vp(r.B), _vp(r.X), _vp(r.R), npad, npad * nrhs, nrhs, self.refine_tol,
-                                              self.refine_max_iter, _vp(r.ts_work), _vp(r.norms), _vp(r.err),
-                                              ctypes.byref(iters), ctypes.byref(resid), stream)
-                if status == _lib.BEM_ERR_NOT_CONVERGED:
-                    # x += (LU)^-1 r does not contract (K close to singular, e.g. near an
-                    # irregular frequency): GMRES on K, preconditioned by the same float32
-                    # factors, from x = 0 to the same tolerance.
-                    stats["escalated_to_gmres"] = stats.get("escalated_to_gmres", 0) + 1
-                    status = lib.bem_gmres_solve(_vp(f.K), n, n * n, n, npad, nb, _vp(r.B), _vp(r.X), npad,
-                                                 npad * nrhs, nrhs, 0.0, self.refine_tol, self.gmres_restart,
-                                                 max(1, self.gmres_escalation_cycles), _vp(f.lu_work_ptr),
-                                                 _vp(r.gmres_work(self.gmres_restart)), _vp(r.err),
-                                                 ctypes.byref(iters), ctypes.byref(resid), stream)
-            stats["refine_iters"] = max(stats.get("refine_iters", 0), iters.value)
-            stats["refine_residual"] = max(stats.get("refine_residual", 0.0), resid.value)
-            if status == _lib.BEM_ERR_NOT_CONVERGED:
-                stats["not_converged"] = stats.get("not_converged", 0) + 1
-                raise _lib.NotConvergedError(status, lib.bem_last_error().decode())
-            _lib.check(status)
-            sol = r.X
-        else:
-            _lib.check(lib.bem_zlu_solve(_vp(f.K), npad, npad, npad * npad, nb, _vp(f.piv), _vp(f.lu_work),
-                                         _vp(r.B), npad, npad * nrhs, nrhs, _vp(r.err), stream))
-            sol = r.B
+                _lib.check(lib.bem_zlu_solve(_vp(f.K), npad, npad, npad * npad, nb, _vp(f.piv), _vp(f.lu_work), Bc,
+                                             npad, ld, nc, _vp(r.err), stream))
         if events:
             events[3].record()
-        _lib.check(lib.bem_zgemm_ts(n, n, nrhs, 1.0, 0.0, _vp(f.S), n, n * n, _vp(sol), npad, npad * nrhs,
-                                    0.0, 0.0, _vp(r.phi), n, n * nrhs, nb, _vp(r.ts_work), stream))
+        for c0 in range(0, nrhs, RHS_CHUNK):
+            nc = min(RHS_CHUNK, nrhs - c0)
+            _lib.check(lib.bem_zgemm_ts(n, n, nc, 1.0, 0.0, _vp(f.S), n, n * n, _vp(sol.data_ptr() + 16 * npad * c0),
+                                        npad, ld, 0.0, 0.0, _vp(r.phi.data_ptr() + 16 * n * c0), n, n * nrhs, nb,
+                                        _vp(r.ts_work), stream))
         out = torch.empty((nb * nrhs * ndof + nb * max(nhead, 1) * ndof,), dtype=torch.complex128, device=dev)
         F = out[:nb * nrhs * ndof]
         FK = out[nb * nrhs * ndof:]
@@ -456,15 +436,49 @@ class B200Engine:
         FK_h = host[nb * nrhs * ndof:].reshape(nb, max(nhead, 1), ndof)[:, :nhead]
         return F_h, FK_h
 
-    def _gmres_solve(self, f, r, nb, atol, rtol, precond_ptr, stats, stream):
-        """Plain float64 GMRES of every RHS column in r.B into r.X (SciPy's
-        settings: restart 20, at most 10 n cycles by default)."""
+    def _refine(self, f, r, nb, Bc, Xc, Rc, nc, stats, stream):
+        """Refined solve of nc columns (B, X, R column pointers, batch stride
+        npad * r.nrhs) with the float32 factors: classical refinement, or GMRES
+        right-preconditioned by the factors; the classical iteration continues
+        with that GMRES when it stops contracting."""
         lib = _lib.load()
-        n, npad, nrhs = f.n, f.npad, r.nrhs
+        n, npad, ld = f.n, f.npad, f.npad * r.nrhs
+        iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
+
+        def gmres(cycles):
+            return lib.bem_gmres_solve(_vp(f.K), n, n * n, n, npad, nb, Bc, Xc, npad, ld, nc, 0.0, self.refine_tol,
+                                       self.gmres_restart, cycles, _vp(f.lu_work_ptr),
+                                       _vp(r.gmres_work(self.gmres_restart)), _vp(r.err), ctypes.byref(iters),
+                                       ctypes.byref(resid), stream)
+        if self.refinement == "gmres":
+            # relative residual refine_tol in every column: atol 0, rtol refine_tol
+            status = gmres(max(1, -(-self.refine_max_iter // self.gmres_restart)))
+        else:
+            status = lib.bem_refine_solve(_vp(f.K), n, n * n, n, npad, nb, _vp(f.lu_work_ptr), _vp(f.piv), Bc, Xc, Rc,
+                                          npad, ld, nc, self.refine_tol, self.refine_max_iter, _vp(r.ts_work),
+                                          _vp(r.norms), _vp(r.err), ctypes.byref(iters), ctypes.byref(resid), stream)
+            if status == _lib.BEM_ERR_NOT_CONVERGED:
+                # x += (LU)^-1 r does not contract (K close to singular, e.g. near an
+                # irregular frequency): GMRES on K, preconditioned by the same float32
+                # factors, from x = 0 to the same tolerance.
+                stats["escalated_to_gmres"] = stats.get("escalated_to_gmres", 0) + 1
+                status = gmres(max(1, self.gmres_escalation_cycles))
+        stats["refine_iters"] = max(stats.get("refine_iters", 0), iters.value)
+        stats["refine_residual"] = max(stats.get("refine_residual", 0.0), resid.value)
+        if status == _lib.BEM_ERR_NOT_CONVERGED:
+            stats["not_converged"] = stats.get("not_converged", 0) + 1
+            raise _lib.NotConvergedError(status, lib.bem_last_error().decode())
+        _lib.check(status)
+
+    def _gmres_solve(self, f, r, nb, atol, rtol, precond_ptr, stats, stream, Bc, Xc, nc):
+        """Plain float64 GMRES of nc RHS columns (column pointers Bc into Xc)
+        with SciPy's settings: restart 20, at most 10 n cycles by default."""
+        lib = _lib.load()
+        n, npad = f.n, f.npad
         maxc = self.gmres_maxiter if self.gmres_maxiter is not None else 10 * n
         iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
-        status = lib.bem_gmres_solve(_vp(f.K), f.ldk, f.strideK, n, npad, nb, _vp(r.B), _vp(r.X), npad, npad * nrhs,
-                                     nrhs, atol, rtol, self.gmres_restart, int(maxc), precond_ptr,
+        status = lib.bem_gmres_solve(_vp(f.K), f.ldk, f.strideK, n, npad, nb, Bc, Xc, npad, npad * r.nrhs, nc, atol,
+                                     rtol, self.gmres_restart, int(maxc), precond_ptr,
                                      _vp(r.gmres_work(self.gmres_restart)), _vp(r.err), ctypes.byref(iters),
                                      ctypes.byref(resid), stream)
         stats["gmres_iters"] = max(stats.get("gmres_iters", 0), iters.value)
@@ -473,7 +487,6 @@ class B200Engine:
             raise _lib.NotConvergedError(status, lib.bem_last_error().decode() +
                                          "\nThis can be due to overlapping panels or irregular frequencies.")
         _lib.check(status)
-        return r.X
 
     @staticmethod
     def _coefficients(body, omegas, heads, F_all, FK_all, stats):

@@ -167,6 +167,42 @@ class Mesh:
         v, f = _clip_faces(self.vertices, self._faces, np.asarray(normal, float), np.asarray(origin, float))
         return Mesh(v, f, quadrature_method=self.quadrature_method, name=name or self.name, clean=True)
 
+    def generate_lid(self, z=0.0, faces_max_radius=None, name=None) -> "Mesh":
+        """Mesh of the interior free surface of the body at height z, for the
+        removal of irregular frequencies (capytaine meshes/meshes.py:655-737):
+        a rectangle slightly larger than the waterplane (panels of the mean
+        face radius of the hull below z, normal -z) keeps the faces whose four
+        vertices lie inside the hull, a vertex being inside when an odd number
+        of hull faces lie under it in the horizontal projection."""
+        if name is None and self.name is not None:
+            name = f"lid for {self.name}"
+        hull = self.clipped(origin=(0.0, 0.0, z), normal=(0.0, 0.0, 1.0))
+        if hull.nb_faces == 0:
+            return Mesh(np.empty((0, 3)), [], name=name, clean=False)
+        v = hull.vertices
+        x_span, y_span = np.ptp(v[:, 0]), np.ptp(v[:, 1])
+        x_mean = (v[:, 0].max() + v[:, 0].min()) / 2
+        y_mean = (v[:, 1].max() + v[:, 1].min()) / 2
+        if faces_max_radius is None:
+            faces_max_radius = float(np.mean(hull.faces_radiuses))
+        size = (max(faces_max_radius / 2, 1.1 * x_span), max(faces_max_radius / 2, 1.1 * y_span))
+        cand = mesh_rectangle(size=(size[1], size[0]), faces_max_radius=faces_max_radius,
+                              center=(x_mean, y_mean, z), normal=(0.0, 0.0, -1.0), name="candidate_lid_mesh")
+        pts = cand.vertices[:, :2]
+        hf = hull.vertices[hull.faces, :2]                      # (F, 4, 2)
+        edges = hf[:, [1, 2, 3, 0], :] - hf                    # consecutive vertices of each face
+        inside = np.zeros(len(pts), dtype=bool)
+        for c0 in range(0, len(pts), 256):  # bounded temporaries: (256, F, 4, 2)
+            loc = pts[c0:c0 + 256, None, None, :] - hf[None]
+            side = loc[..., 0] * edges[..., 1] - loc[..., 1] * edges[..., 0]
+            above = np.all(side <= 0, axis=-1) | np.all(side >= 0, axis=-1)
+            inside[c0:c0 + 256] = np.sum(above, axis=-1) % 2 == 1
+        keep = np.all(inside[cand.faces], axis=1)
+        faces = [list(f) for f in cand.faces[keep]]
+        if not faces:
+            return Mesh(np.empty((0, 3)), [], name=name, clean=False)
+        return Mesh(cand.vertices, faces, name=name, clean=True)
+
     def immersed_part(self, free_surface=0.0) -> "Mesh":
         """Part below z = free_surface; capytaine abstract_meshes.py:383-407 (infinite depth)."""
         if self.z_span[1] <= free_surface:
@@ -345,12 +381,18 @@ def mesh_ellipsoid(*, semi_axes=(1.0, 1.0, 1.0), center=(0.0, 0.0, 0.0), resolut
     return mesh_sphere(radius=1.0, resolution=resolution, name=name).scaled(semi_axes).translated(center)
 
 
-def mesh_rectangle(*, size=(5.0, 5.0), center=(0.0, 0.0, 0.0), resolution=(5, 5),
+def mesh_rectangle(*, size=(5.0, 5.0), center=(0.0, 0.0, 0.0), resolution=(5, 5), faces_max_radius=None,
                    normal=(0.0, 0.0, 1.0), name=None) -> Mesh:
     """One-sided rectangle (capytaine rectangles.py:26-100), built directly in the
-    plane orthogonal to ``normal`` with panels oriented along ``normal``."""
+    plane orthogonal to ``normal`` with panels oriented along ``normal``.  When
+    the panels of ``resolution`` are larger than ``faces_max_radius``, the
+    resolution becomes ceil(side / (sqrt(2) faces_max_radius)) per side
+    (rectangles.py:67-71)."""
     width, height = size
     nw, nh = resolution
+    if faces_max_radius is not None and np.hypot(width / nw, height / nh) / 2 > faces_max_radius:
+        nw = int(np.ceil(width / (np.sqrt(2) * faces_max_radius)))
+        nh = int(np.ceil(height / (np.sqrt(2) * faces_max_radius)))
     normal = np.asarray(normal, float)
     normal = normal / np.linalg.norm(normal)
     # In-plane axes: the reference builds the panel in x=0 with normal -x, then rotates.

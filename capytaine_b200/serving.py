@@ -229,8 +229,6 @@ class SolveServer:
         heads = np.asarray(wave_directions, dtype=float)
         mesh = body.mesh_including_lid
         nrhs = len(body.dofs) + len(heads)
-        if nrhs > 16:
-            raise ValueError("at most 16 right-hand sides per frequency (dofs + headings)")
         fut: cf.Future = cf.Future()
         with self._cv:
             if self._failure is not None:

@@ -289,7 +289,8 @@ int64_t bem_gmres_workspace_bytes(int n, int npad, int nrhs, int batch, int rest
  * mixed-precision LU.  X (ldb,
  * strideB): rows < n written.  work_dev: bem_gmres_workspace_bytes, 256-byte
  * aligned.  iters_out: largest number of inner iterations over the systems;
- * resid_out: largest |b - A x| / |b|.  Synchronises the stream once per group
+ * resid_out: largest |b - A x| / |b| over the systems with |b| >= atol (the
+ * others are solved by x = 0, as SciPy does).  Synchronises the stream once per group
  * of four inner iterations and once per cycle.  Returns BEM_ERR_NOT_CONVERGED
  * when a system breaks down or max_cycles is reached.  Replaces
  * scipy.sparse.linalg.gmres behind capytaine's solve_gmres

@@ -278,6 +278,19 @@ class Dof:
         return np.cross(d, points - np.asarray(self.center, float))
 
 
+@dataclass(frozen=True, eq=False)
+class SubmeshDof:
+    """A dof acting on the faces of `mask` only (capytaine bodies/dofs.py:100-127),
+    zero elsewhere: the dofs of one body of a joined multibody."""
+    dof: object
+    mask: np.ndarray
+
+    def motion(self, points: np.ndarray) -> np.ndarray:
+        m = np.zeros((points.shape[0], 3))
+        m[self.mask] = self.dof.motion(points[self.mask])
+        return m
+
+
 def rigid_body_dofs(rotation_center=(0.0, 0.0, 0.0), only=None) -> Dict[str, Dof]:
     """capytaine bodies/dofs.py:139-172"""
     dofs = {
@@ -332,12 +345,19 @@ def solve_gmres(A, b):
 
 
 def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: float, *, rho=1000.0, g=9.81,
-                    wave_directions=(0.0,), free_surface=0.0, linear_solver="lu"):
+                    wave_directions=(0.0,), free_surface=0.0, linear_solver="lu", hull_mask=None):
     """One frequency-solve, indirect method (solver.py:188-207): assemble S and K at
     k = omega^2/g, factor K once, solve every radiation and diffraction RHS, take
     S @ sigma, integrate pressures.  Returns added mass, damping (dict of dict) and
-    excitation forces (dict heading -> dict dof -> complex)."""
+    excitation forces (dict heading -> dict dof -> complex).  With `hull_mask`
+    (mesh = hull faces then lid faces, problems_and_results.py:373-381,
+    440-449) the boundary conditions are zero on the lid and the pressures are
+    integrated on the hull only; dofs are then evaluated at the hull faces."""
     import scipy.linalg as sl
+
+    if hull_mask is not None:
+        return _solve_frequency_with_lid(gf, mesh, dofs, omega, rho=rho, g=g, wave_directions=wave_directions,
+                                         linear_solver=linear_solver, hull_mask=np.asarray(hull_mask, bool))
 
     k = omega ** 2 / g if free_surface != np.inf else 0.0
     S, K = gf.evaluate(mesh, mesh, free_surface=free_surface, water_depth=np.inf, wavenumber=k,
@@ -372,4 +392,38 @@ def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: flo
             results["diffraction"][key] = forces
             results["froude_krylov"][key] = fk
             results["excitation"][key] = {d: forces[d] + fk[d] for d in forces}
+    return results
+
+
+def _solve_frequency_with_lid(gf, mesh, dofs, omega, *, rho, g, wave_directions, linear_solver, hull_mask):
+    """solve_frequency for a mesh whose faces outside hull_mask are a lid."""
+    import scipy.linalg as sl
+    k = omega ** 2 / g
+    S, K = gf.evaluate(mesh, mesh, free_surface=0.0, water_depth=np.inf, wavenumber=k, adjoint_double_layer=True,
+                       early_dot_product=True, diagonal_term_in_double_layer=True)
+    lu = sl.lu_factor(K) if linear_solver == "lu" else None
+    c, nrm, area = mesh.faces_centers[hull_mask], mesh.faces_normals[hull_mask], mesh.faces_areas[hull_mask]
+    N = mesh.nb_faces
+
+    def solve(bc_hull):
+        bc = np.zeros(N, dtype=np.complex128)
+        bc[hull_mask] = bc_hull
+        sigma = sl.lu_solve(lu, bc) if lu is not None else (solve_gmres(K, bc) if linear_solver == "gmres"
+                                                            else np.linalg.solve(K, bc))
+        return (1j * omega * rho * (S @ sigma))[hull_mask]
+
+    def forces(pressure):
+        return {name: np.sum(pressure * -np.sum(d.motion(c) * nrm, axis=1) * area) for name, d in dofs.items()}
+
+    results = {"added_mass": {}, "radiation_damping": {}, "excitation": {}, "diffraction": {}, "froude_krylov": {}}
+    for name, dof in dofs.items():
+        f = forces(solve(-1j * omega * np.sum(dof.motion(c) * nrm, axis=1)))
+        results["added_mass"][name] = {d: float(np.real(v) / omega ** 2) for d, v in f.items()}
+        results["radiation_damping"][name] = {d: float(np.imag(v) / omega) for d, v in f.items()}
+    for beta in wave_directions:
+        dif = forces(solve(-(airy_waves_velocity(c, omega, k, g, beta) * nrm).sum(axis=1)))
+        fk = forces(airy_waves_pressure(c, omega, k, g, rho, beta))
+        results["diffraction"][beta] = dif
+        results["froude_krylov"][beta] = fk
+        results["excitation"][beta] = {d: dif[d] + fk[d] for d in dif}
     return results

@@ -144,3 +144,24 @@ def test_refinement_reports_non_convergence():
                               ctypes.byref(resid), _lib.stream_ptr())
     assert st == _lib.BEM_ERR_NOT_CONVERGED and iters.value == 2 and 0.0 < resid.value < 1e-5
     assert b"iterative refinement stopped" in lib.bem_last_error()
+
+
+def test_refinement_of_a_column_block_leaves_other_columns_alone():
+    """Columns [0, 2) of a 3-column block of 2 matrices (batch stride covers
+    all 3): the third column of X and R keeps what it held."""
+    import torch
+    n, batch, ncol = 300, 2, 3
+    lib, npad, mats, rhs, K, B, work, wptr, piv, info, err = _setup(n, batch, ncol, 5)
+    X = torch.full_like(B, 3.0)
+    R = torch.full_like(B, 5.0)
+    ts = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, 2, batch)), dtype=torch.uint8, device="cuda")
+    norms = torch.zeros(2 * batch * 2 + 2, dtype=torch.float64, device="cuda")
+    iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
+    _lib.check(lib.bem_refine_solve(_vp(K), n, n * n, n, npad, batch, _vp(wptr), _vp(piv), _vp(B), _vp(X), _vp(R),
+                                    npad, npad * ncol, 2, 1e-10, 30, _vp(ts), _vp(norms), _vp(err),
+                                    ctypes.byref(iters), ctypes.byref(resid), _lib.stream_ptr()))
+    assert resid.value <= 1e-10
+    assert torch.all(X[:, 2, :] == 3.0) and torch.all(R[:, 2, :] == 5.0)
+    for b in range(batch):
+        ref = np.linalg.solve(mats[b], rhs[b][:, :2])
+        assert np.abs(X[b, :2, :n].T.cpu().numpy() - ref).max() / np.abs(ref).max() < 1e-9
