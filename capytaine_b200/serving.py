@@ -372,13 +372,12 @@ class SolveServer:
                 self.counters["max_reserved_bytes"] = max(self.counters["max_reserved_bytes"],
                                                           self._inflight_bytes + self._resident_bytes)
             admitted = time.perf_counter()
-            keep = None
+            keep = result = error = None
             try:
                 with slot:
-                    keep = self._run(req, res, admitted)
+                    result, keep = self._run(req, res, admitted)
             except BaseException as exc:  # the request fails, the server goes on
-                if not req.future.done():
-                    req.future.set_exception(exc)
+                error = exc
             finally:
                 with self._cv:
                     self._inflight_bytes -= need
@@ -392,11 +391,18 @@ class SolveServer:
                             self._resident_bytes += f.nbytes
                         else:
                             release()
-                    if req.future.exception() is None:
+                    if error is None:
                         self.counters["completed"] += 1
+                        if res is not None:
+                            self.counters["reused"] += 1
                     else:
                         self.counters["failed"] += 1
                     self._cv.notify_all()
+            # the caller sees the result after the bookkeeping above
+            if error is None:
+                req.future.set_result(result)
+            else:
+                req.future.set_exception(error)
 
     def _buffers(self, build):
         """build(alloc) with arena views, all or nothing: when the arena has no
@@ -420,7 +426,7 @@ class SolveServer:
 
     def _run(self, req: _Request, res: Optional[_Resident], admitted: float):
         """Enqueue the request's work on the current (slot) stream and wait
-        for it; returns (factors, release) to keep resident, if any."""
+        for it; returns the result and (factors, release) to keep resident, if any."""
         eng = self.engine
         body = req.body
         mesh = body.mesh_including_lid
@@ -462,12 +468,9 @@ class SolveServer:
         ndof = len(body.dofs)
         w = req.omega
         rad, dif, fk = F[0, :ndof, :], F[0, ndof:, :], FK[0]
-        req.future.set_result(SolveResult(
+        result = SolveResult(
             request_id=req.rid, omega=w, dofs=list(body.dofs), wave_directions=req.heads,
             added_mass=np.real(rad) / w ** 2, radiation_damping=np.imag(rad) / w, diffraction=dif,
             froude_krylov=fk, excitation=dif + fk, arrival=req.arrival, admitted=admitted, finished=finished,
-            reused_factors=res is not None, stats=dict(stats)))
-        if res is not None:
-            with self._cv:
-                self.counters["reused"] += 1
-        return keep
+            reused_factors=res is not None, stats=dict(stats))
+        return result, keep
