@@ -58,11 +58,12 @@ def workload_config(args, n):
 RIGID_DOFS = ("Surge", "Sway", "Heave", "Roll", "Pitch", "Yaw")
 
 
-def seeded_bodies(seed, count, panels=(500, 8000)):
+def seeded_bodies(seed, count, panels=(500, 8000), all_dofs=False):
     """Seeded floating bodies with panel counts uniform in `panels`: even
     indices ellipsoids (semi-axes U[1, 10] m, centred on the free surface),
     odd indices vertical cylinders (radius U[1, 8] m, draft U[2, 15] m), the
-    resolution chosen for the panel target; 1 to 6 rigid dofs about the origin."""
+    resolution chosen for the panel target; 1 to 6 rigid dofs about the origin
+    (all 6 with all_dofs)."""
     from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
     from capytaine_b200.meshes import mesh_ellipsoid, mesh_vertical_cylinder
     rng = np.random.default_rng(seed)
@@ -82,6 +83,8 @@ def seeded_bodies(seed, count, panels=(500, 8000)):
             mesh = mesh_vertical_cylinder(length=2 * d, radius=r, resolution=(nr, nth, 2 * nz)).immersed_part()
         ndof = int(rng.integers(1, 7))
         dofs = [RIGID_DOFS[j] for j in sorted(rng.permutation(6)[:ndof])]
+        if all_dofs:
+            dofs = list(RIGID_DOFS)
         bodies.append(FloatingBody(mesh, rigid_body_dofs(only=dofs), name=f"body{i}"))
     return bodies
 
@@ -156,6 +159,68 @@ def run_serving(engine, bodies, *, rate, n_requests, seed, slots, repeat_frac=0.
             "workload": "Poisson arrivals; distinct seeded bodies (ellipsoids / vertical cylinders of 500-8000 "
                         "panels stretched per request), 1-6 dofs, omega ~ U[0.1, 4], 20% repeats of resident "
                         "(mesh, omega) pairs"}
+
+
+def run_bodies(args):
+    """--workload bodies: 64 seeded bodies (ellipsoids and vertical cylinders,
+    300-3000 panels, seed 0), 6 dofs + diffraction heading 0, 30 omega in
+    linspace(0.1, 4): the refined mixed engine batched across bodies
+    (solve_bodies) against one solve_frequencies sweep per body."""
+    import torch
+    from capytaine_b200.engine import B200Engine
+    from capytaine_b200.green_function import Delhommeau
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    bodies = seeded_bodies(0, args.bodies, panels=(300, 3000), all_dofs=True)
+    omegas = np.linspace(0.1, 4.0, 30)
+    gf = Delhommeau(tabulation_cache_dir=None)
+    eng = B200Engine(green_function=gf, precision="mixed", max_batch=16)
+    eng.solve_bodies(bodies[:2], omegas[:2])  # warm-up
+
+    def timed(fn):
+        gf.clear_rankine_cache()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        res = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return res, e0.elapsed_time(e1), time.perf_counter() - t0
+
+    timings, out = {}, {}
+    # 30 frequencies per body: each body fills its own batches (solve_bodies runs one sweep per body);
+    # 3 frequencies per body: bodies of the same padded size share batches
+    for name, oms, fn in (
+            ("solve_bodies_30_omega", omegas, lambda: eng.solve_bodies(bodies, omegas)),
+            ("grouped_3_omega", omegas[::10], lambda: eng.solve_bodies(bodies, omegas[::10],
+                                                                       sync_stats=args.bodies_stats)),
+            ("one_sweep_per_body_3_omega", omegas[::10],
+             lambda: [eng.solve_frequencies(b, omegas[::10]) for b in bodies])):
+        res, ms, wall = timed(fn)
+        out[name] = res
+        timings[name] = {"value": len(bodies) * len(oms) / (ms * 1e-3), "unit": UNIT, "ms": ms, "wall_s": wall}
+    diff = 0.0
+    for a, b in zip(out["grouped_3_omega"], out["one_sweep_per_body_3_omega"]):
+        for c in ("added_mass", "radiation_damping", "excitation"):
+            x, y = getattr(a, c), getattr(b, c)
+            diff = max(diff, float(np.abs(x - y).max() / np.abs(y).max()))
+    panels = [b.mesh.nb_faces for b in bodies]
+    st = out["grouped_3_omega"][0].stats
+    line = {"metric": "freq solves/sec, 64 bodies of 300-3000 panels x 30 omega",
+            "value": timings["solve_bodies_30_omega"]["value"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "dtype": "c128 (assembly, residuals) / f32-tf32 (LU)", "data": "synthetic",
+            "config": {"workload": "64 seeded bodies (ellipsoids semi-axes U[1,10] m / vertical cylinders r U[1,8] m, "
+                                   "draft U[2,15] m), 6 dofs + diffraction heading 0, omega linspace(0.1, 4, 30)",
+                       "bodies": len(bodies), "panels": {"min": min(panels), "mean": float(np.mean(panels)),
+                                                         "max": max(panels)},
+                       "groups": st.get("groups"), "batches": st.get("batches"),
+                       "stages_ms": {k: round(st[k], 2) for k in ("assembly_ms", "lu_ms", "solve_ms") if st.get(k)}},
+            **timings,
+            "grouped_over_per_body_3_omega": (timings["grouped_3_omega"]["value"]
+                                              / timings["one_sweep_per_body_3_omega"]["value"]),
+            "max_rel_diff_grouped_vs_per_body": diff}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def cylinder_array_body():
@@ -486,8 +551,11 @@ def main():
                     help="requests of the serving run (Poisson arrivals); 0 skips it")
     ap.add_argument("--arrival-rate", type=float, default=200.0)
     ap.add_argument("--slots", type=int, default=8)
-    ap.add_argument("--workload", default="barge", choices=["barge", "array"],
-                    help="array: the 3x3 cylinder array with lids (20000 panels), mixed vs float64 GMRES")
+    ap.add_argument("--workload", default="barge", choices=["barge", "array", "bodies"],
+                    help="array: the 3x3 cylinder array with lids (20000 panels), mixed vs float64 GMRES; "
+                         "bodies: 64 bodies of 300-3000 panels batched across bodies")
+    ap.add_argument("--bodies", type=int, default=64)
+    ap.add_argument("--bodies-stats", action="store_true", help="per-stage device times of the batched sweep")
     ap.add_argument("--array-frequencies", type=int, default=40)
     ap.add_argument("--array-batch", type=int, default=4)
     args = ap.parse_args()
@@ -496,6 +564,8 @@ def main():
         return run_reference(args)
     if args.workload == "array":
         return run_array(args)
+    if args.workload == "bodies":
+        return run_bodies(args)
 
     import torch
     rank = int(os.environ.get("RANK", "0"))

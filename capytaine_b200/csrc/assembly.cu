@@ -554,11 +554,21 @@ struct SymFace {
 // both (I, J) and, off the diagonal tiles, (J, I) (through shared memory, so
 // that the mirrored stores stay coalesced).  FP64, complex128 outputs, K with
 // the dot product taken.
-__global__ void __launch_bounds__(kSymT) wave_symmetric_kernel(const bem_assembly_args a, TabView T, double k,
+// Up to kSymBatch wavenumbers per launch (blockIdx.z), passed by value.
+constexpr int kSymBatch = 64;
+struct SymBatch {
+  double k[kSymBatch];
+  int64_t s_stride, k_stride;  // elements between the outputs of consecutive wavenumbers
+};
+
+__global__ void __launch_bounds__(kSymT) wave_symmetric_kernel(bem_assembly_args a, TabView T, SymBatch kb,
                                                                int gf_sing, const double2* __restrict__ rank,
                                                                int64_t rank_ld) {
   const int bi = blockIdx.x, bj = blockIdx.y;
   if (bi > bj) return;
+  const double k = kb.k[blockIdx.z];
+  a.S_dev = reinterpret_cast<double2*>(a.S_dev) + blockIdx.z * kb.s_stride;
+  a.K_dev = reinterpret_cast<double2*>(a.K_dev) + blockIdx.z * kb.k_stride;
   __shared__ SymFace faces[kSymT];
   __shared__ double4 mir[kSymChunk][kSymT];  // (S_w re, S_w im, K_w re, K_w im) of entries (J, I)
   if (T.nr > 1 && T.nz > 1) {
@@ -791,40 +801,95 @@ extern "C" int bem_assemble_rankine_part(const bem_assembly_args* args, void* ou
   return BEM_OK;
 }
 
-extern "C" int bem_assemble_wave_symmetric(const bem_assembly_args* args, const void* rankine_dev, int64_t ld,
-                                           void* stream) {
-  using namespace bem;
-  if (!args || !rankine_dev) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_wave_symmetric: null pointer");
+namespace bem {
+namespace {
+// Shared by the single- and multi-wavenumber entry points: checks, then one
+// launch per group of up to kSymBatch wavenumbers (grid z = wavenumber).
+int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev, int64_t ld, const double* ks,
+                          int nk, int64_t s_stride, int64_t k_stride, void* stream, const char* who) {
+  char msg[200];
+  if (!args || !rankine_dev || !ks || nk <= 0) {
+    std::snprintf(msg, sizeof(msg), "%s: null pointer or no wavenumber", who);
+    return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+  }
   const bem_assembly_args& a = *args;
-  int st = check_common(a, "bem_assemble_wave_symmetric");
+  int st = check_common(a, who);
   if (st) return st;
-  if (!a.S_dev || !a.K_dev) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_wave_symmetric: null output");
+  if (!a.S_dev || !a.K_dev) {
+    std::snprintf(msg, sizeof(msg), "%s: null output", who);
+    return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+  }
   if (a.n != a.nb_faces || a.nb_quad_points != 1 || a.points_dev != a.quad_points_dev ||
-      a.centers_dev != a.quad_points_dev)
-    return set_error(BEM_ERR_INVALID_ARGUMENT,
-                     "bem_assemble_wave_symmetric: needs one mesh, one quadrature point per face, and the same "
-                     "array for points, centres and quadrature points");
-  if (!(a.wavenumber > 0.0) || !std::isfinite(a.wavenumber))
-    return set_error(BEM_ERR_UNSUPPORTED, "bem_assemble_wave_symmetric: wavenumber must be finite and > 0");
-  if (a.out_dtype != BEM_DTYPE_C128 || a.precision != BEM_PREC_FP64)
-    return set_error(BEM_ERR_UNSUPPORTED, "bem_assemble_wave_symmetric: complex128 outputs, float64 only");
-  if (a.lds < a.n || a.ldk < a.n || ld < a.n)
-    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_wave_symmetric: leading dimension < n");
+      a.centers_dev != a.quad_points_dev) {
+    std::snprintf(msg, sizeof(msg), "%s: needs one mesh, one quadrature point per face, and the same array for "
+                  "points, centres and quadrature points", who);
+    return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+  }
+  for (int i = 0; i < nk; ++i)
+    if (!(ks[i] > 0.0) || !std::isfinite(ks[i])) {
+      std::snprintf(msg, sizeof(msg), "%s: wavenumber must be finite and > 0", who);
+      return set_error(BEM_ERR_UNSUPPORTED, msg);
+    }
+  if (a.out_dtype != BEM_DTYPE_C128 || a.precision != BEM_PREC_FP64) {
+    std::snprintf(msg, sizeof(msg), "%s: complex128 outputs, float64 only", who);
+    return set_error(BEM_ERR_UNSUPPORTED, msg);
+  }
+  if (a.lds < a.n || a.ldk < a.n || ld < a.n) {
+    std::snprintf(msg, sizeof(msg), "%s: leading dimension < n", who);
+    return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+  }
+  if (nk > 1 && (s_stride < a.lds * (int64_t)a.n || k_stride < a.ldk * (int64_t)a.n)) {
+    std::snprintf(msg, sizeof(msg), "%s: output strides smaller than one matrix", who);
+    return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+  }
   const bool tabulated = a.nr > 1 && a.nz > 1;
-  if (tabulated && (!a.r_range_dev || !a.z_range_dev || !a.table_dev))
-    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_wave_symmetric: tabulation pointers missing");
-  if (!tabulated && a.tabulation_nb_integration_points <= 0)
-    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_wave_symmetric: nb_integration_points <= 0");
+  if (tabulated && (!a.r_range_dev || !a.z_range_dev || !a.table_dev)) {
+    std::snprintf(msg, sizeof(msg), "%s: tabulation pointers missing", who);
+    return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+  }
+  if (!tabulated && a.tabulation_nb_integration_points <= 0) {
+    std::snprintf(msg, sizeof(msg), "%s: nb_integration_points <= 0", who);
+    return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+  }
   const TabView T{a.tabulation_nb_integration_points, a.tabulation_grid_shape, a.nr, a.nz, a.r_range_dev,
                   a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0};
   const int nb = ceil_div(a.n, kSymT);
   cudaStream_t s = (cudaStream_t)stream;
-  {
-    TimedLaunch tl(kKAssemble, s);
-    wave_symmetric_kernel<<<dim3(nb, nb), kSymT, 0, s>>>(a, T, a.wavenumber, a.gf_singularities,
-                                                         (const double2*)rankine_dev, ld);
+  int launches = 0;
+  for (int k0 = 0; k0 < nk; k0 += kSymBatch) {
+    const int cnt = std::min(kSymBatch, nk - k0);
+    SymBatch kb{};
+    for (int i = 0; i < cnt; ++i) kb.k[i] = ks[k0 + i];
+    kb.s_stride = s_stride;
+    kb.k_stride = k_stride;
+    bem_assembly_args ak = a;
+    ak.S_dev = reinterpret_cast<double2*>(a.S_dev) + (size_t)k0 * s_stride;
+    ak.K_dev = reinterpret_cast<double2*>(a.K_dev) + (size_t)k0 * k_stride;
+    {
+      TimedLaunch tl(kKAssemble, s);
+      wave_symmetric_kernel<<<dim3(nb, nb, cnt), kSymT, 0, s>>>(ak, T, kb, a.gf_singularities,
+                                                                (const double2*)rankine_dev, ld);
+    }
+    ++launches;
   }
-  count_launches(1);
+  count_launches(launches);
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
+}
+}  // namespace
+}  // namespace bem
+
+extern "C" int bem_assemble_wave_symmetric(const bem_assembly_args* args, const void* rankine_dev, int64_t ld,
+                                           void* stream) {
+  using namespace bem;
+  const double k = args ? args->wavenumber : 0.0;
+  return wave_symmetric_launch(args, rankine_dev, ld, &k, 1, 0, 0, stream, "bem_assemble_wave_symmetric");
+}
+
+extern "C" int bem_assemble_wave_symmetric_batched(const bem_assembly_args* args, const void* rankine_dev,
+                                                   int64_t ld, const double* wavenumbers_host, int nk,
+                                                   int64_t s_stride, int64_t k_stride, void* stream) {
+  using namespace bem;
+  return wave_symmetric_launch(args, rankine_dev, ld, wavenumbers_host, nk, s_stride, k_stride, stream,
+                               "bem_assemble_wave_symmetric_batched");
 }

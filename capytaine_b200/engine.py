@@ -29,6 +29,7 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 from . import _lib
+from .arena import DeviceArena
 from .green_function import Delhommeau
 
 LOG = logging.getLogger(__name__)
@@ -342,13 +343,22 @@ class B200Engine:
     def _plain_gmres(self):
         return self.precision == "fp64" and self._linear_solver == "gmres"
 
-    def assemble_stage(self, f: "_Factors", mesh, ks, *, nan_flag=None, reuse_rankine=True):
-        """S and K of the mesh with itself at the wavenumbers ks into f[0:len(ks)]."""
+    def assemble_stage(self, f: "_Factors", mesh, ks, *, nan_flag=None, reuse_rankine=True, first=0, lds=None):
+        """S and K of the mesh with itself at the wavenumbers ks into
+        f[first:first+len(ks)] (one launch for all of them on the Rankine-reuse
+        path when every wavenumber is finite and > 0)."""
         gf = self.green_function
         n = mesh.nb_faces
+        lds = n if lds is None else lds
+        ks = [float(k) for k in ks]
+        if len(ks) > 1 and all(0.0 < k < np.inf for k in ks):
+            gf.assemble_into(mesh, mesh, f.S[first], f.K[first], wavenumber=ks[0], lds=lds, ldk=f.ldk,
+                             nan_flag=nan_flag, precision=self.assembly_precision, reuse_rankine=reuse_rankine,
+                             sweep=(ks, f.S.shape[1], f.K.shape[1]))
+            return
         for b, k in enumerate(ks):
-            gf.assemble_into(mesh, mesh, f.S[b], f.K[b], wavenumber=float(k), lds=n, ldk=f.ldk, nan_flag=nan_flag,
-                             precision=self.assembly_precision, reuse_rankine=reuse_rankine)
+            gf.assemble_into(mesh, mesh, f.S[first + b], f.K[first + b], wavenumber=k, lds=lds, ldk=f.ldk,
+                             nan_flag=nan_flag, precision=self.assembly_precision, reuse_rankine=reuse_rankine)
 
     def factor_stage(self, f: "_Factors", nb, err):
         """LU of K (float64 DMMA, or float32 tcgen05 for the mixed engine); none for plain GMRES."""
@@ -369,30 +379,49 @@ class B200Engine:
         integrals for the frequencies om (f[0:len(om)]); returns host arrays
         F (nb, nrhs, ndof) and FK (nb, nhead, ndof).  Raises the reference's
         exceptions on NaN, zero pivot or non-convergence."""
+        ndof = len(body.dofs)
+        if r.nrhs != ndof + len(heads) or r.batch < len(om):
+            raise ValueError("right-hand side buffers of the wrong shape")
+        (F, FK), = self._solve_segments(f, r, [(body, 0, len(om))], om, heads, rho=rho, g=g, stats=stats,
+                                        events=events)
+        return F, FK
+
+    def _solve_segments(self, f: "_Factors", r: "_Rhs", segments, om, heads, *, rho=1000.0, g=9.81, stats=None,
+                        events=None):
+        """solve_stage for batch entries holding several bodies: segments
+        [(body, j0, m)] give the body of entries j0 .. j0+m-1.  A body smaller
+        than the system (f.n, identity-padded) has zero right-hand-side rows
+        beyond its panels; bodies with fewer dofs than r.nrhs - nhead have zero
+        columns.  Returns [(F (m, nrhs, ndof), FK (m, nhead, ndof))] per segment."""
         import torch
         lib = _lib.load()
         stream = _lib.stream_ptr()
         dev = f.K.device
         stats = {} if stats is None else stats
-        mesh = body.mesh_including_lid
         n, npad = f.n, f.npad
         om = np.asarray(om, dtype=float)
         nb = len(om)
         ks = om ** 2 / g
         heads = np.asarray(heads, dtype=float)
-        ndof, nhead = len(body.dofs), len(heads)
-        nrhs = ndof + nhead
-        if r.nrhs != nrhs or r.batch < nb:
-            raise ValueError("right-hand side buffers of the wrong shape")
-        dm = self.green_function.device_mesh(mesh)
-        dofn, wdof, hull = self._body_arrays(body, mesh)
+        nhead = len(heads)
+        nrhs = r.nrhs
+        ld = npad * nrhs  # batch stride of B, X, R
         small = torch.as_tensor(np.concatenate([om, ks, heads]), dtype=torch.float64, device=dev)
         om_t, k_t, heads_t = small[:nb], small[nb:2 * nb], small[2 * nb:]
         r.B.zero_()
-        _lib.check(lib.bem_build_rhs(n, nb, _vp(om_t), _vp(k_t), g, ndof, _vp(dofn), nhead, _vp(heads_t),
-                                     _vp(dm.centers), _vp(dm.normals), _vp(hull), _vp(r.B), npad, npad * nrhs,
-                                     stream))
-        ld = npad * nrhs  # batch stride of B, X, R
+        seg_arrays = []
+        for body, j0, m in segments:
+            mesh = body.mesh_including_lid
+            ndof = len(body.dofs)
+            if ndof + nhead > nrhs or mesh.nb_faces > n:
+                raise ValueError("right-hand side buffers of the wrong shape")
+            dm = self.green_function.device_mesh(mesh)
+            dofn, wdof, hull = self._body_arrays(body, mesh)
+            seg_arrays.append((mesh.nb_faces, ndof, dm, wdof))
+            _lib.check(lib.bem_build_rhs(mesh.nb_faces, m, _vp(om_t.data_ptr() + 8 * j0),
+                                         _vp(k_t.data_ptr() + 8 * j0), g, ndof, _vp(dofn), nhead, _vp(heads_t),
+                                         _vp(dm.centers), _vp(dm.normals), _vp(hull),
+                                         _vp(r.B.data_ptr() + 16 * j0 * ld), npad, ld, stream))
         sol = r.B if (self.precision == "fp64" and not self._plain_gmres) else r.X
         for c0 in range(0, nrhs, RHS_CHUNK):
             nc = min(RHS_CHUNK, nrhs - c0)
@@ -412,14 +441,19 @@ class B200Engine:
             _lib.check(lib.bem_zgemm_ts(n, n, nc, 1.0, 0.0, _vp(f.S), n, n * n, _vp(sol.data_ptr() + 16 * npad * c0),
                                         npad, ld, 0.0, 0.0, _vp(r.phi.data_ptr() + 16 * n * c0), n, n * nrhs, nb,
                                         _vp(r.ts_work), stream))
-        out = torch.empty((nb * nrhs * ndof + nb * max(nhead, 1) * ndof,), dtype=torch.complex128, device=dev)
-        F = out[:nb * nrhs * ndof]
-        FK = out[nb * nrhs * ndof:]
-        _lib.check(lib.bem_integrate_pressure(n, nb, nrhs, ndof, _vp(r.phi), n, n * nrhs, _vp(om_t), rho,
-                                              _vp(wdof), _vp(F), stream))
-        if nhead > 0:
-            _lib.check(lib.bem_froude_krylov(n, nb, ndof, nhead, _vp(k_t), rho, g, _vp(heads_t), _vp(dm.centers),
-                                             _vp(wdof), _vp(FK), stream))
+        sizes = [(m * nrhs * na[1], m * max(nhead, 1) * na[1]) for (_, _, m), na in zip(segments, seg_arrays)]
+        out = torch.empty((sum(a + b for a, b in sizes),), dtype=torch.complex128, device=dev)
+        views, pos = [], 0
+        for (body, j0, m), (nf, ndof, dm, wdof), (sf, sk) in zip(segments, seg_arrays, sizes):
+            F, FK = out[pos:pos + sf], out[pos + sf:pos + sf + sk]
+            pos += sf + sk
+            views.append((m, ndof, sf))
+            _lib.check(lib.bem_integrate_pressure(nf, m, nrhs, ndof, _vp(r.phi.data_ptr() + 16 * j0 * n * nrhs), n,
+                                                  n * nrhs, _vp(om_t.data_ptr() + 8 * j0), rho, _vp(wdof), _vp(F),
+                                                  stream))
+            if nhead > 0:
+                _lib.check(lib.bem_froude_krylov(nf, m, ndof, nhead, _vp(k_t.data_ptr() + 8 * j0), rho, g,
+                                                 _vp(heads_t), _vp(dm.centers), _vp(wdof), _vp(FK), stream))
         if events:
             events[4].record()
         host = out.cpu().numpy()
@@ -432,9 +466,102 @@ class B200Engine:
                                            f"zero pivot in the LU factorisation (info={flags[:nb].tolist()})")
         if flags[nb] != 0:
             raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
-        F_h = host[:nb * nrhs * ndof].reshape(nb, nrhs, ndof)
-        FK_h = host[nb * nrhs * ndof:].reshape(nb, max(nhead, 1), ndof)[:, :nhead]
-        return F_h, FK_h
+        res, pos = [], 0
+        for (m, ndof, sf), (_, sk) in zip(views, sizes):
+            F_h = host[pos:pos + sf].reshape(m, nrhs, ndof)[:, :ndof + nhead]
+            FK_h = host[pos + sf:pos + sf + sk].reshape(m, max(nhead, 1), ndof)[:, :nhead]
+            pos += sf + sk
+            res.append((F_h, FK_h))
+        return res
+
+    # ---- many bodies --------------------------------------------------------
+    def solve_bodies(self, bodies, omegas: Sequence[float], *, wave_directions: Sequence[float] = (0.0,),
+                     rho: float = 1000.0, g: float = 9.81, batch_bytes: float = 8e9,
+                     sync_stats: bool = False) -> List[FrequencyResults]:
+        """Frequency sweeps of many bodies of uneven panel counts, batched
+        across bodies: bodies whose size rounds up to the same multiple of the
+        LU block (128 for the mixed engine, 64 for float64) form one group,
+        every matrix of the group is identity-padded to that size (the padded
+        unknowns are zero and change nothing), and the (body, omega) pairs of a
+        group are assembled, factored and solved in batches of as many matrices
+        as fit in batch_bytes.  Returns one FrequencyResults per body, in order
+        (what solve_frequencies returns for that body).  With max_batch or more
+        frequencies a body fills batches of its own: each body then runs its
+        own sweep (measured faster: no padding, and a frequency that needs the
+        GMRES fallback holds up its own batch only)."""
+        import torch
+        omegas = np.asarray(omegas, dtype=float)
+        if len(omegas) >= self.max_batch:
+            return [self.solve_frequencies(b, omegas, wave_directions=wave_directions, rho=rho, g=g)
+                    for b in bodies]
+        heads = np.asarray(wave_directions, dtype=float)
+        nhead = len(heads)
+        blk = 128 if self.precision == "mixed" else 64
+        groups: Dict[int, List[int]] = {}
+        for i, b in enumerate(bodies):
+            n = b.mesh_including_lid.nb_faces
+            groups.setdefault(-(-n // blk) * blk, []).append(i)
+        F_all = [np.zeros((len(omegas), len(b.dofs) + nhead, len(b.dofs)), dtype=np.complex128) for b in bodies]
+        FK_all = [np.zeros((len(omegas), max(nhead, 1), len(b.dofs)), dtype=np.complex128) for b in bodies]
+        stats = {"groups": len(groups), "batches": 0, "assembly_ms": 0.0, "lu_ms": 0.0, "solve_ms": 0.0}
+        lib = _lib.load()
+        stream = _lib.stream_ptr()
+        plan = []
+        for npad, idxs in sorted(groups.items()):
+            nrhs = max(len(bodies[i].dofs) for i in idxs) + nhead
+            pairs = [(i, q) for i in idxs for q in range(len(omegas))]
+            B = int(max(1, min(len(pairs), batch_bytes // _Factors.estimate_bytes(npad, 1, self.precision))))
+            need = (_Factors.estimate_bytes(npad, B, self.precision) + _Rhs.estimate_bytes(npad, npad, B, nrhs)
+                    + 64 * (1 << 16))
+            plan.append((npad, idxs, nrhs, pairs, B, need))
+        # one arena for the largest group: no device allocation between groups
+        arena = DeviceArena(max(p[-1] for p in plan), self.device)
+        for npad, idxs, nrhs, pairs, B, _ in plan:
+            alloc, release = arena.allocator()
+            f = _Factors(npad, B, self.device, self.precision, alloc=alloc)
+            r = _Rhs(npad, npad, B, nrhs, self.device, self.precision, alloc=alloc)
+            for start in range(0, len(pairs), B):
+                chunk = pairs[start:start + B]
+                nb = len(chunk)
+                segments = []
+                for j, (i, q) in enumerate(chunk):
+                    if segments and segments[-1][0] is bodies[i]:
+                        segments[-1][2] += 1
+                    else:
+                        segments.append([bodies[i], j, 1])
+                om = omegas[[q for _, q in chunk]]
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)] if sync_stats else None
+                if ev:
+                    ev[0].record()
+                r.flags.zero_()
+                for body, j0, m in segments:
+                    mesh = body.mesh_including_lid
+                    self.assemble_stage(f, mesh, om[j0:j0 + m] ** 2 / g, nan_flag=r.nan, first=j0, lds=npad)
+                    if mesh.nb_faces < npad:
+                        for M in (f.S, f.K):  # zero rows/columns, unit diagonal beyond the body's panels
+                            _lib.check(lib.bem_zpad_identity(_vp(M.data_ptr() + 16 * j0 * npad * npad), npad,
+                                                             npad * npad, m, mesh.nb_faces, npad, stream))
+                if ev:
+                    ev[1].record()
+                self.factor_stage(f, nb, r.err)
+                if ev:
+                    ev[2].record()
+                out = self._solve_segments(f, r, [tuple(sg) for sg in segments], om, heads, rho=rho, g=g,
+                                           stats=stats, events=ev)
+                for (body, j0, m), (F, FK) in zip(segments, out):
+                    i = chunk[j0][0]
+                    qs = [q for _, q in chunk[j0:j0 + m]]
+                    F_all[i][qs] = F
+                    FK_all[i][qs, :nhead] = FK
+                stats["batches"] += 1
+                if ev:
+                    torch.cuda.synchronize()
+                    stats["assembly_ms"] += ev[0].elapsed_time(ev[1])
+                    stats["lu_ms"] += ev[1].elapsed_time(ev[2])
+                    stats["solve_ms"] += ev[2].elapsed_time(ev[4])
+            del f, r
+            release()  # the group's work has completed: its results were copied to the host
+        return [self._coefficients(b, omegas, heads, F_all[i], FK_all[i], dict(stats)) for i, b in enumerate(bodies)]
 
     def _refine(self, f, r, nb, Bc, Xc, Rc, nc, stats, stream):
         """Refined solve of nc columns (B, X, R column pointers, batch stride

@@ -287,11 +287,15 @@ class Delhommeau:
     def assemble_into(self, mesh1, mesh2, S, K, *, free_surface=0.0, water_depth=np.inf, wavenumber=1.0,
                       adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True,
                       lds=None, ldk=None, k_plane_stride=None, precision=None, stream=None, nan_flag=None,
-                      reuse_rankine=True):
+                      reuse_rankine=True, sweep=None):
         """Write S and K into caller-owned device buffers (column-major with
         leading dimensions lds/ldk) through ``bem_assemble``.  For a mesh with
         itself the wavenumber-independent Rankine part is kept and reused
-        across calls unless reuse_rankine is False."""
+        across calls unless reuse_rankine is False.  sweep = (wavenumbers,
+        s_stride, k_stride): S and K of every wavenumber (finite, > 0; the
+        variant is chosen with the first), the outputs of wavenumber i at
+        S + i * s_stride and K + i * k_stride elements, in one launch per 64
+        wavenumbers on the Rankine-reuse path."""
         import torch
         if water_depth != np.inf:
             raise NotImplementedError("finite water depth is outside the B200 path (infinite depth only)")
@@ -350,7 +354,24 @@ class Delhommeau:
             a.points_dev = a.centers_dev = a.quad_points_dev = q
             rank = self._rankine_part(mesh2.content_hash, dm2, a, bool(adjoint_double_layer), sing,
                                       float(free_surface), stream)
+            if sweep is not None:
+                ks, s_stride, k_stride = sweep
+                kh = np.ascontiguousarray(np.asarray(ks, dtype=np.float64))
+                _lib.check(lib.bem_assemble_wave_symmetric_batched(a, rank.data_ptr(), n,
+                                                                   kh.ctypes.data_as(_lib.c_void_p), len(kh),
+                                                                   int(s_stride), int(k_stride),
+                                                                   _lib.stream_ptr(stream)))
+                return
             _lib.check(lib.bem_assemble_wave_symmetric(a, rank.data_ptr(), n, _lib.stream_ptr(stream)))
+            return
+        if sweep is not None:
+            ks, s_stride, k_stride = sweep
+            esize = S.element_size()
+            for i, k in enumerate(ks):
+                a.wavenumber = float(k)
+                a.S_dev = S.data_ptr() + i * int(s_stride) * esize
+                a.K_dev = K.data_ptr() + i * int(k_stride) * esize
+                _lib.check(lib.bem_assemble(a, _lib.stream_ptr(stream)))
             return
         _lib.check(lib.bem_assemble(a, _lib.stream_ptr(stream)))
 

@@ -150,6 +150,16 @@ int bem_assemble_rankine_part(const bem_assembly_args* args, void* out_dev, int6
  * precision and complex128 outputs. */
 int bem_assemble_wave_symmetric(const bem_assembly_args* args, const void* rankine_dev, int64_t ld, void* stream);
 
+/* bem_assemble_wave_symmetric for nk wavenumbers (host array) in one launch per
+ * 64 of them (a small mesh alone does not fill the GPU): the outputs of
+ * wavenumber i are args->S_dev + i * s_stride and args->K_dev + i * k_stride
+ * (complex128 elements); args->wavenumber is not used.  Same results as nk
+ * calls of bem_assemble_wave_symmetric.  No counterpart in the reference
+ * (matrices.f90:28-432 is called once per wavenumber). */
+int bem_assemble_wave_symmetric_batched(const bem_assembly_args* args, const void* rankine_dev, int64_t ld,
+                                        const double* wavenumbers_host, int nk, int64_t s_stride, int64_t k_stride,
+                                        void* stream);
+
 /* ---- dense complex128 linear algebra (batched) ---------------------------- */
 /* Matrices are column-major complex128 (interleaved re, im), `batch` of them
  * `stride` elements apart.  n must be a multiple of 64: pad the system with the

@@ -92,3 +92,33 @@ def test_padded_leading_dimensions(default_oracle_gf, tmp_path):
     _close(S[:, :n].cpu().numpy().T, S_ref)
     _close(K[:, :n].cpu().numpy().T, K_ref)
     assert torch.all(S[:, n:] == complex(7, 7)) and torch.all(K[:, n:] == complex(7, 7))
+
+
+@pytest.mark.parametrize("mesh_name", sorted(MESHES))
+def test_batched_wavenumbers_equal_single_calls(default_oracle_gf, tmp_path, mesh_name):
+    """bem_assemble_wave_symmetric_batched (one launch for several wavenumbers,
+    outputs strided, leading dimension larger than n) writes exactly what one
+    call per wavenumber writes; the general kernel's sweep loop agrees too."""
+    import torch
+    mesh = MESHES[mesh_name]()
+    n = mesh.nb_faces
+    ld = n + 5
+    ks = [0.05, 0.7, 1.3, 40.0]
+    out = {}
+    for name, cache in (("fast", 4 << 30), ("general", 0)):
+        gf = _gf(default_oracle_gf, tmp_path)
+        gf.rankine_cache_bytes = cache
+        S = torch.full((len(ks), ld * n), float("nan"), dtype=torch.complex128, device="cuda")
+        K = torch.full_like(S, float("nan"))
+        gf.assemble_into(mesh, mesh, S[0], K[0], wavenumber=ks[0], lds=ld, ldk=ld, sweep=(ks, ld * n, ld * n))
+        S1, K1 = torch.empty_like(S), torch.empty_like(K)
+        for i, k in enumerate(ks):
+            gf.assemble_into(mesh, mesh, S1[i], K1[i], wavenumber=k, lds=ld, ldk=ld)
+        torch.cuda.synchronize()
+        sv = S.reshape(len(ks), n, ld)[:, :, :n]
+        kv = K.reshape(len(ks), n, ld)[:, :, :n]
+        assert torch.equal(sv, S1.reshape(len(ks), n, ld)[:, :, :n])
+        assert torch.equal(kv, K1.reshape(len(ks), n, ld)[:, :, :n])
+        out[name] = (sv.cpu().numpy(), kv.cpu().numpy())
+    _close(out["fast"][0], out["general"][0])
+    _close(out["fast"][1], out["general"][1])

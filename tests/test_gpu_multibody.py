@@ -46,3 +46,31 @@ def test_two_cylinders_with_lids_against_oracle(oracle_mod, default_oracle_gf, t
                                       hull_mask=body.hull_mask) for w in omegas]
     errs = coefficient_errors(res, ref, body.dofs)
     assert max(errs.values()) < (1e-6 if precision == "fp64" else 1e-5), errs
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_many_bodies_batched_across_bodies(default_oracle_gf, tmp_path, precision):
+    """solve_bodies (bodies of uneven sizes sharing identity-padded batches,
+    different dof counts) gives each body what solve_frequencies gives it."""
+    from capytaine_b200.engine import B200Engine
+    from capytaine_b200.meshes import mesh_ellipsoid, mesh_sphere
+    from test_gpu_mixed import _shared_table_gf
+    gf = _shared_table_gf(default_oracle_gf, tmp_path)
+    bodies = [
+        FloatingBody(mesh_sphere(radius=1.0, resolution=(10, 20)).immersed_part(), rigid_body_dofs(), name="a"),
+        FloatingBody(mesh_ellipsoid(semi_axes=(2.0, 1.0, 1.5), resolution=(10, 22)).immersed_part(),
+                     rigid_body_dofs(only=["Heave", "Pitch"]), name="b"),
+        FloatingBody(mesh_vertical_cylinder(length=6.0, radius=1.5, resolution=(3, 20, 10)).immersed_part(),
+                     rigid_body_dofs(only=["Surge", "Heave", "Yaw"]), name="c"),
+    ]
+    omegas = [0.5, 1.4, 2.9]
+    eng = B200Engine(green_function=gf, precision=precision)
+    together = eng.solve_bodies(bodies, omegas, wave_directions=(0.0, np.pi / 4), batch_bytes=3e8)
+    assert together[0].stats["groups"] >= 2
+    tol = 1e-10 if precision == "fp64" else 1e-8
+    for b, res in zip(bodies, together):
+        alone = eng.solve_frequencies(b, omegas, wave_directions=(0.0, np.pi / 4))
+        for name in ("added_mass", "radiation_damping", "excitation"):
+            a, s = getattr(res, name), getattr(alone, name)
+            assert a.shape == s.shape
+            assert np.abs(a - s).max() <= tol * np.abs(s).max(), (b.name, name)
