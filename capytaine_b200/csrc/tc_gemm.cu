@@ -15,9 +15,12 @@
 // columns: real parts then imaginary parts).  Warp 0 streams operand slices
 // with TMA (128-byte swizzle) through a 2-stage shared-memory ring (two CTAs
 // per SM, so that one CTA's epilogue overlaps the other's MMAs), one thread
-// of warp 1 issues tcgen05.mma (M=128, N=256, K=8 per instruction), warps 2-5
+// of warp 1 issues tcgen05.mma (M=128, N=256, K=8 per instruction), warps 2-9
 // read the accumulator back with tcgen05.ld and apply C -= acc in place, the
-// loads of C running ahead of the accumulator reads.
+// loads of C running ahead of the accumulator reads: two warps per 32-lane
+// quarter of the accumulator, one for the real plane and one for the imaginary
+// plane, so that twice as many loads of C are in flight (the update is bound
+// by the read and write of C).
 // Every mbarrier wait is bounded; on timeout the kernel records an error and
 // still drains its own copies before freeing tensor memory.
 #include <cuda.h>
@@ -149,7 +152,9 @@ struct UpdateArgs {
   int store;         // 0: C -= A B;  1: C = A B (C is not read)
 };
 
-__global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
+constexpr int kThreads = 320;  // producer warp, MMA warp, 8 epilogue warps
+
+__global__ void __launch_bounds__(kThreads, 2) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
                                                                    const __grid_constant__ CUtensorMap mapB,
                                                                    UpdateArgs p) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -224,13 +229,15 @@ __global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_
       mma_commit(accf);
     }
   } else {
-    // epilogue warps 2..5: TMEM lanes 32*(warp % 4) .. +31.  The C tile is read
-    // in 16 chunks of 16 columns through a register double buffer: chunk 0 is
-    // loaded while the MMAs run, chunk i+1 while chunk i is applied.
+    // epilogue warps 2..9: TMEM lanes 32*(warp % 4) .. +31; warps 2-5 take the
+    // real plane (accumulator columns 0..127), warps 6-9 the imaginary plane.
+    // Each reads its plane in 8 chunks of 16 columns through a register double
+    // buffer: the first chunk is loaded while the MMAs run, chunk i+1 while
+    // chunk i is applied.
     constexpr int kCW = 16;                // columns per chunk
-    constexpr int kChunks = kTN / kCW;     // 16 (8 real, 8 imaginary)
     constexpr int kPlaneChunks = kTNc / kCW;
     const int q = warp & 3;
+    const int first = ((warp - 2) >> 2) * kPlaneChunks, last = first + kPlaneChunks;
     const int row = p.c_row0 + tm * kTM + 32 * q + lane;
     float* Cr = p.Cr + (size_t)b * p.c_stride + row;
     float* Ci = p.Ci + (size_t)b * p.c_stride + row;
@@ -244,7 +251,7 @@ __global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_
 #pragma unroll
     for (int j = 0; j < kCW; ++j) cb0[j] = cb1[j] = 0.0f;
     if (rd) {
-      const float* src = at(0);
+      const float* src = at(first);
 #pragma unroll
       for (int j = 0; j < kCW; ++j) cb0[j] = __ldcs(src + j * ldc);
     }
@@ -254,7 +261,7 @@ __global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_
     if (ok) {
       const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16);
 #pragma unroll 1
-      for (int chunk = 0; chunk < kChunks; chunk += 2) {
+      for (int chunk = first; chunk < last; chunk += 2) {
         if (rd) {
           const float* src = at(chunk + 1);
 #pragma unroll
@@ -267,7 +274,7 @@ __global__ void __launch_bounds__(192, 2) cgemm_tf32_update_kernel(const __grid_
 #pragma unroll
           for (int j = 0; j < kCW; ++j) __stcs(dst + j * ldc, rd ? cb0[j] - v[j] : v[j]);
         }
-        if (rd && chunk + 2 < kChunks) {
+        if (rd && chunk + 2 < last) {
           const float* src = at(chunk + 2);
 #pragma unroll
           for (int j = 0; j < kCW; ++j) cb0[j] = __ldcs(src + j * ldc);
@@ -345,7 +352,7 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
   dim3 grid(m / kTM, n / kTNc, batch);
   {
     TimedLaunch tl(kKCgemmTf32, stream);
-    cgemm_tf32_update_kernel<<<grid, 192, smem, stream>>>(mapA, mapB, p);
+    cgemm_tf32_update_kernel<<<grid, kThreads, smem, stream>>>(mapA, mapB, p);
   }
   count_launches(1);
   BEM_CUDA_CHECK(cudaGetLastError());
