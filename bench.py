@@ -433,7 +433,8 @@ def kernel_roofline(kernels, n, frequencies, engine, peaks, peak_src):
         return base | {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
                        "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run (TF32 has no entry in "
                                       "MEASURED_PEAKS.json)",
-                       "algorithmic": "8 m^2 128 real flops per complex update of m x m by depth 128",
+                       "algorithmic": "8 m^2 k real flops per complex update of m x m by depth k (the LU "
+                                      "applies two block steps of 128 per pass: k = 256 beyond the strips)",
                        "traffic": flops * CGEMM_DRAM_BYTES_PER_FLOP,
                        "traffic_note": "DRAM bytes per launch, ncu capture of an m=4736 launch scaled by flops",
                        "hbm_bound_frac": (flops * CGEMM_DRAM_BYTES_PER_FLOP / avg_s / 1e9) / peaks["hbm_gbs"]}

@@ -28,7 +28,8 @@ namespace bem {
 
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
-                      int n, int batch, int* err, cudaStream_t stream, int store = 0);
+                      int n, int batch, int* err, cudaStream_t stream, int store = 0, const float* Aop1 = nullptr,
+                      const float* Bop1 = nullptr);
 int zgemm_ts_enqueue(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
                      int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,
                      double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev,
@@ -40,6 +41,7 @@ constexpr int kB = 128;        // LU block
 constexpr int kPT = 64;        // panel tile width
 constexpr int kSplitK = 6 * kB;  // K' of the split-TF32 panel product: (hi, lo, hi) x (re, im) x 128
 constexpr int kRhs = 16;       // right-hand sides per solve launch
+constexpr int kOpBuffers = 3;  // packed operands of the current, previous and next block steps
 constexpr long long kSpin = 4000000;
 
 __device__ __forceinline__ float2 fmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
@@ -578,10 +580,10 @@ MixedWork carve(void* work, int npad, int batch) {
   MixedWork w;
   w.W = (float*)p;
   p += (size_t)batch * 2 * npad * npad * sizeof(float);
-  w.Aop = (float*)p;  // two buffers of batch x npad x 256
-  p += 2 * (size_t)batch * npad * 2 * kB * sizeof(float);
-  w.Bop = (float*)p;  // two buffers of batch x 2 npad x 256
-  p += 2 * (size_t)batch * 2 * npad * 2 * kB * sizeof(float);
+  w.Aop = (float*)p;  // three buffers of batch x npad x 256
+  p += kOpBuffers * (size_t)batch * npad * 2 * kB * sizeof(float);
+  w.Bop = (float*)p;  // three buffers of batch x 2 npad x 256
+  p += kOpBuffers * (size_t)batch * 2 * npad * 2 * kB * sizeof(float);
   w.inv = (float2*)p;
   p += (size_t)batch * nblk * kB * kB * sizeof(float2);
   w.binv = (float*)p;
@@ -634,8 +636,8 @@ using namespace bem;
 extern "C" int64_t bem_clu_workspace_bytes(int npad, int batch) {
   if (npad <= 0 || npad % kB || batch <= 0) return -1;
   const int64_t nblk = npad / kB;
-  return (int64_t)batch * 2 * npad * (int64_t)npad * 4 + 2 * (int64_t)batch * npad * 2 * kB * 4 +
-         2 * (int64_t)batch * 2 * npad * 2 * kB * 4 + (int64_t)batch * nblk * kB * kB * 8 +
+  return (int64_t)batch * 2 * npad * (int64_t)npad * 4 + kOpBuffers * (int64_t)batch * npad * 2 * kB * 4 +
+         kOpBuffers * (int64_t)batch * 2 * npad * 2 * kB * 4 + (int64_t)batch * nblk * kB * kB * 8 +
          (int64_t)batch * (2 * kB) * kSplitK * 4 + (int64_t)batch * npad * kSplitK * 4 +
          ((int64_t)batch * nblk + 2) * 4 + 1024;
 }
@@ -659,8 +661,8 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
                                                                            npad, W);
   ++launches;
   const size_t abuf = (size_t)batch * npad * 2 * kB, bbuf = (size_t)batch * 2 * npad * 2 * kB;
-  float* Aop[2] = {w.Aop, w.Aop + abuf};
-  float* Bop[2] = {w.Bop, w.Bop + bbuf};
+  float* Aop[kOpBuffers] = {w.Aop, w.Aop + abuf, w.Aop + 2 * abuf};
+  float* Bop[kOpBuffers] = {w.Bop, w.Bop + bbuf, w.Bop + 2 * bbuf};
   // Inverse of the diagonal block, then the panel: A12 and A21 packed, L21 =
   // A21 A_kk^{-1} on the tensor cores into the working matrix, L21 packed.
   auto diag_and_panel = [&](int kk, int buf, cudaStream_t on) -> int {
@@ -687,29 +689,40 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
     return BEM_OK;
   };
   // C rows r0.. (m), complex columns c0.. (nc) -= L21 U12 of the block step whose
-  // packed operands are in buffer buf.
-  auto update = [&](int buf, int r0, int c0, int m, int nc) -> int {
+  // packed operands are in buffer buf, and of a second step (buffer buf2 >= 0)
+  // in the same pass over C (depth 256).
+  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2) -> int {
     if (m <= 0 || nc <= 0) return BEM_OK;
     return cgemm_tf32_update(Aop[buf], npad, r0, Bop[buf], 2 * (int64_t)npad, 2 * c0, 2 * kB, W.re, W.im, npad,
-                             W.stride, r0, c0, m, nc, batch, err_dev, s);
+                             W.stride, r0, c0, m, nc, batch, err_dev, s, 0, buf2 >= 0 ? Aop[buf2] : nullptr,
+                             buf2 >= 0 ? Bop[buf2] : nullptr);
   };
   Lookahead* la = nullptr;
   if ((st = lookahead_for(s, &la))) return st;
   std::lock_guard<std::mutex> lock(la->mu);
-  // Right-looking block LU with a lookahead of one block: after the strips of
-  // step k that block k+1 needs (its block row and block column), the inverse
-  // and panel of block k+1 run on the side stream while the rest of the
-  // trailing update of step k runs on the caller's stream.
+  // Right-looking block LU with a lookahead of one block, the trailing updates
+  // of two consecutive block steps applied in one pass over C (depth 256: the
+  // update is bound by reading and writing C).  Step k: the strips that block
+  // k+1 needs (its block row and block column) get every update still
+  // pending on them, then the inverse and panel of block k+1 run on the side
+  // stream while, at every second step, the rest of the trailing matrix gets
+  // the updates of steps k-1 and k together.  Operands of steps k-1, k, k+1
+  // live in three buffers.
   if ((st = diag_and_panel(0, 0, s))) return st;
   for (int kk = 0, step = 0; kk + kB < npad; kk += kB, ++step) {
-    const int cur = step & 1, kn = kk + kB, rest = npad - kn - kB;
-    if ((st = update(cur, kn, kn, kB, npad - kn))) return st;  // block row kn
-    if ((st = update(cur, kn + kB, kn, rest, kB))) return st;  // block column kn below the diagonal
+    const int cur = step % kOpBuffers, prev = (step + kOpBuffers - 1) % kOpBuffers;
+    const int nxt = (step + 1) % kOpBuffers;
+    const int kn = kk + kB, rest = npad - kn - kB;
+    const int pend = (step & 1) ? prev : -1;  // step k-1 still pending beyond block k
+    if ((st = update(cur, kn, kn, kB, npad - kn, pend))) return st;  // block row kn
+    if ((st = update(cur, kn + kB, kn, rest, kB, pend))) return st;  // block column kn below the diagonal
     BEM_CUDA_CHECK(cudaEventRecord(la->strips, s));
     BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->strips, 0));
-    if ((st = diag_and_panel(kn, cur ^ 1, la->side))) return st;
+    if ((st = diag_and_panel(kn, nxt, la->side))) return st;
     BEM_CUDA_CHECK(cudaEventRecord(la->panel, la->side));
-    if ((st = update(cur, kn + kB, kn + kB, rest, rest))) return st;
+    if (step & 1) {
+      if ((st = update(cur, kn + kB, kn + kB, rest, rest, prev))) return st;
+    }
     BEM_CUDA_CHECK(cudaStreamWaitEvent(s, la->panel, 0));
   }
   count_launches(launches);

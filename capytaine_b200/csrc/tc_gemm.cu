@@ -144,6 +144,7 @@ struct UpdateArgs {
   int c_row0;        // first row of the trailing block in C
   int c_col0;        // first complex column of the trailing block in C
   int nk;            // K' / kKC
+  int nk0;           // chunks read from the first operand pair; the rest from the second
   float* Cr;
   float* Ci;
   int64_t ldc;
@@ -156,6 +157,8 @@ constexpr int kThreads = 320;  // producer warp, MMA warp, 8 epilogue warps
 
 __global__ void __launch_bounds__(kThreads, 2) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
                                                                    const __grid_constant__ CUtensorMap mapB,
+                                                                   const __grid_constant__ CUtensorMap mapA1,
+                                                                   const __grid_constant__ CUtensorMap mapB1,
                                                                    UpdateArgs p) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte alignment of the operand ring (128-byte swizzle atoms)
@@ -201,8 +204,11 @@ __global__ void __launch_bounds__(kThreads, 2) cgemm_tf32_update_kernel(const __
         if (kc >= kStages) ok = mbar_wait(&empty[s], ((kc / kStages) - 1) & 1, p.err);
         if (!ok) break;
         mbar_expect_tx(&full[s], kStageBytes);
-        tma_load_3d(ringA + s * kABytes, &mapA, kc * kKC, p.a_row0 + tm * kTM, b, &full[s]);
-        tma_load_3d(ringB + s * kBBytes, &mapB, kc * kKC, p.b_row0 + tn * kTN, b, &full[s]);
+        // K' chunks [0, nk0) from the first operand pair, the rest from the second
+        const bool first = kc < p.nk0;
+        const int kx = (first ? kc : kc - p.nk0) * kKC;
+        tma_load_3d(ringA + s * kABytes, first ? &mapA : &mapA1, kx, p.a_row0 + tm * kTM, b, &full[s]);
+        tma_load_3d(ringB + s * kBBytes, first ? &mapB : &mapB1, kx, p.b_row0 + tn * kTN, b, &full[s]);
         issued = kc + 1;
       }
       // drain: every issued copy must land before the CTA may exit
@@ -334,25 +340,34 @@ bool g_tc_configured = false;
 // of 128) -= A' B' for `batch` matrices.
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
-                      int n, int batch, int* err, cudaStream_t stream, int store) {
+                      int n, int batch, int* err, cudaStream_t stream, int store, const float* Aop1,
+                      const float* Bop1) {
   if (m <= 0 || n <= 0) return BEM_OK;
   if (m % kTM || n % kTNc || kp % kKC || (a_row0 % 8) || (b_row0 % 8))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: sizes must be multiples of 128 (K' of 32)");
-  CUtensorMap mapA, mapB;
+  if ((Aop1 == nullptr) != (Bop1 == nullptr))
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: second operand pair incomplete");
+  CUtensorMap mapA, mapB, mapA1, mapB1;
   int st = make_operand_map(&mapA, Aop, kp, a_rows, batch, kTM);
   if (st) return st;
   st = make_operand_map(&mapB, Bop, kp, b_rows, batch, kTN);
+  if (st) return st;
+  // second pair (same shapes, the next K' block): C -= A B - A1 B1 in one pass over C
+  st = make_operand_map(&mapA1, Aop1 ? Aop1 : Aop, kp, a_rows, batch, kTM);
+  if (st) return st;
+  st = make_operand_map(&mapB1, Bop1 ? Bop1 : Bop, kp, b_rows, batch, kTN);
   if (st) return st;
   const int smem = kStages * kStageBytes + 1024 + 256;
   if (!g_tc_configured) {
     BEM_CUDA_CHECK(cudaFuncSetAttribute(cgemm_tf32_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     g_tc_configured = true;
   }
-  UpdateArgs p{a_row0, b_row0, c_row0, c_col0, kp / kKC, Cr, Ci, ldc, c_stride, err, store};
+  const int nk0 = kp / kKC;
+  UpdateArgs p{a_row0, b_row0, c_row0, c_col0, Aop1 ? 2 * nk0 : nk0, nk0, Cr, Ci, ldc, c_stride, err, store};
   dim3 grid(m / kTM, n / kTNc, batch);
   {
     TimedLaunch tl(kKCgemmTf32, stream);
-    cgemm_tf32_update_kernel<<<grid, kThreads, smem, stream>>>(mapA, mapB, p);
+    cgemm_tf32_update_kernel<<<grid, kThreads, smem, stream>>>(mapA, mapB, mapA1, mapB1, p);
   }
   count_launches(1);
   BEM_CUDA_CHECK(cudaGetLastError());
@@ -372,5 +387,5 @@ extern "C" int bem_cgemm_tf32_update(const float* Aop_dev, int64_t a_rows, int a
   if ((reinterpret_cast<uintptr_t>(Aop_dev) | reinterpret_cast<uintptr_t>(Bop_dev)) & 15)
     return bem::set_error(BEM_ERR_INVALID_ARGUMENT, "bem_cgemm_tf32_update: operands must be 16-byte aligned");
   return bem::cgemm_tf32_update(Aop_dev, a_rows, a_row0, Bop_dev, b_rows, b_row0, kp, Cr_dev, Ci_dev, ldc, c_stride,
-                                c_row0, c_col0, m, n, batch, err_dev, (cudaStream_t)stream, 0);
+                                c_row0, c_col0, m, n, batch, err_dev, (cudaStream_t)stream, 0, nullptr, nullptr);
 }
