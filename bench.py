@@ -405,10 +405,11 @@ def fp64_tensor_peak_tflops():
 
 
 # DRAM bytes per algorithmic flop of the trailing-update GEMM, from one ncu
-# capture of a full trailing update (m = 4736, 2 matrices: 688.9 MB read +
-# written for 45.9 GFLOP; profiles/cgemm_tf32_update_kernel_barge6084.md); the
-# traffic of the average launch is scaled from it by its flops.
-CGEMM_DRAM_BYTES_PER_FLOP = 688.9e6 / (8 * 4736 ** 2 * 128 * 2)
+# capture of a full trailing update of two block steps (m = 4480, depth 256, 2
+# matrices: 640.0 MB read + written for 82.2 GFLOP;
+# profiles/cgemm_tf32_update_kernel_barge6084.md); the traffic of the average
+# launch is scaled from it by its flops.
+CGEMM_DRAM_BYTES_PER_FLOP = 640.0e6 / (8 * 4480 ** 2 * 256 * 2)
 
 
 def lu_update_flops(npad, block):
@@ -436,7 +437,7 @@ def kernel_roofline(kernels, n, frequencies, engine, peaks, peak_src):
                        "algorithmic": "8 m^2 k real flops per complex update of m x m by depth k (the LU "
                                       "applies two block steps of 128 per pass: k = 256 beyond the strips)",
                        "traffic": flops * CGEMM_DRAM_BYTES_PER_FLOP,
-                       "traffic_note": "DRAM bytes per launch, ncu capture of an m=4736 launch scaled by flops",
+                       "traffic_note": "DRAM bytes per launch, ncu capture of an m=4480 depth-256 launch scaled by flops",
                        "hbm_bound_frac": (flops * CGEMM_DRAM_BYTES_PER_FLOP / avg_s / 1e9) / peaks["hbm_gbs"]}
     if name == "zgemm_dmma_kernel":
         npad = -(-n // 64) * 64
