@@ -12,8 +12,10 @@
 //     tcgen05 tensor cores (TF32 inputs, FP32 accumulation; tc_gemm.cu) from
 //     operands the panel kernel packs.  No row permutation leaves the diagonal
 //     blocks, so the solves need none;
-//   * block substitutions with these factors (persistent kernel, diagonal
-//     inverses applied in the backward sweep);
+//   * block substitutions with these factors (persistent kernel); the block
+//     rows of U are stored pre-multiplied by the diagonal inverses (U' =
+//     A_kk^{-1} A12, computed beside the panel), so that the backward sweep
+//     applies A_ii^{-1} to its own right-hand side before its dependencies;
 //   * iterative refinement: x += LU^{-1} (b - K x) with the residual computed
 //     in float64 against the float64 matrix until the relative residual of
 //     every right-hand side is below the requested tolerance.
@@ -204,7 +206,7 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
 // column-major) = A_kk^{-1}; info flags an exactly zero pivot.
 __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* __restrict__ info,
                                                         float2* __restrict__ inv, int nblk,
-                                                        float* __restrict__ binv) {
+                                                        float* __restrict__ binv, float* __restrict__ ainv) {
   __shared__ float2 colbuf[2][kB];
   __shared__ float2 rowbuf[2][kB];
   __shared__ int s_piv[2];
@@ -236,6 +238,7 @@ __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* _
   // row t: [Re X(:, t) | -Im X(:, t)] per block, row 128 + t: [Im X(:, t) | Re X(:, t)]
   float2* out = inv + ((size_t)b * nblk + kk / kB) * kB * kB;
   float* bo = binv + (size_t)b * (2 * kB) * kSplitK;
+  float* ao = ainv + (size_t)b * kB * 2 * kB;  // row r: [Re A_kk^{-1}(r, :) | Im A_kk^{-1}(r, :)]
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -244,6 +247,8 @@ __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* _
       const int pc = perm[c];
       const float2 v = a[i][m];
       out[r + (size_t)pc * kB] = v;
+      ao[(size_t)r * 2 * kB + pc] = v.x;
+      ao[(size_t)r * 2 * kB + kB + pc] = v.y;
       const float2 hi = make_float2(tf32_hi(v.x), tf32_hi(v.y));
       const float2 lo = make_float2(v.x - hi.x, v.y - hi.y);
       float* rr = bo + (size_t)pc * kSplitK + r;
@@ -343,7 +348,9 @@ __device__ __forceinline__ void st_release_i(int* p, int v) {
 
 // Persistent block substitution with the block LU factors; B complex128 in
 // place.  Forward: y_i = b_i - sum_{j<i} L_ij y_j (unit block lower).  Backward:
-// x_i = A_ii^{-1} (y_i - sum_{j>i} U_ij x_j).  Each CTA owns one 128-row block;
+// x_i = A_ii^{-1} y_i - sum_{j>i} U'_ij x_j with U'_ij = A_ii^{-1} U_ij stored in
+// the factorisation, so each step of the dependency chain is one block product
+// in both sweeps.  Each CTA owns one 128-row block;
 // the off-diagonal block of a dependency is copied to shared memory
 // asynchronously (real and imaginary planes, 16-byte copies) before waiting for
 // that dependency; the diagonal inverse is staged through the same buffer.
@@ -405,6 +412,31 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   const float* Wre = W.re + (size_t)b * W.stride;
   const float* Wim = W.im + (size_t)b * W.stride;
   float2 acc[NC];
+  if (!forward) {
+    // x_i = A_ii^{-1} b_i - sum_j U'_ij x_j with U' = A_ii^{-1} U: the product
+    // with the diagonal inverse comes first, off the chain of dependencies
+    const float2* Inv = inv + ((size_t)b * nblk + i) * kB * kB;
+    for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
+      const float2 v = __ldg(Inv + idx);  // element (idx % 128, idx / 128)
+      Lre[idx] = v.x;
+      Lim[idx] = v.y;
+    }
+    __syncthreads();
+    tile_times_rhs<NC>(Lre, Lim, X, r, h, acc);
+    if (h == 1) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
+    }
+    __syncthreads();
+    if (h == 0) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float2 o = P[r * NC + c];
+        X[r * NC + c] = make_float2(acc[c].x + o.x, acc[c].y + o.y);
+      }
+    }
+    __syncthreads();  // Lre/Lim are reused for the off-diagonal blocks
+  }
   for (int q = 0; q < ndep; ++q) {
     const int j = forward ? q : (nblk - 1 - q);
     // off-diagonal block (does not depend on the flag): 128 columns x 128 rows,
@@ -454,42 +486,13 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
       }
     }
   }
-  if (forward) {
-    // unit block lower factor: y_i = X
-    __syncthreads();
-    for (int idx = tid; idx < kB * NC; idx += blockDim.x) {
-      const int rr = idx & (kB - 1), c = idx >> 7;
-      if (c < nrhs) {
-        const float2 v = X[rr * NC + c];
-        Bb[(size_t)(r0 + rr) + (size_t)c * ldb] = make_double2((double)v.x, (double)v.y);
-      }
-    }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) st_release_i(flags + (size_t)b * nblk + i, 1);
-    return;
-  }
-  // backward: x_i = A_ii^{-1} X; the inverse (interleaved complex) through the planes
-  const float2* Inv = inv + ((size_t)b * nblk + i) * kB * kB;
-  for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
-    const float2 v = __ldg(Inv + idx);  // element (idx % 128, idx / 128)
-    Lre[idx] = v.x;
-    Lim[idx] = v.y;
-  }
+  // forward (unit block lower factor): y_i = X; backward: x_i = X
   __syncthreads();
-  tile_times_rhs<NC>(Lre, Lim, X, r, h, acc);
-  if (h == 1) {
-#pragma unroll
-    for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
-  }
-  __syncthreads();
-  if (h == 0) {
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      if (c < nrhs) {
-        const float2 o = P[r * NC + c];
-        Bb[(size_t)(r0 + r) + (size_t)c * ldb] = make_double2((double)(acc[c].x + o.x), (double)(acc[c].y + o.y));
-      }
+  for (int idx = tid; idx < kB * NC; idx += blockDim.x) {
+    const int rr = idx & (kB - 1), c = idx >> 7;
+    if (c < nrhs) {
+      const float2 v = X[rr * NC + c];
+      Bb[(size_t)(r0 + rr) + (size_t)c * ldb] = make_double2((double)v.x, (double)v.y);
     }
   }
   __threadfence();
@@ -572,6 +575,7 @@ struct MixedWork {
   float2* inv;
   float* binv;  // batch x 256 x kSplitK: packed A_kk^{-1} of the current block
   float* a3;    // batch x npad x kSplitK: split A21 of the current block
+  float* ainv;  // batch x 128 x 256: A_kk^{-1} of the current block as the A operand [Re | Im]
   int* flags;
 };
 MixedWork carve(void* work, int npad, int batch) {
@@ -590,6 +594,8 @@ MixedWork carve(void* work, int npad, int batch) {
   p += (size_t)batch * (2 * kB) * kSplitK * sizeof(float);
   w.a3 = (float*)p;
   p += (size_t)batch * npad * kSplitK * sizeof(float);
+  w.ainv = (float*)p;
+  p += (size_t)batch * kB * 2 * kB * sizeof(float);
   w.flags = (int*)p;
   return w;
 }
@@ -639,6 +645,7 @@ extern "C" int64_t bem_clu_workspace_bytes(int npad, int batch) {
   return (int64_t)batch * 2 * npad * (int64_t)npad * 4 + kOpBuffers * (int64_t)batch * npad * 2 * kB * 4 +
          kOpBuffers * (int64_t)batch * 2 * npad * 2 * kB * 4 + (int64_t)batch * nblk * kB * kB * 8 +
          (int64_t)batch * (2 * kB) * kSplitK * 4 + (int64_t)batch * npad * kSplitK * 4 +
+         (int64_t)batch * kB * 2 * kB * 4 +
          ((int64_t)batch * nblk + 2) * 4 + 1024;
 }
 
@@ -668,7 +675,7 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
   auto diag_and_panel = [&](int kk, int buf, cudaStream_t on) -> int {
     {
       TimedLaunch tl(kKCluGj, on);
-      clu_gj_kernel<<<batch, 512, 0, on>>>(W, kk, info_dev, w.inv, nblk, w.binv);
+      clu_gj_kernel<<<batch, 512, 0, on>>>(W, kk, info_dev, w.inv, nblk, w.binv, w.ainv);
     }
     ++launches;
     const int m = npad - kk - kB;
@@ -684,8 +691,13 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
       if (st2) return st2;
       clu_pack_kernel<<<dim3(m / 32, batch), 256, 0, on>>>(W, npad, kk, 0, kk + kB, kk, Aop[buf], Bop[buf],
                                                            nullptr);
+      // block row of U scaled by the diagonal inverse, U' = A_kk^{-1} A12 (TF32),
+      // for the backward substitution only (A12 itself is packed in Bop already)
+      st2 = cgemm_tf32_update(w.ainv, kB, 0, Bop[buf], 2 * (int64_t)npad, 2 * (kk + kB), 2 * kB, W.re, W.im, npad,
+                              W.stride, kk, kk + kB, kB, m, batch, err_dev, on, 1);
+      if (st2) return st2;
     }
-    launches += 2;
+    launches += 3;
     return BEM_OK;
   };
   // C rows r0.. (m), complex columns c0.. (nc) -= L21 U12 of the block step whose
