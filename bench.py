@@ -594,7 +594,8 @@ def main():
         engine = B200Engine(green_function=gf, precision="fp64", max_batch=args.batch,
                             linear_solver=args.linear_solver)
     # this rank's share of the sweep: frequencies rank, rank + world, ...
-    my_omegas = OMEGAS[rank::world]
+    from capytaine_b200.sharding import frequency_shard, max_over_ranks
+    my_omegas = OMEGAS[frequency_shard(OMEGAS, rank, world)]
     nb = args.batch
     batches = [my_omegas[(s * nb + np.arange(nb)) % len(my_omegas)] for s in range(args.warmup + args.steps)]
 
@@ -635,10 +636,7 @@ def main():
     clocks = sampler.stop()
     t_ms = ev0.elapsed_time(ev1)
     lat = np.array([a.elapsed_time(b) for a, b in step_ms])
-    if dist is not None:
-        t = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
+    t_ms = max_over_ranks(t_ms)
     total_solves = args.steps * nb * world
     value = total_solves / (t_ms * 1e-3)
 
@@ -670,11 +668,7 @@ def main():
         h2d += 8 * (2 * len(body.dofs) * m.nb_faces) + 4 * m.nb_faces + 8 * (2 * nb + 1)
         d2h += 16 * nb * (len(body.dofs) + 1) * len(body.dofs) * 2 + 4 * (nb + 2)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": total_solves / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d / args.steps),
            "d2h_bytes_per_step": int(d2h / args.steps)}
 
@@ -691,11 +685,7 @@ def main():
             eng64.solve_frequencies(body, batches[s])
         f1.record()
         torch.cuda.synchronize()
-        f_ms = f0.elapsed_time(f1)
-        if dist is not None:
-            t = torch.tensor([f_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            f_ms = float(t.item())
+        f_ms = max_over_ranks(f0.elapsed_time(f1))
         fp64 = {"value": args.fp64_steps * nb * world / (f_ms * 1e-3), "unit": UNIT, "steps": args.fp64_steps,
                 "ms_per_step": f_ms / args.fp64_steps}
         fp64["mixed_over_fp64"] = value / fp64["value"]
