@@ -52,7 +52,8 @@ def workload_config(args, n):
                              "lu_decomposition": "float64 DMMA LU"}[args.linear_solver]),
             "depth": "infinite", "l2": "inputs larger than L2 (K: 604 MB complex128 per frequency)",
             "parallelism": f"frequency shards x{args.world}",
-            "rankine_part": "computed once per sweep of the 60 frequencies (cache cleared at each sweep start)"}
+            "rankine_part": "computed once per sweep of the 60 frequencies (cache cleared at each sweep start)",
+            "calls": "one solve_frequencies call per sweep of the body (4 steps of 15 frequencies)"}
 
 
 RIGID_DOFS = ("Surge", "Sway", "Heave", "Roll", "Pitch", "Yaw")
@@ -543,7 +544,7 @@ def main():
     ap.add_argument("--engine", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--fp64-steps", type=int, default=4,
                     help="timed steps of the float64 engine for the refined-mixed vs float64 comparison (0: skip)")
-    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=15, help="frequencies per step (60 = 4 steps of 15 per sweep)")
     ap.add_argument("--refinement", default="classical", choices=["classical", "gmres"],
                     help="refinement of the mixed engine: x += (LU)^-1 r, or GMRES preconditioned by the LU")
     ap.add_argument("--linear-solver", default="lu_decomposition", choices=["lu_decomposition", "gmres"],
@@ -602,14 +603,23 @@ def main():
     def sweep_start(s):
         return (s * nb) % len(my_omegas) < nb
 
+    def calls(s0, s1):
+        """Steps s0..s1-1 grouped into one solve_frequencies call per sweep of the body."""
+        out = []
+        for s in range(s0, s1):
+            if not out or sweep_start(s):
+                out.append([])
+            out[-1].append(s)
+        return [(grp, np.concatenate([batches[s] for s in grp])) for grp in out]
+
     def barrier():
         if dist is not None:
             dist.barrier()
 
     # ---- device-resident timing (value) ----------------------------------
     lib = _lib.load()
-    for s in range(args.warmup):
-        engine.solve_frequencies(body, batches[s])
+    for grp, oms in calls(0, args.warmup):
+        engine.solve_frequencies(body, oms, batch=nb)
     torch.cuda.synchronize()
     sampler = ClockSampler(local_rank)
     sampler.start()
@@ -621,21 +631,21 @@ def main():
     ev1 = torch.cuda.Event(enable_timing=True)
     step_ms = []
     ev0.record()
-    for s in range(args.warmup, args.warmup + args.steps):
+    for grp, oms in calls(args.warmup, args.warmup + args.steps):
         e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e_a.record()
-        if sweep_start(s):
+        if sweep_start(grp[0]):
             gf.clear_rankine_cache()  # the Rankine part is computed once per sweep of the body
-        res = engine.solve_frequencies(body, batches[s])
+        res = engine.solve_frequencies(body, oms, batch=nb)
         e_b.record()
-        step_ms.append((e_a, e_b))
+        step_ms.append((e_a, e_b, len(grp)))
     ev1.record()
     torch.cuda.synchronize()
     launches = lib.bem_launch_count() - launches0
     barrier()
     clocks = sampler.stop()
     t_ms = ev0.elapsed_time(ev1)
-    lat = np.array([a.elapsed_time(b) for a, b in step_ms])
+    lat = np.array([a.elapsed_time(b) / cnt for a, b, cnt in step_ms])  # per step, averaged within a call
     t_ms = max_over_ranks(t_ms)
     total_solves = args.steps * nb * world
     value = total_solves / (t_ms * 1e-3)
@@ -658,15 +668,17 @@ def main():
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     h2d = d2h = 0
-    for s in range(args.warmup, args.warmup + args.steps):
-        gf._mesh_cache.clear()  # mesh arrays come from host memory every step
-        if sweep_start(s):
+    for grp, oms in calls(args.warmup, args.warmup + args.steps):
+        gf._mesh_cache.clear()  # mesh arrays come from host memory every call
+        engine._body_cache.clear()
+        if sweep_start(grp[0]):
             gf.clear_rankine_cache()
-        r = engine.solve_frequencies(body, batches[s])
+        r = engine.solve_frequencies(body, oms, batch=nb)
         m = body.mesh_including_lid
         h2d += 8 * (m.vertices.size + 3 * 3 * m.nb_faces + 2 * m.nb_faces + 4 * m.nb_faces) + 4 * m.faces.size
-        h2d += 8 * (2 * len(body.dofs) * m.nb_faces) + 4 * m.nb_faces + 8 * (2 * nb + 1)
-        d2h += 16 * nb * (len(body.dofs) + 1) * len(body.dofs) * 2 + 4 * (nb + 2)
+        h2d += 8 * (2 * len(body.dofs) * m.nb_faces) + 4 * m.nb_faces
+        h2d += len(grp) * 8 * (2 * nb + 1)
+        d2h += len(grp) * (16 * nb * (len(body.dofs) + 1) * len(body.dofs) * 2 + 4 * (nb + 2))
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": total_solves / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d / args.steps),
@@ -681,8 +693,8 @@ def main():
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record()
-        for s in range(args.warmup, args.warmup + args.fp64_steps):
-            eng64.solve_frequencies(body, batches[s])
+        for grp, oms in calls(args.warmup, args.warmup + args.fp64_steps):
+            eng64.solve_frequencies(body, oms, batch=nb)
         f1.record()
         torch.cuda.synchronize()
         f_ms = max_over_ranks(f0.elapsed_time(f1))
@@ -694,6 +706,8 @@ def main():
     # ---- serving: Poisson request stream, p50 / p99 latency ---------------
     serving = None
     if args.serving_requests > 0:
+        engine.release()  # the server allocates its own arena
+        torch.cuda.empty_cache()
         pool = seeded_bodies(1000 + rank, 32)
         serving = run_serving(B200Engine(green_function=gf, precision=args.engine, refinement=args.refinement)
                               if args.engine == "mixed" else B200Engine(green_function=gf, precision="fp64"),

@@ -276,6 +276,10 @@ class B200Engine:
             self._ws[key] = ws
         return ws
 
+    def release(self):
+        """Drop the engine's device workspaces (they are re-created on demand)."""
+        self._ws.clear()
+
     # ------------------------------------------------------------------------
     # Batched frequency solves
     def _body_arrays(self, body, mesh):
