@@ -208,6 +208,10 @@ class B200Engine:
     bem/engines.py:74-89: atol 1e-6, rtol 1e-5, restart 20; with precision
     "fp64" only), or a callable ``(A, b) -> x`` used by ``linear_solver``.
 
+    method: "indirect" (sources sigma = K^-1 bc, potential S sigma) or "direct"
+    (potential = D^-1 S bc with the double-layer matrix D), as capytaine's
+    BEMSolver(method=...) (bem/solver.py:172-207), for the device sweeps.
+
     refinement (precision "mixed"): "classical" (x += (LU)^-1 r) or "gmres"
     (GMRES on the float64 K right-preconditioned by the float32 LU), both to
     refine_tol relative residual.  When the classical iteration stops
@@ -218,7 +222,8 @@ class B200Engine:
     def __init__(self, *, green_function: Optional[Delhommeau] = None, precision: str = "fp64",
                  linear_solver="lu_decomposition", max_batch: int = 8, device=None,
                  refine_tol: float = 1e-10, refine_max_iter: int = 30, assembly_precision: str = "fp64",
-                 refinement: str = "classical", gmres_restart: int = 20, gmres_maxiter: Optional[int] = None):
+                 refinement: str = "classical", gmres_restart: int = 20, gmres_maxiter: Optional[int] = None,
+                 method: str = "indirect"):
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         if assembly_precision not in ("fp64", "mixed"):
@@ -230,6 +235,12 @@ class B200Engine:
             raise ValueError("linear_solver='gmres' is the float64 solver; use refinement='gmres' with 'mixed'")
         if refinement not in ("classical", "gmres"):
             raise ValueError("refinement must be 'classical' or 'gmres'")
+        if method.lower() not in ("direct", "indirect"):
+            raise ValueError(f"Unrecognized method: {method!r}. Expected \"direct\" or \"indirect\".")
+        # solve_frequencies / solve_bodies / the server: indirect (sources, K) or
+        # direct (potential, D with rhs = S bc), as BEMSolver(method=...) in
+        # capytaine bem/solver.py:172-207
+        self.method = method.lower()
         self.precision = precision
         self.refinement = refinement
         self.gmres_restart = int(gmres_restart)
@@ -255,6 +266,7 @@ class B200Engine:
             "precision": precision,
             "assembly_precision": assembly_precision,
             **({"refinement": refinement} if precision == "mixed" else {}),
+            "method": method.lower(),
             **self.green_function.exportable_settings,
         }
 
@@ -355,14 +367,16 @@ class B200Engine:
         n = mesh.nb_faces
         lds = n if lds is None else lds
         ks = [float(k) for k in ks]
+        adjoint = self.method == "indirect"  # K (adjoint double layer) or D
         if len(ks) > 1 and all(0.0 < k < np.inf for k in ks):
             gf.assemble_into(mesh, mesh, f.S[first], f.K[first], wavenumber=ks[0], lds=lds, ldk=f.ldk,
                              nan_flag=nan_flag, precision=self.assembly_precision, reuse_rankine=reuse_rankine,
-                             sweep=(ks, f.S.shape[1], f.K.shape[1]))
+                             sweep=(ks, f.S.shape[1], f.K.shape[1]), adjoint_double_layer=adjoint)
             return
         for b, k in enumerate(ks):
             gf.assemble_into(mesh, mesh, f.S[first + b], f.K[first + b], wavenumber=k, lds=lds, ldk=f.ldk,
-                             nan_flag=nan_flag, precision=self.assembly_precision, reuse_rankine=reuse_rankine)
+                             nan_flag=nan_flag, precision=self.assembly_precision, reuse_rankine=reuse_rankine,
+                             adjoint_double_layer=adjoint)
 
     def factor_stage(self, f: "_Factors", nb, err):
         """LU of K (float64 DMMA, or float32 tcgen05 for the mixed engine); none for plain GMRES."""
@@ -426,6 +440,16 @@ class B200Engine:
                                          _vp(k_t.data_ptr() + 8 * j0), g, ndof, _vp(dofn), nhead, _vp(heads_t),
                                          _vp(dm.centers), _vp(dm.normals), _vp(hull),
                                          _vp(r.B.data_ptr() + 16 * j0 * ld), npad, ld, stream))
+        direct = self.method == "direct"
+        if direct:
+            # rhs = S bc (bem/solver.py:182-183), through phi into the padded B
+            for c0 in range(0, nrhs, RHS_CHUNK):
+                nc = min(RHS_CHUNK, nrhs - c0)
+                _lib.check(lib.bem_zgemm_ts(n, n, nc, 1.0, 0.0, _vp(f.S), n, n * n,
+                                            _vp(r.B.data_ptr() + 16 * npad * c0), npad, ld, 0.0, 0.0,
+                                            _vp(r.phi.data_ptr() + 16 * n * c0), n, n * nrhs, nb, _vp(r.ts_work),
+                                            stream))
+            r.B.view(r.batch, nrhs, npad)[:nb, :, :n].copy_(r.phi.view(r.batch, nrhs, n)[:nb])
         sol = r.B if (self.precision == "fp64" and not self._plain_gmres) else r.X
         for c0 in range(0, nrhs, RHS_CHUNK):
             nc = min(RHS_CHUNK, nrhs - c0)
@@ -440,11 +464,16 @@ class B200Engine:
                                              npad, ld, nc, _vp(r.err), stream))
         if events:
             events[3].record()
-        for c0 in range(0, nrhs, RHS_CHUNK):
-            nc = min(RHS_CHUNK, nrhs - c0)
-            _lib.check(lib.bem_zgemm_ts(n, n, nc, 1.0, 0.0, _vp(f.S), n, n * n, _vp(sol.data_ptr() + 16 * npad * c0),
-                                        npad, ld, 0.0, 0.0, _vp(r.phi.data_ptr() + 16 * n * c0), n, n * nrhs, nb,
-                                        _vp(r.ts_work), stream))
+        if direct:  # the solution is the potential
+            phi_ptr, ldp, stp = sol.data_ptr(), npad, ld
+        else:       # potential = S sigma
+            for c0 in range(0, nrhs, RHS_CHUNK):
+                nc = min(RHS_CHUNK, nrhs - c0)
+                _lib.check(lib.bem_zgemm_ts(n, n, nc, 1.0, 0.0, _vp(f.S), n, n * n,
+                                            _vp(sol.data_ptr() + 16 * npad * c0), npad, ld, 0.0, 0.0,
+                                            _vp(r.phi.data_ptr() + 16 * n * c0), n, n * nrhs, nb, _vp(r.ts_work),
+                                            stream))
+            phi_ptr, ldp, stp = r.phi.data_ptr(), n, n * nrhs
         sizes = [(m * nrhs * na[1], m * max(nhead, 1) * na[1]) for (_, _, m), na in zip(segments, seg_arrays)]
         out = torch.empty((sum(a + b for a, b in sizes),), dtype=torch.complex128, device=dev)
         views, pos = [], 0
@@ -452,9 +481,8 @@ class B200Engine:
             F, FK = out[pos:pos + sf], out[pos + sf:pos + sf + sk]
             pos += sf + sk
             views.append((m, ndof, sf))
-            _lib.check(lib.bem_integrate_pressure(nf, m, nrhs, ndof, _vp(r.phi.data_ptr() + 16 * j0 * n * nrhs), n,
-                                                  n * nrhs, _vp(om_t.data_ptr() + 8 * j0), rho, _vp(wdof), _vp(F),
-                                                  stream))
+            _lib.check(lib.bem_integrate_pressure(nf, m, nrhs, ndof, _vp(phi_ptr + 16 * j0 * stp), ldp, stp,
+                                                  _vp(om_t.data_ptr() + 8 * j0), rho, _vp(wdof), _vp(F), stream))
             if nhead > 0:
                 _lib.check(lib.bem_froude_krylov(nf, m, ndof, nhead, _vp(k_t.data_ptr() + 8 * j0), rho, g,
                                                  _vp(heads_t), _vp(dm.centers), _vp(wdof), _vp(FK), stream))

@@ -345,16 +345,20 @@ def solve_gmres(A, b):
 
 
 def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: float, *, rho=1000.0, g=9.81,
-                    wave_directions=(0.0,), free_surface=0.0, linear_solver="lu", hull_mask=None):
+                    wave_directions=(0.0,), free_surface=0.0, linear_solver="lu", hull_mask=None,
+                    method="indirect"):
     """One frequency-solve, indirect method (solver.py:188-207): assemble S and K at
     k = omega^2/g, factor K once, solve every radiation and diffraction RHS, take
     S @ sigma, integrate pressures.  Returns added mass, damping (dict of dict) and
     excitation forces (dict heading -> dict dof -> complex).  With `hull_mask`
     (mesh = hull faces then lid faces, problems_and_results.py:373-381,
     440-449) the boundary conditions are zero on the lid and the pressures are
-    integrated on the hull only; dofs are then evaluated at the hull faces."""
+    integrated on the hull only; dofs are then evaluated at the hull faces.
+    method="direct": the potential solves D phi = S bc (bem/solver.py:172-187)."""
     import scipy.linalg as sl
 
+    if method == "direct":
+        return _solve_frequency_direct(gf, mesh, dofs, omega, rho=rho, g=g, wave_directions=wave_directions)
     if hull_mask is not None:
         return _solve_frequency_with_lid(gf, mesh, dofs, omega, rho=rho, g=g, wave_directions=wave_directions,
                                          linear_solver=linear_solver, hull_mask=np.asarray(hull_mask, bool))
@@ -423,6 +427,32 @@ def _solve_frequency_with_lid(gf, mesh, dofs, omega, *, rho, g, wave_directions,
     for beta in wave_directions:
         dif = forces(solve(-(airy_waves_velocity(c, omega, k, g, beta) * nrm).sum(axis=1)))
         fk = forces(airy_waves_pressure(c, omega, k, g, rho, beta))
+        results["diffraction"][beta] = dif
+        results["froude_krylov"][beta] = fk
+        results["excitation"][beta] = {d: dif[d] + fk[d] for d in dif}
+    return results
+
+
+def _solve_frequency_direct(gf, mesh, dofs, omega, *, rho, g, wave_directions):
+    """Direct method (bem/solver.py:172-187): S, D with adjoint_double_layer=False,
+    potential = D^-1 (S bc), pressure i omega rho potential."""
+    import scipy.linalg as sl
+    k = omega ** 2 / g
+    S, D = gf.evaluate(mesh, mesh, free_surface=0.0, water_depth=np.inf, wavenumber=k, adjoint_double_layer=False,
+                       early_dot_product=True, diagonal_term_in_double_layer=True)
+    lu = sl.lu_factor(D)
+    c, nrm = mesh.faces_centers, mesh.faces_normals
+    results = {"added_mass": {}, "radiation_damping": {}, "excitation": {}, "diffraction": {}, "froude_krylov": {}}
+
+    def pressure(bc):
+        return 1j * omega * rho * sl.lu_solve(lu, S @ bc.astype(np.complex128))
+    for name, dof in dofs.items():
+        f = integrate_pressure(mesh, dofs, pressure(-1j * omega * np.sum(dof.motion(c) * nrm, axis=1)))
+        results["added_mass"][name] = {d: float(np.real(v) / omega ** 2) for d, v in f.items()}
+        results["radiation_damping"][name] = {d: float(np.imag(v) / omega) for d, v in f.items()}
+    for beta in wave_directions:
+        dif = integrate_pressure(mesh, dofs, pressure(-(airy_waves_velocity(c, omega, k, g, beta) * nrm).sum(axis=1)))
+        fk = integrate_pressure(mesh, dofs, airy_waves_pressure(c, omega, k, g, rho, beta))
         results["diffraction"][beta] = dif
         results["froude_krylov"][beta] = fk
         results["excitation"][beta] = {d: dif[d] + fk[d] for d in dif}

@@ -198,3 +198,25 @@ def test_matrix_engine_interface(default_oracle_gf, tmp_path):
     Kh, Sh = np.asarray(K), np.asarray(S)
     assert np.abs(Kh @ x - b).max() < 1e-10 * np.abs(b).max()
     assert np.allclose(S @ x, Sh @ x, rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_direct_method_against_oracle(oracle_mod, default_oracle_gf, tmp_path, precision):
+    """method='direct' (potential = D^-1 S bc, bem/solver.py:172-187) against the
+    oracle's direct solve, and close to the indirect method as the reference's
+    test_bem_solver.py:77-83 asks (same forces within 10%)."""
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.engine import B200Engine
+    mesh = mesh_sphere(radius=1.0, resolution=(12, 24)).immersed_part()
+    body = FloatingBody(mesh, rigid_body_dofs())
+    omegas = np.array([0.6, 1.0, 2.2])
+    gf = _shared_table_gf(default_oracle_gf, tmp_path)
+    direct = B200Engine(green_function=gf, precision=precision, method="direct").solve_frequencies(body, omegas)
+    ref = [oracle_mod.solve_frequency(default_oracle_gf, mesh, oracle_mod.rigid_body_dofs(), w, method="direct")
+           for w in omegas]
+    errs = coefficient_errors(direct, ref, body.dofs)
+    assert max(errs.values()) < (1e-6 if precision == "fp64" else 1e-5), errs
+    indirect = B200Engine(green_function=gf, precision=precision).solve_frequencies(body, omegas)
+    surge = list(body.dofs).index("Surge")
+    np.testing.assert_allclose(np.abs(direct.excitation[:, 0, surge]), np.abs(indirect.excitation[:, 0, surge]),
+                               rtol=1e-1)
