@@ -115,6 +115,8 @@ _SIGNATURES = {
                              c_double, c_double, c_void_p, c_i64, c_i64, c_int, c_void_p], c_int),
     "bem_froude_krylov": ([c_int, c_int, c_int, c_int, c_void_p, c_double, c_double, c_void_p, c_void_p,
                            c_void_p, c_void_p, c_void_p], c_int),
+    "bem_block_combine": ([c_void_p, c_i64, c_i64, c_i64, c_void_p, c_i64, c_i64, c_i64, c_void_p, c_void_p, c_int,
+                           c_int, c_int, c_int, c_int, c_void_p], c_int),
 }
 
 _lock = threading.Lock()

@@ -77,44 +77,46 @@ class FloatingBody:
     def __add__(self, other: "FloatingBody") -> "FloatingBody":
         return join_bodies(self, other)
 
+    def _join_lid(self):
+        if "_with_lid" not in self.__dict__:
+            if self.lid_mesh is None:
+                self.__dict__["_with_lid"] = (self.mesh, np.ones(self.mesh.nb_faces, dtype=bool))
+            else:
+                # hull.join_meshes(lid) with masks (bodies.py:104-111): for plain meshes
+                # the hull faces then the lid faces, vertices concatenated unchanged; a
+                # symmetric hull with a lid of the same symmetry stays symmetric (halves
+                # or wedges joined), its hull faces in the order of the hull's faces.
+                joined, masks = self.mesh.join_meshes(self.lid_mesh, return_masks=True)
+                self.__dict__["_with_lid"] = (joined, masks[0])
+        return self.__dict__["_with_lid"]
+
     @property
     def mesh_including_lid(self) -> Mesh:
-        if self.lid_mesh is None:
-            return self.mesh
-        if not hasattr(self, "_with_lid"):
-            # Faces of the hull first, then the lid, vertices concatenated (no merge),
-            # so face i < nb_hull_faces is hull face i.
-            nv = self.mesh.nb_vertices
-            faces = [list(f) for f in self.mesh._faces] + [[i + nv for i in f] for f in self.lid_mesh._faces]
-            self._with_lid = Mesh(np.concatenate([self.mesh.vertices, self.lid_mesh.vertices]), faces,
-                                  quadrature_method=self.mesh.quadrature_method, clean=False)
-        return self._with_lid
+        return self._join_lid()[0]
 
     @property
     def hull_mask(self) -> np.ndarray:
-        n = self.mesh_including_lid.nb_faces
-        mask = np.zeros(n, dtype=bool)
-        mask[: self.mesh.nb_faces] = True
-        return mask
+        return self._join_lid()[1].copy()
 
     def dof_normal_components(self) -> np.ndarray:
         """(ndof, N_with_lid): dof(x_i) . n_i on hull faces, 0 on lid faces."""
-        n_all = self.mesh_including_lid.nb_faces
-        out = np.zeros((len(self.dofs), n_all))
+        mask = self._join_lid()[1]
+        out = np.zeros((len(self.dofs), mask.size))
         c, nrm = self.mesh.faces_centers, self.mesh.faces_normals
         for d, dof in enumerate(self.dofs.values()):
-            out[d, : self.mesh.nb_faces] = np.sum(dof.evaluate_motion(c) * nrm, axis=1)
+            out[d, mask] = np.sum(dof.evaluate_motion(c) * nrm, axis=1)
         return out
 
     def pressure_weights(self) -> np.ndarray:
         """(ndof, N_with_lid): -(dof . n) area on hull faces (bodies.py:238-250), 0 on lid faces."""
+        mask = self._join_lid()[1]
         w = -self.dof_normal_components()
-        w[:, : self.mesh.nb_faces] *= self.mesh.faces_areas[None, :]
+        w[:, mask] *= self.mesh.faces_areas[None, :]
         return w
 
     def integrate_pressure(self, pressure: np.ndarray) -> Dict[str, complex]:
-        """Host version of bodies.py:238-250 on hull pressures."""
-        w = self.pressure_weights()[:, : self.mesh.nb_faces]
+        """Host version of bodies.py:238-250 on hull pressures (in the order of the hull's faces)."""
+        w = self.pressure_weights()[:, self._join_lid()[1]]
         return {name: complex(np.sum(pressure * w[d])) for d, name in enumerate(self.dofs)}
 
 

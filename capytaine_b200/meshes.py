@@ -160,6 +160,26 @@ class Mesh:
     def with_quadrature(self, quadrature_method) -> "Mesh":
         return Mesh(self.vertices, self._faces, quadrature_method=quadrature_method, name=self.name, clean=False)
 
+    def mirrored(self, plane: str, name=None) -> "Mesh":
+        """Image in the plane xOz (y -> -y) or yOz (x -> -x), each face's vertex
+        order reversed so that normals stay outward (capytaine meshes.py:554-573)."""
+        v = self.vertices.copy()
+        if plane == "xOz":
+            v[:, 1] *= -1
+        elif plane == "yOz":
+            v[:, 0] *= -1
+        else:
+            raise ValueError(f"Unsupported value for plane: {plane}")
+        return Mesh(v, [f[::-1] for f in self._faces], quadrature_method=self.quadrature_method,
+                    name=name or self.name, clean=False)
+
+    def rotated_z(self, angle, name=None) -> "Mesh":
+        """Rotation by `angle` (radians, counterclockwise seen from +z) about Oz."""
+        c, s = np.cos(angle), np.sin(angle)
+        R = np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+        return Mesh(self.vertices @ R.T, self._faces, quadrature_method=self.quadrature_method,
+                    name=name or self.name, clean=False)
+
     def merged(self) -> "Mesh":
         return self
 
@@ -209,14 +229,27 @@ class Mesh:
             return self
         return self.clipped(origin=(0, 0, free_surface), normal=(0, 0, 1))
 
-    @staticmethod
-    def join_meshes(*meshes, name=None) -> "Mesh":
+    def join_meshes(self, *meshes, return_masks=False, name=None):
+        """This mesh and `meshes` as one (symmetric meshes are merged first).
+        Without masks the vertices are cleaned; with return_masks the faces are
+        concatenated unchanged, in order, and the boolean face mask of each
+        input is returned as well (capytaine meshes.py:575-640)."""
+        meshes = [m.merged() for m in (self,) + meshes]
         verts, faces, off = [], [], 0
         for m in meshes:
             verts.append(m.vertices)
             faces.extend([[i + off for i in f] for f in m._faces])
             off += m.nb_vertices
-        return Mesh(np.concatenate(verts), faces, name=name, clean=True)
+        if not return_masks:
+            return Mesh(np.concatenate(verts), faces, name=name, clean=True)
+        joined = Mesh(np.concatenate(verts), faces, quadrature_method=self.quadrature_method, name=name, clean=False)
+        counts = np.cumsum([0] + [m.nb_faces for m in meshes])
+        masks = []
+        for a, b in zip(counts[:-1], counts[1:]):
+            mask = np.zeros(joined.nb_faces, dtype=bool)
+            mask[a:b] = True
+            masks.append(mask)
+        return joined, masks
 
 
 # ---------------------------------------------------------------------------
@@ -367,11 +400,16 @@ def _surface_of_revolution(profile_points, n):
     return verts, faces
 
 
-def mesh_sphere(*, radius=1.0, center=(0.0, 0.0, 0.0), resolution=(10, 10), name=None) -> Mesh:
-    """Sphere from a meridian of ntheta+1 points swept nphi times (capytaine spheres.py:26-66)."""
+def mesh_sphere(*, radius=1.0, center=(0.0, 0.0, 0.0), resolution=(10, 10), axial_symmetry=False, name=None):
+    """Sphere from a meridian of ntheta+1 points swept nphi times (capytaine
+    spheres.py:26-66); with axial_symmetry a RotationSymmetricMesh of nphi
+    wedges (same faces, in the same order)."""
     ntheta, nphi = resolution
     theta = np.linspace(0.0, np.pi, ntheta + 1)
     meridian = radius * np.stack([np.sin(theta), np.zeros_like(theta), -np.cos(theta)], axis=1)
+    if axial_symmetry:
+        from .symmetric_meshes import RotationSymmetricMesh
+        return RotationSymmetricMesh.from_profile_points(meridian, nphi, name=name).translated(center)
     verts, faces = _surface_of_revolution(meridian, nphi)
     return Mesh(verts, faces, name=name).translated(center)
 
@@ -427,10 +465,26 @@ def _rotation_aligning(a, b, eps=1e-8):
 
 
 def mesh_parallelepiped(size=(1.0, 1.0, 1.0), center=(0, 0, 0), resolution=(4, 4, 4),
-                        missing_sides=frozenset(), name=None) -> Mesh:
-    """Six rectangles with outward normals (capytaine rectangles.py:103-213)."""
+                        missing_sides=frozenset(), reflection_symmetry=False, name=None):
+    """Six rectangles with outward normals (capytaine rectangles.py:103-213).
+    With reflection_symmetry: the quarter x < 0, y < 0 (its sides on the planes
+    x = 0 and y = 0 left out) mirrored in yOz, then the half in xOz (even
+    resolutions along x and y, centre on Oz)."""
     width, thickness, height = size
     nw, nth, nh = resolution
+    if reflection_symmetry:
+        from .symmetric_meshes import ReflectionSymmetricMesh
+        if nw % 2 == 1 or nth % 2 == 1:
+            raise ValueError("To define a parallelepiped mesh with reflection symmetry, "
+                             "it should have an even number of panels in both direction.")
+        if not np.isclose(center[0], 0.0) or not np.isclose(center[1], 0.0):
+            raise ValueError("To define a rectangle mesh with reflection symmetry, "
+                             "its center should be on the Oz axis (that is x=0 and y=0).")
+        quarter = mesh_parallelepiped(size=(width / 2, thickness / 2, height), resolution=(nw // 2, nth // 2, nh),
+                                      center=(-width / 4, -thickness / 4, 0),
+                                      missing_sides=set(missing_sides) | {"right", "back"})
+        half = ReflectionSymmetricMesh(quarter, plane="yOz")
+        return ReflectionSymmetricMesh(half, plane="xOz", name=name).translated(center)
     sides = []
     if "left" not in missing_sides:
         sides.append(mesh_rectangle(size=(thickness, height), resolution=(nth, nh), center=(-width / 2, 0, 0),
@@ -453,11 +507,30 @@ def mesh_parallelepiped(size=(1.0, 1.0, 1.0), center=(0, 0, 0), resolution=(4, 4
     return Mesh.join_meshes(*sides, name=name).translated(center)
 
 
-def mesh_vertical_cylinder(*, length=10.0, radius=1.0, center=(0, 0, 0), resolution=(2, 8, 10), name=None) -> Mesh:
+def mesh_vertical_cylinder(*, length=10.0, radius=1.0, center=(0, 0, 0), resolution=(2, 8, 10),
+                           reflection_symmetry=False, axial_symmetry=False, name=None, _theta_max=2 * np.pi):
     """Closed vertical cylinder: bottom disc, lateral surface, top disc
-    (capytaine cylinders.py:108-205, full circle)."""
+    (capytaine cylinders.py:108-205).  reflection_symmetry: the half
+    0 <= theta <= pi mirrored in yOz (even ntheta); axial_symmetry: one slice of
+    angle 2 pi / ntheta repeated ntheta times about Oz."""
     nr, ntheta, nz = resolution
-    theta_range = np.linspace(0, 2 * np.pi, ntheta + 1)
+    if reflection_symmetry and axial_symmetry:
+        raise NotImplementedError("Vertical cylinders with both symmetries have not been implemented.")
+    if reflection_symmetry or axial_symmetry:
+        from .symmetric_meshes import ReflectionSymmetricMesh, RotationSymmetricMesh
+        if reflection_symmetry:
+            if ntheta % 2 == 1:
+                raise ValueError("To use the reflection symmetry of the mesh, "
+                                 "it should have an even number of panels in this direction.")
+            half = mesh_vertical_cylinder(length=length, radius=radius, resolution=(nr, ntheta // 2, nz),
+                                          _theta_max=_theta_max / 2)
+            mesh = ReflectionSymmetricMesh(half, plane="yOz", name=name)
+        else:
+            piece = mesh_vertical_cylinder(length=length, radius=radius, resolution=(nr, 1, nz),
+                                           _theta_max=_theta_max / ntheta)
+            mesh = RotationSymmetricMesh(piece, ntheta, axis="z+", name=name)
+        return mesh.translated(center)
+    theta_range = np.linspace(0, _theta_max, ntheta + 1)
     z_range = np.linspace(-length / 2, length / 2, nz + 1)
     if nr > 0:
         r_range = np.linspace(0.0, radius, nr + 1)

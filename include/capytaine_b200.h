@@ -310,6 +310,25 @@ int bem_gmres_solve(const void* A_dev, int64_t lda, int64_t strideA, int n, int 
                     int max_cycles, void* precond_work_dev, void* work_dev, int* err_dev, int* iters_out,
                     double* resid_out, void* stream);
 
+/* ---- symmetric meshes ------------------------------------------------------ */
+/* out[f][o][c][r] = sum_{i < mi} W[o][i] in[f][src[i]][c][r] for o < mo, r < rows,
+ * c < cols, f < nf, complex128; element (f, b, c, r) of `in` at
+ * in + f*in_fstride + b*in_bstride + c*in_cstride + r (elements), likewise for
+ * `out`.  W: mo x mi row-major complex128 on the device; source_dev: mi int32
+ * block indices, or NULL for src[i] = i.  `out` must not overlap `in`.
+ * cols <= 65535 and nf * ceil(mo / 8) <= 65535.
+ * With the first column of blocks of a mesh with reflection or rotation
+ * symmetry as `in` (rows of block j at j * n_sub) and the group's Fourier
+ * weights as W, it writes the independent systems of the block-diagonalised
+ * matrix; with vectors it takes right-hand sides to those systems and
+ * solutions back.  Replaces BlockCirculantMatrix.block_diagonalize, the
+ * np.fft.fft / ifft of the right-hand sides in LUDecomposedBlockCirculantMatrix
+ * .solve and NestedBlockCirculantMatrix.to_BlockCirculantMatrix
+ * (tools/block_circulant_matrices.py:138-162, 226-266, 276-301, 410-419). */
+int bem_block_combine(const void* in_dev, int64_t in_fstride, int64_t in_bstride, int64_t in_cstride, void* out_dev,
+                      int64_t out_fstride, int64_t out_bstride, int64_t out_cstride, const void* weights_dev,
+                      const int32_t* source_dev, int mi, int mo, int rows, int cols, int nf, void* stream);
+
 /* ---- allocation-free variant ---------------------------------------------- */
 /* No counterpart in the reference.  Same operation and arguments as
  * bem_zgemm_ts without the workspace: for callers that can only pass buffers

@@ -457,3 +457,98 @@ def _solve_frequency_direct(gf, mesh, dofs, omega, *, rho, g, wave_directions):
         results["froude_krylov"][beta] = fk
         results["excitation"][beta] = {d: dif[d] + fk[d] for d in dif}
     return results
+
+
+# ---------------------------------------------------------------------------
+# Symmetric meshes (bem/engines.py:178-247, tools/block_circulant_matrices.py)
+def circulant_macro_blocks(blocks, nested):
+    """Blocks of the first block column of a block-circulant matrix, from the
+    first column of blocks of capytaine's matrix classes: BlockCirculantMatrix
+    (nested=False: the blocks themselves) or NestedBlockCirculantMatrix
+    (nested=True, 2n blocks: n macro-blocks of 2 x 2 blocks,
+    NestedBlockCirculantMatrix.to_BlockCirculantMatrix,
+    tools/block_circulant_matrices.py:226-266)."""
+    blocks = np.asarray(blocks)
+    if not nested:
+        return blocks
+    n = len(blocks) // 2
+    macro = []
+    for i in range(n):
+        if i == 0:
+            tl, tr, bl, br = blocks[0], blocks[1], blocks[1], blocks[0]
+        else:
+            tl, tr, bl, br = blocks[2 * i], blocks[2 * n - 2 * i + 1], blocks[2 * i + 1], blocks[2 * n - 2 * i]
+        macro.append(np.block([[tl, tr], [bl, br]]))
+    return np.asarray(macro)
+
+
+def circulant_matvec(macro, x):
+    """y = M x for the block-circulant M of first block column `macro`
+    (BlockCirculantMatrix.__matmul__, tools/block_circulant_matrices.py:97-131):
+    y_I = sum_J macro[(I - J) mod n] x_J."""
+    n = len(macro)
+    xs = np.split(np.asarray(x), n)
+    return np.concatenate([sum(macro[(I - J) % n] @ xs[J] for J in range(n)) for I in range(n)])
+
+
+def circulant_lu(macro):
+    """LUDecomposedBlockCirculantMatrix (tools/block_circulant_matrices.py:404-419):
+    the FFT of the first block column along the block axis, one LU per block."""
+    import scipy.linalg as sl
+    return [sl.lu_factor(b) for b in np.fft.fft(np.asarray(macro), axis=0)]
+
+
+def circulant_solve(lus, b):
+    """LUDecomposedBlockCirculantMatrix.solve: FFT of the right-hand side's
+    segments, the block solves, the inverse FFT."""
+    import scipy.linalg as sl
+    n = len(lus)
+    b = np.asarray(b, dtype=np.complex128)
+    b_fft = np.fft.fft(b.reshape((n, -1)), axis=0)
+    res = np.stack([sl.lu_solve(lu, bi) for lu, bi in zip(lus, b_fft)])
+    return np.fft.ifft(res, axis=0).reshape(b.shape)
+
+
+def solve_frequency_symmetric(gf, mesh, submesh, nb_blocks, nested, dofs, omega, *, rho=1000.0, g=9.81,
+                              wave_directions=(0.0,), hull_mask=None):
+    """solve_frequency for a mesh with symmetries, through capytaine's algorithm:
+    S and K of the whole mesh's collocation points against the panels of the
+    reference sub-mesh (the half, quarter, wedge or half wedge), split into the
+    nb_blocks blocks of the first block column (engines.py:178-247, row blocks
+    of the (N, N/nb_blocks) matrices), the block-circulant LU and solve, and
+    S @ sigma as the block-circulant product.  `mesh` holds the faces of the
+    whole mesh in the reference's order; nested=True for two planes or a
+    rotation of a reflection (NestedBlockCirculantMatrix).  With hull_mask the
+    faces outside it are a lid (zero boundary condition, no pressure)."""
+    k = omega ** 2 / g
+    S, K = gf.evaluate(mesh, submesh, free_surface=0.0, water_depth=np.inf, wavenumber=k, adjoint_double_layer=True,
+                       early_dot_product=True, diagonal_term_in_double_layer=True)
+    ns = submesh.nb_faces
+    Sm = circulant_macro_blocks(np.ascontiguousarray(S).reshape((nb_blocks, ns, ns)), nested)
+    Km = circulant_macro_blocks(np.ascontiguousarray(K).reshape((nb_blocks, ns, ns)), nested)
+    lus = circulant_lu(Km)
+    N = mesh.nb_faces
+    mask = np.ones(N, dtype=bool) if hull_mask is None else np.asarray(hull_mask, bool)
+    c, nrm, area = mesh.faces_centers[mask], mesh.faces_normals[mask], mesh.faces_areas[mask]
+
+    def solve(bc_hull):
+        bc = np.zeros(N, dtype=np.complex128)
+        bc[mask] = bc_hull
+        sigma = circulant_solve(lus, bc)
+        return (1j * omega * rho * circulant_matvec(Sm, sigma))[mask]
+
+    def forces(pressure):
+        return {name: np.sum(pressure * -np.sum(d.motion(c) * nrm, axis=1) * area) for name, d in dofs.items()}
+
+    results = {"added_mass": {}, "radiation_damping": {}, "excitation": {}, "diffraction": {}, "froude_krylov": {}}
+    for name, dof in dofs.items():
+        f = forces(solve(-1j * omega * np.sum(dof.motion(c) * nrm, axis=1)))
+        results["added_mass"][name] = {d: float(np.real(v) / omega ** 2) for d, v in f.items()}
+        results["radiation_damping"][name] = {d: float(np.imag(v) / omega) for d, v in f.items()}
+    for beta in wave_directions:
+        dif = forces(solve(-(airy_waves_velocity(c, omega, k, g, beta) * nrm).sum(axis=1)))
+        fk = forces(airy_waves_pressure(c, omega, k, g, rho, beta))
+        results["diffraction"][beta] = dif
+        results["froude_krylov"][beta] = fk
+        results["excitation"][beta] = {d: dif[d] + fk[d] for d in dif}
+    return results
