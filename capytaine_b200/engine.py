@@ -31,6 +31,7 @@ import numpy as np
 from . import _lib
 from .arena import DeviceArena
 from .green_function import Delhommeau
+from .symmetry import block_structure
 
 LOG = logging.getLogger(__name__)
 
@@ -192,6 +193,61 @@ class _Workspace:
         return self.f.nbytes + self.r.nbytes
 
 
+class _SymWorkspace:
+    """Buffers of the frequency-solves of a mesh with symmetries: the reduced
+    systems (factors and right-hand sides of batch x nsys systems of size
+    n_sys), the first block columns of S and K (N x n_sub per frequency), the
+    right-hand sides and potentials of the whole mesh, and the transform."""
+
+    def __init__(self, st, n_full, batch, nrhs, device, precision):
+        import torch
+        self.st, self.n_full, self.batch, self.nrhs = st, n_full, batch, nrhs
+        self.f = _Factors(st.n_sys, batch * st.nsys, device, precision)
+        self.r = _Rhs(st.n_sys, self.f.npad, batch * st.nsys, nrhs, device, precision)
+        self.cols = torch.empty((2, batch, n_full * st.n_sub), dtype=torch.complex128, device=device)
+        self.full = torch.zeros((batch, n_full * nrhs), dtype=torch.complex128, device=device)
+        self.W = torch.as_tensor(np.ascontiguousarray(st.W), dtype=torch.complex128, device=device)
+        self.Winv = torch.as_tensor(np.ascontiguousarray(st.Winv), dtype=torch.complex128, device=device)
+        # image block of each macro-block at each (row part, column part): None when it is the identity
+        self.src = [[None if st.q == 1 else
+                     torch.as_tensor(np.ascontiguousarray(st.source[:, a, b]), dtype=torch.int32, device=device)
+                     for b in range(st.q)] for a in range(st.q)]
+
+    @property
+    def nbytes(self):
+        return self.f.nbytes + self.r.nbytes + 16 * (self.cols.numel() + self.full.numel())
+
+    def combine_matrices(self, cols, nb, out, ld_out, stride_out, stream):
+        """Systems k of frequencies 0..nb-1 from their first block columns
+        (`cols`: nb x (N x n_sub) column-major, image j at rows j n_sub) into
+        `out` (system f * nsys + k at out + that index * stride_out, leading
+        dimension ld_out)."""
+        st, lib = self.st, _lib.load()
+        ns, N = st.n_sub, self.n_full
+        for a in range(st.q):
+            for b in range(st.q):
+                src = self.src[a][b]
+                _lib.check(lib.bem_block_combine(_vp(cols), N * ns, ns, N,
+                                                 _vp(out.data_ptr() + 16 * (a * ns + b * ns * ld_out)),
+                                                 st.nsys * stride_out, stride_out, ld_out, _vp(self.W),
+                                                 _vp(src) if src is not None else None, st.nsys, st.nsys, ns, ns, nb,
+                                                 stream))
+
+    def to_systems(self, nb, out, ld_out, stride_out, stream):
+        """Right-hand sides of the whole mesh (self.full) to those of the systems."""
+        st, N, nrhs = self.st, self.n_full, self.nrhs
+        _lib.check(_lib.load().bem_block_combine(_vp(self.full), N * nrhs, st.n_sys, N, _vp(out),
+                                                 st.nsys * stride_out, stride_out, ld_out, _vp(self.W), None,
+                                                 st.nsys, st.nsys, st.n_sys, nrhs, nb, stream))
+
+    def from_systems(self, nb, src_ptr, ld_in, stride_in, stream):
+        """Potentials of the systems back to the whole mesh (into self.full)."""
+        st, N, nrhs = self.st, self.n_full, self.nrhs
+        _lib.check(_lib.load().bem_block_combine(_vp(src_ptr), st.nsys * stride_in, stride_in, ld_in,
+                                                 _vp(self.full), N * nrhs, st.n_sys, N, _vp(self.Winv), None,
+                                                 st.nsys, st.nsys, st.n_sys, nrhs, nb, stream))
+
+
 class B200Engine:
     """capytaine-compatible matrix engine running the Delhommeau assembly and the
     dense solves on one B200.
@@ -324,6 +380,9 @@ class B200Engine:
         ndof, nhead = len(body.dofs), len(heads)
         nrhs = ndof + nhead
         B = min(self.max_batch if batch is None else batch, len(omegas))
+        st = block_structure(mesh)
+        if st is not None:
+            return self._solve_frequencies_symmetric(body, st, omegas, heads, rho, g, B, sync_stats)
         ws = self.workspace(n, B, nrhs)
         F_all = np.zeros((len(omegas), nrhs, ndof), dtype=np.complex128)
         FK_all = np.zeros((len(omegas), max(nhead, 1), ndof), dtype=np.complex128)
@@ -342,6 +401,66 @@ class B200Engine:
             if ev:
                 ev[2].record()
             F, FK = self.solve_stage(ws.f, ws.r, body, om, heads, rho=rho, g=g, stats=stats, events=ev)
+            F_all[start:start + nb] = F
+            FK_all[start:start + nb, :nhead] = FK
+            if ev:
+                torch.cuda.synchronize()
+                stats["assembly_ms"] += ev[0].elapsed_time(ev[1])
+                stats["lu_ms"] += ev[1].elapsed_time(ev[2])
+                stats["solve_ms"] += ev[2].elapsed_time(ev[3])
+                stats["post_ms"] += ev[3].elapsed_time(ev[4])
+        return self._coefficients(body, omegas, heads, F_all, FK_all, stats)
+
+    def _solve_frequencies_symmetric(self, body, st, omegas, heads, rho, g, B, sync_stats):
+        """solve_frequencies for a mesh with symmetries (bem/engines.py:178-247,
+        tools/block_circulant_matrices.py): per frequency, S and K of the whole
+        mesh's collocation points against the panels of the reference sub-mesh
+        (the first block column), the nsys independent systems of the
+        block-diagonalised matrices (bem_block_combine), one batched LU of all
+        systems of the batch, right-hand sides taken to the systems, solved,
+        S sigma per system, the potentials taken back to the whole mesh, then
+        the force integrals of the whole mesh."""
+        import torch
+        mesh = body.mesh_including_lid
+        full = mesh.merged()
+        N = full.nb_faces
+        nhead = len(heads)
+        nrhs = len(body.dofs) + nhead
+        key = ("symmetric", st.kind, st.n_sub, st.nsys, N, B, nrhs, self.precision)
+        ws = self._ws.get(key)
+        if ws is None:
+            self._ws.clear()
+            ws = _SymWorkspace(st, N, B, nrhs, self.device, self.precision)
+            self._ws[key] = ws
+        F_all = np.zeros((len(omegas), nrhs, len(body.dofs)), dtype=np.complex128)
+        FK_all = np.zeros((len(omegas), max(nhead, 1), len(body.dofs)), dtype=np.complex128)
+        stats = {"assembly_ms": 0.0, "lu_ms": 0.0, "solve_ms": 0.0, "post_ms": 0.0, "symmetry": st.kind,
+                 "systems_per_frequency": st.nsys, "system_size": st.n_sys}
+        gf = self.green_function
+        adjoint = self.method == "indirect"
+        stream = _lib.stream_ptr()
+        f = ws.f
+        for start in range(0, len(omegas), B):
+            om = omegas[start:start + B]
+            nb = len(om)
+            ks = [float(k) for k in om ** 2 / g]
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)] if sync_stats else None
+            if ev:
+                ev[0].record()
+            ws.r.flags.zero_()
+            cstride = N * st.n_sub
+            gf.assemble_into(full, st.submesh, ws.cols[0, 0], ws.cols[1, 0], wavenumber=ks[0], lds=N, ldk=N,
+                             nan_flag=ws.r.nan, precision=self.assembly_precision, adjoint_double_layer=adjoint,
+                             sweep=(ks, cstride, cstride) if nb > 1 else None)
+            ws.combine_matrices(ws.cols[0], nb, f.S, st.n_sys, st.n_sys * st.n_sys, stream)
+            ws.combine_matrices(ws.cols[1], nb, f.K, f.ldk, f.strideK, stream)
+            if ev:
+                ev[1].record()
+            self.factor_stage(f, nb * st.nsys, ws.r.err)
+            if ev:
+                ev[2].record()
+            (F, FK), = self._solve_segments(f, ws.r, [(body, 0, nb)], om, heads, rho=rho, g=g, stats=stats,
+                                            events=ev, sym=ws)
             F_all[start:start + nb] = F
             FK_all[start:start + nb, :nhead] = FK
             if ev:
@@ -405,12 +524,15 @@ class B200Engine:
         return F, FK
 
     def _solve_segments(self, f: "_Factors", r: "_Rhs", segments, om, heads, *, rho=1000.0, g=9.81, stats=None,
-                        events=None):
+                        events=None, sym: Optional[_SymWorkspace] = None):
         """solve_stage for batch entries holding several bodies: segments
         [(body, j0, m)] give the body of entries j0 .. j0+m-1.  A body smaller
         than the system (f.n, identity-padded) has zero right-hand-side rows
         beyond its panels; bodies with fewer dofs than r.nrhs - nhead have zero
-        columns.  Returns [(F (m, nrhs, ndof), FK (m, nhead, ndof))] per segment."""
+        columns.  With `sym` (one body, a mesh with symmetries) the factors hold
+        sym.st.nsys systems per frequency: right-hand sides go to the systems
+        and potentials come back to the whole mesh through sym's transforms.
+        Returns [(F (m, nrhs, ndof), FK (m, nhead, ndof))] per segment."""
         import torch
         lib = _lib.load()
         stream = _lib.stream_ptr()
@@ -419,6 +541,7 @@ class B200Engine:
         n, npad = f.n, f.npad
         om = np.asarray(om, dtype=float)
         nb = len(om)
+        nbs = nb * (sym.st.nsys if sym is not None else 1)  # systems of this batch
         ks = om ** 2 / g
         heads = np.asarray(heads, dtype=float)
         nhead = len(heads)
@@ -427,11 +550,16 @@ class B200Engine:
         small = torch.as_tensor(np.concatenate([om, ks, heads]), dtype=torch.float64, device=dev)
         om_t, k_t, heads_t = small[:nb], small[nb:2 * nb], small[2 * nb:]
         r.B.zero_()
+        if sym is not None:  # right-hand sides of the whole mesh first
+            rhs, rhs_ld, rhs_stride, n_max = sym.full, sym.n_full, sym.n_full * nrhs, sym.n_full
+            rhs.zero_()
+        else:
+            rhs, rhs_ld, rhs_stride, n_max = r.B, npad, ld, n
         seg_arrays = []
         for body, j0, m in segments:
             mesh = body.mesh_including_lid
             ndof = len(body.dofs)
-            if ndof + nhead > nrhs or mesh.nb_faces > n:
+            if ndof + nhead > nrhs or mesh.nb_faces > n_max:
                 raise ValueError("right-hand side buffers of the wrong shape")
             dm = self.green_function.device_mesh(mesh)
             dofn, wdof, hull = self._body_arrays(body, mesh)
@@ -439,7 +567,9 @@ class B200Engine:
             _lib.check(lib.bem_build_rhs(mesh.nb_faces, m, _vp(om_t.data_ptr() + 8 * j0),
                                          _vp(k_t.data_ptr() + 8 * j0), g, ndof, _vp(dofn), nhead, _vp(heads_t),
                                          _vp(dm.centers), _vp(dm.normals), _vp(hull),
-                                         _vp(r.B.data_ptr() + 16 * j0 * ld), npad, ld, stream))
+                                         _vp(rhs.data_ptr() + 16 * j0 * rhs_stride), rhs_ld, rhs_stride, stream))
+        if sym is not None:
+            sym.to_systems(nb, r.B, npad, ld, stream)
         direct = self.method == "direct"
         if direct:
             # rhs = S bc (bem/solver.py:182-183), through phi into the padded B
@@ -447,20 +577,20 @@ class B200Engine:
                 nc = min(RHS_CHUNK, nrhs - c0)
                 _lib.check(lib.bem_zgemm_ts(n, n, nc, 1.0, 0.0, _vp(f.S), n, n * n,
                                             _vp(r.B.data_ptr() + 16 * npad * c0), npad, ld, 0.0, 0.0,
-                                            _vp(r.phi.data_ptr() + 16 * n * c0), n, n * nrhs, nb, _vp(r.ts_work),
+                                            _vp(r.phi.data_ptr() + 16 * n * c0), n, n * nrhs, nbs, _vp(r.ts_work),
                                             stream))
-            r.B.view(r.batch, nrhs, npad)[:nb, :, :n].copy_(r.phi.view(r.batch, nrhs, n)[:nb])
+            r.B.view(r.batch, nrhs, npad)[:nbs, :, :n].copy_(r.phi.view(r.batch, nrhs, n)[:nbs])
         sol = r.B if (self.precision == "fp64" and not self._plain_gmres) else r.X
         for c0 in range(0, nrhs, RHS_CHUNK):
             nc = min(RHS_CHUNK, nrhs - c0)
             off = 16 * npad * c0  # byte offset of column c0
             Bc, Xc, Rc = (_vp(t.data_ptr() + off) for t in (r.B, r.X, r.R))
             if self._plain_gmres:
-                self._gmres_solve(f, r, nb, 1e-6, 1e-5, None, stats, stream, Bc, Xc, nc)
+                self._gmres_solve(f, r, nbs, 1e-6, 1e-5, None, stats, stream, Bc, Xc, nc)
             elif self.precision == "mixed":
-                self._refine(f, r, nb, Bc, Xc, Rc, nc, stats, stream)
+                self._refine(f, r, nbs, Bc, Xc, Rc, nc, stats, stream)
             else:
-                _lib.check(lib.bem_zlu_solve(_vp(f.K), npad, npad, npad * npad, nb, _vp(f.piv), _vp(f.lu_work), Bc,
+                _lib.check(lib.bem_zlu_solve(_vp(f.K), npad, npad, npad * npad, nbs, _vp(f.piv), _vp(f.lu_work), Bc,
                                              npad, ld, nc, _vp(r.err), stream))
         if events:
             events[3].record()
@@ -471,9 +601,12 @@ class B200Engine:
                 nc = min(RHS_CHUNK, nrhs - c0)
                 _lib.check(lib.bem_zgemm_ts(n, n, nc, 1.0, 0.0, _vp(f.S), n, n * n,
                                             _vp(sol.data_ptr() + 16 * npad * c0), npad, ld, 0.0, 0.0,
-                                            _vp(r.phi.data_ptr() + 16 * n * c0), n, n * nrhs, nb, _vp(r.ts_work),
+                                            _vp(r.phi.data_ptr() + 16 * n * c0), n, n * nrhs, nbs, _vp(r.ts_work),
                                             stream))
             phi_ptr, ldp, stp = r.phi.data_ptr(), n, n * nrhs
+        if sym is not None:  # potentials of the systems back to the whole mesh
+            sym.from_systems(nb, phi_ptr, ldp, stp, stream)
+            phi_ptr, ldp, stp = sym.full.data_ptr(), sym.n_full, sym.n_full * nrhs
         sizes = [(m * nrhs * na[1], m * max(nhead, 1) * na[1]) for (_, _, m), na in zip(segments, seg_arrays)]
         out = torch.empty((sum(a + b for a, b in sizes),), dtype=torch.complex128, device=dev)
         views, pos = [], 0
@@ -489,14 +622,14 @@ class B200Engine:
         if events:
             events[4].record()
         host = out.cpu().numpy()
-        flags = torch.cat([f.info[:nb], r.flags]).cpu().numpy()
-        if flags[nb + 1] != 0:
+        flags = torch.cat([f.info[:nbs], r.flags]).cpu().numpy()
+        if flags[nbs + 1] != 0:
             raise _lib.GreenFunctionEvaluationError(_lib.BEM_ERR_NAN, "Green function returned a NaN in the "
                                                     "interaction matrix.\nIt could be due to overlapping panels.")
-        if np.any(flags[:nb] != 0):
+        if np.any(flags[:nbs] != 0):
             raise _lib.SingularMatrixError(_lib.BEM_ERR_SINGULAR,
-                                           f"zero pivot in the LU factorisation (info={flags[:nb].tolist()})")
-        if flags[nb] != 0:
+                                           f"zero pivot in the LU factorisation (info={flags[:nbs].tolist()})")
+        if flags[nbs] != 0:
             raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
         res, pos = [], 0
         for (m, ndof, sf), (_, sk) in zip(views, sizes):
