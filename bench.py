@@ -302,6 +302,76 @@ def run_array(args):
     return 0
 
 
+def run_symmetric(args):
+    """--workload symmetric: the barge of the headline workload built with its
+    two symmetry planes (mesh_parallelepiped(reflection_symmetry=True): 4
+    systems of 1521 panels per frequency), omega linspace(0.05, 3, 60), one
+    solve_frequencies call per sweep: the refined mixed and the float64 engines
+    on the symmetric mesh against the refined mixed engine on the same faces
+    without symmetry; coefficients against the oracle's block-circulant solve
+    (capytaine's algorithm) at omega = 1.05, which is also timed on the host
+    cores as the CPU baseline."""
+    import torch
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.engine import B200Engine
+    from capytaine_b200.green_function import Delhommeau
+    from capytaine_b200.meshes import mesh_parallelepiped
+    from capytaine_b200.symmetry import block_structure
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    mesh = mesh_parallelepiped(size=(80, 20, 20), resolution=(104, 26, 26), reflection_symmetry=True).immersed_part()
+    body = FloatingBody(mesh, rigid_body_dofs(), name="barge_sym")
+    plain = FloatingBody(mesh.merged(), rigid_body_dofs(), name="barge")
+    st = block_structure(mesh)
+    gf = Delhommeau(tabulation_cache_dir=None)
+    out, results = {}, {}
+    for name, b, prec in (("mixed_symmetric", body, "mixed"), ("fp64_symmetric", body, "fp64"),
+                          ("mixed_plain", plain, "mixed")):
+        eng = B200Engine(green_function=gf, precision=prec, max_batch=args.batch)
+        eng.solve_frequencies(b, OMEGAS[:args.batch])  # warm-up
+        ms = []
+        for _ in range(max(1, args.sweeps)):
+            gf.clear_rankine_cache()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = eng.solve_frequencies(b, OMEGAS)
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        results[name] = res
+        t = float(np.median(ms))
+        out[name] = {"value": len(OMEGAS) / (t * 1e-3), "unit": UNIT, "ms_per_sweep": t, "sweeps": len(ms)}
+        eng.release()
+        del eng
+        torch.cuda.empty_cache()
+    # accuracy and the CPU baseline: the oracle's block-circulant solve at omega = 1.05
+    from oracle import oracle as O
+    cores = len(os.sched_getaffinity(0))
+    gfo = oracle_gf()
+    idx = int(np.argmin(np.abs(OMEGAS - 1.05)))
+    w = float(OMEGAS[idx])
+    t0 = time.perf_counter()
+    ref = O.solve_frequency_symmetric(gfo, mesh.merged(), st.submesh, st.nb_images, True, O.rigid_body_dofs(), w,
+                                      rho=RHO, g=G, wave_directions=(0.0,))
+    cpu_s = time.perf_counter() - t0
+    errs = {name: coefficient_error(results[name], idx, ref) for name in results}
+    line = {"metric": "freq solves/sec at N=6084 with two symmetry planes (4 systems of 1521)",
+            "value": out["mixed_symmetric"]["value"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "dtype": "c128 (assembly, residuals) / f32-tf32 (LU)", "data": "synthetic",
+            "config": {"workload": "barge 80x20x10m with xOz and yOz symmetry, 6 dofs + diffraction (heading 0), "
+                                   "omega linspace(0.05,3,60)", "nb_panels": int(mesh.nb_faces),
+                       "systems_per_frequency": st.nsys, "system_size": st.n_sys, "frequencies_per_batch": args.batch,
+                       "calls": "one solve_frequencies call per sweep of 60 frequencies"},
+            **out,
+            "symmetric_over_plain_mixed": out["mixed_symmetric"]["value"] / out["mixed_plain"]["value"],
+            "mixed_over_fp64_symmetric": out["mixed_symmetric"]["value"] / out["fp64_symmetric"]["value"],
+            "max_rel_err_vs_oracle_block_circulant": errs, "accuracy_omega": w,
+            "cpu_baseline": {"value": 1.0 / cpu_s, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"1 block-circulant frequency-solve (omega={w:.3f}) of the symmetric barge"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------------------
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
@@ -554,9 +624,11 @@ def main():
                     help="requests of the serving run (Poisson arrivals); 0 skips it")
     ap.add_argument("--arrival-rate", type=float, default=200.0)
     ap.add_argument("--slots", type=int, default=8)
-    ap.add_argument("--workload", default="barge", choices=["barge", "array", "bodies"],
+    ap.add_argument("--workload", default="barge", choices=["barge", "array", "bodies", "symmetric"],
                     help="array: the 3x3 cylinder array with lids (20000 panels), mixed vs float64 GMRES; "
-                         "bodies: 64 bodies of 300-3000 panels batched across bodies")
+                         "bodies: 64 bodies of 300-3000 panels batched across bodies; "
+                         "symmetric: the barge with its two symmetry planes")
+    ap.add_argument("--sweeps", type=int, default=3, help="timed sweeps per engine of --workload symmetric")
     ap.add_argument("--bodies", type=int, default=64)
     ap.add_argument("--bodies-stats", action="store_true", help="per-stage device times of the batched sweep")
     ap.add_argument("--array-frequencies", type=int, default=40)
@@ -569,6 +641,8 @@ def main():
         return run_array(args)
     if args.workload == "bodies":
         return run_bodies(args)
+    if args.workload == "symmetric":
+        return run_symmetric(args)
 
     import torch
     rank = int(os.environ.get("RANK", "0"))

@@ -43,3 +43,23 @@ def test_barge_6084_panels_two_frequencies(oracle_mod, default_oracle_gf, tmp_pa
     ref = [oracle_mod.solve_frequency(default_oracle_gf, mesh, oracle_mod.rigid_body_dofs(), w) for w in omegas]
     errs = coefficient_errors(res, ref, body.dofs)
     assert max(errs.values()) < 1e-5, errs
+
+
+def test_symmetric_barge_6084_panels(oracle_mod, default_oracle_gf, tmp_path):
+    """The barge built with its two symmetry planes: 4 systems of 1521 panels
+    per frequency, against the oracle's block-circulant solve."""
+    from capytaine_b200.engine import B200Engine
+    from capytaine_b200.symmetry import block_structure
+    from test_gpu_mixed import _shared_table_gf
+    from test_gpu_solve import coefficient_errors
+    mesh = mesh_parallelepiped(size=(80, 20, 20), resolution=(104, 26, 26), reflection_symmetry=True).immersed_part()
+    st = block_structure(mesh)
+    assert (mesh.nb_faces, st.kind, st.nsys, st.n_sys) == (6084, "reflections", 4, 1521)
+    body = FloatingBody(mesh, rigid_body_dofs())
+    omegas = [1.05, 2.5]
+    res = B200Engine(green_function=_shared_table_gf(default_oracle_gf, tmp_path), precision="mixed",
+                     max_batch=2).solve_frequencies(body, omegas)
+    ref = [oracle_mod.solve_frequency_symmetric(default_oracle_gf, mesh.merged(), st.submesh, 4, True,
+                                                oracle_mod.rigid_body_dofs(), w) for w in omegas]
+    errs = coefficient_errors(res, ref, body.dofs)
+    assert max(errs.values()) < 1e-5, errs
