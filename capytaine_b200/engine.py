@@ -193,6 +193,34 @@ class _Workspace:
         return self.f.nbytes + self.r.nbytes
 
 
+def _combine_first_column(st, W, src, cols_ptr, n_full, nb, out_ptr, ld_out, stride_out, stream):
+    """Systems k of nb first block columns (column-major n_full x n_sub at
+    cols_ptr + f * n_full * n_sub elements, image j at rows j n_sub) into out
+    (system f * nsys + k at out_ptr + that index * stride_out elements, leading
+    dimension ld_out): one bem_block_combine per (row part, column part) of
+    the macro-blocks."""
+    lib = _lib.load()
+    ns = st.n_sub
+    for a in range(st.q):
+        for b in range(st.q):
+            s = src[a][b]
+            _lib.check(lib.bem_block_combine(_vp(cols_ptr), n_full * ns, ns, n_full,
+                                             _vp(int(out_ptr) + 16 * (a * ns + b * ns * ld_out)), st.nsys * stride_out,
+                                             stride_out, ld_out, _vp(W), _vp(s) if s is not None else None, st.nsys,
+                                             st.nsys, ns, ns, nb, stream))
+
+
+def _transform_tensors(st, device):
+    """W, Winv and the per-(row part, column part) image maps on the device."""
+    import torch
+    W = torch.as_tensor(np.ascontiguousarray(st.W), dtype=torch.complex128, device=device)
+    Winv = torch.as_tensor(np.ascontiguousarray(st.Winv), dtype=torch.complex128, device=device)
+    src = [[None if st.q == 1 else
+            torch.as_tensor(np.ascontiguousarray(st.source[:, a, b]), dtype=torch.int32, device=device)
+            for b in range(st.q)] for a in range(st.q)]
+    return W, Winv, src
+
+
 class _SymWorkspace:
     """Buffers of the frequency-solves of a mesh with symmetries: the reduced
     systems (factors and right-hand sides of batch x nsys systems of size
@@ -206,12 +234,7 @@ class _SymWorkspace:
         self.r = _Rhs(st.n_sys, self.f.npad, batch * st.nsys, nrhs, device, precision)
         self.cols = torch.empty((2, batch, n_full * st.n_sub), dtype=torch.complex128, device=device)
         self.full = torch.zeros((batch, n_full * nrhs), dtype=torch.complex128, device=device)
-        self.W = torch.as_tensor(np.ascontiguousarray(st.W), dtype=torch.complex128, device=device)
-        self.Winv = torch.as_tensor(np.ascontiguousarray(st.Winv), dtype=torch.complex128, device=device)
-        # image block of each macro-block at each (row part, column part): None when it is the identity
-        self.src = [[None if st.q == 1 else
-                     torch.as_tensor(np.ascontiguousarray(st.source[:, a, b]), dtype=torch.int32, device=device)
-                     for b in range(st.q)] for a in range(st.q)]
+        self.W, self.Winv, self.src = _transform_tensors(st, device)
 
     @property
     def nbytes(self):
@@ -222,16 +245,8 @@ class _SymWorkspace:
         (`cols`: nb x (N x n_sub) column-major, image j at rows j n_sub) into
         `out` (system f * nsys + k at out + that index * stride_out, leading
         dimension ld_out)."""
-        st, lib = self.st, _lib.load()
-        ns, N = st.n_sub, self.n_full
-        for a in range(st.q):
-            for b in range(st.q):
-                src = self.src[a][b]
-                _lib.check(lib.bem_block_combine(_vp(cols), N * ns, ns, N,
-                                                 _vp(out.data_ptr() + 16 * (a * ns + b * ns * ld_out)),
-                                                 st.nsys * stride_out, stride_out, ld_out, _vp(self.W),
-                                                 _vp(src) if src is not None else None, st.nsys, st.nsys, ns, ns, nb,
-                                                 stream))
+        _combine_first_column(self.st, self.W, self.src, cols.data_ptr(), self.n_full, nb, out.data_ptr(), ld_out,
+                              stride_out, stream)
 
     def to_systems(self, nb, out, ld_out, stride_out, stream):
         """Right-hand sides of the whole mesh (self.full) to those of the systems."""
@@ -803,6 +818,16 @@ class B200Engine:
         self.last_computed_matrices = None
         params = dict(gf_params)
         params.setdefault("early_dot_product", True)
+        st = _shared_structure(mesh1, mesh2) if params["early_dot_product"] else None
+        if st is not None:
+            # bem/engines.py:178-247: the whole first mesh against the reference
+            # sub-mesh of the second, as block-circulant matrices
+            import torch
+            S, K = self.green_function.evaluate_device(mesh1.merged(), st.submesh, dtype=torch.complex128, **params)
+            self.last_computed_inputs = key
+            self.last_computed_matrices = (DeviceBlockCirculantMatrix(S, st, self),
+                                           DeviceBlockCirculantMatrix(K, st, self))
+            return self.last_computed_matrices
         S, K = self.green_function.evaluate_device(mesh1, mesh2, **params)
         self.last_computed_inputs = key
         self.last_computed_matrices = (DeviceMatrix(S, self), DeviceMatrix(K, self))
@@ -829,7 +854,7 @@ class B200Engine:
                 raise ValueError(f"Error in linear solver of {self}: the shape of the output is not the same "
                                  "as the shape of the RHS")
             return x
-        if not isinstance(A, DeviceMatrix):
+        if not isinstance(A, (DeviceMatrix, DeviceBlockCirculantMatrix)):
             A = DeviceMatrix(_to_device(np.asarray(A), self.device), self)
         if self._linear_solver == "gmres":
             x = A.gmres(np.asarray(b), atol=1e-6, rtol=1e-5, restart=self.gmres_restart, maxiter=self.gmres_maxiter)
@@ -840,9 +865,15 @@ class B200Engine:
         return x
 
     def compute_ram_estimation(self, problem):
-        """Device memory (GB) of S, K and the LU (bem/engines.py:348-398, no symmetry)."""
-        n = problem.body.mesh_including_lid.nb_faces if hasattr(problem.body, "mesh_including_lid") \
-            else problem.body.mesh.nb_faces
+        """Device memory (GB) of S, K and the LU (bem/engines.py:348-398): for a
+        mesh with symmetries the first block columns of S and K and the systems
+        of S and K (LU in place)."""
+        mesh = problem.body.mesh_including_lid if hasattr(problem.body, "mesh_including_lid") \
+            else problem.body.mesh
+        n = mesh.nb_faces
+        st = block_structure(mesh)
+        if st is not None:
+            return 16 * (2 * n * st.n_sub + 2 * st.nsys * padded_size(st.n_sys) ** 2) / 1e9
         return 3 * 16 * padded_size(n) ** 2 / 1e9
 
 
@@ -978,3 +1009,161 @@ class DeviceMatrix:
             out[:, c0:c1] = Bd[:, :n].T.cpu().numpy()
         x = out[:, 0] if vec else out.reshape(b.shape)
         return x.astype(np.complex64) if self.t.dtype == torch.complex64 else x
+
+
+def _structure_signature(mesh):
+    """Kind, planes, order and axis of the symmetries of a mesh (None: plain)."""
+    from .symmetric_meshes import ReflectionSymmetricMesh, RotationSymmetricMesh
+    if isinstance(mesh, ReflectionSymmetricMesh):
+        return ("reflection", mesh.plane, _structure_signature(mesh.half))
+    if isinstance(mesh, RotationSymmetricMesh):
+        return ("rotation", mesh.n, mesh.axis, _structure_signature(mesh.wedge))
+    return None
+
+
+def _shared_structure(mesh1, mesh2):
+    """Block structure of the matrices of mesh1 (collocation) against mesh2
+    (panels) when both have the same symmetries (the condition of
+    bem/engines.py:181-235), else None."""
+    if not hasattr(mesh1, "faces_centers"):
+        return None
+    sig = _structure_signature(mesh2)
+    if sig is None or _structure_signature(mesh1) != sig:
+        return None
+    st = block_structure(mesh2)
+    if st is None or mesh1.nb_faces != mesh2.nb_faces:
+        return None
+    return st
+
+
+class DeviceBlockCirculantMatrix:
+    """S or K between two meshes with the same symmetries, kept as its first
+    block column on the device and the independent systems of its
+    block-diagonalisation: what capytaine keeps as a BlockCirculantMatrix /
+    NestedBlockCirculantMatrix (tools/block_circulant_matrices.py:42-301).
+    ``M @ x`` applies the systems between the two transforms,
+    ``engine.linear_solver(M, b)`` factors the systems (batched float64 LU,
+    cached on the matrix, as LUDecomposedBlockCirculantMatrix) and solves, and
+    ``np.asarray(M)`` is the dense matrix."""
+
+    def __init__(self, cols, st, engine: B200Engine):
+        import torch
+        self.st, self.engine = st, engine
+        self.n = st.nb_images * st.n_sub
+        self.cols = cols  # (n, n_sub) column-major view: element (i, j) at i + j * n
+        dev = cols.device
+        self.W, self.Winv, self.src = _transform_tensors(st, dev)
+        self.systems = torch.empty((st.nsys, st.n_sys * st.n_sys), dtype=torch.complex128, device=dev)
+        _combine_first_column(st, self.W, self.src, cols.data_ptr(), self.n, 1, self.systems.data_ptr(), st.n_sys,
+                              st.n_sys * st.n_sys, _lib.stream_ptr())
+        self._lu = None
+
+    @property
+    def shape(self):
+        return (self.n, self.n)
+
+    @property
+    def dtype(self):
+        return np.dtype(np.complex64) if self.engine.green_function.floating_point_precision == "float32" \
+            else np.dtype(np.complex128)
+
+    def __array__(self, dtype=None, copy=None):
+        st = self.st
+        cols = self.cols.cpu().numpy()  # (n, n_sub)
+        a = st.full_matrix(cols.reshape(st.nb_images, st.n_sub, st.n_sub))
+        return a.astype(dtype if dtype is not None else self.dtype)
+
+    def _columns(self, x):
+        """(n, nrhs) complex128 right-hand side as a device (nrhs, n) tensor."""
+        import torch
+        x = np.asarray(x)
+        X = x.reshape(x.shape[0], -1).astype(np.complex128)
+        return torch.as_tensor(np.ascontiguousarray(X.T), device=self.systems.device), x.ndim == 1, x.shape
+
+    def _to_systems(self, Xd, ld):
+        """(nsys, nrhs, ld) device tensor of the right-hand sides of the systems (rows >= n_sys zero)."""
+        import torch
+        st = self.st
+        nrhs = Xd.shape[0]
+        Xh = torch.zeros((st.nsys, nrhs, ld), dtype=torch.complex128, device=Xd.device)
+        _lib.check(_lib.load().bem_block_combine(_vp(Xd), 0, st.n_sys, self.n, _vp(Xh), 0, nrhs * ld, ld,
+                                                 _vp(self.W), None, st.nsys, st.nsys, st.n_sys, nrhs, 1,
+                                                 _lib.stream_ptr()))
+        return Xh
+
+    def _from_systems(self, Yh, ld):
+        import torch
+        st = self.st
+        nrhs = Yh.shape[1]
+        Y = torch.empty((nrhs, self.n), dtype=torch.complex128, device=Yh.device)
+        _lib.check(_lib.load().bem_block_combine(_vp(Yh), 0, nrhs * ld, ld, _vp(Y), 0, st.n_sys, self.n,
+                                                 _vp(self.Winv), None, st.nsys, st.nsys, st.n_sys, nrhs, 1,
+                                                 _lib.stream_ptr()))
+        return Y
+
+    def _out(self, Y, vec, shape):
+        res = Y.T.cpu().numpy()
+        res = res.astype(self.dtype)
+        return res[:, 0] if vec else res.reshape(shape)
+
+    def __matmul__(self, x):
+        import torch
+        st = self.st
+        Xd, vec, shape = self._columns(x)
+        nrhs, ns = Xd.shape[0], st.n_sys
+        Xh = self._to_systems(Xd, ns)
+        Yh = torch.empty_like(Xh)
+        lib = _lib.load()
+        for c0 in range(0, nrhs, RHS_CHUNK):
+            nc = min(RHS_CHUNK, nrhs - c0)
+            work = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(ns, ns, nc, st.nsys)), dtype=torch.uint8,
+                               device=Xh.device)
+            _lib.check(lib.bem_zgemm_ts(ns, ns, nc, 1.0, 0.0, _vp(self.systems), ns, ns * ns,
+                                        _vp(Xh.data_ptr() + 16 * ns * c0), ns, nrhs * ns, 0.0, 0.0,
+                                        _vp(Yh.data_ptr() + 16 * ns * c0), ns, nrhs * ns, st.nsys, _vp(work),
+                                        _lib.stream_ptr()))
+        return self._out(self._from_systems(Yh, ns), vec, shape)
+
+    def _factor(self):
+        import torch
+        if self._lu is not None:
+            return self._lu
+        st = self.st
+        ns, npad = st.n_sys, padded_size(st.n_sys)
+        dev = self.systems.device
+        lib = _lib.load()
+        Kf = torch.zeros((st.nsys, npad, npad), dtype=torch.complex128, device=dev)  # Kf[k].T: column-major
+        Kf.transpose(1, 2)[:, :ns, :ns] = self.systems.view(st.nsys, ns, ns).transpose(1, 2)
+        stream = _lib.stream_ptr()
+        _lib.check(lib.bem_zpad_identity(_vp(Kf), npad, npad * npad, st.nsys, ns, npad, stream))
+        piv = torch.empty((st.nsys, npad), dtype=torch.int32, device=dev)
+        info = torch.zeros(st.nsys, dtype=torch.int32, device=dev)
+        work = torch.empty(int(lib.bem_zlu_workspace_bytes(npad, st.nsys)), dtype=torch.uint8, device=dev)
+        _lib.check(lib.bem_zlu_factor(_vp(Kf), npad, npad, npad * npad, st.nsys, _vp(piv), _vp(info), _vp(work),
+                                      stream))
+        bad = info.cpu().numpy()
+        if np.any(bad != 0):
+            raise _lib.SingularMatrixError(_lib.BEM_ERR_SINGULAR, f"zero pivot (info={bad.tolist()})")
+        self._lu = (Kf, piv, work, npad)
+        return self._lu
+
+    def solve(self, b):
+        import torch
+        Kf, piv, work, npad = self._factor()
+        st = self.st
+        Xd, vec, shape = self._columns(b)
+        nrhs = Xd.shape[0]
+        Bh = self._to_systems(Xd, npad)
+        err = torch.zeros(1, dtype=torch.int32, device=Bh.device)
+        _lib.check(_lib.load().bem_zlu_solve(_vp(Kf), npad, npad, npad * npad, st.nsys, _vp(piv), _vp(work), _vp(Bh),
+                                             npad, npad * nrhs, nrhs, _vp(err), _lib.stream_ptr()))
+        if int(err.item()) != 0:
+            raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
+        return self._out(self._from_systems(Bh, npad), vec, shape)
+
+    def gmres(self, b, **kw):
+        """capytaine's solve_gmres iterates on the whole operator: the dense
+        matrix on the device, then DeviceMatrix.gmres."""
+        import torch
+        dense = torch.as_tensor(np.asfortranarray(np.asarray(self, dtype=np.complex128)), device=self.systems.device)
+        return DeviceMatrix(dense, self.engine).gmres(b, **kw)

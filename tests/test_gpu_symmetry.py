@@ -71,10 +71,9 @@ def _oracle_ref(oracle_mod, gf, mesh, omegas, heads, lid=None):
     st = block_structure(mesh)
     full = mesh.merged()
     nested = st.kind in ("reflections", "dihedral")
-    hull = None
     return [oracle_mod.solve_frequency_symmetric(gf, full, st.submesh, st.nb_images, nested,
                                                  oracle_mod.rigid_body_dofs(), w, wave_directions=heads,
-                                                 hull_mask=hull if lid is None else lid) for w in omegas]
+                                                 hull_mask=lid) for w in omegas]
 
 
 @pytest.mark.parametrize("kind", ["reflection", "reflections", "rotation", "dihedral"])
@@ -136,3 +135,36 @@ def test_symmetric_engine_direct_method_and_lid(oracle_mod, default_oracle_gf, t
     ref = _oracle_ref(oracle_mod, default_oracle_gf, body.mesh_including_lid, omegas, (0.0,), lid=body.hull_mask)
     errs = coefficient_errors(res, ref, body.dofs)
     assert max(errs.values()) < 1e-5, errs
+
+
+@pytest.mark.parametrize("kind", ["reflection", "reflections", "rotation", "dihedral"])
+def test_matrix_engine_block_circulant_matrices(default_oracle_gf, tmp_path, kind):
+    """build_matrices on a mesh with symmetries returns block-circulant device
+    matrices (capytaine's _build_matrices_with_symmetries): dense form, product,
+    LU solve and GMRES against the dense matrices of the merged mesh."""
+    from capytaine_b200.engine import B200Engine, DeviceBlockCirculantMatrix
+    from test_gpu_mixed import _shared_table_gf
+    from test_symmetry_cpu import _symmetric_cases
+    gf = _shared_table_gf(default_oracle_gf, tmp_path)
+    mesh = _symmetric_cases(exact=True)[kind]
+    eng = B200Engine(green_function=gf)
+    S, K = eng.build_matrices(mesh, mesh, wavenumber=1.1)
+    assert isinstance(S, DeviceBlockCirculantMatrix) and isinstance(K, DeviceBlockCirculantMatrix)
+    assert K.shape == (mesh.nb_faces, mesh.nb_faces)
+    full = mesh.merged()
+    Sd, Kd = (np.asarray(m) for m in B200Engine(green_function=gf).build_matrices(full, full, wavenumber=1.1))
+    for a, b in ((S, Sd), (K, Kd)):
+        assert np.abs(np.asarray(a) - b).max() <= 1e-9 * np.abs(b).max()
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((mesh.nb_faces, 3)) + 1j * rng.standard_normal((mesh.nb_faces, 3))
+    np.testing.assert_allclose(S @ x, Sd @ x, rtol=0, atol=1e-9 * np.abs(Sd @ x).max())
+    ref = np.linalg.solve(Kd, x[:, 0])
+    got = eng.linear_solver(K, x[:, 0])
+    assert got.shape == x[:, 0].shape
+    assert np.abs(got - ref).max() <= 1e-9 * np.abs(ref).max()
+    got2 = eng.linear_solver(K, x)  # cached factors, several columns
+    assert np.abs(got2 - np.linalg.solve(Kd, x)).max() <= 1e-9 * np.abs(ref).max()
+    g = B200Engine(green_function=gf, linear_solver="gmres")
+    _, Kg = g.build_matrices(mesh, mesh, wavenumber=1.1)
+    xg = g.linear_solver(Kg, x[:, 0])
+    assert np.linalg.norm(Kd @ xg - x[:, 0]) <= 1e-5 * np.linalg.norm(x[:, 0]) * 1.01
