@@ -563,12 +563,15 @@ struct SymBatch {
   int64_t s_stride, k_stride;  // elements between the outputs of consecutive wavenumbers
 };
 
+// GENERAL: any collocation points (rows, a.n) against the panels of mesh2
+// (columns, a.nb_faces): every tile is evaluated, nothing is mirrored.
 // Five CTAs per SM (the shared-memory limit; 96 registers): 3% faster than four.
+template <bool GENERAL>
 __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_args a, TabView T, SymBatch kb,
                                                                int gf_sing, const double2* __restrict__ rank,
                                                                int64_t rank_ld) {
   const int bi = blockIdx.x, bj = blockIdx.y;
-  if (bi > bj) return;
+  if (!GENERAL && bi > bj) return;
   const double k = kb.k[blockIdx.z];
   a.S_dev = reinterpret_cast<double2*>(a.S_dev) + blockIdx.z * kb.s_stride;
   a.K_dev = reinterpret_cast<double2*>(a.K_dev) + blockIdx.z * kb.k_stride;
@@ -580,15 +583,18 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
   }
   const int tid = threadIdx.x;
   const int N = a.n;
+  const int NJ = GENERAL ? a.nb_faces : a.n;
   const int I0 = bi * kSymT, J0 = bj * kSymT;
+  const bool adjoint = a.adjoint_double_layer != 0;
   {
     const int J = J0 + tid;
-    if (J < N) {
+    if (J < NJ) {
       SymFace& f = faces[tid];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        f.x[d] = a.points_dev[3 * J + d];
-        f.dn[d] = a.dot_normals_dev[3 * J + d];
+        f.x[d] = a.quad_points_dev[3 * J + d];
+        // general: the dot normals are mesh2's only without the adjoint
+        f.dn[d] = (!GENERAL || !adjoint) ? a.dot_normals_dev[3 * J + d] : 0.0;
       }
       f.area = a.areas_dev[J];
       f.w = a.quad_weights_dev[J];
@@ -598,23 +604,22 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
   __syncthreads();
   const int I = I0 + tid;
   const bool row_ok = I < N;
-  const bool diag_tile = bi == bj;
-  const bool adjoint = a.adjoint_double_layer != 0;
-  double M[3] = {0, 0, 0}, nI[3] = {0, 0, 0}, wI = 0, zcI = 0;
+  const bool diag_tile = GENERAL || bi == bj;  // no mirrored entries
+  double M[3] = {0, 0, 0}, nI[3] = {0, 0, 0}, wI = 0;
   if (row_ok) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       M[d] = a.points_dev[3 * I + d];
-      nI[d] = a.dot_normals_dev[3 * I + d];
+      // general: the dot normals are the rows' only with the adjoint
+      nI[d] = (!GENERAL || adjoint) ? a.dot_normals_dev[3 * I + d] : 0.0;
     }
-    wI = a.quad_weights_dev[I];
-    zcI = a.centers_dev[3 * I + 2];
+    if (!GENERAL) wI = a.quad_weights_dev[I];
   }
   const double kwI = k * wI;
   double2* S = reinterpret_cast<double2*>(a.S_dev);
   double2* K = reinterpret_cast<double2*>(a.K_dev);
   bool nan_seen = false;
-  const int nJ = min(kSymT, N - J0);
+  const int nJ = min(kSymT, NJ - J0);
   for (int jc = 0; jc < nJ; jc += kSymChunk) {
 #pragma unroll 1
     for (int u = 0; u < kSymChunk; ++u) {
@@ -673,7 +678,8 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
                                      dm[0] * wi[0] + dm[1] * wi[1] + dm[2] * wi[2]);
         }
       }
-      if (a.diagonal_term && I == J) kre += (fabs(zcI - a.free_surface) < kLit1em8) ? 1.0 : 0.5;
+      // matrices.f90:348: the centre of face I (= J) of mesh2
+      if (a.diagonal_term && I == J) kre += (fabs(f.zc - a.free_surface) < kLit1em8) ? 1.0 : 0.5;
       S[(size_t)I + (size_t)a.lds * J] = make_double2(sre, sim);
       K[(size_t)I + (size_t)a.ldk * J] = make_double2(kre, kim);
       nan_seen |= isnan(sre) || isnan(sim) || isnan(kre) || isnan(kim);
@@ -809,7 +815,8 @@ namespace {
 // Shared by the single- and multi-wavenumber entry points: checks, then one
 // launch per group of up to kSymBatch wavenumbers (grid z = wavenumber).
 int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev, int64_t ld, const double* ks,
-                          int nk, int64_t s_stride, int64_t k_stride, void* stream, const char* who) {
+                          int nk, int64_t s_stride, int64_t k_stride, void* stream, const char* who,
+                          bool general = false) {
   char msg[200];
   if (!args || !rankine_dev || !ks || nk <= 0) {
     std::snprintf(msg, sizeof(msg), "%s: null pointer or no wavenumber", who);
@@ -822,8 +829,14 @@ int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev
     std::snprintf(msg, sizeof(msg), "%s: null output", who);
     return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
   }
-  if (a.n != a.nb_faces || a.nb_quad_points != 1 || a.points_dev != a.quad_points_dev ||
-      a.centers_dev != a.quad_points_dev) {
+  if (general) {
+    if (a.nb_quad_points != 1 || a.centers_dev != a.quad_points_dev) {
+      std::snprintf(msg, sizeof(msg), "%s: needs one quadrature point per face and the same array for the "
+                    "centres and the quadrature points", who);
+      return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+    }
+  } else if (a.n != a.nb_faces || a.nb_quad_points != 1 || a.points_dev != a.quad_points_dev ||
+             a.centers_dev != a.quad_points_dev) {
     std::snprintf(msg, sizeof(msg), "%s: needs one mesh, one quadrature point per face, and the same array for "
                   "points, centres and quadrature points", who);
     return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
@@ -841,7 +854,7 @@ int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev
     std::snprintf(msg, sizeof(msg), "%s: leading dimension < n", who);
     return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
   }
-  if (nk > 1 && (s_stride < a.lds * (int64_t)a.n || k_stride < a.ldk * (int64_t)a.n)) {
+  if (nk > 1 && (s_stride < a.lds * (int64_t)a.nb_faces || k_stride < a.ldk * (int64_t)a.nb_faces)) {
     std::snprintf(msg, sizeof(msg), "%s: output strides smaller than one matrix", who);
     return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
   }
@@ -856,7 +869,7 @@ int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev
   }
   const TabView T{a.tabulation_nb_integration_points, a.tabulation_grid_shape, a.nr, a.nz, a.r_range_dev,
                   a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0};
-  const int nb = ceil_div(a.n, kSymT);
+  const int nbi = ceil_div(a.n, kSymT), nbj = ceil_div(general ? a.nb_faces : a.n, kSymT);
   cudaStream_t s = (cudaStream_t)stream;
   int launches = 0;
   for (int k0 = 0; k0 < nk; k0 += kSymBatch) {
@@ -870,8 +883,12 @@ int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev
     ak.K_dev = reinterpret_cast<double2*>(a.K_dev) + (size_t)k0 * k_stride;
     {
       TimedLaunch tl(kKAssemble, s);
-      wave_symmetric_kernel<<<dim3(nb, nb, cnt), kSymT, 0, s>>>(ak, T, kb, a.gf_singularities,
-                                                                (const double2*)rankine_dev, ld);
+      if (general)
+        wave_symmetric_kernel<true><<<dim3(nbi, nbj, cnt), kSymT, 0, s>>>(ak, T, kb, a.gf_singularities,
+                                                                         (const double2*)rankine_dev, ld);
+      else
+        wave_symmetric_kernel<false><<<dim3(nbi, nbj, cnt), kSymT, 0, s>>>(ak, T, kb, a.gf_singularities,
+                                                                          (const double2*)rankine_dev, ld);
     }
     ++launches;
   }
@@ -895,4 +912,12 @@ extern "C" int bem_assemble_wave_symmetric_batched(const bem_assembly_args* args
   using namespace bem;
   return wave_symmetric_launch(args, rankine_dev, ld, wavenumbers_host, nk, s_stride, k_stride, stream,
                                "bem_assemble_wave_symmetric_batched");
+}
+
+extern "C" int bem_assemble_wave_cached(const bem_assembly_args* args, const void* rankine_dev, int64_t ld,
+                                        const double* wavenumbers_host, int nk, int64_t s_stride, int64_t k_stride,
+                                        void* stream) {
+  using namespace bem;
+  return wave_symmetric_launch(args, rankine_dev, ld, wavenumbers_host, nk, s_stride, k_stride, stream,
+                               "bem_assemble_wave_cached", true);
 }

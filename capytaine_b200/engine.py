@@ -466,7 +466,7 @@ class B200Engine:
             cstride = N * st.n_sub
             gf.assemble_into(full, st.submesh, ws.cols[0, 0], ws.cols[1, 0], wavenumber=ks[0], lds=N, ldk=N,
                              nan_flag=ws.r.nan, precision=self.assembly_precision, adjoint_double_layer=adjoint,
-                             sweep=(ks, cstride, cstride) if nb > 1 else None)
+                             sweep=(ks, cstride, cstride))
             ws.combine_matrices(ws.cols[0], nb, f.S, st.n_sys, st.n_sys * st.n_sys, stream)
             ws.combine_matrices(ws.cols[1], nb, f.K, f.ldk, f.strideK, stream)
             if ev:

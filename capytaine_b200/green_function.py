@@ -364,6 +364,20 @@ class Delhommeau:
                 return
             _lib.check(lib.bem_assemble_wave_symmetric(a, rank.data_ptr(), n, _lib.stream_ptr(stream)))
             return
+        if (reuse_rankine and sweep is not None and not same_mesh and hasattr(mesh1, "faces_centers")
+                and dm2.collocation_at_quadrature and need_wave and sing in ("low_freq", "high_freq")
+                and prec == "fp64" and dtype == _lib.BEM_DTYPE_C128 and early_dot_product
+                and 16 * n * dm2.nb_faces <= self.rankine_cache_bytes):
+            # Any points against a mesh over a sweep (the first block column of a
+            # mesh with symmetries): Rankine part once, wave term per wavenumber.
+            a.centers_dev = a.quad_points_dev = dm2.quad_points.data_ptr()
+            rank = self._rankine_part((mesh1.content_hash, mesh2.content_hash), dm2, a, bool(adjoint_double_layer),
+                                      sing, float(free_surface), stream, rows=n)
+            ks, s_stride, k_stride = sweep
+            kh = np.ascontiguousarray(np.asarray(ks, dtype=np.float64))
+            _lib.check(lib.bem_assemble_wave_cached(a, rank.data_ptr(), n, kh.ctypes.data_as(_lib.c_void_p), len(kh),
+                                                    int(s_stride), int(k_stride), _lib.stream_ptr(stream)))
+            return
         if sweep is not None:
             ks, s_stride, k_stride = sweep
             esize = S.element_size()
@@ -375,9 +389,10 @@ class Delhommeau:
             return
         _lib.check(lib.bem_assemble(a, _lib.stream_ptr(stream)))
 
-    def _rankine_part(self, mesh_key, dm, args, adjoint, sing, free_surface, stream):
-        """Device array of the wavenumber-independent Rankine part of a mesh with
-        itself (bem_assemble_rankine_part), cached per mesh and variant."""
+    def _rankine_part(self, mesh_key, dm, args, adjoint, sing, free_surface, stream, rows=None):
+        """Device array of the wavenumber-independent Rankine part of the rows
+        (collocation points, default: the mesh's own) against the faces of dm
+        (bem_assemble_rankine_part), cached per meshes and variant."""
         import torch
         key = (mesh_key, adjoint, sing == "high_freq", free_surface)
         with self._lock:
@@ -386,11 +401,12 @@ class Delhommeau:
                 self._rankine_cache.move_to_end(key)
                 hit.acquire()
                 return hit.tensors[0]
-            n = dm.nb_faces
+            N = dm.nb_faces
+            n = N if rows is None else rows
             while self._rankine_cache and (sum(e.tensors[0].numel() * 16 for e in self._rankine_cache.values())
-                                           + 16 * n * n > self.rankine_cache_bytes):
+                                           + 16 * n * N > self.rankine_cache_bytes):
                 self._rankine_cache.popitem(last=False)
-            rank = torch.empty((n, n), dtype=torch.complex128, device=self.device)
+            rank = torch.empty((N, n), dtype=torch.complex128, device=self.device)  # column-major n x N
             _lib.check(_lib.load().bem_assemble_rankine_part(args, rank.data_ptr(), n, _lib.stream_ptr(stream)))
             self._rankine_cache[key] = _lib.StreamShared(rank)
             return rank

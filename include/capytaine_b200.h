@@ -160,6 +160,17 @@ int bem_assemble_wave_symmetric_batched(const bem_assembly_args* args, const voi
                                         const double* wavenumbers_host, int nk, int64_t s_stride, int64_t k_stride,
                                         void* stream);
 
+/* Any collocation points (args->n) against a mesh (args->nb_faces panels, one
+ * quadrature point per face, the same device array for centers_dev and
+ * quad_points_dev) at nk wavenumbers, from a Rankine part made by
+ * bem_assemble_rankine_part with the same arguments: the wave term of every
+ * entry plus the cached part, outputs as in bem_assemble_wave_symmetric_batched.
+ * Same results as bem_assemble per wavenumber up to rounding.  The first block
+ * column of a mesh with symmetries (its whole mesh against the reference
+ * sub-mesh) across a frequency sweep.  No counterpart in the reference. */
+int bem_assemble_wave_cached(const bem_assembly_args* args, const void* rankine_dev, int64_t ld,
+                             const double* wavenumbers_host, int nk, int64_t s_stride, int64_t k_stride, void* stream);
+
 /* ---- dense complex128 linear algebra (batched) ---------------------------- */
 /* Matrices are column-major complex128 (interleaved re, im), `batch` of them
  * `stride` elements apart.  n must be a multiple of 64: pad the system with the

@@ -122,3 +122,35 @@ def test_batched_wavenumbers_equal_single_calls(default_oracle_gf, tmp_path, mes
         out[name] = (sv.cpu().numpy(), kv.cpu().numpy())
     _close(out["fast"][0], out["general"][0])
     _close(out["fast"][1], out["general"][1])
+
+
+@pytest.mark.parametrize("sing", ["low_freq", "high_freq"])
+@pytest.mark.parametrize("adjoint", [True, False])
+def test_cached_rankine_for_points_against_a_mesh(default_oracle_gf, tmp_path, sing, adjoint):
+    """bem_assemble_wave_cached (the first block column of a mesh with
+    symmetries across a sweep: whole mesh against its sub-mesh) against the
+    general kernel at each wavenumber, with lid panels on the free surface and
+    the diagonal entries of the first block."""
+    import torch
+    from capytaine_b200.symmetric_meshes import ReflectionSymmetricMesh
+    from capytaine_b200.symmetry import block_structure
+    keep_y_positive = dict(origin=(0.0, 0.0, 0.0), normal=(0.0, -1.0, 0.0))
+    half = Mesh.join_meshes(
+        mesh_sphere(radius=2.0, resolution=(10, 16)).immersed_part().clipped(**keep_y_positive),
+        mesh_rectangle(size=(1.6, 1.6), resolution=(4, 4), normal=(0, 0, 1)).clipped(**keep_y_positive))
+    mesh = ReflectionSymmetricMesh(half, plane="xOz")
+    full, sub = mesh.merged(), block_structure(mesh).submesh
+    fast = _gf(default_oracle_gf, tmp_path, gf_singularities=sing)
+    general = _gf(default_oracle_gf, tmp_path, gf_singularities=sing)
+    general.rankine_cache_bytes = 0
+    ks = [0.05, 1.3, 40.0]
+    n, N = full.nb_faces, sub.nb_faces
+    S = torch.empty((len(ks), N * n), dtype=torch.complex128, device="cuda")
+    K = torch.empty_like(S)
+    fast.assemble_into(full, sub, S[0], K[0], wavenumber=ks[0], adjoint_double_layer=adjoint, lds=n, ldk=n,
+                       sweep=(ks, N * n, N * n))
+    assert len(fast._rankine_cache) == 1
+    for i, k in enumerate(ks):
+        S0, K0 = general.evaluate(full, sub, wavenumber=k, adjoint_double_layer=adjoint)
+        _close(S[i].view(N, n).T.cpu().numpy(), S0)
+        _close(K[i].view(N, n).T.cpu().numpy(), K0)
