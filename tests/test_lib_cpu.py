@@ -78,6 +78,39 @@ def test_symmetric_assembly_preconditions_checked_on_host(lib):
     assert lib.bem_assemble_rankine_part(a, None, 12, None) == _lib.BEM_ERR_INVALID_ARGUMENT
 
 
+def test_cached_wave_and_block_combine_preconditions_checked_on_host(lib):
+    """Entry points of the symmetric engines refuse bad shapes before any launch."""
+    import ctypes
+    fake = 4096
+    a = _lib.AssemblyArgs(n=40, points_dev=8192, dot_normals_dev=fake, nb_faces=10, nb_vertices=4,
+                          vertices_dev=fake, faces_dev=fake, centers_dev=fake, normals_dev=fake, areas_dev=fake,
+                          radii_dev=fake, nb_quad_points=1, quad_points_dev=12288, quad_weights_dev=fake,
+                          wavenumber=1.0, free_surface=0.0, gf_singularities=_lib.BEM_GF_LOW_FREQ,
+                          adjoint_double_layer=1, early_dot_product=1, diagonal_term=1,
+                          precision=_lib.BEM_PREC_FP64, out_dtype=_lib.BEM_DTYPE_C128, S_dev=fake, K_dev=fake,
+                          lds=40, ldk=40)
+    ks = (ctypes.c_double * 2)(0.5, 1.0)
+    # the centres must be the quadrature points (one point per face)
+    assert lib.bem_assemble_wave_cached(a, fake, 40, ks, 2, 400, 400, None) == _lib.BEM_ERR_INVALID_ARGUMENT
+    a.quad_points_dev = fake
+    assert lib.bem_assemble_wave_cached(a, fake, 39, ks, 2, 400, 400, None) == _lib.BEM_ERR_INVALID_ARGUMENT  # ld
+    assert lib.bem_assemble_wave_cached(a, fake, 40, ks, 2, 399, 400, None) == _lib.BEM_ERR_INVALID_ARGUMENT
+    assert lib.bem_assemble_wave_cached(a, None, 40, ks, 2, 400, 400, None) == _lib.BEM_ERR_INVALID_ARGUMENT
+    bad = (ctypes.c_double * 1)(float("inf"))
+    assert lib.bem_assemble_wave_cached(a, fake, 40, bad, 1, 0, 0, None) == _lib.BEM_ERR_UNSUPPORTED
+    # block combine: sizes, pointers, grid limits
+    assert lib.bem_block_combine(fake, 0, 1, 8, fake, 0, 1, 8, fake, None, 2, 2, 8, 4, 0, None) == _lib.BEM_OK
+    assert lib.bem_block_combine(None, 0, 1, 8, fake, 0, 1, 8, fake, None, 2, 2, 8, 4, 1, None) \
+        == _lib.BEM_ERR_INVALID_ARGUMENT
+    assert lib.bem_block_combine(fake, 0, 1, 8, fake, 0, 1, 8, fake, None, 0, 2, 8, 4, 1, None) \
+        == _lib.BEM_ERR_INVALID_ARGUMENT
+    assert lib.bem_block_combine(fake, 0, 1, 7, fake, 0, 1, 8, fake, None, 2, 2, 8, 4, 1, None) \
+        == _lib.BEM_ERR_INVALID_ARGUMENT  # column stride < rows
+    assert lib.bem_block_combine(fake, 0, 1, 8, fake, 0, 1, 8, fake, None, 2, 2, 8, 70000, 1, None) \
+        == _lib.BEM_ERR_INVALID_ARGUMENT
+    assert b"65535" in lib.bem_last_error()
+
+
 _STRUCTS = {"bem_assembly_args": _lib.AssemblyArgs}
 
 
