@@ -566,10 +566,13 @@ struct SymBatch {
 // GENERAL: any collocation points (rows, a.n) against the panels of mesh2
 // (columns, a.nb_faces): every tile is evaluated, nothing is mirrored.
 // Five CTAs per SM (the shared-memory limit; 96 registers): 3% faster than four.
-template <bool GENERAL>
+// INPLACE: the Rankine part is K itself (rank == K, rank_ld == ldk); every
+// entry is read, then written, by one thread, and no entry is read after
+// another thread wrote it (tile (bi, bj), bi < bj, and its mirror (bj, bi)
+// belong to one CTA), so the read-only cache path is not used for it.
+template <bool GENERAL, bool INPLACE = false>
 __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_args a, TabView T, SymBatch kb,
-                                                               int gf_sing, const double2* __restrict__ rank,
-                                                               int64_t rank_ld) {
+                                                               int gf_sing, const double2* rank, int64_t rank_ld) {
   const int bi = blockIdx.x, bj = blockIdx.y;
   if (!GENERAL && bi > bj) return;
   const double k = kb.k[blockIdx.z];
@@ -634,7 +637,8 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
         const double zz = k * (M[2] + f.x[2]);
         self_fs = fabs(rr) < kLit1em10 && fabs(zz) < kLit1em10;
       }
-      const double2 rk = rank[(size_t)I + (size_t)rank_ld * J];
+      const size_t ridx = (size_t)I + (size_t)rank_ld * J;
+      const double2 rk = INPLACE ? rank[ridx] : __ldg(rank + ridx);
       double sre, sim, kre, kim;
       if (self_fs) {
         // Green_wave.f90:128-158, panel on the free surface with itself (I == J)
@@ -694,7 +698,8 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
         const int Ic = I0 + c;
         if (jc + u < nJ && Ic < N) {
           const double4 m = mir[u][c];
-          const double2 rk = rank[(size_t)J + (size_t)rank_ld * Ic];
+          const size_t ridx = (size_t)J + (size_t)rank_ld * Ic;
+          const double2 rk = INPLACE ? rank[ridx] : __ldg(rank + ridx);
           const double sre = kMinusOneOverFourPi * (rk.x + m.x), sim = kMinusOneOverFourPi * m.y;
           const double kre = kMinusOneOverFourPi * (rk.y + m.z), kim = kMinusOneOverFourPi * m.w;
           S[(size_t)J + (size_t)a.lds * Ic] = make_double2(sre, sim);
@@ -816,7 +821,7 @@ namespace {
 // launch per group of up to kSymBatch wavenumbers (grid z = wavenumber).
 int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev, int64_t ld, const double* ks,
                           int nk, int64_t s_stride, int64_t k_stride, void* stream, const char* who,
-                          bool general = false) {
+                          bool general = false, bool inplace = false) {
   char msg[200];
   if (!args || !rankine_dev || !ks || nk <= 0) {
     std::snprintf(msg, sizeof(msg), "%s: null pointer or no wavenumber", who);
@@ -886,6 +891,9 @@ int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev
       if (general)
         wave_symmetric_kernel<true><<<dim3(nbi, nbj, cnt), kSymT, 0, s>>>(ak, T, kb, a.gf_singularities,
                                                                          (const double2*)rankine_dev, ld);
+      else if (inplace)
+        wave_symmetric_kernel<false, true><<<dim3(nbi, nbj, cnt), kSymT, 0, s>>>(ak, T, kb, a.gf_singularities,
+                                                                                (const double2*)rankine_dev, ld);
       else
         wave_symmetric_kernel<false><<<dim3(nbi, nbj, cnt), kSymT, 0, s>>>(ak, T, kb, a.gf_singularities,
                                                                           (const double2*)rankine_dev, ld);
@@ -920,4 +928,24 @@ extern "C" int bem_assemble_wave_cached(const bem_assembly_args* args, const voi
   using namespace bem;
   return wave_symmetric_launch(args, rankine_dev, ld, wavenumbers_host, nk, s_stride, k_stride, stream,
                                "bem_assemble_wave_cached", true);
+}
+
+extern "C" int bem_assemble_symmetric(const bem_assembly_args* args, void* stream) {
+  using namespace bem;
+  if (!args || !args->K_dev) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_symmetric: null pointer");
+  const bem_assembly_args& a = *args;
+  if (a.n != a.nb_faces || a.nb_quad_points != 1 || a.points_dev != a.quad_points_dev ||
+      a.centers_dev != a.quad_points_dev)
+    return set_error(BEM_ERR_INVALID_ARGUMENT,
+                     "bem_assemble_symmetric: needs one mesh, one quadrature point per face, and the same array for "
+                     "points, centres and quadrature points");
+  if (a.out_dtype != BEM_DTYPE_C128 || a.precision != BEM_PREC_FP64)
+    return set_error(BEM_ERR_UNSUPPORTED, "bem_assemble_symmetric: complex128 outputs, float64 only");
+  if (!(a.wavenumber > 0.0) || !std::isfinite(a.wavenumber))
+    return set_error(BEM_ERR_UNSUPPORTED, "bem_assemble_symmetric: wavenumber must be finite and > 0");
+  // the Rankine part into K (same leading dimension), then the wave term in place
+  int st = bem_assemble_rankine_part(args, a.K_dev, a.ldk, stream);
+  if (st) return st;
+  const double k = a.wavenumber;
+  return wave_symmetric_launch(args, a.K_dev, a.ldk, &k, 1, 0, 0, stream, "bem_assemble_symmetric", false, true);
 }

@@ -131,6 +131,9 @@ class Delhommeau:
         # Rankine parts of mesh-with-itself assemblies, reused across wavenumbers
         # (device memory budget in bytes; 0 disables the reuse).
         self.rankine_cache_bytes = 4 << 30
+        # A mesh with itself without a reusable Rankine part: Rankine part into K,
+        # then the wave term once per pair of faces (False: the general kernel).
+        self.symmetric_assembly = True
         self._rankine_cache: "OrderedDict[tuple, object]" = OrderedDict()
         self.exportable_settings = {
             "green_function": self.__class__.__name__,
@@ -363,6 +366,24 @@ class Delhommeau:
                                                                    _lib.stream_ptr(stream)))
                 return
             _lib.check(lib.bem_assemble_wave_symmetric(a, rank.data_ptr(), n, _lib.stream_ptr(stream)))
+            return
+        if (self.symmetric_assembly and same_mesh and dm2.collocation_at_quadrature and need_wave
+                and sing in ("low_freq", "high_freq") and prec == "fp64" and dtype == _lib.BEM_DTYPE_C128
+                and early_dot_product and (ldk if ldk is not None else n) >= n):
+            # One wavenumber at a time, nothing reused: Rankine part into K, then the
+            # wave term once per pair of faces, in place.
+            q = dm2.quad_points.data_ptr()
+            a.points_dev = a.centers_dev = a.quad_points_dev = q
+            todo = [(float(wavenumber), 0, 0)]
+            if sweep is not None:
+                ks, s_stride, k_stride = sweep
+                todo = [(float(k), i * int(s_stride), i * int(k_stride)) for i, k in enumerate(ks)]
+            esize = S.element_size()
+            for k, so, ko in todo:
+                a.wavenumber = k
+                a.S_dev = S.data_ptr() + so * esize
+                a.K_dev = K.data_ptr() + ko * esize
+                _lib.check(lib.bem_assemble_symmetric(a, _lib.stream_ptr(stream)))
             return
         if (reuse_rankine and sweep is not None and not same_mesh and hasattr(mesh1, "faces_centers")
                 and dm2.collocation_at_quadrature and need_wave and sing in ("low_freq", "high_freq")

@@ -160,6 +160,13 @@ int bem_assemble_wave_symmetric_batched(const bem_assembly_args* args, const voi
                                         const double* wavenumbers_host, int nk, int64_t s_stride, int64_t k_stride,
                                         void* stream);
 
+/* S and K of a mesh with itself at one wavenumber (finite, > 0) with no cached
+ * Rankine part: bem_assemble_rankine_part into K_dev, then the wave term once
+ * per unordered pair of faces added in place.  Same requirements as
+ * bem_assemble_wave_symmetric; same results as bem_assemble up to rounding.
+ * One frequency of a body that is not seen again (a request of the server). */
+int bem_assemble_symmetric(const bem_assembly_args* args, void* stream);
+
 /* Any collocation points (args->n) against a mesh (args->nb_faces panels, one
  * quadrature point per face, the same device array for centers_dev and
  * quad_points_dev) at nk wavenumbers, from a Rankine part made by

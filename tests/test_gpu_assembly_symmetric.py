@@ -49,6 +49,7 @@ def test_symmetric_path_matches_general_kernel(default_oracle_gf, tmp_path, mesh
     fast = _gf(default_oracle_gf, tmp_path, gf_singularities=sing)
     general = _gf(default_oracle_gf, tmp_path, gf_singularities=sing)
     general.rankine_cache_bytes = 0
+    general.symmetric_assembly = False
     # small, medium and large k (the last one reaches the asymptotic branch)
     for k in (0.05, 1.3, 40.0):
         S, K = fast.evaluate(mesh, mesh, wavenumber=k, adjoint_double_layer=adjoint)
@@ -108,6 +109,7 @@ def test_batched_wavenumbers_equal_single_calls(default_oracle_gf, tmp_path, mes
     for name, cache in (("fast", 4 << 30), ("general", 0)):
         gf = _gf(default_oracle_gf, tmp_path)
         gf.rankine_cache_bytes = cache
+        gf.symmetric_assembly = cache > 0
         S = torch.full((len(ks), ld * n), float("nan"), dtype=torch.complex128, device="cuda")
         K = torch.full_like(S, float("nan"))
         gf.assemble_into(mesh, mesh, S[0], K[0], wavenumber=ks[0], lds=ld, ldk=ld, sweep=(ks, ld * n, ld * n))
@@ -143,6 +145,7 @@ def test_cached_rankine_for_points_against_a_mesh(default_oracle_gf, tmp_path, s
     fast = _gf(default_oracle_gf, tmp_path, gf_singularities=sing)
     general = _gf(default_oracle_gf, tmp_path, gf_singularities=sing)
     general.rankine_cache_bytes = 0
+    general.symmetric_assembly = False
     ks = [0.05, 1.3, 40.0]
     n, N = full.nb_faces, sub.nb_faces
     S = torch.empty((len(ks), N * n), dtype=torch.complex128, device="cuda")
@@ -154,3 +157,30 @@ def test_cached_rankine_for_points_against_a_mesh(default_oracle_gf, tmp_path, s
         S0, K0 = general.evaluate(full, sub, wavenumber=k, adjoint_double_layer=adjoint)
         _close(S[i].view(N, n).T.cpu().numpy(), S0)
         _close(K[i].view(N, n).T.cpu().numpy(), K0)
+
+
+@pytest.mark.parametrize("mesh_name", sorted(MESHES))
+@pytest.mark.parametrize("sing", ["low_freq", "high_freq"])
+@pytest.mark.parametrize("adjoint", [True, False])
+def test_in_place_symmetric_assembly_without_reuse(default_oracle_gf, tmp_path, mesh_name, sing, adjoint):
+    """bem_assemble_symmetric (Rankine part written into K, wave term added in
+    place, one wavenumber, nothing cached; the request server's assembly)
+    against the general kernel, with leading dimensions larger than n."""
+    import torch
+    mesh = MESHES[mesh_name]()
+    n = mesh.nb_faces
+    ld = n + 3
+    inplace = _gf(default_oracle_gf, tmp_path, gf_singularities=sing)
+    general = _gf(default_oracle_gf, tmp_path, gf_singularities=sing)
+    general.symmetric_assembly = False
+    for k in (0.05, 1.3, 40.0):
+        out = []
+        for gf in (inplace, general):
+            S = torch.full((n * ld,), float("nan"), dtype=torch.complex128, device="cuda")
+            K = torch.full_like(S, float("nan"))
+            gf.assemble_into(mesh, mesh, S, K, wavenumber=k, adjoint_double_layer=adjoint, lds=ld, ldk=ld,
+                             reuse_rankine=False)
+            out.append((S.view(n, ld)[:, :n].cpu().numpy(), K.view(n, ld)[:, :n].cpu().numpy()))
+        _close(out[0][0], out[1][0])
+        _close(out[0][1], out[1][1])
+    assert len(inplace._rankine_cache) == 0
