@@ -18,6 +18,7 @@
 //    (Delhommeau_integrals.f90:104-151).
 //  * Built with -ffp-contract=off so every operation rounds on its own.
 #include <cmath>
+#include <vector>
 #include <cstdint>
 #include <cstring>
 #include <climits>
@@ -529,6 +530,84 @@ void integral_of_reflected_Rankine(const f64* M, const f64* nodes, const f64* c,
   }
 }
 
+// Green_Rankine.f90:300-338: one-point term at the image c0 z + c1 of M.
+void one_point_integral_of_reflected_Rankine(const f64* M, const f64* c, f64 area, bool deriv_first, f64 c0, f64 c1,
+                                             f64& int_G, f64* int_nabla_G) {
+  f64 Mr[3] = {M[0], M[1], c0 * M[2] + c1};
+  one_point_integral_of_Rankine(Mr, c, area, true, int_G, int_nabla_G);
+  int_nabla_G[2] = c0 * int_nabla_G[2];
+  if (!deriv_first) {
+    int_nabla_G[0] = -int_nabla_G[0];
+    int_nabla_G[1] = -int_nabla_G[1];
+    if (c0 > 0) int_nabla_G[2] = -int_nabla_G[2];
+  }
+}
+
+// Green_wave.f90:283-290: image of a point through the sea bottom z = -depth.
+inline void bottom_image(const f64* x, f64 depth, f64* y) {
+  y[0] = x[0];
+  y[1] = x[1];
+  y[2] = -x[2] - 2 * depth;
+}
+
+// Green_wave.f90:311-425: four infinite-depth wave terms (point and face, each
+// possibly reflected through the sea bottom), scaled by Delhommeau's factor.
+void integral_of_wave_parts_finite_depth(const f64* x, const f64* face_center, f64 face_area, int nq,
+                                         const f64* quad_points, const f64* quad_weights, f64 k, f64 depth,
+                                         const Tabulation& T, int gf_sing, bool deriv_first, c64& int_G,
+                                         c64* int_nablaG) {
+  f64 x_sym[3], c_sym[3];
+  bottom_image(x, depth, x_sym);
+  bottom_image(face_center, depth, c_sym);
+  std::vector<f64> q_sym(3 * (size_t)nq);
+  for (int q = 0; q < nq; ++q) bottom_image(quad_points + 3 * q, depth, q_sym.data() + 3 * q);
+  int_G = {0, 0};
+  for (int a = 0; a < 3; ++a) int_nablaG[a] = {0, 0};
+  // (point, face, gradient's z component flipped?)
+  struct Term { const f64* p; const f64* c; const f64* q; bool flip_z; };
+  const Term terms[4] = {
+      {x, face_center, quad_points, false},
+      {x_sym, face_center, quad_points, deriv_first},
+      {x, c_sym, q_sym.data(), !deriv_first},
+      {x_sym, c_sym, q_sym.data(), true},
+  };
+  for (const Term& t : terms) {
+    c64 g, ng[3];
+    integral_of_wave_part_infinite_depth(t.p, t.c, face_area, nq, t.q, quad_weights, k, T, gf_sing, deriv_first, g,
+                                         ng);
+    if (t.flip_z) ng[2] = {-ng[2].re, -ng[2].im};
+    int_G = {int_G.re + g.re, int_G.im + g.im};
+    for (int a = 0; a < 3; ++a) int_nablaG[a] = {int_nablaG[a].re + ng[a].re, int_nablaG[a].im + ng[a].im};
+  }
+  const f64 amh = k * depth;
+  const f64 akh = amh * std::tanh(amh);
+  const f64 A = (amh + akh) * (amh + akh) / (4 * amh * (amh * amh - akh * akh + akh));
+  int_G = {A * int_G.re, A * int_G.im};
+  for (int a = 0; a < 3; ++a) int_nablaG[a] = {A * int_nablaG[a].re, A * int_nablaG[a].im};
+}
+
+// Green_wave.f90:427-508: each exponential (lambda_k, a_k) of the Prony
+// decomposition as four Rankine terms at images of M, weighted a_k / 2.
+void integral_of_prony_decomp_finite_depth(const f64* x, const f64* nodes, const f64* c, const f64* n, f64 area,
+                                           f64 R, f64 depth, int nexp, const f64* lambdas, const f64* amplitudes,
+                                           bool deriv_first, f64& int_G, f64* int_nablaG) {
+  int_G = ZERO;
+  int_nablaG[0] = int_nablaG[1] = int_nablaG[2] = ZERO;
+  for (int e = 0; e < nexp; ++e) {
+    const f64 lam = lambdas[e], a = amplitudes[e];
+    const f64 coefs[4][2] = {{ONE, depth * lam - 2 * depth},
+                             {-ONE, -depth * lam},
+                             {-ONE, depth * lam - 4 * depth},
+                             {ONE, -depth * lam + 2 * depth}};
+    for (const auto& cc : coefs) {
+      f64 g, dg[3];
+      integral_of_reflected_Rankine(x, nodes, c, n, area, R, deriv_first, cc[0], cc[1], g, dg);
+      int_G = int_G + a / 2 * g;
+      for (int d = 0; d < 3; ++d) int_nablaG[d] = int_nablaG[d] + a / 2 * dg[d];
+    }
+  }
+}
+
 struct MeshArgs {
   int n;                 // collocation points
   const f64* colloc;     // (n,3)
@@ -695,6 +774,137 @@ int oracle_build_matrices(int n, const double* colloc, const double* dot_normals
     }
   }
   return 0;
+}
+
+// matrices.f90:28-325, finite depth with Delhommeau's method (finite_depth_method
+// 0 = legacy: one-point free-surface image, 1 = newer).  prony: lambdas then
+// amplitudes (2 x nexp).  Same outputs as oracle_build_matrices.
+int oracle_build_matrices_finite_depth(int n, const double* colloc, const double* dot_normals, int N,
+                                       const double* vertices, const int32_t* faces, const double* centers,
+                                       const double* normals, const double* areas, const double* radii, int nq,
+                                       const double* quad_points, const double* quad_weights, double wavenumber,
+                                       double depth, int npts, int grid, const double* r_range, int nr,
+                                       const double* z_range, int nz, const double* tab, int method, int nexp,
+                                       const double* prony, int gf_sing, int adjoint, int kdim, double* S, double* K,
+                                       int nthreads) {
+  if (!std::isfinite(depth) || depth <= 0) return -1;
+  MeshArgs m{n, colloc, dot_normals, N, vertices, faces, centers, normals, areas, radii, nq, quad_points, quad_weights};
+  Tabulation T{npts, grid, r_range, nr, z_range, nz, tab};
+  const bool deriv_first = adjoint != 0;
+  const bool finite_wavenumber = (ZERO < wavenumber) && std::isfinite(wavenumber);
+  const f64 sign_refl = (gf_sing == HIGH_FREQ) ? -ONE : ONE;
+  const f64* lambdas = prony;
+  const f64* amplitudes = prony + nexp;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic)
+  for (int J = 0; J < N; ++J) {
+    f64 nodes[12];
+    gather_nodes(m, J, nodes);
+    const f64* cJ = centers + 3 * J;
+    const f64* nJ = normals + 3 * J;
+    for (int I = 0; I < n; ++I) {
+      const f64* M = colloc + 3 * I;
+      c64 int_G{0, 0};
+      c64 int_nablaG[3] = {{0, 0}, {0, 0}, {0, 0}};
+      f64 gR, nR[3];
+      auto add_real = [&](f64 coef, f64 g, const f64* dg) {
+        int_G.re = int_G.re + coef * g;
+        for (int a = 0; a < 3; ++a) int_nablaG[a].re = int_nablaG[a].re + coef * dg[a];
+      };
+      integral_of_Rankine(M, nodes, cJ, nJ, areas[J], radii[J], deriv_first, gR, nR);
+      add_real(ONE, gR, nR);
+      if (method == 0)
+        one_point_integral_of_reflected_Rankine(M, cJ, areas[J], deriv_first, -ONE, ZERO, gR, nR);
+      else
+        integral_of_reflected_Rankine(M, nodes, cJ, nJ, areas[J], radii[J], deriv_first, -ONE, ZERO, gR, nR);
+      add_real(sign_refl, gR, nR);
+      if (gf_sing == LOW_FREQ_WITH_RANKINE_PART) int_nablaG[2].re = int_nablaG[2].re + 2 * wavenumber * gR;
+      // images through the sea bottom, and through both boundaries
+      integral_of_reflected_Rankine(M, nodes, cJ, nJ, areas[J], radii[J], deriv_first, -ONE, -2 * depth, gR, nR);
+      add_real(ONE, gR, nR);
+      one_point_integral_of_reflected_Rankine(M, cJ, areas[J], deriv_first, ONE, -2 * depth, gR, nR);
+      add_real(sign_refl, gR, nR);
+      one_point_integral_of_reflected_Rankine(M, cJ, areas[J], deriv_first, ONE, 2 * depth, gR, nR);
+      add_real(sign_refl, gR, nR);
+      one_point_integral_of_reflected_Rankine(M, cJ, areas[J], deriv_first, -ONE, -4 * depth, gR, nR);
+      add_real(sign_refl, gR, nR);
+      if (finite_wavenumber) {
+        c64 gW, nW[3];
+        integral_of_wave_parts_finite_depth(M, cJ, areas[J], nq, quad_points + (size_t)3 * nq * J,
+                                            quad_weights + (size_t)nq * J, wavenumber, depth, T, gf_sing, deriv_first,
+                                            gW, nW);
+        int_G = {int_G.re + gW.re, int_G.im + gW.im};
+        for (int a = 0; a < 3; ++a) int_nablaG[a] = {int_nablaG[a].re + nW[a].re, int_nablaG[a].im + nW[a].im};
+      }
+      integral_of_prony_decomp_finite_depth(M, nodes, cJ, nJ, areas[J], radii[J], depth, nexp, lambdas, amplitudes,
+                                            deriv_first, gR, nR);
+      add_real(ONE, gR, nR);
+      size_t idx = (size_t)I + (size_t)n * J;
+      S[2 * idx] = MINUS_ONE_OVER_FOURPI * int_G.re;
+      S[2 * idx + 1] = MINUS_ONE_OVER_FOURPI * int_G.im;
+      if (kdim == 1) {
+        const f64* dn = adjoint ? dot_normals + 3 * I : dot_normals + 3 * J;
+        f64 re = dn[0] * int_nablaG[0].re + dn[1] * int_nablaG[1].re + dn[2] * int_nablaG[2].re;
+        f64 im = dn[0] * int_nablaG[0].im + dn[1] * int_nablaG[1].im + dn[2] * int_nablaG[2].im;
+        K[2 * idx] = MINUS_ONE_OVER_FOURPI * re;
+        K[2 * idx + 1] = MINUS_ONE_OVER_FOURPI * im;
+      } else {
+        for (int a = 0; a < 3; ++a) {
+          K[2 * (3 * idx + a)] = MINUS_ONE_OVER_FOURPI * int_nablaG[a].re;
+          K[2 * (3 * idx + a) + 1] = MINUS_ONE_OVER_FOURPI * int_nablaG[a].im;
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+// Green_wave.f90:311-425 at one (point, face) pair; out: G (re, im), gradient (3 x (re, im)).
+void oracle_wave_parts_finite_depth(const double* x, const double* face_center, double face_area, int nq,
+                                    const double* quad_points, const double* quad_weights, double k, double depth,
+                                    int npts, int grid, const double* r_range, int nr, const double* z_range, int nz,
+                                    const double* tab, int gf_sing, int deriv_first, double* out8) {
+  Tabulation T{npts, grid, r_range, nr, z_range, nz, tab};
+  c64 g, ng[3];
+  integral_of_wave_parts_finite_depth(x, face_center, face_area, nq, quad_points, quad_weights, k, depth, T, gf_sing,
+                                      deriv_first != 0, g, ng);
+  out8[0] = g.re;
+  out8[1] = g.im;
+  for (int a = 0; a < 3; ++a) {
+    out8[2 + 2 * a] = ng[a].re;
+    out8[3 + 2 * a] = ng[a].im;
+  }
+}
+
+// Green_wave.f90:50-124 at one (point, face) pair, same output layout.
+void oracle_wave_part_integral_infinite_depth(const double* x, const double* face_center, double face_area, int nq,
+                                              const double* quad_points, const double* quad_weights, double k,
+                                              int npts, int grid, const double* r_range, int nr,
+                                              const double* z_range, int nz, const double* tab, int gf_sing,
+                                              int deriv_first, double* out8) {
+  Tabulation T{npts, grid, r_range, nr, z_range, nz, tab};
+  c64 g, ng[3];
+  integral_of_wave_part_infinite_depth(x, face_center, face_area, nq, quad_points, quad_weights, k, T, gf_sing,
+                                       deriv_first != 0, g, ng);
+  out8[0] = g.re;
+  out8[1] = g.im;
+  for (int a = 0; a < 3; ++a) {
+    out8[2 + 2 * a] = ng[a].re;
+    out8[3 + 2 * a] = ng[a].im;
+  }
+}
+
+// Green_wave.f90:427-508 at one (point, face) pair; out: G, gradient (4 reals).
+void oracle_prony_decomp_finite_depth(const double* x, const double* nodes, const double* c, const double* n,
+                                      double area, double R, double depth, int nexp, const double* prony,
+                                      int deriv_first, double* out4) {
+  f64 g, dg[3];
+  integral_of_prony_decomp_finite_depth(x, nodes, c, n, area, R, depth, nexp, prony, prony + nexp, deriv_first != 0,
+                                        g, dg);
+  out4[0] = g;
+  out4[1] = dg[0];
+  out4[2] = dg[1];
+  out4[3] = dg[2];
 }
 
 // matrices.f90:329-364.  centers: (m,3) of the first m faces; K layout as above with (n, N) extents.

@@ -9,9 +9,14 @@ never does.
   restatement of libs/libDelhommeau/src, built by ``oracle/Makefile``), wrapped
   the way capytaine ``green_functions/delhommeau.py:116-261, 336-520`` and
   ``green_functions/abstract_green_function.py:30-72`` wrap the Fortran core.
+  Infinite depth, and finite depth by Delhommeau's method
+  (``matrices.f90:197-305``, ``Green_wave.f90:311-508``) with the Prony
+  decomposition of ``delhommeau.py:269-319`` restated here (seeded).
+* Symmetric meshes: the block-circulant algebra of
+  ``tools/block_circulant_matrices.py`` applied to the first block column.
 * Solver glue: ``bem/solver.py:145-215`` (indirect method), boundary conditions
   ``bem/problems_and_results.py:373-381, 440-449``, Airy waves
-  ``bem/airy_waves.py:19-102``, force integration ``bodies/bodies.py:238-250``,
+  ``bem/airy_waves.py:19-102`` (finite depth too), force integration ``bodies/bodies.py:238-250``,
   coefficients ``bem/problems_and_results.py:583-592``; the linear algebra is
   SciPy's ``lu_factor``/``lu_solve``, which is what the reference calls
   (``tools/block_circulant_matrices.py:361-385``).
@@ -63,6 +68,12 @@ def _load():
     lib.oracle_build_matrices.restype = i
     lib.oracle_add_diagonal_term.argtypes = [i, i, p, p, d, i, p]
     lib.oracle_add_rankine_term_only.argtypes = [i, p, p, i, p, p, p, p, p, p, i, i, p, p, i]
+    lib.oracle_build_matrices_finite_depth.argtypes = [i, p, p, i, p, p, p, p, p, p, i, p, p, d, d, i, i, p, i, p, i,
+                                                       p, i, i, p, i, i, i, p, p, i]
+    lib.oracle_build_matrices_finite_depth.restype = i
+    lib.oracle_wave_parts_finite_depth.argtypes = [p, p, d, i, p, p, d, d, i, i, p, i, p, i, p, i, i, p]
+    lib.oracle_wave_part_integral_infinite_depth.argtypes = [p, p, d, i, p, p, d, i, i, p, i, p, i, p, i, i, p]
+    lib.oracle_prony_decomp_finite_depth.argtypes = [p, p, p, p, d, d, d, i, p, i, p]
     lib.oracle_pi.restype = d
     return lib
 
@@ -142,7 +153,10 @@ class OracleDelhommeau:
 
     def __init__(self, *, tabulation_nr=676, tabulation_rmax=100.0, tabulation_nz=372, tabulation_zmin=-251.0,
                  tabulation_nb_integration_points=1001, tabulation_grid_shape="scaled_nemoh3",
-                 gf_singularities="low_freq", nthreads=0, tabulation=None):
+                 gf_singularities="low_freq", nthreads=0, tabulation=None, finite_depth_method="newer"):
+        if finite_depth_method not in ("legacy", "newer"):
+            raise ValueError(f"finite_depth_method {finite_depth_method!r} is outside the oracle")
+        self.finite_depth_method = finite_depth_method
         self.tabulation_nb_integration_points = int(tabulation_nb_integration_points)
         self.tabulation_grid_shape = tabulation_grid_shape
         self.tabulation_grid_shape_index = GRID_ENUM[tabulation_grid_shape]
@@ -223,22 +237,24 @@ class OracleDelhommeau:
         return S, K
 
     def evaluate(self, mesh1, mesh2, *, free_surface=0.0, water_depth=np.inf, wavenumber=1.0,
-                 adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True):
-        """delhommeau.py:405-520 (infinite depth)."""
+                 adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True, prony=None):
+        """delhommeau.py:405-520.  Finite water_depth: Delhommeau's finite-depth
+        Green function with the Prony decomposition of prony_decomposition(k h)
+        unless `prony` (2 x nexp: growth rates, then amplitudes) is given."""
         if free_surface == np.inf:
             if water_depth != np.inf:
                 raise ValueError("When setting free_surface=inf, the water depth should also be infinite")
             return self.evaluate_rankine_only(mesh1, mesh2, adjoint_double_layer=adjoint_double_layer,
                                               early_dot_product=early_dot_product)
-        if water_depth != np.inf:
-            raise NotImplementedError("finite depth is outside the oracle")
         pts, nrm = self._colloc_and_normals(mesh1, mesh2, adjoint_double_layer)
         n, N = pts.shape[0], mesh2.nb_faces
         kdim = 1 if early_dot_product else 3
         S = np.zeros((n, N), order="F", dtype=np.complex128)
         K = np.zeros((kdim, n, N), order="F", dtype=np.complex128)
         wavenumber = float(wavenumber)
-        if wavenumber == 0.0 and self.gf_singularities != "low_freq":
+        if water_depth < np.inf and self.finite_depth_method == "legacy" and self.gf_singularities != "low_freq":
+            sing = "low_freq"  # delhommeau.py:467-471
+        elif wavenumber == 0.0 and self.gf_singularities != "low_freq":
             sing = "low_freq"
         elif wavenumber == np.inf and self.gf_singularities != "high_freq":
             sing = "high_freq"
@@ -247,10 +263,21 @@ class OracleDelhommeau:
         else:
             sing = self.gf_singularities
         v, f, c, nn, a, r, nq, qp, qw = self._mesh_args(mesh2)
-        status = lib().oracle_build_matrices(n, _ptr(pts), _ptr(nrm), N, _ptr(v), _ptr(f), _ptr(c), _ptr(nn), _ptr(a),
-                                             _ptr(r), nq, _ptr(qp), _ptr(qw), wavenumber, float(water_depth),
-                                             *self._tab_args(), SING_ENUM[sing], int(adjoint_double_layer), kdim,
-                                             _ptr(S), _ptr(K), self.nthreads)
+        if water_depth < np.inf:
+            # delhommeau.py:492-497 and matrices.f90:197-305 (Delhommeau's method)
+            if prony is None:
+                prony = prony_decomposition(wavenumber * water_depth)
+            pr = _c(prony)
+            status = lib().oracle_build_matrices_finite_depth(
+                n, _ptr(pts), _ptr(nrm), N, _ptr(v), _ptr(f), _ptr(c), _ptr(nn), _ptr(a), _ptr(r), nq, _ptr(qp),
+                _ptr(qw), wavenumber, float(water_depth), *self._tab_args(),
+                0 if self.finite_depth_method == "legacy" else 1, pr.shape[1], _ptr(pr), SING_ENUM[sing],
+                int(adjoint_double_layer), kdim, _ptr(S), _ptr(K), self.nthreads)
+        else:
+            status = lib().oracle_build_matrices(n, _ptr(pts), _ptr(nrm), N, _ptr(v), _ptr(f), _ptr(c), _ptr(nn),
+                                                 _ptr(a), _ptr(r), nq, _ptr(qp), _ptr(qw), wavenumber,
+                                                 float(water_depth), *self._tab_args(), SING_ENUM[sing],
+                                                 int(adjoint_double_layer), kdim, _ptr(S), _ptr(K), self.nthreads)
         if status != 0:
             raise RuntimeError(f"oracle_build_matrices failed with status {status}")
         if diagonal_term_in_double_layer:
@@ -259,6 +286,137 @@ class OracleDelhommeau:
         if early_dot_product:
             K = K.reshape((n, N), order="F")
         return S, K
+
+
+    def wave_parts_finite_depth(self, x, face, k, depth, *, gf_singularities=None, deriv_first=True):
+        """Green_wave.f90:311-425 for a point and the first face of `face`:
+        (integral of G, integral of its gradient)."""
+        return self._pair_wave(x, face, k, depth, gf_singularities, deriv_first)
+
+    def wave_part_integral_infinite_depth(self, x, face, k, *, gf_singularities=None, deriv_first=True):
+        """Green_wave.f90:50-124 for a point and the first face of `face`."""
+        return self._pair_wave(x, face, k, None, gf_singularities, deriv_first)
+
+    def _pair_wave(self, x, face, k, depth, gf_singularities, deriv_first):
+        sing = SING_ENUM[gf_singularities or self.gf_singularities]
+        qp, qw = face.quadrature_points
+        x = _c(x)
+        c = _c(face.faces_centers[0])
+        q, w = _c(qp[0]), _c(qw[0])
+        out = np.zeros(8)
+        if depth is None:
+            lib().oracle_wave_part_integral_infinite_depth(_ptr(x), _ptr(c), float(face.faces_areas[0]), len(w),
+                                                           _ptr(q), _ptr(w), float(k), *self._tab_args(), sing,
+                                                           int(deriv_first), _ptr(out))
+        else:
+            lib().oracle_wave_parts_finite_depth(_ptr(x), _ptr(c), float(face.faces_areas[0]), len(w), _ptr(q),
+                                                 _ptr(w), float(k), float(depth), *self._tab_args(), sing,
+                                                 int(deriv_first), _ptr(out))
+        return complex(out[0], out[1]), out[2::2] + 1j * out[3::2]
+
+
+def prony_decomp_finite_depth(x, face, depth, prony, deriv_first=True):
+    """Green_wave.f90:427-508 for a point and the first face of `face`:
+    (integral of the Prony terms, its gradient), real."""
+    x = _c(x)
+    nodes = _c(face.vertices[face.faces[0]])
+    pr = _c(prony)
+    out = np.zeros(4)
+    lib().oracle_prony_decomp_finite_depth(_ptr(x), _ptr(nodes), _ptr(_c(face.faces_centers[0])),
+                                           _ptr(_c(face.faces_normals[0])), float(face.faces_areas[0]),
+                                           float(face.faces_radiuses[0]), float(depth), pr.shape[1], _ptr(pr),
+                                           int(deriv_first), _ptr(out))
+    return out[0], out[1:]
+
+
+# ---------------------------------------------------------------------------
+# Prony decomposition of the finite-depth Green function (restated from the
+# method that capytaine's tools/prony_decomposition.py implements and that
+# green_functions/delhommeau.py:269-319 applies, its default "python" method).
+class PronyFailure(RuntimeError):
+    pass
+
+
+def exponential_fit(X, F, m):
+    """Prony's method: approximate samples F = f(X) on the equispaced X by
+    sum_i a_i exp(lambda_i x) with at most m terms.  The linear prediction
+    F[j + m] = sum_l p_l F[j + m - l] is fitted by least squares, the roots z
+    of z^m - sum_l p_l z^(m - l) give lambda = Re log(z) / dx (roots where the
+    logarithm is undefined dropped, repeated rates merged, rates outside
+    (-20, 0) dropped), then the amplitudes are fitted by least squares."""
+    X, F = np.asarray(X, float), np.asarray(F, float)
+    n = len(F)
+    rows = np.array([F[j:j + m][::-1] for j in range(n - m)])   # F[j + m - 1], ..., F[j]
+    p, *_ = np.linalg.lstsq(rows, F[m:], rcond=None)
+    # z^m - p_1 z^(m-1) - ... - p_m, lowest degree first for polyroots
+    coeffs = np.concatenate([-p[::-1], [1.0]])
+    z = np.polynomial.polynomial.polyroots(coeffs)
+    z = z[(np.imag(z) != 0.0) | (np.real(z) >= 0.0)]
+    lam = np.unique(np.real(np.log(z.astype(complex)) / (X[1] - X[0])))
+    lam = lam[(lam > -20.0) & (lam < 0.0)]
+    E = np.exp(np.outer(X, lam))
+    a, *_ = np.linalg.lstsq(E, F, rcond=None)
+    return a, lam
+
+
+def exponential_fit_error(X, F, a, lam):
+    """Mean square error of sum_i a_i exp(lambda_i x) against F."""
+    return float(np.mean((np.exp(np.outer(X, lam)) @ a - F) ** 2))
+
+
+def best_exponential_fit(f, x_min, x_max, n_range, *, tol=1e-4, noise_std=0.01, rng=None):
+    """First number of terms in n_range whose fit on 4 m + 1 points has a mean
+    square error below tol on 8 m + 1 points; x_max is stretched by a random
+    factor 1 + noise_std U[0, 1) per attempt, so that a point where f is
+    singular (x = kh for the Green function, which is x_max when kh = 20) is
+    not hit twice.  The reference draws from an unseeded generator; here the
+    default generator is seeded, so that the oracle is deterministic."""
+    rng = np.random.default_rng(0) if rng is None else rng
+    for m in n_range:
+        xm = (1 + noise_std * rng.uniform()) * x_max
+        try:
+            X = np.linspace(x_min, xm, 4 * m + 1)
+            a, lam = exponential_fit(X, f(X), m)
+            X = np.linspace(x_min, xm, 8 * m + 1)
+            if exponential_fit_error(X, f(X), a, lam) < tol:
+                return a, lam
+        except Exception:  # a failed attempt moves on to the next size, as in the reference
+            continue
+    raise PronyFailure(f"no exponential decomposition in [{x_min}, {x_max}] for tol={tol} with m in {list(n_range)}")
+
+
+def prony_decomposition(kh, *, noise_std=0.01, rng=None):
+    """(2, nexp) array [growth rates; amplitudes] of the part of Delhommeau's
+    finite-depth Green function approximated by exponentials, at kh = k h
+    (delhommeau.py:296-319): the function of delhommeau.py:303-306 (or its
+    large-kh limit) on [-0.1, 20] with 4 to 30 terms and tol 1e-4."""
+    kh = float(kh)
+    if kh <= 0.1:
+        raise NotImplementedError(f"the finite-depth Green function is not evaluated for kh<=0.1 (kh={kh})")
+    if kh < 1e5:
+        t = np.tanh(kh)
+        sing = (1 + t) ** 2 / (1 - t ** 2 + t / kh)
+
+        def f(x):
+            with np.errstate(all="ignore"):  # x = kh is a removable singularity; an attempt hitting it fails
+                return (x + kh * t) * np.exp(x) / (x * np.sinh(x) - kh * t * np.cosh(x)) - sing / (x - kh) - 2
+    else:
+        def f(x):
+            return -2 / (1 + np.exp(-2 * x)) + 2
+    a, lam = best_exponential_fit(f, -0.1, 20.0, range(4, 31, 2), tol=1e-4, noise_std=noise_std, rng=rng)
+    return np.stack([lam, a])
+
+
+def finite_depth_wavenumber(omega, depth, g=9.81):
+    """Root k > 0 of omega^2 / g = k tanh(k h) (problems_and_results.py:159-163)."""
+    import scipy.optimize as so
+    w2g = omega ** 2 / g
+    if depth == np.inf:
+        return w2g
+    hi = max(w2g, 1.0) * 2 + 1.0 / depth
+    while hi * np.tanh(hi * depth) < w2g:
+        hi *= 2
+    return so.brentq(lambda k: k * np.tanh(k * depth) - w2g, 1e-12, hi, xtol=1e-15, rtol=1e-15)
 
 
 # ---------------------------------------------------------------------------
@@ -306,21 +464,28 @@ def rigid_body_dofs(rotation_center=(0.0, 0.0, 0.0), only=None) -> Dict[str, Dof
     return dofs
 
 
-def airy_waves_velocity(points, omega, k, g, beta):
-    """airy_waves.py:56-95, infinite depth (k*h >= 20 branch)."""
+def _depth_profiles(z, k, depth):
+    """cosh / sinh profiles of airy_waves.py:39-46, 76-81 (exp(kz) when k h >= 20)."""
+    if 0 <= k * depth < 20:
+        return np.cosh(k * (z + depth)) / np.cosh(k * depth), np.sinh(k * (z + depth)) / np.cosh(k * depth)
+    return np.exp(k * z), np.exp(k * z)
+
+
+def airy_waves_velocity(points, omega, k, g, beta, depth=np.inf):
+    """airy_waves.py:56-95."""
     x, y, z = points.T
     wbar = x * np.cos(beta) + y * np.sin(beta)
-    cih = np.exp(k * z)
-    sih = np.exp(k * z)
+    cih, sih = _depth_profiles(z, k, depth)
     v = g * k / omega * np.exp(1j * k * wbar) * np.array([np.cos(beta) * cih, np.sin(beta) * cih, -1j * sih])
     return v.T
 
 
-def airy_waves_pressure(points, omega, k, g, rho, beta):
-    """airy_waves.py:19-53 and 98-99, infinite depth."""
+def airy_waves_pressure(points, omega, k, g, rho, beta, depth=np.inf):
+    """airy_waves.py:19-53 and 98-99."""
     x, y, z = points.T
     wbar = x * np.cos(beta) + y * np.sin(beta)
-    phi = -1j * g / omega * np.exp(k * z) * np.exp(1j * k * wbar)
+    cih, _ = _depth_profiles(z, k, depth)
+    phi = -1j * g / omega * cih * np.exp(1j * k * wbar)
     return 1j * omega * rho * phi
 
 
@@ -346,7 +511,7 @@ def solve_gmres(A, b):
 
 def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: float, *, rho=1000.0, g=9.81,
                     wave_directions=(0.0,), free_surface=0.0, linear_solver="lu", hull_mask=None,
-                    method="indirect"):
+                    method="indirect", water_depth=np.inf):
     """One frequency-solve, indirect method (solver.py:188-207): assemble S and K at
     k = omega^2/g, factor K once, solve every radiation and diffraction RHS, take
     S @ sigma, integrate pressures.  Returns added mass, damping (dict of dict) and
@@ -357,14 +522,16 @@ def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: flo
     method="direct": the potential solves D phi = S bc (bem/solver.py:172-187)."""
     import scipy.linalg as sl
 
+    if water_depth != np.inf and (method == "direct" or hull_mask is not None or free_surface == np.inf):
+        raise NotImplementedError("finite depth: indirect method without lid in the oracle")
     if method == "direct":
         return _solve_frequency_direct(gf, mesh, dofs, omega, rho=rho, g=g, wave_directions=wave_directions)
     if hull_mask is not None:
         return _solve_frequency_with_lid(gf, mesh, dofs, omega, rho=rho, g=g, wave_directions=wave_directions,
                                          linear_solver=linear_solver, hull_mask=np.asarray(hull_mask, bool))
 
-    k = omega ** 2 / g if free_surface != np.inf else 0.0
-    S, K = gf.evaluate(mesh, mesh, free_surface=free_surface, water_depth=np.inf, wavenumber=k,
+    k = finite_depth_wavenumber(omega, water_depth, g) if free_surface != np.inf else 0.0
+    S, K = gf.evaluate(mesh, mesh, free_surface=free_surface, water_depth=water_depth, wavenumber=k,
                        adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True)
     lu = sl.lu_factor(K) if linear_solver == "lu" else None
     normals = mesh.faces_normals
@@ -375,7 +542,7 @@ def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: flo
         rhs_list.append(("rad", name, -1j * omega * disp))
     if free_surface != np.inf:
         for beta in wave_directions:
-            bc = -(airy_waves_velocity(mesh.faces_centers, omega, k, g, beta) * normals).sum(axis=1)
+            bc = -(airy_waves_velocity(mesh.faces_centers, omega, k, g, beta, water_depth) * normals).sum(axis=1)
             rhs_list.append(("dif", beta, bc))
     for kind, key, bc in rhs_list:
         rhs = bc.astype(np.complex128)
@@ -392,7 +559,8 @@ def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: flo
             results["added_mass"][key] = {d: float(np.real(f) / omega ** 2) for d, f in forces.items()}
             results["radiation_damping"][key] = {d: float(np.imag(f) / omega) for d, f in forces.items()}
         else:
-            fk = integrate_pressure(mesh, dofs, airy_waves_pressure(mesh.faces_centers, omega, k, g, rho, key))
+            fk = integrate_pressure(mesh, dofs, airy_waves_pressure(mesh.faces_centers, omega, k, g, rho, key,
+                                                                    water_depth))
             results["diffraction"][key] = forces
             results["froude_krylov"][key] = fk
             results["excitation"][key] = {d: forces[d] + fk[d] for d in forces}

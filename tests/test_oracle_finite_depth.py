@@ -1,0 +1,126 @@
+"""Finite-depth Delhommeau Green function of the oracle (Delhommeau's method,
+libs/libDelhommeau/src/matrices.f90:197-305, Green_wave.f90:311-508) and its
+Prony decomposition (green_functions/delhommeau.py:269-319, the "python"
+method), pinned on the reference's own tests in
+pytest/test_green_functions_finite_depth.py: known-answer Prony fits, the
+deep-water limits of the wave and Prony terms, high_freq against low_freq and
+the infinite-frequency limit, with the reference's tolerances.  The device
+kernels of finite depth are not built; this is the checker they will meet."""
+import numpy as np
+import pytest
+
+from capytaine_b200.meshes import Mesh, mesh_sphere
+
+
+def _face(z):
+    v = np.array([[0.0, 0.0, z], [1.0, 0.0, z], [1.0, 1.0, z], [0.0, 1.0, z]])
+    return Mesh(v, [[0, 1, 2, 3]], clean=False)
+
+
+FACES = {"immersed": _face(-1.0), "free_surface": _face(0.0)}
+
+
+def test_prony_two_exponentials(oracle_mod):
+    """test_green_functions_finite_depth.py:130-135"""
+    x = np.linspace(0.0, 1.0, 100)
+    a, lam = oracle_mod.exponential_fit(x, 2 * np.exp(-x) - 4 * np.exp(-2 * x), 2)
+    order = np.argsort(lam)
+    np.testing.assert_allclose(a[order], [-4.0, 2.0])
+    np.testing.assert_allclose(lam[order], [-2.0, -1.0])
+
+
+def test_best_fit_recovers_six_exponentials(oracle_mod):
+    """test_green_functions_finite_depth.py:138-148 (same seed and draws): the
+    amplitudes are recovered.  (The reference's second assertion compares the
+    reference rates with themselves; the fastest rate, -7.6, decays within the
+    first samples of [0, 100] and is not determined by them; the five others
+    are checked.)"""
+    rng = np.random.default_rng(seed=987654321)
+    a_ref = rng.uniform(-10.0, 10.0, size=6)
+    lam_ref = -rng.chisquare(1.0, size=6)
+
+    def f(x):
+        return sum(a_ref[i] * np.exp(lam_ref[i] * x) for i in range(6))
+    a, lam = oracle_mod.best_exponential_fit(f, 0.0, 100.0, range(2, 15), tol=1e-4, noise_std=0.0)
+    assert np.allclose(np.sort(a), np.sort(a_ref))
+    np.testing.assert_allclose(np.sort(lam)[1:], np.sort(lam_ref)[1:], rtol=1e-5)
+
+
+def test_prony_decomposition_domain(oracle_mod):
+    """test_green_functions_finite_depth.py:114-119, 151-162, 175-177."""
+    for kh in (0.10, 0.01):
+        with pytest.raises(NotImplementedError):
+            oracle_mod.prony_decomposition(kh)
+    for kh in (20.0, 1.0, np.inf):  # 20: x_max is the singular point without the random stretch
+        p = oracle_mod.prony_decomposition(kh)
+        assert p.shape[0] == 2 and 1 <= p.shape[1] <= 30 and np.all(p[0] < 0)
+    np.testing.assert_array_equal(oracle_mod.prony_decomposition(3.0), oracle_mod.prony_decomposition(3.0))
+
+
+@pytest.mark.parametrize("deriv_first", [True, False])
+@pytest.mark.parametrize("face_location,sing", [("immersed", "low_freq"), ("free_surface", "low_freq"),
+                                                ("immersed", "high_freq")])
+def test_deep_water_limit_of_wave_terms(default_oracle_gf, deriv_first, face_location, sing):
+    """test_green_functions_finite_depth.py:26-63: depth 1000, k = 1, rtol 1e-2."""
+    face = FACES[face_location]
+    x = face.faces_centers[0]
+    s_inf, k_inf = default_oracle_gf.wave_part_integral_infinite_depth(x, face, 1.0, gf_singularities=sing,
+                                                                       deriv_first=deriv_first)
+    s_fin, k_fin = default_oracle_gf.wave_parts_finite_depth(x, face, 1.0, 1000.0, gf_singularities=sing,
+                                                             deriv_first=deriv_first)
+    np.testing.assert_allclose(s_fin, s_inf, rtol=1e-2)
+    np.testing.assert_allclose(k_fin, k_inf, rtol=1e-2)
+
+
+@pytest.mark.parametrize("deriv_first", [True, False])
+@pytest.mark.parametrize("face_location", ["immersed", "free_surface"])
+def test_deep_water_limit_of_prony_terms(oracle_mod, deriv_first, face_location):
+    """test_green_functions_finite_depth.py:66-78: the Prony terms vanish at depth 1000."""
+    face = FACES[face_location]
+    decomp = oracle_mod.prony_decomposition(1000.0)
+    s, k = oracle_mod.prony_decomp_finite_depth(face.faces_centers[0], face, 1000.0, decomp, deriv_first)
+    np.testing.assert_allclose(s, 0.0, atol=1e-3)
+    np.testing.assert_allclose(k, 0.0, atol=1e-3)
+
+
+def test_high_freq_against_low_freq(oracle_mod, default_oracle_gf):
+    """test_green_functions_finite_depth.py:81-111: sphere, k = 1, depth 10."""
+    mesh = mesh_sphere().immersed_part()
+    decomp = oracle_mod.prony_decomposition(10.0)
+    out = {}
+    for sing in ("low_freq", "high_freq"):
+        gf = oracle_mod.OracleDelhommeau(gf_singularities=sing, tabulation=default_oracle_gf.tabulation)
+        out[sing] = gf.evaluate(mesh, mesh, water_depth=10.0, wavenumber=1.0, prony=decomp,
+                                diagonal_term_in_double_layer=False)
+    (S_low, K_low), (S_high, K_high) = out["low_freq"], out["high_freq"]
+    np.testing.assert_allclose(S_low, S_high, atol=1e-2 * np.linalg.norm(S_low))
+    np.testing.assert_allclose(K_low, K_high, atol=2e-2 * np.linalg.norm(K_low))
+
+
+def test_infinite_frequency_limit(oracle_mod, default_oracle_gf):
+    """test_green_functions_finite_depth.py:121-127: depth 10, k = 1000 against k = inf."""
+    gf = oracle_mod.OracleDelhommeau(gf_singularities="high_freq", tabulation=default_oracle_gf.tabulation)
+    mesh = mesh_sphere().immersed_part()
+    S_, K_ = gf.evaluate(mesh, mesh, water_depth=10.0, wavenumber=1000.0)
+    S, K = gf.evaluate(mesh, mesh, water_depth=10.0, wavenumber=np.inf)
+    np.testing.assert_allclose(S / np.linalg.norm(S), S_ / np.linalg.norm(S_), atol=1e-3)
+    np.testing.assert_allclose(K / np.linalg.norm(K), K_ / np.linalg.norm(K_), atol=1e-3)
+
+
+def test_deep_finite_depth_solve_approaches_infinite_depth(oracle_mod, default_oracle_gf):
+    """A hemisphere in 1000 m of water: the coefficients of the finite-depth
+    solve (Delhommeau's method, finite-depth Airy waves) approach those of the
+    infinite-depth solve."""
+    mesh = mesh_sphere(radius=1.0, resolution=(6, 12)).immersed_part()
+    dofs = oracle_mod.rigid_body_dofs(only=["Surge", "Heave"])
+    w = 1.5
+    deep = oracle_mod.solve_frequency(default_oracle_gf, mesh, dofs, w)
+    fin = oracle_mod.solve_frequency(default_oracle_gf, mesh, dofs, w, water_depth=1000.0)
+    for fam in ("added_mass", "radiation_damping"):
+        for d in ("Surge", "Heave"):
+            assert fin[fam][d][d] == pytest.approx(deep[fam][d][d], rel=1e-4), (fam, d)
+    for d in ("Surge", "Heave"):
+        assert abs(fin["excitation"][0.0][d] - deep["excitation"][0.0][d]) <= 1e-4 * abs(deep["excitation"][0.0][d])
+    assert oracle_mod.finite_depth_wavenumber(w, 1000.0) == pytest.approx(w ** 2 / 9.81, rel=1e-12)
+    k10 = oracle_mod.finite_depth_wavenumber(w, 10.0)
+    assert k10 * np.tanh(k10 * 10.0) == pytest.approx(w ** 2 / 9.81, rel=1e-13)
