@@ -167,3 +167,43 @@ def test_no_cpu_fallback():
     mesh = mesh_sphere(resolution=(4, 4)).immersed_part()
     with pytest.raises(_lib.BemError):
         gf.evaluate(mesh, mesh, wavenumber=1.0)
+
+
+def test_linear_algebra_arguments_checked_on_host(lib):
+    """Bad shapes, null pointers and misaligned workspaces are refused with
+    BEM_ERR_INVALID_ARGUMENT before anything reaches the device (the status
+    capytaine's callers map to a ValueError through _lib.check)."""
+    import ctypes
+    fake = 1 << 20          # 1 MiB-aligned, never dereferenced: each call fails its host checks
+    bad = _lib.BEM_ERR_INVALID_ARGUMENT
+    it, res = ctypes.c_int32(0), ctypes.c_double(0.0)
+    # identity padding: npad < n, lda < npad
+    assert lib.bem_zpad_identity(fake, 64, 4096, 1, 65, 64, None) == bad
+    assert lib.bem_zpad_identity(fake, 32, 4096, 1, 16, 64, None) == bad
+    assert lib.bem_zpad_identity(fake, 64, 4096, 1, 64, 64, None) == _lib.BEM_OK  # nothing to pad
+    assert lib.bem_zgemm(-1, 4, 4, 1.0, fake, 4, 16, fake, 4, 16, 0.0, fake, 4, 16, 1, None) == bad
+    assert lib.bem_zgemm(4, 4, 4, 1.0, None, 4, 16, fake, 4, 16, 0.0, fake, 4, 16, 1, None) == bad
+    # mixed LU: npad a multiple of 128 at least n, 1024-byte aligned workspace
+    assert lib.bem_clu_factor(fake, 100, 10000, 100, 100, 1, fake, fake, fake, fake, None) == bad
+    assert lib.bem_clu_factor(fake, 200, 40000, 200, 128, 1, fake, fake, fake, fake, None) == bad
+    assert lib.bem_clu_factor(fake, 100, 10000, 100, 128, 1, fake, fake, fake + 512, fake, None) == bad
+    assert b"1024-byte" in lib.bem_last_error()
+    assert lib.bem_clu_solve(fake, 100, 1, fake, fake, 128, 128, 1, fake, None) == bad
+    # refinement: nrhs in [1, 16], ldb >= npad
+    args = (fake, 100, 10000, 100, 128, 1, fake, fake, fake, fake, fake)
+    assert lib.bem_refine_solve(*args, 128, 128 * 17, 17, 1e-10, 10, fake, fake, fake, ctypes.byref(it),
+                                ctypes.byref(res), None) == bad
+    assert lib.bem_refine_solve(*args, 100, 100, 1, 1e-10, 10, fake, fake, fake, ctypes.byref(it),
+                                ctypes.byref(res), None) == bad
+    # GMRES: 256-byte aligned workspace, sizes
+    assert lib.bem_gmres_solve(fake, 100, 10000, 100, 128, 1, fake, fake, 128, 128, 1, 0.0, 1e-5, 20, 5, None,
+                               fake + 16, fake, ctypes.byref(it), ctypes.byref(res), None) == bad
+    assert lib.bem_gmres_solve(fake, 50, 10000, 100, 128, 1, fake, fake, 128, 128, 1, 0.0, 1e-5, 20, 5, None,
+                               fake, fake, ctypes.byref(it), ctypes.byref(res), None) == bad  # lda < n
+    assert lib.bem_gmres_workspace_bytes(100, 128, 1, 1, 20) > 0
+    # right-hand sides and forces: ldb < n, null outputs
+    assert lib.bem_build_rhs(100, 1, fake, fake, 9.81, 1, fake, 1, fake, fake, fake, None, fake, 99, 100 * 2,
+                             None) == bad
+    assert lib.bem_integrate_pressure(100, 1, 2, 1, fake, 99, 200, fake, 1000.0, fake, fake, None) == bad
+    assert lib.bem_integrate_pressure(100, 1, 2, 1, fake, 100, 200, fake, 1000.0, fake, None, None) == bad
+    assert lib.bem_froude_krylov(100, 1, 1, 0, fake, 1000.0, 9.81, fake, fake, fake, fake, None) == bad
