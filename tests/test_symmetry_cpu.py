@@ -234,3 +234,54 @@ def test_oracle_symmetric_solve_equals_dense_solve(oracle_mod, legacy_oracle_gf,
         a = np.array([sym["excitation"][beta][d] for d in dofs])
         b = np.array([dense["excitation"][beta][d] for d in dofs])
         assert np.abs(a - b).max() <= tol * np.abs(b).max()
+
+
+# ---- the reference's own mesh tests, on the same panels ---------------------------
+def _reflection_panel():
+    """pytest/test_meshes_reflection_symmetry.py:29-36"""
+    return Mesh(np.array([[0.5, 0.5, 0.0], [1.0, 0.5, 0.0], [1.0, 1.0, 0.0], [0.5, 1.0, 0.0]]), [[0, 1, 2, 3]],
+                clean=False)
+
+
+def _rotation_panel():
+    """pytest/test_meshes_rotation_symmetry.py:29-36"""
+    return Mesh(np.array([[0.5, 0.0, 0.0], [0.5, 0.0, -0.5], [0.5, 0.5, -0.5], [0.5, 0.5, 0.0]]), [[0, 1, 2, 3]],
+                clean=False)
+
+
+def test_reference_reflection_mesh_cases():
+    """test_meshes_reflection_symmetry.py:39-93: sizes, reflected centres, winding."""
+    for plane, axis in (("xOz", 1), ("yOz", 0)):
+        m = ReflectionSymmetricMesh(_reflection_panel(), plane=plane)
+        assert m.plane == plane and m.nb_faces == 2 and m.nb_vertices == 8
+        merged = m.merged()
+        assert merged.nb_vertices == 8 and merged.nb_faces == 2
+        assert np.isclose(merged.faces_centers[0, axis], 0.75) and np.isclose(merged.faces_centers[1, axis], -0.75)
+        assert np.isclose(merged.faces_normals[0, 2], 1.0) and np.isclose(merged.faces_normals[1, 2], 1.0)
+    nested = ReflectionSymmetricMesh(ReflectionSymmetricMesh(_reflection_panel(), plane="xOz"), plane="yOz")
+    assert nested.nb_faces == 4 and nested.nb_vertices == 16
+    assert nested.merged().nb_faces == 4 and nested.merged().nb_vertices == 16
+
+
+def test_reference_clipped_reflection_case():
+    """test_meshes_reflection_symmetry.py:248-256: the immersed part of a panel
+    crossing the free surface keeps the symmetry and half of the area."""
+    half = Mesh(np.array([[0, 0.5, -0.5], [0, 0.5, 0.5], [0, 1.5, 0.5], [0, 1.5, -0.5]]), [[0, 1, 2, 3]],
+                clean=False)
+    sym = ReflectionSymmetricMesh(half, plane="xOz")
+    wet = sym.immersed_part()
+    assert isinstance(wet, ReflectionSymmetricMesh)
+    assert np.isclose(wet.faces_areas.sum(), 0.5 * sym.faces_areas.sum())
+
+
+def test_reference_rotation_mesh_cases():
+    """test_meshes_rotation_symmetry.py:105-131: a rotation about Oz keeps the
+    symmetry, the merged faces are in the mesh's order, and mirroring commutes
+    with merging (face order included)."""
+    m = RotationSymmetricMesh(_rotation_panel(), 4)
+    assert isinstance(m.rotated_z(np.pi / 4), RotationSymmetricMesh)
+    np.testing.assert_allclose(m.merged().faces_centers, m.faces_centers)
+    np.testing.assert_allclose(m.merged().mirrored("xOz").faces_centers, m.mirrored("xOz").merged().faces_centers,
+                               atol=1e-15)
+    np.testing.assert_allclose(m.merged().mirrored("yOz").faces_centers, m.mirrored("yOz").merged().faces_centers,
+                               atol=1e-15)
