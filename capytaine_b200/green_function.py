@@ -154,6 +154,36 @@ class Delhommeau:
     def __hash__(self):
         return self._hash
 
+    def find_best_exponential_decomposition(self, dimensionless_wavenumber, *, method=None):
+        """Exponential decomposition [rates; amplitudes] (2 x nexp) of the part of
+        the finite-depth Green function at kh = dimensionless_wavenumber, as
+        capytaine's Delhommeau.find_best_exponential_decomposition
+        (delhommeau.py:269-334): method "python" (the default here and there)
+        is capytaine_b200.prony.green_function_decomposition, deterministic for
+        a given kh and cached (128 values); the legacy "fortran" method of Nemoh
+        is not part of this library."""
+        from . import prony
+        method = (method or self.finite_depth_prony_decomposition_method).lower()
+        if method == "fortran":
+            raise NotImplementedError("the legacy Fortran Prony decomposition is not part of capytaine_b200; "
+                                      "use method='python'")
+        if method != "python":
+            raise ValueError(f"Unrecognized name for the Prony decomposition method: {method!r}. "
+                             "Expected 'python' or 'fortran'.")
+        kh = float(dimensionless_wavenumber)
+        cache = self.__dict__.setdefault("_prony_cache", OrderedDict())
+        hit = cache.get(kh)
+        if hit is None:
+            try:
+                hit = prony.green_function_decomposition(kh)
+            except prony.PronyDecompositionFailure as e:
+                raise _lib.GreenFunctionEvaluationError(
+                    _lib.BEM_ERR_NOT_CONVERGED, f"{self} cannot evaluate finite depth Green function for kh={kh}") from e
+            cache[kh] = hit
+            while len(cache) > 128:
+                cache.popitem(last=False)
+        return hit.copy()
+
     def __str__(self):
         items = [f"{k}={v!r}" for k, v in self.exportable_settings.items()
                  if k in _default_parameters and v != _default_parameters[k]]
