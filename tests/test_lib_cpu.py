@@ -207,3 +207,34 @@ def test_linear_algebra_arguments_checked_on_host(lib):
     assert lib.bem_integrate_pressure(100, 1, 2, 1, fake, 99, 200, fake, 1000.0, fake, fake, None) == bad
     assert lib.bem_integrate_pressure(100, 1, 2, 1, fake, 100, 200, fake, 1000.0, fake, None, None) == bad
     assert lib.bem_froude_krylov(100, 1, 1, 0, fake, 1000.0, 9.81, fake, fake, fake, fake, None) == bad
+
+
+def test_c_program_links_against_the_library(lib):
+    """A plain C99 program (not C++) includes the header, links the shared
+    library and calls host-side entry points: what a non-Python host does
+    (a cgo or JNI shim compiles the same way)."""
+    src = r'''
+#include <stdio.h>
+#include "capytaine_b200.h"
+int main(void) {
+  double r[676], z[372];
+  if (bem_version() < 100) return 1;
+  if (bem_default_r_spacing(676, 100.0, BEM_GRID_SCALED_NEMOH3, r) != BEM_OK) return 2;
+  if (bem_default_z_spacing(372, -251.0, BEM_GRID_SCALED_NEMOH3, z) != BEM_OK) return 3;
+  if (bem_assemble(NULL, NULL) != BEM_ERR_INVALID_ARGUMENT) return 4;
+  if (bem_zgemm_ts_static_capacity() <= 0) return 5;
+  printf("%.17g %.17g %s\n", r[675], z[0], bem_last_error());
+  return 0;
+}
+'''
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "host.c")
+        exe = os.path.join(d, "host")
+        open(c, "w").write(src)
+        subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.dirname(HEADER), "-o", exe, c,
+                        "-L", libdir, "-lcapytaine_b200", f"-Wl,-rpath,{libdir}"], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    r = np.zeros(676)
+    lib.bem_default_r_spacing(676, 100.0, _lib.BEM_GRID_SCALED_NEMOH3, r.ctypes.data_as(ctypes.c_void_p))
+    assert float(out[0]) == r[-1]
