@@ -26,6 +26,8 @@ __all__ = [
     "mesh_rectangle",
     "mesh_parallelepiped",
     "mesh_vertical_cylinder",
+    "mesh_horizontal_cylinder",
+    "mesh_disk",
 ]
 
 
@@ -400,11 +402,18 @@ def _surface_of_revolution(profile_points, n):
     return verts, faces
 
 
-def mesh_sphere(*, radius=1.0, center=(0.0, 0.0, 0.0), resolution=(10, 10), axial_symmetry=False, name=None):
+def mesh_sphere(*, radius=1.0, center=(0.0, 0.0, 0.0), resolution=(10, 10), faces_max_radius=None,
+                axial_symmetry=False, name=None):
     """Sphere from a meridian of ntheta+1 points swept nphi times (capytaine
     spheres.py:26-66); with axial_symmetry a RotationSymmetricMesh of nphi
-    wedges (same faces, in the same order)."""
+    wedges (same faces, in the same order).  When the panels of `resolution`
+    are larger than faces_max_radius, ntheta = nphi = ceil(2 pi R / (sqrt(2)
+    faces_max_radius))."""
     ntheta, nphi = resolution
+    if faces_max_radius is not None:
+        perimeter = 2 * np.pi * radius
+        if np.hypot(perimeter / ntheta, perimeter / nphi) / 2 > faces_max_radius:
+            ntheta = nphi = int(np.ceil(perimeter / (np.sqrt(2) * faces_max_radius)))
     theta = np.linspace(0.0, np.pi, ntheta + 1)
     meridian = radius * np.stack([np.sin(theta), np.zeros_like(theta), -np.cos(theta)], axis=1)
     if axial_symmetry:
@@ -420,17 +429,35 @@ def mesh_ellipsoid(*, semi_axes=(1.0, 1.0, 1.0), center=(0.0, 0.0, 0.0), resolut
 
 
 def mesh_rectangle(*, size=(5.0, 5.0), center=(0.0, 0.0, 0.0), resolution=(5, 5), faces_max_radius=None,
-                   normal=(0.0, 0.0, 1.0), name=None) -> Mesh:
+                   normal=(0.0, 0.0, 1.0), reflection_symmetry=False, name=None):
     """One-sided rectangle (capytaine rectangles.py:26-100), built directly in the
     plane orthogonal to ``normal`` with panels oriented along ``normal``.  When
     the panels of ``resolution`` are larger than ``faces_max_radius``, the
     resolution becomes ceil(side / (sqrt(2) faces_max_radius)) per side
-    (rectangles.py:67-71)."""
+    (rectangles.py:67-71).  reflection_symmetry: the half y < 0 mirrored in
+    xOz (even number of panels across the width; centre and normal in the
+    plane y = 0)."""
+    assert len(size) == 2 and all(h > 0 for h in size), "Size of the rectangle mesh should be given as positive values."
+    assert len(resolution) == 2 and all(h > 0 for h in resolution), \
+        "Resolution of the rectangle mesh should be given as positive values."
+    assert all(i == int(i) for i in resolution), "Resolution of a rectangle should be given as integer values."
+    assert len(center) == 3, "Position of the center of a rectangle should be given a 3-ple of values."
     width, height = size
-    nw, nh = resolution
+    nw, nh = (int(i) for i in resolution)
     if faces_max_radius is not None and np.hypot(width / nw, height / nh) / 2 > faces_max_radius:
         nw = int(np.ceil(width / (np.sqrt(2) * faces_max_radius)))
         nh = int(np.ceil(height / (np.sqrt(2) * faces_max_radius)))
+    if reflection_symmetry:
+        from .symmetric_meshes import ReflectionSymmetricMesh
+        if nw % 2 == 1:
+            raise ValueError("To define a rectangle mesh with reflection symmetry, "
+                             "it should have an even number of panels in this direction.")
+        if not np.isclose(center[1], 0.0) or not np.isclose(normal[1], 0.0):
+            raise ValueError("To define a rectangle mesh with reflection symmetry, its center should be in the "
+                             "xOz plane (that is y=0) and so should also be its normal vector.")
+        half = mesh_rectangle(size=(width / 2, height), resolution=(nw // 2, nh), center=(0, -width / 4, 0),
+                              normal=normal)
+        return ReflectionSymmetricMesh(half, plane="xOz", name=name).translated(center)
     normal = np.asarray(normal, float)
     normal = normal / np.linalg.norm(normal)
     # In-plane axes: the reference builds the panel in x=0 with normal -x, then rotates.
@@ -464,7 +491,7 @@ def _rotation_aligning(a, b, eps=1e-8):
     return np.eye(3) + vx + vx @ vx * ((1 - c) / s ** 2)
 
 
-def mesh_parallelepiped(size=(1.0, 1.0, 1.0), center=(0, 0, 0), resolution=(4, 4, 4),
+def mesh_parallelepiped(size=(1.0, 1.0, 1.0), center=(0, 0, 0), resolution=(4, 4, 4), faces_max_radius=None,
                         missing_sides=frozenset(), reflection_symmetry=False, name=None):
     """Six rectangles with outward normals (capytaine rectangles.py:103-213).
     With reflection_symmetry: the quarter x < 0, y < 0 (its sides on the planes
@@ -472,6 +499,12 @@ def mesh_parallelepiped(size=(1.0, 1.0, 1.0), center=(0, 0, 0), resolution=(4, 4
     resolutions along x and y, centre on Oz)."""
     width, thickness, height = size
     nw, nth, nh = resolution
+    if faces_max_radius is not None:
+        dw, dh, dth = width / nw, height / nh, thickness / nth
+        if max(np.hypot(dw, dh), np.hypot(dw, dth), np.hypot(dth, dh)) / 2 > faces_max_radius:
+            nw = int(np.ceil(width / (np.sqrt(2) * faces_max_radius)))
+            nth = int(np.ceil(thickness / (np.sqrt(2) * faces_max_radius)))
+            nh = int(np.ceil(height / (np.sqrt(2) * faces_max_radius)))
     if reflection_symmetry:
         from .symmetric_meshes import ReflectionSymmetricMesh
         if nw % 2 == 1 or nth % 2 == 1:
@@ -508,12 +541,15 @@ def mesh_parallelepiped(size=(1.0, 1.0, 1.0), center=(0, 0, 0), resolution=(4, 4
 
 
 def mesh_vertical_cylinder(*, length=10.0, radius=1.0, center=(0, 0, 0), resolution=(2, 8, 10),
-                           reflection_symmetry=False, axial_symmetry=False, name=None, _theta_max=2 * np.pi):
+                           faces_max_radius=None, reflection_symmetry=False, axial_symmetry=False, name=None,
+                           _theta_max=2 * np.pi):
     """Closed vertical cylinder: bottom disc, lateral surface, top disc
     (capytaine cylinders.py:108-205).  reflection_symmetry: the half
     0 <= theta <= pi mirrored in yOz (even ntheta); axial_symmetry: one slice of
     angle 2 pi / ntheta repeated ntheta times about Oz."""
+    assert length > 0 and radius > 0, "Length and radius of a cylinder should be given as positive values."
     nr, ntheta, nz = resolution
+    nr, ntheta, nz = _cylinder_resolution(length, radius, nr, ntheta, nz, faces_max_radius)
     if reflection_symmetry and axial_symmetry:
         raise NotImplementedError("Vertical cylinders with both symmetries have not been implemented.")
     if reflection_symmetry or axial_symmetry:
@@ -545,3 +581,99 @@ def mesh_vertical_cylinder(*, length=10.0, radius=1.0, center=(0, 0, 0), resolut
     panels = [(j + i * (ntheta + 1), j + (i + 1) * (ntheta + 1), j + 1 + (i + 1) * (ntheta + 1), j + 1 + i * (ntheta + 1))
               for (i, j) in product(range(nz + 2 * len(r_range)), range(ntheta))]
     return Mesh(nodes, panels, name=name, clean=True).translated(center)
+
+
+def _cylinder_resolution(length, radius, nr, ntheta, nl, faces_max_radius):
+    """Resolution of a cylinder whose panels are at most faces_max_radius
+    (cylinders.py:148-157, 242-251): ceil(R / (sqrt(2) r)) along a radius,
+    2 ceil(pi R / (sqrt(2) r)) around, ceil(L / (sqrt(2) r)) along the axis."""
+    if faces_max_radius is None:
+        return nr, ntheta, nl
+    dr, dtheta, dl = radius / max(nr, 1e-300), 2 * np.pi * radius / ntheta, length / nl
+    if max(np.hypot(dr, dtheta), np.hypot(dtheta, dl)) / 2 > faces_max_radius:
+        nr = int(np.ceil(radius / (np.sqrt(2) * faces_max_radius)))
+        ntheta = 2 * int(np.ceil(np.pi * radius / (np.sqrt(2) * faces_max_radius)))
+        nl = int(np.ceil(length / (np.sqrt(2) * faces_max_radius)))
+    return nr, ntheta, nl
+
+
+def _rotated_to(mesh, a, b):
+    """The mesh rotated so that vector a points along b (a symmetric mesh keeps
+    its symmetry when a is already b; otherwise it is merged first)."""
+    a = np.asarray(a, float) / np.linalg.norm(a)
+    b = np.asarray(b, float) / np.linalg.norm(b)
+    R = _rotation_aligning(a, b)
+    if np.allclose(R, np.eye(3), rtol=0, atol=1e-15):
+        return mesh
+    m = mesh.merged()
+    return Mesh(m.vertices @ R.T, m._faces, quadrature_method=m.quadrature_method, name=m.name, clean=False)
+
+
+def mesh_disk(*, radius=1.0, center=(0.0, 0.0, 0.0), normal=(0.0, 0.0, 1.0), resolution=(3, 6),
+              faces_max_radius=None, reflection_symmetry=False, axial_symmetry=False, name=None,
+              _theta_max=2 * np.pi):
+    """One-sided disk (capytaine cylinders.py:26-105): nr rings of ntheta panels
+    (triangles at the centre), built in the plane x = 0 and turned so that
+    its normal is `normal`.  reflection_symmetry: the half y >= 0 mirrored in
+    xOz (even ntheta); axial_symmetry: one sector repeated ntheta times about
+    Oz (for a horizontal disk)."""
+    assert radius > 0, "Radius of the disk mesh should be given as a positive value."
+    assert len(resolution) == 2 and all(h > 0 for h in resolution), \
+        "Resolution of the disk mesh should be given as positive values."
+    assert all(i == int(i) for i in resolution), "Resolution of a disk should be given as integer values."
+    nr, ntheta = (int(i) for i in resolution)
+    if faces_max_radius is not None and np.hypot(radius / nr, 2 * np.pi * radius / ntheta) / 2 > faces_max_radius:
+        nr = int(np.ceil(radius / (np.sqrt(2) * faces_max_radius)))
+        ntheta = int(np.ceil(2 * np.pi * radius / (np.sqrt(2) * faces_max_radius)))
+    if reflection_symmetry and axial_symmetry:
+        raise NotImplementedError("Disks with both symmetries have not been implemented.")
+    if reflection_symmetry or axial_symmetry:
+        from .symmetric_meshes import ReflectionSymmetricMesh, RotationSymmetricMesh
+        if reflection_symmetry:
+            if ntheta % 2 == 1:
+                raise ValueError("To use the reflection symmetry of the mesh, "
+                                 "it should have an even number of panels in this direction.")
+            half = mesh_disk(radius=radius, resolution=(nr, ntheta // 2), _theta_max=_theta_max / 2)
+            mesh = ReflectionSymmetricMesh(half, plane="xOz", name=name)
+        else:
+            piece = mesh_disk(radius=radius, resolution=(nr, 1), _theta_max=_theta_max / ntheta)
+            mesh = RotationSymmetricMesh(piece, ntheta, axis="z+", name=name)
+    else:
+        theta_range = np.linspace(0, _theta_max, ntheta + 1)
+        r_range = np.linspace(0.0, radius, nr + 1)
+        nodes = np.array([(0.0, r * np.sin(t), -r * np.cos(t)) for (r, t) in product(r_range, theta_range)])
+        panels = [(j + i * (ntheta + 1), j + 1 + i * (ntheta + 1), j + 1 + (i + 1) * (ntheta + 1),
+                   j + (i + 1) * (ntheta + 1)) for (i, j) in product(range(nr), range(ntheta))]
+        mesh = Mesh(nodes, panels, name=name, clean=True)
+    mesh = _rotated_to(mesh, mesh.faces_normals[0], normal)
+    return mesh.translated(center, name=name)
+
+
+def mesh_horizontal_cylinder(*, length=10.0, radius=1.0, center=(0.0, 0.0, 0.0), resolution=(2, 8, 10),
+                             faces_max_radius=None, reflection_symmetry=False, name=None, _theta_max=2 * np.pi):
+    """Closed cylinder along Ox (capytaine cylinders.py:204-288): nx slices of
+    ntheta panels, two end disks of nr rings.  reflection_symmetry: the half
+    y >= 0 mirrored in xOz (even ntheta)."""
+    assert length > 0 and radius > 0, "Length and radius of a cylinder should be given as positive values."
+    assert len(resolution) == 3 and all(h >= 0 for h in resolution), \
+        "Resolution of a cylinder should be given as positive values."
+    nr, ntheta, nx = _cylinder_resolution(length, radius, *(int(i) for i in resolution), faces_max_radius)
+    if reflection_symmetry:
+        from .symmetric_meshes import ReflectionSymmetricMesh
+        if ntheta % 2 == 1:
+            raise ValueError("To use the reflection symmetry of the mesh, "
+                             "it should have an even number of panels in this direction.")
+        half = mesh_horizontal_cylinder(length=length, radius=radius, resolution=(nr, ntheta // 2, nx),
+                                        _theta_max=_theta_max / 2)
+        return ReflectionSymmetricMesh(half, plane="xOz", name=name).translated(center, name=name)
+    theta_range = np.linspace(0, _theta_max, ntheta + 1)
+    x_range = np.linspace(-length / 2, length / 2, nx + 1)
+    nodes = np.array([(x, radius * np.sin(t), -radius * np.cos(t)) for (x, t) in product(x_range, theta_range)])
+    panels = [(i + j * (ntheta + 1), i + 1 + j * (ntheta + 1), i + 1 + (j + 1) * (ntheta + 1),
+               i + (j + 1) * (ntheta + 1)) for (i, j) in product(range(ntheta), range(nx))]
+    mesh = Mesh(nodes, panels, name=name, clean=True)
+    if nr > 0:
+        side = mesh_disk(radius=radius, center=(-length / 2, 0, 0), normal=(-1, 0, 0), resolution=(nr, ntheta),
+                         _theta_max=_theta_max)
+        mesh = mesh.join_meshes(side, side.mirrored("yOz"), name=name)
+    return mesh.translated(center, name=name)
