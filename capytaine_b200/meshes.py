@@ -60,6 +60,8 @@ class Mesh:
         self._faces = _as_face_lists(faces)
         if clean and len(self._faces) > 0:
             self.vertices, self._faces = _clean_mesh(self.vertices, self._faces)
+        elif clean:
+            self.vertices = np.empty((0, 3))  # no face, so no used vertex (meshes/clean.py)
         self.quadrature_method = quadrature_method
         self.name = name
 
