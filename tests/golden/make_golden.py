@@ -11,6 +11,8 @@ Sources (paths inside the capytaine project):
 * pytest/test_consistency_with_Nemoh_2.py:36-58  - immersed sphere added mass.
 * pytest/test_consistency_with_Nemoh_2.py:101-153 - floating sphere at omega=1,2.
 * pytest/test_consistency_with_Nemoh_2.py:155-172 - same sphere, rho=450, g=1.625.
+* pytest/test_consistency_with_Nemoh_2.py:175-203 - same sphere in 10 m of water.
+* pytest/test_consistency_with_Nemoh_2.py:206-226 - two spheres 20 m apart in 10 m of water.
 The values are read from the test source with ``ast``; nothing is executed.
 """
 import ast
@@ -87,6 +89,24 @@ def main(ref_root):
                               "added_mass": ast.literal_eval(calls[0].args[1]),
                               "damping": ast.literal_eval(calls[1].args[1]),
                               "diffraction_force_polar": _complex_polar(calls[2].args[1])}
+    fn = funcs["test_floating_sphere_finite_depth"]
+    calls = _isclose_calls(fn)
+    # calls: A, B (omega 1), Kochin, F (omega 1), A, B (omega 2), F (omega 2)
+    golden["floating_sphere_finite_depth"] = {
+        "depth": 10.0,
+        "omega_1": {"added_mass": ast.literal_eval(calls[0].args[1]),
+                    "damping": ast.literal_eval(calls[1].args[1]),
+                    "diffraction_force_polar": _complex_polar(calls[3].args[1])},
+        "omega_2": {"added_mass": ast.literal_eval(calls[4].args[1]),
+                    "damping": ast.literal_eval(calls[5].args[1]),
+                    "diffraction_force_polar": _complex_polar(calls[6].args[1])},
+    }
+    fn = funcs["test_two_distant_spheres_in_finite_depth"]
+    calls = _isclose_calls(fn)
+    golden["two_spheres_finite_depth"] = {"depth": 10.0, "omega": 7.0, "radius": 0.5, "resolution": 4,
+                                          "spacing": 20.0,
+                                          "added_mass_surge": ast.literal_eval(calls[0].args[1]),
+                                          "damping_surge": ast.literal_eval(calls[1].args[1])}
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
     with open(out, "w") as f:
         json.dump(golden, f, indent=1)

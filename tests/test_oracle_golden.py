@@ -1,5 +1,6 @@
 """Pins the CPU oracle against the reference's own known answers
-(pytest/test_consistency_with_Nemoh_2.py, test_green_functions_fortran_core.py,
+(pytest/test_consistency_with_Nemoh_2.py, infinite and finite depth,
+test_green_functions_fortran_core.py,
 test_green_functions_table_density.py in the capytaine project)."""
 import numpy as np
 import pytest
@@ -42,6 +43,45 @@ def test_alien_sphere(legacy_oracle_gf, oracle_mod, golden):
     assert np.isclose(r["radiation_damping"]["Heave"]["Heave"], ref["damping"], atol=atol)
     mod, phase = ref["diffraction_force_polar"]
     assert np.isclose(r["diffraction"][0.0]["Heave"], mod * np.exp(1j * phase), rtol=1e-2)
+
+
+@pytest.fixture(scope="module")
+def legacy_finite_depth_gf(oracle_mod, legacy_oracle_gf):
+    """The Nemoh 2 settings of the reference's finite-depth tests
+    (test_consistency_with_Nemoh_2.py:23-33: legacy table, high_freq, legacy
+    finite-depth method).  The reference decomposes with Nemoh's Fortran
+    Prony routine there; the oracle uses capytaine's Python method, which
+    meets the same tolerances."""
+    return oracle_mod.OracleDelhommeau(tabulation_nr=328, tabulation_nz=46, tabulation_grid_shape="legacy",
+                                       tabulation_nb_integration_points=251, gf_singularities="high_freq",
+                                       finite_depth_method="legacy", tabulation=legacy_oracle_gf.tabulation)
+
+
+@pytest.mark.parametrize("key,omega,tol_ab,tol_f", [("omega_1", 1.0, 1e-3, 1e-3), ("omega_2", 2.0, 1e-2, 1e-2)])
+def test_floating_sphere_finite_depth_nemoh2(legacy_finite_depth_gf, oracle_mod, golden, key, omega, tol_ab, tol_f):
+    # test_consistency_with_Nemoh_2.py:175-203, with the reference's tolerances
+    ref = golden["floating_sphere_finite_depth"]
+    sphere = mesh_sphere(radius=1.0, resolution=(6, 12)).immersed_part()
+    atol = tol_ab * hemisphere_volume(sphere) * 1000.0
+    r = oracle_mod.solve_frequency(legacy_finite_depth_gf, sphere, oracle_mod.rigid_body_dofs(only=["Heave"]), omega,
+                                   water_depth=ref["depth"])
+    assert np.isclose(r["added_mass"]["Heave"]["Heave"], ref[key]["added_mass"], atol=atol)
+    assert np.isclose(r["radiation_damping"]["Heave"]["Heave"], ref[key]["damping"], atol=atol)
+    mod, phase = ref[key]["diffraction_force_polar"]
+    assert np.isclose(r["diffraction"][0.0]["Heave"], mod * np.exp(1j * phase), rtol=tol_f)
+
+
+def test_two_distant_spheres_finite_depth_nemoh2(legacy_finite_depth_gf, oracle_mod, golden):
+    # test_consistency_with_Nemoh_2.py:206-226: both spheres surge together
+    ref = golden["two_spheres_finite_depth"]
+    res = int(2 * np.pi * ref["radius"] * ref["resolution"])
+    buoy = mesh_sphere(radius=ref["radius"], resolution=(res, res)).immersed_part()
+    both, _ = buoy.join_meshes(buoy.translated((ref["spacing"], 0.0, 0.0)), return_masks=True)
+    vol = 2 * 4 / 3 * np.pi * ref["radius"] ** 3
+    r = oracle_mod.solve_frequency(legacy_finite_depth_gf, both, oracle_mod.rigid_body_dofs(only=["Surge"]),
+                                   ref["omega"], water_depth=ref["depth"], wave_directions=())
+    assert np.isclose(r["added_mass"]["Surge"]["Surge"], ref["added_mass_surge"], atol=1e-3 * vol * 1000.0)
+    assert np.isclose(r["radiation_damping"]["Surge"]["Surge"], ref["damping_surge"], atol=1e-2 * vol * 1000.0)
 
 
 def test_immersed_sphere(legacy_oracle_gf, oracle_mod, golden):
