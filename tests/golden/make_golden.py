@@ -13,6 +13,8 @@ Sources (paths inside the capytaine project):
 * pytest/test_consistency_with_Nemoh_2.py:155-172 - same sphere, rho=450, g=1.625.
 * pytest/test_consistency_with_Nemoh_2.py:175-203 - same sphere in 10 m of water.
 * pytest/test_consistency_with_Nemoh_2.py:206-226 - two spheres 20 m apart in 10 m of water.
+* pytest/test_consistency_with_Nemoh_2.py:228-270 - submerged sphere and horizontal cylinder,
+  4 x 4 added mass and damping (rows: influenced dofs, columns: radiating dofs).
 The values are read from the test source with ``ast``; nothing is executed.
 """
 import ast
@@ -107,6 +109,17 @@ def main(ref_root):
                                           "spacing": 20.0,
                                           "added_mass_surge": ast.literal_eval(calls[0].args[1]),
                                           "damping_surge": ast.literal_eval(calls[1].args[1])}
+    fn = funcs["test_multibody"]
+    for node in ast.walk(fn):
+        if isinstance(node, ast.Assign) and isinstance(node.targets[0], ast.Name) \
+                and node.targets[0].id == "data_from_nemoh_2":
+            table = _literal(node.value)
+    golden["multibody_sphere_cylinder"] = {
+        "omega": 1.0,
+        "dofs": ["cylinder_1__Surge", "cylinder_1__Heave", "sphere_0__Surge", "sphere_0__Heave"],
+        "added_mass": [row[0::2] for row in table],
+        "damping": [row[1::2] for row in table],
+    }
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
     with open(out, "w") as f:
         json.dump(golden, f, indent=1)

@@ -84,6 +84,28 @@ def test_two_distant_spheres_finite_depth_nemoh2(legacy_finite_depth_gf, oracle_
     assert np.isclose(r["radiation_damping"]["Surge"]["Surge"], ref["damping_surge"], atol=1e-2 * vol * 1000.0)
 
 
+def test_multibody_sphere_and_cylinder_nemoh2(legacy_oracle_gf, oracle_mod, golden):
+    # test_consistency_with_Nemoh_2.py:228-270: a submerged sphere and a submerged
+    # horizontal cylinder joined, surge and heave of each; the reference's table
+    # has the influenced dof along rows and the radiating dof along columns
+    from capytaine_b200.meshes import mesh_horizontal_cylinder
+    ref = golden["multibody_sphere_cylinder"]
+    cyl = mesh_horizontal_cylinder(length=5.0, radius=1.0, center=(1.5, 3, -3), resolution=(1, 10, 10))
+    sph = mesh_sphere(radius=1.0, center=(0, 0, -2), resolution=(5, 20))
+    both, (mc, ms) = cyl.join_meshes(sph, return_masks=True)
+    dofs = {f"{b}__{d}": oracle_mod.SubmeshDof(oracle_mod.rigid_body_dofs()[d], mask)
+            for b, mask in (("cylinder_1", mc), ("sphere_0", ms)) for d in ("Surge", "Heave")}
+    assert list(dofs) == ref["dofs"]
+    r = oracle_mod.solve_frequency(legacy_oracle_gf, both, dofs, ref["omega"], wave_directions=())
+    atol = 1e-3 * (hemisphere_volume(cyl) + hemisphere_volume(sph)) * 1000.0
+    A = np.array([[r["added_mass"][rad][inf] for rad in dofs] for inf in dofs])
+    B = np.array([[r["radiation_damping"][rad][inf] for rad in dofs] for inf in dofs])
+    np.testing.assert_allclose(A, ref["added_mass"], rtol=0, atol=atol)
+    np.testing.assert_allclose(B, ref["damping"], rtol=0, atol=atol)
+    # the oracle meets it with margin: 0.21 against the tolerance of 18
+    np.testing.assert_allclose(A, ref["added_mass"], rtol=0, atol=0.5)
+
+
 def test_immersed_sphere(legacy_oracle_gf, oracle_mod, golden):
     # test_consistency_with_Nemoh_2.py:36-58 (no free surface: Rankine kernel only)
     sphere = mesh_sphere(radius=1.0, resolution=(10, 40))
