@@ -522,10 +522,11 @@ def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: flo
     method="direct": the potential solves D phi = S bc (bem/solver.py:172-187)."""
     import scipy.linalg as sl
 
-    if water_depth != np.inf and (method == "direct" or hull_mask is not None or free_surface == np.inf):
-        raise NotImplementedError("finite depth: indirect method without lid in the oracle")
+    if water_depth != np.inf and (hull_mask is not None or free_surface == np.inf):
+        raise NotImplementedError("finite depth: no lid in the oracle")
     if method == "direct":
-        return _solve_frequency_direct(gf, mesh, dofs, omega, rho=rho, g=g, wave_directions=wave_directions)
+        return _solve_frequency_direct(gf, mesh, dofs, omega, rho=rho, g=g, wave_directions=wave_directions,
+                                       water_depth=water_depth)
     if hull_mask is not None:
         return _solve_frequency_with_lid(gf, mesh, dofs, omega, rho=rho, g=g, wave_directions=wave_directions,
                                          linear_solver=linear_solver, hull_mask=np.asarray(hull_mask, bool))
@@ -601,13 +602,13 @@ def _solve_frequency_with_lid(gf, mesh, dofs, omega, *, rho, g, wave_directions,
     return results
 
 
-def _solve_frequency_direct(gf, mesh, dofs, omega, *, rho, g, wave_directions):
+def _solve_frequency_direct(gf, mesh, dofs, omega, *, rho, g, wave_directions, water_depth=np.inf):
     """Direct method (bem/solver.py:172-187): S, D with adjoint_double_layer=False,
     potential = D^-1 (S bc), pressure i omega rho potential."""
     import scipy.linalg as sl
-    k = omega ** 2 / g
-    S, D = gf.evaluate(mesh, mesh, free_surface=0.0, water_depth=np.inf, wavenumber=k, adjoint_double_layer=False,
-                       early_dot_product=True, diagonal_term_in_double_layer=True)
+    k = finite_depth_wavenumber(omega, water_depth, g)
+    S, D = gf.evaluate(mesh, mesh, free_surface=0.0, water_depth=water_depth, wavenumber=k,
+                       adjoint_double_layer=False, early_dot_product=True, diagonal_term_in_double_layer=True)
     lu = sl.lu_factor(D)
     c, nrm = mesh.faces_centers, mesh.faces_normals
     results = {"added_mass": {}, "radiation_damping": {}, "excitation": {}, "diffraction": {}, "froude_krylov": {}}
@@ -619,8 +620,9 @@ def _solve_frequency_direct(gf, mesh, dofs, omega, *, rho, g, wave_directions):
         results["added_mass"][name] = {d: float(np.real(v) / omega ** 2) for d, v in f.items()}
         results["radiation_damping"][name] = {d: float(np.imag(v) / omega) for d, v in f.items()}
     for beta in wave_directions:
-        dif = integrate_pressure(mesh, dofs, pressure(-(airy_waves_velocity(c, omega, k, g, beta) * nrm).sum(axis=1)))
-        fk = integrate_pressure(mesh, dofs, airy_waves_pressure(c, omega, k, g, rho, beta))
+        dif = integrate_pressure(mesh, dofs, pressure(-(airy_waves_velocity(c, omega, k, g, beta, water_depth)
+                                                        * nrm).sum(axis=1)))
+        fk = integrate_pressure(mesh, dofs, airy_waves_pressure(c, omega, k, g, rho, beta, water_depth))
         results["diffraction"][beta] = dif
         results["froude_krylov"][beta] = fk
         results["excitation"][beta] = {d: dif[d] + fk[d] for d in dif}

@@ -9,7 +9,7 @@ kernels of finite depth are not built; this is the checker they will meet."""
 import numpy as np
 import pytest
 
-from capytaine_b200.meshes import Mesh, mesh_sphere
+from capytaine_b200.meshes import Mesh, mesh_sphere, mesh_vertical_cylinder
 
 
 def _face(z):
@@ -124,3 +124,23 @@ def test_deep_finite_depth_solve_approaches_infinite_depth(oracle_mod, default_o
     assert oracle_mod.finite_depth_wavenumber(w, 1000.0) == pytest.approx(w ** 2 / 9.81, rel=1e-12)
     k10 = oracle_mod.finite_depth_wavenumber(w, 10.0)
     assert k10 * np.tanh(k10 * 10.0) == pytest.approx(w ** 2 / 9.81, rel=1e-13)
+
+
+@pytest.mark.parametrize("method", ["indirect", "direct"])
+@pytest.mark.parametrize("k", [5.0, 10.0])
+def test_mccamy_and_fuchs(oracle_mod, default_oracle_gf, k, method):
+    """pytest/test_consistency_with_analytical_solutions.py:23-44: surge
+    excitation of a bottom-mounted vertical cylinder (R = 0.3 m, 1 m of water)
+    against McCamy and Fuchs's analytical solution, rtol 5%."""
+    from scipy.special import j0, jn, y0, yn
+    h, R, g, rho = 1.0, 0.3, 9.81, 1000.0
+    mesh = mesh_vertical_cylinder(radius=R, length=h, center=(0, 0, -h / 2), resolution=(0, 30, 20)).immersed_part()
+    omega = np.sqrt(g * k * np.tanh(k * h))
+    m0 = omega ** 2 / g
+    dy = y0(m0 * R) - yn(2, m0 * R)
+    dj = j0(m0 * R) - jn(2, m0 * R)
+    analytical = (4 * rho * g * h * R) * (-1j * 2 * h / R) * np.tanh(m0 * h) / (m0 * h) ** 2 * (dy + 1j * dj) / (
+        dy ** 2 + dj ** 2)
+    r = oracle_mod.solve_frequency(default_oracle_gf, mesh, oracle_mod.rigid_body_dofs(only=["Surge"]), omega,
+                                   water_depth=h, method=method)
+    np.testing.assert_allclose(r["excitation"][0.0]["Surge"], analytical, rtol=0.05)
