@@ -1,0 +1,57 @@
+"""The engine and Green-function seams on the host (no device call): settings
+exported as capytaine's (pytest/test_bem_solver.py:32-61), rejected options,
+the custom linear solver contract (pytest/test_bem_engines_basic_matrix_engine.py:
+56-95) and the repr (:25-27)."""
+import numpy as np
+import pytest
+
+from capytaine_b200.engine import B200Engine
+from capytaine_b200.green_function import Delhommeau
+
+
+def test_exportable_settings():
+    gf = Delhommeau(tabulation_nr=10, tabulation_nz=10, tabulation_grid_shape="legacy",
+                    tabulation_nb_integration_points=50, finite_depth_prony_decomposition_method="fortran",
+                    tabulation_cache_dir=None)
+    assert gf.exportable_settings["green_function"] == "Delhommeau"
+    assert gf.exportable_settings["tabulation_nb_integration_points"] == 50
+    assert gf.exportable_settings["tabulation_grid_shape"] == "legacy"
+    assert gf.exportable_settings["finite_depth_prony_decomposition_method"] == "fortran"
+    engine = B200Engine(green_function=gf)
+    assert engine.exportable_settings["engine"] == "B200Engine"
+    assert engine.exportable_settings["linear_solver"] == "lu_decomposition"
+    assert engine.exportable_settings["tabulation_nb_integration_points"] == 50
+    assert "Delhommeau" in repr(engine)
+    assert hash(gf) == hash(Delhommeau(tabulation_nr=10, tabulation_nz=10, tabulation_grid_shape="legacy",
+                                       tabulation_nb_integration_points=50,
+                                       finite_depth_prony_decomposition_method="fortran", tabulation_cache_dir=None))
+
+
+def test_rejected_options():
+    gf = Delhommeau(tabulation_cache_dir=None)
+    with pytest.raises(ValueError):
+        B200Engine(green_function=gf, precision="half")
+    with pytest.raises(NotImplementedError):
+        B200Engine(green_function=gf, linear_solver="cholesky")
+    with pytest.raises(ValueError):
+        B200Engine(green_function=gf, precision="mixed", linear_solver="gmres")
+    with pytest.raises(ValueError):
+        B200Engine(green_function=gf, method="galerkin")
+    with pytest.raises(ValueError):
+        B200Engine(green_function=gf, refinement="newton")
+    with pytest.raises(KeyError):
+        Delhommeau(tabulation_grid_shape="unknown", tabulation_cache_dir=None)
+    with pytest.raises(NotImplementedError):
+        Delhommeau(floating_point_precision="float16", tabulation_cache_dir=None)
+
+
+def test_custom_linear_solver_contract():
+    gf = Delhommeau(tabulation_cache_dir=None)
+    A = np.array([[2.0, 0.0], [0.0, 4.0]], dtype=complex)
+    b = np.array([2.0, 4.0], dtype=complex)
+    engine = B200Engine(green_function=gf, linear_solver=lambda A, b: np.linalg.solve(A, b))
+    np.testing.assert_allclose(engine.linear_solver(A, b), [1.0, 1.0])
+    assert engine.exportable_settings["linear_solver"].startswith("<function")
+    wrong = B200Engine(green_function=gf, linear_solver=lambda A, b: np.ones(3))
+    with pytest.raises(ValueError):
+        wrong.linear_solver(A, b)
