@@ -20,7 +20,6 @@ import ctypes
 import logging
 import math
 import threading
-import time
 import weakref
 from collections import OrderedDict
 from dataclasses import dataclass, field

@@ -15,7 +15,7 @@ from __future__ import annotations
 import hashlib
 from functools import cached_property
 from itertools import product
-from typing import List, Optional, Sequence
+from typing import List, Optional
 
 import numpy as np
 

@@ -27,7 +27,7 @@ import ctypes
 import os
 import subprocess
 from dataclasses import dataclass
-from typing import Dict, Optional, Sequence
+from typing import Dict, Sequence
 
 import numpy as np
 

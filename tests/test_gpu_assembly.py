@@ -12,7 +12,6 @@ import numpy as np
 import pytest
 
 from capytaine_b200.meshes import Mesh, mesh_sphere, mesh_rectangle, mesh_parallelepiped
-from conftest import hemisphere_volume
 
 pytestmark = pytest.mark.gpu
 

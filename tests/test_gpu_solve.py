@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from capytaine_b200 import _lib
-from capytaine_b200.meshes import mesh_sphere, mesh_parallelepiped
+from capytaine_b200.meshes import mesh_sphere
 
 pytestmark = pytest.mark.gpu
 
