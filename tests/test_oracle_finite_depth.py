@@ -5,7 +5,7 @@ method), pinned on the reference's own tests in
 pytest/test_green_functions_finite_depth.py: known-answer Prony fits, the
 deep-water limits of the wave and Prony terms, high_freq against low_freq and
 the infinite-frequency limit, with the reference's tolerances.  The device
-kernels of finite depth are not built; this is the checker they will meet."""
+kernels of finite depth are not built; these are the references they will be tested against."""
 import numpy as np
 import pytest
 
