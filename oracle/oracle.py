@@ -522,13 +522,14 @@ def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: flo
     method="direct": the potential solves D phi = S bc (bem/solver.py:172-187)."""
     import scipy.linalg as sl
 
-    if water_depth != np.inf and (hull_mask is not None or free_surface == np.inf):
-        raise NotImplementedError("finite depth: no lid in the oracle")
+    if water_depth != np.inf and free_surface == np.inf:
+        raise ValueError("When setting free_surface=inf, the water depth should also be infinite")
     if method == "direct":
         return _solve_frequency_direct(gf, mesh, dofs, omega, rho=rho, g=g, wave_directions=wave_directions,
                                        water_depth=water_depth)
     if hull_mask is not None:
         return _solve_frequency_with_lid(gf, mesh, dofs, omega, rho=rho, g=g, wave_directions=wave_directions,
+                                         water_depth=water_depth,
                                          linear_solver=linear_solver, hull_mask=np.asarray(hull_mask, bool))
 
     k = finite_depth_wavenumber(omega, water_depth, g) if free_surface != np.inf else 0.0
@@ -568,12 +569,13 @@ def solve_frequency(gf: OracleDelhommeau, mesh, dofs: Dict[str, Dof], omega: flo
     return results
 
 
-def _solve_frequency_with_lid(gf, mesh, dofs, omega, *, rho, g, wave_directions, linear_solver, hull_mask):
+def _solve_frequency_with_lid(gf, mesh, dofs, omega, *, rho, g, wave_directions, linear_solver, hull_mask,
+                              water_depth=np.inf):
     """solve_frequency for a mesh whose faces outside hull_mask are a lid."""
     import scipy.linalg as sl
-    k = omega ** 2 / g
-    S, K = gf.evaluate(mesh, mesh, free_surface=0.0, water_depth=np.inf, wavenumber=k, adjoint_double_layer=True,
-                       early_dot_product=True, diagonal_term_in_double_layer=True)
+    k = finite_depth_wavenumber(omega, water_depth, g)
+    S, K = gf.evaluate(mesh, mesh, free_surface=0.0, water_depth=water_depth, wavenumber=k,
+                       adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True)
     lu = sl.lu_factor(K) if linear_solver == "lu" else None
     c, nrm, area = mesh.faces_centers[hull_mask], mesh.faces_normals[hull_mask], mesh.faces_areas[hull_mask]
     N = mesh.nb_faces
@@ -594,8 +596,8 @@ def _solve_frequency_with_lid(gf, mesh, dofs, omega, *, rho, g, wave_directions,
         results["added_mass"][name] = {d: float(np.real(v) / omega ** 2) for d, v in f.items()}
         results["radiation_damping"][name] = {d: float(np.imag(v) / omega) for d, v in f.items()}
     for beta in wave_directions:
-        dif = forces(solve(-(airy_waves_velocity(c, omega, k, g, beta) * nrm).sum(axis=1)))
-        fk = forces(airy_waves_pressure(c, omega, k, g, rho, beta))
+        dif = forces(solve(-(airy_waves_velocity(c, omega, k, g, beta, water_depth) * nrm).sum(axis=1)))
+        fk = forces(airy_waves_pressure(c, omega, k, g, rho, beta, water_depth))
         results["diffraction"][beta] = dif
         results["froude_krylov"][beta] = fk
         results["excitation"][beta] = {d: dif[d] + fk[d] for d in dif}

@@ -29,12 +29,14 @@ def test_lid_leaves_the_hull_blocks_unchanged(oracle_mod, default_oracle_gf, bod
         np.testing.assert_allclose(K_w[:n, :n], K_o, atol=1e-8)
 
 
-def test_lid_and_the_forces(oracle_mod, default_oracle_gf, bodies):
+@pytest.mark.parametrize("water_depth", [np.inf, 10.0])
+def test_lid_and_the_forces(oracle_mod, default_oracle_gf, bodies, water_depth):
     without, with_lid = bodies
     dofs = oracle_mod.rigid_body_dofs(only=["Heave"])
-    omega = np.sqrt(9.81 * 2 * np.pi / 3.0)  # wavelength 3 m
-    r_o = oracle_mod.solve_frequency(default_oracle_gf, without.mesh, dofs, omega)
+    k = 2 * np.pi / 3.0  # wavelength 3 m
+    omega = np.sqrt(9.81 * k * np.tanh(k * water_depth))
+    r_o = oracle_mod.solve_frequency(default_oracle_gf, without.mesh, dofs, omega, water_depth=water_depth)
     r_w = oracle_mod.solve_frequency(default_oracle_gf, with_lid.mesh_including_lid, dofs, omega,
-                                     hull_mask=with_lid.hull_mask)
+                                     hull_mask=with_lid.hull_mask, water_depth=water_depth)
     assert r_w["froude_krylov"][0.0]["Heave"] == pytest.approx(r_o["froude_krylov"][0.0]["Heave"])
     assert r_w["diffraction"][0.0]["Heave"] == pytest.approx(r_o["diffraction"][0.0]["Heave"], rel=5e-2)
