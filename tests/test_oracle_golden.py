@@ -231,3 +231,15 @@ def test_layout_equivalences(default_oracle_gf):
         for i in range(mesh.nb_faces):
             diag[:, i, i] = mesh.faces_normals[i]
         np.testing.assert_allclose(g0, gradG - 0.5 * diag, atol=1e-10, rtol=1e-10)
+
+
+def test_direct_and_indirect_methods_agree(oracle_mod, default_oracle_gf):
+    # test_bem_solver.py:24-83: coarse sphere, surge diffraction force at omega = 1, rel 1e-1;
+    # the two formulations converge slowly with the mesh (5.6%, 7.4%, 4.2% apart at 4x4,
+    # 10x20, 20x40 panels), so the finer mesh and the finite-depth case keep the same bound
+    dofs = oracle_mod.rigid_body_dofs(only=["Surge"])
+    for resolution, depth, rel in (((4, 4), np.inf, 1e-1), ((10, 20), np.inf, 1e-1), ((10, 20), 5.0, 1e-1)):
+        sphere = mesh_sphere(radius=1.0, resolution=resolution).immersed_part()
+        d = oracle_mod.solve_frequency(default_oracle_gf, sphere, dofs, 1.0, method="direct", water_depth=depth)
+        i = oracle_mod.solve_frequency(default_oracle_gf, sphere, dofs, 1.0, method="indirect", water_depth=depth)
+        assert d["diffraction"][0.0]["Surge"] == pytest.approx(i["diffraction"][0.0]["Surge"], rel=rel)
