@@ -411,7 +411,7 @@ def finite_depth_wavenumber(omega, depth, g=9.81):
     """Root k > 0 of omega^2 / g = k tanh(k h) (problems_and_results.py:159-163)."""
     import scipy.optimize as so
     w2g = omega ** 2 / g
-    if depth == np.inf:
+    if depth == np.inf or w2g in (0.0, np.inf):
         return w2g
     hi = max(w2g, 1.0) * 2 + 1.0 / depth
     while hi * np.tanh(hi * depth) < w2g:
@@ -724,3 +724,37 @@ def solve_frequency_symmetric(gf, mesh, submesh, nb_blocks, nested, dofs, omega,
         results["froude_krylov"][beta] = fk
         results["excitation"][beta] = {d: dif[d] + fk[d] for d in dif}
     return results
+
+
+def solve_radiation_limit_frequency(gf, mesh, dofs, omega, *, rho=1000.0, method="indirect", hull_mask=None,
+                                    water_depth=np.inf):
+    """Radiation problems at omega = 0 or infinity (bem/problems_and_results.py:
+    440-449, 583-592 with the symbolic frequency of tools/symbolic_multiplication.py):
+    the boundary condition -i omega (dof . n) and the pressure i omega rho phi
+    carry omega as a symbolic factor that the added mass Re(F) / omega^2 cancels,
+    so A = Re(F') with F' the force of the problem with boundary condition
+    -i (dof . n) and pressure i rho phi, solved with the Green function at
+    k = 0 (omega = 0, low_freq variant) or k = infinity (high_freq variant);
+    the damping is zero.  Returns {"added_mass": {i: {j}}, "radiation_damping": ...}.
+    Finite depth at omega = 0 raises NotImplementedError (no Prony
+    decomposition at kh = 0), as the reference does."""
+    import scipy.linalg as sl
+    if omega not in (0.0, np.inf):
+        raise ValueError("omega must be 0 or infinity")
+    k = 0.0 if omega == 0.0 else np.inf
+    mask = np.ones(mesh.nb_faces, dtype=bool) if hull_mask is None else np.asarray(hull_mask, bool)
+    c, nrm, area = mesh.faces_centers[mask], mesh.faces_normals[mask], mesh.faces_areas[mask]
+    adjoint = method == "indirect"
+    S, K = gf.evaluate(mesh, mesh, free_surface=0.0, water_depth=water_depth, wavenumber=k,
+                       adjoint_double_layer=adjoint, early_dot_product=True, diagonal_term_in_double_layer=True)
+    lu = sl.lu_factor(K)
+    out = {"added_mass": {}, "radiation_damping": {}}
+    for name, dof in dofs.items():
+        bc = np.zeros(mesh.nb_faces, dtype=np.complex128)
+        bc[mask] = -1j * np.sum(dof.motion(c) * nrm, axis=1)
+        phi = sl.lu_solve(lu, S @ bc) if not adjoint else S @ sl.lu_solve(lu, bc)
+        p = (1j * rho * phi)[mask]
+        forces = {d: np.sum(p * -np.sum(dd.motion(c) * nrm, axis=1) * area) for d, dd in dofs.items()}
+        out["added_mass"][name] = {d: float(np.real(v)) for d, v in forces.items()}
+        out["radiation_damping"][name] = {d: 0.0 for d in forces}
+    return out
