@@ -55,3 +55,13 @@ def test_custom_linear_solver_contract():
     wrong = B200Engine(green_function=gf, linear_solver=lambda A, b: np.ones(3))
     with pytest.raises(ValueError):
         wrong.linear_solver(A, b)
+
+
+def test_tabulation_cache_file_name_is_the_reference_one():
+    """delhommeau.py:221-225: a table cached by capytaine is read here and the
+    other way round (same name, same npz keys r_range, z_range, values)."""
+    assert Delhommeau(tabulation_cache_dir=None)._cache_filename == \
+        "tabulation_float64_scaled_nemoh3_676_100.0_372_-251.0_1001.npz"
+    gf = Delhommeau(tabulation_nr=3, tabulation_rmax=1, tabulation_nz=3, tabulation_zmin=-1,
+                    tabulation_nb_integration_points=10, tabulation_grid_shape="legacy", tabulation_cache_dir=None)
+    assert gf._cache_filename == "tabulation_float64_legacy_3_1.0_3_-1.0_10.npz"
