@@ -682,7 +682,7 @@ def circulant_solve(lus, b):
 
 
 def solve_frequency_symmetric(gf, mesh, submesh, nb_blocks, nested, dofs, omega, *, rho=1000.0, g=9.81,
-                              wave_directions=(0.0,), hull_mask=None):
+                              wave_directions=(0.0,), hull_mask=None, water_depth=np.inf):
     """solve_frequency for a mesh with symmetries, through capytaine's algorithm:
     S and K of the whole mesh's collocation points against the panels of the
     reference sub-mesh (the half, quarter, wedge or half wedge), split into the
@@ -692,9 +692,9 @@ def solve_frequency_symmetric(gf, mesh, submesh, nb_blocks, nested, dofs, omega,
     whole mesh in the reference's order; nested=True for two planes or a
     rotation of a reflection (NestedBlockCirculantMatrix).  With hull_mask the
     faces outside it are a lid (zero boundary condition, no pressure)."""
-    k = omega ** 2 / g
-    S, K = gf.evaluate(mesh, submesh, free_surface=0.0, water_depth=np.inf, wavenumber=k, adjoint_double_layer=True,
-                       early_dot_product=True, diagonal_term_in_double_layer=True)
+    k = finite_depth_wavenumber(omega, water_depth, g)
+    S, K = gf.evaluate(mesh, submesh, free_surface=0.0, water_depth=water_depth, wavenumber=k,
+                       adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True)
     ns = submesh.nb_faces
     Sm = circulant_macro_blocks(np.ascontiguousarray(S).reshape((nb_blocks, ns, ns)), nested)
     Km = circulant_macro_blocks(np.ascontiguousarray(K).reshape((nb_blocks, ns, ns)), nested)
@@ -718,8 +718,8 @@ def solve_frequency_symmetric(gf, mesh, submesh, nb_blocks, nested, dofs, omega,
         results["added_mass"][name] = {d: float(np.real(v) / omega ** 2) for d, v in f.items()}
         results["radiation_damping"][name] = {d: float(np.imag(v) / omega) for d, v in f.items()}
     for beta in wave_directions:
-        dif = forces(solve(-(airy_waves_velocity(c, omega, k, g, beta) * nrm).sum(axis=1)))
-        fk = forces(airy_waves_pressure(c, omega, k, g, rho, beta))
+        dif = forces(solve(-(airy_waves_velocity(c, omega, k, g, beta, water_depth) * nrm).sum(axis=1)))
+        fk = forces(airy_waves_pressure(c, omega, k, g, rho, beta, water_depth))
         results["diffraction"][beta] = dif
         results["froude_krylov"][beta] = fk
         results["excitation"][beta] = {d: dif[d] + fk[d] for d in dif}

@@ -285,3 +285,25 @@ def test_reference_rotation_mesh_cases():
                                atol=1e-15)
     np.testing.assert_allclose(m.merged().mirrored("yOz").faces_centers, m.mirrored("yOz").merged().faces_centers,
                                atol=1e-15)
+
+
+@pytest.mark.parametrize("kind", ["reflection", "reflections", "rotation", "dihedral"])
+def test_oracle_symmetric_solve_in_finite_depth(oracle_mod, legacy_oracle_gf, kind):
+    """The block structure holds in finite depth too (the sea-bottom images and
+    the Prony terms are invariant under the same symmetries): the oracle's
+    block-circulant solve equals its dense solve at 8 m of water."""
+    mesh = _symmetric_cases(True)[kind]
+    st = block_structure(mesh)
+    full = mesh.merged()
+    dofs = oracle_mod.rigid_body_dofs()
+    nested = kind in ("reflections", "dihedral")
+    sym = oracle_mod.solve_frequency_symmetric(legacy_oracle_gf, full, st.submesh, st.nb_images, nested, dofs, 1.3,
+                                               water_depth=8.0)
+    dense = oracle_mod.solve_frequency(legacy_oracle_gf, full, dofs, 1.3, water_depth=8.0)
+    for fam in ("added_mass", "radiation_damping"):
+        a = np.array([[sym[fam][i][j] for j in dofs] for i in dofs])
+        b = np.array([[dense[fam][i][j] for j in dofs] for i in dofs])
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
+    a = np.array([sym["excitation"][0.0][d] for d in dofs])
+    b = np.array([dense["excitation"][0.0][d] for d in dofs])
+    assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
