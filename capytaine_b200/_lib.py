@@ -84,6 +84,7 @@ _SIGNATURES = {
     "bem_assemble_wave_symmetric_batched": ([ctypes.POINTER(AssemblyArgs), c_void_p, c_i64, c_void_p, c_int, c_i64,
                                              c_i64, c_void_p], c_int),
     "bem_assemble_symmetric": ([ctypes.POINTER(AssemblyArgs), c_void_p], c_int),
+    "bem_assemble_finite_depth": ([ctypes.POINTER(AssemblyArgs), c_double, c_int, c_void_p, c_int, c_void_p], c_int),
     "bem_assemble_wave_cached": ([ctypes.POINTER(AssemblyArgs), c_void_p, c_i64, c_void_p, c_int, c_i64, c_i64,
                                   c_void_p], c_int),
     "bem_zpad_identity": ([c_void_p, c_i64, c_i64, c_int, c_int, c_int, c_void_p], c_int),

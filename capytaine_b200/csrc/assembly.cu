@@ -713,6 +713,227 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
   if (nan_seen && a.nan_flag_dev) atomicOr(a.nan_flag_dev, 1);
 }
 
+// ---- finite depth (Delhommeau's method) -------------------------------------
+// Green_Rankine.f90:202-338: Rankine term at the image (x, y, c0 z + c1) of M,
+// exact or one point by the distance to the face (one point when forced).
+__device__ __forceinline__ void reflected_rankine(const double M[3], const FaceRec& f, bool deriv_first, double c0,
+                                                  double c1, bool one_point, double& G, double dG[3]) {
+  const double Mr[3] = {M[0], M[1], c0 * M[2] + c1};
+  const double r1 = hypot(norm2_2(M[0] - f.c[0], M[1] - f.c[1]), Mr[2] - f.c[2]);
+  if (one_point || r1 > 7 * f.radius) {
+    one_point_rankine<double>(f.c[0] - Mr[0], f.c[1] - Mr[1], f.c[2] - Mr[2], f.area, G, dG);
+  } else {
+    exact_rankine(Mr, f, true, G, dG);
+  }
+  dG[2] = c0 * dG[2];
+  if (!deriv_first) {
+    dG[0] = -dG[0];
+    dG[1] = -dG[1];
+    if (c0 > 0) dG[2] = -dG[2];
+  }
+}
+
+// Green_wave.f90:50-124 for the point x and the face of centre c (quadrature
+// points of face J, each mirrored through the sea bottom when mirror_face).
+__device__ void wave_term(const double x[3], const double c[3], const bem_assembly_args& a, const FaceRec& f, int J,
+                          bool mirror_face, double depth, double k, const TabView& T, int sing, bool deriv_first,
+                          double& gre, double& gim, double dr[3], double di[3]) {
+  gre = gim = 0;
+  dr[0] = dr[1] = dr[2] = di[0] = di[1] = di[2] = 0;
+  const double rr = k * norm2_2(x[0] - c[0], x[1] - c[1]);
+  const double zz = k * (x[2] + c[2]);
+  if (fabs(rr) < kLit1em10 && fabs(zz) < kLit1em10) {
+    // Green_wave.f90:128-158, panel on the free surface with itself
+    const double re = (1 - log(k * k * f.area / kPI)) + 2 * (kEulerGamma - kLog2);
+    gre = k * f.area * re;
+    gim = k * f.area * (-2 * kPI);
+    dr[2] = k * (gre + 4 * sqrt(kPI * f.area));
+    di[2] = k * gim;
+  } else {
+    for (int q = 0; q < a.nb_quad_points; ++q) {
+      const double* qp = a.quad_points_dev + ((size_t)a.nb_quad_points * J + q) * 3;
+      const double xq[3] = {qp[0], qp[1], mirror_face ? -qp[2] - 2 * depth : qp[2]};
+      wave_part<double>(x, xq, k, T, sing, a.quad_weights_dev[(size_t)a.nb_quad_points * J + q], gre, gim, dr, di);
+    }
+  }
+  if (!deriv_first) {
+    dr[0] = -dr[0];
+    dr[1] = -dr[1];
+    di[0] = -di[0];
+    di[1] = -di[1];
+  }
+}
+
+// matrices.f90:28-325 in finite depth, Delhommeau's method: the
+// infinite-depth Rankine terms, the Rankine images through the sea bottom
+// (matrices.f90:212-268), the four wave terms of Green_wave.f90:311-425 and the
+// Prony terms of Green_wave.f90:427-508.  One thread per collocation point,
+// the panels of a tile in shared memory; float64, complex128 outputs, K with
+// the dot product taken.  prony: rates then amplitudes (2 x nexp).
+__global__ void __launch_bounds__(kRows) assemble_finite_depth_kernel(const bem_assembly_args a, TabView T,
+                                                                      double depth, int legacy,
+                                                                      const double* __restrict__ prony, int nexp,
+                                                                      int gf_sing) {
+  __shared__ FaceRec faces[kTileJ];
+  if (T.nr > 1 && T.nz > 1) {
+    T.rmax = __ldg(T.r_range + T.nr - 1);
+    T.zlast = __ldg(T.z_range + T.nz - 1);
+  }
+  const int J0 = blockIdx.y * kTileJ;
+  const int nJ = min(kTileJ, a.nb_faces - J0);
+  if ((int)threadIdx.x < nJ) {
+    const int J = J0 + threadIdx.x;
+    FaceRec& f = faces[threadIdx.x];
+#pragma unroll
+    for (int L = 0; L < 4; ++L) {
+      const int v = a.faces_dev[4 * J + L];
+      f.v[3 * L] = a.vertices_dev[3 * v];
+      f.v[3 * L + 1] = a.vertices_dev[3 * v + 1];
+      f.v[3 * L + 2] = a.vertices_dev[3 * v + 2];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      f.c[d] = a.centers_dev[3 * J + d];
+      f.n[d] = a.normals_dev[3 * J + d];
+      f.q0[d] = a.quad_points_dev[(size_t)3 * a.nb_quad_points * J + d];
+    }
+    f.area = a.areas_dev[J];
+    f.radius = a.radii_dev[J];
+    f.w0 = a.quad_weights_dev[(size_t)a.nb_quad_points * J];
+  }
+  __syncthreads();
+  const int I = blockIdx.x * kRows + threadIdx.x;
+  if (I >= a.n) return;
+  const double M[3] = {a.points_dev[3 * I], a.points_dev[3 * I + 1], a.points_dev[3 * I + 2]};
+  const double Msym[3] = {M[0], M[1], -M[2] - 2 * depth};
+  const bool adjoint = a.adjoint_double_layer != 0;
+  double nI[3] = {0, 0, 0};
+  if (adjoint) {
+    nI[0] = a.dot_normals_dev[3 * I];
+    nI[1] = a.dot_normals_dev[3 * I + 1];
+    nI[2] = a.dot_normals_dev[3 * I + 2];
+  }
+  const double k = a.wavenumber;
+  const bool finite_k = k > 0.0 && isfinite(k);
+  const double sign_refl = (gf_sing == kHighFreq) ? -1.0 : 1.0;
+  const int diag_limit = min(a.n, a.nb_faces);
+  double diag_coef = 0.5;
+  if (a.diagonal_term && I < diag_limit)
+    diag_coef = (fabs(a.centers_dev[3 * I + 2] - a.free_surface) < kLit1em8) ? 1.0 : 0.5;
+  double A = 0.0;
+  if (finite_k) {
+    const double amh = k * depth;
+    const double akh = amh * tanh(amh);
+    A = (amh + akh) * (amh + akh) / (4 * amh * (amh * amh - akh * akh + akh));
+  }
+  double2* S = reinterpret_cast<double2*>(a.S_dev);
+  double2* K = reinterpret_cast<double2*>(a.K_dev);
+  bool nan_seen = false;
+  for (int jj = 0; jj < nJ; ++jj) {
+    const FaceRec& f = faces[jj];
+    const int J = J0 + jj;
+    double Gre = 0, Gim = 0, dGre[3] = {0, 0, 0}, dGim[3] = {0, 0, 0};
+    double g, dg[3];
+    // direct Rankine term
+    {
+      const double d0 = M[0] - f.c[0], d1 = M[1] - f.c[1], d2 = M[2] - f.c[2];
+      if (norm2_3(d0, d1, d2) > 7 * f.radius) {
+        one_point_rankine<double>(-d0, -d1, -d2, f.area, g, dg);
+      } else {
+        exact_rankine(M, f, true, g, dg);
+      }
+      if (!adjoint) {
+        dg[0] = -dg[0];
+        dg[1] = -dg[1];
+        dg[2] = -dg[2];
+      }
+      Gre += g;
+      dGre[0] += dg[0];
+      dGre[1] += dg[1];
+      dGre[2] += dg[2];
+    }
+    // free-surface image (one point in the legacy method), with the variant's sign
+    reflected_rankine(M, f, adjoint, -1.0, 0.0, legacy != 0, g, dg);
+    Gre += sign_refl * g;
+    dGre[0] += sign_refl * dg[0];
+    dGre[1] += sign_refl * dg[1];
+    dGre[2] += sign_refl * dg[2];
+    if (gf_sing == kLowFreqWithRankinePart) dGre[2] += 2 * k * g;
+    // sea-bottom image, then the images through both boundaries
+    reflected_rankine(M, f, adjoint, -1.0, -2 * depth, false, g, dg);
+    Gre += g;
+    dGre[0] += dg[0];
+    dGre[1] += dg[1];
+    dGre[2] += dg[2];
+    const double c_one_point[3][2] = {{1.0, -2 * depth}, {1.0, 2 * depth}, {-1.0, -4 * depth}};
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+      reflected_rankine(M, f, adjoint, c_one_point[t][0], c_one_point[t][1], true, g, dg);
+      Gre += sign_refl * g;
+      dGre[0] += sign_refl * dg[0];
+      dGre[1] += sign_refl * dg[1];
+      dGre[2] += sign_refl * dg[2];
+    }
+    // four infinite-depth wave terms (point, face, each possibly mirrored through the bottom)
+    if (finite_k) {
+      const double csym[3] = {f.c[0], f.c[1], -f.c[2] - 2 * depth};
+      double wre = 0, wim = 0, wdr[3] = {0, 0, 0}, wdi[3] = {0, 0, 0};
+#pragma unroll 1
+      for (int t = 0; t < 4; ++t) {
+        const bool mx = (t & 1) != 0, mf = (t & 2) != 0;
+        // z of the gradient mirrored: (x_sym, face) when deriv_first, (x, face_sym)
+        // otherwise, (x_sym, face_sym) always (Green_wave.f90:375-411)
+        const bool flip_z = (mx && mf) || (mx && adjoint) || (mf && !adjoint);
+        double gr, gi, dr[3], di[3];
+        wave_term(mx ? Msym : M, mf ? csym : f.c, a, f, J, mf, depth, k, T, gf_sing, adjoint, gr, gi, dr, di);
+        if (flip_z) {
+          dr[2] = -dr[2];
+          di[2] = -di[2];
+        }
+        wre += gr;
+        wim += gi;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          wdr[d] += dr[d];
+          wdi[d] += di[d];
+        }
+      }
+      Gre += A * wre;
+      Gim += A * wim;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        dGre[d] += A * wdr[d];
+        dGim[d] += A * wdi[d];
+      }
+    }
+    // Prony exponentials: four Rankine images each, weighted a / 2
+    for (int e = 0; e < nexp; ++e) {
+      const double lam = __ldg(prony + e), amp = __ldg(prony + nexp + e);
+      const double cp[4][2] = {{1.0, depth * lam - 2 * depth},
+                               {-1.0, -depth * lam},
+                               {-1.0, depth * lam - 4 * depth},
+                               {1.0, -depth * lam + 2 * depth}};
+#pragma unroll 1
+      for (int t = 0; t < 4; ++t) {
+        reflected_rankine(M, f, adjoint, cp[t][0], cp[t][1], false, g, dg);
+        Gre += amp / 2 * g;
+        dGre[0] += amp / 2 * dg[0];
+        dGre[1] += amp / 2 * dg[1];
+        dGre[2] += amp / 2 * dg[2];
+      }
+    }
+    const double* dn = adjoint ? nI : (a.dot_normals_dev + 3 * J);
+    const double sre = kMinusOneOverFourPi * Gre, sim = kMinusOneOverFourPi * Gim;
+    double kre = kMinusOneOverFourPi * (dn[0] * dGre[0] + dn[1] * dGre[1] + dn[2] * dGre[2]);
+    const double kim = kMinusOneOverFourPi * (dn[0] * dGim[0] + dn[1] * dGim[1] + dn[2] * dGim[2]);
+    if (a.diagonal_term && I == J && I < diag_limit) kre += diag_coef;
+    S[(size_t)I + (size_t)a.lds * J] = make_double2(sre, sim);
+    K[(size_t)I + (size_t)a.ldk * J] = make_double2(kre, kim);
+    nan_seen |= isnan(sre) || isnan(sim) || isnan(kre) || isnan(kim);
+  }
+  if (nan_seen && a.nan_flag_dev) atomicOr(a.nan_flag_dev, 1);
+}
+
 }  // namespace
 }  // namespace bem
 
@@ -948,4 +1169,53 @@ extern "C" int bem_assemble_symmetric(const bem_assembly_args* args, void* strea
   if (st) return st;
   const double k = a.wavenumber;
   return wave_symmetric_launch(args, a.K_dev, a.ldk, &k, 1, 0, 0, stream, "bem_assemble_symmetric", false, true);
+}
+
+extern "C" int bem_assemble_finite_depth(const bem_assembly_args* args, double depth, int method,
+                                         const double* prony_dev, int nexp, void* stream) {
+  using namespace bem;
+  if (!args) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: null args");
+  const bem_assembly_args& a = *args;
+  if (a.n < 0 || a.nb_faces < 0) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: negative size");
+  if (a.n == 0 || a.nb_faces == 0) return BEM_OK;
+  if (!a.points_dev || !a.vertices_dev || !a.faces_dev || !a.centers_dev || !a.normals_dev || !a.areas_dev ||
+      !a.radii_dev || !a.quad_points_dev || !a.quad_weights_dev || !a.S_dev || !a.K_dev || !a.dot_normals_dev)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: null pointer");
+  if (!(depth > 0.0) || !std::isfinite(depth))
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: depth must be finite and > 0");
+  if (std::isinf(a.free_surface))
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: a finite depth needs a free surface");
+  if (nexp < 0 || nexp > 64 || (nexp > 0 && !prony_dev))
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: 0 to 64 Prony terms");
+  if (method != 0 && method != 1)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: method 0 (legacy) or 1 (newer)");
+  if (!a.early_dot_product || a.out_dtype != BEM_DTYPE_C128 || a.precision != BEM_PREC_FP64)
+    return set_error(BEM_ERR_UNSUPPORTED,
+                     "bem_assemble_finite_depth: early dot product, complex128 outputs and float64 only");
+  if (a.nb_quad_points < 1 || a.lds < a.n || a.ldk < a.n)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: quadrature or leading dimension");
+  if (!(a.wavenumber >= 0.0))
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: wavenumber must be >= 0");
+  const bool tabulated = a.nr > 1 && a.nz > 1;
+  const bool finite_k = a.wavenumber > 0.0 && std::isfinite(a.wavenumber);
+  if (finite_k && tabulated && (!a.r_range_dev || !a.z_range_dev || !a.table_dev))
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: tabulation pointers missing");
+  if (finite_k && !tabulated && a.tabulation_nb_integration_points <= 0)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: nb_integration_points <= 0");
+  const TabView T{a.tabulation_nb_integration_points, a.tabulation_grid_shape, a.nr, a.nz, a.r_range_dev,
+                  a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0};
+  // the caller picks the variant (delhommeau.py:467-487: the legacy method
+  // takes low_freq before the wavenumber rules apply)
+  const int gf_sing = a.gf_singularities;
+  if (gf_sing < kHighFreq || gf_sing > kLowFreqWithRankinePart)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: unknown gf_singularities");
+  dim3 grid(ceil_div(a.n, kRows), ceil_div(a.nb_faces, kTileJ));
+  cudaStream_t s = (cudaStream_t)stream;
+  {
+    TimedLaunch tl(kKAssemble, s);
+    assemble_finite_depth_kernel<<<grid, kRows, 0, s>>>(a, T, depth, method == 0 ? 1 : 0, prony_dev, nexp, gf_sing);
+  }
+  count_launches(1);
+  BEM_CUDA_CHECK(cudaGetLastError());
+  return BEM_OK;
 }

@@ -330,10 +330,15 @@ class Delhommeau:
         S + i * s_stride and K + i * k_stride elements, in one launch per 64
         wavenumbers on the Rankine-reuse path."""
         import torch
-        if water_depth != np.inf:
-            raise NotImplementedError("finite water depth is outside the B200 path (infinite depth only)")
         if free_surface == np.inf and water_depth != np.inf:
             raise ValueError("When setting free_surface=inf, the water depth should also be infinite")
+        if water_depth != np.inf:
+            return self._assemble_finite_depth(mesh1, mesh2, S, K, free_surface=free_surface, water_depth=water_depth,
+                                               wavenumber=wavenumber, adjoint_double_layer=adjoint_double_layer,
+                                               early_dot_product=early_dot_product,
+                                               diagonal_term_in_double_layer=diagonal_term_in_double_layer,
+                                               lds=lds, ldk=ldk, precision=precision, stream=stream,
+                                               nan_flag=nan_flag, sweep=sweep)
         pts, nrm = self._collocation(mesh1, mesh2, adjoint_double_layer)
         dm2 = self.device_mesh(mesh2)
         n = pts.shape[0]
@@ -439,6 +444,86 @@ class Delhommeau:
                 _lib.check(lib.bem_assemble(a, _lib.stream_ptr(stream)))
             return
         _lib.check(lib.bem_assemble(a, _lib.stream_ptr(stream)))
+
+    def _assemble_finite_depth(self, mesh1, mesh2, S, K, *, free_surface, water_depth, wavenumber,
+                               adjoint_double_layer, early_dot_product, diagonal_term_in_double_layer, lds, ldk,
+                               precision, stream, nan_flag, sweep=None):
+        """S and K in water of finite depth by Delhommeau's method
+        (matrices.f90:197-305) through bem_assemble_finite_depth, with the Prony
+        decomposition of find_best_exponential_decomposition(k h) and the
+        variant rules of delhommeau.py:467-487 (the legacy method uses low_freq).
+        float64, complex128 outputs, K with the dot product taken; a sweep is
+        one launch per wavenumber (each has its own decomposition)."""
+        todo = [(float(wavenumber), 0, 0)]
+        if sweep is not None:
+            ks, s_stride, k_stride = sweep
+            todo = [(float(k), i * int(s_stride), i * int(k_stride)) for i, k in enumerate(ks)]
+        for k, so, ko in todo:
+            self._assemble_finite_depth_one(mesh1, mesh2, S, K, so, ko, free_surface=free_surface,
+                                            water_depth=water_depth, wavenumber=k,
+                                            adjoint_double_layer=adjoint_double_layer,
+                                            early_dot_product=early_dot_product,
+                                            diagonal_term_in_double_layer=diagonal_term_in_double_layer, lds=lds,
+                                            ldk=ldk, precision=precision, stream=stream, nan_flag=nan_flag)
+
+    def _assemble_finite_depth_one(self, mesh1, mesh2, S, K, s_offset, k_offset, *, free_surface, water_depth,
+                                   wavenumber, adjoint_double_layer, early_dot_product,
+                                   diagonal_term_in_double_layer, lds, ldk, precision, stream, nan_flag):
+        """One wavenumber of _assemble_finite_depth, S and K written s_offset and
+        k_offset elements after the start of their buffers."""
+        import torch
+        prec = self.precision if precision is None else precision
+        if S.dtype != torch.complex128 or K.dtype != torch.complex128 or prec != "fp64" or not early_dot_product:
+            raise NotImplementedError("finite depth on the device: float64 assembly, complex128 outputs and the "
+                                      "dot product taken (early_dot_product=True) only")
+        pts, nrm = self._collocation(mesh1, mesh2, adjoint_double_layer)
+        dm2 = self.device_mesh(mesh2)
+        n = pts.shape[0]
+        k = float(wavenumber)
+        if self.finite_depth_method not in ("legacy", "newer"):
+            raise NotImplementedError(f"finite_depth_method={self.finite_depth_method!r} is not part of this library")
+        if self.finite_depth_method == "legacy" and self.gf_singularities != "low_freq":
+            sing = "low_freq"
+        else:
+            sing = self._variant(dm2.centers_z, k)
+        decomposition = self.find_best_exponential_decomposition(k * float(water_depth))
+        prony = torch.as_tensor(np.ascontiguousarray(decomposition, dtype=np.float64), device=self.device)
+        if stream is not None:
+            stream.wait_stream(torch.cuda.current_stream())
+        finite_k = 0.0 < k < np.inf
+        if finite_k:
+            r, z, table, table32 = self._device_tabulation()
+        else:
+            r = z = table = table32 = None
+        nr = r.numel() if r is not None else 0
+        nz = z.numel() if z is not None else 0
+        a = _lib.AssemblyArgs(
+            n=n, points_dev=pts.data_ptr(), dot_normals_dev=nrm.data_ptr(),
+            nb_faces=dm2.nb_faces, nb_vertices=dm2.nb_vertices, vertices_dev=dm2.vertices.data_ptr(),
+            faces_dev=dm2.faces.data_ptr(), centers_dev=dm2.centers.data_ptr(), normals_dev=dm2.normals.data_ptr(),
+            areas_dev=dm2.areas.data_ptr(), radii_dev=dm2.radii.data_ptr(), nb_quad_points=dm2.nb_quad_points,
+            quad_points_dev=dm2.quad_points.data_ptr(), quad_weights_dev=dm2.quad_weights.data_ptr(),
+            tabulation_nb_integration_points=self.tabulation_nb_integration_points,
+            tabulation_grid_shape=self.tabulation_grid_shape_index, nr=nr if nr > 1 and nz > 1 else 0,
+            nz=nz if nr > 1 and nz > 1 else 0,
+            r_range_dev=r.data_ptr() if r is not None else 0, z_range_dev=z.data_ptr() if z is not None else 0,
+            table_dev=table.data_ptr() if table is not None else 0,
+            table32_dev=table32.data_ptr() if table32 is not None else 0,
+            wavenumber=k, free_surface=float(free_surface), gf_singularities=_SING[sing],
+            adjoint_double_layer=int(bool(adjoint_double_layer)), early_dot_product=1,
+            diagonal_term=int(bool(diagonal_term_in_double_layer)), precision=_lib.BEM_PREC_FP64,
+            out_dtype=_lib.BEM_DTYPE_C128, S_dev=S.data_ptr() + s_offset * S.element_size(),
+            K_dev=K.data_ptr() + k_offset * K.element_size(),
+            lds=lds if lds is not None else n, ldk=ldk if ldk is not None else n, k_plane_stride=0,
+            nan_flag_dev=nan_flag.data_ptr() if nan_flag is not None else 0,
+        )
+        _lib.check(_lib.load().bem_assemble_finite_depth(a, float(water_depth),
+                                                         0 if self.finite_depth_method == "legacy" else 1,
+                                                         _lib.c_void_p(prony.data_ptr()), decomposition.shape[1],
+                                                         _lib.stream_ptr(stream)))
+        if stream is not None:
+            # the decomposition was copied on the current stream and is freed on return
+            prony.record_stream(stream)
 
     def _rankine_part(self, mesh_key, dm, args, adjoint, sing, free_surface, stream, rows=None):
         """Device array of the wavenumber-independent Rankine part of the rows

@@ -167,6 +167,19 @@ int bem_assemble_wave_symmetric_batched(const bem_assembly_args* args, const voi
  * One frequency of a body that is not seen again (a request of the server). */
 int bem_assemble_symmetric(const bem_assembly_args* args, void* stream);
 
+/* S and K in water of depth `depth` (finite, > 0), Delhommeau's method:
+ * bem_assemble's terms plus the Rankine images through the sea bottom, the
+ * four infinite-depth wave terms of the point and the face and of their
+ * images through the bottom (scaled by Delhommeau's factor), and four Rankine
+ * images per exponential of the Prony decomposition prony_dev (device, 2 x nexp
+ * float64: growth rates, then amplitudes; nexp <= 64).  method: 0 = legacy
+ * (one-point free-surface image), 1 = newer.  float64, complex128 outputs, K
+ * with the dot product taken.  Replaces the finite-depth branch of
+ * matrices::build_matrices (libs/libDelhommeau/src/matrices.f90:197-305,
+ * Green_wave.f90:311-508), called from delhommeau.py:492-515. */
+int bem_assemble_finite_depth(const bem_assembly_args* args, double depth, int method, const double* prony_dev,
+                              int nexp, void* stream);
+
 /* Any collocation points (args->n) against a mesh (args->nb_faces panels, one
  * quadrature point per face, the same device array for centers_dev and
  * quad_points_dev) at nk wavenumbers, from a Rankine part made by

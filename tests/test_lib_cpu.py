@@ -78,6 +78,41 @@ def test_symmetric_assembly_preconditions_checked_on_host(lib):
     assert lib.bem_assemble_rankine_part(a, None, 12, None) == _lib.BEM_ERR_INVALID_ARGUMENT
 
 
+def test_finite_depth_assembly_preconditions_checked_on_host(lib):
+    """bem_assemble_finite_depth refuses bad depths, Prony sizes, methods and
+    output formats before any launch."""
+    fake = 4096  # never dereferenced: every call below fails its host checks
+    a = _lib.AssemblyArgs(n=12, points_dev=fake, dot_normals_dev=fake, nb_faces=12, nb_vertices=4,
+                          vertices_dev=fake, faces_dev=fake, centers_dev=fake, normals_dev=fake, areas_dev=fake,
+                          radii_dev=fake, nb_quad_points=1, quad_points_dev=fake, quad_weights_dev=fake,
+                          tabulation_nb_integration_points=101, wavenumber=1.0, free_surface=0.0,
+                          gf_singularities=_lib.BEM_GF_LOW_FREQ, adjoint_double_layer=1, early_dot_product=1,
+                          diagonal_term=1, precision=_lib.BEM_PREC_FP64, out_dtype=_lib.BEM_DTYPE_C128, S_dev=fake,
+                          K_dev=fake, lds=12, ldk=12)
+    bad, unsupported = _lib.BEM_ERR_INVALID_ARGUMENT, _lib.BEM_ERR_UNSUPPORTED
+    assert lib.bem_assemble_finite_depth(None, 10.0, 1, fake, 4, None) == bad
+    for depth in (0.0, -1.0, float("inf"), float("nan")):
+        assert lib.bem_assemble_finite_depth(a, depth, 1, fake, 4, None) == bad
+    assert b"depth" in lib.bem_last_error()
+    assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 65, None) == bad  # more than 64 exponentials
+    assert lib.bem_assemble_finite_depth(a, 10.0, 1, None, 4, None) == bad  # no decomposition
+    assert lib.bem_assemble_finite_depth(a, 10.0, 2, fake, 4, None) == bad  # unknown method
+    a.gf_singularities = 7
+    assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == bad
+    a.gf_singularities = _lib.BEM_GF_LOW_FREQ
+    a.free_surface = float("inf")
+    assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == bad
+    a.free_surface = 0.0
+    a.out_dtype = _lib.BEM_DTYPE_C64
+    assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == unsupported
+    a.out_dtype = _lib.BEM_DTYPE_C128
+    a.early_dot_product = 0
+    assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == unsupported
+    a.early_dot_product = 1
+    a.ldk = 11
+    assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == bad
+
+
 def test_cached_wave_and_block_combine_preconditions_checked_on_host(lib):
     """Entry points of the symmetric engines refuse bad shapes before any launch."""
     import ctypes
