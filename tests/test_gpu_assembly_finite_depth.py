@@ -102,3 +102,50 @@ def test_finite_depth_sweep_writes_every_wavenumber(oracle_mod, default_oracle_g
                                                   prony=gf.find_best_exponential_decomposition(k * depth))
         _close(S[i].T.cpu().numpy(), S_ref, FP64_RTOL)
         _close(K[i].T.cpu().numpy(), K_ref, FP64_RTOL)
+
+
+def _matrix_engine(oracle_gf, tmp_path):
+    from capytaine_b200.engine import B200Engine
+    return B200Engine(green_function=_gpu_gf(oracle_gf, tmp_path))
+
+
+def _coefficient_error(value, ref, scale):
+    return abs(value - ref) / max(abs(ref), 1e-3 * scale)
+
+
+@pytest.mark.parametrize("depth,omega", [(4.0, 1.3), (1.5, 0.8)])
+def test_finite_depth_solve_through_matrix_engine(oracle_mod, default_oracle_gf, tmp_path, depth, omega):
+    """capytaine's BEMSolver in finite depth over this engine (bem/solver.py:188-207):
+    build_matrices(water_depth=h) through the finite-depth kernel, then
+    linear_solver and S @ sigma on the device, with the radiation and
+    finite-depth diffraction right-hand sides the reference's problems build
+    (problems_and_results.py:373-381,440-449, airy_waves.py:56-95); added mass,
+    damping and excitation against the oracle's finite-depth solve."""
+    mesh = mesh_sphere(resolution=(8, 12)).immersed_part()
+    dofs = oracle_mod.rigid_body_dofs(only=["Surge", "Heave", "Pitch"])
+    rho, g = 1000.0, 9.81
+    eng = _matrix_engine(default_oracle_gf, tmp_path)
+    k = oracle_mod.finite_depth_wavenumber(omega, depth, g)
+    S, K = eng.build_matrices(mesh, mesh, free_surface=0.0, water_depth=depth, wavenumber=k,
+                              adjoint_double_layer=True, diagonal_term_in_double_layer=True)
+    ref = oracle_mod.solve_frequency(default_oracle_gf, mesh, dofs, omega, water_depth=depth)
+    centers, normals = mesh.faces_centers, mesh.faces_normals
+
+    def forces(bc):
+        sigma = eng.linear_solver(K, bc)
+        return oracle_mod.integrate_pressure(mesh, dofs, 1j * omega * rho * (S @ sigma))
+
+    added, damping = {}, {}
+    for name, dof in dofs.items():
+        f = forces(-1j * omega * np.sum(dof.motion(centers) * normals, axis=1))
+        added[name] = {d: np.real(v) / omega ** 2 for d, v in f.items()}
+        damping[name] = {d: np.imag(v) / omega for d, v in f.items()}
+    diffraction = forces(-(oracle_mod.airy_waves_velocity(centers, omega, k, g, 0.0, depth) * normals).sum(axis=1))
+    for got, want in ((added, ref["added_mass"]), (damping, ref["radiation_damping"])):
+        scale = max(abs(v) for row in want.values() for v in row.values())
+        errs = [_coefficient_error(got[r][c], want[r][c], scale) for r in want for c in want[r]]
+        assert max(errs) < 1e-7, errs
+    want = ref["diffraction"][0.0]
+    scale = max(abs(v) for v in want.values())
+    errs = [_coefficient_error(diffraction[d], want[d], scale) for d in want]
+    assert max(errs) < 1e-7, errs
