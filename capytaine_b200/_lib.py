@@ -94,8 +94,8 @@ _SIGNATURES = {
     "bem_zlu_factor": ([c_void_p, c_int, c_i64, c_i64, c_int, c_void_p, c_void_p, c_void_p, c_void_p], c_int),
     "bem_zlu_solve": ([c_void_p, c_int, c_i64, c_i64, c_int, c_void_p, c_void_p, c_void_p, c_i64, c_i64, c_int,
                        c_void_p, c_void_p], c_int),
-    "bem_build_rhs": ([c_int, c_int, c_void_p, c_void_p, c_double, c_int, c_void_p, c_int, c_void_p, c_void_p,
-                       c_void_p, c_void_p, c_void_p, c_i64, c_i64, c_void_p], c_int),
+    "bem_build_rhs": ([c_int, c_int, c_void_p, c_void_p, c_double, c_double, c_int, c_void_p, c_int, c_void_p,
+                       c_void_p, c_void_p, c_void_p, c_void_p, c_i64, c_i64, c_void_p], c_int),
     "bem_zgemm_ts_workspace_bytes": ([c_int, c_int, c_int, c_int], c_i64),
     "bem_zgemm_ts": ([c_int, c_int, c_int, c_double, c_double, c_void_p, c_i64, c_i64, c_void_p, c_i64, c_i64,
                       c_double, c_double, c_void_p, c_i64, c_i64, c_int, c_void_p, c_void_p], c_int),
@@ -117,7 +117,7 @@ _SIGNATURES = {
     "bem_zgemm_ts_static_capacity": ([], c_i64),
     "bem_zgemm_ts_static": ([c_int, c_int, c_int, c_double, c_double, c_void_p, c_i64, c_i64, c_void_p, c_i64, c_i64,
                              c_double, c_double, c_void_p, c_i64, c_i64, c_int, c_void_p], c_int),
-    "bem_froude_krylov": ([c_int, c_int, c_int, c_int, c_void_p, c_double, c_double, c_void_p, c_void_p,
+    "bem_froude_krylov": ([c_int, c_int, c_int, c_int, c_void_p, c_double, c_double, c_double, c_void_p, c_void_p,
                            c_void_p, c_void_p, c_void_p], c_int),
     "bem_block_combine": ([c_void_p, c_i64, c_i64, c_i64, c_void_p, c_i64, c_i64, c_i64, c_void_p, c_void_p, c_int,
                            c_int, c_int, c_int, c_int, c_void_p], c_int),

@@ -3,7 +3,7 @@
 // * bem_build_rhs: radiation boundary conditions -i*omega*(dof . n) and
 //   diffraction boundary conditions -(u_Airy . n) on the hull, zero on lid
 //   panels (capytaine bem/problems_and_results.py:373-381, 440-449;
-//   bem/airy_waves.py:56-95, infinite depth).
+//   bem/airy_waves.py:56-95, infinite or finite depth).
 // * bem_zgemm_ts: Y = alpha A X + beta Y for a tall matrix A (n x K, complex128,
 //   column-major) and a few columns X (K x nrhs): the potential S @ sigma
 //   (bem/solver.py:197-198) and the residuals b - K x.  Memory-bound on A: split
@@ -12,14 +12,35 @@
 //   F_d = sum_i p_i (-dof_d . n_i) area_i (bodies/bodies.py:238-250) of the
 //   radiated/diffracted pressure i*omega*rho*phi and of the incident-wave
 //   pressure (airy_waves.py:19-53, 98-102).
+#include <cmath>
+
 #include "common.cuh"
 
 namespace bem {
 namespace {
 
 
+// Depth profiles of the Airy wave at height z (airy_waves.py:41-47, 80-85):
+// cosh(k (z + h)) / cosh(k h) and sinh(k (z + h)) / cosh(k h) when 0 <= k h < 20,
+// else both e^{k z} (the infinite-depth profile).
+template <bool FINITE_DEPTH>
+__device__ __forceinline__ void airy_profiles(double k, double z, double depth, double& cih, double& sih) {
+  if constexpr (FINITE_DEPTH) {
+    const double kh = k * depth;
+    if (kh >= 0.0 && kh < 20.0) {
+      const double ch = cosh(kh);
+      cih = cosh(k * (z + depth)) / ch;
+      sih = sinh(k * (z + depth)) / ch;
+      return;
+    }
+  }
+  cih = exp(k * z);
+  sih = cih;
+}
+
+template <bool FINITE_DEPTH>
 __global__ void build_rhs_kernel(int n, int64_t ldb, int64_t strideB, int batch, const double* __restrict__ omega,
-                                 const double* __restrict__ wavenumber, double g, int ndof,
+                                 const double* __restrict__ wavenumber, double g, double depth, int ndof,
                                  const double* __restrict__ dofn, int nhead, const double* __restrict__ headings,
                                  const double* __restrict__ centers, const double* __restrict__ normals,
                                  const int* __restrict__ hull, double2* __restrict__ B) {
@@ -44,12 +65,15 @@ __global__ void build_rhs_kernel(int n, int64_t ldb, int64_t strideB, int batch,
       const double wbar = x * cb + y * sb;
       double s, c;
       sincos(k * wbar, &s, &c);
-      const double amp = g * k / w * exp(k * z);
-      // v = amp e^{i k wbar} (cos b, sin b, -i); v . n
-      const double2 e = make_double2(amp * c, amp * s);
+      double cih, sih;
+      airy_profiles<FINITE_DEPTH>(k, z, depth, cih, sih);
+      const double amp_c = g * k / w * cih, amp_s = g * k / w * sih;
+      // v = (g k / w) e^{i k wbar} (cos b cih, sin b cih, -i sih); v . n
+      const double2 ec = make_double2(amp_c * c, amp_c * s);
+      const double2 es = make_double2(amp_s * c, amp_s * s);
       const double horiz = cb * nx + sb * ny;
-      // e * horiz + e * (-i) * nz
-      const double2 vn = make_double2(e.x * horiz + e.y * nz, e.y * horiz - e.x * nz);
+      // ec * horiz + es * (-i) * nz
+      const double2 vn = make_double2(ec.x * horiz + es.y * nz, ec.y * horiz - es.x * nz);
       bc = make_double2(-vn.x, -vn.y);
     }
     Bb[(size_t)i + (size_t)(ndof + h) * ldb] = bc;
@@ -165,9 +189,10 @@ __global__ void integrate_pressure_kernel(int n, int nrhs, int ndof, const doubl
   }
 }
 
-// Froude-Krylov: p0 = rho g e^{k z} e^{i k (x cos b + y sin b)}, F[b][h][d] = sum_i p0_i w[d][i]
+// Froude-Krylov: p0 = rho g cih(z) e^{i k (x cos b + y sin b)}, F[b][h][d] = sum_i p0_i w[d][i]
+template <bool FINITE_DEPTH>
 __global__ void froude_krylov_kernel(int n, int ndof, int nhead, const double* __restrict__ wavenumber, double rho,
-                                     double g, const double* __restrict__ headings,
+                                     double g, double depth, const double* __restrict__ headings,
                                      const double* __restrict__ centers, const double* __restrict__ wdof,
                                      double2* __restrict__ F) {
   const int d = blockIdx.x, h = blockIdx.y, b = blockIdx.z;
@@ -180,7 +205,9 @@ __global__ void froude_krylov_kernel(int n, int ndof, int nhead, const double* _
     const double x = centers[3 * i], y = centers[3 * i + 1], z = centers[3 * i + 2];
     double s, c;
     sincos(k * (x * cb + y * sb), &s, &c);
-    const double amp = rho * g * exp(k * z) * w[i];
+    double cih, sih;
+    airy_profiles<FINITE_DEPTH>(k, z, depth, cih, sih);
+    const double amp = rho * g * cih * w[i];
     sx += amp * c;
     sy += amp * s;
   }
@@ -204,16 +231,24 @@ __global__ void froude_krylov_kernel(int n, int ndof, int nhead, const double* _
 using namespace bem;
 
 extern "C" int bem_build_rhs(int n, int batch, const double* omega_dev, const double* wavenumber_dev, double g,
-                             int ndof, const double* dofn_dev, int nhead, const double* headings_dev,
-                             const double* centers_dev, const double* normals_dev, const int32_t* hull_dev,
-                             void* B_dev, int64_t ldb, int64_t strideB, void* stream) {
+                             double water_depth, int ndof, const double* dofn_dev, int nhead,
+                             const double* headings_dev, const double* centers_dev, const double* normals_dev,
+                             const int32_t* hull_dev, void* B_dev, int64_t ldb, int64_t strideB, void* stream) {
   if (n <= 0 || batch <= 0 || ndof < 0 || nhead < 0 || ldb < n || !B_dev || !omega_dev || !wavenumber_dev ||
-      (ndof > 0 && !dofn_dev) || (nhead > 0 && (!headings_dev || !centers_dev || !normals_dev)))
+      (ndof > 0 && !dofn_dev) || (nhead > 0 && (!headings_dev || !centers_dev || !normals_dev)) ||
+      !(water_depth > 0.0))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_build_rhs: bad arguments");
   dim3 grid(ceil_div(n, 128), batch);
-  build_rhs_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(n, ldb, strideB, batch, omega_dev, wavenumber_dev, g, ndof,
-                                                           dofn_dev, nhead, headings_dev, centers_dev, normals_dev,
-                                                           hull_dev, (double2*)B_dev);
+  if (std::isinf(water_depth))
+    build_rhs_kernel<false><<<grid, 128, 0, (cudaStream_t)stream>>>(n, ldb, strideB, batch, omega_dev, wavenumber_dev,
+                                                                    g, water_depth, ndof, dofn_dev, nhead,
+                                                                    headings_dev, centers_dev, normals_dev, hull_dev,
+                                                                    (double2*)B_dev);
+  else
+    build_rhs_kernel<true><<<grid, 128, 0, (cudaStream_t)stream>>>(n, ldb, strideB, batch, omega_dev, wavenumber_dev,
+                                                                   g, water_depth, ndof, dofn_dev, nhead,
+                                                                   headings_dev, centers_dev, normals_dev, hull_dev,
+                                                                   (double2*)B_dev);
   count_launches(1);
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
@@ -287,13 +322,18 @@ extern "C" int bem_integrate_pressure(int n, int batch, int nrhs, int ndof, cons
 }
 
 extern "C" int bem_froude_krylov(int n, int batch, int ndof, int nhead, const double* wavenumber_dev, double rho,
-                                 double g, const double* headings_dev, const double* centers_dev,
+                                 double g, double water_depth, const double* headings_dev, const double* centers_dev,
                                  const double* wdof_dev, void* F_dev, void* stream) {
   if (n <= 0 || batch <= 0 || ndof <= 0 || nhead <= 0 || !wavenumber_dev || !headings_dev || !centers_dev ||
-      !wdof_dev || !F_dev)
+      !wdof_dev || !F_dev || !(water_depth > 0.0))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_froude_krylov: bad arguments");
-  froude_krylov_kernel<<<dim3(ndof, nhead, batch), 256, 0, (cudaStream_t)stream>>>(
-      n, ndof, nhead, wavenumber_dev, rho, g, headings_dev, centers_dev, wdof_dev, (double2*)F_dev);
+  const dim3 grid(ndof, nhead, batch);
+  if (std::isinf(water_depth))
+    froude_krylov_kernel<false><<<grid, 256, 0, (cudaStream_t)stream>>>(
+        n, ndof, nhead, wavenumber_dev, rho, g, water_depth, headings_dev, centers_dev, wdof_dev, (double2*)F_dev);
+  else
+    froude_krylov_kernel<true><<<grid, 256, 0, (cudaStream_t)stream>>>(
+        n, ndof, nhead, wavenumber_dev, rho, g, water_depth, headings_dev, centers_dev, wdof_dev, (double2*)F_dev);
   count_launches(1);
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;

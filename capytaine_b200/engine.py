@@ -4,8 +4,9 @@ Two entry points:
 
 * ``B200Engine.solve_frequencies(body, omegas, ...)``: the whole indirect
   solve of many frequencies of one body, batched on the device (assembly of S
-  and K at k = omega^2/g, LU of K, every radiation and diffraction RHS, S @ sigma,
-  pressure integration) with only the coefficients coming back to the host.
+  and K at the wavenumber of each omega, k = omega^2/g in infinite depth, LU of
+  K, every radiation and diffraction RHS, S @ sigma, pressure integration) with
+  only the coefficients coming back to the host.
   One frequency-solve is what capytaine does for one (body, omega) group in
   ``BEMSolver.solve_all`` (bem/solver.py:268-372, problems grouped by
   bem/problems_and_results.py:267-275).
@@ -44,6 +45,48 @@ def padded_size(n: int) -> int:
 
 def _vp(x):
     return ctypes.c_void_p(x.data_ptr() if hasattr(x, "data_ptr") else int(x))
+
+
+def wavenumbers(omegas, water_depth: float = np.inf, g: float = 9.81) -> np.ndarray:
+    """Wavenumbers of the angular frequencies omegas: omega^2 / g in infinite
+    depth, else the root k > 0 of the dispersion relation k tanh(k h) = omega^2 / g
+    (bem/problems_and_results.py:159-163), by Newton's method kept inside a
+    bracket [lo, hi] that halves whenever a step leaves it.  0 and +inf map to
+    themselves."""
+    omegas = np.asarray(omegas, dtype=float)
+    w2g = omegas ** 2 / g
+    if water_depth == np.inf:
+        return w2g
+    if not water_depth > 0:
+        raise ValueError(f"water_depth must be > 0 (got {water_depth})")
+    h = float(water_depth)
+    out = np.empty_like(w2g)
+    for i, c in enumerate(w2g.ravel()):
+        if c == 0.0 or c == np.inf:
+            out.flat[i] = c
+            continue
+        # k tanh(k h) is increasing, below k, and above c at k = hi
+        lo, hi = c, c + np.sqrt(c / h)
+        while hi * np.tanh(hi * h) <= c:
+            hi *= 2.0
+        k = 0.5 * (lo + hi)
+        for _ in range(200):
+            t = np.tanh(k * h)
+            f = k * t - c
+            if f > 0:
+                hi = k
+            else:
+                lo = k
+            step = f / (t + k * h * (1.0 - t * t))
+            k_new = k - step
+            if not lo < k_new < hi:
+                k_new = 0.5 * (lo + hi)
+            if abs(k_new - k) <= 4e-16 * k_new:
+                k = k_new
+                break
+            k = k_new
+        out.flat[i] = k
+    return out
 
 
 @dataclass
@@ -384,9 +427,16 @@ class B200Engine:
             return arrays
 
     def solve_frequencies(self, body, omegas: Sequence[float], *, wave_directions: Sequence[float] = (0.0,),
-                          rho: float = 1000.0, g: float = 9.81, batch: Optional[int] = None,
-                          sync_stats: bool = False) -> FrequencyResults:
+                          rho: float = 1000.0, g: float = 9.81, water_depth: float = np.inf,
+                          batch: Optional[int] = None, sync_stats: bool = False) -> FrequencyResults:
+        """Added mass, damping and excitation of `body` at every omega (finite,
+        > 0) and wave direction, in water of depth water_depth (+inf: infinite
+        depth; finite: Delhommeau's finite-depth Green function with its Prony
+        decomposition, the assembly then in float64 whatever
+        assembly_precision, and finite-depth Airy waves)."""
         import torch
+        if not water_depth > 0:
+            raise ValueError(f"water_depth must be > 0 (got {water_depth})")
         mesh = body.mesh_including_lid
         n = mesh.nb_faces
         omegas = np.asarray(omegas, dtype=float)
@@ -396,7 +446,7 @@ class B200Engine:
         B = min(self.max_batch if batch is None else batch, len(omegas))
         st = block_structure(mesh)
         if st is not None:
-            return self._solve_frequencies_symmetric(body, st, omegas, heads, rho, g, B, sync_stats)
+            return self._solve_frequencies_symmetric(body, st, omegas, heads, rho, g, B, sync_stats, water_depth)
         ws = self.workspace(n, B, nrhs)
         F_all = np.zeros((len(omegas), nrhs, ndof), dtype=np.complex128)
         FK_all = np.zeros((len(omegas), max(nhead, 1), ndof), dtype=np.complex128)
@@ -408,13 +458,15 @@ class B200Engine:
             if ev:
                 ev[0].record()
             ws.r.flags.zero_()
-            self.assemble_stage(ws.f, mesh, om ** 2 / g, nan_flag=ws.r.nan)
+            self.assemble_stage(ws.f, mesh, wavenumbers(om, water_depth, g), nan_flag=ws.r.nan,
+                                water_depth=water_depth)
             if ev:
                 ev[1].record()
             self.factor_stage(ws.f, nb, ws.r.err)
             if ev:
                 ev[2].record()
-            F, FK = self.solve_stage(ws.f, ws.r, body, om, heads, rho=rho, g=g, stats=stats, events=ev)
+            F, FK = self.solve_stage(ws.f, ws.r, body, om, heads, rho=rho, g=g, stats=stats, events=ev,
+                                     water_depth=water_depth)
             F_all[start:start + nb] = F
             FK_all[start:start + nb, :nhead] = FK
             if ev:
@@ -425,7 +477,7 @@ class B200Engine:
                 stats["post_ms"] += ev[3].elapsed_time(ev[4])
         return self._coefficients(body, omegas, heads, F_all, FK_all, stats)
 
-    def _solve_frequencies_symmetric(self, body, st, omegas, heads, rho, g, B, sync_stats):
+    def _solve_frequencies_symmetric(self, body, st, omegas, heads, rho, g, B, sync_stats, water_depth=np.inf):
         """solve_frequencies for a mesh with symmetries (bem/engines.py:178-247,
         tools/block_circulant_matrices.py): per frequency, S and K of the whole
         mesh's collocation points against the panels of the reference sub-mesh
@@ -457,7 +509,7 @@ class B200Engine:
         for start in range(0, len(omegas), B):
             om = omegas[start:start + B]
             nb = len(om)
-            ks = [float(k) for k in om ** 2 / g]
+            ks = [float(k) for k in wavenumbers(om, water_depth, g)]
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)] if sync_stats else None
             if ev:
                 ev[0].record()
@@ -465,7 +517,7 @@ class B200Engine:
             cstride = N * st.n_sub
             gf.assemble_into(full, st.submesh, ws.cols[0, 0], ws.cols[1, 0], wavenumber=ks[0], lds=N, ldk=N,
                              nan_flag=ws.r.nan, precision=self.assembly_precision, adjoint_double_layer=adjoint,
-                             sweep=(ks, cstride, cstride))
+                             sweep=(ks, cstride, cstride), water_depth=water_depth)
             ws.combine_matrices(ws.cols[0], nb, f.S, st.n_sys, st.n_sys * st.n_sys, stream)
             ws.combine_matrices(ws.cols[1], nb, f.K, f.ldk, f.strideK, stream)
             if ev:
@@ -474,7 +526,7 @@ class B200Engine:
             if ev:
                 ev[2].record()
             (F, FK), = self._solve_segments(f, ws.r, [(body, 0, nb)], om, heads, rho=rho, g=g, stats=stats,
-                                            events=ev, sym=ws)
+                                            events=ev, sym=ws, water_depth=water_depth)
             F_all[start:start + nb] = F
             FK_all[start:start + nb, :nhead] = FK
             if ev:
@@ -492,10 +544,12 @@ class B200Engine:
     def _plain_gmres(self):
         return self.precision == "fp64" and self._linear_solver == "gmres"
 
-    def assemble_stage(self, f: "_Factors", mesh, ks, *, nan_flag=None, reuse_rankine=True, first=0, lds=None):
+    def assemble_stage(self, f: "_Factors", mesh, ks, *, nan_flag=None, reuse_rankine=True, first=0, lds=None,
+                       water_depth=np.inf):
         """S and K of the mesh with itself at the wavenumbers ks into
         f[first:first+len(ks)] (one launch for all of them on the Rankine-reuse
-        path when every wavenumber is finite and > 0)."""
+        path when every wavenumber is finite and > 0; one per wavenumber in
+        finite depth)."""
         gf = self.green_function
         n = mesh.nb_faces
         lds = n if lds is None else lds
@@ -504,12 +558,13 @@ class B200Engine:
         if len(ks) > 1 and all(0.0 < k < np.inf for k in ks):
             gf.assemble_into(mesh, mesh, f.S[first], f.K[first], wavenumber=ks[0], lds=lds, ldk=f.ldk,
                              nan_flag=nan_flag, precision=self.assembly_precision, reuse_rankine=reuse_rankine,
-                             sweep=(ks, f.S.shape[1], f.K.shape[1]), adjoint_double_layer=adjoint)
+                             sweep=(ks, f.S.shape[1], f.K.shape[1]), adjoint_double_layer=adjoint,
+                             water_depth=water_depth)
             return
         for b, k in enumerate(ks):
             gf.assemble_into(mesh, mesh, f.S[first + b], f.K[first + b], wavenumber=k, lds=lds, ldk=f.ldk,
                              nan_flag=nan_flag, precision=self.assembly_precision, reuse_rankine=reuse_rankine,
-                             adjoint_double_layer=adjoint)
+                             adjoint_double_layer=adjoint, water_depth=water_depth)
 
     def factor_stage(self, f: "_Factors", nb, err):
         """LU of K (float64 DMMA, or float32 tcgen05 for the mixed engine); none for plain GMRES."""
@@ -525,7 +580,7 @@ class B200Engine:
                                           _vp(f.lu_work), stream))
 
     def solve_stage(self, f: "_Factors", r: "_Rhs", body, om, heads, *, rho=1000.0, g=9.81, stats=None,
-                    events=None):
+                    events=None, water_depth=np.inf):
         """Right-hand sides, solve with the factors, S @ sigma and the force
         integrals for the frequencies om (f[0:len(om)]); returns host arrays
         F (nb, nrhs, ndof) and FK (nb, nhead, ndof).  Raises the reference's
@@ -534,11 +589,11 @@ class B200Engine:
         if r.nrhs != ndof + len(heads) or r.batch < len(om):
             raise ValueError("right-hand side buffers of the wrong shape")
         (F, FK), = self._solve_segments(f, r, [(body, 0, len(om))], om, heads, rho=rho, g=g, stats=stats,
-                                        events=events)
+                                        events=events, water_depth=water_depth)
         return F, FK
 
     def _solve_segments(self, f: "_Factors", r: "_Rhs", segments, om, heads, *, rho=1000.0, g=9.81, stats=None,
-                        events=None, sym: Optional[_SymWorkspace] = None):
+                        events=None, sym: Optional[_SymWorkspace] = None, water_depth=np.inf):
         """solve_stage for batch entries holding several bodies: segments
         [(body, j0, m)] give the body of entries j0 .. j0+m-1.  A body smaller
         than the system (f.n, identity-padded) has zero right-hand-side rows
@@ -556,7 +611,7 @@ class B200Engine:
         om = np.asarray(om, dtype=float)
         nb = len(om)
         nbs = nb * (sym.st.nsys if sym is not None else 1)  # systems of this batch
-        ks = om ** 2 / g
+        ks = wavenumbers(om, water_depth, g)
         heads = np.asarray(heads, dtype=float)
         nhead = len(heads)
         nrhs = r.nrhs
@@ -579,8 +634,8 @@ class B200Engine:
             dofn, wdof, hull = self._body_arrays(body, mesh)
             seg_arrays.append((mesh.nb_faces, ndof, dm, wdof))
             _lib.check(lib.bem_build_rhs(mesh.nb_faces, m, _vp(om_t.data_ptr() + 8 * j0),
-                                         _vp(k_t.data_ptr() + 8 * j0), g, ndof, _vp(dofn), nhead, _vp(heads_t),
-                                         _vp(dm.centers), _vp(dm.normals), _vp(hull),
+                                         _vp(k_t.data_ptr() + 8 * j0), g, float(water_depth), ndof, _vp(dofn),
+                                         nhead, _vp(heads_t), _vp(dm.centers), _vp(dm.normals), _vp(hull),
                                          _vp(rhs.data_ptr() + 16 * j0 * rhs_stride), rhs_ld, rhs_stride, stream))
         if sym is not None:
             sym.to_systems(nb, r.B, npad, ld, stream)
@@ -632,7 +687,8 @@ class B200Engine:
                                                   _vp(om_t.data_ptr() + 8 * j0), rho, _vp(wdof), _vp(F), stream))
             if nhead > 0:
                 _lib.check(lib.bem_froude_krylov(nf, m, ndof, nhead, _vp(k_t.data_ptr() + 8 * j0), rho, g,
-                                                 _vp(heads_t), _vp(dm.centers), _vp(wdof), _vp(FK), stream))
+                                                 float(water_depth), _vp(heads_t), _vp(dm.centers), _vp(wdof),
+                                                 _vp(FK), stream))
         if events:
             events[4].record()
         host = out.cpu().numpy()

@@ -470,12 +470,13 @@ class Delhommeau:
                                    wavenumber, adjoint_double_layer, early_dot_product,
                                    diagonal_term_in_double_layer, lds, ldk, precision, stream, nan_flag):
         """One wavenumber of _assemble_finite_depth, S and K written s_offset and
-        k_offset elements after the start of their buffers."""
+        k_offset elements after the start of their buffers.  Every term in
+        float64, whatever `precision` asks (there is no mixed-precision
+        finite-depth kernel)."""
         import torch
-        prec = self.precision if precision is None else precision
-        if S.dtype != torch.complex128 or K.dtype != torch.complex128 or prec != "fp64" or not early_dot_product:
-            raise NotImplementedError("finite depth on the device: float64 assembly, complex128 outputs and the "
-                                      "dot product taken (early_dot_product=True) only")
+        if S.dtype != torch.complex128 or K.dtype != torch.complex128 or not early_dot_product:
+            raise NotImplementedError("finite depth on the device: complex128 outputs and the dot product taken "
+                                      "(early_dot_product=True) only")
         pts, nrm = self._collocation(mesh1, mesh2, adjoint_double_layer)
         dm2 = self.device_mesh(mesh2)
         n = pts.shape[0]

@@ -226,15 +226,17 @@ int bem_zlu_solve(const void* A_dev, int n, int64_t lda, int64_t stride, int bat
 
 /* ---- right-hand sides, potentials, forces --------------------------------- */
 /* Columns 0..ndof-1: radiation BC -1j*omega*(dof . n) (dofn_dev: ndof x n);
- * columns ndof..ndof+nhead-1: diffraction BC -(u_Airy . n), infinite depth.
- * Zero where hull_dev[i] == 0 (lid panels; hull_dev may be NULL).  One batch
- * entry per frequency (omega_dev, wavenumber_dev: batch doubles).
- * Replaces bem/problems_and_results.py:373-381, 440-449 and
- * bem/airy_waves.py:56-95. */
-int bem_build_rhs(int n, int batch, const double* omega_dev, const double* wavenumber_dev, double g, int ndof,
-                  const double* dofn_dev, int nhead, const double* headings_dev, const double* centers_dev,
-                  const double* normals_dev, const int32_t* hull_dev, void* B_dev, int64_t ldb, int64_t strideB,
-                  void* stream);
+ * columns ndof..ndof+nhead-1: diffraction BC -(u_Airy . n) in water of depth
+ * water_depth (> 0; +inf: infinite depth): depth profiles cosh(k(z+h))/cosh(kh)
+ * and sinh(k(z+h))/cosh(kh) when 0 <= kh < 20, else e^{kz}.  Zero where
+ * hull_dev[i] == 0 (lid panels; hull_dev may be NULL).  One batch entry per
+ * frequency (omega_dev, wavenumber_dev: batch doubles; the wavenumbers are the
+ * roots of the dispersion relation in that depth).  Replaces
+ * bem/problems_and_results.py:373-381, 440-449 and bem/airy_waves.py:56-95. */
+int bem_build_rhs(int n, int batch, const double* omega_dev, const double* wavenumber_dev, double g,
+                  double water_depth, int ndof, const double* dofn_dev, int nhead, const double* headings_dev,
+                  const double* centers_dev, const double* normals_dev, const int32_t* hull_dev, void* B_dev,
+                  int64_t ldb, int64_t strideB, void* stream);
 
 /* Y = alpha A X + beta Y, A (M x K) complex128, X (K x nrhs), nrhs <= 16:
  * the potential S @ sigma (bem/solver.py:197-198) and residuals. */
@@ -250,10 +252,11 @@ int bem_integrate_pressure(int n, int batch, int nrhs, int ndof, const void* phi
                            const double* omega_dev, double rho, const double* wdof_dev, void* F_dev, void* stream);
 
 /* Froude-Krylov force of each heading: F[b][h][d] = sum_i p0_i wdof[d][i],
- * p0 = rho g exp(k z) exp(i k (x cos beta + y sin beta)) (airy_waves.py:19-53,98-102). */
+ * p0 = rho g cih(z) exp(i k (x cos beta + y sin beta)), cih the depth profile
+ * of bem_build_rhs (exp(k z) in infinite depth) (airy_waves.py:19-53,98-102). */
 int bem_froude_krylov(int n, int batch, int ndof, int nhead, const double* wavenumber_dev, double rho, double g,
-                      const double* headings_dev, const double* centers_dev, const double* wdof_dev, void* F_dev,
-                      void* stream);
+                      double water_depth, const double* headings_dev, const double* centers_dev,
+                      const double* wdof_dev, void* F_dev, void* stream);
 
 /* ---- tensor-core complex update (mixed precision) ------------------------- */
 /* C -= A B for complex A (m x k) and B (k x n) on the tcgen05 tensor cores with

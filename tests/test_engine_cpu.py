@@ -65,3 +65,29 @@ def test_tabulation_cache_file_name_is_the_reference_one():
     gf = Delhommeau(tabulation_nr=3, tabulation_rmax=1, tabulation_nz=3, tabulation_zmin=-1,
                     tabulation_nb_integration_points=10, tabulation_grid_shape="legacy", tabulation_cache_dir=None)
     assert gf._cache_filename == "tabulation_float64_legacy_3_1.0_3_-1.0_10.npz"
+
+
+@pytest.mark.parametrize("depth", [0.5, 1.0, 10.0, 1000.0])
+def test_finite_depth_wavenumbers(oracle_mod, depth):
+    """The dispersion relation omega^2 = g k tanh(k h) of the finite-depth
+    problems (bem/problems_and_results.py:159-163; the reference's
+    test_bem_problems_and_results.py:43-46 checks the same identity), against
+    the oracle's root, from shallow to deep water."""
+    from capytaine_b200.engine import wavenumbers
+    omegas = np.array([1e-3, 0.05, 0.3, 1.0, 2.5, 8.0])
+    ks = wavenumbers(omegas, depth)
+    np.testing.assert_allclose(9.81 * ks * np.tanh(ks * depth), omegas ** 2, rtol=1e-14)
+    ref = [oracle_mod.finite_depth_wavenumber(w, depth) for w in omegas]
+    np.testing.assert_allclose(ks, ref, rtol=1e-12)
+    assert np.all(ks >= omegas ** 2 / 9.81)  # tanh < 1: longer waves than in deep water
+
+
+def test_infinite_depth_wavenumbers_and_limits():
+    from capytaine_b200.engine import wavenumbers
+    omegas = np.array([0.1, 1.0, 3.0])
+    assert np.array_equal(wavenumbers(omegas), omegas ** 2 / 9.81)  # exactly, as the reference
+    assert np.array_equal(wavenumbers(omegas, np.inf, 9.8), omegas ** 2 / 9.8)
+    np.testing.assert_array_equal(wavenumbers([0.0, np.inf], 10.0), [0.0, np.inf])
+    for depth in (0.0, -1.0, np.nan):
+        with pytest.raises(ValueError):
+            wavenumbers([1.0], depth)

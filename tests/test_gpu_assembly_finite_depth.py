@@ -149,3 +149,54 @@ def test_finite_depth_solve_through_matrix_engine(oracle_mod, default_oracle_gf,
     scale = max(abs(v) for v in want.values())
     errs = [_coefficient_error(diffraction[d], want[d], scale) for d in want]
     assert max(errs) < 1e-7, errs
+
+
+@pytest.mark.parametrize("precision,gate", [("fp64", 1e-6), ("mixed", 1e-5)])
+def test_finite_depth_frequency_solve_matches_oracle(oracle_mod, default_oracle_gf, tmp_path, precision, gate):
+    """B200Engine.solve_frequencies(water_depth=h): wavenumbers of the
+    finite-depth dispersion relation, the finite-depth assembly, the LU, the
+    finite-depth Airy right-hand sides and Froude-Krylov forces, against the
+    oracle's finite-depth solve; a shallow case (Airy profiles cosh / sinh) and
+    a deep one where k h >= 20 at the highest frequency (profiles e^{kz}).
+    Gates of the frequency-solve metric (float64 1e-6, mixed 1e-5 per
+    coefficient, floor 1e-3 of the largest): the float64 solve was seen at
+    4.7e-8 in 50 m of water (a few 1e-11 of the largest coefficient)."""
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.engine import B200Engine
+    from test_gpu_solve import coefficient_errors
+    mesh = mesh_sphere(radius=1.0, resolution=(10, 20)).immersed_part()
+    body = FloatingBody(mesh, rigid_body_dofs())
+    heads = (0.0, np.pi / 3)
+    eng = B200Engine(green_function=_gpu_gf(default_oracle_gf, tmp_path), precision=precision, max_batch=2)
+    odofs = oracle_mod.rigid_body_dofs()
+    for depth, omegas in ((3.0, np.array([0.6, 1.4, 3.0])), (50.0, np.array([0.6, 3.0]))):
+        res = eng.solve_frequencies(body, omegas, wave_directions=heads, water_depth=depth)
+        ref = [oracle_mod.solve_frequency(default_oracle_gf, mesh, odofs, w, wave_directions=heads,
+                                          water_depth=depth) for w in omegas]
+        errs = coefficient_errors(res, ref, body.dofs)
+        assert max(errs.values()) < gate, (depth, errs)
+
+
+@pytest.mark.parametrize("kind", ["reflections", "rotation"])
+def test_finite_depth_symmetric_frequency_solve_matches_oracle(oracle_mod, default_oracle_gf, tmp_path, kind):
+    """Meshes with symmetries in finite depth: the first block column assembled
+    by the finite-depth kernel (the whole mesh's points against the sub-mesh),
+    the block-diagonalised systems, against the oracle's block-circulant solve
+    in the same depth."""
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.engine import B200Engine
+    from capytaine_b200.symmetry import block_structure
+    from test_gpu_solve import coefficient_errors
+    from test_symmetry_cpu import _symmetric_cases
+    mesh = _symmetric_cases(exact=False)[kind]
+    body = FloatingBody(mesh, rigid_body_dofs())
+    depth, omegas, heads = 5.0, np.array([0.7, 1.8]), (0.0, 0.7)
+    eng = B200Engine(green_function=_gpu_gf(default_oracle_gf, tmp_path), max_batch=2)
+    res = eng.solve_frequencies(body, omegas, wave_directions=heads, water_depth=depth)
+    assert res.stats["symmetry"] == kind
+    st = block_structure(mesh)
+    ref = [oracle_mod.solve_frequency_symmetric(default_oracle_gf, mesh.merged(), st.submesh, st.nb_images,
+                                                st.kind in ("reflections", "dihedral"), oracle_mod.rigid_body_dofs(),
+                                                w, wave_directions=heads, water_depth=depth) for w in omegas]
+    errs = coefficient_errors(res, ref, body.dofs)
+    assert max(errs.values()) < 1e-6, errs

@@ -237,11 +237,16 @@ def test_linear_algebra_arguments_checked_on_host(lib):
                                fake, fake, ctypes.byref(it), ctypes.byref(res), None) == bad  # lda < n
     assert lib.bem_gmres_workspace_bytes(100, 128, 1, 1, 20) > 0
     # right-hand sides and forces: ldb < n, null outputs
-    assert lib.bem_build_rhs(100, 1, fake, fake, 9.81, 1, fake, 1, fake, fake, fake, None, fake, 99, 100 * 2,
+    inf = float("inf")
+    assert lib.bem_build_rhs(100, 1, fake, fake, 9.81, inf, 1, fake, 1, fake, fake, fake, None, fake, 99, 100 * 2,
                              None) == bad
+    for depth in (0.0, -5.0, float("nan")):  # water depth must be > 0 (+inf: infinite depth)
+        assert lib.bem_build_rhs(100, 1, fake, fake, 9.81, depth, 1, fake, 1, fake, fake, fake, None, fake, 100,
+                                 100 * 2, None) == bad
+        assert lib.bem_froude_krylov(100, 1, 1, 1, fake, 1000.0, 9.81, depth, fake, fake, fake, fake, None) == bad
     assert lib.bem_integrate_pressure(100, 1, 2, 1, fake, 99, 200, fake, 1000.0, fake, fake, None) == bad
     assert lib.bem_integrate_pressure(100, 1, 2, 1, fake, 100, 200, fake, 1000.0, fake, None, None) == bad
-    assert lib.bem_froude_krylov(100, 1, 1, 0, fake, 1000.0, 9.81, fake, fake, fake, fake, None) == bad
+    assert lib.bem_froude_krylov(100, 1, 1, 0, fake, 1000.0, 9.81, inf, fake, fake, fake, fake, None) == bad
 
 
 def test_c_program_links_against_the_library(lib):
