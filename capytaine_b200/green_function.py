@@ -171,17 +171,19 @@ class Delhommeau:
             raise ValueError(f"Unrecognized name for the Prony decomposition method: {method!r}. "
                              "Expected 'python' or 'fortran'.")
         kh = float(dimensionless_wavenumber)
-        cache = self.__dict__.setdefault("_prony_cache", OrderedDict())
-        hit = cache.get(kh)
+        with self._lock:
+            cache = self.__dict__.setdefault("_prony_cache", OrderedDict())
+            hit = cache.get(kh)
         if hit is None:
             try:
                 hit = prony.green_function_decomposition(kh)
             except prony.PronyDecompositionFailure as e:
                 raise _lib.GreenFunctionEvaluationError(
                     _lib.BEM_ERR_NOT_CONVERGED, f"{self} cannot evaluate finite depth Green function for kh={kh}") from e
-            cache[kh] = hit
-            while len(cache) > 128:
-                cache.popitem(last=False)
+            with self._lock:
+                cache[kh] = hit
+                while len(cache) > 128:
+                    cache.popitem(last=False)
         return hit.copy()
 
     def __str__(self):

@@ -36,6 +36,51 @@ def test_library_exports_every_declared_symbol(lib):
     assert sorted(_lib.exported_symbols()) == declared
 
 
+def _prototypes():
+    """{name: (return type, [parameter types])} of the header's functions."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for ret, name, params in re.findall(r"([\w\s\*]+?)\s*\b(bem_\w+)\s*\(([^)]*)\)\s*;", text):
+        params = " ".join(params.split())
+        plist = [] if params in ("", "void") else [p.strip() for p in params.split(",")]
+        out[name] = (" ".join(ret.split()), plist)
+    return out
+
+
+def _c_kind(decl):
+    """Argument class of a C declaration: pointer, double, int64 or int32."""
+    if "*" in decl:
+        return "pointer"
+    words = decl.replace("const ", "").split()
+    base = " ".join(words[:-1]) if len(words) > 1 else words[0]
+    return {"double": "double", "int64_t": "int64", "long long": "int64", "int": "int32",
+            "int32_t": "int32"}[base]
+
+
+def _ctypes_kind(t):
+    if t in (ctypes.c_void_p, ctypes.c_char_p) or (isinstance(t, type) and issubclass(t, ctypes._Pointer)):
+        return "pointer"
+    if t is ctypes.c_double:
+        return "double"
+    if ctypes.sizeof(t) == 8:
+        return "int64"
+    assert ctypes.sizeof(t) == 4, t
+    return "int32"
+
+
+def test_binding_signatures_match_header():
+    """Every ctypes signature has the header prototype's number and classes of
+    arguments and its return class: a mismatch would pass arguments in the
+    wrong registers without any error."""
+    protos = _prototypes()
+    assert sorted(protos) == _declared_functions()
+    for name, (argtypes, restype) in _lib._SIGNATURES.items():
+        ret, params = protos[name]
+        assert [_c_kind(p) for p in params] == [_ctypes_kind(t) for t in argtypes], name
+        ret_kind = "pointer" if "*" in ret else _c_kind(ret + " r")
+        assert ret_kind == _ctypes_kind(restype), name
+
+
 def test_version_and_error_string(lib):
     assert lib.bem_version() >= 100
     assert isinstance(lib.bem_last_error(), bytes)
