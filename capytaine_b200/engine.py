@@ -429,17 +429,23 @@ class B200Engine:
     def solve_frequencies(self, body, omegas: Sequence[float], *, wave_directions: Sequence[float] = (0.0,),
                           rho: float = 1000.0, g: float = 9.81, water_depth: float = np.inf,
                           batch: Optional[int] = None, sync_stats: bool = False) -> FrequencyResults:
-        """Added mass, damping and excitation of `body` at every omega (finite,
-        > 0) and wave direction, in water of depth water_depth (+inf: infinite
-        depth; finite: Delhommeau's finite-depth Green function with its Prony
-        decomposition, the assembly then in float64 whatever
-        assembly_precision, and finite-depth Airy waves)."""
+        """Added mass, damping and excitation of `body` at every omega and wave
+        direction, in water of depth water_depth (+inf: infinite depth; finite:
+        Delhommeau's finite-depth Green function with its Prony decomposition,
+        the assembly then in float64 whatever assembly_precision, and
+        finite-depth Airy waves).  omega = 0 and omega = infinity give the
+        limit-frequency radiation coefficients (zero damping) and NaN wave
+        forces, as capytaine's symbolic-frequency problems do; omega = 0 in
+        finite depth raises NotImplementedError (no Prony decomposition at
+        k h = 0), as capytaine does."""
         import torch
         if not water_depth > 0:
             raise ValueError(f"water_depth must be > 0 (got {water_depth})")
         mesh = body.mesh_including_lid
         n = mesh.nb_faces
         omegas = np.asarray(omegas, dtype=float)
+        if np.any(np.isnan(omegas)) or np.any(omegas < 0):
+            raise ValueError("angular frequencies must be >= 0 (or infinity)")
         heads = np.asarray(wave_directions, dtype=float)
         ndof, nhead = len(body.dofs), len(heads)
         nrhs = ndof + nhead
@@ -612,6 +618,14 @@ class B200Engine:
         nb = len(om)
         nbs = nb * (sym.st.nsys if sym is not None else 1)  # systems of this batch
         ks = wavenumbers(om, water_depth, g)
+        # omega = 0 or infinity: the frequency of the radiation problems is a
+        # symbolic factor that the added mass cancels (problems_and_results.py:
+        # 440-449, 583-592), so their right-hand sides and pressures take
+        # omega = 1 (the matrices keep k = 0 or infinity); their diffraction
+        # columns are left at zero (k = 0) and reported as NaN.
+        limit = (om == 0.0) | np.isinf(om)
+        om = np.where(limit, 1.0, om)
+        ks = np.where(limit, 0.0, ks)
         heads = np.asarray(heads, dtype=float)
         nhead = len(heads)
         nrhs = r.nrhs
@@ -852,13 +866,22 @@ class B200Engine:
 
     @staticmethod
     def _coefficients(body, omegas, heads, F_all, FK_all, stats):
+        """Added mass Re(F) / omega^2, damping Im(F) / omega and the wave forces
+        (problems_and_results.py:583-592); at omega = 0 or infinity the forces
+        were computed with omega = 1, the damping is zero and the wave forces
+        are NaN (the reference's limit-frequency results, airy_waves.py:36-37)."""
         ndof = len(body.dofs)
-        w = omegas[:, None, None]
+        omegas = np.asarray(omegas, dtype=float)
+        limit = (omegas == 0.0) | np.isinf(omegas)
+        w = np.where(limit, 1.0, omegas)[:, None, None]
         rad = F_all[:, :ndof, :]
         added_mass = np.real(rad) / w ** 2
         damping = np.imag(rad) / w
-        diffraction = F_all[:, ndof:, :]
-        fk = FK_all[:, : len(heads), :]
+        damping[limit] = 0.0
+        diffraction = F_all[:, ndof:, :].copy()
+        fk = FK_all[:, : len(heads), :].copy()
+        diffraction[limit] = np.nan
+        fk[limit] = np.nan
         return FrequencyResults(omegas=omegas, dofs=list(body.dofs), wave_directions=heads, added_mass=added_mass,
                                 radiation_damping=damping, diffraction=diffraction, froude_krylov=fk,
                                 excitation=diffraction + fk, stats=stats)

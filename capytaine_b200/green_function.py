@@ -346,7 +346,12 @@ class Delhommeau:
         n = pts.shape[0]
         wavenumber = float(wavenumber)
         sing = self._variant(dm2.centers_z, wavenumber) if free_surface != np.inf else self.gf_singularities
-        need_wave = free_surface != np.inf and 0.0 < wavenumber < np.inf
+        # the table is loaded when any wavenumber of the call is finite and > 0;
+        # the paths that share work across a sweep need every one of them to be
+        ks_all = [wavenumber] if sweep is None else [float(k) for k in sweep[0]]
+        finite_ks = [0.0 < k < np.inf for k in ks_all]
+        need_wave = free_surface != np.inf and any(finite_ks)
+        all_wave = free_surface != np.inf and all(finite_ks)
         prec = self.precision if precision is None else precision
         if need_wave:
             r, z, table, table32 = self._device_tabulation()
@@ -385,7 +390,7 @@ class Delhommeau:
         )
         lib = _lib.load()
         same_mesh = hasattr(mesh1, "faces_centers") and mesh1.content_hash == mesh2.content_hash
-        if (reuse_rankine and same_mesh and dm2.collocation_at_quadrature and need_wave
+        if (reuse_rankine and same_mesh and dm2.collocation_at_quadrature and all_wave
                 and sing in ("low_freq", "high_freq")
                 and prec == "fp64" and dtype == _lib.BEM_DTYPE_C128 and early_dot_product
                 and 16 * n * n <= self.rankine_cache_bytes):
@@ -404,7 +409,7 @@ class Delhommeau:
                 return
             _lib.check(lib.bem_assemble_wave_symmetric(a, rank.data_ptr(), n, _lib.stream_ptr(stream)))
             return
-        if (self.symmetric_assembly and same_mesh and dm2.collocation_at_quadrature and need_wave
+        if (self.symmetric_assembly and same_mesh and dm2.collocation_at_quadrature and all_wave
                 and sing in ("low_freq", "high_freq") and prec == "fp64" and dtype == _lib.BEM_DTYPE_C128
                 and early_dot_product and (ldk if ldk is not None else n) >= n):
             # One wavenumber at a time, nothing reused: Rankine part into K, then the
@@ -423,7 +428,7 @@ class Delhommeau:
                 _lib.check(lib.bem_assemble_symmetric(a, _lib.stream_ptr(stream)))
             return
         if (reuse_rankine and sweep is not None and not same_mesh and hasattr(mesh1, "faces_centers")
-                and dm2.collocation_at_quadrature and need_wave and sing in ("low_freq", "high_freq")
+                and dm2.collocation_at_quadrature and all_wave and sing in ("low_freq", "high_freq")
                 and prec == "fp64" and dtype == _lib.BEM_DTYPE_C128 and early_dot_product
                 and 16 * n * dm2.nb_faces <= self.rankine_cache_bytes):
             # Any points against a mesh over a sweep (the first block column of a
@@ -441,6 +446,8 @@ class Delhommeau:
             esize = S.element_size()
             for i, k in enumerate(ks):
                 a.wavenumber = float(k)
+                if free_surface != np.inf:  # the variant of each wavenumber (delhommeau.py:466-490)
+                    a.gf_singularities = _SING[self._variant(dm2.centers_z, float(k))]
                 a.S_dev = S.data_ptr() + i * int(s_stride) * esize
                 a.K_dev = K.data_ptr() + i * int(k_stride) * esize
                 _lib.check(lib.bem_assemble(a, _lib.stream_ptr(stream)))

@@ -145,6 +145,9 @@ class SolveServer:
     # ---- public API ---------------------------------------------------------
     def submit(self, body, omega: float, *, wave_directions: Sequence[float] = (0.0,), rho: float = 1000.0,
                g: float = 9.81) -> cf.Future:
+        if not 0.0 < float(omega) < np.inf:
+            raise ValueError("the request server solves finite, non-zero frequencies; omega = 0 or infinity "
+                             "goes through B200Engine.solve_frequencies")
         heads = np.asarray(wave_directions, dtype=float)
         mesh = body.mesh_including_lid
         nrhs = len(body.dofs) + len(heads)

@@ -91,3 +91,24 @@ def test_infinite_depth_wavenumbers_and_limits():
     for depth in (0.0, -1.0, np.nan):
         with pytest.raises(ValueError):
             wavenumbers([1.0], depth)
+
+
+def test_limit_frequency_coefficients():
+    """At omega = 0 and infinity the forces come computed with omega = 1: the
+    added mass is Re(F), the damping exactly zero and the wave forces NaN
+    (capytaine's symbolic-frequency results, problems_and_results.py:583-592,
+    airy_waves.py:36-37); finite omegas divide as usual."""
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.meshes import mesh_sphere
+    body = FloatingBody(mesh_sphere(resolution=(4, 4)).immersed_part(), rigid_body_dofs(only=["Surge", "Heave"]))
+    omegas = np.array([0.0, 2.0, np.inf])
+    rng = np.random.default_rng(0)
+    F = rng.standard_normal((3, 3, 2)) + 1j * rng.standard_normal((3, 3, 2))  # 2 dofs + 1 heading
+    FK = rng.standard_normal((3, 1, 2)) + 1j * rng.standard_normal((3, 1, 2))
+    res = B200Engine._coefficients(body, omegas, np.array([0.0]), F, FK, {})
+    np.testing.assert_array_equal(res.added_mass[[0, 2]], F[[0, 2], :2].real)
+    np.testing.assert_allclose(res.added_mass[1], F[1, :2].real / 4.0)
+    assert np.all(res.radiation_damping[[0, 2]] == 0.0)
+    np.testing.assert_allclose(res.radiation_damping[1], F[1, :2].imag / 2.0)
+    assert np.all(np.isnan(res.excitation[[0, 2]])) and np.all(np.isnan(res.froude_krylov[[0, 2]]))
+    np.testing.assert_allclose(res.excitation[1], F[1, 2:] + FK[1])

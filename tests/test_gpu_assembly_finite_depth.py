@@ -3,6 +3,7 @@ Delhommeau's method of matrices.f90:197-305 and Green_wave.f90:311-508) with
 the CPU oracle.  Both sides take the same tabulation (through the cache file)
 and the same Prony decomposition, so only floating-point rounding is left:
 1e-10 relative to the largest entry, as the infinite-depth float64 path."""
+import dataclasses
 import os
 
 import numpy as np
@@ -200,3 +201,65 @@ def test_finite_depth_symmetric_frequency_solve_matches_oracle(oracle_mod, defau
                                                 w, wave_directions=heads, water_depth=depth) for w in omegas]
     errs = coefficient_errors(res, ref, body.dofs)
     assert max(errs.values()) < 1e-6, errs
+
+
+def _limit_added_mass_error(res, idx, ref, dofs):
+    want = np.array([[ref["added_mass"][i][j] for j in dofs] for i in dofs])
+    floor = 1e-3 * np.abs(want).max()
+    return float(np.max(np.abs(res.added_mass[idx] - want) / np.maximum(np.abs(want), floor)))
+
+
+@pytest.mark.parametrize("precision,gate", [("fp64", 1e-7), ("mixed", 1e-5)])
+def test_limit_frequencies_in_the_frequency_sweep(oracle_mod, default_oracle_gf, tmp_path, precision, gate):
+    """omega = 0 and infinity inside a sweep of B200Engine.solve_frequencies
+    (capytaine's pytest/test_bem_zero_and_infinite_freq.py:118-155): added
+    mass against the oracle's symbolic-frequency solve, damping exactly zero,
+    NaN wave forces, and the finite frequency of the same batch unchanged; in
+    finite depth omega = infinity solves and omega = 0 raises."""
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.engine import B200Engine
+    from test_gpu_solve import coefficient_errors
+    mesh = mesh_sphere(radius=1.0, resolution=(8, 16)).immersed_part()
+    body = FloatingBody(mesh, rigid_body_dofs())
+    odofs = oracle_mod.rigid_body_dofs()
+    eng = B200Engine(green_function=_gpu_gf(default_oracle_gf, tmp_path), precision=precision, max_batch=3)
+    res = eng.solve_frequencies(body, [0.0, 1.2, np.inf])
+    for idx, omega in ((0, 0.0), (2, np.inf)):
+        ref = oracle_mod.solve_radiation_limit_frequency(default_oracle_gf, mesh, odofs, omega)
+        assert _limit_added_mass_error(res, idx, ref, list(body.dofs)) < gate, omega
+        assert np.all(res.radiation_damping[idx] == 0.0)
+        assert np.all(np.isnan(res.excitation[idx]))
+    finite = eng.solve_frequencies(body, [1.2])
+    for name in ("added_mass", "radiation_damping", "excitation"):
+        a, b = getattr(res, name)[1], getattr(finite, name)[0]
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max(), name
+    res = eng.solve_frequencies(body, [1.0, np.inf], water_depth=5.0)
+    ref = oracle_mod.solve_radiation_limit_frequency(default_oracle_gf, mesh, odofs, np.inf, water_depth=5.0)
+    assert _limit_added_mass_error(res, 1, ref, list(body.dofs)) < gate
+    assert np.all(res.radiation_damping[1] == 0.0)
+    first = dataclasses.replace(res, **{k: getattr(res, k)[:1] for k in (
+        "omegas", "added_mass", "radiation_damping", "diffraction", "froude_krylov", "excitation")})
+    ref = [oracle_mod.solve_frequency(default_oracle_gf, mesh, odofs, 1.0, water_depth=5.0)]
+    errs = coefficient_errors(first, ref, body.dofs)
+    assert max(errs.values()) < 1e-5, errs
+    with pytest.raises(NotImplementedError):
+        eng.solve_frequencies(body, [0.0], water_depth=5.0)
+
+
+def test_limit_frequencies_on_a_symmetric_mesh(oracle_mod, default_oracle_gf, tmp_path):
+    """The symmetric sweep at omega = 0 and infinity (the first block column
+    assembled by the general kernel at k = 0 and infinity) against the oracle's
+    limit solve of the merged mesh, on a mesh whose images are exact."""
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.engine import B200Engine
+    from test_symmetry_cpu import _symmetric_cases
+    mesh = _symmetric_cases(exact=True)["reflections"]
+    body = FloatingBody(mesh, rigid_body_dofs())
+    eng = B200Engine(green_function=_gpu_gf(default_oracle_gf, tmp_path), max_batch=2)
+    res = eng.solve_frequencies(body, [0.0, np.inf])
+    assert res.stats["symmetry"] == "reflections"
+    for idx, omega in ((0, 0.0), (1, np.inf)):
+        ref = oracle_mod.solve_radiation_limit_frequency(default_oracle_gf, mesh.merged(),
+                                                         oracle_mod.rigid_body_dofs(), omega)
+        assert _limit_added_mass_error(res, idx, ref, list(body.dofs)) < 1e-6, omega
+        assert np.all(res.radiation_damping[idx] == 0.0)

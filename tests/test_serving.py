@@ -213,3 +213,12 @@ def test_server_against_the_oracle(oracle_mod, default_oracle_gf, tmp_path):
         E = np.array([ref["excitation"][0.0][j] for j in body.dofs])
         assert np.max(np.abs(r.added_mass - A) / np.maximum(np.abs(A), 1e-3 * np.abs(A).max())) < 1e-5
         assert np.max(np.abs(r.excitation[0] - E) / np.maximum(np.abs(E), 1e-3 * np.abs(E).max())) < 1e-5
+
+
+def test_server_rejects_limit_frequencies_before_queueing():
+    eng = _StandInEngine()
+    with _server(eng, slots=1, memory_budget=1 << 28) as srv:
+        for omega in (0.0, np.inf, -1.0, np.nan):
+            with pytest.raises(ValueError):
+                srv.submit(_body(4), omega)
+        assert srv.counters["submitted"] == 0 and not eng.calls
