@@ -230,9 +230,10 @@ def test_limit_frequencies_in_the_frequency_sweep(oracle_mod, default_oracle_gf,
         assert np.all(res.radiation_damping[idx] == 0.0)
         assert np.all(np.isnan(res.excitation[idx]))
     finite = eng.solve_frequencies(body, [1.2])
+    same = 1e-9 if precision == "fp64" else 1e-7  # the refinement may take other iteration counts alone
     for name in ("added_mass", "radiation_damping", "excitation"):
         a, b = getattr(res, name)[1], getattr(finite, name)[0]
-        assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max(), name
+        assert np.abs(a - b).max() <= same * np.abs(b).max(), name
     res = eng.solve_frequencies(body, [1.0, np.inf], water_depth=5.0)
     ref = oracle_mod.solve_radiation_limit_frequency(default_oracle_gf, mesh, odofs, np.inf, water_depth=5.0)
     assert _limit_added_mass_error(res, 1, ref, list(body.dofs)) < gate
