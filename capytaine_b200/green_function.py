@@ -444,10 +444,14 @@ class Delhommeau:
         if sweep is not None:
             ks, s_stride, k_stride = sweep
             esize = S.element_size()
+            variants = {}  # the variant of each wavenumber (delhommeau.py:466-490): finite, 0 or infinity
             for i, k in enumerate(ks):
                 a.wavenumber = float(k)
-                if free_surface != np.inf:  # the variant of each wavenumber (delhommeau.py:466-490)
-                    a.gf_singularities = _SING[self._variant(dm2.centers_z, float(k))]
+                if free_surface != np.inf:
+                    key = a.wavenumber if a.wavenumber in (0.0, np.inf) else 1.0
+                    if key not in variants:
+                        variants[key] = _SING[self._variant(dm2.centers_z, key)]
+                    a.gf_singularities = variants[key]
                 a.S_dev = S.data_ptr() + i * int(s_stride) * esize
                 a.K_dev = K.data_ptr() + i * int(k_stride) * esize
                 _lib.check(lib.bem_assemble(a, _lib.stream_ptr(stream)))
