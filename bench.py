@@ -372,6 +372,72 @@ def run_symmetric(args):
     return 0
 
 
+def run_finite_depth(args):
+    """--workload finite_depth: the headline barge (6084 panels, 6 dofs +
+    diffraction) in 40 m of water, omega linspace(0.1, 3, 60) (k h > 0.1 at the
+    lowest frequency), one solve_frequencies call per sweep: the refined mixed
+    and the float64 engines (finite-depth assembly in float64 in both, one
+    launch per frequency with its own Prony decomposition), coefficients
+    against the oracle's finite-depth solve at omega = 1.05, which is also
+    timed on the host cores as the CPU baseline."""
+    import torch
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.engine import B200Engine
+    from capytaine_b200.green_function import Delhommeau
+    from capytaine_b200.meshes import mesh_parallelepiped
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    depth = 40.0
+    omegas = np.linspace(0.1, 3.0, 60)
+    mesh = mesh_parallelepiped(size=(80, 20, 20), resolution=(104, 26, 26)).immersed_part()
+    body = FloatingBody(mesh, rigid_body_dofs(), name="barge")
+    gf = Delhommeau(tabulation_cache_dir=None)
+    out, results = {}, {}
+    for prec in ("mixed", "fp64"):
+        eng = B200Engine(green_function=gf, precision=prec, max_batch=args.batch)
+        eng.solve_frequencies(body, omegas[:args.batch], water_depth=depth)  # warm-up
+        ms = []
+        for _ in range(max(1, args.sweeps)):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = eng.solve_frequencies(body, omegas, water_depth=depth)
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        results[prec] = res
+        t = float(np.median(ms))
+        # stage times of one batch, untimed (the stages synchronise to be read)
+        stages = eng.solve_frequencies(body, omegas[:args.batch], water_depth=depth, sync_stats=True).stats
+        out[prec] = {"value": len(omegas) / (t * 1e-3), "unit": UNIT, "ms_per_sweep": t, "sweeps": len(ms),
+                     "stage_ms_one_batch": {k: v for k, v in stages.items() if k.endswith("_ms")}}
+        eng.release()
+        del eng
+        torch.cuda.empty_cache()
+    from oracle import oracle as O
+    cores = len(os.sched_getaffinity(0))
+    gfo = oracle_gf()
+    idx = int(np.argmin(np.abs(omegas - 1.05)))
+    w = float(omegas[idx])
+    t0 = time.perf_counter()
+    ref = O.solve_frequency(gfo, mesh, O.rigid_body_dofs(), w, rho=RHO, g=G, wave_directions=(0.0,),
+                            water_depth=depth)
+    cpu_s = time.perf_counter() - t0
+    errs = {name: coefficient_error(results[name], idx, ref) for name in results}
+    line = {"metric": "freq solves/sec at N=6084 in 40 m of water (finite-depth Green function)",
+            "value": out["mixed"]["value"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "dtype": "c128 (assembly, residuals) / f32-tf32 (LU)", "data": "synthetic",
+            "config": {"workload": "barge 80x20x10m in 40 m of water, 6 dofs + diffraction (heading 0), "
+                                   "omega linspace(0.1,3,60)", "nb_panels": int(mesh.nb_faces),
+                       "water_depth": depth, "frequencies_per_batch": args.batch,
+                       "calls": "one solve_frequencies call per sweep of 60 frequencies"},
+            **out, "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
+            "max_rel_err_vs_oracle": errs, "accuracy_omega": w,
+            "cpu_baseline": {"value": 1.0 / cpu_s, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"1 finite-depth frequency-solve (omega={w:.3f}) of the barge"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------------------
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
@@ -624,11 +690,14 @@ def main():
                     help="requests of the serving run (Poisson arrivals); 0 skips it")
     ap.add_argument("--arrival-rate", type=float, default=200.0)
     ap.add_argument("--slots", type=int, default=8)
-    ap.add_argument("--workload", default="barge", choices=["barge", "array", "bodies", "symmetric"],
+    ap.add_argument("--workload", default="barge",
+                    choices=["barge", "array", "bodies", "symmetric", "finite_depth"],
                     help="array: the 3x3 cylinder array with lids (20000 panels), mixed vs float64 GMRES; "
                          "bodies: 64 bodies of 300-3000 panels batched across bodies; "
-                         "symmetric: the barge with its two symmetry planes")
-    ap.add_argument("--sweeps", type=int, default=3, help="timed sweeps per engine of --workload symmetric")
+                         "symmetric: the barge with its two symmetry planes; "
+                         "finite_depth: the barge in 40 m of water")
+    ap.add_argument("--sweeps", type=int, default=3,
+                    help="timed sweeps per engine of --workload symmetric and finite_depth")
     ap.add_argument("--bodies", type=int, default=64)
     ap.add_argument("--bodies-stats", action="store_true", help="per-stage device times of the batched sweep")
     ap.add_argument("--array-frequencies", type=int, default=40)
@@ -643,6 +712,8 @@ def main():
         return run_bodies(args)
     if args.workload == "symmetric":
         return run_symmetric(args)
+    if args.workload == "finite_depth":
+        return run_finite_depth(args)
 
     import torch
     rank = int(os.environ.get("RANK", "0"))
