@@ -30,7 +30,7 @@ extern "C" {
 #define BEM_ERR_SINGULAR 4        /* zero pivot in the LU factorisation                */
 #define BEM_ERR_NOT_CONVERGED 5   /* iterative refinement / GMRES did not converge    */
 #define BEM_ERR_OUT_OF_MEMORY 6
-#define BEM_ERR_UNSUPPORTED 7     /* option outside the implemented path (finite depth) */
+#define BEM_ERR_UNSUPPORTED 7     /* option outside the implemented path               */
 #define BEM_ERR_TIMEOUT 8         /* a bounded device-side wait gave up                */
 
 /* ---- enums (values of libDelhommeau constants.f90:40-52) ------------------ */
