@@ -1,0 +1,152 @@
+"""Host-side dispatch of Delhommeau.assemble_into on the CPU: which C-ABI entry
+point each call reaches, with which wavenumber, variant, output offset, depth,
+method and Prony decomposition.  The library is replaced by a recorder and the
+device by host memory; nothing is computed, so no GPU is needed."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from capytaine_b200 import _lib
+from capytaine_b200.meshes import mesh_sphere
+
+
+class _Recorder:
+    """Stands for the loaded library: every bem_* call is recorded with a copy
+    of its assembly arguments and returns BEM_OK."""
+
+    def __init__(self):
+        self.calls = []
+
+    def __getattr__(self, name):
+        if not name.startswith("bem_"):
+            raise AttributeError(name)
+
+        def call(*args):
+            rec = [name]
+            for a in args:
+                if isinstance(a, _lib.AssemblyArgs):
+                    rec.append({f: getattr(a, f) for f, _ in a._fields_})
+                elif hasattr(a, "_obj") and isinstance(a._obj, _lib.AssemblyArgs):  # byref
+                    rec.append({f: getattr(a._obj, f) for f, _ in a._obj._fields_})
+                else:
+                    rec.append(a.value if isinstance(a, ctypes.c_void_p) else a)
+            self.calls.append(rec)
+            return _lib.BEM_OK
+        return call
+
+
+class _Shared:
+    def __init__(self, *tensors):
+        self.tensors = tensors
+
+    def acquire(self):
+        return self
+
+
+@pytest.fixture
+def host_gf(monkeypatch):
+    import torch
+    from capytaine_b200 import green_function as G
+    rec = _Recorder()
+    monkeypatch.setattr(_lib, "require_cuda", lambda device=None: torch.device("cpu"))
+    monkeypatch.setattr(_lib, "load", lambda build_if_missing=False: rec)
+    monkeypatch.setattr(_lib, "stream_ptr", lambda stream=None: ctypes.c_void_p(0))
+    monkeypatch.setattr(_lib, "StreamShared", _Shared)
+
+    def make(**kw):
+        gf = G.Delhommeau(tabulation_cache_dir=None, **kw)
+        r = torch.linspace(0.0, 1.0, 8, dtype=torch.float64)
+        z = torch.linspace(-1.0, 0.0, 6, dtype=torch.float64)
+        table = torch.zeros((8, 6, 5), dtype=torch.float64)
+        gf._device_tabulation = lambda: (r, z, table, table.float())
+        rec.calls.clear()  # the grid spacings of the constructor
+        return gf
+    return make, rec
+
+
+def _buffers(n, nk):
+    import torch
+    S = torch.zeros((nk, n * n), dtype=torch.complex128)
+    K = torch.zeros_like(S)
+    return S, K
+
+
+def test_finite_depth_sweep_launches_once_per_wavenumber(host_gf):
+    make, rec = host_gf
+    gf = make()
+    mesh = mesh_sphere(resolution=(4, 6)).immersed_part()
+    n = mesh.nb_faces
+    ks = [0.3, 0.9, np.inf]
+    S, K = _buffers(n, len(ks))
+    gf.assemble_into(mesh, mesh, S[0], K[0], water_depth=4.0, wavenumber=ks[0], sweep=(ks, n * n, n * n))
+    calls = [c for c in rec.calls if c[0] == "bem_assemble_finite_depth"]
+    assert len(calls) == len(ks) and len(calls) == len(rec.calls)
+    for i, (name, a, depth, method, prony_ptr, nexp, stream) in enumerate(calls):
+        assert a["wavenumber"] == ks[i] and depth == 4.0 and method == 1
+        assert a["S_dev"] == S.data_ptr() + 16 * i * n * n and a["K_dev"] == K.data_ptr() + 16 * i * n * n
+        assert nexp == gf.find_best_exponential_decomposition(ks[i] * 4.0).shape[1]
+        # low_freq for finite k, high_freq at k = infinity (delhommeau.py:466-490)
+        want = _lib.BEM_GF_HIGH_FREQ if ks[i] == np.inf else _lib.BEM_GF_LOW_FREQ
+        assert a["gf_singularities"] == want
+        assert (a["nr"] > 0) == (0 < ks[i] < np.inf)  # the table only where there is a wave term
+        assert a["early_dot_product"] == 1 and a["precision"] == _lib.BEM_PREC_FP64
+
+
+def test_finite_depth_legacy_method_forces_low_freq(host_gf):
+    make, rec = host_gf
+    gf = make(finite_depth_method="legacy", gf_singularities="high_freq")
+    mesh = mesh_sphere(resolution=(4, 6)).immersed_part()
+    S, K = _buffers(mesh.nb_faces, 1)
+    for k in (0.5, np.inf):
+        gf.assemble_into(mesh, mesh, S[0], K[0], water_depth=3.0, wavenumber=k)
+    assert [c[3] for c in rec.calls] == [0, 0]  # method 0: legacy
+    assert [c[1]["gf_singularities"] for c in rec.calls] == [_lib.BEM_GF_LOW_FREQ] * 2
+
+
+def test_finite_depth_rejects_what_the_kernel_does_not_cover(host_gf):
+    import torch
+    make, rec = host_gf
+    gf = make()
+    mesh = mesh_sphere(resolution=(4, 6)).immersed_part()
+    n = mesh.nb_faces
+    S = torch.zeros((n, n), dtype=torch.complex64)
+    with pytest.raises(NotImplementedError):
+        gf.assemble_into(mesh, mesh, S, S.clone(), water_depth=3.0, wavenumber=1.0)
+    S, K = _buffers(n, 1)
+    with pytest.raises(NotImplementedError):
+        gf.assemble_into(mesh, mesh, S[0], K[0], water_depth=3.0, wavenumber=1.0, early_dot_product=False)
+    with pytest.raises(NotImplementedError):  # no Prony decomposition at k h = 0
+        gf.assemble_into(mesh, mesh, S[0], K[0], water_depth=3.0, wavenumber=0.0)
+    assert not rec.calls
+
+
+def test_infinite_depth_sweep_with_limit_wavenumbers_takes_the_general_kernel(host_gf):
+    make, rec = host_gf
+    gf = make(gf_singularities="high_freq")
+    mesh = mesh_sphere(resolution=(4, 6)).immersed_part()
+    n = mesh.nb_faces
+    ks = [0.0, 0.7, np.inf]
+    S, K = _buffers(n, len(ks))
+    gf.assemble_into(mesh, mesh, S[0], K[0], wavenumber=ks[0], sweep=(ks, n * n, n * n))
+    assert [c[0] for c in rec.calls] == ["bem_assemble"] * 3
+    args = [c[1] for c in rec.calls]
+    assert [a["wavenumber"] for a in args] == ks
+    # the variant of each wavenumber, not of the first one
+    assert [a["gf_singularities"] for a in args] == [_lib.BEM_GF_LOW_FREQ, _lib.BEM_GF_HIGH_FREQ,
+                                                     _lib.BEM_GF_HIGH_FREQ]
+    assert all(a["nr"] > 0 for a in args)  # one finite wavenumber needs the table
+    assert [a["S_dev"] - S.data_ptr() for a in args] == [16 * i * n * n for i in range(3)]
+
+
+def test_infinite_depth_sweep_of_finite_wavenumbers_is_one_batched_launch(host_gf):
+    make, rec = host_gf
+    gf = make()
+    mesh = mesh_sphere(resolution=(4, 6)).immersed_part()
+    n = mesh.nb_faces
+    ks = [0.2, 0.7, 1.9]
+    S, K = _buffers(n, len(ks))
+    gf.assemble_into(mesh, mesh, S[0], K[0], wavenumber=ks[0], sweep=(ks, n * n, n * n))
+    names = [c[0] for c in rec.calls]
+    assert names == ["bem_assemble_rankine_part", "bem_assemble_wave_symmetric_batched"]
+    assert rec.calls[1][5] == len(ks)
