@@ -150,3 +150,79 @@ def test_infinite_depth_sweep_of_finite_wavenumbers_is_one_batched_launch(host_g
     names = [c[0] for c in rec.calls]
     assert names == ["bem_assemble_rankine_part", "bem_assemble_wave_symmetric_batched"]
     assert rec.calls[1][5] == len(ks)
+
+
+def _doubles(ptr, n):
+    return np.array((ctypes.c_double * n).from_address(ptr))
+
+
+class _ReadingRecorder(_Recorder):
+    """Also reads, at call time, the per-frequency arrays the right-hand-side and
+    force entry points receive (host memory here)."""
+
+    def __getattr__(self, name):
+        call = super().__getattr__(name)
+
+        def reading(*args):
+            call(*args)
+            rec = self.calls[-1]
+            if name == "bem_build_rhs":     # (n, batch, omega, k, g, depth, ...)
+                rec.append({"omega": _doubles(rec[3], rec[2]), "k": _doubles(rec[4], rec[2]), "depth": rec[6]})
+            elif name == "bem_integrate_pressure":  # (n, batch, nrhs, ndof, phi, ldp, strideP, omega, ...)
+                rec.append({"omega": _doubles(rec[8], rec[2])})
+            elif name == "bem_froude_krylov":  # (n, batch, ndof, nhead, k, rho, g, depth, ...)
+                rec.append({"k": _doubles(rec[5], rec[2]), "depth": rec[8]})
+            return _lib.BEM_OK
+        return reading
+
+
+@pytest.fixture
+def host_engine(host_gf, monkeypatch):
+    from capytaine_b200.engine import B200Engine
+    make, _ = host_gf
+    rec = _ReadingRecorder()
+    monkeypatch.setattr(_lib, "load", lambda build_if_missing=False: rec)
+    return (lambda **kw: B200Engine(green_function=make(), **kw)), rec
+
+
+def test_engine_limit_frequencies_use_omega_one_and_zero_wave(host_engine):
+    """solve_frequencies at omega = 0, finite and infinity: the matrices at k = 0,
+    omega^2/g and infinity; the right-hand sides and pressures with omega = 1 at
+    the limits and the incident wave switched off there (k = 0); zero damping
+    and NaN wave forces reported at the limits."""
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    new_engine, rec = host_engine
+    body = FloatingBody(mesh_sphere(resolution=(4, 6)).immersed_part(), rigid_body_dofs(only=["Heave"]))
+    res = new_engine().solve_frequencies(body, [0.0, 1.2, np.inf])
+    k = 1.2 ** 2 / 9.81
+    assembled = [c[1]["wavenumber"] for c in rec.calls if c[0] == "bem_assemble"] + \
+        [c[1]["wavenumber"] for c in rec.calls if c[0] == "bem_assemble_wave_symmetric"]
+    assert sorted(assembled) == [0.0, k, np.inf]
+    rhs, = [c[-1] for c in rec.calls if c[0] == "bem_build_rhs"]
+    np.testing.assert_array_equal(rhs["omega"], [1.0, 1.2, 1.0])
+    np.testing.assert_array_equal(rhs["k"], [0.0, k, 0.0])
+    assert rhs["depth"] == np.inf
+    pres, = [c[-1] for c in rec.calls if c[0] == "bem_integrate_pressure"]
+    np.testing.assert_array_equal(pres["omega"], [1.0, 1.2, 1.0])
+    assert np.all(res.radiation_damping[[0, 2]] == 0.0)
+    assert np.all(np.isnan(res.excitation[[0, 2]])) and not np.any(np.isnan(res.excitation[1]))
+
+
+def test_engine_finite_depth_passes_the_depth_and_its_wavenumbers(host_engine):
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.engine import wavenumbers
+    new_engine, rec = host_engine
+    body = FloatingBody(mesh_sphere(resolution=(4, 6)).immersed_part(), rigid_body_dofs(only=["Surge", "Heave"]))
+    omegas = [0.8, 2.0, np.inf]
+    new_engine(precision="mixed").solve_frequencies(body, omegas, water_depth=5.0)
+    ks = wavenumbers(omegas, 5.0)
+    fd = [c for c in rec.calls if c[0] == "bem_assemble_finite_depth"]
+    assert [c[1]["wavenumber"] for c in fd] == list(ks) and all(c[2] == 5.0 for c in fd)
+    assert all(c[1]["precision"] == _lib.BEM_PREC_FP64 for c in fd)  # float64 assembly in finite depth
+    rhs, = [c[-1] for c in rec.calls if c[0] == "bem_build_rhs"]
+    np.testing.assert_array_equal(rhs["k"], [ks[0], ks[1], 0.0])
+    assert rhs["depth"] == 5.0
+    fk, = [c[-1] for c in rec.calls if c[0] == "bem_froude_krylov"]
+    np.testing.assert_array_equal(fk["k"], [ks[0], ks[1], 0.0])
+    assert fk["depth"] == 5.0
+    np.testing.assert_allclose(9.81 * ks[:2] * np.tanh(ks[:2] * 5.0), np.square(omegas[:2]), rtol=1e-14)
