@@ -226,3 +226,35 @@ def test_engine_finite_depth_passes_the_depth_and_its_wavenumbers(host_engine):
     np.testing.assert_array_equal(fk["k"], [ks[0], ks[1], 0.0])
     assert fk["depth"] == 5.0
     np.testing.assert_allclose(9.81 * ks[:2] * np.tanh(ks[:2] * 5.0), np.square(omegas[:2]), rtol=1e-14)
+
+
+def test_symmetric_engine_first_block_column_in_finite_depth_and_at_limits(host_engine):
+    """Meshes with symmetries: the first block column (all N points against the
+    n_sub panels of the reference sub-mesh) assembled per wavenumber by the
+    finite-depth kernel, or by the general kernel when a limit frequency is in
+    the sweep, each into its own N x n_sub slot."""
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.meshes import mesh_parallelepiped
+    from capytaine_b200.symmetry import block_structure
+    new_engine, rec = host_engine
+    mesh = mesh_parallelepiped(size=(6, 4, 4), resolution=(4, 4, 4), reflection_symmetry=True).immersed_part()
+    st = block_structure(mesh)
+    N = mesh.nb_faces
+    body = FloatingBody(mesh, rigid_body_dofs(only=["Heave"]))
+    eng = new_engine()
+    for depth, omegas, entry in ((5.0, [0.7, np.inf], "bem_assemble_finite_depth"),
+                                 (np.inf, [0.0, 1.0], "bem_assemble")):
+        rec.calls.clear()
+        res = eng.solve_frequencies(body, omegas, water_depth=depth)
+        assert res.stats["symmetry"] == "reflections"
+        calls = [c for c in rec.calls if c[0] == entry]
+        assert len(calls) == 2
+        base = calls[0][1]["S_dev"]
+        for i, c in enumerate(calls):
+            a = c[1]
+            assert a["n"] == N and a["nb_faces"] == st.n_sub and a["lds"] == N and a["ldk"] == N
+            assert a["S_dev"] - base == 16 * i * N * st.n_sub
+        assert not any(c[0] in ("bem_assemble_wave_cached", "bem_assemble_rankine_part") for c in rec.calls)
+        rhs, = [c[-1] for c in rec.calls if c[0] == "bem_build_rhs"]
+        assert rhs["depth"] == depth
+        assert np.all(res.radiation_damping[np.isinf(omegas) | (np.asarray(omegas) == 0)] == 0.0)
