@@ -768,8 +768,11 @@ __device__ void wave_term(const double x[3], const double c[3], const bem_assemb
 // infinite-depth Rankine terms, the Rankine images through the sea bottom
 // (matrices.f90:212-268), the four wave terms of Green_wave.f90:311-425 and the
 // Prony terms of Green_wave.f90:427-508.  One thread per collocation point,
-// the panels of a tile in shared memory; float64, complex128 outputs, K with
-// the dot product taken.  prony: rates then amplitudes (2 x nexp).
+// the panels of a tile in shared memory; every term in float64, outputs Out
+// (complex128 or complex64), K with the dot product taken or the three
+// gradient planes, as the general kernel.  prony: rates then amplitudes
+// (2 x nexp).
+template <class Out>
 __global__ void __launch_bounds__(kRows) assemble_finite_depth_kernel(const bem_assembly_args a, TabView T,
                                                                       double depth, int legacy,
                                                                       const double* __restrict__ prony, int nexp,
@@ -826,8 +829,8 @@ __global__ void __launch_bounds__(kRows) assemble_finite_depth_kernel(const bem_
     const double akh = amh * tanh(amh);
     A = (amh + akh) * (amh + akh) / (4 * amh * (amh * amh - akh * akh + akh));
   }
-  double2* S = reinterpret_cast<double2*>(a.S_dev);
-  double2* K = reinterpret_cast<double2*>(a.K_dev);
+  Out* S = reinterpret_cast<Out*>(a.S_dev);
+  Out* K = reinterpret_cast<Out*>(a.K_dev);
   bool nan_seen = false;
   for (int jj = 0; jj < nJ; ++jj) {
     const FaceRec& f = faces[jj];
@@ -922,14 +925,28 @@ __global__ void __launch_bounds__(kRows) assemble_finite_depth_kernel(const bem_
         dGre[2] += amp / 2 * dg[2];
       }
     }
-    const double* dn = adjoint ? nI : (a.dot_normals_dev + 3 * J);
     const double sre = kMinusOneOverFourPi * Gre, sim = kMinusOneOverFourPi * Gim;
-    double kre = kMinusOneOverFourPi * (dn[0] * dGre[0] + dn[1] * dGre[1] + dn[2] * dGre[2]);
-    const double kim = kMinusOneOverFourPi * (dn[0] * dGim[0] + dn[1] * dGim[1] + dn[2] * dGim[2]);
-    if (a.diagonal_term && I == J && I < diag_limit) kre += diag_coef;
-    S[(size_t)I + (size_t)a.lds * J] = make_double2(sre, sim);
-    K[(size_t)I + (size_t)a.ldk * J] = make_double2(kre, kim);
-    nan_seen |= isnan(sre) || isnan(sim) || isnan(kre) || isnan(kim);
+    S[(size_t)I + (size_t)a.lds * J] = OutT<Out>::make(sre, sim);
+    nan_seen |= isnan(sre) || isnan(sim);
+    const bool on_diag = a.diagonal_term && I == J && I < diag_limit;
+    const size_t kidx = (size_t)I + (size_t)a.ldk * J;
+    if (a.early_dot_product) {
+      const double* dn = adjoint ? nI : (a.dot_normals_dev + 3 * J);
+      double kre = kMinusOneOverFourPi * (dn[0] * dGre[0] + dn[1] * dGre[1] + dn[2] * dGre[2]);
+      const double kim = kMinusOneOverFourPi * (dn[0] * dGim[0] + dn[1] * dGim[1] + dn[2] * dGim[2]);
+      if (on_diag) kre += diag_coef;
+      K[kidx] = OutT<Out>::make(kre, kim);
+      nan_seen |= isnan(kre) || isnan(kim);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double kre = kMinusOneOverFourPi * dGre[c];
+        const double kim = kMinusOneOverFourPi * dGim[c];
+        if (on_diag) kre += diag_coef * a.dot_normals_dev[3 * I + c];
+        K[kidx + (size_t)c * a.k_plane_stride] = OutT<Out>::make(kre, kim);
+        nan_seen |= isnan(kre) || isnan(kim);
+      }
+    }
   }
   if (nan_seen && a.nan_flag_dev) atomicOr(a.nan_flag_dev, 1);
 }
@@ -1189,11 +1206,14 @@ extern "C" int bem_assemble_finite_depth(const bem_assembly_args* args, double d
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: 0 to 64 Prony terms");
   if (method != 0 && method != 1)
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: method 0 (legacy) or 1 (newer)");
-  if (!a.early_dot_product || a.out_dtype != BEM_DTYPE_C128 || a.precision != BEM_PREC_FP64)
-    return set_error(BEM_ERR_UNSUPPORTED,
-                     "bem_assemble_finite_depth: early dot product, complex128 outputs and float64 only");
+  if (a.precision != BEM_PREC_FP64)
+    return set_error(BEM_ERR_UNSUPPORTED, "bem_assemble_finite_depth: float64 arithmetic only");
+  if (a.out_dtype != BEM_DTYPE_C128 && a.out_dtype != BEM_DTYPE_C64)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: unknown out_dtype");
   if (a.nb_quad_points < 1 || a.lds < a.n || a.ldk < a.n)
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: quadrature or leading dimension");
+  if (!a.early_dot_product && a.k_plane_stride < a.ldk * (int64_t)a.nb_faces)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: gradient planes overlap");
   if (!(a.wavenumber >= 0.0))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: wavenumber must be >= 0");
   const bool tabulated = a.nr > 1 && a.nz > 1;
@@ -1213,7 +1233,12 @@ extern "C" int bem_assemble_finite_depth(const bem_assembly_args* args, double d
   cudaStream_t s = (cudaStream_t)stream;
   {
     TimedLaunch tl(kKAssemble, s);
-    assemble_finite_depth_kernel<<<grid, kRows, 0, s>>>(a, T, depth, method == 0 ? 1 : 0, prony_dev, nexp, gf_sing);
+    if (a.out_dtype == BEM_DTYPE_C128)
+      assemble_finite_depth_kernel<double2><<<grid, kRows, 0, s>>>(a, T, depth, method == 0 ? 1 : 0, prony_dev, nexp,
+                                                                   gf_sing);
+    else
+      assemble_finite_depth_kernel<float2><<<grid, kRows, 0, s>>>(a, T, depth, method == 0 ? 1 : 0, prony_dev, nexp,
+                                                                  gf_sing);
   }
   count_launches(1);
   BEM_CUDA_CHECK(cudaGetLastError());

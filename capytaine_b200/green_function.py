@@ -339,8 +339,8 @@ class Delhommeau:
                                                wavenumber=wavenumber, adjoint_double_layer=adjoint_double_layer,
                                                early_dot_product=early_dot_product,
                                                diagonal_term_in_double_layer=diagonal_term_in_double_layer,
-                                               lds=lds, ldk=ldk, precision=precision, stream=stream,
-                                               nan_flag=nan_flag, sweep=sweep)
+                                               lds=lds, ldk=ldk, k_plane_stride=k_plane_stride,
+                                               precision=precision, stream=stream, nan_flag=nan_flag, sweep=sweep)
         pts, nrm = self._collocation(mesh1, mesh2, adjoint_double_layer)
         dm2 = self.device_mesh(mesh2)
         n = pts.shape[0]
@@ -460,13 +460,14 @@ class Delhommeau:
 
     def _assemble_finite_depth(self, mesh1, mesh2, S, K, *, free_surface, water_depth, wavenumber,
                                adjoint_double_layer, early_dot_product, diagonal_term_in_double_layer, lds, ldk,
-                               precision, stream, nan_flag, sweep=None):
+                               k_plane_stride=None, precision=None, stream=None, nan_flag=None, sweep=None):
         """S and K in water of finite depth by Delhommeau's method
         (matrices.f90:197-305) through bem_assemble_finite_depth, with the Prony
         decomposition of find_best_exponential_decomposition(k h) and the
         variant rules of delhommeau.py:467-487 (the legacy method uses low_freq).
-        float64, complex128 outputs, K with the dot product taken; a sweep is
-        one launch per wavenumber (each has its own decomposition)."""
+        Every term in float64; complex128 or complex64 outputs; K with the dot
+        product taken or the three gradient planes; a sweep is one launch per
+        wavenumber (each has its own decomposition)."""
         todo = [(float(wavenumber), 0, 0)]
         if sweep is not None:
             ks, s_stride, k_stride = sweep
@@ -477,19 +478,20 @@ class Delhommeau:
                                             adjoint_double_layer=adjoint_double_layer,
                                             early_dot_product=early_dot_product,
                                             diagonal_term_in_double_layer=diagonal_term_in_double_layer, lds=lds,
-                                            ldk=ldk, precision=precision, stream=stream, nan_flag=nan_flag)
+                                            ldk=ldk, k_plane_stride=k_plane_stride, stream=stream,
+                                            nan_flag=nan_flag)
 
     def _assemble_finite_depth_one(self, mesh1, mesh2, S, K, s_offset, k_offset, *, free_surface, water_depth,
                                    wavenumber, adjoint_double_layer, early_dot_product,
-                                   diagonal_term_in_double_layer, lds, ldk, precision, stream, nan_flag):
+                                   diagonal_term_in_double_layer, lds, ldk, k_plane_stride, stream, nan_flag):
         """One wavenumber of _assemble_finite_depth, S and K written s_offset and
         k_offset elements after the start of their buffers.  Every term in
-        float64, whatever `precision` asks (there is no mixed-precision
+        float64, whatever precision was asked (there is no mixed-precision
         finite-depth kernel)."""
         import torch
-        if S.dtype != torch.complex128 or K.dtype != torch.complex128 or not early_dot_product:
-            raise NotImplementedError("finite depth on the device: complex128 outputs and the dot product taken "
-                                      "(early_dot_product=True) only")
+        dtypes = {torch.complex128: _lib.BEM_DTYPE_C128, torch.complex64: _lib.BEM_DTYPE_C64}
+        if S.dtype not in dtypes or K.dtype != S.dtype:
+            raise TypeError(f"unsupported output dtypes {S.dtype}, {K.dtype}")
         pts, nrm = self._collocation(mesh1, mesh2, adjoint_double_layer)
         dm2 = self.device_mesh(mesh2)
         n = pts.shape[0]
@@ -524,11 +526,12 @@ class Delhommeau:
             table_dev=table.data_ptr() if table is not None else 0,
             table32_dev=table32.data_ptr() if table32 is not None else 0,
             wavenumber=k, free_surface=float(free_surface), gf_singularities=_SING[sing],
-            adjoint_double_layer=int(bool(adjoint_double_layer)), early_dot_product=1,
+            adjoint_double_layer=int(bool(adjoint_double_layer)), early_dot_product=int(bool(early_dot_product)),
             diagonal_term=int(bool(diagonal_term_in_double_layer)), precision=_lib.BEM_PREC_FP64,
-            out_dtype=_lib.BEM_DTYPE_C128, S_dev=S.data_ptr() + s_offset * S.element_size(),
+            out_dtype=dtypes[S.dtype], S_dev=S.data_ptr() + s_offset * S.element_size(),
             K_dev=K.data_ptr() + k_offset * K.element_size(),
-            lds=lds if lds is not None else n, ldk=ldk if ldk is not None else n, k_plane_stride=0,
+            lds=lds if lds is not None else n, ldk=ldk if ldk is not None else n,
+            k_plane_stride=k_plane_stride if k_plane_stride is not None else 0,
             nan_flag_dev=nan_flag.data_ptr() if nan_flag is not None else 0,
         )
         _lib.check(_lib.load().bem_assemble_finite_depth(a, float(water_depth),

@@ -173,8 +173,11 @@ int bem_assemble_symmetric(const bem_assembly_args* args, void* stream);
  * images through the bottom (scaled by Delhommeau's factor), and four Rankine
  * images per exponential of the Prony decomposition prony_dev (device, 2 x nexp
  * float64: growth rates, then amplitudes; nexp <= 64).  method: 0 = legacy
- * (one-point free-surface image), 1 = newer.  float64, complex128 outputs, K
- * with the dot product taken.  Replaces the finite-depth branch of
+ * (one-point free-surface image), 1 = newer.  args->precision must be
+ * BEM_PREC_FP64 (every term in float64); complex128 or complex64 outputs; K
+ * with the dot product taken or the three gradient planes, as bem_assemble.
+ * The variant args->gf_singularities is used as given (the caller applies
+ * delhommeau.py:467-487).  Replaces the finite-depth branch of
  * matrices::build_matrices (libs/libDelhommeau/src/matrices.f90:197-305,
  * Green_wave.f90:311-508), called from delhommeau.py:492-515. */
 int bem_assemble_finite_depth(const bem_assembly_args* args, double depth, int method, const double* prony_dev,

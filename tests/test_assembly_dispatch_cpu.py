@@ -104,20 +104,31 @@ def test_finite_depth_legacy_method_forces_low_freq(host_gf):
     assert [c[1]["gf_singularities"] for c in rec.calls] == [_lib.BEM_GF_LOW_FREQ] * 2
 
 
-def test_finite_depth_rejects_what_the_kernel_does_not_cover(host_gf):
+def test_finite_depth_output_formats(host_gf):
+    """complex64 outputs and the three gradient planes reach the finite-depth
+    entry point with their flags; mismatched dtypes and k h = 0 are refused on
+    the host (no Prony decomposition at k h = 0, as capytaine)."""
     import torch
     make, rec = host_gf
-    gf = make()
+    gf = make(gf_singularities="high_freq")
     mesh = mesh_sphere(resolution=(4, 6)).immersed_part()
     n = mesh.nb_faces
     S = torch.zeros((n, n), dtype=torch.complex64)
+    gf.assemble_into(mesh, mesh, S, S.clone(), water_depth=3.0, wavenumber=1.0)
+    K3 = torch.zeros((3, n, n), dtype=torch.complex128)
+    S2 = torch.zeros((n, n), dtype=torch.complex128)
+    gf.assemble_into(mesh, mesh, S2, K3, water_depth=3.0, wavenumber=1.0, early_dot_product=False,
+                     k_plane_stride=n * n, adjoint_double_layer=False)
+    (_, a64, *_), (_, a3, *_) = rec.calls
+    assert a64["out_dtype"] == _lib.BEM_DTYPE_C64 and a64["early_dot_product"] == 1
+    assert a3["out_dtype"] == _lib.BEM_DTYPE_C128 and a3["early_dot_product"] == 0
+    assert a3["k_plane_stride"] == n * n and a3["adjoint_double_layer"] == 0
+    assert a64["gf_singularities"] == a3["gf_singularities"] == _lib.BEM_GF_HIGH_FREQ
+    rec.calls.clear()
+    with pytest.raises(TypeError):
+        gf.assemble_into(mesh, mesh, S, S2, water_depth=3.0, wavenumber=1.0)
     with pytest.raises(NotImplementedError):
-        gf.assemble_into(mesh, mesh, S, S.clone(), water_depth=3.0, wavenumber=1.0)
-    S, K = _buffers(n, 1)
-    with pytest.raises(NotImplementedError):
-        gf.assemble_into(mesh, mesh, S[0], K[0], water_depth=3.0, wavenumber=1.0, early_dot_product=False)
-    with pytest.raises(NotImplementedError):  # no Prony decomposition at k h = 0
-        gf.assemble_into(mesh, mesh, S[0], K[0], water_depth=3.0, wavenumber=0.0)
+        gf.assemble_into(mesh, mesh, S2, S2.clone(), water_depth=3.0, wavenumber=0.0)
     assert not rec.calls
 
 

@@ -47,6 +47,9 @@ CASES = {
     "deep_water_large_kh": (lambda: _hemisphere(), 20.0, 2.0, "newer", "low_freq", {}),
     "no_diagonal_term": (lambda: _hemisphere(), 5.0, 1.0, "newer", "low_freq",
                          dict(diagonal_term_in_double_layer=False)),
+    "full_gradient": (lambda: _hemisphere(), 5.0, 1.0, "newer", "low_freq", dict(early_dot_product=False)),
+    "direct_full_gradient": (lambda: _hemisphere(), 3.0, 0.7, "newer", "high_freq",
+                             dict(early_dot_product=False, adjoint_double_layer=False)),
 }
 
 
@@ -63,6 +66,22 @@ def test_finite_depth_assembly_matches_oracle(oracle_mod, default_oracle_gf, tmp
     assert S.dtype == np.complex128 and K.dtype == np.complex128
     _close(S, S_ref, FP64_RTOL)
     _close(K, K_ref, FP64_RTOL)
+
+
+def test_finite_depth_complex64_outputs(oracle_mod, default_oracle_gf, tmp_path):
+    """floating_point_precision="float32": complex64 outputs of the same
+    float64 arithmetic, within float32 rounding of the oracle's entries."""
+    mesh = _hemisphere()
+    depth, k = 4.0, 1.3
+    gf = _gpu_gf(default_oracle_gf, tmp_path, floating_point_precision="float32")
+    decomposition = gf.find_best_exponential_decomposition(k * depth)
+    for kw in ({}, dict(early_dot_product=False)):
+        S_ref, K_ref = default_oracle_gf.evaluate(mesh, mesh, wavenumber=k, water_depth=depth,
+                                                  prony=decomposition, **kw)
+        S, K = gf.evaluate(mesh, mesh, wavenumber=k, water_depth=depth, **kw)
+        assert S.dtype == np.complex64 and K.dtype == np.complex64
+        _close(S, S_ref, 1e-6)
+        _close(K, K_ref, 1e-6)
 
 
 def test_finite_depth_free_surface_panels_and_points(oracle_mod, default_oracle_gf, tmp_path):

@@ -148,11 +148,15 @@ def test_finite_depth_assembly_preconditions_checked_on_host(lib):
     a.free_surface = float("inf")
     assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == bad
     a.free_surface = 0.0
-    a.out_dtype = _lib.BEM_DTYPE_C64
-    assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == unsupported
+    a.out_dtype = 7
+    assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == bad
     a.out_dtype = _lib.BEM_DTYPE_C128
-    a.early_dot_product = 0
+    a.precision = _lib.BEM_PREC_MIXED
     assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == unsupported
+    a.precision = _lib.BEM_PREC_FP64
+    a.early_dot_product = 0
+    a.k_plane_stride = 12 * 12 - 1  # gradient planes overlap
+    assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == bad
     a.early_dot_product = 1
     a.ldk = 11
     assert lib.bem_assemble_finite_depth(a, 10.0, 1, fake, 4, None) == bad
