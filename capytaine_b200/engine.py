@@ -725,7 +725,7 @@ class B200Engine:
 
     # ---- many bodies --------------------------------------------------------
     def solve_bodies(self, bodies, omegas: Sequence[float], *, wave_directions: Sequence[float] = (0.0,),
-                     rho: float = 1000.0, g: float = 9.81, batch_bytes: float = 8e9,
+                     rho: float = 1000.0, g: float = 9.81, water_depth: float = np.inf, batch_bytes: float = 8e9,
                      sync_stats: bool = False) -> List[FrequencyResults]:
         """Frequency sweeps of many bodies of uneven panel counts, batched
         across bodies: bodies whose size rounds up to the same multiple of the
@@ -737,12 +737,15 @@ class B200Engine:
         (what solve_frequencies returns for that body).  With max_batch or more
         frequencies a body fills batches of its own: each body then runs its
         own sweep (measured faster: no padding, and a frequency that needs the
-        GMRES fallback holds up its own batch only)."""
+        GMRES fallback holds up its own batch only).  water_depth as in
+        solve_frequencies."""
         import torch
+        if not water_depth > 0:
+            raise ValueError(f"water_depth must be > 0 (got {water_depth})")
         omegas = np.asarray(omegas, dtype=float)
         if len(omegas) >= self.max_batch:
-            return [self.solve_frequencies(b, omegas, wave_directions=wave_directions, rho=rho, g=g)
-                    for b in bodies]
+            return [self.solve_frequencies(b, omegas, wave_directions=wave_directions, rho=rho, g=g,
+                                           water_depth=water_depth) for b in bodies]
         heads = np.asarray(wave_directions, dtype=float)
         nhead = len(heads)
         blk = 128 if self.precision == "mixed" else 64
@@ -785,7 +788,8 @@ class B200Engine:
                 r.flags.zero_()
                 for body, j0, m in segments:
                     mesh = body.mesh_including_lid
-                    self.assemble_stage(f, mesh, om[j0:j0 + m] ** 2 / g, nan_flag=r.nan, first=j0, lds=npad)
+                    self.assemble_stage(f, mesh, wavenumbers(om[j0:j0 + m], water_depth, g), nan_flag=r.nan,
+                                        first=j0, lds=npad, water_depth=water_depth)
                     if mesh.nb_faces < npad:
                         for M in (f.S, f.K):  # zero rows/columns, unit diagonal beyond the body's panels
                             _lib.check(lib.bem_zpad_identity(_vp(M.data_ptr() + 16 * j0 * npad * npad), npad,
@@ -796,7 +800,7 @@ class B200Engine:
                 if ev:
                     ev[2].record()
                 out = self._solve_segments(f, r, [tuple(sg) for sg in segments], om, heads, rho=rho, g=g,
-                                           stats=stats, events=ev)
+                                           stats=stats, events=ev, water_depth=water_depth)
                 for (body, j0, m), (F, FK) in zip(segments, out):
                     i = chunk[j0][0]
                     qs = [q for _, q in chunk[j0:j0 + m]]

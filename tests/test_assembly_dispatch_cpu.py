@@ -269,3 +269,25 @@ def test_symmetric_engine_first_block_column_in_finite_depth_and_at_limits(host_
         rhs, = [c[-1] for c in rec.calls if c[0] == "bem_build_rhs"]
         assert rhs["depth"] == depth
         assert np.all(res.radiation_damping[np.isinf(omegas) | (np.asarray(omegas) == 0)] == 0.0)
+
+
+def test_solve_bodies_in_finite_depth(host_engine):
+    """solve_bodies batched across bodies of two padded sizes in finite depth:
+    one finite-depth launch per (body, omega) into the padded slot of its
+    group, and the depth on the right-hand sides of every batch."""
+    from capytaine_b200.bodies import FloatingBody, rigid_body_dofs
+    from capytaine_b200.engine import padded_size, wavenumbers
+    new_engine, rec = host_engine
+    bodies = [FloatingBody(mesh_sphere(resolution=res).immersed_part(), rigid_body_dofs(only=["Heave"]))
+              for res in ((4, 6), (10, 16))]
+    omegas = [0.9, 1.6]
+    new_engine(max_batch=8).solve_bodies(bodies, omegas, water_depth=6.0)
+    fd = [c[1] for c in rec.calls if c[0] == "bem_assemble_finite_depth"]
+    assert len(fd) == len(bodies) * len(omegas)
+    for body in bodies:
+        n = body.mesh.nb_faces
+        mine = [a for a in fd if a["nb_faces"] == n]
+        assert [a["wavenumber"] for a in mine] == list(wavenumbers(omegas, 6.0))
+        assert all(a["lds"] == padded_size(n) for a in mine)
+    rhs = [c[-1] for c in rec.calls if c[0] == "bem_build_rhs"]
+    assert rhs and all(r["depth"] == 6.0 for r in rhs)
