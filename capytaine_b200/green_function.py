@@ -135,6 +135,8 @@ class Delhommeau:
         # then the wave term once per pair of faces (False: the general kernel).
         self.symmetric_assembly = True
         self._rankine_cache: "OrderedDict[tuple, object]" = OrderedDict()
+        # Prony decompositions by k h (128 most recent)
+        self._prony_cache: "OrderedDict[float, np.ndarray]" = OrderedDict()
         self.exportable_settings = {
             "green_function": self.__class__.__name__,
             "tabulation_nr": tabulation_nr,
@@ -171,8 +173,8 @@ class Delhommeau:
             raise ValueError(f"Unrecognized name for the Prony decomposition method: {method!r}. "
                              "Expected 'python' or 'fortran'.")
         kh = float(dimensionless_wavenumber)
+        cache = self._prony_cache
         with self._lock:
-            cache = self.__dict__.setdefault("_prony_cache", OrderedDict())
             hit = cache.get(kh)
         if hit is None:
             try:
