@@ -1,8 +1,17 @@
-"""Parity of the finite-depth assembly kernel (bem_assemble_finite_depth,
-Delhommeau's method of matrices.f90:197-305 and Green_wave.f90:311-508) with
-the CPU oracle.  Both sides take the same tabulation (through the cache file)
-and the same Prony decomposition, so only floating-point rounding is left:
-1e-10 relative to the largest entry, as the infinite-depth float64 path."""
+"""Finite depth and limit frequencies on the device against the CPU oracle.
+
+* The finite-depth assembly kernel (bem_assemble_finite_depth, Delhommeau's
+  method of matrices.f90:197-305 and Green_wave.f90:311-508): both sides take
+  the same tabulation (through the cache file) and the same Prony
+  decomposition, so only floating-point rounding is left: 1e-10 relative to
+  the largest entry, as the infinite-depth float64 path (1e-6 for complex64
+  outputs).
+* Finite-depth solves: through capytaine's MatrixEngine seam, and through
+  B200Engine.solve_frequencies (dense and symmetric meshes, float64 and mixed
+  engines) with the finite-depth Airy right-hand sides, at the gates of the
+  frequency-solve metric.
+* omega = 0 and infinity inside frequency sweeps, against the oracle's
+  symbolic-frequency radiation solve."""
 import dataclasses
 import os
 
