@@ -543,9 +543,8 @@ def fp64_tensor_peak_tflops():
 
 # DRAM bytes per algorithmic flop of the trailing-update GEMM, from one ncu
 # capture of a full trailing update of two block steps (m = 4480, depth 256, 2
-# matrices: 640.0 MB read + written for 82.2 GFLOP;
-# profiles/cgemm_tf32_update_kernel_barge6084.md); the traffic of the average
-# launch is scaled from it by its flops.
+# matrices: 640.0 MB read + written for 82.2 GFLOP); the traffic of the
+# average launch is scaled from it by its flops.
 CGEMM_DRAM_BYTES_PER_FLOP = 640.0e6 / (8 * 4480 ** 2 * 256 * 2)
 
 
@@ -661,8 +660,11 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": workload_config(args, body.mesh.nb_faces) | {"engine": "oracle port (C++ OpenMP + SciPy LU)",
-                                                                    "frequencies_per_step": 1},
+            "config": {k: v for k, v in workload_config(args, body.mesh.nb_faces).items()
+                       if k not in ("rankine_part", "calls")} | {
+                "engine": "oracle port (C++ OpenMP + SciPy LU)",
+                "solver": "SciPy zgetrf/zgetrs (complex128 LU, one right-hand side at a time), "
+                          "C++ OpenMP assembly", "frequencies_per_step": 1},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{len(times)} frequency-solves of the 6084-panel barge, one per step"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

@@ -21,9 +21,14 @@
 //    several host threads without ordering) race on the array and must be
 //    serialised by the caller;
 //  * the first call on each device looks up the array's device address
-//    (cudaGetSymbolAddress, with that device current) and caches it; make that
-//    first call before any stream capture on that device.
+//    (cudaGetSymbolAddress, with that device current) and caches it with the
+//    device's current context; make that first call before any stream capture
+//    on that device.  A call made in a different context of that device (the
+//    primary context was reset by cudaDeviceReset and re-created) looks the
+//    address up again, so that no stale address reaches a kernel;
+//  * batch <= 65535 (one grid z-slice per matrix).
 // No cudaMalloc, cudaFree or allocating library routine is called here.
+#include <cuda.h>
 #include <algorithm>
 #include <mutex>
 #include "common.cuh"
@@ -40,17 +45,49 @@ static __device__ __align__(256) double2 g_static_scratch[kStaticScratch];
 
 std::mutex g_scratch_mutex;
 double2* g_scratch_ptr[kMaxDevices] = {nullptr};
+CUcontext g_scratch_ctx[kMaxDevices] = {nullptr};
 
-// Device address of g_static_scratch for the current device (set-up on first use).
+// cuCtxGetCurrent through the runtime's driver entry points (no link-time
+// dependency on libcuda, as for the tensor maps).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current_fn() {
+  static CtxGetCurrentFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(p);
+  }
+  return fn;
+}
+
+// Device address of g_static_scratch for the current device, looked up on the
+// first call in each context of the device.
 int static_scratch_address(double2** out) {
   int dev = 0;
   BEM_CUDA_CHECK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return set_error(BEM_ERR_UNSUPPORTED, "device index out of range");
+  CtxGetCurrentFn get_ctx = ctx_get_current_fn();
+  if (!get_ctx) return set_error(BEM_ERR_CUDA, "cuCtxGetCurrent is not available from the driver");
+  // null until the runtime has made a context current in this host thread
+  CUcontext ctx = nullptr;
+  if (get_ctx(&ctx) != CUDA_SUCCESS) ctx = nullptr;
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (g_scratch_ptr[dev] == nullptr) {
+  if (g_scratch_ptr[dev] == nullptr || ctx == nullptr || g_scratch_ctx[dev] != ctx) {
     void* p = nullptr;
-    BEM_CUDA_CHECK(cudaGetSymbolAddress(&p, g_static_scratch));
+    // also makes the device's primary context current in this thread
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      g_scratch_ptr[dev] = nullptr;
+      return set_error(BEM_ERR_CUDA, "cudaGetSymbolAddress of the static scratch array failed");
+    }
+    if (get_ctx(&ctx) != CUDA_SUCCESS || ctx == nullptr) {
+      g_scratch_ptr[dev] = nullptr;
+      return set_error(BEM_ERR_CUDA, "no current CUDA context for the static scratch array");
+    }
     g_scratch_ptr[dev] = static_cast<double2*>(p);
+    g_scratch_ctx[dev] = ctx;
   }
   *out = g_scratch_ptr[dev];
   return BEM_OK;
@@ -139,6 +176,8 @@ extern "C" int bem_zgemm_ts_static(int M, int K, int nrhs, double alpha_re, doub
   if (M <= 0 || K <= 0 || nrhs <= 0 || nrhs > kSMaxRhs || batch <= 0 || !A_dev || !X_dev || !Y_dev || lda < M ||
       ldx < K || ldy < M)
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zgemm_ts_static: bad arguments (nrhs must be <= 16)");
+  if (batch > 65535)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zgemm_ts_static: batch must be <= 65535 (one grid slice each)");
   const long long per_split = (long long)M * nrhs * batch;
   if (per_split > kStaticScratch) {
     char msg[256];

@@ -135,7 +135,7 @@ class Delhommeau:
         # then the wave term once per pair of faces (False: the general kernel).
         self.symmetric_assembly = True
         self._rankine_cache: "OrderedDict[tuple, object]" = OrderedDict()
-        # Prony decompositions by k h (128 most recent)
+        # Prony decompositions by k h (the 128 most recently used)
         self._prony_cache: "OrderedDict[float, np.ndarray]" = OrderedDict()
         self.exportable_settings = {
             "green_function": self.__class__.__name__,
@@ -176,6 +176,8 @@ class Delhommeau:
         cache = self._prony_cache
         with self._lock:
             hit = cache.get(kh)
+            if hit is not None:
+                cache.move_to_end(kh)  # least recently used first out
         if hit is None:
             try:
                 hit = prony.green_function_decomposition(kh)

@@ -439,11 +439,11 @@ def mesh_rectangle(*, size=(5.0, 5.0), center=(0.0, 0.0, 0.0), resolution=(5, 5)
     (rectangles.py:67-71).  reflection_symmetry: the half y < 0 mirrored in
     xOz (even number of panels across the width; centre and normal in the
     plane y = 0)."""
-    assert len(size) == 2 and all(h > 0 for h in size), "Size of the rectangle mesh should be given as positive values."
+    assert len(size) == 2 and all(h > 0 for h in size), "mesh_rectangle: size must be two lengths > 0"
     assert len(resolution) == 2 and all(h > 0 for h in resolution), \
-        "Resolution of the rectangle mesh should be given as positive values."
-    assert all(i == int(i) for i in resolution), "Resolution of a rectangle should be given as integer values."
-    assert len(center) == 3, "Position of the center of a rectangle should be given a 3-ple of values."
+        "mesh_rectangle: resolution must be two panel counts > 0"
+    assert all(i == int(i) for i in resolution), "mesh_rectangle: panel counts must be whole numbers"
+    assert len(center) == 3, "mesh_rectangle: center must have three coordinates"
     width, height = size
     nw, nh = (int(i) for i in resolution)
     if faces_max_radius is not None and np.hypot(width / nw, height / nh) / 2 > faces_max_radius:
@@ -452,11 +452,11 @@ def mesh_rectangle(*, size=(5.0, 5.0), center=(0.0, 0.0, 0.0), resolution=(5, 5)
     if reflection_symmetry:
         from .symmetric_meshes import ReflectionSymmetricMesh
         if nw % 2 == 1:
-            raise ValueError("To define a rectangle mesh with reflection symmetry, "
-                             "it should have an even number of panels in this direction.")
+            raise ValueError("mesh_rectangle: a mirrored rectangle needs an even panel count "
+                             "across the mirror plane.")
         if not np.isclose(center[1], 0.0) or not np.isclose(normal[1], 0.0):
-            raise ValueError("To define a rectangle mesh with reflection symmetry, its center should be in the "
-                             "xOz plane (that is y=0) and so should also be its normal vector.")
+            raise ValueError("mesh_rectangle: a mirrored rectangle needs its center and its normal "
+                             "in the mirror plane y = 0.")
         half = mesh_rectangle(size=(width / 2, height), resolution=(nw // 2, nh), center=(0, -width / 4, 0),
                               normal=normal)
         return ReflectionSymmetricMesh(half, plane="xOz", name=name).translated(center)
@@ -510,11 +510,11 @@ def mesh_parallelepiped(size=(1.0, 1.0, 1.0), center=(0, 0, 0), resolution=(4, 4
     if reflection_symmetry:
         from .symmetric_meshes import ReflectionSymmetricMesh
         if nw % 2 == 1 or nth % 2 == 1:
-            raise ValueError("To define a parallelepiped mesh with reflection symmetry, "
-                             "it should have an even number of panels in both direction.")
+            raise ValueError("mesh_parallelepiped: the two mirror planes need even panel counts "
+                             "along x and y.")
         if not np.isclose(center[0], 0.0) or not np.isclose(center[1], 0.0):
-            raise ValueError("To define a rectangle mesh with reflection symmetry, "
-                             "its center should be on the Oz axis (that is x=0 and y=0).")
+            raise ValueError("mesh_parallelepiped: the two mirror planes need the center "
+                             "on the vertical axis (x = y = 0).")
         quarter = mesh_parallelepiped(size=(width / 2, thickness / 2, height), resolution=(nw // 2, nth // 2, nh),
                                       center=(-width / 4, -thickness / 4, 0),
                                       missing_sides=set(missing_sides) | {"right", "back"})
@@ -549,17 +549,17 @@ def mesh_vertical_cylinder(*, length=10.0, radius=1.0, center=(0, 0, 0), resolut
     (capytaine cylinders.py:108-205).  reflection_symmetry: the half
     0 <= theta <= pi mirrored in yOz (even ntheta); axial_symmetry: one slice of
     angle 2 pi / ntheta repeated ntheta times about Oz."""
-    assert length > 0 and radius > 0, "Length and radius of a cylinder should be given as positive values."
+    assert length > 0 and radius > 0, "cylinder: length and radius must be > 0"
     nr, ntheta, nz = resolution
     nr, ntheta, nz = _cylinder_resolution(length, radius, nr, ntheta, nz, faces_max_radius)
     if reflection_symmetry and axial_symmetry:
-        raise NotImplementedError("Vertical cylinders with both symmetries have not been implemented.")
+        raise NotImplementedError("mesh_vertical_cylinder: reflection and axial symmetry together are not supported")
     if reflection_symmetry or axial_symmetry:
         from .symmetric_meshes import ReflectionSymmetricMesh, RotationSymmetricMesh
         if reflection_symmetry:
             if ntheta % 2 == 1:
-                raise ValueError("To use the reflection symmetry of the mesh, "
-                                 "it should have an even number of panels in this direction.")
+                raise ValueError("a mirrored mesh needs an even number of panels "
+                                 "around the axis (ntheta).")
             half = mesh_vertical_cylinder(length=length, radius=radius, resolution=(nr, ntheta // 2, nz),
                                           _theta_max=_theta_max / 2)
             mesh = ReflectionSymmetricMesh(half, plane="yOz", name=name)
@@ -619,22 +619,22 @@ def mesh_disk(*, radius=1.0, center=(0.0, 0.0, 0.0), normal=(0.0, 0.0, 1.0), res
     its normal is `normal`.  reflection_symmetry: the half y >= 0 mirrored in
     xOz (even ntheta); axial_symmetry: one sector repeated ntheta times about
     Oz (for a horizontal disk)."""
-    assert radius > 0, "Radius of the disk mesh should be given as a positive value."
+    assert radius > 0, "mesh_disk: radius must be > 0"
     assert len(resolution) == 2 and all(h > 0 for h in resolution), \
-        "Resolution of the disk mesh should be given as positive values."
-    assert all(i == int(i) for i in resolution), "Resolution of a disk should be given as integer values."
+        "mesh_disk: resolution must be two counts > 0"
+    assert all(i == int(i) for i in resolution), "mesh_disk: counts must be whole numbers"
     nr, ntheta = (int(i) for i in resolution)
     if faces_max_radius is not None and np.hypot(radius / nr, 2 * np.pi * radius / ntheta) / 2 > faces_max_radius:
         nr = int(np.ceil(radius / (np.sqrt(2) * faces_max_radius)))
         ntheta = int(np.ceil(2 * np.pi * radius / (np.sqrt(2) * faces_max_radius)))
     if reflection_symmetry and axial_symmetry:
-        raise NotImplementedError("Disks with both symmetries have not been implemented.")
+        raise NotImplementedError("mesh_disk: reflection and axial symmetry together are not supported")
     if reflection_symmetry or axial_symmetry:
         from .symmetric_meshes import ReflectionSymmetricMesh, RotationSymmetricMesh
         if reflection_symmetry:
             if ntheta % 2 == 1:
-                raise ValueError("To use the reflection symmetry of the mesh, "
-                                 "it should have an even number of panels in this direction.")
+                raise ValueError("a mirrored mesh needs an even number of panels "
+                                 "around the axis (ntheta).")
             half = mesh_disk(radius=radius, resolution=(nr, ntheta // 2), _theta_max=_theta_max / 2)
             mesh = ReflectionSymmetricMesh(half, plane="xOz", name=name)
         else:
@@ -656,15 +656,15 @@ def mesh_horizontal_cylinder(*, length=10.0, radius=1.0, center=(0.0, 0.0, 0.0),
     """Closed cylinder along Ox (capytaine cylinders.py:204-288): nx slices of
     ntheta panels, two end disks of nr rings.  reflection_symmetry: the half
     y >= 0 mirrored in xOz (even ntheta)."""
-    assert length > 0 and radius > 0, "Length and radius of a cylinder should be given as positive values."
+    assert length > 0 and radius > 0, "cylinder: length and radius must be > 0"
     assert len(resolution) == 3 and all(h >= 0 for h in resolution), \
-        "Resolution of a cylinder should be given as positive values."
+        "mesh_horizontal_cylinder: resolution must be three counts >= 0"
     nr, ntheta, nx = _cylinder_resolution(length, radius, *(int(i) for i in resolution), faces_max_radius)
     if reflection_symmetry:
         from .symmetric_meshes import ReflectionSymmetricMesh
         if ntheta % 2 == 1:
-            raise ValueError("To use the reflection symmetry of the mesh, "
-                             "it should have an even number of panels in this direction.")
+            raise ValueError("a mirrored mesh needs an even number of panels "
+                             "around the axis (ntheta).")
         half = mesh_horizontal_cylinder(length=length, radius=radius, resolution=(nr, ntheta // 2, nx),
                                         _theta_max=_theta_max / 2)
         return ReflectionSymmetricMesh(half, plane="xOz", name=name).translated(center, name=name)

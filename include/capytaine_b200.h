@@ -373,9 +373,10 @@ int bem_block_combine(const void* in_dev, int64_t in_fstride, int64_t in_bstride
  * a loop where a cudaMalloc is unacceptable).  The split-K partial sums live in
  * a static device array of bem_zgemm_ts_static_capacity() = 524288 complex128
  * entries (8 MiB, held on every GPU that loads the library until exit);
- * M * nrhs * batch must not exceed it (else BEM_ERR_INVALID_ARGUMENT).  The
- * first call on a device looks the array up (make it before any stream
- * capture); calls that overlap on the GPU share the array and race. */
+ * M * nrhs * batch must not exceed it and batch must not exceed 65535 (else
+ * BEM_ERR_INVALID_ARGUMENT).  The first call on a device (and the first after
+ * its context was reset and re-created) looks the array up: make it before
+ * any stream capture.  Calls that overlap on the GPU share the array and race. */
 int64_t bem_zgemm_ts_static_capacity(void);
 int bem_zgemm_ts_static(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
                         int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,

@@ -1,10 +1,12 @@
 """The allocation-free entry point bem_zgemm_ts_static, for callers that can
 only pass buffers they already own (no device allocation of their own), must
-give the same result as bem_zgemm_ts with a caller workspace.
+give the same result as bem_zgemm_ts with a caller workspace, and must not
+take device memory of its own once the library is loaded.
 
 Two calls in a row share the library's static scratch array: the second call
 (different sizes, beta != 0) must not see anything left by the first.  The
-file is named so that pytest collects it last; it needs no other test."""
+file name sorts after every other test file, so pytest collects it last; it
+needs no other test."""
 import ctypes
 
 import numpy as np
@@ -64,6 +66,34 @@ def test_static_scratch_variant_matches_workspace_variant_twice():
         ref = _run(False, At, Xt, Yt, M, K, nrhs, batch, alpha, beta)
         got = _run(True, At, Xt, Yt, M, K, nrhs, batch, alpha, beta)
         assert np.abs(got - ref).max() / np.abs(ref).max() < RTOL, i
+
+
+def test_static_call_takes_no_device_memory():
+    """Free device memory (cudaMemGetInfo) is the same before and after a
+    static call made once the first call has looked the array up."""
+    import torch
+    lib = _lib.load()
+    M, K, nrhs, batch = 3000, 2000, 8, 2
+    At, Xt, Yt = _case(M, K, nrhs, batch, seed=7)
+    args = (M, K, nrhs, 1.0, 0.0, _vp(At), M, M * K, _vp(Xt), K, K * nrhs, 0.0, 0.0, _vp(Yt), M, M * nrhs, batch,
+            _lib.stream_ptr())
+    _lib.check(lib.bem_zgemm_ts_static(*args))
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    _lib.check(lib.bem_zgemm_ts_static(*args))
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+
+
+def test_static_scratch_batch_limit():
+    import torch
+    lib = _lib.load()
+    A = torch.zeros((4, 4), dtype=torch.complex128, device="cuda")
+    status = lib.bem_zgemm_ts_static(1, 4, 1, 1.0, 0.0, _vp(A), 1, 0, _vp(A), 4, 0, 0.0, 0.0, _vp(A), 1, 0, 70000,
+                                     _lib.stream_ptr())
+    assert status == _lib.BEM_ERR_INVALID_ARGUMENT
+    assert b"65535" in lib.bem_last_error()
 
 
 def test_static_scratch_capacity_is_enforced():
