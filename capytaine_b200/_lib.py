@@ -67,6 +67,27 @@ class AssemblyArgs(ctypes.Structure):
     ]
 
 
+class GreenFunctionParams(ctypes.Structure):
+    """Mirror of ``bem_green_function_params``."""
+    _fields_ = [("tabulation_nr", c_int), ("tabulation_rmax", c_double), ("tabulation_nz", c_int),
+                ("tabulation_zmin", c_double), ("tabulation_nb_integration_points", c_int),
+                ("tabulation_grid_shape", c_int), ("gf_singularities", c_int)]
+
+
+class MeshDesc(ctypes.Structure):
+    """Mirror of ``bem_mesh_desc`` (host pointers)."""
+    _fields_ = [("nb_faces", c_int), ("nb_vertices", c_int), ("vertices", c_void_p), ("faces", c_void_p),
+                ("centers", c_void_p), ("normals", c_void_p), ("areas", c_void_p), ("radii", c_void_p),
+                ("hull_mask", c_void_p)]
+
+
+class SolveStats(ctypes.Structure):
+    """Mirror of ``bem_solve_stats``."""
+    _fields_ = [("iterations", c_int), ("residual", c_double), ("escalated_to_gmres", c_int)]
+
+
+BEM_PENDING = 9
+
 _SIGNATURES = {
     "bem_last_error": ([], ctypes.c_char_p),
     "bem_version": ([], c_int),
@@ -107,6 +128,11 @@ _SIGNATURES = {
     "bem_clu_factor": ([c_void_p, c_i64, c_i64, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                         c_void_p], c_int),
     "bem_clu_solve": ([c_void_p, c_int, c_int, c_void_p, c_void_p, c_i64, c_i64, c_int, c_void_p, c_void_p], c_int),
+    "bem_clu_solve_bounded": ([c_void_p, c_int, c_int, c_void_p, c_void_p, c_i64, c_i64, c_int, ctypes.c_longlong,
+                               c_int, c_void_p, c_void_p], c_int),
+    "bem_zlu_refine_solve": ([c_void_p, c_i64, c_i64, c_int, c_void_p, c_int, c_i64, c_i64, c_int, c_void_p,
+                              c_void_p, c_void_p, c_void_p, c_void_p, c_i64, c_i64, c_int, c_double, c_int, c_void_p,
+                              c_void_p, c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_double), c_void_p], c_int),
     "bem_refine_solve": ([c_void_p, c_i64, c_i64, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                           c_void_p, c_i64, c_i64, c_int, c_double, c_int, c_void_p, c_void_p, c_void_p,
                           ctypes.POINTER(c_int), ctypes.POINTER(c_double), c_void_p], c_int),
@@ -119,6 +145,18 @@ _SIGNATURES = {
                              c_double, c_double, c_void_p, c_i64, c_i64, c_int, c_void_p], c_int),
     "bem_froude_krylov": ([c_int, c_int, c_int, c_int, c_void_p, c_double, c_double, c_double, c_void_p, c_void_p,
                            c_void_p, c_void_p, c_void_p], c_int),
+    "bem_context_create": ([c_int, ctypes.POINTER(GreenFunctionParams), ctypes.POINTER(c_void_p)], c_int),
+    "bem_context_tabulation": ([c_void_p, c_void_p, c_void_p, c_void_p], c_int),
+    "bem_context_set_tabulation": ([c_void_p, c_void_p], c_int),
+    "bem_solve_frequency": ([c_void_p, ctypes.POINTER(MeshDesc), c_int, c_void_p, c_int, c_void_p, c_int, c_void_p,
+                             c_double, c_double, c_int, c_void_p, c_void_p, c_void_p, ctypes.POINTER(SolveStats)],
+                            c_int),
+    "bem_solve_submit": ([c_void_p, ctypes.POINTER(MeshDesc), c_int, c_void_p, c_int, c_void_p, c_int, c_void_p,
+                          c_double, c_double, c_int, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_void_p)], c_int),
+    "bem_request_poll": ([c_void_p, c_int, ctypes.POINTER(SolveStats)], c_int),
+    "bem_lu_factor": ([c_void_p, c_void_p, c_i64, c_int, c_int, ctypes.POINTER(c_void_p)], c_int),
+    "bem_lu_solve": ([c_void_p, c_void_p, c_i64, c_int, c_void_p, c_i64, ctypes.POINTER(SolveStats)], c_int),
+    "bem_release": ([c_void_p], c_int),
     "bem_block_combine": ([c_void_p, c_i64, c_i64, c_i64, c_void_p, c_i64, c_i64, c_i64, c_void_p, c_void_p, c_int,
                            c_int, c_int, c_int, c_int, c_void_p], c_int),
 }

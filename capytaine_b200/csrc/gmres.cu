@@ -29,12 +29,6 @@
 
 namespace bem {
 
-int zgemm_ts_enqueue(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
-                     int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,
-                     double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev,
-                     void* stream, const int* skip);
-int clu_solve_enqueue(void* work_dev, int npad, int batch, void* B_dev, int64_t ldb, int64_t strideB, int nrhs,
-                      int* err_dev, cudaStream_t s, const int* skip);
 
 namespace {
 

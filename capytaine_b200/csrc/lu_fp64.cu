@@ -369,7 +369,9 @@ __global__ void __launch_bounds__(256) ztrsm_persistent_kernel(const double2* __
                                                                const int* __restrict__ piv, int64_t piv_stride,
                                                                const double2* __restrict__ inv, double2* B,
                                                                int64_t ldb, int64_t strideB, int nrhs, int forward,
-                                                               int* flags, int* ticket, int* err) {
+                                                               int* flags, int* ticket, int* err, const int* skip,
+                                                               long long spin_limit) {
+  if (skip && *skip) return;  // refinement already converged
   extern __shared__ double2 sm[];
   double2* Inv = sm;                 // inverse of the diagonal block, Inv[m*kLd + r]
   double2* L = Inv + kNB * kLd;      // off-diagonal block A[i-block, j-block], L[m*kLd + r]
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(256) ztrsm_persistent_kernel(const double2* __
     if (tid == 0) {
       long long it = 0;
       while (ld_acquire(flags + (size_t)b * nblk + j) == 0) {
-        if (++it > kSpinLimit) {
+        if (++it > spin_limit) {
           atomicExch(err, 1);
           break;
         }
@@ -575,16 +577,22 @@ extern "C" int bem_zlu_factor(void* A_dev, int n, int64_t lda, int64_t stride, i
   return BEM_OK;
 }
 
-extern "C" int bem_zlu_solve(const void* A_dev, int n, int64_t lda, int64_t stride, int batch, const int* piv_dev,
-                             const void* work_dev, void* B_dev, int64_t ldb, int64_t strideB, int nrhs,
-                             int* err_dev, void* stream) {
-  int st = check_lu_args(A_dev, n, lda, batch);
+namespace bem {
+// Address of the "converged" flag of a refinement with these factors: an int
+// in the workspace tail after the block-row flags and the ticket.
+int* zlu_done_flag(void* work_dev, int n, int batch) {
+  const int nblk = n / kNB;
+  int* flags = (int*)((char*)work_dev + (size_t)batch * nblk * 2 * kNB * kNB * sizeof(double2));
+  return flags + (size_t)batch * nblk + 1;
+}
+
+// Forward and backward block substitutions with the float64 factors, in place
+// on B; every launch returns at once while *skip != 0.
+int zlu_solve_enqueue(const void* A_dev, int n, int64_t lda, int64_t stride, int batch, const int* piv_dev,
+                      const void* work_dev, void* B_dev, int64_t ldb, int64_t strideB, int nrhs, int* err_dev,
+                      cudaStream_t s, const int* skip, long long spin_limit) {
+  int st = configure_smem();
   if (st) return st;
-  if (!piv_dev || !work_dev || !B_dev || !err_dev) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zlu_solve: null");
-  if (nrhs <= 0 || nrhs > kNB) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zlu_solve: nrhs must be in [1, 64]");
-  if (ldb < n) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zlu_solve: ldb < n");
-  if ((st = configure_smem())) return st;
-  cudaStream_t s = (cudaStream_t)stream;
   const int nblk = n / kNB;
   const double2* inv = (const double2*)work_dev;
   int* flags = (int*)((char*)work_dev + (size_t)batch * nblk * 2 * kNB * kNB * sizeof(double2));
@@ -598,10 +606,24 @@ extern "C" int bem_zlu_solve(const void* A_dev, int n, int64_t lda, int64_t stri
       TimedLaunch tl(kKZtrsm, s);
       ztrsm_persistent_kernel<<<nblk * batch, 256, smem, s>>>((const double2*)A_dev, lda, stride, nblk, batch,
                                                              piv_dev, n, inv, Bc, ldb, strideB, nc, forward, flags,
-                                                             ticket, err_dev);
+                                                             ticket, err_dev, skip, spin_limit);
       count_launches(1);
     }
   }
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
 }
+}  // namespace bem
+
+extern "C" int bem_zlu_solve(const void* A_dev, int n, int64_t lda, int64_t stride, int batch, const int* piv_dev,
+                             const void* work_dev, void* B_dev, int64_t ldb, int64_t strideB, int nrhs,
+                             int* err_dev, void* stream) {
+  int st = check_lu_args(A_dev, n, lda, batch);
+  if (st) return st;
+  if (!piv_dev || !work_dev || !B_dev || !err_dev) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zlu_solve: null");
+  if (nrhs <= 0 || nrhs > kNB) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zlu_solve: nrhs must be in [1, 64]");
+  if (ldb < n) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zlu_solve: ldb < n");
+  return zlu_solve_enqueue(A_dev, n, lda, stride, batch, piv_dev, work_dev, B_dev, ldb, strideB, nrhs, err_dev,
+                           (cudaStream_t)stream, nullptr, kSpinLimit);
+}
+

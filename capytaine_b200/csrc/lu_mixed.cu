@@ -31,11 +31,7 @@ namespace bem {
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store = 0, const float* Aop1 = nullptr,
-                      const float* Bop1 = nullptr);
-int zgemm_ts_enqueue(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
-                     int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,
-                     double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev,
-                     void* stream, const int* skip);
+                      const float* Bop1 = nullptr, int max_ctas = 0, long long wait_limit = 0);
 
 namespace {
 
@@ -44,7 +40,6 @@ constexpr int kPT = 64;        // panel tile width
 constexpr int kSplitK = 6 * kB;  // K' of the split-TF32 panel product: (hi, lo, hi) x (re, im) x 128
 constexpr int kRhs = 16;       // right-hand sides per solve launch
 constexpr int kOpBuffers = 3;  // packed operands of the current, previous and next block steps
-constexpr long long kSpin = 4000000;
 
 __device__ __forceinline__ float2 fmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 __device__ __forceinline__ float2 ffms(float2 acc, float2 a, float2 b) {
@@ -94,20 +89,15 @@ __global__ void convert_pad_kernel(const double2* __restrict__ K, int64_t ldk, i
   }
 }
 
-// Inverse of the diagonal block A_kk by Gauss-Jordan elimination with partial
-// pivoting among its rows.  The 128 x 128 block lives in registers: thread
-// (warp w, lane l) owns rows l + 32 a (a < 4) and columns w + 16 m (m < 8).
-// Per column: the owning warp picks the pivot and publishes the column, all
-// warps swap the two rows with shuffles and publish the pivot row, then every
-// thread updates its 32 entries.  Two barriers per column; the published
-// column/row alternate between two buffers.  Output: inv (128 x 128,
-// column-major) = A_kk^{-1}; info flags an exactly zero pivot.
 // One Gauss-Jordan column step with the owner slot JM of column j known at
-// compile time (j = 16 JM + jw).
+// compile time (j = 16 JM + jw).  Thread (warp w, lane l) owns rows l + 32 a
+// (a < 4) and columns w + 16 m (m < 8): the pivot row's entries in a warp's
+// columns all live in that warp, so only the pivot column crosses warps, through
+// shared memory, with one barrier per column (the column buffers alternate, and
+// a barrier separates the reads of one from the next write of the same one).
 template <int JM>
 __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b, int lane, int w, int tid,
-                                        float2 (*colbuf)[kB], float2 (*rowbuf)[kB], int* s_piv, int* perm,
-                                        int* __restrict__ info) {
+                                        float2 (*colbuf)[kB], int* s_piv, int* perm, int* __restrict__ info) {
   constexpr int SJ = JM >> 1;  // register slot of row j (j >> 5)
   const int j = 16 * JM + jw;
   const int buf = j & 1;
@@ -132,6 +122,7 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
         bi = oi;
       }
     }
+    // the pivot column with rows j and bi exchanged (entry j is the pivot)
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int r = lane + 32 * i;
@@ -145,19 +136,22 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
   }
   __syncthreads();
   const int p = s_piv[buf];
-  const int lj = j & 31;
+  const int lj = j & 31, lp = p & 31, sp = p >> 5;
+  // the pivot row in this warp's columns, in every lane; then rows j and p exchanged
+  float2 prow[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    float2 vp = a[0][m];
+#pragma unroll
+    for (int i = 1; i < 4; ++i)
+      if (i == sp) vp = a[i][m];
+    prow[m] = make_float2(__shfl_sync(0xffffffffu, vp.x, lp), __shfl_sync(0xffffffffu, vp.y, lp));
+  }
   if (p != j) {
-    const int lp = p & 31, sp = p >> 5;
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
-      float2 vp = a[0][m];
-#pragma unroll
-      for (int i = 1; i < 4; ++i)
-        if (i == sp) vp = a[i][m];
       const float2 vj = a[SJ][m];
-      const float2 from_p = make_float2(__shfl_sync(0xffffffffu, vp.x, lp), __shfl_sync(0xffffffffu, vp.y, lp));
       const float2 from_j = make_float2(__shfl_sync(0xffffffffu, vj.x, lj), __shfl_sync(0xffffffffu, vj.y, lj));
-      if (lane == lj) a[SJ][m] = from_p;
 #pragma unroll
       for (int i = 0; i < 4; ++i)
         if (i == sp && lane == lp) a[i][m] = from_j;
@@ -168,16 +162,11 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
       perm[p] = t;
     }
   }
-  if (lane == lj) {
-#pragma unroll
-    for (int m = 0; m < 8; ++m) rowbuf[buf][w + 16 * m] = a[SJ][m];
-  }
-  __syncthreads();
-  const float2 piv = rowbuf[buf][j];
+  const float2 piv = colbuf[buf][j];
   const float2 dinv = fabs1(piv) > 0.0f ? fdiv(make_float2(1.0f, 0.0f), piv) : make_float2(0.0f, 0.0f);
   float2 u[8];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) u[m] = (m == JM && w == jw) ? dinv : fmul(rowbuf[buf][w + 16 * m], dinv);
+  for (int m = 0; m < 8; ++m) u[m] = (m == JM && w == jw) ? dinv : fmul(prow[m], dinv);
   const float2 mdinv = make_float2(-dinv.x, -dinv.y);
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -198,17 +187,16 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
 // Inverse of the diagonal block A_kk by Gauss-Jordan elimination with partial
 // pivoting among its rows.  The 128 x 128 block lives in registers: thread
 // (warp w, lane l) owns rows l + 32 a (a < 4) and columns w + 16 m (m < 8).
-// Per column: the owning warp picks the pivot and publishes the column, all
-// warps swap the two rows with shuffles and publish the pivot row, then every
-// thread updates its 32 entries.  Two barriers per column; the published
-// column/row alternate between two buffers.  Columns are visited slot by slot
+// Per column: the owning warp picks the pivot and publishes the column, every
+// warp takes the pivot row of its own columns by shuffles and swaps the two
+// rows, then every thread updates its 32 entries: one barrier per column.
+// Columns are visited slot by slot
 // so that register indices are compile-time constants.  Output: inv (128 x 128,
 // column-major) = A_kk^{-1}; info flags an exactly zero pivot.
 __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* __restrict__ info,
                                                         float2* __restrict__ inv, int nblk,
                                                         float* __restrict__ binv, float* __restrict__ ainv) {
   __shared__ float2 colbuf[2][kB];
-  __shared__ float2 rowbuf[2][kB];
   __shared__ int s_piv[2];
   __shared__ int perm[kB];
   const int b = blockIdx.x, tid = threadIdx.x;
@@ -221,7 +209,7 @@ __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* _
   if (tid < kB) perm[tid] = tid;
   __syncthreads();
 #define BEM_GJ_SLOT(JM) \
-  for (int jw = 0; jw < 16; ++jw) gj_step<JM>(a, jw, kk, b, lane, w, tid, colbuf, rowbuf, s_piv, perm, info);
+  for (int jw = 0; jw < 16; ++jw) gj_step<JM>(a, jw, kk, b, lane, w, tid, colbuf, s_piv, perm, info);
   BEM_GJ_SLOT(0)
   BEM_GJ_SLOT(1)
   BEM_GJ_SLOT(2)
@@ -381,7 +369,8 @@ template <int NC>
 __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nblk, int batch,
                                                                const float2* __restrict__ inv, double2* B,
                                                                int64_t ldb, int64_t strideB, int nrhs, int forward,
-                                                               int* flags, int* ticket, int* err, const int* skip) {
+                                                               int* flags, int* ticket, int* err, const int* skip,
+                                                               long long spin_limit, int withheld) {
   if (skip && *skip) return;  // refinement already converged
   extern __shared__ __align__(16) float fsmf[];
   float* Lre = fsmf;  // Lre[m*kB + r], 128 x 128
@@ -450,7 +439,7 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
     if (tid == 0) {
       long long it = 0;
       while (ld_acquire_i(flags + (size_t)b * nblk + j) == 0) {
-        if (++it > kSpin) {
+        if (++it > spin_limit) {
           atomicExch(err, 1);
           break;
         }
@@ -497,7 +486,9 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   }
   __threadfence();
   __syncthreads();
-  if (tid == 0) st_release_i(flags + (size_t)b * nblk + i, 1);
+  // withheld >= 0 only from the bounded-wait test entry point: that block row
+  // never publishes its flag, so the waits on it run out
+  if (tid == 0 && i != withheld) st_release_i(flags + (size_t)b * nblk + i, 1);
 }
 
 constexpr int trsm_smem_bytes(int nc) { return 2 * kB * kB * (int)sizeof(float) + 3 * kB * nc * (int)sizeof(float2); }
@@ -668,11 +659,21 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
                                                                            npad, W);
   ++launches;
   const size_t abuf = (size_t)batch * npad * 2 * kB, bbuf = (size_t)batch * 2 * npad * 2 * kB;
+  // The trailing updates are persistent kernels holding one CTA per SM; the
+  // lookahead's Gauss-Jordan inverses (one CTA per matrix, a whole SM each)
+  // and panel products run on the side stream meanwhile, on SMs kept free.
+  int sms = 0;
+  {
+    int dev = 0;
+    BEM_CUDA_CHECK(cudaGetDevice(&dev));
+    BEM_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const int reserve = std::max(1, std::min(batch, sms / 4));
   float* Aop[kOpBuffers] = {w.Aop, w.Aop + abuf, w.Aop + 2 * abuf};
   float* Bop[kOpBuffers] = {w.Bop, w.Bop + bbuf, w.Bop + 2 * bbuf};
   // Inverse of the diagonal block, then the panel: A12 and A21 packed, L21 =
   // A21 A_kk^{-1} on the tensor cores into the working matrix, L21 packed.
-  auto diag_and_panel = [&](int kk, int buf, cudaStream_t on) -> int {
+  auto diag_and_panel = [&](int kk, int buf, cudaStream_t on, int side_ctas) -> int {
     {
       TimedLaunch tl(kKCluGj, on);
       clu_gj_kernel<<<batch, 512, 0, on>>>(W, kk, info_dev, w.inv, nblk, w.binv, w.ainv);
@@ -687,14 +688,14 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
                                                                     Bop[buf], w.a3);
       // split TF32: A_hi B_hi + A_lo B_hi + A_hi B_lo, float32-level multipliers
       int st2 = cgemm_tf32_update(w.a3, npad, kk + kB, w.binv, 2 * kB, 0, kSplitK, W.re, W.im, npad, W.stride,
-                                  kk + kB, kk, m, kB, batch, err_dev, on, 1);
+                                  kk + kB, kk, m, kB, batch, err_dev, on, 1, nullptr, nullptr, side_ctas);
       if (st2) return st2;
       clu_pack_kernel<<<dim3(m / 32, batch), 256, 0, on>>>(W, npad, kk, 0, kk + kB, kk, Aop[buf], Bop[buf],
                                                            nullptr);
       // block row of U scaled by the diagonal inverse, U' = A_kk^{-1} A12 (TF32),
       // for the backward substitution only (A12 itself is packed in Bop already)
       st2 = cgemm_tf32_update(w.ainv, kB, 0, Bop[buf], 2 * (int64_t)npad, 2 * (kk + kB), 2 * kB, W.re, W.im, npad,
-                              W.stride, kk, kk + kB, kB, m, batch, err_dev, on, 1);
+                              W.stride, kk, kk + kB, kB, m, batch, err_dev, on, 1, nullptr, nullptr, side_ctas);
       if (st2) return st2;
     }
     launches += 3;
@@ -703,11 +704,11 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
   // C rows r0.. (m), complex columns c0.. (nc) -= L21 U12 of the block step whose
   // packed operands are in buffer buf, and of a second step (buffer buf2 >= 0)
   // in the same pass over C (depth 256).
-  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2) -> int {
+  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2, int ctas) -> int {
     if (m <= 0 || nc <= 0) return BEM_OK;
     return cgemm_tf32_update(Aop[buf], npad, r0, Bop[buf], 2 * (int64_t)npad, 2 * c0, 2 * kB, W.re, W.im, npad,
                              W.stride, r0, c0, m, nc, batch, err_dev, s, 0, buf2 >= 0 ? Aop[buf2] : nullptr,
-                             buf2 >= 0 ? Bop[buf2] : nullptr);
+                             buf2 >= 0 ? Bop[buf2] : nullptr, ctas);
   };
   Lookahead* la = nullptr;
   if ((st = lookahead_for(s, &la))) return st;
@@ -720,20 +721,21 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
   // stream while, at every second step, the rest of the trailing matrix gets
   // the updates of steps k-1 and k together.  Operands of steps k-1, k, k+1
   // live in three buffers.
-  if ((st = diag_and_panel(0, 0, s))) return st;
+  if ((st = diag_and_panel(0, 0, s, 0))) return st;
   for (int kk = 0, step = 0; kk + kB < npad; kk += kB, ++step) {
     const int cur = step % kOpBuffers, prev = (step + kOpBuffers - 1) % kOpBuffers;
     const int nxt = (step + 1) % kOpBuffers;
     const int kn = kk + kB, rest = npad - kn - kB;
     const int pend = (step & 1) ? prev : -1;  // step k-1 still pending beyond block k
-    if ((st = update(cur, kn, kn, kB, npad - kn, pend))) return st;  // block row kn
-    if ((st = update(cur, kn + kB, kn, rest, kB, pend))) return st;  // block column kn below the diagonal
+    if ((st = update(cur, kn, kn, kB, npad - kn, pend, 0))) return st;  // block row kn
+    if ((st = update(cur, kn + kB, kn, rest, kB, pend, 0))) return st;  // block column kn below the diagonal
     BEM_CUDA_CHECK(cudaEventRecord(la->strips, s));
     BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->strips, 0));
-    if ((st = diag_and_panel(kn, nxt, la->side))) return st;
+    const bool big = (step & 1) && rest > 0;
+    if ((st = diag_and_panel(kn, nxt, la->side, big ? reserve : 0))) return st;
     BEM_CUDA_CHECK(cudaEventRecord(la->panel, la->side));
-    if (step & 1) {
-      if ((st = update(cur, kn + kB, kn + kB, rest, rest, prev))) return st;
+    if (big) {
+      if ((st = update(cur, kn + kB, kn + kB, rest, rest, prev, sms - reserve))) return st;
     }
     BEM_CUDA_CHECK(cudaStreamWaitEvent(s, la->panel, 0));
   }
@@ -747,7 +749,7 @@ namespace bem {
 // B (npad x nrhs complex128 per matrix); returns at once while *skip != 0.  Also
 // the preconditioner of the GMRES solver.
 int clu_solve_enqueue(void* work_dev, int npad, int batch, void* B_dev, int64_t ldb, int64_t strideB, int nrhs,
-                      int* err_dev, cudaStream_t s, const int* skip) {
+                      int* err_dev, cudaStream_t s, const int* skip, long long spin_limit, int withheld) {
   int st = configure_mixed();
   if (st) return st;
   MixedWork w = carve(work_dev, npad, batch);
@@ -763,10 +765,12 @@ int clu_solve_enqueue(void* work_dev, int npad, int batch, void* B_dev, int64_t 
       TimedLaunch tl(kKCtrsm, s);
       if (nc <= 8)
         ctrsm_persistent_kernel<8><<<nblk * batch, 256, trsm_smem_bytes(8), s>>>(
-            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip);
+            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip, spin_limit,
+            withheld);
       else
         ctrsm_persistent_kernel<16><<<nblk * batch, 256, trsm_smem_bytes(16), s>>>(
-            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip);
+            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip, spin_limit,
+            withheld);
       ++launches;
     }
   }
@@ -785,26 +789,39 @@ extern "C" int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv
                            nullptr);
 }
 
+extern "C" int bem_clu_solve_bounded(void* work_dev, int npad, int batch, const int* piv_dev, void* B_dev,
+                                     int64_t ldb, int64_t strideB, int nrhs, long long spin_limit, int withheld_block,
+                                     int* err_dev, void* stream) {
+  if (!work_dev || !piv_dev || !B_dev || !err_dev || npad <= 0 || npad % kB || batch <= 0 || nrhs <= 0 ||
+      ldb < npad || spin_limit <= 0 || withheld_block < -1 || withheld_block >= npad / kB)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_clu_solve_bounded: bad arguments");
+  return clu_solve_enqueue(work_dev, npad, batch, B_dev, ldb, strideB, nrhs, err_dev, (cudaStream_t)stream,
+                           nullptr, spin_limit, withheld_block);
+}
+
 extern "C" int bem_zgemm_ts(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
                             int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,
                             double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev,
                             void* stream);
 
-extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
-                                void* work_dev, const int* piv_dev, const void* B_dev, void* X_dev, void* R_dev,
-                                int64_t ldb, int64_t strideB, int nrhs, double tol, int max_iter, void* ts_work_dev,
-                                double* norms_dev, int* err_dev, int* iters_out, double* resid_out, void* stream) {
-  if (!K_dev || !work_dev || !piv_dev || !B_dev || !X_dev || !R_dev || !ts_work_dev || !norms_dev || !err_dev ||
-      !iters_out || !resid_out || nrhs <= 0 || nrhs > 16 || max_iter <= 0 || ldb < npad || npad % kB || n > npad ||
-      batch <= 0)
-    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_refine_solve: bad arguments (nrhs <= 16)");
-  cudaStream_t s = (cudaStream_t)stream;
+namespace bem {
+// Iterative refinement x += F^{-1} (b - K x) with the residual in float64
+// against the float64 K, where F^{-1} is `solve_in_place` (the float32 block
+// LU of the mixed engine, or the float64 block LU itself, whose pivoting stays
+// inside the diagonal blocks: the residual test then checks, and the
+// iteration repairs, what that pivoting loses).  x = 0, r = b to start; per
+// iteration: r <- F^{-1} r, x += r, r = b - K x, worst relative residual per
+// column, convergence flag on the device.  `done` is an int of the solver's
+// workspace; norms_dev holds 2 batch nrhs + 2 doubles.
+template <class Solve>
+int refine_loop(Solve solve_in_place, int* done, const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad,
+                int batch, const void* B_dev, void* X_dev, void* R_dev, int64_t ldb, int64_t strideB, int nrhs,
+                double tol, int max_iter, void* ts_work_dev, double* norms_dev, int* iters_out, double* resid_out,
+                cudaStream_t s) {
   const int nvec = batch * nrhs;
   double* bn = norms_dev;
   double* rn = norms_dev + nvec;
   double* state = norms_dev + 2 * nvec;  // [worst, iterations]
-  MixedWork w = carve(work_dev, npad, batch);
-  int* done = w.flags + (size_t)batch * (npad / kB) + 1;
   int launches = 1;
   // |b|^2 per column; x = 0, r = b, not converged
   colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)B_dev, n, ldb, strideB, bn, nullptr);
@@ -827,14 +844,14 @@ extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK,
   while (enqueued < max_iter) {
     const int group = std::min(kGroup, max_iter - enqueued);
     for (int g = 0; g < group; ++g) {
-      // r <- (LU)^{-1} r in place (float32 factors; the padded rows of r stay zero)
-      int st = clu_solve_enqueue(work_dev, npad, batch, R_dev, ldb, strideB, nrhs, err_dev, s, done);
+      // r <- F^{-1} r in place (the padded rows of r stay zero)
+      int st = solve_in_place(R_dev, (const int*)done);
       if (st) return st;
       // x += r ; r = b ; r -= K x (float64)
       ir_update_kernel<<<dim3(ceil_div(n, 256), nrhs, batch), 256, 0, s>>>(
           (double2*)X_dev, (double2*)R_dev, (const double2*)B_dev, n, nrhs, ldb, strideB, done);
       st = zgemm_ts_enqueue(n, n, nrhs, -1.0, 0.0, K_dev, ldk, strideK, X_dev, ldb, strideB, 1.0, 0.0, R_dev, ldb,
-                            strideB, batch, ts_work_dev, stream, done);
+                            strideB, batch, ts_work_dev, s, done);
       if (st) return st;
       colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)R_dev, n, ldb, strideB, rn, done);
       refine_check_kernel<<<1, 256, 0, s>>>(bn, rn, nvec, tol, done, state);
@@ -846,8 +863,8 @@ extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK,
     BEM_CUDA_CHECK(cudaStreamSynchronize(s));
     if (host_state[0] <= tol && host_state[1] > 0.0) break;
     // A contracting iteration gains far more than a factor 2 per group; one
-    // that does not (the float32 factors too far from K, e.g. near an
-    // irregular frequency) stops here and reports non-convergence.
+    // that does not (the factors too far from K, e.g. near an irregular
+    // frequency) stops here and reports non-convergence.
     if (enqueued > group && !(host_state[0] < 0.5 * before)) break;
   }
   count_launches(launches);
@@ -861,4 +878,43 @@ extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK,
     return set_error(BEM_ERR_NOT_CONVERGED, msg);
   }
   return BEM_OK;
+}
+}  // namespace bem
+
+extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
+                                void* work_dev, const int* piv_dev, const void* B_dev, void* X_dev, void* R_dev,
+                                int64_t ldb, int64_t strideB, int nrhs, double tol, int max_iter, void* ts_work_dev,
+                                double* norms_dev, int* err_dev, int* iters_out, double* resid_out, void* stream) {
+  if (!K_dev || !work_dev || !piv_dev || !B_dev || !X_dev || !R_dev || !ts_work_dev || !norms_dev || !err_dev ||
+      !iters_out || !resid_out || nrhs <= 0 || nrhs > 16 || max_iter <= 0 || ldb < npad || npad % kB || n > npad ||
+      batch <= 0)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_refine_solve: bad arguments (nrhs <= 16)");
+  cudaStream_t s = (cudaStream_t)stream;
+  MixedWork w = carve(work_dev, npad, batch);
+  int* done = w.flags + (size_t)batch * (npad / kB) + 1;
+  auto solve = [&](void* R, const int* skip) {
+    return clu_solve_enqueue(work_dev, npad, batch, R, ldb, strideB, nrhs, err_dev, s, skip);
+  };
+  return refine_loop(solve, done, K_dev, ldk, strideK, n, npad, batch, B_dev, X_dev, R_dev, ldb, strideB, nrhs, tol,
+                     max_iter, ts_work_dev, norms_dev, iters_out, resid_out, s);
+}
+
+extern "C" int bem_zlu_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, const void* LU_dev,
+                                    int npad, int64_t ldlu, int64_t strideLU, int batch, const int* piv_dev,
+                                    void* lu_work_dev, const void* B_dev, void* X_dev, void* R_dev, int64_t ldb,
+                                    int64_t strideB, int nrhs, double tol, int max_iter, void* ts_work_dev,
+                                    double* norms_dev, int* err_dev, int* iters_out, double* resid_out,
+                                    void* stream) {
+  if (!K_dev || !LU_dev || !lu_work_dev || !piv_dev || !B_dev || !X_dev || !R_dev || !ts_work_dev || !norms_dev ||
+      !err_dev || !iters_out || !resid_out || nrhs <= 0 || nrhs > 16 || max_iter <= 0 || npad <= 0 || npad % 64 ||
+      n > npad || n <= 0 || ldk < n || ldlu < npad || ldb < npad || batch <= 0)
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zlu_refine_solve: bad arguments (nrhs <= 16, npad % 64 == 0)");
+  cudaStream_t s = (cudaStream_t)stream;
+  int* done = zlu_done_flag(lu_work_dev, npad, batch);
+  auto solve = [&](void* R, const int* skip) {
+    return zlu_solve_enqueue(LU_dev, npad, ldlu, strideLU, batch, piv_dev, lu_work_dev, R, ldb, strideB, nrhs,
+                             err_dev, s, skip, kDefaultSpinLimit);
+  };
+  return refine_loop(solve, done, K_dev, ldk, strideK, n, npad, batch, B_dev, X_dev, R_dev, ldb, strideB, nrhs, tol,
+                     max_iter, ts_work_dev, norms_dev, iters_out, resid_out, s);
 }

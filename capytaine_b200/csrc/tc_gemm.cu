@@ -25,6 +25,7 @@
 // still drains its own copies before freeing tensor memory.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <algorithm>
 #include "common.cuh"
 
 namespace bem {
@@ -34,12 +35,11 @@ constexpr int kTM = 128;            // tile rows
 constexpr int kTNc = 128;           // tile complex columns
 constexpr int kTN = 2 * kTNc;       // accumulator columns (MMA N)
 constexpr int kKC = 32;             // K' values per stage (128 bytes of fp32)
-constexpr int kStages = 2;
+constexpr int kStages = 4;
 constexpr int kABytes = kTM * kKC * 4;   // 16 KiB
 constexpr int kBBytes = kTN * kKC * 4;   // 32 KiB
 constexpr int kStageBytes = kABytes + kBBytes;
-constexpr int kTmemCols = 256;
-constexpr long long kWaitLimit = 1ll << 20;  // try_wait polls; ends a stuck wait within seconds
+constexpr long long kWaitLimit = 1ll << 22;  // default polls of a bounded mbarrier wait (~ a second)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -61,18 +61,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: returns false (and records an error) when the limit is reached.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-  long long it = 0;
-  while (!mbar_try_wait(bar, parity)) {
-    if (++it > kWaitLimit) {
-      atomicExch(err, 1);
-      return false;
-    }
-  }
-  return true;
-}
-
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
                                             uint64_t* bar) {
   asm volatile(
@@ -138,6 +126,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
 struct UpdateArgs {
   int a_row0;        // first operand row of the trailing block (Aop)
   int b_row0;        // first operand row of the trailing block (Bop), = 2 * first complex column
@@ -151,11 +143,36 @@ struct UpdateArgs {
   int64_t c_stride;  // elements between matrices
   int* err;
   int store;         // 0: C -= A B;  1: C = A B (C is not read)
+  int tiles_m;       // tile grid: tiles_m x tiles_n x batch, tm fastest
+  int tiles_n;
+  int ntiles;
+  long long wait_limit;  // polls of a bounded mbarrier wait
 };
 
-constexpr int kThreads = 320;  // producer warp, MMA warp, 8 epilogue warps
+constexpr int kEpiWarps = 16;                  // 4 lane quarters x 4 groups of 64 accumulator columns
+constexpr int kThreads = 32 * (2 + kEpiWarps);  // producer warp, MMA warp, epilogue warps
+constexpr int kAccCols = kTN;                  // TMEM columns of one accumulator
+constexpr int kTmemAlloc = 2 * kAccCols;       // two accumulators: all 512 columns of the SM
 
-__global__ void __launch_bounds__(kThreads, 2) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
+// Bounded wait with the limit of the launch.
+__device__ __forceinline__ bool mbar_wait_n(uint64_t* bar, uint32_t parity, int* err, long long limit) {
+  long long it = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    if (++it > limit) {
+      atomicExch(err, 1);
+      return false;
+    }
+  }
+  return true;
+}
+
+// Persistent trailing update: one CTA per SM walks the 128 x 128 complex tiles
+// t = blockIdx.x, blockIdx.x + gridDim.x, ... with two accumulators in tensor
+// memory, so that the epilogue of tile i (read C, subtract, write C) overlaps
+// the MMAs of tile i+1.  Barriers: full/empty per operand stage (TMA -> MMA ->
+// TMA), acc_full per accumulator (MMA commit -> epilogue), acc_empty per
+// accumulator (one arrival per epilogue warp -> MMA).
+__global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
                                                                    const __grid_constant__ CUtensorMap mapB,
                                                                    const __grid_constant__ CUtensorMap mapA1,
                                                                    const __grid_constant__ CUtensorMap mapB1,
@@ -168,24 +185,30 @@ __global__ void __launch_bounds__(kThreads, 2) cgemm_tf32_update_kernel(const __
   unsigned char* ringB = smem + kStages * kABytes;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accf = empty + kStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+  uint64_t* acc_full = empty + kStages;  // [2]
+  uint64_t* acc_empty = acc_full + 2;    // [2]
+  uint64_t* mma_done = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tm = blockIdx.x, tn = blockIdx.y, b = blockIdx.z;
+  const long long limit = p.wait_limit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accf, 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], kEpiWarps);
+    }
+    mbar_init(mma_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
     __syncwarp();
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
-                 "r"(kTmemCols)
+                 "r"(kTmemAlloc)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
@@ -193,113 +216,131 @@ __global__ void __launch_bounds__(kThreads, 2) cgemm_tf32_update_kernel(const __
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
+  const int per_matrix = p.tiles_m * p.tiles_n;
 
   if (warp == 0) {
     if (lane == 0) {
-      // producer
+      // producer: operand slices of every tile of this CTA through the ring
       bool ok = true;
-      int issued = 0;
-      for (int kc = 0; kc < p.nk && ok; ++kc) {
-        const int s = kc % kStages;
-        if (kc >= kStages) ok = mbar_wait(&empty[s], ((kc / kStages) - 1) & 1, p.err);
-        if (!ok) break;
-        mbar_expect_tx(&full[s], kStageBytes);
-        // K' chunks [0, nk0) from the first operand pair, the rest from the second
-        const bool first = kc < p.nk0;
-        const int kx = (first ? kc : kc - p.nk0) * kKC;
-        tma_load_3d(ringA + s * kABytes, first ? &mapA : &mapA1, kx, p.a_row0 + tm * kTM, b, &full[s]);
-        tma_load_3d(ringB + s * kBBytes, first ? &mapB : &mapB1, kx, p.b_row0 + tn * kTN, b, &full[s]);
-        issued = kc + 1;
+      long long g = 0;  // stage uses so far
+      for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+        const int b = t / per_matrix, r = t - b * per_matrix;
+        const int tn = r / p.tiles_m, tm = r - tn * p.tiles_m;
+        for (int kc = 0; kc < p.nk; ++kc, ++g) {
+          const int s = (int)(g % kStages);
+          const uint32_t use = (uint32_t)(g / kStages);
+          if (g >= kStages && !(ok = mbar_wait_n(&empty[s], (use - 1) & 1, p.err, limit))) break;
+          mbar_expect_tx(&full[s], kStageBytes);
+          // K' chunks [0, nk0) from the first operand pair, the rest from the second
+          const bool first = kc < p.nk0;
+          const int kx = (first ? kc : kc - p.nk0) * kKC;
+          tma_load_3d(ringA + s * kABytes, first ? &mapA : &mapA1, kx, p.a_row0 + tm * kTM, b, &full[s]);
+          tma_load_3d(ringB + s * kBBytes, first ? &mapB : &mapB1, kx, p.b_row0 + tn * kTN, b, &full[s]);
+        }
       }
       // drain: every issued copy must land before the CTA may exit
-      for (int kc = (issued > kStages ? issued - kStages : 0); kc < issued; ++kc)
-        mbar_wait(&full[kc % kStages], (kc / kStages) & 1, p.err);
+      for (long long q = (g > kStages ? g - kStages : 0); q < g; ++q)
+        mbar_wait_n(&full[q % kStages], (uint32_t)(q / kStages) & 1, p.err, limit);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       // MMA issuer
       bool ok = true;
-      for (int kc = 0; kc < p.nk && ok; ++kc) {
-        const int s = kc % kStages;
-        ok = mbar_wait(&full[s], (kc / kStages) & 1, p.err);
-        if (!ok) break;
+      long long g = 0;
+      int i = 0;  // tiles of this CTA so far
+      for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++i) {
+        const int acc = i & 1;
+        const uint32_t use = (uint32_t)(i >> 1);
+        // the epilogue must have drained this accumulator's previous tile
+        if (i >= 2 && !(ok = mbar_wait_n(&acc_empty[acc], (use - 1) & 1, p.err, limit))) break;
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        const uint32_t a0 = smem_u32(ringA + s * kABytes), b0 = smem_u32(ringB + s * kBBytes);
+        const uint32_t tacc = tmem + (uint32_t)(acc * kAccCols);
+        for (int kc = 0; kc < p.nk; ++kc, ++g) {
+          const int s = (int)(g % kStages);
+          if (!(ok = mbar_wait_n(&full[s], (uint32_t)(g / kStages) & 1, p.err, limit))) break;
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          const uint32_t a0 = smem_u32(ringA + s * kABytes), b0 = smem_u32(ringB + s * kBBytes);
 #pragma unroll
-        for (int kk = 0; kk < kKC / 8; ++kk) {
-          // K = 8 tf32 = 32 bytes per instruction inside the 128-byte swizzle atom
-          mma_tf32(tmem, smem_desc_k_sw128(a0 + kk * 32), smem_desc_k_sw128(b0 + kk * 32), (kc | kk) != 0);
+          for (int kk = 0; kk < kKC / 8; ++kk) {
+            // K = 8 tf32 = 32 bytes per instruction inside the 128-byte swizzle atom
+            mma_tf32(tacc, smem_desc_k_sw128(a0 + kk * 32), smem_desc_k_sw128(b0 + kk * 32), (kc | kk) != 0);
+          }
+          mma_commit(&empty[s]);
         }
-        mma_commit(&empty[s]);
+        if (!ok) break;
+        mma_commit(&acc_full[acc]);
       }
-      mma_commit(accf);
+      // every MMA issued by this thread has completed before tensor memory is freed
+      mma_commit(mma_done);
+      mbar_wait_n(mma_done, 0, p.err, limit);
     }
   } else {
-    // epilogue warps 2..9: TMEM lanes 32*(warp % 4) .. +31; warps 2-5 take the
-    // real plane (accumulator columns 0..127), warps 6-9 the imaginary plane.
-    // Each reads its plane in 8 chunks of 16 columns through a register double
-    // buffer: the first chunk is loaded while the MMAs run, chunk i+1 while
-    // chunk i is applied.
-    constexpr int kCW = 16;                // columns per chunk
-    constexpr int kPlaneChunks = kTNc / kCW;
-    const int q = warp & 3;
-    const int first = ((warp - 2) >> 2) * kPlaneChunks, last = first + kPlaneChunks;
-    const int row = p.c_row0 + tm * kTM + 32 * q + lane;
-    float* Cr = p.Cr + (size_t)b * p.c_stride + row;
-    float* Ci = p.Ci + (size_t)b * p.c_stride + row;
-    const int col0 = p.c_col0 + tn * kTNc;
-    const int64_t ldc = p.ldc;
-    auto at = [&](int chunk) -> float* {
-      return (chunk < kPlaneChunks ? Cr : Ci) + (size_t)(col0 + (chunk % kPlaneChunks) * kCW) * ldc;
-    };
+    // epilogue warp: TMEM lanes 32 q .. 32 q + 31 (q = warp % 4, the quarter a
+    // warp may access), accumulator columns 64 cg .. 64 cg + 63 (cg 0, 1: real
+    // plane; 2, 3: imaginary plane), in 4 chunks of 16 columns through a
+    // register double buffer of C.
+    constexpr int kCW = 16;
+    constexpr int kChunks = 64 / kCW;
+    const int q = warp & 3, cg = (warp - 2) >> 2;
+    const int plane = cg >> 1, cbase = (cg & 1) * 64;
     const bool rd = p.store == 0;
-    float cb0[kCW], cb1[kCW];
+    const int64_t ldc = p.ldc;
+    bool ok = true;
+    int i = 0;
+    for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++i) {
+      const int b = t / per_matrix, r = t - b * per_matrix;
+      const int tn = r / p.tiles_m, tm = r - tn * p.tiles_m;
+      const int acc = i & 1;
+      const int row = p.c_row0 + tm * kTM + 32 * q + lane;
+      float* C = (plane ? p.Ci : p.Cr) + (size_t)b * p.c_stride + row +
+                 (size_t)(p.c_col0 + tn * kTNc + cbase) * ldc;
+      float cb0[kCW], cb1[kCW];
 #pragma unroll
-    for (int j = 0; j < kCW; ++j) cb0[j] = cb1[j] = 0.0f;
-    if (rd) {
-      const float* src = at(first);
+      for (int j = 0; j < kCW; ++j) cb0[j] = cb1[j] = 0.0f;
+      if (rd) {
 #pragma unroll
-      for (int j = 0; j < kCW; ++j) cb0[j] = __ldcs(src + j * ldc);
-    }
-    const bool ok = __all_sync(0xffffffffu, mbar_wait(accf, 0, p.err));
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    __syncwarp();
-    if (ok) {
-      const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16);
-#pragma unroll 1
-      for (int chunk = first; chunk < last; chunk += 2) {
+        for (int j = 0; j < kCW; ++j) cb0[j] = __ldcs(C + (size_t)j * ldc);
+      }
+      ok = __all_sync(0xffffffffu, mbar_wait_n(&acc_full[acc], (uint32_t)(i >> 1) & 1, p.err, limit));
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      __syncwarp();
+      if (!ok) break;
+      const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kAccCols + plane * kTNc + cbase);
+#pragma unroll
+      for (int chunk = 0; chunk < kChunks; chunk += 2) {
         if (rd) {
-          const float* src = at(chunk + 1);
 #pragma unroll
-          for (int j = 0; j < kCW; ++j) cb1[j] = __ldcs(src + j * ldc);
+          for (int j = 0; j < kCW; ++j) cb1[j] = __ldcs(C + (size_t)((chunk + 1) * kCW + j) * ldc);
         }
         {
           float v[kCW];
           tmem_ld16(tbase + (uint32_t)(chunk * kCW), v);
-          float* dst = at(chunk);
 #pragma unroll
-          for (int j = 0; j < kCW; ++j) __stcs(dst + j * ldc, rd ? cb0[j] - v[j] : v[j]);
+          for (int j = 0; j < kCW; ++j) __stcs(C + (size_t)(chunk * kCW + j) * ldc, rd ? cb0[j] - v[j] : v[j]);
         }
-        if (rd && chunk + 2 < last) {
-          const float* src = at(chunk + 2);
+        if (rd && chunk + 2 < kChunks) {
 #pragma unroll
-          for (int j = 0; j < kCW; ++j) cb0[j] = __ldcs(src + j * ldc);
+          for (int j = 0; j < kCW; ++j) cb0[j] = __ldcs(C + (size_t)((chunk + 2) * kCW + j) * ldc);
         }
         {
           float v[kCW];
           tmem_ld16(tbase + (uint32_t)((chunk + 1) * kCW), v);
-          float* dst = at(chunk + 1);
 #pragma unroll
-          for (int j = 0; j < kCW; ++j) __stcs(dst + j * ldc, rd ? cb1[j] - v[j] : v[j]);
+          for (int j = 0; j < kCW; ++j)
+            __stcs(C + (size_t)((chunk + 1) * kCW + j) * ldc, rd ? cb1[j] - v[j] : v[j]);
         }
       }
+      // this warp's reads of the accumulator are complete: release it
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[acc]);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     __syncwarp();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemAlloc) : "memory");
   }
 }
 
@@ -333,15 +374,26 @@ int make_operand_map(CUtensorMap* map, const float* base, int kp, int64_t rows, 
 }
 
 bool g_tc_configured = false;
+int g_num_sms[64] = {0};
+
+int num_sms(int* out) {
+  int dev = 0;
+  BEM_CUDA_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(BEM_ERR_UNSUPPORTED, "device index out of range");
+  if (!g_num_sms[dev]) BEM_CUDA_CHECK(cudaDeviceGetAttribute(&g_num_sms[dev], cudaDevAttrMultiProcessorCount, dev));
+  *out = g_num_sms[dev];
+  return BEM_OK;
+}
 
 }  // namespace
 
 // Host entry shared with the LU: C (trailing block m x n complex, both multiples
-// of 128) -= A' B' for `batch` matrices.
+// of 128) -= A' B' for `batch` matrices.  max_ctas > 0 caps the persistent grid
+// (SMs left free for work on other streams); 0: one CTA per SM.
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store, const float* Aop1,
-                      const float* Bop1) {
+                      const float* Bop1, int max_ctas, long long wait_limit) {
   if (m <= 0 || n <= 0) return BEM_OK;
   if (m % kTM || n % kTNc || kp % kKC || (a_row0 % 8) || (b_row0 % 8))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: sizes must be multiples of 128 (K' of 32)");
@@ -362,12 +414,20 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
     BEM_CUDA_CHECK(cudaFuncSetAttribute(cgemm_tf32_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     g_tc_configured = true;
   }
+  int sms = 0;
+  if ((st = num_sms(&sms))) return st;
   const int nk0 = kp / kKC;
-  UpdateArgs p{a_row0, b_row0, c_row0, c_col0, Aop1 ? 2 * nk0 : nk0, nk0, Cr, Ci, ldc, c_stride, err, store};
-  dim3 grid(m / kTM, n / kTNc, batch);
+  const int tiles_m = m / kTM, tiles_n = n / kTNc;
+  const long long ntiles = (long long)tiles_m * tiles_n * batch;
+  if (ntiles > (1ll << 30)) return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: too many tiles");
+  int ctas = max_ctas > 0 ? std::min(max_ctas, sms) : sms;
+  ctas = (int)std::min<long long>(ctas, ntiles);
+  UpdateArgs p{a_row0,  b_row0,  c_row0,  c_col0, Aop1 ? 2 * nk0 : nk0, nk0,           Cr,
+               Ci,      ldc,     c_stride, err,   store,               tiles_m,       tiles_n,
+               (int)ntiles, wait_limit > 0 ? wait_limit : kWaitLimit};
   {
     TimedLaunch tl(kKCgemmTf32, stream);
-    cgemm_tf32_update_kernel<<<grid, kThreads, smem, stream>>>(mapA, mapB, mapA1, mapB1, p);
+    cgemm_tf32_update_kernel<<<ctas, kThreads, smem, stream>>>(mapA, mapB, mapA1, mapB1, p);
   }
   count_launches(1);
   BEM_CUDA_CHECK(cudaGetLastError());
@@ -387,5 +447,5 @@ extern "C" int bem_cgemm_tf32_update(const float* Aop_dev, int64_t a_rows, int a
   if ((reinterpret_cast<uintptr_t>(Aop_dev) | reinterpret_cast<uintptr_t>(Bop_dev)) & 15)
     return bem::set_error(BEM_ERR_INVALID_ARGUMENT, "bem_cgemm_tf32_update: operands must be 16-byte aligned");
   return bem::cgemm_tf32_update(Aop_dev, a_rows, a_row0, Bop_dev, b_rows, b_row0, kp, Cr_dev, Ci_dev, ldc, c_stride,
-                                c_row0, c_col0, m, n, batch, err_dev, (cudaStream_t)stream, 0, nullptr, nullptr);
+                                c_row0, c_col0, m, n, batch, err_dev, (cudaStream_t)stream, 0, nullptr, nullptr, 0, 0);
 }

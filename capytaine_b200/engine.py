@@ -37,6 +37,10 @@ LOG = logging.getLogger(__name__)
 
 NB = 64  # LU block size; matrices are padded to a multiple of it
 RHS_CHUNK = 16  # right-hand sides per refinement / GMRES / tall-GEMM call
+# Relative residual |b - K x| / |b| that a float64 LU solve is refined to; a
+# solve whose residual stops decreasing above it (the float64 floor of an
+# ill-conditioned K) is accepted up to the engine's refine_tol.
+FP64_RESIDUAL_TOL = 1e-12
 
 
 def padded_size(n: int) -> int:
@@ -125,22 +129,28 @@ class _Factors:
     """Device storage of the matrices of `batch` frequency-solves of one mesh
     (n panels): S, K and the factorisation of K.
 
-    fp64:  K padded to a multiple of 64 (LU in place, identity padding).
+    fp64:  K with leading dimension npad (a multiple of 64) and, unless lu is
+           False (plain GMRES), its float64 LU in a second buffer of the same
+           layout (identity padding), so that every solve checks its residual
+           against K.
     mixed: K unpadded (float64 residuals) and the float32 LU workspace padded
            to a multiple of 128."""
 
-    def __init__(self, n, batch, device, precision, alloc=None):
+    def __init__(self, n, batch, device, precision, alloc=None, lu=True):
         import torch
         self.n, self.batch, self.precision = n, batch, precision
         lib = _lib.load()
         mk = _allocator(device, alloc)
         self.S = mk((batch, n * n), torch.complex128)
         self.info = mk((batch,), torch.int32, True)
+        self.LU = None
         if precision == "fp64":
             self.npad = padded_size(n)
             self.K = mk((batch, self.npad * self.npad), torch.complex128)
             self.ldk = self.npad
             self.strideK = self.npad * self.npad
+            if lu:
+                self.LU = mk((batch, self.npad * self.npad), torch.complex128)
             self.lu_work = mk((int(lib.bem_zlu_workspace_bytes(self.npad, batch)),), torch.uint8)
             self.lu_work_ptr = self.lu_work.data_ptr()
         else:
@@ -154,18 +164,20 @@ class _Factors:
         self.piv = mk((batch, self.npad), torch.int32)
 
     @staticmethod
-    def estimate_bytes(n, batch, precision):
+    def estimate_bytes(n, batch, precision, lu=True):
         """Device bytes of a _Factors of this shape (admission by footprint)."""
         lib = _lib.load()
         if precision == "fp64":
             npad = padded_size(n)
-            return batch * (16 * n * n + 16 * npad * npad) + int(lib.bem_zlu_workspace_bytes(npad, batch))
+            return (batch * (16 * n * n + (32 if lu else 16) * npad * npad)
+                    + int(lib.bem_zlu_workspace_bytes(npad, batch)))
         npad = int(math.ceil(n / 128) * 128)
         return batch * 32 * n * n + int(lib.bem_clu_workspace_bytes(npad, batch)) + 1024
 
     @property
     def nbytes(self):
-        return sum(t.numel() * t.element_size() for t in (self.S, self.K, self.lu_work, self.piv, self.info))
+        ts = [self.S, self.K, self.lu_work, self.piv, self.info] + ([self.LU] if self.LU is not None else [])
+        return sum(t.numel() * t.element_size() for t in ts)
 
 
 class _Rhs:
@@ -225,9 +237,9 @@ class _Workspace:
     """Factor storage and RHS buffers of one (n, batch, nrhs, precision) shape,
     reused across the batches of a sweep."""
 
-    def __init__(self, n, batch, nrhs, device, precision):
+    def __init__(self, n, batch, nrhs, device, precision, lu=True):
         self.n, self.batch, self.nrhs, self.precision = n, batch, nrhs, precision
-        self.f = _Factors(n, batch, device, precision)
+        self.f = _Factors(n, batch, device, precision, lu=lu)
         self.r = _Rhs(n, self.f.npad, batch, nrhs, device, precision)
 
     @property
@@ -397,7 +409,7 @@ class B200Engine:
         ws = self._ws.get(key)
         if ws is None:
             self._ws.clear()  # one resident shape at a time (memory)
-            ws = _Workspace(n, batch, nrhs, self.device, self.precision)
+            ws = _Workspace(n, batch, nrhs, self.device, self.precision, lu=not self._plain_gmres)
             self._ws[key] = ws
         return ws
 
@@ -581,8 +593,11 @@ class B200Engine:
             _lib.check(lib.bem_clu_factor(_vp(f.K), n, n * n, n, npad, nb, _vp(f.piv), _vp(f.info),
                                           _vp(f.lu_work_ptr), _vp(err), stream))
         elif not self._plain_gmres:
-            _lib.check(lib.bem_zpad_identity(_vp(f.K), npad, npad * npad, nb, n, npad, stream))
-            _lib.check(lib.bem_zlu_factor(_vp(f.K), npad, npad, npad * npad, nb, _vp(f.piv), _vp(f.info),
+            # K stays as assembled (the residual of every solve is taken against
+            # it); the LU is computed in place in a copy
+            f.LU[:nb].copy_(f.K[:nb])
+            _lib.check(lib.bem_zpad_identity(_vp(f.LU), npad, npad * npad, nb, n, npad, stream))
+            _lib.check(lib.bem_zlu_factor(_vp(f.LU), npad, npad, npad * npad, nb, _vp(f.piv), _vp(f.info),
                                           _vp(f.lu_work), stream))
 
     def solve_stage(self, f: "_Factors", r: "_Rhs", body, om, heads, *, rho=1000.0, g=9.81, stats=None,
@@ -663,7 +678,7 @@ class B200Engine:
                                             _vp(r.phi.data_ptr() + 16 * n * c0), n, n * nrhs, nbs, _vp(r.ts_work),
                                             stream))
             r.B.view(r.batch, nrhs, npad)[:nbs, :, :n].copy_(r.phi.view(r.batch, nrhs, n)[:nbs])
-        sol = r.B if (self.precision == "fp64" and not self._plain_gmres) else r.X
+        sol = r.X
         for c0 in range(0, nrhs, RHS_CHUNK):
             nc = min(RHS_CHUNK, nrhs - c0)
             off = 16 * npad * c0  # byte offset of column c0
@@ -673,8 +688,7 @@ class B200Engine:
             elif self.precision == "mixed":
                 self._refine(f, r, nbs, Bc, Xc, Rc, nc, stats, stream)
             else:
-                _lib.check(lib.bem_zlu_solve(_vp(f.K), npad, npad, npad * npad, nbs, _vp(f.piv), _vp(f.lu_work), Bc,
-                                             npad, ld, nc, _vp(r.err), stream))
+                self._solve_fp64(f, r, nbs, Bc, Xc, Rc, nc, stats, stream)
         if events:
             events[3].record()
         if direct:  # the solution is the potential
@@ -850,6 +864,29 @@ class B200Engine:
             raise _lib.NotConvergedError(status, lib.bem_last_error().decode())
         _lib.check(status)
 
+    def _solve_fp64(self, f, r, nb, Bc, Xc, Rc, nc, stats, stream):
+        """Float64 LU solve of nc columns with its residual checked against K
+        (bem_zlu_refine_solve): the block-local pivoting of the factorisation
+        cannot lose accuracy unnoticed; stats carry the worst relative
+        residual and the iterations (1 when the first solve already meets
+        refine_tol)."""
+        lib = _lib.load()
+        n, npad, ld = f.n, f.npad, f.npad * r.nrhs
+        iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
+        status = lib.bem_zlu_refine_solve(_vp(f.K), npad, npad * npad, n, _vp(f.LU), npad, npad, npad * npad, nb,
+                                          _vp(f.piv), _vp(f.lu_work), Bc, Xc, Rc, npad, ld, nc, FP64_RESIDUAL_TOL,
+                                          self.refine_max_iter, _vp(r.ts_work), _vp(r.norms), _vp(r.err),
+                                          ctypes.byref(iters), ctypes.byref(resid), stream)
+        stats["fp64_residual"] = max(stats.get("fp64_residual", 0.0), resid.value)
+        stats["fp64_solve_iters"] = max(stats.get("fp64_solve_iters", 0), iters.value)
+        if status == _lib.BEM_ERR_NOT_CONVERGED and resid.value <= self.refine_tol:
+            status = _lib.BEM_OK  # at the float64 floor of an ill-conditioned K, below the accepted residual
+        if status == _lib.BEM_ERR_NOT_CONVERGED:
+            stats["not_converged"] = stats.get("not_converged", 0) + 1
+            raise _lib.NotConvergedError(status, lib.bem_last_error().decode() +
+                                         " (float64 LU with pivoting inside its diagonal blocks)")
+        _lib.check(status)
+
     def _gmres_solve(self, f, r, nb, atol, rtol, precond_ptr, stats, stream, Bc, Xc, nc):
         """Plain float64 GMRES of nc RHS columns (column pointers Bc into Xc)
         with SciPy's settings: restart 20, at most 10 n cycles by default."""
@@ -965,6 +1002,42 @@ def _to_device(a: np.ndarray, device):
     return t
 
 
+def _fp64_checked_solve(K_ptr, ldk, strideK, n, lu, batch, Bh, nrhs, tol=FP64_RESIDUAL_TOL, accept=1e-10,
+                        max_iter=30):
+    """X solving K X = B for `batch` systems with the float64 factors lu =
+    (Kf, piv, work, npad) of bem_zlu_factor, the residual of every column
+    checked (and refined) against the unfactored K at K_ptr (n x n,
+    column-major, ldk, strideK apart) by bem_zlu_refine_solve.  Bh: (batch,
+    nrhs, npad) complex128 device tensor, rows >= n zero.  A residual that
+    stops decreasing above tol is accepted up to `accept`.  Returns X shaped
+    like Bh."""
+    import torch
+    Kf, piv, work, npad = lu
+    lib = _lib.load()
+    stream = _lib.stream_ptr()
+    X = torch.zeros_like(Bh)
+    R = torch.empty_like(Bh)
+    err = torch.zeros(1, dtype=torch.int32, device=Bh.device)
+    for c0 in range(0, nrhs, RHS_CHUNK):
+        nc = min(RHS_CHUNK, nrhs - c0)
+        ts = torch.empty(int(lib.bem_zgemm_ts_workspace_bytes(n, n, nc, batch)), dtype=torch.uint8, device=Bh.device)
+        norms = torch.zeros(2 * batch * nc + 2, dtype=torch.float64, device=Bh.device)
+        iters, resid = ctypes.c_int32(0), ctypes.c_double(0.0)
+        off = 16 * npad * c0
+        status = lib.bem_zlu_refine_solve(_vp(K_ptr), ldk, strideK, n, _vp(Kf), npad, npad, npad * npad, batch,
+                                          _vp(piv), _vp(work), _vp(Bh.data_ptr() + off), _vp(X.data_ptr() + off),
+                                          _vp(R.data_ptr() + off), npad, npad * nrhs, nc, tol, max_iter, _vp(ts),
+                                          _vp(norms), _vp(err), ctypes.byref(iters), ctypes.byref(resid), stream)
+        if status == _lib.BEM_ERR_NOT_CONVERGED and resid.value <= accept:
+            status = _lib.BEM_OK
+        if status == _lib.BEM_ERR_NOT_CONVERGED:
+            raise _lib.NotConvergedError(status, lib.bem_last_error().decode())
+        _lib.check(status)
+    if int(err.item()) != 0:
+        raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
+    return X
+
+
 class DeviceMatrix:
     """A device-resident influence matrix usable where capytaine expects an
     ndarray: ``M @ x`` and ``engine.linear_solver(M, b)`` run on the GPU."""
@@ -1030,7 +1103,11 @@ class DeviceMatrix:
                                       _lib.stream_ptr()))
         if int(info.item()) != 0:
             raise _lib.SingularMatrixError(_lib.BEM_ERR_SINGULAR, f"zero pivot at column {int(info.item())}")
+        # the unfactored matrix, column-major complex128, for the residual checks
+        Kcm = torch.empty((n, n), dtype=torch.complex128, device=dev)  # Kcm[j, i] = K[i, j]
+        Kcm.copy_(self.t.to(torch.complex128).T)
         self._lu = (Kf, piv, work, npad)
+        self._kcm = Kcm
         return self._lu
 
     def gmres(self, b: np.ndarray, *, atol=1e-6, rtol=1e-5, restart=20, maxiter=None) -> np.ndarray:
@@ -1077,18 +1154,10 @@ class DeviceMatrix:
         Bm = b.reshape(b.shape[0], -1).astype(np.complex128)
         n, nrhs = Bm.shape
         dev = Kf.device
-        lib = _lib.load()
-        out = np.empty_like(Bm)
-        for c0 in range(0, nrhs, 64):
-            c1 = min(nrhs, c0 + 64)
-            Bd = torch.zeros((c1 - c0, npad), dtype=torch.complex128, device=dev)  # column-major npad x nrhs
-            Bd[:, :n] = torch.as_tensor(Bm[:, c0:c1].T.copy(), device=dev)
-            err = torch.zeros(1, dtype=torch.int32, device=dev)
-            _lib.check(lib.bem_zlu_solve(_vp(Kf), npad, npad, npad * npad, 1, _vp(piv), _vp(work), _vp(Bd), npad,
-                                         npad * (c1 - c0), c1 - c0, _vp(err), _lib.stream_ptr()))
-            if int(err.item()) != 0:
-                raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
-            out[:, c0:c1] = Bd[:, :n].T.cpu().numpy()
+        Bd = torch.zeros((1, nrhs, npad), dtype=torch.complex128, device=dev)  # column-major npad x nrhs
+        Bd[0, :, :n] = torch.as_tensor(Bm.T.copy(), device=dev)
+        X = _fp64_checked_solve(self._kcm, n, 0, n, (Kf, piv, work, npad), 1, Bd, nrhs)
+        out = X[0, :, :n].T.cpu().numpy()
         x = out[:, 0] if vec else out.reshape(b.shape)
         return x.astype(np.complex64) if self.t.dtype == torch.complex64 else x
 
@@ -1236,12 +1305,9 @@ class DeviceBlockCirculantMatrix:
         Xd, vec, shape = self._columns(b)
         nrhs = Xd.shape[0]
         Bh = self._to_systems(Xd, npad)
-        err = torch.zeros(1, dtype=torch.int32, device=Bh.device)
-        _lib.check(_lib.load().bem_zlu_solve(_vp(Kf), npad, npad, npad * npad, st.nsys, _vp(piv), _vp(work), _vp(Bh),
-                                             npad, npad * nrhs, nrhs, _vp(err), _lib.stream_ptr()))
-        if int(err.item()) != 0:
-            raise _lib.BemError(_lib.BEM_ERR_TIMEOUT, "bounded wait in the triangular solve timed out")
-        return self._out(self._from_systems(Bh, npad), vec, shape)
+        X = _fp64_checked_solve(self.systems, st.n_sys, st.n_sys * st.n_sys, st.n_sys, (Kf, piv, work, npad),
+                                st.nsys, Bh, nrhs)
+        return self._out(self._from_systems(X, npad), vec, shape)
 
     def gmres(self, b, **kw):
         """capytaine's solve_gmres iterates on the whole operator: the dense

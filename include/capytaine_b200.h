@@ -32,6 +32,7 @@ extern "C" {
 #define BEM_ERR_OUT_OF_MEMORY 6
 #define BEM_ERR_UNSUPPORTED 7     /* option outside the implemented path               */
 #define BEM_ERR_TIMEOUT 8         /* a bounded device-side wait gave up                */
+#define BEM_PENDING 9             /* bem_request_poll: the request is still running    */
 
 /* ---- enums (values of libDelhommeau constants.f90:40-52) ------------------ */
 #define BEM_GRID_LEGACY 0
@@ -227,6 +228,28 @@ int bem_zlu_solve(const void* A_dev, int n, int64_t lda, int64_t stride, int bat
                   const void* work_dev, void* B_dev, int64_t ldb, int64_t strideB, int nrhs, int* err_dev,
                   void* stream);
 
+/* Float64 solve with a residual check: X solves K X = B with the factors of
+ * bem_zlu_factor (LU_dev: the factored copy of K, npad x npad, ldlu, strideLU)
+ * and the residual r = b - K x is evaluated in float64 against the
+ * unfactored K (n x n, ldk, strideK) after each solve; while the worst
+ * relative residual |r| / |b| of a column exceeds tol, x += LU^{-1} r.  The
+ * factorisation pivots inside its 64-row diagonal blocks only, where LAPACK's
+ * zgetrf searches the whole column: this check reports, and the iteration
+ * repairs, any accuracy that the restricted pivoting loses (a well-pivoted
+ * factorisation converges in one iteration).  B, X, R: complex128 npad x nrhs
+ * (rows n..npad-1 of B zero), nrhs <= 16; ts_work_dev sized by
+ * bem_zgemm_ts_workspace_bytes(n, n, nrhs, batch); norms_dev 2*batch*nrhs + 2
+ * doubles; iters_out / resid_out: iterations taken and the final worst
+ * relative residual.  BEM_ERR_NOT_CONVERGED (X holds the last iterate) as
+ * bem_refine_solve.  Replaces zgetrs behind scipy.linalg.lu_solve
+ * (tools/block_circulant_matrices.py:382-385) together with the check that
+ * zgetrf's full-column pivoting makes unnecessary there. */
+int bem_zlu_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, const void* LU_dev, int npad,
+                         int64_t ldlu, int64_t strideLU, int batch, const int* piv_dev, void* lu_work_dev,
+                         const void* B_dev, void* X_dev, void* R_dev, int64_t ldb, int64_t strideB, int nrhs,
+                         double tol, int max_iter, void* ts_work_dev, double* norms_dev, int* err_dev,
+                         int* iters_out, double* resid_out, void* stream);
+
 /* ---- right-hand sides, potentials, forces --------------------------------- */
 /* Columns 0..ndof-1: radiation BC -1j*omega*(dof . n) (dofn_dev: ndof x n);
  * columns ndof..ndof+nhead-1: diffraction BC -(u_Airy . n) in water of depth
@@ -300,6 +323,17 @@ int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, int n, int n
 int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv_dev, void* B_dev, int64_t ldb,
                   int64_t strideB, int nrhs, int* err_dev, void* stream);
 
+/* No counterpart in the reference: a test of the bounded waits.  bem_clu_solve
+ * with the iteration limit of the flag waits of its block substitutions given
+ * (spin_limit > 0 polls of ~64 ns; bem_clu_solve uses 4e6) and, when
+ * withheld_block >= 0, that block row's completion flag never published, so
+ * that every wait on it runs out: each waiting block then sets *err_dev = 1
+ * and finishes (its result is invalid, every access stays in bounds), and the
+ * stream remains usable.  withheld_block = -1 gives bem_clu_solve's result. */
+int bem_clu_solve_bounded(void* work_dev, int npad, int batch, const int* piv_dev, void* B_dev, int64_t ldb,
+                          int64_t strideB, int nrhs, long long spin_limit, int withheld_block, int* err_dev,
+                          void* stream);
+
 /* Iterative refinement: X solves K X = B to a relative residual below tol in
  * every column (residual r = b - K x evaluated in float64 against the float64
  * K, correction from the float32 LU, solved in place in R).  B, X, R:
@@ -365,6 +399,117 @@ int bem_gmres_solve(const void* A_dev, int64_t lda, int64_t strideA, int n, int 
 int bem_block_combine(const void* in_dev, int64_t in_fstride, int64_t in_bstride, int64_t in_cstride, void* out_dev,
                       int64_t out_fstride, int64_t out_bstride, int64_t out_cstride, const void* weights_dev,
                       const int32_t* source_dev, int mi, int mo, int rows, int cols, int nf, void* stream);
+
+/* ---- whole frequency-solves, LU handles, requests ------------------------- */
+/* Opaque handles owned by the library until bem_release. */
+typedef struct bem_context bem_context;
+typedef struct bem_lu bem_lu;
+typedef struct bem_request bem_request;
+
+/* Parameters of the Delhommeau Green function, as the keywords of
+ * Delhommeau.__init__ (green_functions/delhommeau.py:30-41, 116-140): reference
+ * defaults 676, 100.0, 372, -251.0, 1001, BEM_GRID_SCALED_NEMOH3,
+ * BEM_GF_LOW_FREQ.  tabulation_nr or _nz <= 1: no table (direct integration). */
+typedef struct {
+  int32_t tabulation_nr;
+  double tabulation_rmax;
+  int32_t tabulation_nz;
+  double tabulation_zmin;
+  int32_t tabulation_nb_integration_points;
+  int32_t tabulation_grid_shape;  /* BEM_GRID_*                                   */
+  int32_t gf_singularities;       /* BEM_GF_HIGH_FREQ or BEM_GF_LOW_FREQ          */
+} bem_green_function_params;
+
+/* A mesh in host memory, with the per-face arrays capytaine computes
+ * (meshes/geometry.py:35-85) and passes to matrices::build_matrices
+ * (matrices.f90:28-90): the quadrature is the default one point per face (the
+ * centre, weight = area, meshes/meshes.py:472-486).  hull_mask: 1 for hull
+ * faces, 0 for lid faces (irregular-frequency removal, meshes.py:655-737);
+ * NULL: every face is hull. */
+typedef struct {
+  int32_t nb_faces;
+  int32_t nb_vertices;
+  const double* vertices;   /* (nb_vertices, 3)            */
+  const int32_t* faces;     /* (nb_faces, 4), 0-based      */
+  const double* centers;    /* (nb_faces, 3)               */
+  const double* normals;    /* (nb_faces, 3)               */
+  const double* areas;      /* (nb_faces)                  */
+  const double* radii;      /* (nb_faces)                  */
+  const int32_t* hull_mask; /* (nb_faces) or NULL          */
+} bem_mesh_desc;
+
+typedef struct {
+  int32_t iterations;          /* most refinement (or GMRES) iterations of a solve     */
+  double residual;             /* worst final relative residual |b - K x| / |b|         */
+  int32_t escalated_to_gmres;  /* solves whose refinement continued with GMRES         */
+} bem_solve_stats;
+
+/* A context on `device`: the tabulation of the Green function built on the
+ * device (delhommeau.py:208-261, Delhommeau_integrals.f90:190-204) and kept
+ * until bem_release.  Replaces Delhommeau.__init__.  Synchronous. */
+int bem_context_create(int device, const bem_green_function_params* params, bem_context** out);
+/* Copies of the context's grid (nr, nz) and table (nr, nz, 5 C-order) to host
+ * memory (any pointer may be NULL), and replacement of the table by a host copy
+ * (a table loaded from capytaine's npz cache, delhommeau.py:221-251). */
+int bem_context_tabulation(const bem_context* ctx, double* r_range_host, double* z_range_host, double* table_host);
+int bem_context_set_tabulation(bem_context* ctx, const double* table_host);
+
+/* The frequency-solves of one body in infinite depth, host buffers in and out:
+ * for each of the nomega angular frequencies (finite, > 0; k = omega^2 / g),
+ * S and K assembled on the device (the wavenumber-independent Rankine part
+ * once for the call), K factored (precision BEM_PREC_MIXED: float32 block LU
+ * with tcgen05 trailing updates and float64-residual refinement to 1e-10,
+ * continued with preconditioned GMRES when it stops contracting;
+ * BEM_PREC_FP64: float64 block LU with the residual refined to 1e-12), the
+ * radiation problems of the ndof dofs (dof_normals: ndof x nb_faces, the
+ * normal component dof(x_i) . n_i of each dof's motion at the face centres,
+ * problems_and_results.py:440-449) and the diffraction problems of the nhead
+ * wave directions (radians, Airy waves, airy_waves.py:56-95), the potential
+ * S sigma, the forces on the hull faces (bodies/bodies.py:238-250) and the
+ * coefficients (problems_and_results.py:583-592):
+ *   added_mass[w][i][j] = Re F_ij / omega^2, damping[w][i][j] = Im F_ij / omega
+ *   (i the radiating dof, j the influenced one; ndof x ndof per frequency),
+ *   excitation[w][h][j] = diffraction + Froude-Krylov force, complex as
+ *   (re, im) pairs (nhead x ndof x 2 doubles per frequency; NULL if nhead = 0).
+ * ndof + nhead <= 64.  The variant overrides of delhommeau.py:466-490 apply
+ * (faces on the free surface force low_freq).  Synchronous; calls on one
+ * context from several host threads may overlap (each call has its own stream
+ * and buffers).  Replaces the solve_all loop of one body over its problems
+ * (bem/solver.py:268-372) for the indirect method. */
+int bem_solve_frequency(const bem_context* ctx, const bem_mesh_desc* mesh, int nomega, const double* omegas,
+                        int ndof, const double* dof_normals, int nhead, const double* headings, double rho, double g,
+                        int precision, double* added_mass, double* damping, double* excitation,
+                        bem_solve_stats* stats);
+
+/* bem_solve_frequency on a worker thread: returns at once with a request; the
+ * mesh, its arrays and the input and output buffers must stay valid until
+ * bem_request_poll has reported completion.  bem_request_poll(req, wait = 0)
+ * returns BEM_PENDING while the request runs, else its status (wait != 0
+ * blocks until it completes); release the request with bem_release.  No
+ * counterpart in the reference (capytaine runs problems in joblib processes,
+ * bem/solver.py:327-369). */
+int bem_solve_submit(const bem_context* ctx, const bem_mesh_desc* mesh, int nomega, const double* omegas, int ndof,
+                     const double* dof_normals, int nhead, const double* headings, double rho, double g,
+                     int precision, double* added_mass, double* damping, double* excitation, bem_request** out);
+int bem_request_poll(bem_request* req, int wait, bem_solve_stats* stats);
+
+/* LU handle of a complex128 matrix K (n x n, column-major, leading dimension
+ * ldk, device memory): the library copies K (kept for the residuals) and
+ * factors it (precision as bem_solve_frequency).  Replaces lu_decompose /
+ * LUDecomposedMatrix (tools/block_circulant_matrices.py:361-378) behind
+ * DefaultMatrixEngine.linear_solver (bem/engines.py:300-346), which keeps the
+ * factors in its cache in place of K.  Synchronous; BEM_ERR_SINGULAR for a
+ * zero pivot. */
+int bem_lu_factor(const bem_context* ctx, const void* K_dev, int64_t ldk, int n, int precision, bem_lu** out);
+/* X (n x nrhs, ldx, device) solving K X = B (ldb, device) with the handle's
+ * factors, refined against the kept K as bem_solve_frequency's solves.
+ * Replaces lu_solve (tools/block_circulant_matrices.py:382-385).
+ * Synchronous. */
+int bem_lu_solve(bem_lu* lu, const void* B_dev, int64_t ldb, int nrhs, void* X_dev, int64_t ldx,
+                 bem_solve_stats* stats);
+/* Frees a context, an LU handle or a finished request (a running request is
+ * waited for).  NULL is accepted. */
+int bem_release(void* handle);
 
 /* ---- allocation-free variant ---------------------------------------------- */
 /* No counterpart in the reference.  Same operation and arguments as

@@ -30,7 +30,10 @@ def pack_b(B):
     return out
 
 
-@pytest.mark.parametrize("m,n,k,batch", [(128, 128, 16, 1), (256, 384, 64, 2), (512, 256, 128, 1)])
+# the last case has 512 tiles of 128 x 128: more than one per SM, so each CTA of
+# the persistent kernel alternates between its two tensor-memory accumulators
+@pytest.mark.parametrize("m,n,k,batch", [(128, 128, 16, 1), (256, 384, 64, 2), (512, 256, 128, 1),
+                                         (2048, 2048, 64, 2)])
 def test_cgemm_tf32_update(m, n, k, batch):
     import torch
     rng = np.random.default_rng(m + n + k)

@@ -195,7 +195,8 @@ def test_cached_wave_and_block_combine_preconditions_checked_on_host(lib):
     assert b"65535" in lib.bem_last_error()
 
 
-_STRUCTS = {"bem_assembly_args": _lib.AssemblyArgs}
+_STRUCTS = {"bem_assembly_args": _lib.AssemblyArgs, "bem_green_function_params": _lib.GreenFunctionParams,
+            "bem_mesh_desc": _lib.MeshDesc, "bem_solve_stats": _lib.SolveStats}
 
 
 @pytest.mark.parametrize("cname", sorted(_STRUCTS))
@@ -298,6 +299,31 @@ def test_linear_algebra_arguments_checked_on_host(lib):
     assert lib.bem_froude_krylov(100, 1, 1, 0, fake, 1000.0, 9.81, inf, fake, fake, fake, fake, None) == bad
 
 
+def test_frequency_solve_api_arguments_checked_on_host(lib):
+    """The handle-based entry points refuse bad arguments before touching a
+    device, and bem_release only frees handles of this library."""
+    bad = _lib.BEM_ERR_INVALID_ARGUMENT
+    out = ctypes.c_void_p()
+    assert lib.bem_release(None) == _lib.BEM_OK
+    junk = (ctypes.c_uint32 * 16)()  # not a handle
+    assert lib.bem_release(ctypes.addressof(junk)) == bad
+    assert lib.bem_context_create(0, None, ctypes.byref(out)) == bad and out.value is None
+    p = _lib.GreenFunctionParams(676, 100.0, 372, -251.0, 1001, _lib.BEM_GRID_SCALED_NEMOH3,
+                                 _lib.BEM_GF_LOW_FREQ_WITH_RANKINE_PART)
+    assert lib.bem_context_create(0, ctypes.byref(p), ctypes.byref(out)) == bad
+    assert b"gf_singularities" in lib.bem_last_error()
+    mesh = _lib.MeshDesc()
+    w = (ctypes.c_double * 1)(1.0)
+    stats = _lib.SolveStats()
+    assert lib.bem_solve_frequency(None, ctypes.byref(mesh), 1, w, 1, w, 0, None, 1000.0, 9.81, 0, w, w, None,
+                                   ctypes.byref(stats)) == bad
+    assert lib.bem_solve_submit(None, ctypes.byref(mesh), 1, w, 1, w, 0, None, 1000.0, 9.81, 0, w, w, None,
+                                ctypes.byref(out)) == bad
+    assert lib.bem_lu_factor(None, None, 4, 4, 0, ctypes.byref(out)) == bad
+    assert lib.bem_lu_solve(ctypes.addressof(junk), None, 4, 1, None, 4, None) == bad
+    assert lib.bem_request_poll(ctypes.addressof(junk), 0, None) == bad
+
+
 def test_c_program_links_against_the_library(lib):
     """A plain C99 program (not C++) includes the header, links the shared
     library and calls host-side entry points: what a non-Python host does
@@ -312,6 +338,8 @@ int main(void) {
   if (bem_default_z_spacing(372, -251.0, BEM_GRID_SCALED_NEMOH3, z) != BEM_OK) return 3;
   if (bem_assemble(NULL, NULL) != BEM_ERR_INVALID_ARGUMENT) return 4;
   if (bem_zgemm_ts_static_capacity() <= 0) return 5;
+  if (bem_release(NULL) != BEM_OK) return 6;
+  if (bem_context_create(0, NULL, NULL) != BEM_ERR_INVALID_ARGUMENT) return 7;
   printf("%.17g %.17g %s\n", r[675], z[0], bem_last_error());
   return 0;
 }
