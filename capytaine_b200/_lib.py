@@ -127,6 +127,8 @@ _SIGNATURES = {
     "bem_clu_workspace_bytes": ([c_int, c_int], c_i64),
     "bem_clu_factor": ([c_void_p, c_i64, c_i64, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                         c_void_p], c_int),
+    "bem_clu_factor_grouped": ([c_void_p, c_i64, c_i64, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                c_void_p, c_void_p], c_int),
     "bem_clu_solve": ([c_void_p, c_int, c_int, c_void_p, c_void_p, c_i64, c_i64, c_int, c_void_p, c_void_p], c_int),
     "bem_clu_solve_bounded": ([c_void_p, c_int, c_int, c_void_p, c_void_p, c_i64, c_i64, c_int, ctypes.c_longlong,
                                c_int, c_void_p, c_void_p], c_int),

@@ -542,6 +542,78 @@ __device__ __forceinline__ void wave_core(const double x[3], const double xj[3],
   }
 }
 
+// The same wave term with the table interpolation, the asymptotic form and the
+// gradient assembly in float32 (the mixed-precision assembly of a mesh with
+// itself).  r and z, the stencil indices and the distances to the stencil
+// nodes stay float64, so that the stencil is the float64 one and the Lagrange
+// weights lose nothing to cancellation.
+__device__ __forceinline__ float pl2_f(double x, double u1, double u2, double u3) {
+  return ((float)(x - u1) * (float)(x - u2)) / ((float)(u3 - u1) * (float)(u3 - u2));
+}
+__device__ __forceinline__ void integrals_at_f32(double r, double z, const TabView& T, float out[5]) {
+  if (fabs(z) < fabs(T.zlast) && r < T.rmax) {
+    int i = nearest_r_index(r, T.nr, T.rmax, T.grid);
+    i = max(2, min(T.nr - 1, i));
+    int j = nearest_z_index(z, T.nz, T.zlast, T.grid);
+    j = max(2, min(T.nz - 1, j));
+    const int ic = i - 1, jc = j - 1;
+    const double r1 = __ldg(T.r_range + ic - 1), r2 = __ldg(T.r_range + ic), r3 = __ldg(T.r_range + ic + 1);
+    const double z1 = __ldg(T.z_range + jc - 1), z2 = __ldg(T.z_range + jc), z3 = __ldg(T.z_range + jc + 1);
+    const float xl[3] = {pl2_f(r, r2, r3, r1), pl2_f(r, r3, r1, r2), pl2_f(r, r1, r2, r3)};
+    const float zl0 = pl2_f(z, z2, z3, z1), zl1 = pl2_f(z, z3, z1, z2), zl2 = pl2_f(z, z1, z2, z3);
+    float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float* t = T.tab32 + ((size_t)(ic - 1 + a) * T.nz + (jc - 1)) * kNbTab;
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        acc[k] += xl[a] * (__ldg(t + k) * zl0 + __ldg(t + kNbTab + k) * zl1 + __ldg(t + 2 * kNbTab + k) * zl2);
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = acc[k];
+    return;
+  }
+  asymptotic<float>((float)r, (float)z, out);
+}
+__device__ __forceinline__ void wave_core_f32(const double x[3], const double xj[3], double k, const TabView& T,
+                                              int sing, double& gre, double& gim, double dr[3], double di[3]) {
+  const double dx = x[0] - xj[0], dy = x[1] - xj[1];
+  const double r = k * norm2_2(dx, dy);
+  const double z = k * (x[2] + xj[2]);
+  const float rf = (float)r, zf = (float)z;
+  const float r1 = sqrtf(rf * rf + zf * zf);
+  float drdx1 = 0.f, drdx2 = 0.f;
+  if (fabs(r) > 16 * kEpsilon) {
+    const float kk = (float)(k * k) / rf;
+    drdx1 = kk * (float)dx;
+    drdx2 = kk * (float)dy;
+  }
+  const float dzdx3 = (float)k;
+  float I[5];
+  integrals_at_f32(r, z, T, I);
+  float g_re, d0, d1, d2;
+  if (sing == kHighFreq) {
+    g_re = I[1];
+    const float r13 = r1 * r1 * r1;
+    d0 = drdx1 * I[3] - 2.f * drdx1 * rf / r13;
+    d1 = drdx2 * I[3] - 2.f * drdx2 * rf / r13;
+    d2 = dzdx3 * g_re - 2.f * dzdx3 * zf / r13;
+  } else {
+    g_re = I[0];
+    d0 = drdx1 * I[3];
+    d1 = drdx2 * I[3];
+    d2 = (sing == kLowFreq) ? dzdx3 * (g_re + 2.f / r1) : dzdx3 * g_re;
+  }
+  gre = g_re;
+  gim = I[2];
+  dr[0] = d0;
+  dr[1] = d1;
+  dr[2] = d2;
+  di[0] = drdx1 * I[4];
+  di[1] = drdx2 * I[4];
+  di[2] = dzdx3 * I[2];
+}
+
 constexpr int kSymT = 128;    // square tile: 128 rows x 128 columns, one thread per row
 constexpr int kSymChunk = 8;  // columns per mirrored write-back
 
@@ -570,7 +642,9 @@ struct SymBatch {
 // entry is read, then written, by one thread, and no entry is read after
 // another thread wrote it (tile (bi, bj), bi < bj, and its mirror (bj, bi)
 // belong to one CTA), so the read-only cache path is not used for it.
-template <bool GENERAL, bool INPLACE = false>
+// F32: the wave term by wave_core_f32 (float32 interpolation; the cached
+// Rankine part and the accumulation stay float64).
+template <bool GENERAL, bool INPLACE = false, bool F32 = false>
 __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_args a, TabView T, SymBatch kb,
                                                                int gf_sing, const double2* rank, int64_t rank_ld) {
   const int bi = blockIdx.x, bj = blockIdx.y;
@@ -652,7 +726,8 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
         kre = kMinusOneOverFourPi * (rk.y + dn[2] * dz_re);
         kim = kMinusOneOverFourPi * (dn[2] * dz_im);
       } else {
-        wave_core(M, f.x, k, T, gf_sing, gre, gim, dr, di);
+        if constexpr (F32) wave_core_f32(M, f.x, k, T, gf_sing, gre, gim, dr, di);
+        else wave_core(M, f.x, k, T, gf_sing, gre, gim, dr, di);
         const double kwJ = k * f.w;
         double vr[3] = {kwJ * dr[0], kwJ * dr[1], kwJ * dr[2]};
         double vi[3] = {kwJ * di[0], kwJ * di[1], kwJ * di[2]};
@@ -1089,8 +1164,8 @@ int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev
       std::snprintf(msg, sizeof(msg), "%s: wavenumber must be finite and > 0", who);
       return set_error(BEM_ERR_UNSUPPORTED, msg);
     }
-  if (a.out_dtype != BEM_DTYPE_C128 || a.precision != BEM_PREC_FP64) {
-    std::snprintf(msg, sizeof(msg), "%s: complex128 outputs, float64 only", who);
+  if (a.out_dtype != BEM_DTYPE_C128 || (a.precision != BEM_PREC_FP64 && a.precision != BEM_PREC_MIXED)) {
+    std::snprintf(msg, sizeof(msg), "%s: complex128 outputs only", who);
     return set_error(BEM_ERR_UNSUPPORTED, msg);
   }
   if (a.lds < a.n || a.ldk < a.n || ld < a.n) {
@@ -1110,6 +1185,12 @@ int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev
     std::snprintf(msg, sizeof(msg), "%s: nb_integration_points <= 0", who);
     return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
   }
+  // float32 wave term: needs the float32 copy of the table (direct integration stays float64)
+  const bool f32 = a.precision == BEM_PREC_MIXED && tabulated;
+  if (f32 && !a.table32_dev) {
+    std::snprintf(msg, sizeof(msg), "%s: mixed precision needs table32_dev", who);
+    return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
+  }
   const TabView T{a.tabulation_nb_integration_points, a.tabulation_grid_shape, a.nr, a.nz, a.r_range_dev,
                   a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0};
   const int nbi = ceil_div(a.n, kSymT), nbj = ceil_div(general ? a.nb_faces : a.n, kSymT);
@@ -1126,7 +1207,16 @@ int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev
     ak.K_dev = reinterpret_cast<double2*>(a.K_dev) + (size_t)k0 * k_stride;
     {
       TimedLaunch tl(kKAssemble, s);
-      if (general)
+      if (f32 && !general && !inplace)
+        wave_symmetric_kernel<false, false, true><<<dim3(nbi, nbj, cnt), kSymT, 0, s>>>(
+            ak, T, kb, a.gf_singularities, (const double2*)rankine_dev, ld);
+      else if (f32 && !general)
+        wave_symmetric_kernel<false, true, true><<<dim3(nbi, nbj, cnt), kSymT, 0, s>>>(
+            ak, T, kb, a.gf_singularities, (const double2*)rankine_dev, ld);
+      else if (f32)
+        wave_symmetric_kernel<true, false, true><<<dim3(nbi, nbj, cnt), kSymT, 0, s>>>(
+            ak, T, kb, a.gf_singularities, (const double2*)rankine_dev, ld);
+      else if (general)
         wave_symmetric_kernel<true><<<dim3(nbi, nbj, cnt), kSymT, 0, s>>>(ak, T, kb, a.gf_singularities,
                                                                          (const double2*)rankine_dev, ld);
       else if (inplace)

@@ -31,7 +31,8 @@ namespace bem {
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store = 0, const float* Aop1 = nullptr,
-                      const float* Bop1 = nullptr, int max_ctas = 0, long long wait_limit = 0);
+                      const float* Bop1 = nullptr, int max_ctas = 0, long long wait_limit = 0,
+                      const int* limit_host = nullptr);
 
 namespace {
 
@@ -640,8 +641,34 @@ extern "C" int64_t bem_clu_workspace_bytes(int npad, int batch) {
          ((int64_t)batch * nblk + 2) * 4 + 1024;
 }
 
+namespace bem {
+namespace {
+int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch, const int* act,
+                    int* piv_dev, int* info_dev, void* work_dev, int* err_dev, void* stream);
+}
+}  // namespace bem
+
 extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
                               int* piv_dev, int* info_dev, void* work_dev, int* err_dev, void* stream) {
+  return clu_factor_impl(K_dev, ldk, strideK, n, npad, batch, nullptr, piv_dev, info_dev, work_dev, err_dev, stream);
+}
+
+extern "C" int bem_clu_factor_grouped(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
+                                      const int* active_host, int* piv_dev, int* info_dev, void* work_dev,
+                                      int* err_dev, void* stream) {
+  if (!active_host) return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_clu_factor_grouped: null active sizes");
+  for (int b = 0; b < batch; ++b)
+    if (active_host[b] <= 0 || active_host[b] % kB || active_host[b] > npad)
+      return set_error(BEM_ERR_INVALID_ARGUMENT,
+                       "bem_clu_factor_grouped: active sizes must be multiples of 128 in (0, npad]");
+  return clu_factor_impl(K_dev, ldk, strideK, n, npad, batch, active_host, piv_dev, info_dev, work_dev, err_dev,
+                         stream);
+}
+
+namespace bem {
+namespace {
+int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch, const int* act,
+                    int* piv_dev, int* info_dev, void* work_dev, int* err_dev, void* stream) {
   if (!K_dev || !piv_dev || !info_dev || !work_dev || !err_dev || n <= 0 || npad < n || npad % kB || batch <= 0 ||
       ldk < n)
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_clu_factor: bad arguments (npad multiple of 128, >= n)");
@@ -688,14 +715,15 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
                                                                     Bop[buf], w.a3);
       // split TF32: A_hi B_hi + A_lo B_hi + A_hi B_lo, float32-level multipliers
       int st2 = cgemm_tf32_update(w.a3, npad, kk + kB, w.binv, 2 * kB, 0, kSplitK, W.re, W.im, npad, W.stride,
-                                  kk + kB, kk, m, kB, batch, err_dev, on, 1, nullptr, nullptr, side_ctas);
+                                  kk + kB, kk, m, kB, batch, err_dev, on, 1, nullptr, nullptr, side_ctas, 0, act);
       if (st2) return st2;
       clu_pack_kernel<<<dim3(m / 32, batch), 256, 0, on>>>(W, npad, kk, 0, kk + kB, kk, Aop[buf], Bop[buf],
                                                            nullptr);
       // block row of U scaled by the diagonal inverse, U' = A_kk^{-1} A12 (TF32),
       // for the backward substitution only (A12 itself is packed in Bop already)
       st2 = cgemm_tf32_update(w.ainv, kB, 0, Bop[buf], 2 * (int64_t)npad, 2 * (kk + kB), 2 * kB, W.re, W.im, npad,
-                              W.stride, kk, kk + kB, kB, m, batch, err_dev, on, 1, nullptr, nullptr, side_ctas);
+                              W.stride, kk, kk + kB, kB, m, batch, err_dev, on, 1, nullptr, nullptr, side_ctas, 0,
+                              act);
       if (st2) return st2;
     }
     launches += 3;
@@ -708,7 +736,7 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
     if (m <= 0 || nc <= 0) return BEM_OK;
     return cgemm_tf32_update(Aop[buf], npad, r0, Bop[buf], 2 * (int64_t)npad, 2 * c0, 2 * kB, W.re, W.im, npad,
                              W.stride, r0, c0, m, nc, batch, err_dev, s, 0, buf2 >= 0 ? Aop[buf2] : nullptr,
-                             buf2 >= 0 ? Bop[buf2] : nullptr, ctas);
+                             buf2 >= 0 ? Bop[buf2] : nullptr, ctas, 0, act);
   };
   Lookahead* la = nullptr;
   if ((st = lookahead_for(s, &la))) return st;
@@ -743,6 +771,8 @@ extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, i
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
 }
+}  // namespace
+}  // namespace bem
 
 namespace bem {
 // Forward and backward block substitution with the float32 factors, in place on

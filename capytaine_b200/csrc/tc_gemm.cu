@@ -39,7 +39,8 @@ constexpr int kStages = 4;
 constexpr int kABytes = kTM * kKC * 4;   // 16 KiB
 constexpr int kBBytes = kTN * kKC * 4;   // 32 KiB
 constexpr int kStageBytes = kABytes + kBBytes;
-constexpr long long kWaitLimit = 1ll << 22;  // default polls of a bounded mbarrier wait (~ a second)
+constexpr long long kWaitLimit = 1ll << 22;
+constexpr int kMaxGroup = 64;  // matrices of one grouped launch  // default polls of a bounded mbarrier wait (~ a second)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -147,7 +148,31 @@ struct UpdateArgs {
   int tiles_n;
   int ntiles;
   long long wait_limit;  // polls of a bounded mbarrier wait
+  // Grouped launch (ngroup > 0): matrix b has gtm[b] x gtn[b] tiles of its own,
+  // tiles gstart[b] .. gstart[b+1]-1 (matrices of different active sizes)
+  int ngroup;
+  int batch0;  // matrix index of local matrix 0 (operand batch coordinate, C offset)
+  int gstart[kMaxGroup + 1];
+  short gtm[kMaxGroup];
+  short gtn[kMaxGroup];
 };
+
+// Matrix and tile coordinates of tile t of the launch.
+__device__ __forceinline__ void decode_tile(const UpdateArgs& p, int t, int& b, int& tm, int& tn) {
+  if (p.ngroup > 0) {
+    b = 0;
+    while (b + 1 < p.ngroup && p.gstart[b + 1] <= t) ++b;
+    const int r = t - p.gstart[b];
+    tn = r / p.gtm[b];
+    tm = r - tn * p.gtm[b];
+    return;
+  }
+  const int per_matrix = p.tiles_m * p.tiles_n;
+  b = t / per_matrix;
+  const int r = t - b * per_matrix;
+  tn = r / p.tiles_m;
+  tm = r - tn * p.tiles_m;
+}
 
 constexpr int kEpiWarps = 16;                  // 4 lane quarters x 4 groups of 64 accumulator columns
 constexpr int kThreads = 32 * (2 + kEpiWarps);  // producer warp, MMA warp, epilogue warps
@@ -216,7 +241,6 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  const int per_matrix = p.tiles_m * p.tiles_n;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -224,8 +248,9 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
       bool ok = true;
       long long g = 0;  // stage uses so far
       for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
-        const int b = t / per_matrix, r = t - b * per_matrix;
-        const int tn = r / p.tiles_m, tm = r - tn * p.tiles_m;
+        int b, tm, tn;
+        decode_tile(p, t, b, tm, tn);
+        b += p.batch0;
         for (int kc = 0; kc < p.nk; ++kc, ++g) {
           const int s = (int)(g % kStages);
           const uint32_t use = (uint32_t)(g / kStages);
@@ -288,8 +313,9 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
     bool ok = true;
     int i = 0;
     for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++i) {
-      const int b = t / per_matrix, r = t - b * per_matrix;
-      const int tn = r / p.tiles_m, tm = r - tn * p.tiles_m;
+      int b, tm, tn;
+      decode_tile(p, t, b, tm, tn);
+      b += p.batch0;
       const int acc = i & 1;
       const int row = p.c_row0 + tm * kTM + 32 * q + lane;
       float* C = (plane ? p.Ci : p.Cr) + (size_t)b * p.c_stride + row +
@@ -393,7 +419,7 @@ int num_sms(int* out) {
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store, const float* Aop1,
-                      const float* Bop1, int max_ctas, long long wait_limit) {
+                      const float* Bop1, int max_ctas, long long wait_limit, const int* limit_host) {
   if (m <= 0 || n <= 0) return BEM_OK;
   if (m % kTM || n % kTNc || kp % kKC || (a_row0 % 8) || (b_row0 % 8))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: sizes must be multiples of 128 (K' of 32)");
@@ -418,18 +444,56 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
   if ((st = num_sms(&sms))) return st;
   const int nk0 = kp / kKC;
   const int tiles_m = m / kTM, tiles_n = n / kTNc;
-  const long long ntiles = (long long)tiles_m * tiles_n * batch;
-  if (ntiles > (1ll << 30)) return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: too many tiles");
-  int ctas = max_ctas > 0 ? std::min(max_ctas, sms) : sms;
-  ctas = (int)std::min<long long>(ctas, ntiles);
-  UpdateArgs p{a_row0,  b_row0,  c_row0,  c_col0, Aop1 ? 2 * nk0 : nk0, nk0,           Cr,
-               Ci,      ldc,     c_stride, err,   store,               tiles_m,       tiles_n,
-               (int)ntiles, wait_limit > 0 ? wait_limit : kWaitLimit};
-  {
-    TimedLaunch tl(kKCgemmTf32, stream);
-    cgemm_tf32_update_kernel<<<ctas, kThreads, smem, stream>>>(mapA, mapB, mapA1, mapB1, p);
+  UpdateArgs p{};
+  p.a_row0 = a_row0;
+  p.b_row0 = b_row0;
+  p.c_row0 = c_row0;
+  p.c_col0 = c_col0;
+  p.nk = Aop1 ? 2 * nk0 : nk0;
+  p.nk0 = nk0;
+  p.Cr = Cr;
+  p.Ci = Ci;
+  p.ldc = ldc;
+  p.c_stride = c_stride;
+  p.err = err;
+  p.store = store;
+  p.tiles_m = tiles_m;
+  p.tiles_n = tiles_n;
+  p.wait_limit = wait_limit > 0 ? wait_limit : kWaitLimit;
+  int launches = 0;
+  // Grouped: matrix b covers only rows and columns below limit_host[b] (its
+  // active size), launches of at most kMaxGroup matrices
+  for (int b0 = 0; b0 < batch; b0 += limit_host ? kMaxGroup : batch) {
+    const int nb = limit_host ? std::min(kMaxGroup, batch - b0) : batch;
+    long long ntiles = (long long)tiles_m * tiles_n * nb;
+    if (limit_host) {
+      p.ngroup = nb;
+      ntiles = 0;
+      for (int i = 0; i < nb; ++i) {
+        const int lim = limit_host[b0 + i];
+        const int mb = std::max(0, std::min(m, lim - c_row0)) / kTM;
+        const int nbc = std::max(0, std::min(n, lim - c_col0)) / kTNc;
+        p.gtm[i] = (short)std::max(mb, 1);  // never divides by zero; no tile when gtn is 0
+        p.gtn[i] = (short)(mb > 0 ? nbc : 0);
+        p.gstart[i] = (int)ntiles;
+        ntiles += (long long)(mb > 0 ? mb : 0) * (mb > 0 ? nbc : 0);
+      }
+      p.gstart[nb] = (int)ntiles;
+    }
+    if (ntiles > (1ll << 30)) return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: too many tiles");
+    if (ntiles == 0) continue;
+    p.ntiles = (int)ntiles;
+    int ctas = max_ctas > 0 ? std::min(max_ctas, sms) : sms;
+    ctas = (int)std::min<long long>(ctas, ntiles);
+    UpdateArgs q = p;
+    q.batch0 = b0;  // the matrices of this launch: b0 .. b0 + nb - 1
+    {
+      TimedLaunch tl(kKCgemmTf32, stream);
+      cgemm_tf32_update_kernel<<<ctas, kThreads, smem, stream>>>(mapA, mapB, mapA1, mapB1, q);
+    }
+    ++launches;
   }
-  count_launches(1);
+  count_launches(launches);
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
 }
@@ -447,5 +511,6 @@ extern "C" int bem_cgemm_tf32_update(const float* Aop_dev, int64_t a_rows, int a
   if ((reinterpret_cast<uintptr_t>(Aop_dev) | reinterpret_cast<uintptr_t>(Bop_dev)) & 15)
     return bem::set_error(BEM_ERR_INVALID_ARGUMENT, "bem_cgemm_tf32_update: operands must be 16-byte aligned");
   return bem::cgemm_tf32_update(Aop_dev, a_rows, a_row0, Bop_dev, b_rows, b_row0, kp, Cr_dev, Ci_dev, ldc, c_stride,
-                                c_row0, c_col0, m, n, batch, err_dev, (cudaStream_t)stream, 0, nullptr, nullptr, 0, 0);
+                                c_row0, c_col0, m, n, batch, err_dev, (cudaStream_t)stream, 0, nullptr, nullptr, 0, 0,
+                                nullptr);
 }

@@ -41,6 +41,9 @@ RHS_CHUNK = 16  # right-hand sides per refinement / GMRES / tall-GEMM call
 # solve whose residual stops decreasing above it (the float64 floor of an
 # ill-conditioned K) is accepted up to the engine's refine_tol.
 FP64_RESIDUAL_TOL = 1e-12
+# assembly_precision="auto": float32 wave term from this k L on (L the body's
+# horizontal size).
+FLOAT32_WAVE_MIN_KL = 2.0
 
 
 def padded_size(n: int) -> int:
@@ -351,8 +354,8 @@ class B200Engine:
                  method: str = "indirect"):
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
-        if assembly_precision not in ("fp64", "mixed"):
-            raise ValueError("assembly_precision must be 'fp64' or 'mixed'")
+        if assembly_precision not in ("fp64", "mixed", "auto"):
+            raise ValueError("assembly_precision must be 'fp64', 'mixed' or 'auto'")
         if not callable(linear_solver) and linear_solver not in ("lu_decomposition",
                                                                  "lu_decomposition_with_overwrite", "gmres"):
             raise NotImplementedError(f"Unknown `linear_solver` in B200Engine: {linear_solver}")
@@ -534,8 +537,9 @@ class B200Engine:
             ws.r.flags.zero_()
             cstride = N * st.n_sub
             gf.assemble_into(full, st.submesh, ws.cols[0, 0], ws.cols[1, 0], wavenumber=ks[0], lds=N, ldk=N,
-                             nan_flag=ws.r.nan, precision=self.assembly_precision, adjoint_double_layer=adjoint,
-                             sweep=(ks, cstride, cstride), water_depth=water_depth)
+                             nan_flag=ws.r.nan,
+                             precision="fp64" if self.assembly_precision == "auto" else self.assembly_precision,
+                             adjoint_double_layer=adjoint, sweep=(ks, cstride, cstride), water_depth=water_depth)
             ws.combine_matrices(ws.cols[0], nb, f.S, st.n_sys, st.n_sys * st.n_sys, stream)
             ws.combine_matrices(ws.cols[1], nb, f.K, f.ldk, f.strideK, stream)
             if ev:
@@ -573,16 +577,37 @@ class B200Engine:
         lds = n if lds is None else lds
         ks = [float(k) for k in ks]
         adjoint = self.method == "indirect"  # K (adjoint double layer) or D
+        precs = [self._wave_precision(mesh, k, water_depth) for k in ks]
         if len(ks) > 1 and all(0.0 < k < np.inf for k in ks):
-            gf.assemble_into(mesh, mesh, f.S[first], f.K[first], wavenumber=ks[0], lds=lds, ldk=f.ldk,
-                             nan_flag=nan_flag, precision=self.assembly_precision, reuse_rankine=reuse_rankine,
-                             sweep=(ks, f.S.shape[1], f.K.shape[1]), adjoint_double_layer=adjoint,
-                             water_depth=water_depth)
+            # one sweep call per run of consecutive wavenumbers of the same precision
+            i = 0
+            while i < len(ks):
+                j = i
+                while j < len(ks) and precs[j] == precs[i]:
+                    j += 1
+                gf.assemble_into(mesh, mesh, f.S[first + i], f.K[first + i], wavenumber=ks[i], lds=lds,
+                                 ldk=f.ldk, nan_flag=nan_flag, precision=precs[i], reuse_rankine=reuse_rankine,
+                                 sweep=(ks[i:j], f.S.shape[1], f.K.shape[1]), adjoint_double_layer=adjoint,
+                                 water_depth=water_depth)
+                i = j
             return
         for b, k in enumerate(ks):
             gf.assemble_into(mesh, mesh, f.S[first + b], f.K[first + b], wavenumber=k, lds=lds, ldk=f.ldk,
-                             nan_flag=nan_flag, precision=self.assembly_precision, reuse_rankine=reuse_rankine,
+                             nan_flag=nan_flag, precision=precs[b], reuse_rankine=reuse_rankine,
                              adjoint_double_layer=adjoint, water_depth=water_depth)
+
+    def _wave_precision(self, mesh, k, water_depth=np.inf):
+        """Precision of the wave term at wavenumber k: assembly_precision, or
+        with "auto" float32 once k times the body's horizontal size reaches
+        FLOAT32_WAVE_MIN_KL (below, the damping carried by the O(k)-small
+        imaginary parts needs the float64 wave term)."""
+        if self.assembly_precision != "auto":
+            return self.assembly_precision
+        if water_depth != np.inf or not (0.0 < k < np.inf):
+            return "fp64"
+        c = mesh.faces_centers
+        size = float(np.hypot(np.ptp(c[:, 0]), np.ptp(c[:, 1])))
+        return "mixed" if k * size >= FLOAT32_WAVE_MIN_KL else "fp64"
 
     def factor_stage(self, f: "_Factors", nb, err):
         """LU of K (float64 DMMA, or float32 tcgen05 for the mixed engine); none for plain GMRES."""

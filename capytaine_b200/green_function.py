@@ -396,13 +396,16 @@ class Delhommeau:
         same_mesh = hasattr(mesh1, "faces_centers") and mesh1.content_hash == mesh2.content_hash
         if (reuse_rankine and same_mesh and dm2.collocation_at_quadrature and all_wave
                 and sing in ("low_freq", "high_freq")
-                and prec == "fp64" and dtype == _lib.BEM_DTYPE_C128 and early_dot_product
-                and 16 * n * n <= self.rankine_cache_bytes):
-            # Rankine part reused across wavenumbers; wave term once per pair of faces.
+                and (prec == "fp64" or (prec == "mixed" and nr > 1 and nz > 1)) and dtype == _lib.BEM_DTYPE_C128
+                and early_dot_product and 16 * n * n <= self.rankine_cache_bytes):
+            # Rankine part reused across wavenumbers (float64 always); wave term
+            # once per pair of faces (float32 interpolation with "mixed").
             q = dm2.quad_points.data_ptr()
             a.points_dev = a.centers_dev = a.quad_points_dev = q
+            a.precision = _lib.BEM_PREC_FP64
             rank = self._rankine_part(mesh2.content_hash, dm2, a, bool(adjoint_double_layer), sing,
                                       float(free_surface), stream)
+            a.precision = _lib.BEM_PREC_MIXED if prec == "mixed" else _lib.BEM_PREC_FP64
             if sweep is not None:
                 ks, s_stride, k_stride = sweep
                 kh = np.ascontiguousarray(np.asarray(ks, dtype=np.float64))

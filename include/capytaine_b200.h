@@ -319,6 +319,18 @@ int64_t bem_clu_workspace_bytes(int npad, int batch);
 int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch, int* piv_dev,
                    int* info_dev, void* work_dev, int* err_dev, void* stream);
 
+/* bem_clu_factor for a batch of matrices of different sizes held in one
+ * padded batch: matrix b is identity-padded beyond its active size
+ * active_host[b] (a multiple of 128, <= npad; host array), and the
+ * tensor-core updates skip every tile beyond it (those updates are exact
+ * no-ops: the padding's off-diagonal blocks are zero), so each matrix costs
+ * the flops of its own size.  Same factors as bem_clu_factor, bit for bit.
+ * No counterpart in the reference (capytaine solves one problem at a time,
+ * bem/solver.py:327-369). */
+int bem_clu_factor_grouped(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
+                           const int* active_host, int* piv_dev, int* info_dev, void* work_dev, int* err_dev,
+                           void* stream);
+
 /* B <- (LU)^{-1} B with the float32 block factors; B complex128 (npad x nrhs, ldb); piv_dev reserved. */
 int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv_dev, void* B_dev, int64_t ldb,
                   int64_t strideB, int nrhs, int* err_dev, void* stream);

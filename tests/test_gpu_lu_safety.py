@@ -181,3 +181,55 @@ def test_bounded_wait_arguments_checked():
     st = lib.bem_clu_solve_bounded(_vp(buf), 256, 1, _vp(buf), _vp(buf), 256, 256, 1, 100, 2, _vp(buf),
                                    _lib.stream_ptr())
     assert st == _lib.BEM_ERR_INVALID_ARGUMENT
+
+
+def test_grouped_factorisation_equals_the_padded_one():
+    """Matrices of different sizes in one padded batch: the grouped
+    factorisation (tiles beyond each matrix's active size skipped) gives the
+    factors of the plain batched one bit for bit, and solves each system."""
+    import torch
+    lib = _lib.load()
+    rng = np.random.default_rng(21)
+    npad, nrhs = 640, 2
+    sizes = [250, 640, 380, 129]
+    active = (ctypes.c_int32 * len(sizes))(*[-(-m // 128) * 128 for m in sizes])
+    batch = len(sizes)
+    K = torch.zeros((batch, npad, npad), dtype=torch.complex128, device="cuda")  # K[b].T column-major
+    mats, rhs = [], []
+    for b, m in enumerate(sizes):
+        A = _dominant(m, rng)
+        mats.append(A)
+        K[b].T[:m, :m] = torch.as_tensor(A)
+        K[b].T[m:, m:] = torch.eye(npad - m, dtype=torch.complex128)  # identity padding
+        rhs.append(rng.standard_normal((m, nrhs)) + 1j * rng.standard_normal((m, nrhs)))
+    B = torch.zeros((batch, nrhs, npad), dtype=torch.complex128, device="cuda")
+    for b, m in enumerate(sizes):
+        B[b, :, :m] = torch.as_tensor(rhs[b].T)
+    s = _lib.stream_ptr()
+    out = []
+    for grouped in (False, True):
+        nbytes = int(lib.bem_clu_workspace_bytes(npad, batch))
+        work = torch.empty(nbytes + 1024, dtype=torch.uint8, device="cuda")
+        wptr = (work.data_ptr() + 1023) // 1024 * 1024
+        piv = torch.zeros((batch, npad), dtype=torch.int32, device="cuda")
+        info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        if grouped:
+            _lib.check(lib.bem_clu_factor_grouped(_vp(K), npad, npad * npad, npad, npad, batch, active, _vp(piv),
+                                                  _vp(info), _vp(wptr), _vp(err), s))
+        else:
+            _lib.check(lib.bem_clu_factor(_vp(K), npad, npad * npad, npad, npad, batch, _vp(piv), _vp(info),
+                                          _vp(wptr), _vp(err), s))
+        X = B.clone()
+        _lib.check(lib.bem_clu_solve(_vp(wptr), npad, batch, _vp(piv), _vp(X), npad, npad * nrhs, nrhs, _vp(err), s))
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0 and info.cpu().numpy().tolist() == [0] * batch
+        out.append(X)
+    assert torch.equal(out[0], out[1])
+    for b, m in enumerate(sizes):
+        x = out[1][b, :, :m].T.cpu().numpy()
+        ref = np.linalg.solve(mats[b], rhs[b])
+        assert np.abs(x - ref).max() / np.abs(ref).max() < 5e-3
+    bad = (ctypes.c_int32 * batch)(128, 100, 128, 128)  # not a multiple of 128
+    assert lib.bem_clu_factor_grouped(_vp(K), npad, npad * npad, npad, npad, batch, bad, _vp(piv), _vp(info),
+                                      _vp(wptr), _vp(err), s) == _lib.BEM_ERR_INVALID_ARGUMENT
