@@ -96,6 +96,28 @@ def wavenumbers(omegas, water_depth: float = np.inf, g: float = 9.81) -> np.ndar
     return out
 
 
+def band_batches(sizes, nq, band, capacity):
+    """Batches of (body, omega index) pairs for the grouped factorisation:
+    bodies in decreasing padded size (sizes[i]), the nq frequencies of each
+    together, a new batch when a body is smaller than the batch's largest
+    divided by band or when the batch holds capacity(largest) pairs.
+    Returns [(padded size of the batch, [(i, q), ...]), ...]."""
+    order = sorted(range(len(sizes)), key=lambda i: (-sizes[i], i))
+    out, cur, top, cap = [], [], 0, 0
+    for i in order:
+        for q in range(nq):
+            if cur and (sizes[i] * band < top or len(cur) >= cap):
+                out.append((top, cur))
+                cur = []
+            if not cur:
+                top = sizes[i]
+                cap = max(1, int(capacity(top)))
+            cur.append((i, q))
+    if cur:
+        out.append((top, cur))
+    return out
+
+
 @dataclass
 class FrequencyResults:
     """Coefficients of a frequency sweep.  Arrays are indexed [omega, ...]:
@@ -351,7 +373,7 @@ class B200Engine:
                  linear_solver="lu_decomposition", max_batch: int = 8, device=None,
                  refine_tol: float = 1e-10, refine_max_iter: int = 30, assembly_precision: str = "fp64",
                  refinement: str = "classical", gmres_restart: int = 20, gmres_maxiter: Optional[int] = None,
-                 method: str = "indirect"):
+                 method: str = "indirect", batch_tuner=None):
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         if assembly_precision not in ("fp64", "mixed", "auto"):
@@ -382,6 +404,9 @@ class B200Engine:
         self.green_function = green_function if green_function is not None else Delhommeau()
         self._linear_solver = linear_solver
         self.max_batch = int(max_batch)
+        # matrices per grouped factorisation of solve_bodies, per size class
+        from .tuning import DEFAULT_TUNER
+        self.batch_tuner = batch_tuner if batch_tuner is not None else DEFAULT_TUNER
         self._device = device
         self._ws: Dict[tuple, _Workspace] = {}
         self._body_cache: "OrderedDict[tuple, tuple]" = OrderedDict()
@@ -609,12 +634,18 @@ class B200Engine:
         size = float(np.hypot(np.ptp(c[:, 0]), np.ptp(c[:, 1])))
         return "mixed" if k * size >= FLOAT32_WAVE_MIN_KL else "fp64"
 
-    def factor_stage(self, f: "_Factors", nb, err):
-        """LU of K (float64 DMMA, or float32 tcgen05 for the mixed engine); none for plain GMRES."""
+    def factor_stage(self, f: "_Factors", nb, err, active=None):
+        """LU of K (float64 DMMA, or float32 tcgen05 for the mixed engine); none
+        for plain GMRES.  active (mixed engine): each matrix's own padded size,
+        the rest of it identity padding, for the grouped LU."""
         lib = _lib.load()
         stream = _lib.stream_ptr()
         n, npad = f.n, f.npad
-        if self.precision == "mixed":
+        if self.precision == "mixed" and active is not None:
+            act = (ctypes.c_int32 * nb)(*[int(min(a, npad)) for a in active])
+            _lib.check(lib.bem_clu_factor_grouped(_vp(f.K), n, n * n, n, npad, nb, act, _vp(f.piv), _vp(f.info),
+                                                  _vp(f.lu_work_ptr), _vp(err), stream))
+        elif self.precision == "mixed":
             _lib.check(lib.bem_clu_factor(_vp(f.K), n, n * n, n, npad, nb, _vp(f.piv), _vp(f.info),
                                           _vp(f.lu_work_ptr), _vp(err), stream))
         elif not self._plain_gmres:
@@ -765,95 +796,128 @@ class B200Engine:
     # ---- many bodies --------------------------------------------------------
     def solve_bodies(self, bodies, omegas: Sequence[float], *, wave_directions: Sequence[float] = (0.0,),
                      rho: float = 1000.0, g: float = 9.81, water_depth: float = np.inf, batch_bytes: float = 8e9,
-                     sync_stats: bool = False) -> List[FrequencyResults]:
+                     sync_stats: bool = False, grouping: Optional[str] = None,
+                     band: float = 1.3) -> List[FrequencyResults]:
         """Frequency sweeps of many bodies of uneven panel counts, batched
-        across bodies: bodies whose size rounds up to the same multiple of the
-        LU block (128 for the mixed engine, 64 for float64) form one group,
-        every matrix of the group is identity-padded to that size (the padded
-        unknowns are zero and change nothing), and the (body, omega) pairs of a
-        group are assembled, factored and solved in batches of as many matrices
-        as fit in batch_bytes.  Returns one FrequencyResults per body, in order
-        (what solve_frequencies returns for that body).  With max_batch or more
-        frequencies a body fills batches of its own: each body then runs its
-        own sweep (measured faster: no padding, and a frequency that needs the
-        GMRES fallback holds up its own batch only).  water_depth as in
-        solve_frequencies."""
-        import torch
+        across bodies.  Returns one FrequencyResults per body, in order (what
+        solve_frequencies returns for that body); water_depth as in
+        solve_frequencies.
+
+        grouping "bands" (the default of the mixed engine): the (body, omega)
+        pairs, largest bodies first, fill batches whose sizes lie within a
+        factor `band` of the batch's largest; every matrix is identity-padded
+        to that size and factored by the grouped LU
+        (bem_clu_factor_grouped), whose tensor-core updates stop at each
+        matrix's own size, so a small body in a batch costs the update flops
+        of its own size.  The batch size per size class comes from
+        BatchTuner (timed once per class, cached).
+        grouping "size" (the float64 engine's): bodies whose size rounds up to
+        the same multiple of the LU block form one group, factored together;
+        with max_batch or more frequencies each body runs its own sweep."""
         if not water_depth > 0:
             raise ValueError(f"water_depth must be > 0 (got {water_depth})")
         omegas = np.asarray(omegas, dtype=float)
-        if len(omegas) >= self.max_batch:
+        grouping = grouping or ("bands" if self.precision == "mixed" else "size")
+        if grouping not in ("bands", "size"):
+            raise ValueError("grouping must be 'bands' or 'size'")
+        if grouping == "bands" and self.precision != "mixed":
+            raise ValueError("grouping='bands' needs the mixed engine (grouped LU)")
+        if grouping == "size" and len(omegas) >= self.max_batch:
             return [self.solve_frequencies(b, omegas, wave_directions=wave_directions, rho=rho, g=g,
                                            water_depth=water_depth) for b in bodies]
         heads = np.asarray(wave_directions, dtype=float)
         nhead = len(heads)
         blk = 128 if self.precision == "mixed" else 64
-        groups: Dict[int, List[int]] = {}
-        for i, b in enumerate(bodies):
-            n = b.mesh_including_lid.nb_faces
-            groups.setdefault(-(-n // blk) * blk, []).append(i)
-        F_all = [np.zeros((len(omegas), len(b.dofs) + nhead, len(b.dofs)), dtype=np.complex128) for b in bodies]
-        FK_all = [np.zeros((len(omegas), max(nhead, 1), len(b.dofs)), dtype=np.complex128) for b in bodies]
-        stats = {"groups": len(groups), "batches": 0, "assembly_ms": 0.0, "lu_ms": 0.0, "solve_ms": 0.0}
+        sizes = [-(-b.mesh_including_lid.nb_faces // blk) * blk for b in bodies]
+        nq = len(omegas)
+        plan = []  # (npad, nrhs, pairs, B, need, grouped)
+        if grouping == "size":
+            groups: Dict[int, List[int]] = {}
+            for i, npad in enumerate(sizes):
+                groups.setdefault(npad, []).append(i)
+            for npad, idxs in sorted(groups.items()):
+                nrhs = max(len(bodies[i].dofs) for i in idxs) + nhead
+                pairs = [(i, q) for i in idxs for q in range(nq)]
+                B = int(max(1, min(len(pairs), batch_bytes // _Factors.estimate_bytes(npad, 1, self.precision))))
+                for c0 in range(0, len(pairs), B):
+                    plan.append((npad, nrhs, pairs[c0:c0 + B], B, False))
+        else:
+            for npad, pairs in band_batches(sizes, nq, band,
+                                            lambda top: self.batch_tuner.batch_for(self, top, batch_bytes)):
+                plan.append((npad, max(len(bodies[i].dofs) for i, _ in pairs) + nhead, pairs, len(pairs), True))
+        need = max(_Factors.estimate_bytes(npad, B, self.precision) + _Rhs.estimate_bytes(npad, npad, B, nrhs)
+                   + 64 * (1 << 16) for npad, nrhs, _, B, _ in plan)
+        F_all = [np.zeros((nq, len(b.dofs) + nhead, len(b.dofs)), dtype=np.complex128) for b in bodies]
+        FK_all = [np.zeros((nq, max(nhead, 1), len(b.dofs)), dtype=np.complex128) for b in bodies]
+        stats = {"groups": len({p[0] for p in plan}), "batches": 0, "assembly_ms": 0.0, "lu_ms": 0.0,
+                 "solve_ms": 0.0, "grouping": grouping}
+        arena = DeviceArena(need, self.device)  # one arena: no device allocation between batches
+        shape = None
+        f = r = release = None
+        for npad, nrhs, chunk, B, grouped in plan:
+            if shape != (npad, nrhs, B):
+                if release is not None:
+                    del f, r
+                    release()  # the previous batches' work completed: their results reached the host
+                alloc, release = arena.allocator()
+                f = _Factors(npad, B, self.device, self.precision, alloc=alloc)
+                r = _Rhs(npad, npad, B, nrhs, self.device, self.precision, alloc=alloc)
+                shape = (npad, nrhs, B)
+            self._solve_body_batch(bodies, omegas, heads, chunk, f, r, npad,
+                                   [sizes[i] for i, _ in chunk] if grouped else None, rho, g, water_depth,
+                                   stats, F_all, FK_all, sync_stats)
+        if release is not None:
+            del f, r
+            release()
+        return [self._coefficients(b, omegas, heads, F_all[i], FK_all[i], dict(stats)) for i, b in enumerate(bodies)]
+
+    def _solve_body_batch(self, bodies, omegas, heads, chunk, f, r, npad, active, rho, g, water_depth, stats,
+                          F_all, FK_all, sync_stats):
+        """One batch of solve_bodies: the (body, omega) pairs of chunk, each
+        body's matrices identity-padded to npad (active: each matrix's own
+        padded size for the grouped LU, or None)."""
+        import torch
         lib = _lib.load()
         stream = _lib.stream_ptr()
-        plan = []
-        for npad, idxs in sorted(groups.items()):
-            nrhs = max(len(bodies[i].dofs) for i in idxs) + nhead
-            pairs = [(i, q) for i in idxs for q in range(len(omegas))]
-            B = int(max(1, min(len(pairs), batch_bytes // _Factors.estimate_bytes(npad, 1, self.precision))))
-            need = (_Factors.estimate_bytes(npad, B, self.precision) + _Rhs.estimate_bytes(npad, npad, B, nrhs)
-                    + 64 * (1 << 16))
-            plan.append((npad, idxs, nrhs, pairs, B, need))
-        # one arena for the largest group: no device allocation between groups
-        arena = DeviceArena(max(p[-1] for p in plan), self.device)
-        for npad, idxs, nrhs, pairs, B, _ in plan:
-            alloc, release = arena.allocator()
-            f = _Factors(npad, B, self.device, self.precision, alloc=alloc)
-            r = _Rhs(npad, npad, B, nrhs, self.device, self.precision, alloc=alloc)
-            for start in range(0, len(pairs), B):
-                chunk = pairs[start:start + B]
-                nb = len(chunk)
-                segments = []
-                for j, (i, q) in enumerate(chunk):
-                    if segments and segments[-1][0] is bodies[i]:
-                        segments[-1][2] += 1
-                    else:
-                        segments.append([bodies[i], j, 1])
-                om = omegas[[q for _, q in chunk]]
-                ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)] if sync_stats else None
-                if ev:
-                    ev[0].record()
-                r.flags.zero_()
-                for body, j0, m in segments:
-                    mesh = body.mesh_including_lid
-                    self.assemble_stage(f, mesh, wavenumbers(om[j0:j0 + m], water_depth, g), nan_flag=r.nan,
-                                        first=j0, lds=npad, water_depth=water_depth)
-                    if mesh.nb_faces < npad:
-                        for M in (f.S, f.K):  # zero rows/columns, unit diagonal beyond the body's panels
-                            _lib.check(lib.bem_zpad_identity(_vp(M.data_ptr() + 16 * j0 * npad * npad), npad,
-                                                             npad * npad, m, mesh.nb_faces, npad, stream))
-                if ev:
-                    ev[1].record()
-                self.factor_stage(f, nb, r.err)
-                if ev:
-                    ev[2].record()
-                out = self._solve_segments(f, r, [tuple(sg) for sg in segments], om, heads, rho=rho, g=g,
-                                           stats=stats, events=ev, water_depth=water_depth)
-                for (body, j0, m), (F, FK) in zip(segments, out):
-                    i = chunk[j0][0]
-                    qs = [q for _, q in chunk[j0:j0 + m]]
-                    F_all[i][qs] = F
-                    FK_all[i][qs, :nhead] = FK
-                stats["batches"] += 1
-                if ev:
-                    torch.cuda.synchronize()
-                    stats["assembly_ms"] += ev[0].elapsed_time(ev[1])
-                    stats["lu_ms"] += ev[1].elapsed_time(ev[2])
-                    stats["solve_ms"] += ev[2].elapsed_time(ev[4])
-            del f, r
-            release()  # the group's work has completed: its results were copied to the host
-        return [self._coefficients(b, omegas, heads, F_all[i], FK_all[i], dict(stats)) for i, b in enumerate(bodies)]
+        nhead = len(heads)
+        nb = len(chunk)
+        segments = []
+        for j, (i, q) in enumerate(chunk):
+            if segments and segments[-1][0] is bodies[i]:
+                segments[-1][2] += 1
+            else:
+                segments.append([bodies[i], j, 1])
+        om = omegas[[q for _, q in chunk]]
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)] if sync_stats else None
+        if ev:
+            ev[0].record()
+        r.flags.zero_()
+        for body, j0, m in segments:
+            mesh = body.mesh_including_lid
+            self.assemble_stage(f, mesh, wavenumbers(om[j0:j0 + m], water_depth, g), nan_flag=r.nan,
+                                first=j0, lds=npad, water_depth=water_depth)
+            if mesh.nb_faces < npad:
+                for M in (f.S, f.K):  # zero rows/columns, unit diagonal beyond the body's panels
+                    _lib.check(lib.bem_zpad_identity(_vp(M.data_ptr() + 16 * j0 * npad * npad), npad,
+                                                     npad * npad, m, mesh.nb_faces, npad, stream))
+        if ev:
+            ev[1].record()
+        self.factor_stage(f, nb, r.err, active=active)
+        if ev:
+            ev[2].record()
+        out = self._solve_segments(f, r, [tuple(sg) for sg in segments], om, heads, rho=rho, g=g,
+                                   stats=stats, events=ev, water_depth=water_depth)
+        for (body, j0, m), (F, FK) in zip(segments, out):
+            i = chunk[j0][0]
+            qs = [q for _, q in chunk[j0:j0 + m]]
+            F_all[i][qs] = F
+            FK_all[i][qs, :nhead] = FK
+        stats["batches"] += 1
+        if ev:
+            torch.cuda.synchronize()
+            stats["assembly_ms"] += ev[0].elapsed_time(ev[1])
+            stats["lu_ms"] += ev[1].elapsed_time(ev[2])
+            stats["solve_ms"] += ev[2].elapsed_time(ev[4])
 
     def _refine(self, f, r, nb, Bc, Xc, Rc, nc, stats, stream):
         """Refined solve of nc columns (B, X, R column pointers, batch stride
