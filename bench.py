@@ -101,7 +101,7 @@ def scaled_body(body, factors, name):
     return FloatingBody(m, body.dofs, name=name)
 
 
-def run_serving(engine, bodies, *, rate, n_requests, seed, slots, repeat_frac=0.2):
+def run_serving(engine, bodies, *, rate, n_requests, seed, slots, repeat_frac=0.2, batch_max=1):
     """Poisson arrivals (mean `rate` per second, seeded) of frequency-solve
     requests on the SolveServer: each new request a distinct body (a body of
     the pool stretched by U[0.8, 1.25] along each axis) at omega ~ U[0.1, 4];
@@ -120,7 +120,7 @@ def run_serving(engine, bodies, *, rate, n_requests, seed, slots, repeat_frac=0.
             plan.append(pair)
             recent = (recent + [pair])[-16:]
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
-    with SolveServer(engine, slots=slots) as srv:
+    with SolveServer(engine, slots=slots, batch_max=batch_max) as srv:
         warm = [srv.submit(b, 1.0) for b in bodies[:2 * slots]]  # kernels loaded, every slot used
         for f in warm:
             f.result()
@@ -148,7 +148,8 @@ def run_serving(engine, bodies, *, rate, n_requests, seed, slots, repeat_frac=0.
     panels = np.array([b.mesh_including_lid.nb_faces for b, _ in plan])
     return {"arrival_rate_per_s": rate, "requests": n_requests, "slots": slots,
             "completed": len(res), "failed": len(errors), "first_error": errors[0] if errors else None,
-            "escalated_to_gmres": escalated,
+            "escalated_to_gmres": escalated, "batched_requests": counters.get("batched", 0),
+            "batch_max": batch_max,
             "solves_per_s": len(res) / (last - first), "offered_s": float(arrivals[-1]),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "max": float(lat.max())},
@@ -701,6 +702,8 @@ def main():
                     help="requests of the serving run (Poisson arrivals); 0 skips it")
     ap.add_argument("--arrival-rate", type=float, default=200.0)
     ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--serving-batch", type=int, default=4,
+                    help="requests of similar sizes factored together by the server (1: one per factorisation)")
     ap.add_argument("--workload", default="barge",
                     choices=["barge", "array", "bodies", "symmetric", "finite_depth"],
                     help="array: the 3x3 cylinder array with lids (20000 panels), mixed vs float64 GMRES; "
@@ -870,7 +873,7 @@ def main():
         serving = run_serving(B200Engine(green_function=gf, precision=args.engine, refinement=args.refinement)
                               if args.engine == "mixed" else B200Engine(green_function=gf, precision="fp64"),
                               pool, rate=args.arrival_rate, n_requests=args.serving_requests, seed=7 + rank,
-                              slots=args.slots)
+                              slots=args.slots, batch_max=args.serving_batch)
 
     # ---- CPU baseline (oracle port on the host cores) and accuracy --------
     cpu = None

@@ -634,6 +634,18 @@ class B200Engine:
         size = float(np.hypot(np.ptp(c[:, 0]), np.ptp(c[:, 1])))
         return "mixed" if k * size >= FLOAT32_WAVE_MIN_KL else "fp64"
 
+    def pad_stage(self, f: "_Factors", first, m, n_body):
+        """Matrices first .. first+m-1 of f hold a body of n_body < f.n panels:
+        zero rows and columns and a unit diagonal beyond its panels in S and K
+        (the padded unknowns are zero and change nothing)."""
+        if n_body >= f.n:
+            return
+        lib = _lib.load()
+        n = f.n
+        for M in (f.S, f.K):
+            _lib.check(lib.bem_zpad_identity(_vp(M.data_ptr() + 16 * first * n * n), n, n * n, m, n_body, n,
+                                             _lib.stream_ptr()))
+
     def factor_stage(self, f: "_Factors", nb, err, active=None):
         """LU of K (float64 DMMA, or float32 tcgen05 for the mixed engine); none
         for plain GMRES.  active (mixed engine): each matrix's own padded size,
@@ -896,10 +908,7 @@ class B200Engine:
             mesh = body.mesh_including_lid
             self.assemble_stage(f, mesh, wavenumbers(om[j0:j0 + m], water_depth, g), nan_flag=r.nan,
                                 first=j0, lds=npad, water_depth=water_depth)
-            if mesh.nb_faces < npad:
-                for M in (f.S, f.K):  # zero rows/columns, unit diagonal beyond the body's panels
-                    _lib.check(lib.bem_zpad_identity(_vp(M.data_ptr() + 16 * j0 * npad * npad), npad,
-                                                     npad * npad, m, mesh.nb_faces, npad, stream))
+            self.pad_stage(f, j0, m, mesh.nb_faces)
         if ev:
             ev[1].record()
         self.factor_stage(f, nb, r.err, active=active)

@@ -113,7 +113,7 @@ class SolveServer:
     """
 
     def __init__(self, engine: Optional[B200Engine] = None, *, slots: int = 4, memory_budget: Optional[int] = None,
-                 keep_factors: bool = True):
+                 keep_factors: bool = True, batch_max: int = 1, band: float = 1.3):
         import torch
         self.engine = engine if engine is not None else B200Engine(precision="mixed")
         dev = torch.device(self.engine.device)
@@ -125,6 +125,12 @@ class SolveServer:
             memory_budget = int(0.6 * total)
         self.memory_budget = int(memory_budget)
         self.keep_factors = bool(keep_factors)
+        # continuous batching of factorisations: a slot that admits a new
+        # request also takes up to batch_max - 1 waiting ones of similar size
+        # (padded sizes within a factor `band`, same headings, rho and g) and
+        # factors them together with the grouped LU (mixed engine only)
+        self.batch_max = max(1, int(batch_max)) if self.engine.precision == "mixed" else 1
+        self.band = float(band)
         self._arena = DeviceArena(self.memory_budget, self.device)
         self._cv = threading.Condition()
         self._pending: Deque[_Request] = deque()
@@ -226,12 +232,54 @@ class SolveServer:
             self._drop_locked(victim)
         return True
 
+    @staticmethod
+    def _padded(n: int) -> int:
+        return -(-n // 128) * 128
+
+    def _batch_footprint(self, reqs: List[_Request]) -> int:
+        """Device bytes of one grouped batch of new requests (all identity-padded
+        to the largest), with the GMRES workspace of the refinement fallback."""
+        npad = max(self._padded(q.n) for q in reqs)
+        nrhs = max(q.nrhs for q in reqs)
+        B = len(reqs)
+        g_bytes = int(_lib.load().bem_gmres_workspace_bytes(npad, npad, min(nrhs, 16), B,
+                                                            self.engine.gmres_restart)) + 256
+        return _Factors.estimate_bytes(npad, B, "mixed") + g_bytes + _Rhs.estimate_bytes(npad, npad, B, nrhs)
+
+    def _companions_locked(self, head: _Request) -> List[_Request]:
+        """Waiting new requests that can share head's factorisation."""
+        if self.batch_max <= 1:
+            return []
+        p0 = self._padded(head.n)
+        out = []
+        for q in list(self._pending)[1:]:
+            if len(out) + 1 >= self.batch_max:
+                break
+            p = self._padded(q.n)
+            if (q.key in self._resident or q.key == head.key or any(q.key == o.key for o in out)
+                    or max(p, p0) > self.band * min(p, p0) or q.rho != head.rho or q.g != head.g
+                    or q.heads.shape != head.heads.shape or not np.array_equal(q.heads, head.heads)):
+                continue
+            out.append(q)
+        return out
+
     def _take_locked(self):
-        """Admission in arrival order: the head of the queue when it fits."""
+        """Admission in arrival order: the head of the queue when it fits (with
+        the waiting requests that join its factorisation, when batching)."""
         if not self._pending:
             return None
         head = self._pending[0]
         res = self._resident.get(head.key)
+        if res is None:
+            extra = self._companions_locked(head)
+            while extra:
+                need = self._batch_footprint([head] + extra)
+                if need <= self.memory_budget and self._make_room_locked(need):
+                    self._pending.popleft()
+                    for q in extra:
+                        self._pending.remove(q)
+                    return [head] + extra, None, need
+                extra.pop()
         need = self._footprint(head, res is not None)
         if need > self.memory_budget:
             self._pending.popleft()
@@ -248,7 +296,7 @@ class SolveServer:
                 res.users -= 1
             return None
         self._pending.popleft()
-        return head, res, need
+        return [head], res, need
 
     def _slot_stream(self):
         """Context placing the calling thread's work on its own CUDA stream."""
@@ -287,44 +335,52 @@ class SolveServer:
                     if got is not None:
                         break
                     self._cv.wait()
-                req, res, need = got
+                reqs, res, need = got
                 self._inflight_bytes += need
-                self._inflight += 1
+                self._inflight += len(reqs)
                 self.counters["max_inflight_requests"] = max(self.counters["max_inflight_requests"], self._inflight)
                 self.counters["max_reserved_bytes"] = max(self.counters["max_reserved_bytes"],
                                                           self._inflight_bytes + self._resident_bytes)
             admitted = time.perf_counter()
-            keep = result = error = None
+            keep = results = error = None
             try:
                 with slot:
-                    result, keep = self._run(req, res, admitted)
-            except BaseException as exc:  # the request fails, the server goes on
+                    if len(reqs) == 1:
+                        result, keep = self._run(reqs[0], res, admitted)
+                        results = [result]
+                    else:
+                        results = self._run_batch(reqs, admitted)
+            except BaseException as exc:  # the requests fail, the server goes on
                 error = exc
             finally:
                 with self._cv:
                     self._inflight_bytes -= need
-                    self._inflight -= 1
+                    self._inflight -= len(reqs)
                     if res is not None:
                         res.users -= 1
                     if keep is not None:
                         f, release = keep
-                        if req.key not in self._resident and self._make_room_locked(f.nbytes):
-                            self._resident[req.key] = _Resident(f, f.nbytes, release)
+                        key = reqs[0].key
+                        if key not in self._resident and self._make_room_locked(f.nbytes):
+                            self._resident[key] = _Resident(f, f.nbytes, release)
                             self._resident_bytes += f.nbytes
                         else:
                             release()
                     if error is None:
-                        self.counters["completed"] += 1
+                        self.counters["completed"] += len(reqs)
                         if res is not None:
                             self.counters["reused"] += 1
+                        if len(reqs) > 1:
+                            self.counters["batched"] = self.counters.get("batched", 0) + len(reqs)
                     else:
-                        self.counters["failed"] += 1
+                        self.counters["failed"] += len(reqs)
                     self._cv.notify_all()
-            # the caller sees the result after the bookkeeping above
-            if error is None:
-                req.future.set_result(result)
-            else:
-                req.future.set_exception(error)
+            # the callers see the results after the bookkeeping above
+            for i, req in enumerate(reqs):
+                if error is None:
+                    req.future.set_result(results[i])
+                else:
+                    req.future.set_exception(error)
 
     def _buffers(self, build):
         """build(alloc) with arena views, all or nothing: when the arena has no
@@ -345,6 +401,53 @@ class SolveServer:
                         self._drop_locked(victim)
                     else:
                         self._cv.wait(timeout=0.05)
+
+    def _run_batch(self, reqs: List[_Request], admitted: float) -> List[SolveResult]:
+        """New requests of similar sizes in one grouped factorisation: each
+        request's S and K are assembled into its slot of a batch padded to the
+        largest (identity padding), the grouped LU factors them at the cost of
+        their own sizes, the right-hand sides of every request are solved
+        together and the forces integrated per request.  No factors are kept
+        resident (they share one allocation)."""
+        eng = self.engine
+        npad = max(self._padded(q.n) for q in reqs)
+        nrhs = max(q.nrhs for q in reqs)
+        B = len(reqs)
+        stats: Dict[str, float] = {}
+        f, release = self._buffers(lambda a: _Factors(npad, B, self.device, "mixed", alloc=a))
+        try:
+            def rhs(alloc):
+                r = _Rhs(npad, npad, B, nrhs, self.device, "mixed", alloc=alloc)
+                r.gmres_work(eng.gmres_restart)
+                return r
+            r, release_r = self._buffers(rhs)
+            try:
+                r.flags.zero_()
+                om = np.array([q.omega for q in reqs])
+                for j, q in enumerate(reqs):
+                    mesh = q.body.mesh_including_lid
+                    eng.assemble_stage(f, mesh, [q.omega ** 2 / q.g], nan_flag=r.nan, reuse_rankine=False,
+                                       first=j, lds=npad)
+                    eng.pad_stage(f, j, 1, mesh.nb_faces)
+                eng.factor_stage(f, B, r.err, active=[self._padded(q.n) for q in reqs])
+                out = eng._solve_segments(f, r, [(q.body, j, 1) for j, q in enumerate(reqs)], om, reqs[0].heads,
+                                          rho=reqs[0].rho, g=reqs[0].g, stats=stats)
+            finally:
+                release_r()
+        finally:
+            release()
+        finished = time.perf_counter()
+        results = []
+        for q, (F, FK) in zip(reqs, out):
+            ndof = len(q.body.dofs)
+            w = q.omega
+            rad, dif, fk = F[0, :ndof, :], F[0, ndof:, :], FK[0]
+            results.append(SolveResult(
+                request_id=q.rid, omega=w, dofs=list(q.body.dofs), wave_directions=q.heads,
+                added_mass=np.real(rad) / w ** 2, radiation_damping=np.imag(rad) / w, diffraction=dif,
+                froude_krylov=fk, excitation=dif + fk, arrival=q.arrival, admitted=admitted, finished=finished,
+                reused_factors=False, stats=dict(stats, batched=B)))
+        return results
 
     def _run(self, req: _Request, res: Optional[_Resident], admitted: float):
         """Enqueue the request's work on the current (slot) stream and wait

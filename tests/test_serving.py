@@ -36,11 +36,23 @@ class _StandInEngine:
         with self.lock:
             self.running -= 1
 
-    def assemble_stage(self, f, mesh, ks, nan_flag=None, reuse_rankine=True):
+    def assemble_stage(self, f, mesh, ks, nan_flag=None, reuse_rankine=True, first=0, lds=None):
         self._enter(("assemble", mesh.nb_faces, float(ks[0])))
 
-    def factor_stage(self, f, nb, err):
-        self._enter(("factor", f.n))
+    def pad_stage(self, f, first, m, n_body):
+        self.calls.append(("pad", first, n_body))
+
+    def factor_stage(self, f, nb, err, active=None):
+        self._enter(("factor", f.n) if active is None else ("factor_grouped", f.n, tuple(active)))
+
+    def _solve_segments(self, f, r, segments, om, heads, rho=1000.0, g=9.81, stats=None):
+        self._enter(("solve_batch", f.n, len(segments)))
+        out = []
+        for body, j0, m in segments:
+            n = body.mesh_including_lid.nb_faces
+            ndof, nhead = len(body.dofs), len(heads)
+            out.append((np.full((m, ndof + nhead, ndof), n + 1j * om[j0]), np.full((m, nhead, ndof), 2.0 * n)))
+        return out
 
     def solve_stage(self, f, r, body, om, heads, rho=1000.0, g=9.81, stats=None, events=None):
         self._enter(("solve", f.n, float(om[0])))
@@ -154,6 +166,33 @@ def test_scheduler_admits_in_arrival_order():
     assert order == sorted(order) and admitted == sorted(admitted)
 
 
+def test_scheduler_batches_waiting_requests_of_similar_sizes():
+    """With batch_max > 1, a slot that admits a new request takes waiting new
+    requests whose padded sizes lie within the band into one grouped
+    factorisation; requests of other sizes, repeats of resident factors and
+    other headings stay out; every request gets its own result."""
+    eng = _StandInEngine(delay=0.05)
+    with _server(eng, slots=1, memory_budget=1 << 30, batch_max=4) as srv:
+        blocker = srv.submit(_body(4), 0.1)  # occupies the slot while the others queue
+        time.sleep(0.02)
+        same = [_body(10), _body(9), _body(10, dofs=("Heave", "Surge"))]  # 300, 297, 300 panels
+        far = _body(24)
+        futs = [srv.submit(b, 0.5 + 0.1 * i) for i, b in enumerate(same)]
+        f_far = srv.submit(far, 0.9)
+        f_head = srv.submit(same[0], 1.7, wave_directions=(0.0, 1.0))  # other headings
+        res = [f.result(timeout=60) for f in futs]
+        blocker.result(timeout=60)
+        r_far, r_head = f_far.result(timeout=60), f_head.result(timeout=60)
+    grouped = [c for c in eng.calls if c[0] == "factor_grouped"]
+    assert len(grouped) == 1 and len(grouped[0][2]) == 3
+    for b, r in zip(same, res):
+        n = b.mesh_including_lid.nb_faces
+        assert r.stats["batched"] == 3 and r.radiation_damping.shape == (len(b.dofs), len(b.dofs))
+        assert np.all(r.added_mass == n / r.omega ** 2)
+    assert "batched" not in r_far.stats and "batched" not in r_head.stats
+    assert srv.counters["batched"] == 3 and srv.counters["completed"] == 6
+
+
 # ---------------------------------------------------------------------------
 @pytest.mark.gpu
 def test_results_same_alone_and_in_the_mix(oracle_mod, default_oracle_gf, tmp_path):
@@ -194,6 +233,38 @@ def test_results_same_alone_and_in_the_mix(oracle_mod, default_oracle_gf, tmp_pa
             for name in ("added_mass", "radiation_damping", "excitation"):
                 a = getattr(sweep, name)[j]
                 assert np.abs(a - getattr(s, name)).max() <= 1e-8 * np.abs(a).max(), name
+
+
+@pytest.mark.gpu
+def test_batched_requests_same_as_alone(oracle_mod, default_oracle_gf, tmp_path):
+    """Requests factored together (batch_max 4: waiting requests of similar
+    sizes share one grouped factorisation, identity-padded to the largest)
+    give each request's result alone within the refinement tolerance."""
+    from capytaine_b200.engine import B200Engine
+    from capytaine_b200.serving import SolveServer
+    from test_gpu_mixed import _shared_table_gf
+    gf = _shared_table_gf(default_oracle_gf, tmp_path)
+    bodies = [
+        FloatingBody(mesh_sphere(radius=1.0, resolution=(10, 20)).immersed_part(), rigid_body_dofs()),
+        FloatingBody(mesh_sphere(radius=1.5, resolution=(10, 22)).immersed_part(),
+                     rigid_body_dofs(only=["Surge", "Heave", "Pitch"])),
+        FloatingBody(mesh_vertical_cylinder(length=6.0, radius=2.0, resolution=(3, 20, 10)).immersed_part(),
+                     rigid_body_dofs(only=["Heave"])),
+    ]
+    reqs = [(b, w) for w in (0.4, 1.3, 2.6) for b in bodies]
+    eng = B200Engine(green_function=gf, precision="mixed")
+    with SolveServer(eng, slots=1, memory_budget=4 << 30) as alone:
+        solo = [alone.solve(b, w, timeout=300) for b, w in reqs]
+    with SolveServer(eng, slots=1, memory_budget=4 << 30, batch_max=4, keep_factors=False) as srv:
+        blocker = srv.submit(bodies[0], 3.3)  # the others queue behind it and are batched
+        futs = [srv.submit(b, w) for b, w in reqs]
+        got = [f.result(timeout=600) for f in futs]
+        blocker.result(timeout=600)
+        assert srv.counters.get("batched", 0) >= 4
+    for i in range(len(reqs)):
+        for name in ("added_mass", "radiation_damping", "excitation"):
+            a, s = getattr(got[i], name), getattr(solo[i], name)
+            assert np.abs(a - s).max() <= 1e-8 * np.abs(s).max(), (i, name)
 
 
 @pytest.mark.gpu
