@@ -31,7 +31,7 @@ namespace bem {
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store = 0, const float* Aop1 = nullptr,
-                      const float* Bop1 = nullptr, int max_ctas = 0, long long wait_limit = 0,
+                      const float* Bop1 = nullptr, int run = 0, long long wait_limit = 0,
                       const int* limit_host = nullptr);
 
 namespace {
@@ -686,21 +686,16 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
                                                                            npad, W);
   ++launches;
   const size_t abuf = (size_t)batch * npad * 2 * kB, bbuf = (size_t)batch * 2 * npad * 2 * kB;
-  // The trailing updates are persistent kernels holding one CTA per SM; the
-  // lookahead's Gauss-Jordan inverses (one CTA per matrix, a whole SM each)
-  // and panel products run on the side stream meanwhile, on SMs kept free.
-  int sms = 0;
-  {
-    int dev = 0;
-    BEM_CUDA_CHECK(cudaGetDevice(&dev));
-    BEM_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  }
-  const int reserve = std::max(1, std::min(batch, sms / 4));
+  // The big trailing updates give each CTA runs of 8 tiles (the accumulator
+  // double buffer pays over a run); the side stream's panel products, whose
+  // latency is the lookahead chain, one tile per CTA.  CTAs retire after their
+  // run, so the side stream's kernels take SMs as they free up.
+  constexpr int kBigRun = 8, kSideRun = 1;
   float* Aop[kOpBuffers] = {w.Aop, w.Aop + abuf, w.Aop + 2 * abuf};
   float* Bop[kOpBuffers] = {w.Bop, w.Bop + bbuf, w.Bop + 2 * bbuf};
   // Inverse of the diagonal block, then the panel: A12 and A21 packed, L21 =
   // A21 A_kk^{-1} on the tensor cores into the working matrix, L21 packed.
-  auto diag_and_panel = [&](int kk, int buf, cudaStream_t on, int side_ctas) -> int {
+  auto diag_and_panel = [&](int kk, int buf, cudaStream_t on) -> int {
     {
       TimedLaunch tl(kKCluGj, on);
       clu_gj_kernel<<<batch, 512, 0, on>>>(W, kk, info_dev, w.inv, nblk, w.binv, w.ainv);
@@ -715,14 +710,14 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
                                                                     Bop[buf], w.a3);
       // split TF32: A_hi B_hi + A_lo B_hi + A_hi B_lo, float32-level multipliers
       int st2 = cgemm_tf32_update(w.a3, npad, kk + kB, w.binv, 2 * kB, 0, kSplitK, W.re, W.im, npad, W.stride,
-                                  kk + kB, kk, m, kB, batch, err_dev, on, 1, nullptr, nullptr, side_ctas, 0, act);
+                                  kk + kB, kk, m, kB, batch, err_dev, on, 1, nullptr, nullptr, kSideRun, 0, act);
       if (st2) return st2;
       clu_pack_kernel<<<dim3(m / 32, batch), 256, 0, on>>>(W, npad, kk, 0, kk + kB, kk, Aop[buf], Bop[buf],
                                                            nullptr);
       // block row of U scaled by the diagonal inverse, U' = A_kk^{-1} A12 (TF32),
       // for the backward substitution only (A12 itself is packed in Bop already)
       st2 = cgemm_tf32_update(w.ainv, kB, 0, Bop[buf], 2 * (int64_t)npad, 2 * (kk + kB), 2 * kB, W.re, W.im, npad,
-                              W.stride, kk, kk + kB, kB, m, batch, err_dev, on, 1, nullptr, nullptr, side_ctas, 0,
+                              W.stride, kk, kk + kB, kB, m, batch, err_dev, on, 1, nullptr, nullptr, kSideRun, 0,
                               act);
       if (st2) return st2;
     }
@@ -732,11 +727,11 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   // C rows r0.. (m), complex columns c0.. (nc) -= L21 U12 of the block step whose
   // packed operands are in buffer buf, and of a second step (buffer buf2 >= 0)
   // in the same pass over C (depth 256).
-  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2, int ctas) -> int {
+  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2, int run) -> int {
     if (m <= 0 || nc <= 0) return BEM_OK;
     return cgemm_tf32_update(Aop[buf], npad, r0, Bop[buf], 2 * (int64_t)npad, 2 * c0, 2 * kB, W.re, W.im, npad,
                              W.stride, r0, c0, m, nc, batch, err_dev, s, 0, buf2 >= 0 ? Aop[buf2] : nullptr,
-                             buf2 >= 0 ? Bop[buf2] : nullptr, ctas, 0, act);
+                             buf2 >= 0 ? Bop[buf2] : nullptr, run, 0, act);
   };
   Lookahead* la = nullptr;
   if ((st = lookahead_for(s, &la))) return st;
@@ -749,7 +744,7 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   // stream while, at every second step, the rest of the trailing matrix gets
   // the updates of steps k-1 and k together.  Operands of steps k-1, k, k+1
   // live in three buffers.
-  if ((st = diag_and_panel(0, 0, s, 0))) return st;
+  if ((st = diag_and_panel(0, 0, s))) return st;
   for (int kk = 0, step = 0; kk + kB < npad; kk += kB, ++step) {
     const int cur = step % kOpBuffers, prev = (step + kOpBuffers - 1) % kOpBuffers;
     const int nxt = (step + 1) % kOpBuffers;
@@ -759,11 +754,10 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
     if ((st = update(cur, kn + kB, kn, rest, kB, pend, 0))) return st;  // block column kn below the diagonal
     BEM_CUDA_CHECK(cudaEventRecord(la->strips, s));
     BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->strips, 0));
-    const bool big = (step & 1) && rest > 0;
-    if ((st = diag_and_panel(kn, nxt, la->side, big ? reserve : 0))) return st;
+    if ((st = diag_and_panel(kn, nxt, la->side))) return st;
     BEM_CUDA_CHECK(cudaEventRecord(la->panel, la->side));
-    if (big) {
-      if ((st = update(cur, kn + kB, kn + kB, rest, rest, prev, sms - reserve))) return st;
+    if ((step & 1) && rest > 0) {
+      if ((st = update(cur, kn + kB, kn + kB, rest, rest, prev, kBigRun))) return st;
     }
     BEM_CUDA_CHECK(cudaStreamWaitEvent(s, la->panel, 0));
   }

@@ -31,7 +31,7 @@ constexpr uint32_t kLuMagic = 0x42454d4cu;   // "BEML"
 constexpr uint32_t kReqMagic = 0x42454d52u;  // "BEMR"
 constexpr int kChunk = 16;                   // right-hand sides per refinement call
 constexpr double kMixedTol = 1e-10;          // relative residual of the refined solves
-constexpr double kFp64Tol = 1e-12;           // float64 solves, accepted up to kMixedTol at the float64 floor
+constexpr double kFp64Tol = 1e-13;           // float64 solves, accepted up to kMixedTol at the float64 floor
 constexpr int kMaxIter = 30;
 
 // Makes a device current for the duration of a call and restores the caller's.

@@ -147,6 +147,7 @@ struct UpdateArgs {
   int tiles_m;       // tile grid: tiles_m x tiles_n x batch, tm fastest
   int tiles_n;
   int ntiles;
+  int tiles_per_cta;     // consecutive tiles of one CTA
   long long wait_limit;  // polls of a bounded mbarrier wait
   // Grouped launch (ngroup > 0): matrix b has gtm[b] x gtn[b] tiles of its own,
   // tiles gstart[b] .. gstart[b+1]-1 (matrices of different active sizes)
@@ -191,11 +192,14 @@ __device__ __forceinline__ bool mbar_wait_n(uint64_t* bar, uint32_t parity, int*
   return true;
 }
 
-// Persistent trailing update: one CTA per SM walks the 128 x 128 complex tiles
-// t = blockIdx.x, blockIdx.x + gridDim.x, ... with two accumulators in tensor
-// memory, so that the epilogue of tile i (read C, subtract, write C) overlaps
-// the MMAs of tile i+1.  Barriers: full/empty per operand stage (TMA -> MMA ->
-// TMA), acc_full per accumulator (MMA commit -> epilogue), acc_empty per
+// Trailing update with double-buffered accumulators: a CTA (one per SM: 197 KB
+// of shared memory, all 512 tensor-memory columns) takes a run of
+// tiles_per_cta consecutive 128 x 128 complex tiles and alternates between two
+// accumulators in tensor memory, so that the epilogue of tile i (read C,
+// subtract, write C) overlaps the MMAs of tile i+1.  CTAs retire after their
+// run, so kernels of other streams (the lookahead of the block LU) get SMs
+// within one run.  Barriers: full/empty per operand stage (TMA -> MMA -> TMA),
+// acc_full per accumulator (MMA commit -> epilogue), acc_empty per
 // accumulator (one arrival per epilogue warp -> MMA).
 __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
                                                                    const __grid_constant__ CUtensorMap mapB,
@@ -241,13 +245,16 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
+  // this CTA's tiles: a run of consecutive tiles (tm fastest: they share B)
+  const int t_begin = blockIdx.x * p.tiles_per_cta;
+  const int t_end = min(p.ntiles, t_begin + p.tiles_per_cta);
 
   if (warp == 0) {
     if (lane == 0) {
       // producer: operand slices of every tile of this CTA through the ring
       bool ok = true;
       long long g = 0;  // stage uses so far
-      for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+      for (int t = t_begin; t < t_end && ok; ++t) {
         int b, tm, tn;
         decode_tile(p, t, b, tm, tn);
         b += p.batch0;
@@ -273,7 +280,7 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
       bool ok = true;
       long long g = 0;
       int i = 0;  // tiles of this CTA so far
-      for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++i) {
+      for (int t = t_begin; t < t_end && ok; ++t, ++i) {
         const int acc = i & 1;
         const uint32_t use = (uint32_t)(i >> 1);
         // the epilogue must have drained this accumulator's previous tile
@@ -312,7 +319,7 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
     const int64_t ldc = p.ldc;
     bool ok = true;
     int i = 0;
-    for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++i) {
+    for (int t = t_begin; t < t_end && ok; ++t, ++i) {
       int b, tm, tn;
       decode_tile(p, t, b, tm, tn);
       b += p.batch0;
@@ -414,12 +421,12 @@ int num_sms(int* out) {
 }  // namespace
 
 // Host entry shared with the LU: C (trailing block m x n complex, both multiples
-// of 128) -= A' B' for `batch` matrices.  max_ctas > 0 caps the persistent grid
-// (SMs left free for work on other streams); 0: one CTA per SM.
+// of 128) -= A' B' for `batch` matrices.  run > 0: tiles per CTA; 0: chosen
+// from the tile count (up to 8 while there are at least two runs per SM).
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store, const float* Aop1,
-                      const float* Bop1, int max_ctas, long long wait_limit, const int* limit_host) {
+                      const float* Bop1, int run, long long wait_limit, const int* limit_host) {
   if (m <= 0 || n <= 0) return BEM_OK;
   if (m % kTM || n % kTNc || kp % kKC || (a_row0 % 8) || (b_row0 % 8))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: sizes must be multiples of 128 (K' of 32)");
@@ -483,13 +490,14 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
     if (ntiles > (1ll << 30)) return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: too many tiles");
     if (ntiles == 0) continue;
     p.ntiles = (int)ntiles;
-    int ctas = max_ctas > 0 ? std::min(max_ctas, sms) : sms;
-    ctas = (int)std::min<long long>(ctas, ntiles);
+    int tpc = run > 0 ? run : (int)std::max(1ll, std::min(8ll, ntiles / (2ll * sms)));
+    const long long ctas = (ntiles + tpc - 1) / tpc;
     UpdateArgs q = p;
+    q.tiles_per_cta = tpc;
     q.batch0 = b0;  // the matrices of this launch: b0 .. b0 + nb - 1
     {
       TimedLaunch tl(kKCgemmTf32, stream);
-      cgemm_tf32_update_kernel<<<ctas, kThreads, smem, stream>>>(mapA, mapB, mapA1, mapB1, q);
+      cgemm_tf32_update_kernel<<<(unsigned)ctas, kThreads, smem, stream>>>(mapA, mapB, mapA1, mapB1, q);
     }
     ++launches;
   }

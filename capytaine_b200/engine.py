@@ -40,10 +40,7 @@ RHS_CHUNK = 16  # right-hand sides per refinement / GMRES / tall-GEMM call
 # Relative residual |b - K x| / |b| that a float64 LU solve is refined to; a
 # solve whose residual stops decreasing above it (the float64 floor of an
 # ill-conditioned K) is accepted up to the engine's refine_tol.
-FP64_RESIDUAL_TOL = 1e-12
-# assembly_precision="auto": float32 wave term from this k L on (L the body's
-# horizontal size).
-FLOAT32_WAVE_MIN_KL = 2.0
+FP64_RESIDUAL_TOL = 1e-13
 
 
 def padded_size(n: int) -> int:
@@ -376,8 +373,8 @@ class B200Engine:
                  method: str = "indirect", batch_tuner=None):
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
-        if assembly_precision not in ("fp64", "mixed", "auto"):
-            raise ValueError("assembly_precision must be 'fp64', 'mixed' or 'auto'")
+        if assembly_precision not in ("fp64", "mixed"):
+            raise ValueError("assembly_precision must be 'fp64' or 'mixed'")
         if not callable(linear_solver) and linear_solver not in ("lu_decomposition",
                                                                  "lu_decomposition_with_overwrite", "gmres"):
             raise NotImplementedError(f"Unknown `linear_solver` in B200Engine: {linear_solver}")
@@ -563,7 +560,7 @@ class B200Engine:
             cstride = N * st.n_sub
             gf.assemble_into(full, st.submesh, ws.cols[0, 0], ws.cols[1, 0], wavenumber=ks[0], lds=N, ldk=N,
                              nan_flag=ws.r.nan,
-                             precision="fp64" if self.assembly_precision == "auto" else self.assembly_precision,
+                             precision=self.assembly_precision,
                              adjoint_double_layer=adjoint, sweep=(ks, cstride, cstride), water_depth=water_depth)
             ws.combine_matrices(ws.cols[0], nb, f.S, st.n_sys, st.n_sys * st.n_sys, stream)
             ws.combine_matrices(ws.cols[1], nb, f.K, f.ldk, f.strideK, stream)
@@ -622,17 +619,10 @@ class B200Engine:
                              adjoint_double_layer=adjoint, water_depth=water_depth)
 
     def _wave_precision(self, mesh, k, water_depth=np.inf):
-        """Precision of the wave term at wavenumber k: assembly_precision, or
-        with "auto" float32 once k times the body's horizontal size reaches
-        FLOAT32_WAVE_MIN_KL (below, the damping carried by the O(k)-small
-        imaginary parts needs the float64 wave term)."""
-        if self.assembly_precision != "auto":
-            return self.assembly_precision
-        if water_depth != np.inf or not (0.0 < k < np.inf):
-            return "fp64"
-        c = mesh.faces_centers
-        size = float(np.hypot(np.ptp(c[:, 0]), np.ptp(c[:, 1])))
-        return "mixed" if k * size >= FLOAT32_WAVE_MIN_KL else "fp64"
+        """Precision of the wave term at wavenumber k (one per engine: a
+        per-frequency choice was measured and rejected, the float32 wave term
+        loses accuracy at low and at high k alike)."""
+        return self.assembly_precision
 
     def pad_stage(self, f: "_Factors", first, m, n_body):
         """Matrices first .. first+m-1 of f hold a body of n_body < f.n panels:

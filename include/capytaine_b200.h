@@ -472,7 +472,7 @@ int bem_context_set_tabulation(bem_context* ctx, const double* table_host);
  * once for the call), K factored (precision BEM_PREC_MIXED: float32 block LU
  * with tcgen05 trailing updates and float64-residual refinement to 1e-10,
  * continued with preconditioned GMRES when it stops contracting;
- * BEM_PREC_FP64: float64 block LU with the residual refined to 1e-12), the
+ * BEM_PREC_FP64: float64 block LU with the residual refined to 1e-13), the
  * radiation problems of the ndof dofs (dof_normals: ndof x nb_faces, the
  * normal component dof(x_i) . n_i of each dof's motion at the face centres,
  * problems_and_results.py:440-449) and the diffraction problems of the nhead
