@@ -343,27 +343,89 @@ __device__ __forceinline__ void st_release_i(int* p, int v) {
 // the off-diagonal block of a dependency is copied to shared memory
 // asynchronously (real and imaginary planes, 16-byte copies) before waiting for
 // that dependency; the diagonal inverse is staged through the same buffer.
-// Thread (r, h) accumulates row r over the half h of the 128-long inner
-// dimension for all NC columns (one float pair per entry of the tile, NC/2
-// 16-byte broadcast reads of the right-hand sides); the halves meet in P.
+// Each block product (128 x 128 complex tile times the 128 x NC right-hand
+// sides) runs on the tensor cores with warp-level TF32 MMAs (m16n8k8), each
+// operand split into a TF32 head and a TF32 tail and three products taken
+// (head x head, head x tail, tail x head), which keeps float32 accuracy; the
+// complex product is the real product [acc_r | acc_i] = [Tr | Ti] [[Yr, Yi],
+// [-Yi, Yr]] (K = 256).  Warp w owns rows 16 w .. 16 w + 15 of the tile.
+constexpr int kLdT = kB + 8;  // column stride of a staged tile: conflict-free fragment reads
+
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = tf32_rna(x);
+  lo = tf32_rna(x - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_16x8x8_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// d[nt] (n-tile nt of 8 real columns: real parts of the complex columns for
+// nt < NT/2, imaginary parts beyond) = rows 16 w .. of T times Y (Y[m*NC + c]).
 template <int NC>
-__device__ __forceinline__ void tile_times_rhs(const float* __restrict__ Tre, const float* __restrict__ Tim,
-                                               const float2* __restrict__ Y, int r, int h, float2 (&acc)[NC]) {
+__device__ __forceinline__ void tile_mma(const float* __restrict__ Tre, const float* __restrict__ Tim,
+                                         const float2* __restrict__ Y, int w, int lane, float (&d)[NC / 4][4]) {
+  constexpr int NT = NC / 4;  // 2 NC real columns in tiles of 8
+  const int g = lane >> 2, t = lane & 3;
+  const int row = 16 * w + g;
 #pragma unroll
-  for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.0f, 0.0f);
-#pragma unroll 4
-  for (int m = 64 * h; m < 64 * h + 64; ++m) {
-    const float ar = Tre[m * kB + r], ai = Tim[m * kB + r];
-    const float4* y4 = reinterpret_cast<const float4*>(Y + m * NC);
+  for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
-    for (int c2 = 0; c2 < NC / 2; ++c2) {
-      const float4 y = y4[c2];
-      acc[2 * c2].x = fmaf(ar, y.x, fmaf(-ai, y.y, acc[2 * c2].x));
-      acc[2 * c2].y = fmaf(ar, y.y, fmaf(ai, y.x, acc[2 * c2].y));
-      acc[2 * c2 + 1].x = fmaf(ar, y.z, fmaf(-ai, y.w, acc[2 * c2 + 1].x));
-      acc[2 * c2 + 1].y = fmaf(ar, y.w, fmaf(ai, y.z, acc[2 * c2 + 1].y));
+    for (int e = 0; e < 4; ++e) d[nt][e] = 0.0f;
+#pragma unroll 2
+  for (int ks = 0; ks < 32; ++ks) {
+    const int half = ks >> 4;  // K rows 0..127: Tr against (Yr | Yi); 128..255: Ti against (-Yi | Yr)
+    const int m0 = (ks & 15) * 8;
+    const float* T = half ? Tim : Tre;
+    const float a[4] = {T[(m0 + t) * kLdT + row], T[(m0 + t) * kLdT + row + 8], T[(m0 + t + 4) * kLdT + row],
+                        T[(m0 + t + 4) * kLdT + row + 8]};
+    uint32_t ah[4], al[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) split_tf32(a[e], ah[e], al[e]);
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const bool im_col = nt >= NT / 2;
+      const int c = (nt % (NT / 2)) * 8 + g;
+      const float2 y0 = Y[(m0 + t) * NC + c], y1 = Y[(m0 + t + 4) * NC + c];
+      const float v0 = half == 0 ? (im_col ? y0.y : y0.x) : (im_col ? y0.x : -y0.y);
+      const float v1 = half == 0 ? (im_col ? y1.y : y1.x) : (im_col ? y1.x : -y1.y);
+      uint32_t b0h, b0l, b1h, b1l;
+      split_tf32(v0, b0h, b0l);
+      split_tf32(v1, b1h, b1l);
+      mma_16x8x8_tf32(d[nt], ah, b0h, b1h);
+      mma_16x8x8_tf32(d[nt], ah, b0l, b1l);
+      mma_16x8x8_tf32(d[nt], al, b0h, b1h);
     }
   }
+}
+
+// X (rows of warp w) = sign * d + (accumulate ? X : 0).
+template <int NC>
+__device__ __forceinline__ void tile_apply(float2* X, int w, int lane, const float (&d)[NC / 4][4], float sign,
+                                           bool accumulate) {
+  constexpr int NT = NC / 4;
+  const int g = lane >> 2, t = lane & 3;
+  const int row = 16 * w + g;
+#pragma unroll
+  for (int nt = 0; nt < NT / 2; ++nt)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int c = nt * 8 + 2 * t + e;
+#pragma unroll
+      for (int hv = 0; hv < 2; ++hv) {
+        float2* x = X + (row + 8 * hv) * NC + c;
+        const float re = sign * d[nt][2 * hv + e], im = sign * d[nt + NT / 2][2 * hv + e];
+        *x = accumulate ? make_float2(x->x + re, x->y + im) : make_float2(re, im);
+      }
+    }
 }
 
 template <int NC>
@@ -374,14 +436,13 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
                                                                long long spin_limit, int withheld) {
   if (skip && *skip) return;  // refinement already converged
   extern __shared__ __align__(16) float fsmf[];
-  float* Lre = fsmf;  // Lre[m*kB + r], 128 x 128
-  float* Lim = Lre + kB * kB;
-  float2* X = reinterpret_cast<float2*>(Lim + kB * kB);  // X[r*NC + c]
-  float2* Y = X + kB * NC;                                 // Y[m*NC + c]
-  float2* P = Y + kB * NC;                                 // P[r*NC + c]
+  float* Lre = fsmf;  // Lre[m*kLdT + r], 128 x 128
+  float* Lim = Lre + kB * kLdT;
+  float2* X = reinterpret_cast<float2*>(Lim + kB * kLdT);  // X[r*NC + c]
+  float2* Y = X + kB * NC;                                   // Y[m*NC + c]
   __shared__ int s_t;
   const int tid = threadIdx.x;
-  const int r = tid & (kB - 1), h = tid >> 7;
+  const int warp = tid >> 5, lane = tid & 31;
   if (tid == 0) s_t = atomicAdd(ticket, 1);
   __syncthreads();
   const int t = s_t;
@@ -401,30 +462,20 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   const int ndep = forward ? i : (nblk - 1 - i);
   const float* Wre = W.re + (size_t)b * W.stride;
   const float* Wim = W.im + (size_t)b * W.stride;
-  float2 acc[NC];
+  float d[NC / 4][4];
   if (!forward) {
     // x_i = A_ii^{-1} b_i - sum_j U'_ij x_j with U' = A_ii^{-1} U: the product
     // with the diagonal inverse comes first, off the chain of dependencies
     const float2* Inv = inv + ((size_t)b * nblk + i) * kB * kB;
     for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
       const float2 v = __ldg(Inv + idx);  // element (idx % 128, idx / 128)
-      Lre[idx] = v.x;
-      Lim[idx] = v.y;
+      Lre[(idx >> 7) * kLdT + (idx & (kB - 1))] = v.x;
+      Lim[(idx >> 7) * kLdT + (idx & (kB - 1))] = v.y;
     }
     __syncthreads();
-    tile_times_rhs<NC>(Lre, Lim, X, r, h, acc);
-    if (h == 1) {
-#pragma unroll
-      for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
-    }
-    __syncthreads();
-    if (h == 0) {
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const float2 o = P[r * NC + c];
-        X[r * NC + c] = make_float2(acc[c].x + o.x, acc[c].y + o.y);
-      }
-    }
+    tile_mma<NC>(Lre, Lim, X, warp, lane, d);
+    __syncthreads();  // every warp has read all of X
+    tile_apply<NC>(X, warp, lane, d, 1.0f, false);
     __syncthreads();  // Lre/Lim are reused for the off-diagonal blocks
   }
   for (int q = 0; q < ndep; ++q) {
@@ -434,8 +485,8 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
     for (int idx = tid; idx < kB * 32; idx += blockDim.x) {
       const int m = idx >> 5, piece = idx & 31;
       const size_t g = (size_t)(r0 + piece * 4) + (size_t)(j * kB + m) * W.ld;
-      cp_async16(Lre + m * kB + piece * 4, Wre + g);
-      cp_async16(Lim + m * kB + piece * 4, Wim + g);
+      cp_async16(Lre + m * kLdT + piece * 4, Wre + g);
+      cp_async16(Lim + m * kLdT + piece * 4, Wim + g);
     }
     if (tid == 0) {
       long long it = 0;
@@ -459,22 +510,9 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
     }
     cp_async_wait_all();
     __syncthreads();
-    tile_times_rhs<NC>(Lre, Lim, Y, r, h, acc);
-    if (h == 1) {
-#pragma unroll
-      for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
-    }
-    __syncthreads();
-    if (h == 0) {
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const float2 o = P[r * NC + c];
-        float2 x = X[r * NC + c];
-        x.x -= acc[c].x + o.x;
-        x.y -= acc[c].y + o.y;
-        X[r * NC + c] = x;
-      }
-    }
+    tile_mma<NC>(Lre, Lim, Y, warp, lane, d);
+    tile_apply<NC>(X, warp, lane, d, -1.0f, true);  // rows of this warp only
+    __syncthreads();  // Lre/Lim and Y are overwritten by the next dependency
   }
   // forward (unit block lower factor): y_i = X; backward: x_i = X
   __syncthreads();
@@ -492,7 +530,7 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   if (tid == 0 && i != withheld) st_release_i(flags + (size_t)b * nblk + i, 1);
 }
 
-constexpr int trsm_smem_bytes(int nc) { return 2 * kB * kB * (int)sizeof(float) + 3 * kB * nc * (int)sizeof(float2); }
+constexpr int trsm_smem_bytes(int nc) { return 2 * kB * kLdT * (int)sizeof(float) + 2 * kB * nc * (int)sizeof(float2); }
 
 // x += r (the correction solved in place in r), then r = b for the residual.
 __global__ void ir_update_kernel(double2* __restrict__ X, double2* __restrict__ R, const double2* __restrict__ Bv,
