@@ -90,72 +90,104 @@ __global__ void convert_pad_kernel(const double2* __restrict__ K, int64_t ldk, i
   }
 }
 
-// One Gauss-Jordan column step with the owner slot JM of column j known at
-// compile time (j = 16 JM + jw).  Thread (warp w, lane l) owns rows l + 32 a
-// (a < 4) and columns w + 16 m (m < 8): the pivot row's entries in a warp's
-// columns all live in that warp, so only the pivot column crosses warps, through
-// shared memory, with one barrier per column (the column buffers alternate, and
-// a barrier separates the reads of one from the next write of the same one).
+// Pivot of column j (register slot M of warp j % 16), among rows j..127:
+// publishes the column with rows j and the pivot exchanged (entry j is then
+// the pivot) to colbuf[j & 1] and the pivot row to s_piv[j & 1]; flags an
+// exactly zero pivot in info.
+template <int M>
+__device__ __forceinline__ void gj_pivot(const float2 (&a)[4][8], int j, int kk, int b, int lane,
+                                         float2 (*colbuf)[kB], int* s_piv, int* __restrict__ info) {
+  float best = -1.0f;
+  int bi = j;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = lane + 32 * i;
+    const float av = fabs1(a[i][M]);
+    if (r >= j && (av > best || (av == best && r < bi))) {
+      best = av;
+      bi = r;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+    if (ob > best || (ob == best && oi < bi)) {
+      best = ob;
+      bi = oi;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = lane + 32 * i;
+    const int dst = (r == j) ? bi : ((r == bi) ? j : r);
+    colbuf[j & 1][dst] = a[i][M];
+  }
+  if (lane == 0) {
+    s_piv[j & 1] = bi;
+    if (!(best > 0.0f) && info[b] == 0) info[b] = kk + j + 1;
+  }
+}
+
+// Update of register slot M of this thread's entries for column step j: row j
+// becomes the normalised pivot row u, the pivot column (slot JM of warp jw)
+// -f / pivot, every other entry a - f u.
+template <int M>
+__device__ __forceinline__ void gj_update(float2 (&a)[4][8], const float2 (&f)[4], const float2 (&u)[8], int SJ,
+                                          bool own_row_j, bool pivot_col, float2 mdinv) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (i == SJ && own_row_j) a[i][M] = u[M];
+    else if (pivot_col) a[i][M] = fmul(f[i], mdinv);
+    else a[i][M] = ffms(a[i][M], f[i], u[M]);
+  }
+}
+
+// One Gauss-Jordan column step, column j = 16 JM + jw (slot JM of warp jw,
+// known at compile time).  Thread (warp w, lane l) owns rows l + 32 a (a < 4)
+// and columns w + 16 m (m < 8).  Only the pivot column crosses warps (shared
+// memory, double buffered, one barrier per column); the rows j and p of a
+// warp's own columns are exchanged through a per-warp buffer.  The owner of
+// column j + 1 updates that column first and searches its pivot while the
+// other warps are still updating, so the search is off the critical path.
 template <int JM>
 __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b, int lane, int w, int tid,
-                                        float2 (*colbuf)[kB], int* s_piv, int* perm, int* __restrict__ info) {
+                                        float2 (*colbuf)[kB], float2 (*xbuf)[2][8], int* s_piv, int* perm,
+                                        int* __restrict__ info) {
   constexpr int SJ = JM >> 1;  // register slot of row j (j >> 5)
   const int j = 16 * JM + jw;
   const int buf = j & 1;
-  if (w == jw) {
-    float best = -1.0f;
-    int bi = j;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = lane + 32 * i;
-      const float av = fabs1(a[i][JM]);
-      if (r >= j && (av > best || (av == best && r < bi))) {
-        best = av;
-        bi = r;
-      }
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const float ob = __shfl_xor_sync(0xffffffffu, best, off);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-      if (ob > best || (ob == best && oi < bi)) {
-        best = ob;
-        bi = oi;
-      }
-    }
-    // the pivot column with rows j and bi exchanged (entry j is the pivot)
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = lane + 32 * i;
-      const int dst = (r == j) ? bi : ((r == bi) ? j : r);
-      colbuf[buf][dst] = a[i][JM];
-    }
-    if (lane == 0) {
-      s_piv[buf] = bi;
-      if (!(best > 0.0f) && info[b] == 0) info[b] = kk + j + 1;
-    }
-  }
-  __syncthreads();
+  __syncthreads();  // column j and its pivot row are published
   const int p = s_piv[buf];
   const int lj = j & 31, lp = p & 31, sp = p >> 5;
-  // the pivot row in this warp's columns, in every lane; then rows j and p exchanged
-  float2 prow[8];
-#pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    float2 vp = a[0][m];
-#pragma unroll
-    for (int i = 1; i < 4; ++i)
-      if (i == sp) vp = a[i][m];
-    prow[m] = make_float2(__shfl_sync(0xffffffffu, vp.x, lp), __shfl_sync(0xffffffffu, vp.y, lp));
-  }
-  if (p != j) {
+  // rows p and j of this warp's columns: lane lp writes row p, lane lj row j
+  if (lane == lp) {
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
-      const float2 vj = a[SJ][m];
-      const float2 from_j = make_float2(__shfl_sync(0xffffffffu, vj.x, lj), __shfl_sync(0xffffffffu, vj.y, lj));
+      float2 v = a[0][m];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if (i == sp && lane == lp) a[i][m] = from_j;
+      for (int i = 1; i < 4; ++i)
+        if (i == sp) v = a[i][m];
+      xbuf[w][0][m] = v;
+    }
+  }
+  if (p != j && lane == lj) {
+#pragma unroll
+    for (int m = 0; m < 8; ++m) xbuf[w][1][m] = a[SJ][m];
+  }
+  __syncwarp();
+  float2 prow[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) prow[m] = xbuf[w][0][m];
+  if (p != j) {
+    if (lane == lp) {  // row p takes the old row j; row j becomes u below
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const float2 v = xbuf[w][1][m];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (i == sp) a[i][m] = v;
+      }
     }
     if (tid == 0) {
       const int t = perm[j];
@@ -169,19 +201,27 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
 #pragma unroll
   for (int m = 0; m < 8; ++m) u[m] = (m == JM && w == jw) ? dinv : fmul(prow[m], dinv);
   const float2 mdinv = make_float2(-dinv.x, -dinv.y);
+  float2 f[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    if (i == SJ && lane == lj) {
+  for (int i = 0; i < 4; ++i) f[i] = colbuf[buf][lane + 32 * i];
+  const bool own_row_j = lane == lj;
+  const int w1 = (j + 1) & 15;  // owner of column j + 1
+  // slot JM first (column j + 1 lives there when jw < 15)
+  gj_update<JM>(a, f, u, SJ, own_row_j, w == jw, mdinv);
+  if (jw < 15 && w == w1) gj_pivot<JM>(a, j + 1, kk, b, lane, colbuf, s_piv, info);
+  if constexpr (JM < 7) {
+    gj_update<JM + 1>(a, f, u, SJ, own_row_j, false, mdinv);
+    if (jw == 15 && w == w1) gj_pivot<JM + 1>(a, j + 1, kk, b, lane, colbuf, s_piv, info);
+  }
 #pragma unroll
-      for (int m = 0; m < 8; ++m) a[i][m] = u[m];
-    } else {
-      const float2 f = colbuf[buf][lane + 32 * i];
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        if (m == JM && w == jw) a[i][m] = fmul(f, mdinv);
-        else a[i][m] = ffms(a[i][m], f, u[m]);
-      }
-    }
+  for (int m = 0; m < 8; ++m) {
+    if (m == JM || m == JM + 1) continue;
+    // slots other than JM never hold the pivot column
+#define BEM_GJ_UPD(MM) \
+    if (m == MM) gj_update<MM>(a, f, u, SJ, own_row_j, false, mdinv);
+    BEM_GJ_UPD(0) BEM_GJ_UPD(1) BEM_GJ_UPD(2) BEM_GJ_UPD(3) BEM_GJ_UPD(4) BEM_GJ_UPD(5) BEM_GJ_UPD(6)
+    BEM_GJ_UPD(7)
+#undef BEM_GJ_UPD
   }
 }
 
@@ -189,15 +229,15 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
 // pivoting among its rows.  The 128 x 128 block lives in registers: thread
 // (warp w, lane l) owns rows l + 32 a (a < 4) and columns w + 16 m (m < 8).
 // Per column: the owning warp picks the pivot and publishes the column, every
-// warp takes the pivot row of its own columns by shuffles and swaps the two
-// rows, then every thread updates its 32 entries: one barrier per column.
-// Columns are visited slot by slot
+// warp exchanges the two rows of its own columns, then every thread updates its
+// 32 entries: one barrier per column (gj_step).  Columns are visited slot by slot
 // so that register indices are compile-time constants.  Output: inv (128 x 128,
 // column-major) = A_kk^{-1}; info flags an exactly zero pivot.
 __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* __restrict__ info,
                                                         float2* __restrict__ inv, int nblk,
                                                         float* __restrict__ binv, float* __restrict__ ainv) {
   __shared__ float2 colbuf[2][kB];
+  __shared__ float2 xbuf[16][2][8];  // per warp: its columns of the pivot row and of row j
   __shared__ int s_piv[2];
   __shared__ int perm[kB];
   const int b = blockIdx.x, tid = threadIdx.x;
@@ -208,9 +248,9 @@ __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* _
 #pragma unroll
     for (int m = 0; m < 8; ++m) a[i][m] = ldp(W, b, kk + lane + 32 * i, kk + w + 16 * m);
   if (tid < kB) perm[tid] = tid;
-  __syncthreads();
+  if (w == 0) gj_pivot<0>(a, 0, kk, b, lane, colbuf, s_piv, info);  // column 0 (warp 0, slot 0)
 #define BEM_GJ_SLOT(JM) \
-  for (int jw = 0; jw < 16; ++jw) gj_step<JM>(a, jw, kk, b, lane, w, tid, colbuf, s_piv, perm, info);
+  for (int jw = 0; jw < 16; ++jw) gj_step<JM>(a, jw, kk, b, lane, w, tid, colbuf, xbuf, s_piv, perm, info);
   BEM_GJ_SLOT(0)
   BEM_GJ_SLOT(1)
   BEM_GJ_SLOT(2)
