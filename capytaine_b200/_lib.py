@@ -63,7 +63,8 @@ class AssemblyArgs(ctypes.Structure):
         ("wavenumber", c_double), ("free_surface", c_double), ("gf_singularities", c_int),
         ("adjoint_double_layer", c_int), ("early_dot_product", c_int), ("diagonal_term", c_int), ("precision", c_int),
         ("out_dtype", c_int), ("S_dev", c_void_p), ("K_dev", c_void_p), ("lds", c_i64), ("ldk", c_i64),
-        ("k_plane_stride", c_i64), ("nan_flag_dev", c_void_p),
+        ("k_plane_stride", c_i64), ("nan_flag_dev", c_void_p), ("r_inv_den_dev", c_void_p),
+        ("z_inv_den_dev", c_void_p),
     ]
 
 
@@ -99,6 +100,7 @@ _SIGNATURES = {
     "bem_default_r_spacing": ([c_int, c_double, c_int, c_void_p], c_int),
     "bem_default_z_spacing": ([c_int, c_double, c_int, c_void_p], c_int),
     "bem_construct_tabulation": ([c_void_p, c_int, c_void_p, c_int, c_int, c_void_p, c_void_p], c_int),
+    "bem_tabulation_inverse_denominators": ([c_void_p, c_int, c_void_p], c_int),
     "bem_assemble": ([ctypes.POINTER(AssemblyArgs), c_void_p], c_int),
     "bem_assemble_rankine_part": ([ctypes.POINTER(AssemblyArgs), c_void_p, c_i64, c_void_p], c_int),
     "bem_assemble_wave_symmetric": ([ctypes.POINTER(AssemblyArgs), c_void_p, c_i64, c_void_p], c_int),

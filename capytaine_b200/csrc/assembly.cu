@@ -176,15 +176,17 @@ __device__ __forceinline__ int nearest_r_index(double r, int nr, double rmax, in
   if (r < 1.0) return f_nint((log10(r) / 10.0 + 1.0) * (double)(index_of_1 - 1) + 1);
   return f_nint((r - 1) * (double)(nr - index_of_1) / (rmax - 1) + (double)index_of_1);
 }
-__device__ __forceinline__ int nearest_z_index(double z, int nz, double zlast, int grid) {
+// dz: (log10|z_last| + 10) / nz of the scaled grid, computed once per thread
+// (the same arithmetic as per call).
+__device__ __forceinline__ int nearest_z_index(double z, int nz, double zlast, int grid, double dz) {
   const double absz = fabs(z);
   if (grid == kLegacyGrid) {
     if (absz > kLit1em2) return f_int(8 * (log10(absz) + 4.5));
     return f_int(5 * (log10(absz) + 6));
   }
-  const double dz = (log10(fabs(zlast)) + 10.0) / (double)nz;
   return f_nint((log10(absz) + 10) / dz);
 }
+__device__ __forceinline__ double scaled_dz(double zlast, int nz) { return (log10(fabs(zlast)) + 10.0) / (double)nz; }
 
 __device__ __forceinline__ double pl2(double u1, double u2, double u3, double x) {
   return ((x - u1) * (x - u2)) / ((u3 - u1) * (u3 - u2));
@@ -213,7 +215,33 @@ struct TabView {
   const double* tab;
   const float* tab32;
   double rmax, zlast;
+  // optional: reciprocals of the Lagrange denominators of each stencil
+  // (3 per centre node, bem_tabulation_inverse_denominators); NULL: divisions
+  const double* rinv;
+  const double* zinv;
+  double dz;
 };
+__device__ __forceinline__ void tab_prologue(TabView& T) {
+  if (T.nr > 1 && T.nz > 1) {
+    T.rmax = __ldg(T.r_range + T.nr - 1);
+    T.zlast = __ldg(T.z_range + T.nz - 1);
+    T.dz = scaled_dz(T.zlast, T.nz);
+  }
+}
+// Lagrange weights of the three stencil nodes u[0..2] at x (node i's weight
+// prod_{k != i} (x - u_k) / (u_i - u_k)), the reciprocal denominators from inv
+// when given.
+__device__ __forceinline__ void lagrange3(double x, double u1, double u2, double u3, const double* inv, double w[3]) {
+  if (inv) {
+    w[0] = ((x - u2) * (x - u3)) * __ldg(inv);
+    w[1] = ((x - u3) * (x - u1)) * __ldg(inv + 1);
+    w[2] = ((x - u1) * (x - u2)) * __ldg(inv + 2);
+  } else {
+    w[0] = pl2(u2, u3, u1, x);
+    w[1] = pl2(u3, u1, u2, x);
+    w[2] = pl2(u1, u2, u3, x);
+  }
+}
 
 // The five integrals at (r, z): table (3x3 Lagrange), asymptotic form or
 // direct integration (Green_wave.f90:226-240).
@@ -229,13 +257,16 @@ __device__ void integrals_at(double r, double z, const TabView& T, R out[5]) {
   if (fabs(z) < fabs(T.zlast) && r < T.rmax) {
     int i = nearest_r_index(r, T.nr, T.rmax, T.grid);
     i = max(2, min(T.nr - 1, i));
-    int j = nearest_z_index(z, T.nz, T.zlast, T.grid);
+    int j = nearest_z_index(z, T.nz, T.zlast, T.grid, T.dz);
     j = max(2, min(T.nz - 1, j));
     const int ic = i - 1, jc = j - 1;
     const double r1 = __ldg(T.r_range + ic - 1), r2 = __ldg(T.r_range + ic), r3 = __ldg(T.r_range + ic + 1);
     const double z1 = __ldg(T.z_range + jc - 1), z2 = __ldg(T.z_range + jc), z3 = __ldg(T.z_range + jc + 1);
-    const R xl0 = (R)pl2(r2, r3, r1, r), xl1 = (R)pl2(r3, r1, r2, r), xl2 = (R)pl2(r1, r2, r3, r);
-    const R zl0 = (R)pl2(z2, z3, z1, z), zl1 = (R)pl2(z3, z1, z2, z), zl2 = (R)pl2(z1, z2, z3, z);
+    double wr[3], wz[3];
+    lagrange3(r, r1, r2, r3, T.rinv ? T.rinv + 3 * ic : nullptr, wr);
+    lagrange3(z, z1, z2, z3, T.zinv ? T.zinv + 3 * jc : nullptr, wz);
+    const R xl0 = (R)wr[0], xl1 = (R)wr[1], xl2 = (R)wr[2];
+    const R zl0 = (R)wz[0], zl1 = (R)wz[1], zl2 = (R)wz[2];
     R acc[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) acc[k] = 0;
@@ -331,8 +362,7 @@ __global__ void __launch_bounds__(kRows, 4) assemble_kernel(const bem_assembly_a
   __shared__ FaceRec faces[kTileJ];
   if (T.nr > 1 && T.nz > 1) {
     // Grid bounds of the tabulation (last r and z values).
-    T.rmax = __ldg(T.r_range + T.nr - 1);
-    T.zlast = __ldg(T.z_range + T.nz - 1);
+    tab_prologue(T);
   }
   const int J0 = blockIdx.y * kTileJ;
   const int nJ = min(kTileJ, a.nb_faces - J0);
@@ -554,7 +584,7 @@ __device__ __forceinline__ void integrals_at_f32(double r, double z, const TabVi
   if (fabs(z) < fabs(T.zlast) && r < T.rmax) {
     int i = nearest_r_index(r, T.nr, T.rmax, T.grid);
     i = max(2, min(T.nr - 1, i));
-    int j = nearest_z_index(z, T.nz, T.zlast, T.grid);
+    int j = nearest_z_index(z, T.nz, T.zlast, T.grid, T.dz);
     j = max(2, min(T.nz - 1, j));
     const int ic = i - 1, jc = j - 1;
     const double r1 = __ldg(T.r_range + ic - 1), r2 = __ldg(T.r_range + ic), r3 = __ldg(T.r_range + ic + 1);
@@ -655,8 +685,7 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
   __shared__ SymFace faces[kSymT];
   __shared__ double4 mir[kSymChunk][kSymT];  // (S_w re, S_w im, K_w re, K_w im) of entries (J, I)
   if (T.nr > 1 && T.nz > 1) {
-    T.rmax = __ldg(T.r_range + T.nr - 1);
-    T.zlast = __ldg(T.z_range + T.nz - 1);
+    tab_prologue(T);
   }
   const int tid = threadIdx.x;
   const int N = a.n;
@@ -854,8 +883,7 @@ __global__ void __launch_bounds__(kRows) assemble_finite_depth_kernel(const bem_
                                                                       int gf_sing) {
   __shared__ FaceRec faces[kTileJ];
   if (T.nr > 1 && T.nz > 1) {
-    T.rmax = __ldg(T.r_range + T.nr - 1);
-    T.zlast = __ldg(T.z_range + T.nz - 1);
+    tab_prologue(T);
   }
   const int J0 = blockIdx.y * kTileJ;
   const int nJ = min(kTileJ, a.nb_faces - J0);
@@ -1056,7 +1084,7 @@ extern "C" int bem_assemble(const bem_assembly_args* args, void* stream) {
       return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble: mixed precision needs the float32 table");
   }
   const TabView T{a.tabulation_nb_integration_points, a.tabulation_grid_shape, a.nr, a.nz, a.r_range_dev,
-                  a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0};
+                  a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0, a.r_inv_den_dev, a.z_inv_den_dev, 0.0};
   int gf_sing = a.gf_singularities;
   // Singularity variant overrides of delhommeau.py:472-487.
   if (a.wavenumber == 0.0) gf_sing = kLowFreq;
@@ -1115,7 +1143,7 @@ extern "C" int bem_assemble_rankine_part(const bem_assembly_args* args, void* ou
   if (a.wavenumber == 0.0) gf_sing = kLowFreq;
   else if (std::isinf(a.wavenumber)) gf_sing = kHighFreq;
   const double sign_refl = (gf_sing == kHighFreq) ? -1.0 : 1.0;
-  const TabView T{0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0};
+  const TabView T{0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, 0.0};
   dim3 grid(ceil_div(a.n, kRows), ceil_div(a.nb_faces, kTileJ));
   cudaStream_t s = (cudaStream_t)stream;
   {
@@ -1192,7 +1220,7 @@ int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev
     return set_error(BEM_ERR_INVALID_ARGUMENT, msg);
   }
   const TabView T{a.tabulation_nb_integration_points, a.tabulation_grid_shape, a.nr, a.nz, a.r_range_dev,
-                  a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0};
+                  a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0, a.r_inv_den_dev, a.z_inv_den_dev, 0.0};
   const int nbi = ceil_div(a.n, kSymT), nbj = ceil_div(general ? a.nb_faces : a.n, kSymT);
   cudaStream_t s = (cudaStream_t)stream;
   int launches = 0;
@@ -1313,7 +1341,7 @@ extern "C" int bem_assemble_finite_depth(const bem_assembly_args* args, double d
   if (finite_k && !tabulated && a.tabulation_nb_integration_points <= 0)
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_assemble_finite_depth: nb_integration_points <= 0");
   const TabView T{a.tabulation_nb_integration_points, a.tabulation_grid_shape, a.nr, a.nz, a.r_range_dev,
-                  a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0};
+                  a.z_range_dev, a.table_dev, a.table32_dev, 0.0, 0.0, a.r_inv_den_dev, a.z_inv_den_dev, 0.0};
   // the caller picks the variant (delhommeau.py:467-487: the legacy method
   // takes low_freq before the wavenumber rules apply)
   const int gf_sing = a.gf_singularities;

@@ -77,13 +77,15 @@ constexpr long long kDefaultSpinLimit = 4000000;
 int zgemm_ts_enqueue(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
                      int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,
                      double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev,
-                     void* stream, const int* skip);
+                     void* stream, const int* skip, const int* mskip = nullptr);
+// skip: one flag (the whole call returns at once while it is set); mskip:
+// per-matrix flags (the work of matrix b is skipped while mskip[b] is set).
 int clu_solve_enqueue(void* work_dev, int npad, int batch, void* B_dev, int64_t ldb, int64_t strideB, int nrhs,
                       int* err_dev, cudaStream_t s, const int* skip, long long spin_limit = kDefaultSpinLimit,
-                      int withheld = -1);
+                      int withheld = -1, const int* mskip = nullptr);
 int zlu_solve_enqueue(const void* A_dev, int n, int64_t lda, int64_t stride, int batch, const int* piv_dev,
                       const void* work_dev, void* B_dev, int64_t ldb, int64_t strideB, int nrhs, int* err_dev,
-                      cudaStream_t s, const int* skip, long long spin_limit);
+                      cudaStream_t s, const int* skip, long long spin_limit, const int* mskip = nullptr);
 int* zlu_done_flag(void* work_dev, int n, int batch);
 
 }  // namespace bem

@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(256) ztrsm_persistent_kernel(const double2* __
                                                                const double2* __restrict__ inv, double2* B,
                                                                int64_t ldb, int64_t strideB, int nrhs, int forward,
                                                                int* flags, int* ticket, int* err, const int* skip,
-                                                               long long spin_limit) {
+                                                               long long spin_limit, const int* mskip) {
   if (skip && *skip) return;  // refinement already converged
   extern __shared__ double2 sm[];
   double2* Inv = sm;                 // inverse of the diagonal block, Inv[m*kLd + r]
@@ -383,6 +383,7 @@ __global__ void __launch_bounds__(256) ztrsm_persistent_kernel(const double2* __
   __syncthreads();
   const int t = s_t;
   const int b = t % batch;
+  if (mskip && mskip[b]) return;  // converged matrix: every CTA of it returns, no wait targets it
   const int step = t / batch;
   const int i = forward ? step : (nblk - 1 - step);
   const double2* Ab = A + (size_t)b * stride;
@@ -533,7 +534,9 @@ extern "C" int bem_zgemm(int M, int N, int K, double alpha, const void* A_dev, i
 
 extern "C" int64_t bem_zlu_workspace_bytes(int n, int batch) {
   const int nblk = n / kNB;
-  return (int64_t)batch * nblk * 2 * kNB * kNB * (int64_t)sizeof(double2) + (int64_t)batch * nblk * 4 + 256;
+  // inverses, block-row flags, then ticket, refinement flag and per-matrix convergence flags
+  return (int64_t)batch * nblk * 2 * kNB * kNB * (int64_t)sizeof(double2) + (int64_t)batch * nblk * 4 +
+         (int64_t)batch * 4 + 256;
 }
 
 extern "C" int bem_zlu_factor(void* A_dev, int n, int64_t lda, int64_t stride, int batch, int* piv_dev,
@@ -590,7 +593,7 @@ int* zlu_done_flag(void* work_dev, int n, int batch) {
 // on B; every launch returns at once while *skip != 0.
 int zlu_solve_enqueue(const void* A_dev, int n, int64_t lda, int64_t stride, int batch, const int* piv_dev,
                       const void* work_dev, void* B_dev, int64_t ldb, int64_t strideB, int nrhs, int* err_dev,
-                      cudaStream_t s, const int* skip, long long spin_limit) {
+                      cudaStream_t s, const int* skip, long long spin_limit, const int* mskip) {
   int st = configure_smem();
   if (st) return st;
   const int nblk = n / kNB;
@@ -606,7 +609,7 @@ int zlu_solve_enqueue(const void* A_dev, int n, int64_t lda, int64_t stride, int
       TimedLaunch tl(kKZtrsm, s);
       ztrsm_persistent_kernel<<<nblk * batch, 256, smem, s>>>((const double2*)A_dev, lda, stride, nblk, batch,
                                                              piv_dev, n, inv, Bc, ldb, strideB, nc, forward, flags,
-                                                             ticket, err_dev, skip, spin_limit);
+                                                             ticket, err_dev, skip, spin_limit, mskip);
       count_launches(1);
     }
   }

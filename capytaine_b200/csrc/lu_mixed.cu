@@ -132,15 +132,18 @@ __device__ __forceinline__ void gj_pivot(const float2 (&a)[4][8], int j, int kk,
 // Update of register slot M of this thread's entries for column step j: row j
 // becomes the normalised pivot row u, the pivot column (slot JM of warp jw)
 // -f / pivot, every other entry a - f u.
-template <int M>
-__device__ __forceinline__ void gj_update(float2 (&a)[4][8], const float2 (&f)[4], const float2 (&u)[8], int SJ,
+// (The rank-one update runs on every entry without conditions; the two
+// special cases are overwritten after it.)
+template <int M, int SJ>
+__device__ __forceinline__ void gj_update(float2 (&a)[4][8], const float2 (&f)[4], const float2 (&u)[8],
                                           bool own_row_j, bool pivot_col, float2 mdinv) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    if (i == SJ && own_row_j) a[i][M] = u[M];
-    else if (pivot_col) a[i][M] = fmul(f[i], mdinv);
-    else a[i][M] = ffms(a[i][M], f[i], u[M]);
+  for (int i = 0; i < 4; ++i) a[i][M] = ffms(a[i][M], f[i], u[M]);
+  if (pivot_col) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i][M] = fmul(f[i], mdinv);
   }
+  if (own_row_j) a[SJ][M] = u[M];
 }
 
 // One Gauss-Jordan column step, column j = 16 JM + jw (slot JM of warp jw,
@@ -162,13 +165,13 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
   const int lj = j & 31, lp = p & 31, sp = p >> 5;
   // rows p and j of this warp's columns: lane lp writes row p, lane lj row j
   if (lane == lp) {
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      float2 v = a[0][m];
-#pragma unroll
-      for (int i = 1; i < 4; ++i)
-        if (i == sp) v = a[i][m];
-      xbuf[w][0][m] = v;
+    switch (sp) {  // one lane: a branch per register slot instead of selects
+#define BEM_GJ_ROWOUT(S) \
+  case S:                \
+    _Pragma("unroll") for (int m = 0; m < 8; ++m) xbuf[w][0][m] = a[S][m]; \
+    break;
+      BEM_GJ_ROWOUT(0) BEM_GJ_ROWOUT(1) BEM_GJ_ROWOUT(2) BEM_GJ_ROWOUT(3)
+#undef BEM_GJ_ROWOUT
     }
   }
   if (p != j && lane == lj) {
@@ -181,12 +184,13 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
   for (int m = 0; m < 8; ++m) prow[m] = xbuf[w][0][m];
   if (p != j) {
     if (lane == lp) {  // row p takes the old row j; row j becomes u below
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const float2 v = xbuf[w][1][m];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          if (i == sp) a[i][m] = v;
+      switch (sp) {
+#define BEM_GJ_ROWIN(S) \
+  case S:               \
+    _Pragma("unroll") for (int m = 0; m < 8; ++m) a[S][m] = xbuf[w][1][m]; \
+    break;
+        BEM_GJ_ROWIN(0) BEM_GJ_ROWIN(1) BEM_GJ_ROWIN(2) BEM_GJ_ROWIN(3)
+#undef BEM_GJ_ROWIN
       }
     }
     if (tid == 0) {
@@ -207,22 +211,18 @@ __device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b
   const bool own_row_j = lane == lj;
   const int w1 = (j + 1) & 15;  // owner of column j + 1
   // slot JM first (column j + 1 lives there when jw < 15)
-  gj_update<JM>(a, f, u, SJ, own_row_j, w == jw, mdinv);
+  gj_update<JM, SJ>(a, f, u, own_row_j, w == jw, mdinv);
   if (jw < 15 && w == w1) gj_pivot<JM>(a, j + 1, kk, b, lane, colbuf, s_piv, info);
   if constexpr (JM < 7) {
-    gj_update<JM + 1>(a, f, u, SJ, own_row_j, false, mdinv);
+    gj_update<JM + 1, SJ>(a, f, u, own_row_j, false, mdinv);
     if (jw == 15 && w == w1) gj_pivot<JM + 1>(a, j + 1, kk, b, lane, colbuf, s_piv, info);
   }
-#pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    if (m == JM || m == JM + 1) continue;
-    // slots other than JM never hold the pivot column
+  // slots other than JM never hold the pivot column
 #define BEM_GJ_UPD(MM) \
-    if (m == MM) gj_update<MM>(a, f, u, SJ, own_row_j, false, mdinv);
-    BEM_GJ_UPD(0) BEM_GJ_UPD(1) BEM_GJ_UPD(2) BEM_GJ_UPD(3) BEM_GJ_UPD(4) BEM_GJ_UPD(5) BEM_GJ_UPD(6)
-    BEM_GJ_UPD(7)
+  if constexpr (MM != JM && MM != JM + 1) gj_update<MM, SJ>(a, f, u, own_row_j, false, mdinv);
+  BEM_GJ_UPD(0) BEM_GJ_UPD(1) BEM_GJ_UPD(2) BEM_GJ_UPD(3) BEM_GJ_UPD(4) BEM_GJ_UPD(5) BEM_GJ_UPD(6)
+  BEM_GJ_UPD(7)
 #undef BEM_GJ_UPD
-  }
 }
 
 // Inverse of the diagonal block A_kk by Gauss-Jordan elimination with partial
@@ -383,89 +383,27 @@ __device__ __forceinline__ void st_release_i(int* p, int v) {
 // the off-diagonal block of a dependency is copied to shared memory
 // asynchronously (real and imaginary planes, 16-byte copies) before waiting for
 // that dependency; the diagonal inverse is staged through the same buffer.
-// Each block product (128 x 128 complex tile times the 128 x NC right-hand
-// sides) runs on the tensor cores with warp-level TF32 MMAs (m16n8k8), each
-// operand split into a TF32 head and a TF32 tail and three products taken
-// (head x head, head x tail, tail x head), which keeps float32 accuracy; the
-// complex product is the real product [acc_r | acc_i] = [Tr | Ti] [[Yr, Yi],
-// [-Yi, Yr]] (K = 256).  Warp w owns rows 16 w .. 16 w + 15 of the tile.
-constexpr int kLdT = kB + 8;  // column stride of a staged tile: conflict-free fragment reads
-
-__device__ __forceinline__ uint32_t tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
-  return r;
-}
-__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
-  hi = tf32_rna(x);
-  lo = tf32_rna(x - __uint_as_float(hi));
-}
-__device__ __forceinline__ void mma_16x8x8_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// d[nt] (n-tile nt of 8 real columns: real parts of the complex columns for
-// nt < NT/2, imaginary parts beyond) = rows 16 w .. of T times Y (Y[m*NC + c]).
+// Thread (r, h) accumulates row r over the half h of the 128-long inner
+// dimension for all NC columns (one float pair per entry of the tile, NC/2
+// 16-byte broadcast reads of the right-hand sides); the halves meet in P.
 template <int NC>
-__device__ __forceinline__ void tile_mma(const float* __restrict__ Tre, const float* __restrict__ Tim,
-                                         const float2* __restrict__ Y, int w, int lane, float (&d)[NC / 4][4]) {
-  constexpr int NT = NC / 4;  // 2 NC real columns in tiles of 8
-  const int g = lane >> 2, t = lane & 3;
-  const int row = 16 * w + g;
+__device__ __forceinline__ void tile_times_rhs(const float* __restrict__ Tre, const float* __restrict__ Tim,
+                                               const float2* __restrict__ Y, int r, int h, float2 (&acc)[NC]) {
 #pragma unroll
-  for (int nt = 0; nt < NT; ++nt)
+  for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.0f, 0.0f);
+#pragma unroll 4
+  for (int m = 64 * h; m < 64 * h + 64; ++m) {
+    const float ar = Tre[m * kB + r], ai = Tim[m * kB + r];
+    const float4* y4 = reinterpret_cast<const float4*>(Y + m * NC);
 #pragma unroll
-    for (int e = 0; e < 4; ++e) d[nt][e] = 0.0f;
-#pragma unroll 2
-  for (int ks = 0; ks < 32; ++ks) {
-    const int half = ks >> 4;  // K rows 0..127: Tr against (Yr | Yi); 128..255: Ti against (-Yi | Yr)
-    const int m0 = (ks & 15) * 8;
-    const float* T = half ? Tim : Tre;
-    const float a[4] = {T[(m0 + t) * kLdT + row], T[(m0 + t) * kLdT + row + 8], T[(m0 + t + 4) * kLdT + row],
-                        T[(m0 + t + 4) * kLdT + row + 8]};
-    uint32_t ah[4], al[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) split_tf32(a[e], ah[e], al[e]);
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-      const bool im_col = nt >= NT / 2;
-      const int c = (nt % (NT / 2)) * 8 + g;
-      const float2 y0 = Y[(m0 + t) * NC + c], y1 = Y[(m0 + t + 4) * NC + c];
-      const float v0 = half == 0 ? (im_col ? y0.y : y0.x) : (im_col ? y0.x : -y0.y);
-      const float v1 = half == 0 ? (im_col ? y1.y : y1.x) : (im_col ? y1.x : -y1.y);
-      uint32_t b0h, b0l, b1h, b1l;
-      split_tf32(v0, b0h, b0l);
-      split_tf32(v1, b1h, b1l);
-      mma_16x8x8_tf32(d[nt], ah, b0h, b1h);
-      mma_16x8x8_tf32(d[nt], ah, b0l, b1l);
-      mma_16x8x8_tf32(d[nt], al, b0h, b1h);
+    for (int c2 = 0; c2 < NC / 2; ++c2) {
+      const float4 y = y4[c2];
+      acc[2 * c2].x = fmaf(ar, y.x, fmaf(-ai, y.y, acc[2 * c2].x));
+      acc[2 * c2].y = fmaf(ar, y.y, fmaf(ai, y.x, acc[2 * c2].y));
+      acc[2 * c2 + 1].x = fmaf(ar, y.z, fmaf(-ai, y.w, acc[2 * c2 + 1].x));
+      acc[2 * c2 + 1].y = fmaf(ar, y.w, fmaf(ai, y.z, acc[2 * c2 + 1].y));
     }
   }
-}
-
-// X (rows of warp w) = sign * d + (accumulate ? X : 0).
-template <int NC>
-__device__ __forceinline__ void tile_apply(float2* X, int w, int lane, const float (&d)[NC / 4][4], float sign,
-                                           bool accumulate) {
-  constexpr int NT = NC / 4;
-  const int g = lane >> 2, t = lane & 3;
-  const int row = 16 * w + g;
-#pragma unroll
-  for (int nt = 0; nt < NT / 2; ++nt)
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int c = nt * 8 + 2 * t + e;
-#pragma unroll
-      for (int hv = 0; hv < 2; ++hv) {
-        float2* x = X + (row + 8 * hv) * NC + c;
-        const float re = sign * d[nt][2 * hv + e], im = sign * d[nt + NT / 2][2 * hv + e];
-        *x = accumulate ? make_float2(x->x + re, x->y + im) : make_float2(re, im);
-      }
-    }
 }
 
 template <int NC>
@@ -473,20 +411,23 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
                                                                const float2* __restrict__ inv, double2* B,
                                                                int64_t ldb, int64_t strideB, int nrhs, int forward,
                                                                int* flags, int* ticket, int* err, const int* skip,
-                                                               long long spin_limit, int withheld) {
+                                                               long long spin_limit, int withheld,
+                                                               const int* mskip) {
   if (skip && *skip) return;  // refinement already converged
   extern __shared__ __align__(16) float fsmf[];
-  float* Lre = fsmf;  // Lre[m*kLdT + r], 128 x 128
-  float* Lim = Lre + kB * kLdT;
-  float2* X = reinterpret_cast<float2*>(Lim + kB * kLdT);  // X[r*NC + c]
-  float2* Y = X + kB * NC;                                   // Y[m*NC + c]
+  float* Lre = fsmf;  // Lre[m*kB + r], 128 x 128
+  float* Lim = Lre + kB * kB;
+  float2* X = reinterpret_cast<float2*>(Lim + kB * kB);  // X[r*NC + c]
+  float2* Y = X + kB * NC;                                 // Y[m*NC + c]
+  float2* P = Y + kB * NC;                                 // P[r*NC + c]
   __shared__ int s_t;
   const int tid = threadIdx.x;
-  const int warp = tid >> 5, lane = tid & 31;
+  const int r = tid & (kB - 1), h = tid >> 7;
   if (tid == 0) s_t = atomicAdd(ticket, 1);
   __syncthreads();
   const int t = s_t;
   const int b = t % batch, step = t / batch;
+  if (mskip && mskip[b]) return;  // converged matrix: every CTA of it returns, no wait targets it
   const int i = forward ? step : (nblk - 1 - step);
   double2* Bb = B + (size_t)b * strideB;
   const int r0 = i * kB;
@@ -502,20 +443,30 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   const int ndep = forward ? i : (nblk - 1 - i);
   const float* Wre = W.re + (size_t)b * W.stride;
   const float* Wim = W.im + (size_t)b * W.stride;
-  float d[NC / 4][4];
+  float2 acc[NC];
   if (!forward) {
     // x_i = A_ii^{-1} b_i - sum_j U'_ij x_j with U' = A_ii^{-1} U: the product
     // with the diagonal inverse comes first, off the chain of dependencies
     const float2* Inv = inv + ((size_t)b * nblk + i) * kB * kB;
     for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
       const float2 v = __ldg(Inv + idx);  // element (idx % 128, idx / 128)
-      Lre[(idx >> 7) * kLdT + (idx & (kB - 1))] = v.x;
-      Lim[(idx >> 7) * kLdT + (idx & (kB - 1))] = v.y;
+      Lre[idx] = v.x;
+      Lim[idx] = v.y;
     }
     __syncthreads();
-    tile_mma<NC>(Lre, Lim, X, warp, lane, d);
-    __syncthreads();  // every warp has read all of X
-    tile_apply<NC>(X, warp, lane, d, 1.0f, false);
+    tile_times_rhs<NC>(Lre, Lim, X, r, h, acc);
+    if (h == 1) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
+    }
+    __syncthreads();
+    if (h == 0) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float2 o = P[r * NC + c];
+        X[r * NC + c] = make_float2(acc[c].x + o.x, acc[c].y + o.y);
+      }
+    }
     __syncthreads();  // Lre/Lim are reused for the off-diagonal blocks
   }
   for (int q = 0; q < ndep; ++q) {
@@ -525,8 +476,8 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
     for (int idx = tid; idx < kB * 32; idx += blockDim.x) {
       const int m = idx >> 5, piece = idx & 31;
       const size_t g = (size_t)(r0 + piece * 4) + (size_t)(j * kB + m) * W.ld;
-      cp_async16(Lre + m * kLdT + piece * 4, Wre + g);
-      cp_async16(Lim + m * kLdT + piece * 4, Wim + g);
+      cp_async16(Lre + m * kB + piece * 4, Wre + g);
+      cp_async16(Lim + m * kB + piece * 4, Wim + g);
     }
     if (tid == 0) {
       long long it = 0;
@@ -550,9 +501,22 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
     }
     cp_async_wait_all();
     __syncthreads();
-    tile_mma<NC>(Lre, Lim, Y, warp, lane, d);
-    tile_apply<NC>(X, warp, lane, d, -1.0f, true);  // rows of this warp only
-    __syncthreads();  // Lre/Lim and Y are overwritten by the next dependency
+    tile_times_rhs<NC>(Lre, Lim, Y, r, h, acc);
+    if (h == 1) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
+    }
+    __syncthreads();
+    if (h == 0) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float2 o = P[r * NC + c];
+        float2 x = X[r * NC + c];
+        x.x -= acc[c].x + o.x;
+        x.y -= acc[c].y + o.y;
+        X[r * NC + c] = x;
+      }
+    }
   }
   // forward (unit block lower factor): y_i = X; backward: x_i = X
   __syncthreads();
@@ -570,13 +534,14 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   if (tid == 0 && i != withheld) st_release_i(flags + (size_t)b * nblk + i, 1);
 }
 
-constexpr int trsm_smem_bytes(int nc) { return 2 * kB * kLdT * (int)sizeof(float) + 2 * kB * nc * (int)sizeof(float2); }
+constexpr int trsm_smem_bytes(int nc) { return 2 * kB * kB * (int)sizeof(float) + 3 * kB * nc * (int)sizeof(float2); }
 
 // x += r (the correction solved in place in r), then r = b for the residual.
 __global__ void ir_update_kernel(double2* __restrict__ X, double2* __restrict__ R, const double2* __restrict__ Bv,
-                                 int n, int nrhs, int64_t ld, int64_t stride, const int* skip) {
+                                 int n, int nrhs, int64_t ld, int64_t stride, const int* skip, const int* mskip) {
   if (skip && *skip) return;
   const int b = blockIdx.z, c = blockIdx.y;
+  if (mskip && mskip[b]) return;  // this matrix has converged
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const size_t o = (size_t)b * stride + (size_t)c * ld + r;
     const double2 x = X[o], d = R[o];
@@ -587,9 +552,10 @@ __global__ void ir_update_kernel(double2* __restrict__ X, double2* __restrict__ 
 
 // Squared norms of columns: out[(b*nrhs + c)] = sum |V(:, c)|^2 over n rows.
 __global__ void colnorm2_kernel(const double2* __restrict__ V, int n, int64_t ld, int64_t stride,
-                                double* __restrict__ out, const int* skip) {
+                                double* __restrict__ out, const int* skip, const int* mskip) {
   if (skip && *skip) return;
   const int c = blockIdx.x, b = blockIdx.y, nrhs = gridDim.x;
+  if (mskip && mskip[b]) return;
   const double2* v = V + (size_t)b * stride + (size_t)c * ld;
   double s = 0.0;
   for (int r = threadIdx.x; r < n; r += blockDim.x) s += v[r].x * v[r].x + v[r].y * v[r].y;
@@ -603,17 +569,30 @@ __global__ void colnorm2_kernel(const double2* __restrict__ V, int n, int64_t ld
   if (threadIdx.x == 0) out[(size_t)b * nrhs + c] = red[0];
 }
 
-// Convergence test of one refinement iteration on the device: worst relative
-// residual max_v sqrt(|r_v|^2 / |b_v|^2) (absolute where b_v = 0), iteration
-// count; sets *done when worst <= tol so that the iterations enqueued after
-// this one return at once.  state: [worst, iterations].
-__global__ void refine_check_kernel(const double* __restrict__ bn, const double* __restrict__ rn, int nvec,
-                                    double tol, int* done, double* state) {
+// Convergence test of one refinement iteration on the device: relative
+// residual sqrt(|r_v|^2 / |b_v|^2) (absolute where b_v = 0) of every column,
+// per matrix the worst of its nrhs columns: a matrix whose worst is <= tol is
+// marked converged in mdone (the next iterations skip its work); *done when
+// every matrix has converged (the iterations enqueued after return at once).
+// state: [worst over all matrices, iterations].
+__global__ void refine_check_kernel(const double* __restrict__ bn, const double* __restrict__ rn, int nrhs,
+                                    int batch, double tol, int* done, double* state, int* mdone) {
   if (*done) return;
   __shared__ double red[32];
+  __shared__ int all_done;
+  if (threadIdx.x == 0) all_done = 1;
+  __syncthreads();
   double worst = 0.0;
-  for (int v = threadIdx.x; v < nvec; v += blockDim.x)
-    worst = fmax(worst, bn[v] > 0.0 ? sqrt(rn[v] / bn[v]) : sqrt(rn[v]));
+  for (int b = threadIdx.x; b < batch; b += blockDim.x) {
+    double wb = 0.0;
+    for (int c = 0; c < nrhs; ++c) {
+      const int v = b * nrhs + c;
+      wb = fmax(wb, bn[v] > 0.0 ? sqrt(rn[v] / bn[v]) : sqrt(rn[v]));
+    }
+    if (wb <= tol) mdone[b] = 1;
+    else all_done = 0;  // benign race: every writer writes 0
+    worst = fmax(worst, wb);
+  }
   for (int off = 16; off > 0; off >>= 1) worst = fmax(worst, __shfl_xor_sync(0xffffffffu, worst, off));
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = worst;
   __syncthreads();
@@ -621,7 +600,7 @@ __global__ void refine_check_kernel(const double* __restrict__ bn, const double*
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) worst = fmax(worst, red[w]);
     state[0] = worst;
     state[1] += 1.0;
-    if (worst <= tol) *done = 1;
+    if (all_done) *done = 1;
   }
 }
 
@@ -716,7 +695,7 @@ extern "C" int64_t bem_clu_workspace_bytes(int npad, int batch) {
          kOpBuffers * (int64_t)batch * 2 * npad * 2 * kB * 4 + (int64_t)batch * nblk * kB * kB * 8 +
          (int64_t)batch * (2 * kB) * kSplitK * 4 + (int64_t)batch * npad * kSplitK * 4 +
          (int64_t)batch * kB * 2 * kB * 4 +
-         ((int64_t)batch * nblk + 2) * 4 + 1024;
+         ((int64_t)batch * nblk + 2 + batch) * 4 + 1024;
 }
 
 namespace bem {
@@ -764,11 +743,12 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
                                                                            npad, W);
   ++launches;
   const size_t abuf = (size_t)batch * npad * 2 * kB, bbuf = (size_t)batch * 2 * npad * 2 * kB;
-  // The big trailing updates give each CTA runs of 8 tiles (the accumulator
-  // double buffer pays over a run); the side stream's panel products, whose
-  // latency is the lookahead chain, one tile per CTA.  CTAs retire after their
-  // run, so the side stream's kernels take SMs as they free up.
-  constexpr int kBigRun = 8, kSideRun = 1;
+  // The big trailing updates give each CTA runs of up to 32 tiles (the
+  // accumulator double buffer pays over a run; the runs end at staggered
+  // times, so an SM frees up every few microseconds); the side stream's panel
+  // products, whose latency is the lookahead chain, one tile per CTA.  The
+  // side stream's kernels take SMs as they free up.
+  constexpr int kBigRun = 0, kSideRun = 1;
   float* Aop[kOpBuffers] = {w.Aop, w.Aop + abuf, w.Aop + 2 * abuf};
   float* Bop[kOpBuffers] = {w.Bop, w.Bop + bbuf, w.Bop + 2 * bbuf};
   // Inverse of the diagonal block, then the panel: A12 and A21 packed, L21 =
@@ -851,7 +831,8 @@ namespace bem {
 // B (npad x nrhs complex128 per matrix); returns at once while *skip != 0.  Also
 // the preconditioner of the GMRES solver.
 int clu_solve_enqueue(void* work_dev, int npad, int batch, void* B_dev, int64_t ldb, int64_t strideB, int nrhs,
-                      int* err_dev, cudaStream_t s, const int* skip, long long spin_limit, int withheld) {
+                      int* err_dev, cudaStream_t s, const int* skip, long long spin_limit, int withheld,
+                      const int* mskip) {
   int st = configure_mixed();
   if (st) return st;
   MixedWork w = carve(work_dev, npad, batch);
@@ -868,11 +849,11 @@ int clu_solve_enqueue(void* work_dev, int npad, int batch, void* B_dev, int64_t 
       if (nc <= 8)
         ctrsm_persistent_kernel<8><<<nblk * batch, 256, trsm_smem_bytes(8), s>>>(
             W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip, spin_limit,
-            withheld);
+            withheld, mskip);
       else
         ctrsm_persistent_kernel<16><<<nblk * batch, 256, trsm_smem_bytes(16), s>>>(
             W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip, spin_limit,
-            withheld);
+            withheld, mskip);
       ++launches;
     }
   }
@@ -916,7 +897,8 @@ namespace bem {
 // column, convergence flag on the device.  `done` is an int of the solver's
 // workspace; norms_dev holds 2 batch nrhs + 2 doubles.
 template <class Solve>
-int refine_loop(Solve solve_in_place, int* done, const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad,
+int refine_loop(Solve solve_in_place, int* done, int* mdone, const void* K_dev, int64_t ldk, int64_t strideK, int n,
+                int npad,
                 int batch, const void* B_dev, void* X_dev, void* R_dev, int64_t ldb, int64_t strideB, int nrhs,
                 double tol, int max_iter, void* ts_work_dev, double* norms_dev, int* iters_out, double* resid_out,
                 cudaStream_t s) {
@@ -926,7 +908,8 @@ int refine_loop(Solve solve_in_place, int* done, const void* K_dev, int64_t ldk,
   double* state = norms_dev + 2 * nvec;  // [worst, iterations]
   int launches = 1;
   // |b|^2 per column; x = 0, r = b, not converged
-  colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)B_dev, n, ldb, strideB, bn, nullptr);
+  colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)B_dev, n, ldb, strideB, bn, nullptr,
+                                                    nullptr);
   // Only the nrhs columns of each matrix: the caller may interleave other
   // columns (a wider right-hand-side block solved in chunks) between them.
   for (int b = 0; b < batch; ++b) {
@@ -937,6 +920,7 @@ int refine_loop(Solve solve_in_place, int* done, const void* K_dev, int64_t ldk,
                                      s));
   }
   BEM_CUDA_CHECK(cudaMemsetAsync(done, 0, sizeof(int), s));
+  BEM_CUDA_CHECK(cudaMemsetAsync(mdone, 0, sizeof(int) * batch, s));
   BEM_CUDA_CHECK(cudaMemsetAsync(state, 0, 2 * sizeof(double), s));
   // Iterations are enqueued in groups without host synchronisation; once the
   // device-side test has converged the rest of the group returns at once.
@@ -947,16 +931,16 @@ int refine_loop(Solve solve_in_place, int* done, const void* K_dev, int64_t ldk,
     const int group = std::min(kGroup, max_iter - enqueued);
     for (int g = 0; g < group; ++g) {
       // r <- F^{-1} r in place (the padded rows of r stay zero)
-      int st = solve_in_place(R_dev, (const int*)done);
+      int st = solve_in_place(R_dev, (const int*)done, (const int*)mdone);
       if (st) return st;
-      // x += r ; r = b ; r -= K x (float64)
+      // x += r ; r = b ; r -= K x (float64); matrices already converged skip all of it
       ir_update_kernel<<<dim3(ceil_div(n, 256), nrhs, batch), 256, 0, s>>>(
-          (double2*)X_dev, (double2*)R_dev, (const double2*)B_dev, n, nrhs, ldb, strideB, done);
+          (double2*)X_dev, (double2*)R_dev, (const double2*)B_dev, n, nrhs, ldb, strideB, done, mdone);
       st = zgemm_ts_enqueue(n, n, nrhs, -1.0, 0.0, K_dev, ldk, strideK, X_dev, ldb, strideB, 1.0, 0.0, R_dev, ldb,
-                            strideB, batch, ts_work_dev, s, done);
+                            strideB, batch, ts_work_dev, s, done, mdone);
       if (st) return st;
-      colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)R_dev, n, ldb, strideB, rn, done);
-      refine_check_kernel<<<1, 256, 0, s>>>(bn, rn, nvec, tol, done, state);
+      colnorm2_kernel<<<dim3(nrhs, batch), 256, 0, s>>>((const double2*)R_dev, n, ldb, strideB, rn, done, mdone);
+      refine_check_kernel<<<1, 256, 0, s>>>(bn, rn, nrhs, batch, tol, done, state, mdone);
       launches += 3;
     }
     enqueued += group;
@@ -994,10 +978,12 @@ extern "C" int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK,
   cudaStream_t s = (cudaStream_t)stream;
   MixedWork w = carve(work_dev, npad, batch);
   int* done = w.flags + (size_t)batch * (npad / kB) + 1;
-  auto solve = [&](void* R, const int* skip) {
-    return clu_solve_enqueue(work_dev, npad, batch, R, ldb, strideB, nrhs, err_dev, s, skip);
+  int* mdone = done + 1;  // batch ints (bem_clu_workspace_bytes counts them)
+  auto solve = [&](void* R, const int* skip, const int* mskip) {
+    return clu_solve_enqueue(work_dev, npad, batch, R, ldb, strideB, nrhs, err_dev, s, skip, kDefaultSpinLimit, -1,
+                             mskip);
   };
-  return refine_loop(solve, done, K_dev, ldk, strideK, n, npad, batch, B_dev, X_dev, R_dev, ldb, strideB, nrhs, tol,
+  return refine_loop(solve, done, mdone, K_dev, ldk, strideK, n, npad, batch, B_dev, X_dev, R_dev, ldb, strideB, nrhs, tol,
                      max_iter, ts_work_dev, norms_dev, iters_out, resid_out, s);
 }
 
@@ -1013,10 +999,11 @@ extern "C" int bem_zlu_refine_solve(const void* K_dev, int64_t ldk, int64_t stri
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zlu_refine_solve: bad arguments (nrhs <= 16, npad % 64 == 0)");
   cudaStream_t s = (cudaStream_t)stream;
   int* done = zlu_done_flag(lu_work_dev, npad, batch);
-  auto solve = [&](void* R, const int* skip) {
+  int* mdone = done + 1;  // batch ints (bem_zlu_workspace_bytes counts them)
+  auto solve = [&](void* R, const int* skip, const int* mskip) {
     return zlu_solve_enqueue(LU_dev, npad, ldlu, strideLU, batch, piv_dev, lu_work_dev, R, ldb, strideB, nrhs,
-                             err_dev, s, skip, kDefaultSpinLimit);
+                             err_dev, s, skip, kDefaultSpinLimit, mskip);
   };
-  return refine_loop(solve, done, K_dev, ldk, strideK, n, npad, batch, B_dev, X_dev, R_dev, ldb, strideB, nrhs, tol,
+  return refine_loop(solve, done, mdone, K_dev, ldk, strideK, n, npad, batch, B_dev, X_dev, R_dev, ldb, strideB, nrhs, tol,
                      max_iter, ts_work_dev, norms_dev, iters_out, resid_out, s);
 }

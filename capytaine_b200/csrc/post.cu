@@ -93,10 +93,12 @@ __global__ void __launch_bounds__(kTsRows) zgemm_ts_partial_kernel(int M, int K,
                                                                   const double2* __restrict__ A, int64_t lda,
                                                                   int64_t strideA, const double2* __restrict__ X,
                                                                   int64_t ldx, int64_t strideX,
-                                                                  double2* __restrict__ part, const int* skip) {
+                                                                  double2* __restrict__ part, const int* skip,
+                                                                  const int* mskip) {
   if (skip && *skip) return;
   extern __shared__ double2 xs[];  // xs[kk * NC + c]
   const int b = blockIdx.z;
+  if (mskip && mskip[b]) return;  // matrix b is not needed (converged)
   const int split = blockIdx.y;
   const int k0 = split * kchunk;
   const int kc = min(K, k0 + kchunk) - k0;
@@ -138,10 +140,11 @@ __global__ void __launch_bounds__(kTsRows) zgemm_ts_partial_kernel(int M, int K,
 
 __global__ void zgemm_ts_reduce_kernel(int M, int nrhs, int nsplit, double2 alpha, double2 beta,
                                        const double2* __restrict__ part, double2* __restrict__ Y, int64_t ldy,
-                                       int64_t strideY, const int* skip) {
+                                       int64_t strideY, const int* skip, const int* mskip) {
   if (skip && *skip) return;
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   const int c = blockIdx.y, b = blockIdx.z;
+  if (mskip && mskip[b]) return;
   if (row >= M) return;
   double2 s = make_double2(0.0, 0.0);
   for (int sp = 0; sp < nsplit; ++sp) {
@@ -266,7 +269,7 @@ namespace bem {
 int zgemm_ts_enqueue(int M, int K, int nrhs, double alpha_re, double alpha_im, const void* A_dev, int64_t lda,
                      int64_t strideA, const void* X_dev, int64_t ldx, int64_t strideX, double beta_re,
                      double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev,
-                     void* stream, const int* skip) {
+                     void* stream, const int* skip, const int* mskip) {
   if (M <= 0 || K <= 0 || nrhs <= 0 || nrhs > kTsMaxRhs || batch <= 0 || !A_dev || !X_dev || !Y_dev || !work_dev ||
       lda < M || ldx < K || ldy < M)
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_zgemm_ts: bad arguments (nrhs must be <= 16)");
@@ -288,13 +291,15 @@ int zgemm_ts_enqueue(int M, int K, int nrhs, double alpha_re, double alpha_im, c
   const dim3 grid(ceil_div(M, kTsRows), nsplit, batch);
   if (nc == 8)
     zgemm_ts_partial_kernel<8><<<grid, kTsRows, smem, s>>>(M, K, nrhs, kchunk, (const double2*)A_dev, lda, strideA,
-                                                           (const double2*)X_dev, ldx, strideX, (double2*)work_dev, skip);
+                                                           (const double2*)X_dev, ldx, strideX, (double2*)work_dev, skip,
+                                                           mskip);
   else
     zgemm_ts_partial_kernel<16><<<grid, kTsRows, smem, s>>>(M, K, nrhs, kchunk, (const double2*)A_dev, lda, strideA,
-                                                            (const double2*)X_dev, ldx, strideX, (double2*)work_dev, skip);
+                                                            (const double2*)X_dev, ldx, strideX, (double2*)work_dev, skip,
+                                                           mskip);
   zgemm_ts_reduce_kernel<<<dim3(ceil_div(M, 256), nrhs, batch), 256, 0, s>>>(
       M, nrhs, nsplit, make_double2(alpha_re, alpha_im), make_double2(beta_re, beta_im), (const double2*)work_dev,
-      (double2*)Y_dev, ldy, strideY, skip);
+      (double2*)Y_dev, ldy, strideY, skip, mskip);
   count_launches(2);
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
@@ -306,7 +311,7 @@ extern "C" int bem_zgemm_ts(int M, int K, int nrhs, double alpha_re, double alph
                             double beta_im, void* Y_dev, int64_t ldy, int64_t strideY, int batch, void* work_dev,
                             void* stream) {
   return bem::zgemm_ts_enqueue(M, K, nrhs, alpha_re, alpha_im, A_dev, lda, strideA, X_dev, ldx, strideX, beta_re,
-                               beta_im, Y_dev, ldy, strideY, batch, work_dev, stream, nullptr);
+                               beta_im, Y_dev, ldy, strideY, batch, work_dev, stream, nullptr, nullptr);
 }
 
 extern "C" int bem_integrate_pressure(int n, int batch, int nrhs, int ndof, const void* phi_dev, int64_t ldp,

@@ -84,3 +84,16 @@ extern "C" int bem_construct_tabulation(const double* r_range_dev, int nr, const
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;
 }
+
+extern "C" int bem_tabulation_inverse_denominators(const double* range_host, int n, double* out_host) {
+  if (!range_host || !out_host || n < 3)
+    return bem::set_error(BEM_ERR_INVALID_ARGUMENT, "bem_tabulation_inverse_denominators: bad arguments");
+  for (int i = 0; i < 3 * n; ++i) out_host[i] = 0.0;
+  for (int c = 1; c + 1 < n; ++c) {
+    const double u1 = range_host[c - 1], u2 = range_host[c], u3 = range_host[c + 1];
+    out_host[3 * c] = 1.0 / ((u1 - u2) * (u1 - u3));
+    out_host[3 * c + 1] = 1.0 / ((u2 - u3) * (u2 - u1));
+    out_host[3 * c + 2] = 1.0 / ((u3 - u1) * (u3 - u2));
+  }
+  return BEM_OK;
+}

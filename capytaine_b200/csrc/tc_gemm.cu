@@ -422,7 +422,7 @@ int num_sms(int* out) {
 
 // Host entry shared with the LU: C (trailing block m x n complex, both multiples
 // of 128) -= A' B' for `batch` matrices.  run > 0: tiles per CTA; 0: chosen
-// from the tile count (up to 8 while there are at least two runs per SM).
+// from the tile count (up to 32 while there are at least two runs per SM).
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store, const float* Aop1,
@@ -490,7 +490,7 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
     if (ntiles > (1ll << 30)) return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: too many tiles");
     if (ntiles == 0) continue;
     p.ntiles = (int)ntiles;
-    int tpc = run > 0 ? run : (int)std::max(1ll, std::min(8ll, ntiles / (2ll * sms)));
+    int tpc = run > 0 ? run : (int)std::max(1ll, std::min(32ll, ntiles / (2ll * sms)));
     const long long ctas = (ntiles + tpc - 1) / tpc;
     UpdateArgs q = p;
     q.tiles_per_cta = tpc;

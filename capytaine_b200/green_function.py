@@ -123,6 +123,7 @@ class Delhommeau:
         self.tabulated_z_range = self._spacing("z")
         self._tab_host = None
         self._dev_tab = None
+        self._dev_tab_inv = (0, 0)
         self._mesh_cache: "OrderedDict[str, DeviceMesh]" = OrderedDict()
         # The caches are shared by the threads (and CUDA streams) of a request
         # server: dictionary updates under this lock, device readiness through
@@ -268,6 +269,20 @@ class Delhommeau:
                     except OSError:
                         LOG.warning("Could not save tabulation to %s", path)
         self._dev_tab = (r, z, table, table.to(torch.float32))
+        # reciprocal denominators of the Lagrange weights of both grids: the
+        # lookup multiplies instead of dividing (bem_tabulation_inverse_denominators)
+        self._dev_tab_inv = (0, 0)
+        if nr > 2 and nz > 2:
+            inv = []
+            for rng in (np.ascontiguousarray(self.tabulated_r_range, dtype=np.float64),
+                        np.ascontiguousarray(self.tabulated_z_range, dtype=np.float64)):
+                out = np.zeros(3 * len(rng))
+                _lib.check(_lib.load().bem_tabulation_inverse_denominators(rng.ctypes.data_as(_lib.c_void_p),
+                                                                           len(rng),
+                                                                           out.ctypes.data_as(_lib.c_void_p)))
+                inv.append(torch.as_tensor(out, device=dev))
+            self._dev_tab_inv_tensors = tuple(inv)
+            self._dev_tab_inv = tuple(t.data_ptr() for t in inv)
         self._dev_tab_shared = _lib.StreamShared(*self._dev_tab)
 
     @property
@@ -383,6 +398,8 @@ class Delhommeau:
             r_range_dev=r.data_ptr() if r is not None else 0, z_range_dev=z.data_ptr() if z is not None else 0,
             table_dev=table.data_ptr() if table is not None else 0,
             table32_dev=table32.data_ptr() if table32 is not None else 0,
+            r_inv_den_dev=self._dev_tab_inv[0] if table is not None else 0,
+            z_inv_den_dev=self._dev_tab_inv[1] if table is not None else 0,
             wavenumber=wavenumber, free_surface=float(free_surface), gf_singularities=_SING[sing],
             adjoint_double_layer=int(bool(adjoint_double_layer)), early_dot_product=int(bool(early_dot_product)),
             diagonal_term=int(bool(diagonal_term_in_double_layer)),
@@ -532,6 +549,8 @@ class Delhommeau:
             r_range_dev=r.data_ptr() if r is not None else 0, z_range_dev=z.data_ptr() if z is not None else 0,
             table_dev=table.data_ptr() if table is not None else 0,
             table32_dev=table32.data_ptr() if table32 is not None else 0,
+            r_inv_den_dev=self._dev_tab_inv[0] if table is not None else 0,
+            z_inv_den_dev=self._dev_tab_inv[1] if table is not None else 0,
             wavenumber=k, free_surface=float(free_surface), gf_singularities=_SING[sing],
             adjoint_double_layer=int(bool(adjoint_double_layer)), early_dot_product=int(bool(early_dot_product)),
             diagonal_term=int(bool(diagonal_term_in_double_layer)), precision=_lib.BEM_PREC_FP64,

@@ -80,6 +80,15 @@ int bem_default_z_spacing(int nz, double zmin, int grid_shape, double* z_range_h
 int bem_construct_tabulation(const double* r_range_dev, int nr, const double* z_range_dev, int nz,
                              int nb_integration_points, double* table_dev, void* stream);
 
+/* Reciprocals of the denominators of the 3-point Lagrange weights of a grid
+ * (range, n values, host): out[3 c + i] = 1 / prod_{k != i} (u_i - u_k) for
+ * the stencil u = range[c - 1 .. c + 1] centred on node c (1 <= c <= n - 2;
+ * the other rows are zero).  Given to the assembly (bem_assembly_args
+ * r_inv_den_dev / z_inv_den_dev), the interpolation of the tabulated integrals
+ * (Delhommeau_integrals.f90:383-392) multiplies instead of dividing; the
+ * weights change by an ulp at most.  No counterpart in the reference. */
+int bem_tabulation_inverse_denominators(const double* range_host, int n, double* out_host);
+
 /* ---- assembly of the influence matrices ----------------------------------- */
 typedef struct {
   /* collocation side (mesh1 or a raw list of points) */
@@ -123,6 +132,10 @@ typedef struct {
   int64_t ldk;
   int64_t k_plane_stride;          /* elements between gradient planes when !early_dot_product */
   int32_t* nan_flag_dev;           /* optional: set to 1 if a NaN was produced                  */
+  /* optional: reciprocal Lagrange denominators of the table's r and z grids
+   * (3 per node, bem_tabulation_inverse_denominators); NULL: divided each time */
+  const double* r_inv_den_dev;     /* (nr, 3)                                                  */
+  const double* z_inv_den_dev;     /* (nz, 3)                                                  */
 } bem_assembly_args;
 
 /* S and K (or D, or the full gradient) for one wavenumber, infinite depth.

@@ -6,7 +6,8 @@
   float64 solve therefore checks its residual against the unfactored matrix
   and refines it (bem_zlu_refine_solve).  Matrices whose correct pivots lie
   outside the diagonal blocks (rows of a diagonally dominant matrix moved to
-  other blocks) must still match numpy's solve to 1e-12, or be flagged.
+  other blocks) must still match numpy's solve to 1e-12 (normwise, per right-hand side), or
+  be flagged.
 * The flag waits of the persistent block substitutions are bounded: with one
   block row's completion flag withheld, the waits on it run out, the kernel
   reports BEM_ERR_TIMEOUT through the error flag, and the stream stays usable.
@@ -53,7 +54,8 @@ def test_fp64_solve_with_off_block_pivots(perm, n):
         x = eng.linear_solver(DeviceMatrix(_to_device(np.asfortranarray(K), eng.device), eng), b)
     except (_lib.NotConvergedError, _lib.SingularMatrixError):
         return  # flagged: acceptable, never a silent loss
-    assert np.abs(x - ref).max() / np.abs(ref).max() < 1e-12, perm
+    # normwise relative error per right-hand side (the residual test is normwise)
+    assert np.max(np.linalg.norm(x - ref, axis=0) / np.linalg.norm(ref, axis=0)) < 1e-12, perm
 
 
 def test_fp64_refined_solve_through_the_c_abi():
@@ -95,7 +97,7 @@ def test_fp64_refined_solve_through_the_c_abi():
     for i in range(batch):
         x = X[i, :, :n].T.cpu().numpy()
         ref = np.linalg.solve(mats[i], rhs[i])
-        assert np.abs(x - ref).max() / np.abs(ref).max() < 1e-12, i
+        assert np.max(np.linalg.norm(x - ref, axis=0) / np.linalg.norm(ref, axis=0)) < 1e-12, i
 
 
 def test_fp64_engine_reports_its_residual(oracle_mod, default_oracle_gf, tmp_path):
