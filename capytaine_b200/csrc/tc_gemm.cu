@@ -147,7 +147,8 @@ struct UpdateArgs {
   int tiles_m;       // tile grid: tiles_m x tiles_n x batch, tm fastest
   int tiles_n;
   int ntiles;
-  int tiles_per_cta;     // consecutive tiles of one CTA
+  int tiles_per_cta;     // tiles of one CTA
+  int group_width;       // CTAs per group (the SM count)
   long long wait_limit;  // polls of a bounded mbarrier wait
   // Grouped launch (ngroup > 0): matrix b has gtm[b] x gtn[b] tiles of its own,
   // tiles gstart[b] .. gstart[b+1]-1 (matrices of different active sizes)
@@ -194,11 +195,12 @@ __device__ __forceinline__ bool mbar_wait_n(uint64_t* bar, uint32_t parity, int*
 
 // Trailing update with double-buffered accumulators: a CTA (one per SM: 197 KB
 // of shared memory, all 512 tensor-memory columns) takes a run of
-// tiles_per_cta consecutive 128 x 128 complex tiles and alternates between two
-// accumulators in tensor memory, so that the epilogue of tile i (read C,
-// subtract, write C) overlaps the MMAs of tile i+1.  CTAs retire after their
-// run, so kernels of other streams (the lookahead of the block LU) get SMs
-// within one run.  Barriers: full/empty per operand stage (TMA -> MMA -> TMA),
+// tiles_per_cta 128 x 128 complex tiles, spaced so that the CTAs of a group
+// work on consecutive tiles at any time (their operands stay in L2), and
+// alternates between two accumulators in tensor memory, so that the epilogue
+// of tile i (read C, subtract, write C) overlaps the MMAs of tile i+1.  CTAs
+// retire after their run, so kernels of other streams (the lookahead of the
+// block LU) get SMs within one run.  Barriers: full/empty per operand stage (TMA -> MMA -> TMA),
 // acc_full per accumulator (MMA commit -> epilogue), acc_empty per
 // accumulator (one arrival per epilogue warp -> MMA).
 __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
@@ -245,16 +247,22 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  // this CTA's tiles: a run of consecutive tiles (tm fastest: they share B)
-  const int t_begin = blockIdx.x * p.tiles_per_cta;
-  const int t_end = min(p.ntiles, t_begin + p.tiles_per_cta);
+  // This CTA's tiles: CTAs form groups of group_width (one per SM); group g
+  // covers tiles [g W T, (g+1) W T) and its CTA l takes the tiles
+  // g W T + l + j W_g (j < T, W_g the width of this group), so the CTAs of a
+  // group work on W consecutive tiles at a time (tm fastest: they share the
+  // operands in L2) and each retires after T tiles.
+  const int T = p.tiles_per_cta, Wd = p.group_width;
+  const int grp = blockIdx.x / Wd, l = blockIdx.x - grp * Wd;
+  const int Wg = min(Wd, (int)gridDim.x - grp * Wd);
+  const int t_first = grp * Wd * T + l;
 
   if (warp == 0) {
     if (lane == 0) {
       // producer: operand slices of every tile of this CTA through the ring
       bool ok = true;
       long long g = 0;  // stage uses so far
-      for (int t = t_begin; t < t_end && ok; ++t) {
+      for (int jt = 0, t = t_first; jt < T && t < p.ntiles && ok; ++jt, t += Wg) {
         int b, tm, tn;
         decode_tile(p, t, b, tm, tn);
         b += p.batch0;
@@ -280,7 +288,7 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
       bool ok = true;
       long long g = 0;
       int i = 0;  // tiles of this CTA so far
-      for (int t = t_begin; t < t_end && ok; ++t, ++i) {
+      for (int jt = 0, t = t_first; jt < T && t < p.ntiles && ok; ++jt, t += Wg, ++i) {
         const int acc = i & 1;
         const uint32_t use = (uint32_t)(i >> 1);
         // the epilogue must have drained this accumulator's previous tile
@@ -319,7 +327,7 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
     const int64_t ldc = p.ldc;
     bool ok = true;
     int i = 0;
-    for (int t = t_begin; t < t_end && ok; ++t, ++i) {
+    for (int jt = 0, t = t_first; jt < T && t < p.ntiles && ok; ++jt, t += Wg, ++i) {
       int b, tm, tn;
       decode_tile(p, t, b, tm, tn);
       b += p.batch0;
@@ -494,6 +502,7 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
     const long long ctas = (ntiles + tpc - 1) / tpc;
     UpdateArgs q = p;
     q.tiles_per_cta = tpc;
+    q.group_width = sms;
     q.batch0 = b0;  // the matrices of this launch: b0 .. b0 + nb - 1
     {
       TimedLaunch tl(kKCgemmTf32, stream);
