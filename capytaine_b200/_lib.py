@@ -254,5 +254,17 @@ class StreamShared:
         return self
 
 
+def upload(a, dtype, device):
+    """Host array -> device tensor of `dtype` on the current stream without
+    waiting for the stream: the values go through pinned host memory (the
+    caching host allocator keeps the staging block until the copy has run)."""
+    import numpy as np
+    import torch
+    host = torch.from_numpy(np.ascontiguousarray(a)).to(dtype)
+    if torch.device(device).type != "cuda":
+        return host.to(device)
+    return host.pin_memory().to(device, non_blocking=True)
+
+
 def ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)

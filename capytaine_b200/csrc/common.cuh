@@ -88,6 +88,27 @@ int zlu_solve_enqueue(const void* A_dev, int n, int64_t lda, int64_t stride, int
                       cudaStream_t s, const int* skip, long long spin_limit, const int* mskip = nullptr);
 int* zlu_done_flag(void* work_dev, int n, int batch);
 
+// Packed copies of a complex update's result (tc_gemm.cu), written by its
+// epilogue in the operand layouts of the next block step of the mixed LU:
+//   kPackRows:      row i -> [Re C(i, 0..127) | Im C(i, 0..127)]           (n = 128)
+//   kPackRowsSplit: row i -> [hi | lo | hi] of that row, hi the TF32 part  (n = 128)
+//   kPackCols:      complex column j0 + t (j0 the tile's first column) ->
+//                   rows 2 j0 + t: [Re C(:, j) | -Im C(:, j)] and
+//                   2 j0 + 128 + t: [Im C(:, j) | Re C(:, j)] over the
+//                   128 rows of C                                          (m = 128)
+enum PackMode { kPackNone = 0, kPackRows = 1, kPackRowsSplit = 2, kPackCols = 3 };
+
+// C (m x n complex in two float32 planes) -= A' B' (store = 0) or = A' B'
+// (store = 1) on the tensor cores from packed operands; an optional second
+// operand pair adds K' depth in the same pass over C; limit_host: per-matrix
+// active sizes (grouped launches); pack: a packed copy of the result.
+int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
+                      int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
+                      int n, int batch, int* err, cudaStream_t stream, int store = 0, const float* Aop1 = nullptr,
+                      const float* Bop1 = nullptr, int run = 0, long long wait_limit = 0,
+                      const int* limit_host = nullptr, float* pack = nullptr, int pack_mode = kPackNone,
+                      int64_t pack_stride = 0);
+
 }  // namespace bem
 
 #define BEM_CUDA_CHECK(call)                                  \

@@ -10,8 +10,8 @@
 //     with partial pivoting among its rows, held in registers; the panel is the
 //     product A21 A_kk^{-1}; the trailing update C -= L21 U12 runs on the
 //     tcgen05 tensor cores (TF32 inputs, FP32 accumulation; tc_gemm.cu) from
-//     operands the panel kernel packs.  No row permutation leaves the diagonal
-//     blocks, so the solves need none;
+//     operands that the epilogues of the updates finishing them write packed.
+//     No row permutation leaves the diagonal blocks, so the solves need none;
 //   * block substitutions with these factors (persistent kernel); the block
 //     rows of U are stored pre-multiplied by the diagonal inverses (U' =
 //     A_kk^{-1} A12, computed beside the panel), so that the backward sweep
@@ -27,12 +27,6 @@
 #include "common.cuh"
 
 namespace bem {
-
-int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
-                      int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
-                      int n, int batch, int* err, cudaStream_t stream, int store = 0, const float* Aop1 = nullptr,
-                      const float* Bop1 = nullptr, int run = 0, long long wait_limit = 0,
-                      const int* limit_host = nullptr);
 
 namespace {
 
@@ -297,17 +291,16 @@ __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* _
     }
 }
 
-// Operand packing of step kk of the block LU (A_kk^{-1} comes packed from the
-// Gauss-Jordan kernel).  Blocks [0, nrest): the block row to the right of the
-// diagonal, 64 columns each, packed as the B operand (U12 = A12).  Blocks
-// [nrest, nrest + nrows/32): 32 rows of the block column [col0, col0 + 128)
-// from row row0 on, packed K-major: into A3 as the split-TF32 operand of the
-// panel product (A21), or into Aop as [Re(128) | Im(128)] (L21, the A operand
-// of the trailing update).
-// Aop: [batch][npad][2*kB]; Bop: [batch][2*npad][2*kB].
+// Operand packing of the first block step of the block LU (later steps get
+// their operands from the epilogues of the updates that finish them; A_kk^{-1}
+// comes packed from the Gauss-Jordan kernel).  Blocks [0, nrest): the block
+// row to the right of the diagonal, 64 columns each, packed as the B operand
+// (U12 = A12).  Blocks [nrest, nrest + nrows/32): 32 rows of the block column
+// [col0, col0 + 128) from row row0 on, packed K-major into A3 as the
+// split-TF32 operand of the panel product (A21).
+// Bop: [batch][2*npad][2*kB]; A3: [batch][npad][kSplitK].
 __global__ void __launch_bounds__(256) clu_pack_kernel(Planes W, int npad, int kk, int nrest, int row0, int col0,
-                                                       float* __restrict__ Aop, float* __restrict__ Bop,
-                                                       float* __restrict__ A3) {
+                                                       float* __restrict__ Bop, float* __restrict__ A3) {
   __shared__ float tre[kB][33], tim[kB][33];  // [column][row] of a 32 x 128 tile
   const int b = blockIdx.y, tid = threadIdx.x;
   const size_t kp = 2 * kB;
@@ -341,11 +334,6 @@ __global__ void __launch_bounds__(256) clu_pack_kernel(Planes W, int npad, int k
   }
   __syncthreads();
   const int c = tid & (kB - 1);
-  if (!A3) {
-    float* dst = Aop + (size_t)b * npad * kp + (size_t)r0 * kp;
-    for (int i = 0; i < 32; ++i) dst[(size_t)i * kp + tid] = (tid < kB) ? tre[c][i] : tim[c][i];
-    return;
-  }
   // split rows [hi | lo | hi], each [Re(128) | Im(128)], for the panel product
   float* dst = A3 + (size_t)b * npad * kSplitK + (size_t)r0 * kSplitK;
   for (int i = 0; i < 32; ++i) {
@@ -624,7 +612,7 @@ struct MixedWork {
   float2* inv;
   float* binv;  // batch x 256 x kSplitK: packed A_kk^{-1} of the current block
   float* a3;    // batch x npad x kSplitK: split A21 of the current block
-  float* ainv;  // batch x 128 x 256: A_kk^{-1} of the current block as the A operand [Re | Im]
+  float* ainv;  // 2 x batch x 128 x 256: A_kk^{-1} of the last two blocks as the A operand [Re | Im]
   int* flags;
 };
 MixedWork carve(void* work, int npad, int batch) {
@@ -644,7 +632,7 @@ MixedWork carve(void* work, int npad, int batch) {
   w.a3 = (float*)p;
   p += (size_t)batch * npad * kSplitK * sizeof(float);
   w.ainv = (float*)p;
-  p += (size_t)batch * kB * 2 * kB * sizeof(float);
+  p += 2 * (size_t)batch * kB * 2 * kB * sizeof(float);
   w.flags = (int*)p;
   return w;
 }
@@ -652,16 +640,21 @@ Planes planes_of(const MixedWork& w, int npad) {
   return Planes{w.W, w.W + (size_t)npad * npad, npad, 2 * (int64_t)npad * npad};
 }
 
-// Side stream (highest priority) and the two events of the lookahead in the
-// block LU, one set per (device, caller stream): factorisations enqueued on
-// different streams (concurrent requests of a server) overlap on the device
-// without sharing a side stream.  The mutex is held while a factorisation is
-// enqueued, so the events are never re-recorded by another caller in between.
+// Streams (highest priority) and events of the lookahead in the block LU, one
+// set per (device, caller stream): factorisations enqueued on different streams
+// (concurrent requests of a server) overlap on the device without sharing a
+// side stream.  `side` runs the chain of the next block (inverse, panel),
+// `upper` the block rows of U' that only the solves need.  The mutex is held
+// while a factorisation is enqueued, so the events are never re-recorded by
+// another caller in between.
 struct Lookahead {
   std::mutex mu;
   cudaStream_t side = nullptr;
+  cudaStream_t upper = nullptr;
+  cudaEvent_t diag = nullptr;
   cudaEvent_t strips = nullptr;
   cudaEvent_t panel = nullptr;
+  cudaEvent_t upper_done[2] = {nullptr, nullptr};
 };
 std::mutex g_lookahead_mu;
 std::map<std::pair<int, cudaStream_t>, std::unique_ptr<Lookahead>> g_lookahead;
@@ -675,8 +668,11 @@ int lookahead_for(cudaStream_t caller, Lookahead** out) {
     int least = 0, greatest = 0;
     BEM_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     BEM_CUDA_CHECK(cudaStreamCreateWithPriority(&fresh->side, cudaStreamNonBlocking, greatest));
+    BEM_CUDA_CHECK(cudaStreamCreateWithPriority(&fresh->upper, cudaStreamNonBlocking, greatest));
+    BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->diag, cudaEventDisableTiming));
     BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->strips, cudaEventDisableTiming));
     BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->panel, cudaEventDisableTiming));
+    for (auto& e : fresh->upper_done) BEM_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     la = std::move(fresh);
   }
   *out = la.get();
@@ -694,7 +690,7 @@ extern "C" int64_t bem_clu_workspace_bytes(int npad, int batch) {
   return (int64_t)batch * 2 * npad * (int64_t)npad * 4 + kOpBuffers * (int64_t)batch * npad * 2 * kB * 4 +
          kOpBuffers * (int64_t)batch * 2 * npad * 2 * kB * 4 + (int64_t)batch * nblk * kB * kB * 8 +
          (int64_t)batch * (2 * kB) * kSplitK * 4 + (int64_t)batch * npad * kSplitK * 4 +
-         (int64_t)batch * kB * 2 * kB * 4 +
+         2 * (int64_t)batch * kB * 2 * kB * 4 +
          ((int64_t)batch * nblk + 2 + batch) * 4 + 1024;
 }
 
@@ -745,80 +741,113 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   const size_t abuf = (size_t)batch * npad * 2 * kB, bbuf = (size_t)batch * 2 * npad * 2 * kB;
   // The big trailing updates give each CTA runs of up to 32 tiles (the
   // accumulator double buffer pays over a run; the runs end at staggered
-  // times, so an SM frees up every few microseconds); the side stream's panel
-  // products, whose latency is the lookahead chain, one tile per CTA.  The
-  // side stream's kernels take SMs as they free up.
+  // times, so an SM frees up every few microseconds); the lookahead chain's
+  // products, whose latency is the chain, one tile per CTA.  The side
+  // streams' kernels take SMs as they free up.
   constexpr int kBigRun = 0, kSideRun = 1;
   float* Aop[kOpBuffers] = {w.Aop, w.Aop + abuf, w.Aop + 2 * abuf};
   float* Bop[kOpBuffers] = {w.Bop, w.Bop + bbuf, w.Bop + 2 * bbuf};
-  // Inverse of the diagonal block, then the panel: A12 and A21 packed, L21 =
-  // A21 A_kk^{-1} on the tensor cores into the working matrix, L21 packed.
-  auto diag_and_panel = [&](int kk, int buf, cudaStream_t on) -> int {
-    {
-      TimedLaunch tl(kKCluGj, on);
-      clu_gj_kernel<<<batch, 512, 0, on>>>(W, kk, info_dev, w.inv, nblk, w.binv, w.ainv);
-    }
+  const size_t ainv_buf = (size_t)batch * kB * 2 * kB;
+  const int64_t a_stride = (int64_t)npad * 2 * kB, b_stride = 2 * (int64_t)npad * 2 * kB,
+                a3_stride = (int64_t)npad * kSplitK;
+  // Inverse of diagonal block kk (its A operand copy in ainv buffer of the
+  // block's parity).
+  auto inverse = [&](int kk, cudaStream_t on) {
+    TimedLaunch tl(kKCluGj, on);
+    clu_gj_kernel<<<batch, 512, 0, on>>>(W, kk, info_dev, w.inv, nblk, w.binv,
+                                         w.ainv + ((kk / kB) & 1) * ainv_buf);
     ++launches;
+  };
+  // L21 = A21 A_kk^{-1} (split TF32: A_hi B_hi + A_lo B_hi + A_hi B_lo,
+  // float32-level multipliers) into the working matrix and, packed, into the
+  // A operand buffer of the block.
+  auto panel = [&](int kk, int buf, cudaStream_t on) -> int {
     const int m = npad - kk - kB;
     if (m <= 0) return BEM_OK;
-    const int nrest = m / kPT;
-    {
-      TimedLaunch tl(kKCluPanel, on);
-      clu_pack_kernel<<<dim3(nrest + m / 32, batch), 256, 0, on>>>(W, npad, kk, nrest, kk + kB, kk, Aop[buf],
-                                                                    Bop[buf], w.a3);
-      // split TF32: A_hi B_hi + A_lo B_hi + A_hi B_lo, float32-level multipliers
-      int st2 = cgemm_tf32_update(w.a3, npad, kk + kB, w.binv, 2 * kB, 0, kSplitK, W.re, W.im, npad, W.stride,
-                                  kk + kB, kk, m, kB, batch, err_dev, on, 1, nullptr, nullptr, kSideRun, 0, act);
-      if (st2) return st2;
-      clu_pack_kernel<<<dim3(m / 32, batch), 256, 0, on>>>(W, npad, kk, 0, kk + kB, kk, Aop[buf], Bop[buf],
-                                                           nullptr);
-      // block row of U scaled by the diagonal inverse, U' = A_kk^{-1} A12 (TF32),
-      // for the backward substitution only (A12 itself is packed in Bop already)
-      st2 = cgemm_tf32_update(w.ainv, kB, 0, Bop[buf], 2 * (int64_t)npad, 2 * (kk + kB), 2 * kB, W.re, W.im, npad,
-                              W.stride, kk, kk + kB, kB, m, batch, err_dev, on, 1, nullptr, nullptr, kSideRun, 0,
-                              act);
-      if (st2) return st2;
-    }
-    launches += 3;
-    return BEM_OK;
+    TimedLaunch tl(kKCluPanel, on);
+    return cgemm_tf32_update(w.a3, npad, kk + kB, w.binv, 2 * kB, 0, kSplitK, W.re, W.im, npad, W.stride, kk + kB,
+                             kk, m, kB, batch, err_dev, on, 1, nullptr, nullptr, kSideRun, 0, act, Aop[buf],
+                             kPackRows, a_stride);
+  };
+  // Block row of U scaled by the diagonal inverse, U' = A_kk^{-1} A12 (TF32),
+  // for the backward substitution only (A12 itself is packed in Bop).
+  auto upper = [&](int kk, int buf, cudaStream_t on) -> int {
+    const int m = npad - kk - kB;
+    if (m <= 0) return BEM_OK;
+    TimedLaunch tl(kKCluPanel, on);
+    return cgemm_tf32_update(w.ainv + ((kk / kB) & 1) * ainv_buf, kB, 0, Bop[buf], 2 * (int64_t)npad,
+                             2 * (kk + kB), 2 * kB, W.re, W.im, npad, W.stride, kk, kk + kB, kB, m, batch, err_dev,
+                             on, 1, nullptr, nullptr, kSideRun, 0, act);
   };
   // C rows r0.. (m), complex columns c0.. (nc) -= L21 U12 of the block step whose
   // packed operands are in buffer buf, and of a second step (buffer buf2 >= 0)
-  // in the same pass over C (depth 256).
-  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2, int run) -> int {
+  // in the same pass over C (depth 256); optionally a packed copy of the result.
+  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2, int run, float* pack = nullptr,
+                    int pack_mode = kPackNone, int64_t pack_stride = 0) -> int {
     if (m <= 0 || nc <= 0) return BEM_OK;
     return cgemm_tf32_update(Aop[buf], npad, r0, Bop[buf], 2 * (int64_t)npad, 2 * c0, 2 * kB, W.re, W.im, npad,
                              W.stride, r0, c0, m, nc, batch, err_dev, s, 0, buf2 >= 0 ? Aop[buf2] : nullptr,
-                             buf2 >= 0 ? Bop[buf2] : nullptr, run, 0, act);
+                             buf2 >= 0 ? Bop[buf2] : nullptr, run, 0, act, pack, pack_mode, pack_stride);
   };
   Lookahead* la = nullptr;
   if ((st = lookahead_for(s, &la))) return st;
   std::lock_guard<std::mutex> lock(la->mu);
   // Right-looking block LU with a lookahead of one block, the trailing updates
   // of two consecutive block steps applied in one pass over C (depth 256: the
-  // update is bound by reading and writing C).  Step k: the strips that block
-  // k+1 needs (its block row and block column) get every update still
-  // pending on them, then the inverse and panel of block k+1 run on the side
-  // stream while, at every second step, the rest of the trailing matrix gets
-  // the updates of steps k-1 and k together.  Operands of steps k-1, k, k+1
-  // live in three buffers.
-  if ((st = diag_and_panel(0, 0, s))) return st;
+  // update is bound by reading and writing C).  Step k, on the caller's
+  // stream: the diagonal block k+1 gets every update still pending on it and
+  // its inverse starts on the side stream; then block row and block column
+  // k+1 get theirs, their epilogues packing the operands of step k+1 (A12 as
+  // the B operand, A21 split for the panel product); the panel L21 follows
+  // on the side stream (its epilogue packs the A operand), U' on the third
+  // stream.  Meanwhile, at every second step, the rest of the trailing matrix
+  // gets the updates of steps k-1 and k together.  Operands of steps k-1, k,
+  // k+1 live in three buffers; A_kk^{-1} for U' in two.
+  // Block 0: the operands come straight from the converted matrix.
+  inverse(0, s);
+  if (npad > kB) {
+    const int m = npad - kB;
+    TimedLaunch tl(kKCluPanel, s);
+    clu_pack_kernel<<<dim3(m / kPT + m / 32, batch), 256, 0, s>>>(W, npad, 0, m / kPT, kB, 0, Bop[0], w.a3);
+    ++launches;
+  }
+  if ((st = panel(0, 0, s))) return st;
+  BEM_CUDA_CHECK(cudaEventRecord(la->panel, s));
+  BEM_CUDA_CHECK(cudaStreamWaitEvent(la->upper, la->panel, 0));
+  if ((st = upper(0, 0, la->upper))) return st;
+  BEM_CUDA_CHECK(cudaEventRecord(la->upper_done[0], la->upper));
   for (int kk = 0, step = 0; kk + kB < npad; kk += kB, ++step) {
     const int cur = step % kOpBuffers, prev = (step + kOpBuffers - 1) % kOpBuffers;
     const int nxt = (step + 1) % kOpBuffers;
     const int kn = kk + kB, rest = npad - kn - kB;
     const int pend = (step & 1) ? prev : -1;  // step k-1 still pending beyond block k
-    if ((st = update(cur, kn, kn, kB, npad - kn, pend, 0))) return st;  // block row kn
-    if ((st = update(cur, kn + kB, kn, rest, kB, pend, 0))) return st;  // block column kn below the diagonal
+    // U' of block k-1 (third stream) has read the A_kk^{-1} copy that the
+    // inverse of block k+1 overwrites (and, before it, U' of block k-2 the
+    // operand buffer that the strips below overwrite)
+    BEM_CUDA_CHECK(cudaStreamWaitEvent(s, la->upper_done[(step + 1) & 1], 0));
+    if ((st = update(cur, kn, kn, kB, kB, pend, kSideRun))) return st;  // diagonal block kn
+    BEM_CUDA_CHECK(cudaEventRecord(la->diag, s));
+    BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->diag, 0));
+    inverse(kn, la->side);
+    // block row kn (packed as the B operand) and block column kn below the
+    // diagonal (packed split for the panel product)
+    if ((st = update(cur, kn, kn + kB, kB, rest, pend, 0, Bop[nxt], kPackCols, b_stride))) return st;
+    if ((st = update(cur, kn + kB, kn, rest, kB, pend, 0, w.a3, kPackRowsSplit, a3_stride))) return st;
     BEM_CUDA_CHECK(cudaEventRecord(la->strips, s));
     BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->strips, 0));
-    if ((st = diag_and_panel(kn, nxt, la->side))) return st;
+    if ((st = panel(kn, nxt, la->side))) return st;
     BEM_CUDA_CHECK(cudaEventRecord(la->panel, la->side));
+    BEM_CUDA_CHECK(cudaStreamWaitEvent(la->upper, la->panel, 0));
+    if ((st = upper(kn, nxt, la->upper))) return st;
+    BEM_CUDA_CHECK(cudaEventRecord(la->upper_done[(step + 1) & 1], la->upper));
     if ((step & 1) && rest > 0) {
       if ((st = update(cur, kn + kB, kn + kB, rest, rest, prev, kBigRun))) return st;
     }
     BEM_CUDA_CHECK(cudaStreamWaitEvent(s, la->panel, 0));
   }
+  // the last block rows of U' are part of the factors
+  BEM_CUDA_CHECK(cudaEventRecord(la->upper_done[0], la->upper));
+  BEM_CUDA_CHECK(cudaStreamWaitEvent(s, la->upper_done[0], 0));
   count_launches(launches);
   BEM_CUDA_CHECK(cudaGetLastError());
   return BEM_OK;

@@ -39,8 +39,8 @@ constexpr int kStages = 4;
 constexpr int kABytes = kTM * kKC * 4;   // 16 KiB
 constexpr int kBBytes = kTN * kKC * 4;   // 32 KiB
 constexpr int kStageBytes = kABytes + kBBytes;
-constexpr long long kWaitLimit = 1ll << 22;
-constexpr int kMaxGroup = 64;  // matrices of one grouped launch  // default polls of a bounded mbarrier wait (~ a second)
+constexpr long long kWaitLimit = 1ll << 22;  // default polls of a bounded mbarrier wait (~ a second)
+constexpr int kMaxGroup = 64;  // matrices of one grouped launch
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -154,6 +154,11 @@ struct UpdateArgs {
   // tiles gstart[b] .. gstart[b+1]-1 (matrices of different active sizes)
   int ngroup;
   int batch0;  // matrix index of local matrix 0 (operand batch coordinate, C offset)
+  // Packed copy of the result for the next block step's products (kPack*):
+  // the operand layouts the LU's update reads, written by the epilogue
+  float* pack;
+  int64_t pack_stride;  // floats between matrices
+  int pack_mode;
   int gstart[kMaxGroup + 1];
   short gtm[kMaxGroup];
   short gtn[kMaxGroup];
@@ -191,6 +196,48 @@ __device__ __forceinline__ bool mbar_wait_n(uint64_t* bar, uint32_t parity, int*
     }
   }
   return true;
+}
+
+// Packed copy of 16 result values of one thread: columns t0 .. t0 + 15 of the
+// tile in plane `plane` (0 real, 1 imaginary); off = t0 - cbase, the offset
+// from the thread's pack pointer in the row layouts.
+__device__ __forceinline__ void pack_chunk(int mode, float* pk, int plane, int t0, int off, const float (&v)[16]) {
+  if (mode == kPackRows) {
+    float4* d = reinterpret_cast<float4*>(pk + off);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) d[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+  } else if (mode == kPackRowsSplit) {
+    float4* hi0 = reinterpret_cast<float4*>(pk + off);
+    float4* lo = reinterpret_cast<float4*>(pk + kTN + off);
+    float4* hi1 = reinterpret_cast<float4*>(pk + 2 * kTN + off);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float h[4], l[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        h[e] = __uint_as_float(__float_as_uint(v[4 * j + e]) & 0xffffe000u);  // the TF32 part
+        l[e] = v[4 * j + e] - h[e];                                           // exact remainder
+      }
+      hi0[j] = make_float4(h[0], h[1], h[2], h[3]);
+      lo[j] = make_float4(l[0], l[1], l[2], l[3]);
+      hi1[j] = make_float4(h[0], h[1], h[2], h[3]);
+    }
+  } else {
+    // B operand rows of complex columns t: Re to (t, k) and (128 + t, 128 + k);
+    // Im to (t, 128 + k) negated and (128 + t, k); k is the lane's row
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      float* r0 = pk + (size_t)(t0 + j) * kTN;
+      float* r1 = pk + (size_t)(kTNc + t0 + j) * kTN;
+      if (plane == 0) {
+        r0[0] = v[j];
+        r1[kTNc] = v[j];
+      } else {
+        r0[kTNc] = -v[j];
+        r1[0] = v[j];
+      }
+    }
+  }
 }
 
 // Trailing update with double-buffered accumulators: a CTA (one per SM: 197 KB
@@ -347,6 +394,15 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
       __syncwarp();
       if (!ok) break;
       const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kAccCols + plane * kTNc + cbase);
+      // packed copy: this thread's row of the tile (kPackRows*), or its K'
+      // index within the block row (kPackCols)
+      float* pk = nullptr;
+      if (p.pack_mode == kPackRows || p.pack_mode == kPackRowsSplit) {
+        const int kpk = p.pack_mode == kPackRows ? kTN : 3 * kTN;
+        pk = p.pack + (size_t)b * p.pack_stride + (size_t)row * kpk + plane * kTNc + cbase;
+      } else if (p.pack_mode == kPackCols) {
+        pk = p.pack + (size_t)b * p.pack_stride + (size_t)(2 * (p.c_col0 + tn * kTNc)) * kTN + 32 * q + lane;
+      }
 #pragma unroll
       for (int chunk = 0; chunk < kChunks; chunk += 2) {
         if (rd) {
@@ -357,7 +413,11 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
           float v[kCW];
           tmem_ld16(tbase + (uint32_t)(chunk * kCW), v);
 #pragma unroll
-          for (int j = 0; j < kCW; ++j) __stcs(C + (size_t)(chunk * kCW + j) * ldc, rd ? cb0[j] - v[j] : v[j]);
+          for (int j = 0; j < kCW; ++j) {
+            v[j] = rd ? cb0[j] - v[j] : v[j];
+            __stcs(C + (size_t)(chunk * kCW + j) * ldc, v[j]);
+          }
+          if (pk) pack_chunk(p.pack_mode, pk, plane, cbase + chunk * kCW, chunk * kCW, v);
         }
         if (rd && chunk + 2 < kChunks) {
 #pragma unroll
@@ -367,8 +427,11 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
           float v[kCW];
           tmem_ld16(tbase + (uint32_t)((chunk + 1) * kCW), v);
 #pragma unroll
-          for (int j = 0; j < kCW; ++j)
-            __stcs(C + (size_t)((chunk + 1) * kCW + j) * ldc, rd ? cb1[j] - v[j] : v[j]);
+          for (int j = 0; j < kCW; ++j) {
+            v[j] = rd ? cb1[j] - v[j] : v[j];
+            __stcs(C + (size_t)((chunk + 1) * kCW + j) * ldc, v[j]);
+          }
+          if (pk) pack_chunk(p.pack_mode, pk, plane, cbase + (chunk + 1) * kCW, (chunk + 1) * kCW, v);
         }
       }
       // this warp's reads of the accumulator are complete: release it
@@ -434,8 +497,14 @@ int num_sms(int* out) {
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store, const float* Aop1,
-                      const float* Bop1, int run, long long wait_limit, const int* limit_host) {
+                      const float* Bop1, int run, long long wait_limit, const int* limit_host, float* pack,
+                      int pack_mode, int64_t pack_stride) {
   if (m <= 0 || n <= 0) return BEM_OK;
+  if (pack_mode != kPackNone &&
+      (!pack || (pack_mode == kPackCols ? m != kTM : n != kTNc) || (reinterpret_cast<uintptr_t>(pack) & 15) ||
+       pack_mode < kPackNone || pack_mode > kPackCols))
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: packed copy needs one tile row (columns) or "
+                                               "one tile column (rows) and a 16-byte aligned destination");
   if (m % kTM || n % kTNc || kp % kKC || (a_row0 % 8) || (b_row0 % 8))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: sizes must be multiples of 128 (K' of 32)");
   if ((Aop1 == nullptr) != (Bop1 == nullptr))
@@ -475,6 +544,9 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
   p.tiles_m = tiles_m;
   p.tiles_n = tiles_n;
   p.wait_limit = wait_limit > 0 ? wait_limit : kWaitLimit;
+  p.pack = pack;
+  p.pack_stride = pack_stride;
+  p.pack_mode = pack_mode;
   int launches = 0;
   // Grouped: matrix b covers only rows and columns below limit_host[b] (its
   // active size), launches of at most kMaxGroup matrices

@@ -454,14 +454,16 @@ class B200Engine:
             if hit is not None and hit[0]() is body:
                 hit[1].acquire()
                 return hit[1].tensors
-            dev = self.device
-            arrays = (torch.as_tensor(body.dof_normal_components(), dtype=torch.float64, device=dev).contiguous(),
-                      torch.as_tensor(body.pressure_weights(), dtype=torch.float64, device=dev).contiguous(),
-                      torch.as_tensor(body.hull_mask.astype(np.int32), device=dev))
+        # host arrays and uploads outside the lock (other threads' bodies go on)
+        dev = self.device
+        arrays = (_lib.upload(body.dof_normal_components(), torch.float64, dev),
+                  _lib.upload(body.pressure_weights(), torch.float64, dev),
+                  _lib.upload(body.hull_mask.astype(np.int32), torch.int32, dev))
+        with self._lock:
             self._body_cache[key] = (weakref.ref(body), _lib.StreamShared(*arrays))
             while len(self._body_cache) > 32:
                 self._body_cache.popitem(last=False)
-            return arrays
+        return arrays
 
     def solve_frequencies(self, body, omegas: Sequence[float], *, wave_directions: Sequence[float] = (0.0,),
                           rho: float = 1000.0, g: float = 9.81, water_depth: float = np.inf,
@@ -703,7 +705,7 @@ class B200Engine:
         nhead = len(heads)
         nrhs = r.nrhs
         ld = npad * nrhs  # batch stride of B, X, R
-        small = torch.as_tensor(np.concatenate([om, ks, heads]), dtype=torch.float64, device=dev)
+        small = _lib.upload(np.concatenate([om, ks, heads]), torch.float64, dev)
         om_t, k_t, heads_t = small[:nb], small[nb:2 * nb], small[2 * nb:]
         r.B.zero_()
         if sym is not None:  # right-hand sides of the whole mesh first

@@ -54,18 +54,19 @@ class DeviceMesh:
     def __init__(self, mesh, device):
         import torch
         qp, qw = mesh.quadrature_points
-        f64 = dict(dtype=torch.float64, device=device)
+        f64 = torch.float64
+        up = _lib.upload  # no wait for the stream's earlier work
         self.nb_faces = mesh.nb_faces
         self.nb_vertices = mesh.nb_vertices
-        self.vertices = torch.as_tensor(np.ascontiguousarray(mesh.vertices), **f64)
-        self.faces = torch.as_tensor(np.ascontiguousarray(mesh.faces, dtype=np.int32), device=device)
-        self.centers = torch.as_tensor(np.ascontiguousarray(mesh.faces_centers), **f64)
-        self.normals = torch.as_tensor(np.ascontiguousarray(mesh.faces_normals), **f64)
-        self.areas = torch.as_tensor(np.ascontiguousarray(mesh.faces_areas), **f64)
-        self.radii = torch.as_tensor(np.ascontiguousarray(mesh.faces_radiuses), **f64)
+        self.vertices = up(mesh.vertices, f64, device)
+        self.faces = up(np.asarray(mesh.faces, dtype=np.int32), torch.int32, device)
+        self.centers = up(mesh.faces_centers, f64, device)
+        self.normals = up(mesh.faces_normals, f64, device)
+        self.areas = up(mesh.faces_areas, f64, device)
+        self.radii = up(mesh.faces_radiuses, f64, device)
         self.nb_quad_points = qp.shape[1]
-        self.quad_points = torch.as_tensor(np.ascontiguousarray(qp), **f64)
-        self.quad_weights = torch.as_tensor(np.ascontiguousarray(qw), **f64)
+        self.quad_points = up(qp, f64, device)
+        self.quad_weights = up(qw, f64, device)
         self.centers_z = np.asarray(mesh.faces_centers[:, 2])
         # one quadrature point per face, at the face centre (collocation point)
         self.collocation_at_quadrature = bool(qp.shape[1] == 1 and np.array_equal(qp[:, 0, :], mesh.faces_centers))
@@ -300,8 +301,17 @@ class Delhommeau:
         key = mesh.content_hash
         with self._lock:
             dm = self._mesh_cache.get(key)
-            if dm is None:
-                dm = DeviceMesh(mesh, self.device)
+            if dm is not None:
+                self._mesh_cache.move_to_end(key)
+                dm.shared.acquire()
+                return dm
+        # built outside the lock (host geometry and uploads on this thread's
+        # stream), so that threads with cached meshes do not wait for it
+        fresh = DeviceMesh(mesh, self.device)
+        with self._lock:
+            dm = self._mesh_cache.get(key)
+            if dm is None:  # another thread may have built the same mesh meanwhile
+                dm = fresh
                 self._mesh_cache[key] = dm
                 while len(self._mesh_cache) > 8:
                     self._mesh_cache.popitem(last=False)
