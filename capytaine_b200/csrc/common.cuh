@@ -88,15 +88,10 @@ int zlu_solve_enqueue(const void* A_dev, int n, int64_t lda, int64_t stride, int
                       cudaStream_t s, const int* skip, long long spin_limit, const int* mskip = nullptr);
 int* zlu_done_flag(void* work_dev, int n, int batch);
 
-// Packed copies of a complex update's result (tc_gemm.cu), written by its
-// epilogue in the operand layouts of the next block step of the mixed LU:
-//   kPackRows:      row i -> [Re C(i, 0..127) | Im C(i, 0..127)]           (n = 128)
-//   kPackRowsSplit: row i -> [hi | lo | hi] of that row, hi the TF32 part  (n = 128)
-//   kPackCols:      complex column j0 + t (j0 the tile's first column) ->
-//                   rows 2 j0 + t: [Re C(:, j) | -Im C(:, j)] and
-//                   2 j0 + 128 + t: [Im C(:, j) | Re C(:, j)] over the
-//                   128 rows of C                                          (m = 128)
-enum PackMode { kPackNone = 0, kPackRows = 1, kPackRowsSplit = 2, kPackCols = 3 };
+// Packed copy of a complex update's result (tc_gemm.cu), written by its
+// epilogue in the A operand layout of the next block step of the mixed LU:
+//   kPackRows: row i -> [Re C(i, 0..127) | Im C(i, 0..127)]  (n = 128)
+enum PackMode { kPackNone = 0, kPackRows = 1 };
 
 // C (m x n complex in two float32 planes) -= A' B' (store = 0) or = A' B'
 // (store = 1) on the tensor cores from packed operands; an optional second

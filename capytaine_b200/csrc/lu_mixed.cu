@@ -10,8 +10,9 @@
 //     with partial pivoting among its rows, held in registers; the panel is the
 //     product A21 A_kk^{-1}; the trailing update C -= L21 U12 runs on the
 //     tcgen05 tensor cores (TF32 inputs, FP32 accumulation; tc_gemm.cu) from
-//     operands that the epilogues of the updates finishing them write packed.
-//     No row permutation leaves the diagonal blocks, so the solves need none;
+//     packed operands (A12 and A21 by a pack kernel, L21 by the epilogue of
+//     the panel product).  No row permutation leaves the diagonal blocks, so
+//     the solves need none;
 //   * block substitutions with these factors (persistent kernel); the block
 //     rows of U are stored pre-multiplied by the diagonal inverses (U' =
 //     A_kk^{-1} A12, computed beside the panel), so that the backward sweep
@@ -84,20 +85,55 @@ __global__ void convert_pad_kernel(const double2* __restrict__ K, int64_t ldk, i
   }
 }
 
-// Pivot of column j (register slot M of warp j % 16), among rows j..127:
-// publishes the column with rows j and the pivot exchanged (entry j is then
-// the pivot) to colbuf[j & 1] and the pivot row to s_piv[j & 1]; flags an
-// exactly zero pivot in info.
+// Gauss-Jordan inverse of a diagonal block: 8 warps, thread (warp w, lane l)
+// owns rows l + 32 a (a < 4) and columns w + 8 m (m < 16) of the 128 x 128
+// block in registers; column j = 8 JM + jw is slot JM of warp jw.
+// Pivoting is implicit: rows never move.  Step j picks the pivot of column j
+// among the rows not yet used as pivot rows (row p_j) and eliminates column j
+// from every other row with the unnormalised row p_j:
+//   a_r -= (a_rj / a_pj) a_p   (r != p_j),
+// the in-place inverse's column j ending as -a_rj / a_pj, with 1 in row p_j.
+// Row p_j thus stays scaled by its pivot; at the end
+//   A^{-1}(j', p_c) = a(p_j', c) / pivot_j'
+// (row p_j' holds the j'-th pivot row, the slot of column c the inverse's
+// column p_c).
+constexpr int kGjWarps = 8;
+constexpr int kGjSlots = kB / kGjWarps;  // columns per warp
+
+// acc - a b in two fused multiply-adds per component.
+__device__ __forceinline__ float2 cfms(float2 acc, float2 a, float2 b) {
+  acc.x = fmaf(-a.x, b.x, acc.x);
+  acc.x = fmaf(a.y, b.y, acc.x);
+  acc.y = fmaf(-a.x, b.y, acc.y);
+  acc.y = fmaf(-a.y, b.x, acc.y);
+  return acc;
+}
+
+struct GjShared {
+  float2 colbuf[2][kB];             // pivot column of the step, by row (double buffered)
+  float2 xbuf[kGjWarps][kGjSlots];  // per warp: its entries of the pivot row
+  float2 rowscale[kB];              // 1 / pivot of the step whose pivot row is this row
+  int piv_row[kB];                  // pivot row of each step
+  int jinv[kB];                     // step of each pivot row
+  unsigned used[kB / 32];           // rows already used as pivot rows
+  int s_piv[2];
+};
+
+// Pivot of column j (register slot M of this warp) among the unused rows:
+// publishes the column to colbuf[j & 1] and the pivot row to s_piv[j & 1],
+// marks the row used, then sets the column in registers to the unit vector of
+// the pivot row (the step's update turns it into the inverse's column); flags
+// an exactly zero pivot in info.
 template <int M>
-__device__ __forceinline__ void gj_pivot(const float2 (&a)[4][8], int j, int kk, int b, int lane,
-                                         float2 (*colbuf)[kB], int* s_piv, int* __restrict__ info) {
+__device__ __forceinline__ void gj_pivot(float2 (&a)[4][kGjSlots], int j, int kk, int b, int lane, GjShared& sh,
+                                         int* __restrict__ info) {
   float best = -1.0f;
-  int bi = j;
+  int bi = kB;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int r = lane + 32 * i;
     const float av = fabs1(a[i][M]);
-    if (r >= j && (av > best || (av == best && r < bi))) {
+    if (!((sh.used[i] >> lane) & 1u) && (av > best || (av == best && r < bi))) {
       best = av;
       bi = r;
     }
@@ -111,140 +147,114 @@ __device__ __forceinline__ void gj_pivot(const float2 (&a)[4][8], int j, int kk,
       bi = oi;
     }
   }
+  if (bi >= kB) {  // no comparable candidate (NaN): the first unused row
+#pragma unroll
+    for (int i = 3; i >= 0; --i)
+      if (~sh.used[i]) bi = 32 * i + __ffs(~sh.used[i]) - 1;
+  }
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int r = lane + 32 * i;
-    const int dst = (r == j) ? bi : ((r == bi) ? j : r);
-    colbuf[j & 1][dst] = a[i][M];
+    sh.colbuf[j & 1][r] = a[i][M];
+    a[i][M] = make_float2(r == bi ? 1.0f : 0.0f, 0.0f);
   }
   if (lane == 0) {
-    s_piv[j & 1] = bi;
+    sh.s_piv[j & 1] = bi;
+    sh.piv_row[j] = bi;
+    sh.used[bi >> 5] |= 1u << (bi & 31);
     if (!(best > 0.0f) && info[b] == 0) info[b] = kk + j + 1;
   }
 }
 
-// Update of register slot M of this thread's entries for column step j: row j
-// becomes the normalised pivot row u, the pivot column (slot JM of warp jw)
-// -f / pivot, every other entry a - f u.
-// (The rank-one update runs on every entry without conditions; the two
-// special cases are overwritten after it.)
-template <int M, int SJ>
-__device__ __forceinline__ void gj_update(float2 (&a)[4][8], const float2 (&f)[4], const float2 (&u)[8],
-                                          bool own_row_j, bool pivot_col, float2 mdinv) {
+// Rank-one update of register slot M: a - f u (u the pivot row, read from the
+// warp's buffer).
+template <int M>
+__device__ __forceinline__ void gj_update(float2 (&a)[4][kGjSlots], const float2 (&f)[4], const float2* u) {
+  const float2 um = u[M];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) a[i][M] = ffms(a[i][M], f[i], u[M]);
-  if (pivot_col) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) a[i][M] = fmul(f[i], mdinv);
-  }
-  if (own_row_j) a[SJ][M] = u[M];
+  for (int i = 0; i < 4; ++i) a[i][M] = cfms(a[i][M], f[i], um);
 }
 
-// One Gauss-Jordan column step, column j = 16 JM + jw (slot JM of warp jw,
-// known at compile time).  Thread (warp w, lane l) owns rows l + 32 a (a < 4)
-// and columns w + 16 m (m < 8).  Only the pivot column crosses warps (shared
-// memory, double buffered, one barrier per column); the rows j and p of a
-// warp's own columns are exchanged through a per-warp buffer.  The owner of
-// column j + 1 updates that column first and searches its pivot while the
-// other warps are still updating, so the search is off the critical path.
+// One Gauss-Jordan column step, column j = 8 JM + jw (slot JM of warp jw,
+// known at compile time).  Only the pivot column crosses warps (shared memory,
+// double buffered, one barrier per column); the pivot row's entries of a
+// warp's columns go through the warp's buffer.
 template <int JM>
-__device__ __forceinline__ void gj_step(float2 (&a)[4][8], int jw, int kk, int b, int lane, int w, int tid,
-                                        float2 (*colbuf)[kB], float2 (*xbuf)[2][8], int* s_piv, int* perm,
-                                        int* __restrict__ info) {
-  constexpr int SJ = JM >> 1;  // register slot of row j (j >> 5)
-  const int j = 16 * JM + jw;
+__device__ __forceinline__ void gj_step(float2 (&a)[4][kGjSlots], int jw, int kk, int b, int lane, int w, int tid,
+                                        GjShared& sh, int* __restrict__ info) {
+  const int j = kGjWarps * JM + jw;
   const int buf = j & 1;
   __syncthreads();  // column j and its pivot row are published
-  const int p = s_piv[buf];
-  const int lj = j & 31, lp = p & 31, sp = p >> 5;
-  // rows p and j of this warp's columns: lane lp writes row p, lane lj row j
+  const int p = sh.s_piv[buf];
+  const int lp = p & 31, sp = p >> 5;
+  float2* xw = sh.xbuf[w];
   if (lane == lp) {
     switch (sp) {  // one lane: a branch per register slot instead of selects
 #define BEM_GJ_ROWOUT(S) \
   case S:                \
-    _Pragma("unroll") for (int m = 0; m < 8; ++m) xbuf[w][0][m] = a[S][m]; \
+    _Pragma("unroll") for (int m = 0; m < kGjSlots; ++m) xw[m] = a[S][m]; \
     break;
       BEM_GJ_ROWOUT(0) BEM_GJ_ROWOUT(1) BEM_GJ_ROWOUT(2) BEM_GJ_ROWOUT(3)
 #undef BEM_GJ_ROWOUT
     }
   }
-  if (p != j && lane == lj) {
+  const float2 piv = sh.colbuf[buf][p];
+  const float d = piv.x * piv.x + piv.y * piv.y;
+  const float rd = d > 0.0f ? 1.0f / d : 0.0f;
+  const float2 dinv = make_float2(piv.x * rd, -piv.y * rd);
+  if (tid == 0) sh.rowscale[p] = dinv;
+  float2 f[4];  // multipliers a_rj / pivot; 0 on the pivot row, which stays as it is
 #pragma unroll
-    for (int m = 0; m < 8; ++m) xbuf[w][1][m] = a[SJ][m];
+  for (int i = 0; i < 4; ++i) {
+    const float2 c = sh.colbuf[buf][lane + 32 * i];
+    f[i] = (lane + 32 * i == p) ? make_float2(0.0f, 0.0f) : fmul(c, dinv);
   }
   __syncwarp();
-  float2 prow[8];
-#pragma unroll
-  for (int m = 0; m < 8; ++m) prow[m] = xbuf[w][0][m];
-  if (p != j) {
-    if (lane == lp) {  // row p takes the old row j; row j becomes u below
-      switch (sp) {
-#define BEM_GJ_ROWIN(S) \
-  case S:               \
-    _Pragma("unroll") for (int m = 0; m < 8; ++m) a[S][m] = xbuf[w][1][m]; \
-    break;
-        BEM_GJ_ROWIN(0) BEM_GJ_ROWIN(1) BEM_GJ_ROWIN(2) BEM_GJ_ROWIN(3)
-#undef BEM_GJ_ROWIN
-      }
-    }
-    if (tid == 0) {
-      const int t = perm[j];
-      perm[j] = perm[p];
-      perm[p] = t;
-    }
-  }
-  const float2 piv = colbuf[buf][j];
-  const float2 dinv = fabs1(piv) > 0.0f ? fdiv(make_float2(1.0f, 0.0f), piv) : make_float2(0.0f, 0.0f);
-  float2 u[8];
-#pragma unroll
-  for (int m = 0; m < 8; ++m) u[m] = (m == JM && w == jw) ? dinv : fmul(prow[m], dinv);
-  const float2 mdinv = make_float2(-dinv.x, -dinv.y);
-  float2 f[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) f[i] = colbuf[buf][lane + 32 * i];
-  const bool own_row_j = lane == lj;
-  const int w1 = (j + 1) & 15;  // owner of column j + 1
-  // slot JM first (column j + 1 lives there when jw < 15)
-  gj_update<JM, SJ>(a, f, u, own_row_j, w == jw, mdinv);
-  if (jw < 15 && w == w1) gj_pivot<JM>(a, j + 1, kk, b, lane, colbuf, s_piv, info);
-  if constexpr (JM < 7) {
-    gj_update<JM + 1, SJ>(a, f, u, own_row_j, false, mdinv);
-    if (jw == 15 && w == w1) gj_pivot<JM + 1>(a, j + 1, kk, b, lane, colbuf, s_piv, info);
-  }
-  // slots other than JM never hold the pivot column
-#define BEM_GJ_UPD(MM) \
-  if constexpr (MM != JM && MM != JM + 1) gj_update<MM, SJ>(a, f, u, own_row_j, false, mdinv);
+  const float2* u = xw;
+#define BEM_GJ_UPD(MM) gj_update<MM>(a, f, u);
   BEM_GJ_UPD(0) BEM_GJ_UPD(1) BEM_GJ_UPD(2) BEM_GJ_UPD(3) BEM_GJ_UPD(4) BEM_GJ_UPD(5) BEM_GJ_UPD(6)
-  BEM_GJ_UPD(7)
+  BEM_GJ_UPD(7) BEM_GJ_UPD(8) BEM_GJ_UPD(9) BEM_GJ_UPD(10) BEM_GJ_UPD(11) BEM_GJ_UPD(12) BEM_GJ_UPD(13)
+  BEM_GJ_UPD(14) BEM_GJ_UPD(15)
 #undef BEM_GJ_UPD
+  __syncwarp();  // the warp's reads of its buffer are done before the next step rewrites it
+  // the owner of column j + 1 (slot JM, or JM + 1 after the last warp) picks
+  // its pivot; one straight sequence of updates before it keeps the step's
+  // code small
+  if (w == ((j + 1) & (kGjWarps - 1))) {
+    if (jw < kGjWarps - 1)
+      gj_pivot<JM>(a, j + 1, kk, b, lane, sh, info);
+    else if constexpr (JM < kGjSlots - 1)
+      gj_pivot<JM + 1>(a, j + 1, kk, b, lane, sh, info);
+  }
 }
 
 // Inverse of the diagonal block A_kk by Gauss-Jordan elimination with partial
-// pivoting among its rows.  The 128 x 128 block lives in registers: thread
-// (warp w, lane l) owns rows l + 32 a (a < 4) and columns w + 16 m (m < 8).
-// Per column: the owning warp picks the pivot and publishes the column, every
-// warp exchanges the two rows of its own columns, then every thread updates its
-// 32 entries: one barrier per column (gj_step).  Columns are visited slot by slot
-// so that register indices are compile-time constants.  Output: inv (128 x 128,
-// column-major) = A_kk^{-1}; info flags an exactly zero pivot.
-__global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* __restrict__ info,
-                                                        float2* __restrict__ inv, int nblk,
-                                                        float* __restrict__ binv, float* __restrict__ ainv) {
-  __shared__ float2 colbuf[2][kB];
-  __shared__ float2 xbuf[16][2][8];  // per warp: its columns of the pivot row and of row j
-  __shared__ int s_piv[2];
-  __shared__ int perm[kB];
+// pivoting among its rows (implicit, see above), the block in registers: per
+// column the owning warp picks the pivot and publishes the column, every warp
+// takes the pivot row's entries of its own columns and updates its entries;
+// one barrier per column.  Columns are visited slot by slot so that register
+// indices are compile-time constants.  Output: inv (128 x 128, column-major) =
+// A_kk^{-1}, and its packed copies for the panel product (binv) and the block
+// row of U' (ainv); info flags an exactly zero pivot.
+__global__ void __launch_bounds__(32 * kGjWarps, 1) clu_gj_kernel(Planes W, int kk, int* __restrict__ info,
+                                                                 float2* __restrict__ inv, int nblk,
+                                                                 float* __restrict__ binv,
+                                                                 float* __restrict__ ainv) {
+  __shared__ GjShared sh;
   const int b = blockIdx.x, tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
-  float2 a[4][8];
+  float2 a[4][kGjSlots];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int m = 0; m < 8; ++m) a[i][m] = ldp(W, b, kk + lane + 32 * i, kk + w + 16 * m);
-  if (tid < kB) perm[tid] = tid;
-  if (w == 0) gj_pivot<0>(a, 0, kk, b, lane, colbuf, s_piv, info);  // column 0 (warp 0, slot 0)
+    for (int m = 0; m < kGjSlots; ++m) a[i][m] = ldp(W, b, kk + lane + 32 * i, kk + w + kGjWarps * m);
+  if (tid < kB / 32) sh.used[tid] = 0u;
+  __syncthreads();
+  if (w == 0) gj_pivot<0>(a, 0, kk, b, lane, sh, info);  // column 0 (warp 0, slot 0)
+  // the 8 column steps of one slot stay a loop: one copy of the step's code
+  // is reused from the instruction cache
 #define BEM_GJ_SLOT(JM) \
-  for (int jw = 0; jw < 16; ++jw) gj_step<JM>(a, jw, kk, b, lane, w, tid, colbuf, xbuf, s_piv, perm, info);
+  _Pragma("unroll 1") for (int jw = 0; jw < kGjWarps; ++jw) gj_step<JM>(a, jw, kk, b, lane, w, tid, sh, info);
   BEM_GJ_SLOT(0)
   BEM_GJ_SLOT(1)
   BEM_GJ_SLOT(2)
@@ -253,29 +263,41 @@ __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* _
   BEM_GJ_SLOT(5)
   BEM_GJ_SLOT(6)
   BEM_GJ_SLOT(7)
+  BEM_GJ_SLOT(8)
+  BEM_GJ_SLOT(9)
+  BEM_GJ_SLOT(10)
+  BEM_GJ_SLOT(11)
+  BEM_GJ_SLOT(12)
+  BEM_GJ_SLOT(13)
+  BEM_GJ_SLOT(14)
+  BEM_GJ_SLOT(15)
 #undef BEM_GJ_SLOT
   __syncthreads();
-  // inverse of A_kk = (P A_kk)^{-1} P: column c of the result goes to column perm[c]
-  // and packed as the B operand of the split-TF32 product L21 = A21 A_kk^{-1}
-  // (three K-blocks of 256: hi, hi, lo; see clu_pack_kernel for the A side):
+  if (tid < kB) sh.jinv[sh.piv_row[tid]] = tid;
+  __syncthreads();
+  // A_kk^{-1}(jinv[r], piv_row[c]) = a(r, c) / pivot, also packed as the B
+  // operand of the split-TF32 product L21 = A21 A_kk^{-1} (three K-blocks of
+  // 256: hi, hi, lo; see clu_pack_kernel for the A side):
   // row t: [Re X(:, t) | -Im X(:, t)] per block, row 128 + t: [Im X(:, t) | Re X(:, t)]
   float2* out = inv + ((size_t)b * nblk + kk / kB) * kB * kB;
   float* bo = binv + (size_t)b * (2 * kB) * kSplitK;
   float* ao = ainv + (size_t)b * kB * 2 * kB;  // row r: [Re A_kk^{-1}(r, :) | Im A_kk^{-1}(r, :)]
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 4; ++i) {
+    const int r = lane + 32 * i;
+    const int row = sh.jinv[r];
+    const float2 sc = sh.rowscale[r];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      const int r = lane + 32 * i, c = w + 16 * m;
-      const int pc = perm[c];
-      const float2 v = a[i][m];
-      out[r + (size_t)pc * kB] = v;
-      ao[(size_t)r * 2 * kB + pc] = v.x;
-      ao[(size_t)r * 2 * kB + kB + pc] = v.y;
+    for (int m = 0; m < kGjSlots; ++m) {
+      const int col = sh.piv_row[w + kGjWarps * m];
+      const float2 v = fmul(a[i][m], sc);
+      out[row + (size_t)col * kB] = v;
+      ao[(size_t)row * 2 * kB + col] = v.x;
+      ao[(size_t)row * 2 * kB + kB + col] = v.y;
       const float2 hi = make_float2(tf32_hi(v.x), tf32_hi(v.y));
       const float2 lo = make_float2(v.x - hi.x, v.y - hi.y);
-      float* rr = bo + (size_t)pc * kSplitK + r;
-      float* ri = bo + (size_t)(kB + pc) * kSplitK + r;
+      float* rr = bo + (size_t)col * kSplitK + row;
+      float* ri = bo + (size_t)(kB + col) * kSplitK + row;
       rr[0] = hi.x;
       rr[kB] = -hi.y;
       rr[2 * kB] = hi.x;
@@ -289,15 +311,16 @@ __global__ void __launch_bounds__(512, 1) clu_gj_kernel(Planes W, int kk, int* _
       ri[4 * kB] = lo.y;
       ri[5 * kB] = lo.x;
     }
+  }
 }
 
-// Operand packing of the first block step of the block LU (later steps get
-// their operands from the epilogues of the updates that finish them; A_kk^{-1}
-// comes packed from the Gauss-Jordan kernel).  Blocks [0, nrest): the block
-// row to the right of the diagonal, 64 columns each, packed as the B operand
-// (U12 = A12).  Blocks [nrest, nrest + nrows/32): 32 rows of the block column
-// [col0, col0 + 128) from row row0 on, packed K-major into A3 as the
-// split-TF32 operand of the panel product (A21).
+// Operand packing of block step kk of the block LU (A_kk^{-1} comes packed
+// from the Gauss-Jordan kernel, L21 from the epilogue of the panel product).
+// Blocks [0, nrest): the block row to the right of the diagonal, 64 columns
+// each, packed as the B operand (U12 = A12).  Blocks [nrest, nrest +
+// nrows/32): 32 rows of the block column [col0, col0 + 128) from row row0 on,
+// packed K-major into A3 as the split-TF32 operand of the panel product (A21).
+// Both through shared memory, so that reads and writes are coalesced.
 // Bop: [batch][2*npad][2*kB]; A3: [batch][npad][kSplitK].
 __global__ void __launch_bounds__(256) clu_pack_kernel(Planes W, int npad, int kk, int nrest, int row0, int col0,
                                                        float* __restrict__ Bop, float* __restrict__ A3) {
@@ -640,11 +663,12 @@ Planes planes_of(const MixedWork& w, int npad) {
   return Planes{w.W, w.W + (size_t)npad * npad, npad, 2 * (int64_t)npad * npad};
 }
 
-// Streams (highest priority) and events of the lookahead in the block LU, one
-// set per (device, caller stream): factorisations enqueued on different streams
-// (concurrent requests of a server) overlap on the device without sharing a
-// side stream.  `side` runs the chain of the next block (inverse, panel),
-// `upper` the block rows of U' that only the solves need.  The mutex is held
+// Streams and events of the lookahead in the block LU, one set per (device,
+// caller stream): factorisations enqueued on different streams (concurrent
+// requests of a server) overlap on the device without sharing a side stream.
+// `side` (highest priority) runs the chain of the next block (inverse,
+// panel), `upper` (lowest priority) the block rows of U' that only the solves
+// need.  The mutex is held
 // while a factorisation is enqueued, so the events are never re-recorded by
 // another caller in between.
 struct Lookahead {
@@ -668,7 +692,7 @@ int lookahead_for(cudaStream_t caller, Lookahead** out) {
     int least = 0, greatest = 0;
     BEM_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     BEM_CUDA_CHECK(cudaStreamCreateWithPriority(&fresh->side, cudaStreamNonBlocking, greatest));
-    BEM_CUDA_CHECK(cudaStreamCreateWithPriority(&fresh->upper, cudaStreamNonBlocking, greatest));
+    BEM_CUDA_CHECK(cudaStreamCreateWithPriority(&fresh->upper, cudaStreamNonBlocking, least));
     BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->diag, cudaEventDisableTiming));
     BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->strips, cudaEventDisableTiming));
     BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->panel, cudaEventDisableTiming));
@@ -739,22 +763,21 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
                                                                            npad, W);
   ++launches;
   const size_t abuf = (size_t)batch * npad * 2 * kB, bbuf = (size_t)batch * 2 * npad * 2 * kB;
-  // The big trailing updates give each CTA runs of up to 32 tiles (the
-  // accumulator double buffer pays over a run; the runs end at staggered
-  // times, so an SM frees up every few microseconds); the lookahead chain's
-  // products, whose latency is the chain, one tile per CTA.  The side
-  // streams' kernels take SMs as they free up.
+  // The updates and the panel product give each CTA an even share of up to
+  // 32 tiles (the accumulator double buffer pays over a run; the runs end at
+  // staggered times, so an SM frees up every few microseconds); U' (low
+  // priority, off the chain) one tile per CTA, so that it never holds SMs
+  // the chain needs for long.
   constexpr int kBigRun = 0, kSideRun = 1;
   float* Aop[kOpBuffers] = {w.Aop, w.Aop + abuf, w.Aop + 2 * abuf};
   float* Bop[kOpBuffers] = {w.Bop, w.Bop + bbuf, w.Bop + 2 * bbuf};
   const size_t ainv_buf = (size_t)batch * kB * 2 * kB;
-  const int64_t a_stride = (int64_t)npad * 2 * kB, b_stride = 2 * (int64_t)npad * 2 * kB,
-                a3_stride = (int64_t)npad * kSplitK;
+  const int64_t a_stride = (int64_t)npad * 2 * kB;
   // Inverse of diagonal block kk (its A operand copy in ainv buffer of the
   // block's parity).
   auto inverse = [&](int kk, cudaStream_t on) {
     TimedLaunch tl(kKCluGj, on);
-    clu_gj_kernel<<<batch, 512, 0, on>>>(W, kk, info_dev, w.inv, nblk, w.binv,
+    clu_gj_kernel<<<batch, 32 * kGjWarps, 0, on>>>(W, kk, info_dev, w.inv, nblk, w.binv,
                                          w.ainv + ((kk / kB) & 1) * ainv_buf);
     ++launches;
   };
@@ -766,7 +789,7 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
     if (m <= 0) return BEM_OK;
     TimedLaunch tl(kKCluPanel, on);
     return cgemm_tf32_update(w.a3, npad, kk + kB, w.binv, 2 * kB, 0, kSplitK, W.re, W.im, npad, W.stride, kk + kB,
-                             kk, m, kB, batch, err_dev, on, 1, nullptr, nullptr, kSideRun, 0, act, Aop[buf],
+                             kk, m, kB, batch, err_dev, on, 1, nullptr, nullptr, kBigRun, 0, act, Aop[buf],
                              kPackRows, a_stride);
   };
   // Block row of U scaled by the diagonal inverse, U' = A_kk^{-1} A12 (TF32),
@@ -797,12 +820,13 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   // update is bound by reading and writing C).  Step k, on the caller's
   // stream: the diagonal block k+1 gets every update still pending on it and
   // its inverse starts on the side stream; then block row and block column
-  // k+1 get theirs, their epilogues packing the operands of step k+1 (A12 as
-  // the B operand, A21 split for the panel product); the panel L21 follows
-  // on the side stream (its epilogue packs the A operand), U' on the third
-  // stream.  Meanwhile, at every second step, the rest of the trailing matrix
-  // gets the updates of steps k-1 and k together.  Operands of steps k-1, k,
-  // k+1 live in three buffers; A_kk^{-1} for U' in two.
+  // k+1 get theirs and are packed as the operands of step k+1 (A12 as the B
+  // operand, A21 split for the panel product), all while the inverse runs;
+  // the panel L21 follows on the side stream (its epilogue packs the A
+  // operand), U' on the third stream.  Meanwhile, at every second step, the
+  // rest of the trailing matrix gets the updates of steps k-1 and k together.
+  // Operands of steps k-1, k, k+1 live in three buffers; A_kk^{-1} for U' in
+  // two.
   // Block 0: the operands come straight from the converted matrix.
   inverse(0, s);
   if (npad > kB) {
@@ -829,10 +853,16 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
     BEM_CUDA_CHECK(cudaEventRecord(la->diag, s));
     BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->diag, 0));
     inverse(kn, la->side);
-    // block row kn (packed as the B operand) and block column kn below the
-    // diagonal (packed split for the panel product)
-    if ((st = update(cur, kn, kn + kB, kB, rest, pend, 0, Bop[nxt], kPackCols, b_stride))) return st;
-    if ((st = update(cur, kn + kB, kn, rest, kB, pend, 0, w.a3, kPackRowsSplit, a3_stride))) return st;
+    // block row kn and block column kn below the diagonal, then their packed
+    // copies (A12 as the B operand, A21 split for the panel product)
+    if ((st = update(cur, kn, kn + kB, kB, rest, pend, 0))) return st;
+    if ((st = update(cur, kn + kB, kn, rest, kB, pend, 0))) return st;
+    if (rest > 0) {
+      TimedLaunch tl(kKCluPanel, s);
+      clu_pack_kernel<<<dim3(rest / kPT + rest / 32, batch), 256, 0, s>>>(W, npad, kn, rest / kPT, kn + kB, kn,
+                                                                         Bop[nxt], w.a3);
+      ++launches;
+    }
     BEM_CUDA_CHECK(cudaEventRecord(la->strips, s));
     BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->strips, 0));
     if ((st = panel(kn, nxt, la->side))) return st;

@@ -147,8 +147,8 @@ struct UpdateArgs {
   int tiles_m;       // tile grid: tiles_m x tiles_n x batch, tm fastest
   int tiles_n;
   int ntiles;
-  int tiles_per_cta;     // tiles of one CTA
-  int group_width;       // CTAs per group (the SM count)
+  int waves;             // CTA groups, each over its own range of consecutive tiles
+  int group_width;       // CTAs per group (at most the SM count)
   long long wait_limit;  // polls of a bounded mbarrier wait
   // Grouped launch (ngroup > 0): matrix b has gtm[b] x gtn[b] tiles of its own,
   // tiles gstart[b] .. gstart[b+1]-1 (matrices of different active sizes)
@@ -198,56 +198,23 @@ __device__ __forceinline__ bool mbar_wait_n(uint64_t* bar, uint32_t parity, int*
   return true;
 }
 
-// Packed copy of 16 result values of one thread: columns t0 .. t0 + 15 of the
-// tile in plane `plane` (0 real, 1 imaginary); off = t0 - cbase, the offset
-// from the thread's pack pointer in the row layouts.
-__device__ __forceinline__ void pack_chunk(int mode, float* pk, int plane, int t0, int off, const float (&v)[16]) {
-  if (mode == kPackRows) {
-    float4* d = reinterpret_cast<float4*>(pk + off);
+// Packed copy of 16 result values of one thread (row layout [Re | Im], 256
+// floats per row): off is the offset from the thread's pack pointer.
+__device__ __forceinline__ void pack_chunk(float* pk, int off, const float (&v)[16]) {
+  float4* d = reinterpret_cast<float4*>(pk + off);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) d[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-  } else if (mode == kPackRowsSplit) {
-    float4* hi0 = reinterpret_cast<float4*>(pk + off);
-    float4* lo = reinterpret_cast<float4*>(pk + kTN + off);
-    float4* hi1 = reinterpret_cast<float4*>(pk + 2 * kTN + off);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      float h[4], l[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        h[e] = __uint_as_float(__float_as_uint(v[4 * j + e]) & 0xffffe000u);  // the TF32 part
-        l[e] = v[4 * j + e] - h[e];                                           // exact remainder
-      }
-      hi0[j] = make_float4(h[0], h[1], h[2], h[3]);
-      lo[j] = make_float4(l[0], l[1], l[2], l[3]);
-      hi1[j] = make_float4(h[0], h[1], h[2], h[3]);
-    }
-  } else {
-    // B operand rows of complex columns t: Re to (t, k) and (128 + t, 128 + k);
-    // Im to (t, 128 + k) negated and (128 + t, k); k is the lane's row
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      float* r0 = pk + (size_t)(t0 + j) * kTN;
-      float* r1 = pk + (size_t)(kTNc + t0 + j) * kTN;
-      if (plane == 0) {
-        r0[0] = v[j];
-        r1[kTNc] = v[j];
-      } else {
-        r0[kTNc] = -v[j];
-        r1[0] = v[j];
-      }
-    }
-  }
+  for (int j = 0; j < 4; ++j) d[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
 }
 
 // Trailing update with double-buffered accumulators: a CTA (one per SM: 197 KB
-// of shared memory, all 512 tensor-memory columns) takes a run of
-// tiles_per_cta 128 x 128 complex tiles, spaced so that the CTAs of a group
-// work on consecutive tiles at any time (their operands stay in L2), and
-// alternates between two accumulators in tensor memory, so that the epilogue
-// of tile i (read C, subtract, write C) overlaps the MMAs of tile i+1.  CTAs
-// retire after their run, so kernels of other streams (the lookahead of the
-// block LU) get SMs within one run.  Barriers: full/empty per operand stage (TMA -> MMA -> TMA),
+// of shared memory, all 512 tensor-memory columns) takes a run of 128 x 128
+// complex tiles (an even share of its group's tile range), spaced so that the
+// CTAs of a group work on consecutive tiles at any time (their operands stay
+// in L2), and alternates between two accumulators in tensor memory, so that
+// the epilogue of tile i (read C, subtract, write C) overlaps the MMAs of tile
+// i+1.  CTAs retire after their run, so kernels of other streams (the
+// lookahead of the block LU) get SMs within one run.  Barriers: full/empty per
+// operand stage (TMA -> MMA -> TMA),
 // acc_full per accumulator (MMA commit -> epilogue), acc_empty per
 // accumulator (one arrival per epilogue warp -> MMA).
 __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __grid_constant__ CUtensorMap mapA,
@@ -294,22 +261,23 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  // This CTA's tiles: CTAs form groups of group_width (one per SM); group g
-  // covers tiles [g W T, (g+1) W T) and its CTA l takes the tiles
-  // g W T + l + j W_g (j < T, W_g the width of this group), so the CTAs of a
-  // group work on W consecutive tiles at a time (tm fastest: they share the
-  // operands in L2) and each retires after T tiles.
-  const int T = p.tiles_per_cta, Wd = p.group_width;
-  const int grp = blockIdx.x / Wd, l = blockIdx.x - grp * Wd;
-  const int Wg = min(Wd, (int)gridDim.x - grp * Wd);
-  const int t_first = grp * Wd * T + l;
+  // This CTA's tiles: `waves` groups of group_width CTAs (one CTA per SM);
+  // group g covers the tiles [g N / G, (g+1) N / G) and its CTA l takes the
+  // tiles start + l + j W, so the CTAs of a group work on W consecutive tiles
+  // at a time (tm fastest: they share the operands in L2), every CTA of a
+  // group has the same number of tiles to within one, and each retires after
+  // its share (the next group takes its SM).
+  const int Wg = p.group_width;
+  const int grp = blockIdx.x / Wg, l = blockIdx.x - grp * Wg;
+  const int t_first = (int)((long long)grp * p.ntiles / p.waves) + l;
+  const int t_end = (int)((long long)(grp + 1) * p.ntiles / p.waves);
 
   if (warp == 0) {
     if (lane == 0) {
       // producer: operand slices of every tile of this CTA through the ring
       bool ok = true;
       long long g = 0;  // stage uses so far
-      for (int jt = 0, t = t_first; jt < T && t < p.ntiles && ok; ++jt, t += Wg) {
+      for (int t = t_first; t < t_end && ok; t += Wg) {
         int b, tm, tn;
         decode_tile(p, t, b, tm, tn);
         b += p.batch0;
@@ -335,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
       bool ok = true;
       long long g = 0;
       int i = 0;  // tiles of this CTA so far
-      for (int jt = 0, t = t_first; jt < T && t < p.ntiles && ok; ++jt, t += Wg, ++i) {
+      for (int t = t_first; t < t_end && ok; t += Wg, ++i) {
         const int acc = i & 1;
         const uint32_t use = (uint32_t)(i >> 1);
         // the epilogue must have drained this accumulator's previous tile
@@ -374,7 +342,7 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
     const int64_t ldc = p.ldc;
     bool ok = true;
     int i = 0;
-    for (int jt = 0, t = t_first; jt < T && t < p.ntiles && ok; ++jt, t += Wg, ++i) {
+    for (int t = t_first; t < t_end && ok; t += Wg, ++i) {
       int b, tm, tn;
       decode_tile(p, t, b, tm, tn);
       b += p.batch0;
@@ -394,15 +362,10 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
       __syncwarp();
       if (!ok) break;
       const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kAccCols + plane * kTNc + cbase);
-      // packed copy: this thread's row of the tile (kPackRows*), or its K'
-      // index within the block row (kPackCols)
-      float* pk = nullptr;
-      if (p.pack_mode == kPackRows || p.pack_mode == kPackRowsSplit) {
-        const int kpk = p.pack_mode == kPackRows ? kTN : 3 * kTN;
-        pk = p.pack + (size_t)b * p.pack_stride + (size_t)row * kpk + plane * kTNc + cbase;
-      } else if (p.pack_mode == kPackCols) {
-        pk = p.pack + (size_t)b * p.pack_stride + (size_t)(2 * (p.c_col0 + tn * kTNc)) * kTN + 32 * q + lane;
-      }
+      // packed copy: this thread's row of the tile
+      float* pk = p.pack_mode == kPackRows
+                      ? p.pack + (size_t)b * p.pack_stride + (size_t)row * kTN + plane * kTNc + cbase
+                      : nullptr;
 #pragma unroll
       for (int chunk = 0; chunk < kChunks; chunk += 2) {
         if (rd) {
@@ -417,7 +380,7 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
             v[j] = rd ? cb0[j] - v[j] : v[j];
             __stcs(C + (size_t)(chunk * kCW + j) * ldc, v[j]);
           }
-          if (pk) pack_chunk(p.pack_mode, pk, plane, cbase + chunk * kCW, chunk * kCW, v);
+          if (pk) pack_chunk(pk, chunk * kCW, v);
         }
         if (rd && chunk + 2 < kChunks) {
 #pragma unroll
@@ -431,7 +394,7 @@ __global__ void __launch_bounds__(kThreads, 1) cgemm_tf32_update_kernel(const __
             v[j] = rd ? cb1[j] - v[j] : v[j];
             __stcs(C + (size_t)((chunk + 1) * kCW + j) * ldc, v[j]);
           }
-          if (pk) pack_chunk(p.pack_mode, pk, plane, cbase + (chunk + 1) * kCW, (chunk + 1) * kCW, v);
+          if (pk) pack_chunk(pk, (chunk + 1) * kCW, v);
         }
       }
       // this warp's reads of the accumulator are complete: release it
@@ -501,10 +464,9 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
                       int pack_mode, int64_t pack_stride) {
   if (m <= 0 || n <= 0) return BEM_OK;
   if (pack_mode != kPackNone &&
-      (!pack || (pack_mode == kPackCols ? m != kTM : n != kTNc) || (reinterpret_cast<uintptr_t>(pack) & 15) ||
-       pack_mode < kPackNone || pack_mode > kPackCols))
-    return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: packed copy needs one tile row (columns) or "
-                                               "one tile column (rows) and a 16-byte aligned destination");
+      (pack_mode != kPackRows || !pack || n != kTNc || (reinterpret_cast<uintptr_t>(pack) & 15)))
+    return set_error(BEM_ERR_INVALID_ARGUMENT,
+                     "cgemm_tf32_update: a packed copy needs one tile column and a 16-byte aligned destination");
   if (m % kTM || n % kTNc || kp % kKC || (a_row0 % 8) || (b_row0 % 8))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: sizes must be multiples of 128 (K' of 32)");
   if ((Aop1 == nullptr) != (Bop1 == nullptr))
@@ -570,11 +532,16 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
     if (ntiles > (1ll << 30)) return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: too many tiles");
     if (ntiles == 0) continue;
     p.ntiles = (int)ntiles;
-    int tpc = run > 0 ? run : (int)std::max(1ll, std::min(32ll, ntiles / (2ll * sms)));
-    const long long ctas = (ntiles + tpc - 1) / tpc;
+    // groups of up to one CTA per SM, each CTA with about `per` tiles (run, or
+    // up to 32 for the big updates so that other streams get SMs within a run)
+    const long long per = run > 0 ? run : 32;
+    const long long waves = (ntiles + (long long)sms * per - 1) / ((long long)sms * per);
+    const long long width = std::min<long long>(sms, (ntiles + waves * (run > 0 ? run : 1) - 1) /
+                                                         (waves * (run > 0 ? run : 1)));
+    const long long ctas = waves * width;
     UpdateArgs q = p;
-    q.tiles_per_cta = tpc;
-    q.group_width = sms;
+    q.waves = (int)waves;
+    q.group_width = (int)width;
     q.batch0 = b0;  // the matrices of this launch: b0 .. b0 + nb - 1
     {
       TimedLaunch tl(kKCgemmTf32, stream);
