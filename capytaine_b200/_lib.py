@@ -225,10 +225,18 @@ def require_cuda(device=None):
     return torch.device(device if device is not None else "cuda")
 
 
-def stream_ptr(stream=None):
+def current_stream_handle() -> int:
+    """cudaStream_t of the current stream of the current device (torch's raw
+    query, without the Stream object that torch.cuda.current_stream builds)."""
     import torch
-    s = stream if stream is not None else torch.cuda.current_stream()
-    return ctypes.c_void_p(s.cuda_stream)
+    try:
+        return torch._C._cuda_getCurrentRawStream(torch._C._cuda_getDevice())
+    except AttributeError:  # a torch without the raw query
+        return torch.cuda.current_stream().cuda_stream
+
+
+def stream_ptr(stream=None):
+    return ctypes.c_void_p(stream.cuda_stream if stream is not None else current_stream_handle())
 
 
 class StreamShared:
@@ -254,16 +262,68 @@ class StreamShared:
         return self
 
 
+class _Staging(threading.local):
+    """A thread's pinned staging ring for uploads (one allocation, reused)."""
+    buf = None
+    off = 0
+    event = None
+    copy_stream = None
+
+
+_staging = _Staging()
+_STAGING_MIN = 32 << 20
+
+
 def upload(a, dtype, device):
-    """Host array -> device tensor of `dtype` on the current stream without
-    waiting for the stream: the values go through pinned host memory (the
-    caching host allocator keeps the staging block until the copy has run)."""
+    """Host array -> device tensor of `dtype` (see upload_many)."""
+    return upload_many([(a, dtype)], device)[0]
+
+
+def upload_many(arrays, device):
+    """Host arrays -> device tensors [(array, torch dtype), ...] in one
+    transfer, ready for the current stream without waiting for its earlier
+    work: the values go through the calling thread's pinned staging ring (one
+    allocation, reused) and its own copy stream into one device allocation
+    that the returned tensors view; the current stream waits for the copy on
+    the device.  The ring waits on the host only for its own last copy, and
+    only when it wraps around."""
     import numpy as np
     import torch
-    host = torch.from_numpy(np.ascontiguousarray(a)).to(dtype)
+    hosts = [torch.from_numpy(np.ascontiguousarray(a)).to(dt) for a, dt in arrays]
     if torch.device(device).type != "cuda":
-        return host.to(device)
-    return host.pin_memory().to(device, non_blocking=True)
+        return [h.to(device) for h in hosts]
+    offs, total = [], 0
+    for h in hosts:
+        offs.append(total)
+        total += -(-(h.numel() * h.element_size()) // 256) * 256
+    st = _staging
+    compute = torch.cuda.current_stream()
+    if st.copy_stream is None or st.copy_stream.device != compute.device:
+        if st.event is not None:
+            st.event.synchronize()
+        st.copy_stream = torch.cuda.Stream(device=compute.device)
+        st.buf = None
+    if st.buf is None or total > st.buf.numel():
+        if st.event is not None:
+            st.event.synchronize()  # the old ring's copies have run before it is dropped
+        st.buf = torch.empty(max(_STAGING_MIN, 2 * total), dtype=torch.uint8, pin_memory=True)
+        st.off = 0
+        st.event = torch.cuda.Event()
+    elif st.off + total > st.buf.numel():
+        st.event.synchronize()  # the copies out of the ring's start have run
+        st.off = 0
+    stage = st.buf[st.off:st.off + total]
+    for h, o in zip(hosts, offs):
+        nb = h.numel() * h.element_size()
+        stage[o:o + nb].view(h.dtype).view(h.shape).copy_(h)
+    with torch.cuda.stream(st.copy_stream):
+        dev = torch.empty(total, dtype=torch.uint8, device=compute.device)
+        dev.copy_(stage, non_blocking=True)
+        st.event.record(st.copy_stream)
+    compute.wait_event(st.event)
+    dev.record_stream(compute)  # its memory is not reused before the current stream is done with it
+    st.off += total
+    return [dev[o:o + h.numel() * h.element_size()].view(h.dtype).view(h.shape) for h, o in zip(hosts, offs)]
 
 
 def ptr(t):

@@ -805,12 +805,11 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   // C rows r0.. (m), complex columns c0.. (nc) -= L21 U12 of the block step whose
   // packed operands are in buffer buf, and of a second step (buffer buf2 >= 0)
   // in the same pass over C (depth 256); optionally a packed copy of the result.
-  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2, int run, float* pack = nullptr,
-                    int pack_mode = kPackNone, int64_t pack_stride = 0) -> int {
+  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2, int run, bool lshape = false) -> int {
     if (m <= 0 || nc <= 0) return BEM_OK;
     return cgemm_tf32_update(Aop[buf], npad, r0, Bop[buf], 2 * (int64_t)npad, 2 * c0, 2 * kB, W.re, W.im, npad,
                              W.stride, r0, c0, m, nc, batch, err_dev, s, 0, buf2 >= 0 ? Aop[buf2] : nullptr,
-                             buf2 >= 0 ? Bop[buf2] : nullptr, run, 0, act, pack, pack_mode, pack_stride);
+                             buf2 >= 0 ? Bop[buf2] : nullptr, run, 0, act, nullptr, kPackNone, 0, lshape);
   };
   Lookahead* la = nullptr;
   if ((st = lookahead_for(s, &la))) return st;
@@ -853,11 +852,11 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
     BEM_CUDA_CHECK(cudaEventRecord(la->diag, s));
     BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->diag, 0));
     inverse(kn, la->side);
-    // block row kn and block column kn below the diagonal, then their packed
-    // copies (A12 as the B operand, A21 split for the panel product)
-    if ((st = update(cur, kn, kn + kB, kB, rest, pend, 0))) return st;
-    if ((st = update(cur, kn + kB, kn, rest, kB, pend, 0))) return st;
+    // block row kn and block column kn below the diagonal (one L-shaped
+    // launch), then their packed copies (A12 as the B operand, A21 split for
+    // the panel product)
     if (rest > 0) {
+      if ((st = update(cur, kn, kn, rest + kB, rest + kB, pend, 0, true))) return st;
       TimedLaunch tl(kKCluPanel, s);
       clu_pack_kernel<<<dim3(rest / kPT + rest / 32, batch), 256, 0, s>>>(W, npad, kn, rest / kPT, kn + kB, kn,
                                                                          Bop[nxt], w.a3);

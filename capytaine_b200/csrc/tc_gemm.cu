@@ -159,6 +159,10 @@ struct UpdateArgs {
   float* pack;
   int64_t pack_stride;  // floats between matrices
   int pack_mode;
+  // L-shaped launch: only the first tile row and the first tile column of the
+  // m x n block, without the corner tile (R = tiles_m - 1 of each; grouped:
+  // R of matrix b in gtm[b])
+  int lshape;
   int gstart[kMaxGroup + 1];
   short gtm[kMaxGroup];
   short gtn[kMaxGroup];
@@ -166,6 +170,27 @@ struct UpdateArgs {
 
 // Matrix and tile coordinates of tile t of the launch.
 __device__ __forceinline__ void decode_tile(const UpdateArgs& p, int t, int& b, int& tm, int& tn) {
+  if (p.lshape) {
+    int R, r;
+    if (p.ngroup > 0) {
+      b = 0;
+      while (b + 1 < p.ngroup && p.gstart[b + 1] <= t) ++b;
+      R = p.gtm[b];
+      r = t - p.gstart[b];
+    } else {
+      R = p.tiles_m - 1;
+      b = t / (2 * R);
+      r = t - b * 2 * R;
+    }
+    if (r < R) {
+      tm = 0;
+      tn = r + 1;
+    } else {
+      tm = r - R + 1;
+      tn = 0;
+    }
+    return;
+  }
   if (p.ngroup > 0) {
     b = 0;
     while (b + 1 < p.ngroup && p.gstart[b + 1] <= t) ++b;
@@ -461,8 +486,11 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store, const float* Aop1,
                       const float* Bop1, int run, long long wait_limit, const int* limit_host, float* pack,
-                      int pack_mode, int64_t pack_stride) {
+                      int pack_mode, int64_t pack_stride, bool lshape) {
   if (m <= 0 || n <= 0) return BEM_OK;
+  if (lshape && (m != n || m <= kTM || pack_mode != kPackNone))
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: an L-shaped update needs a square block of "
+                                               "more than one tile and no packed copy");
   if (pack_mode != kPackNone &&
       (pack_mode != kPackRows || !pack || n != kTNc || (reinterpret_cast<uintptr_t>(pack) & 15)))
     return set_error(BEM_ERR_INVALID_ARGUMENT,
@@ -509,12 +537,13 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
   p.pack = pack;
   p.pack_stride = pack_stride;
   p.pack_mode = pack_mode;
+  p.lshape = lshape ? 1 : 0;
   int launches = 0;
   // Grouped: matrix b covers only rows and columns below limit_host[b] (its
   // active size), launches of at most kMaxGroup matrices
   for (int b0 = 0; b0 < batch; b0 += limit_host ? kMaxGroup : batch) {
     const int nb = limit_host ? std::min(kMaxGroup, batch - b0) : batch;
-    long long ntiles = (long long)tiles_m * tiles_n * nb;
+    long long ntiles = lshape ? 2ll * (tiles_m - 1) * nb : (long long)tiles_m * tiles_n * nb;
     if (limit_host) {
       p.ngroup = nb;
       ntiles = 0;
@@ -522,9 +551,16 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
         const int lim = limit_host[b0 + i];
         const int mb = std::max(0, std::min(m, lim - c_row0)) / kTM;
         const int nbc = std::max(0, std::min(n, lim - c_col0)) / kTNc;
+        p.gstart[i] = (int)ntiles;
+        if (lshape) {  // R tiles in the row and R in the column beyond the corner
+          const int R = std::max(0, mb - 1);
+          p.gtm[i] = (short)R;
+          p.gtn[i] = 0;
+          ntiles += 2ll * R;
+          continue;
+        }
         p.gtm[i] = (short)std::max(mb, 1);  // never divides by zero; no tile when gtn is 0
         p.gtn[i] = (short)(mb > 0 ? nbc : 0);
-        p.gstart[i] = (int)ntiles;
         ntiles += (long long)(mb > 0 ? mb : 0) * (mb > 0 ? nbc : 0);
       }
       p.gstart[nb] = (int)ntiles;
@@ -568,5 +604,5 @@ extern "C" int bem_cgemm_tf32_update(const float* Aop_dev, int64_t a_rows, int a
     return bem::set_error(BEM_ERR_INVALID_ARGUMENT, "bem_cgemm_tf32_update: operands must be 16-byte aligned");
   return bem::cgemm_tf32_update(Aop_dev, a_rows, a_row0, Bop_dev, b_rows, b_row0, kp, Cr_dev, Ci_dev, ldc, c_stride,
                                 c_row0, c_col0, m, n, batch, err_dev, (cudaStream_t)stream, 0, nullptr, nullptr, 0, 0,
-                                nullptr);
+                                nullptr, nullptr, bem::kPackNone, 0, false);
 }

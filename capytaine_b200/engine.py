@@ -456,9 +456,12 @@ class B200Engine:
                 return hit[1].tensors
         # host arrays and uploads outside the lock (other threads' bodies go on)
         dev = self.device
-        arrays = (_lib.upload(body.dof_normal_components(), torch.float64, dev),
-                  _lib.upload(body.pressure_weights(), torch.float64, dev),
-                  _lib.upload(body.hull_mask.astype(np.int32), torch.int32, dev))
+        dnc = body.dof_normal_components()
+        mask = body.hull_mask
+        pw = -dnc  # pressure weights -(dof . n) area on the hull (FloatingBody.pressure_weights)
+        pw[:, mask] *= body.mesh.faces_areas[None, :]
+        arrays = tuple(_lib.upload_many([(dnc, torch.float64), (pw, torch.float64),
+                                         (mask.astype(np.int32), torch.int32)], dev))
         with self._lock:
             self._body_cache[key] = (weakref.ref(body), _lib.StreamShared(*arrays))
             while len(self._body_cache) > 32:

@@ -55,18 +55,15 @@ class DeviceMesh:
         import torch
         qp, qw = mesh.quadrature_points
         f64 = torch.float64
-        up = _lib.upload  # no wait for the stream's earlier work
         self.nb_faces = mesh.nb_faces
         self.nb_vertices = mesh.nb_vertices
-        self.vertices = up(mesh.vertices, f64, device)
-        self.faces = up(np.asarray(mesh.faces, dtype=np.int32), torch.int32, device)
-        self.centers = up(mesh.faces_centers, f64, device)
-        self.normals = up(mesh.faces_normals, f64, device)
-        self.areas = up(mesh.faces_areas, f64, device)
-        self.radii = up(mesh.faces_radiuses, f64, device)
+        # one transfer, no wait for the stream's earlier work
+        (self.vertices, self.faces, self.centers, self.normals, self.areas, self.radii, self.quad_points,
+         self.quad_weights) = _lib.upload_many(
+            [(mesh.vertices, f64), (np.asarray(mesh.faces, dtype=np.int32), torch.int32), (mesh.faces_centers, f64),
+             (mesh.faces_normals, f64), (mesh.faces_areas, f64), (mesh.faces_radiuses, f64), (qp, f64), (qw, f64)],
+            device)
         self.nb_quad_points = qp.shape[1]
-        self.quad_points = up(qp, f64, device)
-        self.quad_weights = up(qw, f64, device)
         self.centers_z = np.asarray(mesh.faces_centers[:, 2])
         # one quadrature point per face, at the face centre (collocation point)
         self.collocation_at_quadrature = bool(qp.shape[1] == 1 and np.array_equal(qp[:, 0, :], mesh.faces_centers))
