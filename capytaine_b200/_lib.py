@@ -262,18 +262,6 @@ class StreamShared:
         return self
 
 
-class _Staging(threading.local):
-    """A thread's pinned staging ring for uploads (one allocation, reused)."""
-    buf = None
-    off = 0
-    event = None
-    copy_stream = None
-
-
-_staging = _Staging()
-_STAGING_MIN = 32 << 20
-
-
 def upload(a, dtype, device):
     """Host array -> device tensor of `dtype` (see upload_many)."""
     return upload_many([(a, dtype)], device)[0]
@@ -281,49 +269,42 @@ def upload(a, dtype, device):
 
 def upload_many(arrays, device):
     """Host arrays -> device tensors [(array, torch dtype), ...] in one
-    transfer, ready for the current stream without waiting for its earlier
-    work: the values go through the calling thread's pinned staging ring (one
-    allocation, reused) and its own copy stream into one device allocation
-    that the returned tensors view; the current stream waits for the copy on
-    the device.  The ring waits on the host only for its own last copy, and
-    only when it wraps around."""
+    transfer on the current stream, without waiting for the stream's earlier
+    work: the values are packed into one host buffer (256-byte aligned
+    pieces) and copied asynchronously (the driver stages pageable memory
+    before returning), into one device allocation that the returned tensors
+    view.  Two CUDA calls per group of arrays: an allocation from the caching
+    allocator and the copy."""
     import numpy as np
     import torch
-    hosts = [torch.from_numpy(np.ascontiguousarray(a)).to(dt) for a, dt in arrays]
+    hosts = [np.ascontiguousarray(np.asarray(a), dtype=_NP_OF[dt]) for a, dt in arrays]
     if torch.device(device).type != "cuda":
-        return [h.to(device) for h in hosts]
+        return [torch.from_numpy(h).to(device) for h in hosts]
     offs, total = [], 0
     for h in hosts:
         offs.append(total)
-        total += -(-(h.numel() * h.element_size()) // 256) * 256
-    st = _staging
-    compute = torch.cuda.current_stream()
-    if st.copy_stream is None or st.copy_stream.device != compute.device:
-        if st.event is not None:
-            st.event.synchronize()
-        st.copy_stream = torch.cuda.Stream(device=compute.device)
-        st.buf = None
-    if st.buf is None or total > st.buf.numel():
-        if st.event is not None:
-            st.event.synchronize()  # the old ring's copies have run before it is dropped
-        st.buf = torch.empty(max(_STAGING_MIN, 2 * total), dtype=torch.uint8, pin_memory=True)
-        st.off = 0
-        st.event = torch.cuda.Event()
-    elif st.off + total > st.buf.numel():
-        st.event.synchronize()  # the copies out of the ring's start have run
-        st.off = 0
-    stage = st.buf[st.off:st.off + total]
+        total += -(-h.nbytes // 256) * 256
+    buf = np.empty(max(total, 1), dtype=np.uint8)
     for h, o in zip(hosts, offs):
-        nb = h.numel() * h.element_size()
-        stage[o:o + nb].view(h.dtype).view(h.shape).copy_(h)
-    with torch.cuda.stream(st.copy_stream):
-        dev = torch.empty(total, dtype=torch.uint8, device=compute.device)
-        dev.copy_(stage, non_blocking=True)
-        st.event.record(st.copy_stream)
-    compute.wait_event(st.event)
-    dev.record_stream(compute)  # its memory is not reused before the current stream is done with it
-    st.off += total
-    return [dev[o:o + h.numel() * h.element_size()].view(h.dtype).view(h.shape) for h, o in zip(hosts, offs)]
+        buf[o:o + h.nbytes] = h.reshape(-1).view(np.uint8)
+    dev = torch.from_numpy(buf).to(device, non_blocking=True)
+    return [dev[o:o + h.nbytes].view(dt).view(h.shape) for h, o, (_, dt) in zip(hosts, offs, arrays)]
+
+
+def _np_of():
+    import numpy as np
+    import torch
+    return {torch.float64: np.float64, torch.float32: np.float32, torch.int32: np.int32, torch.int64: np.int64,
+            torch.complex128: np.complex128, torch.complex64: np.complex64, torch.uint8: np.uint8}
+
+
+class _NpOf(dict):
+    def __missing__(self, key):
+        self.update(_np_of())
+        return dict.__getitem__(self, key)
+
+
+_NP_OF = _NpOf()
 
 
 def ptr(t):

@@ -390,22 +390,27 @@ __device__ __forceinline__ void st_release_i(int* p, int v) {
 // place.  Forward: y_i = b_i - sum_{j<i} L_ij y_j (unit block lower).  Backward:
 // x_i = A_ii^{-1} y_i - sum_{j>i} U'_ij x_j with U'_ij = A_ii^{-1} U_ij stored in
 // the factorisation, so each step of the dependency chain is one block product
-// in both sweeps.  Each CTA owns one 128-row block;
-// the off-diagonal block of a dependency is copied to shared memory
-// asynchronously (real and imaginary planes, 16-byte copies) before waiting for
-// that dependency; the diagonal inverse is staged through the same buffer.
-// Thread (r, h) accumulates row r over the half h of the 128-long inner
-// dimension for all NC columns (one float pair per entry of the tile, NC/2
-// 16-byte broadcast reads of the right-hand sides); the halves meet in P.
+// in both sweeps.  Each CTA owns one 128-row block.  The off-diagonal blocks
+// of its dependencies stream through a ring of kRing shared-memory slots, a
+// quarter block (32 columns, real and imaginary planes) per slot, copied
+// asynchronously (16-byte pieces) kRing - 1 quarters ahead of the product, so
+// the next blocks load while the current one is multiplied; only the
+// right-hand side of a dependency waits for its flag.  Thread (r, h)
+// accumulates row r over the half h of each quarter's columns for all NC
+// columns (NC/2 16-byte broadcast reads of the right-hand sides); the halves
+// meet in P at the end of each block.
+constexpr int kRing = 5;
+constexpr int kQCols = 32;                   // columns of a quarter block
+constexpr int kQFloats = 2 * kQCols * kB;    // one slot: [plane][column][row]
+
 template <int NC>
-__device__ __forceinline__ void tile_times_rhs(const float* __restrict__ Tre, const float* __restrict__ Tim,
-                                               const float2* __restrict__ Y, int r, int h, float2 (&acc)[NC]) {
-#pragma unroll
-  for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.0f, 0.0f);
+__device__ __forceinline__ void quarter_times_rhs(const float* __restrict__ Tre, const float* __restrict__ Tim,
+                                                  const float2* __restrict__ Y, int r, int h,
+                                                  float2 (&acc)[NC]) {
 #pragma unroll 4
-  for (int m = 64 * h; m < 64 * h + 64; ++m) {
-    const float ar = Tre[m * kB + r], ai = Tim[m * kB + r];
-    const float4* y4 = reinterpret_cast<const float4*>(Y + m * NC);
+  for (int mm = 16 * h; mm < 16 * h + 16; ++mm) {
+    const float ar = Tre[mm * kB + r], ai = Tim[mm * kB + r];
+    const float4* y4 = reinterpret_cast<const float4*>(Y + mm * NC);
 #pragma unroll
     for (int c2 = 0; c2 < NC / 2; ++c2) {
       const float4 y = y4[c2];
@@ -417,6 +422,12 @@ __device__ __forceinline__ void tile_times_rhs(const float* __restrict__ Tre, co
   }
 }
 
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 template <int NC>
 __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nblk, int batch,
                                                                const float2* __restrict__ inv, double2* B,
@@ -426,11 +437,10 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
                                                                const int* mskip) {
   if (skip && *skip) return;  // refinement already converged
   extern __shared__ __align__(16) float fsmf[];
-  float* Lre = fsmf;  // Lre[m*kB + r], 128 x 128
-  float* Lim = Lre + kB * kB;
-  float2* X = reinterpret_cast<float2*>(Lim + kB * kB);  // X[r*NC + c]
-  float2* Y = X + kB * NC;                                 // Y[m*NC + c]
-  float2* P = Y + kB * NC;                                 // P[r*NC + c]
+  float* ring = fsmf;                                                  // kRing slots of kQFloats
+  float2* X = reinterpret_cast<float2*>(ring + kRing * kQFloats);      // X[r*NC + c]
+  float2* Y = X + kB * NC;                                             // Y[m*NC + c]
+  float2* P = Y + kB * NC;                                             // P[r*NC + c]
   __shared__ int s_t;
   const int tid = threadIdx.x;
   const int r = tid & (kB - 1), h = tid >> 7;
@@ -455,17 +465,26 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   const float* Wre = W.re + (size_t)b * W.stride;
   const float* Wim = W.im + (size_t)b * W.stride;
   float2 acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.0f, 0.0f);
   if (!forward) {
     // x_i = A_ii^{-1} b_i - sum_j U'_ij x_j with U' = A_ii^{-1} U: the product
-    // with the diagonal inverse comes first, off the chain of dependencies
+    // with the diagonal inverse comes first, off the chain of dependencies,
+    // its four quarters staged in the first four slots
     const float2* Inv = inv + ((size_t)b * nblk + i) * kB * kB;
     for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
       const float2 v = __ldg(Inv + idx);  // element (idx % 128, idx / 128)
-      Lre[idx] = v.x;
-      Lim[idx] = v.y;
+      const int col = idx >> 7, row = idx & (kB - 1);
+      float* slot = ring + (col / kQCols) * kQFloats;
+      slot[(col % kQCols) * kB + row] = v.x;
+      slot[kQCols * kB + (col % kQCols) * kB + row] = v.y;
     }
     __syncthreads();
-    tile_times_rhs<NC>(Lre, Lim, X, r, h, acc);
+#pragma unroll 1
+    for (int qq = 0; qq < 4; ++qq) {
+      const float* slot = ring + qq * kQFloats;
+      quarter_times_rhs<NC>(slot, slot + kQCols * kB, X + qq * kQCols * NC, r, h, acc);
+    }
     if (h == 1) {
 #pragma unroll
       for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
@@ -478,57 +497,84 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
         X[r * NC + c] = make_float2(acc[c].x + o.x, acc[c].y + o.y);
       }
     }
-    __syncthreads();  // Lre/Lim are reused for the off-diagonal blocks
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.0f, 0.0f);
+    __syncthreads();  // the slots are reused for the off-diagonal blocks
   }
-  for (int q = 0; q < ndep; ++q) {
-    const int j = forward ? q : (nblk - 1 - q);
-    // off-diagonal block (does not depend on the flag): 128 columns x 128 rows,
-    // 32 sixteen-byte pieces per column and plane
-    for (int idx = tid; idx < kB * 32; idx += blockDim.x) {
-      const int m = idx >> 5, piece = idx & 31;
-      const size_t g = (size_t)(r0 + piece * 4) + (size_t)(j * kB + m) * W.ld;
-      cp_async16(Lre + m * kB + piece * 4, Wre + g);
-      cp_async16(Lim + m * kB + piece * 4, Wim + g);
+  // quarter q of the dependencies (block q / 4, columns 32 (q % 4) ..) into
+  // its ring slot: 32 columns x 128 rows per plane, 8 sixteen-byte pieces per
+  // thread
+  const int nq = 4 * ndep;
+  auto issue = [&](int q) {
+    const int jd = q >> 2, qq = q & 3;
+    const int j = forward ? jd : (nblk - 1 - jd);
+    float* slot = ring + (q % kRing) * kQFloats;
+    for (int idx = tid; idx < kQCols * 32; idx += blockDim.x) {
+      const int mm = idx >> 5, piece = idx & 31;
+      const size_t g = (size_t)(r0 + piece * 4) + (size_t)(j * kB + qq * kQCols + mm) * W.ld;
+      cp_async16(slot + mm * kB + piece * 4, Wre + g);
+      cp_async16(slot + kQCols * kB + mm * kB + piece * 4, Wim + g);
     }
-    if (tid == 0) {
-      long long it = 0;
-      while (ld_acquire_i(flags + (size_t)b * nblk + j) == 0) {
-        if (++it > spin_limit) {
-          atomicExch(err, 1);
-          break;
+  };
+#pragma unroll 1
+  for (int q = 0; q < kRing - 1; ++q) {
+    if (q < nq) issue(q);
+    cp_async_commit();
+  }
+#pragma unroll 1
+  for (int q = 0; q < nq; ++q) {
+    const int jd = q >> 2, qq = q & 3;
+    __syncthreads();  // every thread is done with the slot refilled below (and with Y, at a new block)
+    if (qq == 0) {
+      const int j = forward ? jd : (nblk - 1 - jd);
+      if (tid == 0) {
+        long long it = 0;
+        while (ld_acquire_i(flags + (size_t)b * nblk + j) == 0) {
+          if (++it > spin_limit) {
+            atomicExch(err, 1);
+            break;
+          }
+          __nanosleep(64);
         }
-        __nanosleep(64);
+      }
+      __syncthreads();
+      for (int idx = tid; idx < kB * NC; idx += blockDim.x) {
+        const int m = idx & (kB - 1), c = idx >> 7;
+        float2 v = make_float2(0.0f, 0.0f);
+        if (c < nrhs) {
+          const double2 d = __ldcg(Bb + (size_t)(j * kB + m) + (size_t)c * ldb);
+          v = make_float2((float)d.x, (float)d.y);
+        }
+        Y[m * NC + c] = v;
       }
     }
-    __syncthreads();
-    for (int idx = tid; idx < kB * NC; idx += blockDim.x) {
-      const int m = idx & (kB - 1), c = idx >> 7;
-      float2 v = make_float2(0.0f, 0.0f);
-      if (c < nrhs) {
-        const double2 d = __ldcg(Bb + (size_t)(j * kB + m) + (size_t)c * ldb);
-        v = make_float2((float)d.x, (float)d.y);
-      }
-      Y[m * NC + c] = v;
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    tile_times_rhs<NC>(Lre, Lim, Y, r, h, acc);
-    if (h == 1) {
+    if (q + kRing - 1 < nq) issue(q + kRing - 1);
+    cp_async_commit();
+    cp_async_wait_group<kRing - 1>();  // this thread's copies of quarter q have landed
+    __syncthreads();                   // everyone's copies, and Y
+    const float* slot = ring + (q % kRing) * kQFloats;
+    quarter_times_rhs<NC>(slot, slot + kQCols * kB, Y + qq * kQCols * NC, r, h, acc);
+    if (qq == 3) {
+      if (h == 1) {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
-    }
-    __syncthreads();
-    if (h == 0) {
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const float2 o = P[r * NC + c];
-        float2 x = X[r * NC + c];
-        x.x -= acc[c].x + o.x;
-        x.y -= acc[c].y + o.y;
-        X[r * NC + c] = x;
+        for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
       }
+      __syncthreads();
+      if (h == 0) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const float2 o = P[r * NC + c];
+          float2 x = X[r * NC + c];
+          x.x -= acc[c].x + o.x;
+          x.y -= acc[c].y + o.y;
+          X[r * NC + c] = x;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.0f, 0.0f);
     }
   }
+  cp_async_wait_all();
   // forward (unit block lower factor): y_i = X; backward: x_i = X
   __syncthreads();
   for (int idx = tid; idx < kB * NC; idx += blockDim.x) {
@@ -545,7 +591,7 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   if (tid == 0 && i != withheld) st_release_i(flags + (size_t)b * nblk + i, 1);
 }
 
-constexpr int trsm_smem_bytes(int nc) { return 2 * kB * kB * (int)sizeof(float) + 3 * kB * nc * (int)sizeof(float2); }
+constexpr int trsm_smem_bytes(int nc) { return kRing * kQFloats * (int)sizeof(float) + 3 * kB * nc * (int)sizeof(float2); }
 
 // x += r (the correction solved in place in r), then r = b for the residual.
 __global__ void ir_update_kernel(double2* __restrict__ X, double2* __restrict__ R, const double2* __restrict__ Bv,
