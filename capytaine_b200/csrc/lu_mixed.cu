@@ -865,11 +865,12 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   // update is bound by reading and writing C).  Step k, on the caller's
   // stream: the diagonal block k+1 gets every update still pending on it and
   // its inverse starts on the side stream; then block row and block column
-  // k+1 get theirs and are packed as the operands of step k+1 (A12 as the B
-  // operand, A21 split for the panel product), all while the inverse runs;
-  // the panel L21 follows on the side stream (its epilogue packs the A
-  // operand), U' on the third stream.  Meanwhile, at every second step, the
-  // rest of the trailing matrix gets the updates of steps k-1 and k together.
+  // k+1 get theirs (one L-shaped launch) and are packed as the operands of
+  // step k+1 (A12 as the B operand, A21 split for the panel product) while
+  // the inverse runs; the panel L21 follows on the side stream (its epilogue
+  // packs the A operand), U' on the third stream.  Meanwhile, at every
+  // second step, the rest of the trailing matrix gets the updates of steps
+  // k-1 and k together.
   // Operands of steps k-1, k, k+1 live in three buffers; A_kk^{-1} for U' in
   // two.
   // Block 0: the operands come straight from the converted matrix.
@@ -900,7 +901,11 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
     inverse(kn, la->side);
     // block row kn and block column kn below the diagonal (one L-shaped
     // launch), then their packed copies (A12 as the B operand, A21 split for
-    // the panel product)
+    // the panel product), beside the inverse.  (Packing behind the inverse on
+    // the side stream at the steps with a big update, so that the big update
+    // starts right after the strips, measured slower: the pack then shares
+    // the SMs and HBM with the big update.)
+    const bool big_step = (step & 1) && rest > 0;
     if (rest > 0) {
       if ((st = update(cur, kn, kn, rest + kB, rest + kB, pend, 0, true))) return st;
       TimedLaunch tl(kKCluPanel, s);
@@ -915,7 +920,7 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
     BEM_CUDA_CHECK(cudaStreamWaitEvent(la->upper, la->panel, 0));
     if ((st = upper(kn, nxt, la->upper))) return st;
     BEM_CUDA_CHECK(cudaEventRecord(la->upper_done[(step + 1) & 1], la->upper));
-    if ((step & 1) && rest > 0) {
+    if (big_step) {
       if ((st = update(cur, kn + kB, kn + kB, rest, rest, prev, kBigRun))) return st;
     }
     BEM_CUDA_CHECK(cudaStreamWaitEvent(s, la->panel, 0));
