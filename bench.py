@@ -448,6 +448,55 @@ def run_finite_depth(args):
     return 0
 
 
+def run_profile_case(case):
+    """Small cases of the LU kernels for ncu captures (a few GB on the device at
+    most, inputs of the update above L2): the launches are those of the
+    6084-panel barge's LU at smaller batch."""
+    import ctypes
+    import torch
+    from capytaine_b200 import _lib
+    lib = _lib.load()
+    s = _lib.stream_ptr()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def vp(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def factor(n, batch):
+        K = 0.05 * torch.randn((batch, n, n), dtype=torch.complex128, device="cuda")
+        K.diagonal(dim1=1, dim2=2).add_(3.0)
+        work = torch.empty(int(lib.bem_clu_workspace_bytes(n, batch)) + 1024, dtype=torch.uint8, device="cuda")
+        wv = work[(-work.data_ptr()) % 1024:]
+        piv = torch.zeros((batch, n), dtype=torch.int32, device="cuda")
+        info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+        _lib.check(lib.bem_clu_factor(vp(K), n, n * n, n, n, batch, vp(piv), vp(info), vp(wv), vp(err), s))
+        return K, wv, piv
+
+    if case == "gemm":
+        m, kp, batch = 4480, 512, 2
+        Aop = torch.randn((batch, m, kp), device="cuda", dtype=torch.float32)
+        Bop = torch.randn((batch, 2 * m, kp), device="cuda", dtype=torch.float32)
+        Cr = torch.randn((batch, m, m), device="cuda", dtype=torch.float32)
+        Ci = torch.randn((batch, m, m), device="cuda", dtype=torch.float32)
+        for _ in range(3):
+            _lib.check(lib.bem_cgemm_tf32_update(vp(Aop), m, 0, vp(Bop), 2 * m, 0, kp, vp(Cr), vp(Ci), m, m * m,
+                                                 0, 0, m, m, batch, vp(err), s))
+    elif case == "gj":
+        for _ in range(2):
+            factor(1024, 2)
+    else:
+        n, batch, nrhs = 4096, 4, 7
+        K, wv, piv = factor(n, batch)
+        B = torch.ones((batch, nrhs, n), dtype=torch.complex128, device="cuda")
+        for _ in range(2):
+            _lib.check(lib.bem_clu_solve(vp(wv), n, batch, vp(piv), vp(B), n, n * nrhs, nrhs, vp(err), s))
+    torch.cuda.synchronize()
+    if int(err.item()) != 0:
+        raise RuntimeError(f"profile case {case}: kernel error flag set")
+    print(json.dumps({"profile_case": case, "ok": True}))
+    return 0
+
+
 # ---------------------------------------------------------------------------
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
@@ -718,7 +767,13 @@ def main():
     ap.add_argument("--array-batch", type=int, default=4)
     ap.add_argument("--accuracy-stride", type=int, default=5,
                     help="the accuracy leg checks every n-th frequency of the sweep against the oracle")
+    ap.add_argument("--profile-case", choices=["gemm", "gj", "trsm"],
+                    help="run one small case for an ncu capture and exit: gemm = three trailing updates of "
+                         "depth 256 (m = 4480, 2 matrices); gj = two mixed LUs of 2 x 1024 (16 Gauss-Jordan "
+                         "inverses); trsm = a 4 x 4096 mixed LU and two solves of 7 right-hand sides")
     args = ap.parse_args()
+    if args.profile_case:
+        return run_profile_case(args.profile_case)
     args.world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         return run_reference(args)
