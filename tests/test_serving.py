@@ -171,12 +171,14 @@ def test_scheduler_batches_waiting_requests_of_similar_sizes():
     requests whose padded sizes lie within the band into one grouped
     factorisation; requests of other sizes, repeats of resident factors and
     other headings stay out; every request gets its own result."""
-    eng = _StandInEngine(delay=0.05)
+    eng = _StandInEngine(delay=0.2)
+    same = [_body(10), _body(9), _body(10, dofs=("Heave", "Surge"))]  # 300, 297, 300 panels
+    far = _body(24)
+    for b in same + [far]:  # geometry and hashes ready, so that the submissions below are quick
+        _ = b.mesh_including_lid.content_hash
     with _server(eng, slots=1, memory_budget=1 << 30, batch_max=4) as srv:
         blocker = srv.submit(_body(4), 0.1)  # occupies the slot while the others queue
         time.sleep(0.02)
-        same = [_body(10), _body(9), _body(10, dofs=("Heave", "Surge"))]  # 300, 297, 300 panels
-        far = _body(24)
         futs = [srv.submit(b, 0.5 + 0.1 * i) for i, b in enumerate(same)]
         f_far = srv.submit(far, 0.9)
         f_head = srv.submit(same[0], 1.7, wave_directions=(0.0, 1.0))  # other headings
