@@ -399,7 +399,11 @@ __device__ __forceinline__ void st_release_i(int* p, int v) {
 // accumulates row r over the half h of each quarter's columns for all NC
 // columns (NC/2 16-byte broadcast reads of the right-hand sides); the halves
 // meet in P at the end of each block.
-constexpr int kRing = 5;
+// Ring sizes: 5 slots (188 KB with 8 right-hand sides, one CTA per SM) when
+// every block row of the launch is resident at once; 2 slots (88 KB, two
+// CTAs per SM) when the block rows fill more than one wave of SMs, where
+// twice the resident CTAs hide more latency than a deeper ring.
+constexpr int kRingDeep = 5, kRingShallow = 2;
 constexpr int kQCols = 32;                   // columns of a quarter block
 constexpr int kQFloats = 2 * kQCols * kB;    // one slot: [plane][column][row]
 
@@ -428,13 +432,19 @@ __device__ __forceinline__ void cp_async_wait_group() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-template <int NC>
+template <int NC, int kRing>
 __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nblk, int batch,
                                                                const float2* __restrict__ inv, double2* B,
                                                                int64_t ldb, int64_t strideB, int nrhs, int forward,
                                                                int* flags, int* ticket, int* err, const int* skip,
                                                                long long spin_limit, int withheld,
                                                                const int* mskip) {
+  static_assert(kRing >= 2, "the ring keeps one quarter in flight beside the one multiplied");
+  // quarters of the diagonal inverse staged at a time: all four, or two per
+  // pass when the ring has fewer than four slots (a divisor of 4, never more
+  // slots than the ring has)
+  constexpr int kDiagPass = kRing >= 4 ? 4 : 2;
+  static_assert(4 % kDiagPass == 0 && kDiagPass <= kRing, "diagonal staging must fit the ring");
   if (skip && *skip) return;  // refinement already converged
   extern __shared__ __align__(16) float fsmf[];
   float* ring = fsmf;                                                  // kRing slots of kQFloats
@@ -470,20 +480,25 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   if (!forward) {
     // x_i = A_ii^{-1} b_i - sum_j U'_ij x_j with U' = A_ii^{-1} U: the product
     // with the diagonal inverse comes first, off the chain of dependencies,
-    // its four quarters staged in the first four slots
+    // its four quarters staged kDiagPass at a time in the first slots
     const float2* Inv = inv + ((size_t)b * nblk + i) * kB * kB;
-    for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
-      const float2 v = __ldg(Inv + idx);  // element (idx % 128, idx / 128)
-      const int col = idx >> 7, row = idx & (kB - 1);
-      float* slot = ring + (col / kQCols) * kQFloats;
-      slot[(col % kQCols) * kB + row] = v.x;
-      slot[kQCols * kB + (col % kQCols) * kB + row] = v.y;
-    }
-    __syncthreads();
 #pragma unroll 1
-    for (int qq = 0; qq < 4; ++qq) {
-      const float* slot = ring + qq * kQFloats;
-      quarter_times_rhs<NC>(slot, slot + kQCols * kB, X + qq * kQCols * NC, r, h, acc);
+    for (int q0 = 0; q0 < 4; q0 += kDiagPass) {
+      // columns [32 q0, 32 (q0 + kDiagPass)) of the inverse into slots 0 .. kDiagPass - 1
+      for (int idx = tid; idx < kDiagPass * kQCols * kB; idx += blockDim.x) {
+        const int col = q0 * kQCols + (idx >> 7), row = idx & (kB - 1);
+        const float2 v = __ldg(Inv + (size_t)col * kB + row);  // element (row, col)
+        float* slot = ring + (col / kQCols - q0) * kQFloats;
+        slot[(col % kQCols) * kB + row] = v.x;
+        slot[kQCols * kB + (col % kQCols) * kB + row] = v.y;
+      }
+      __syncthreads();
+#pragma unroll 1
+      for (int qq = q0; qq < q0 + kDiagPass; ++qq) {
+        const float* slot = ring + (qq - q0) * kQFloats;
+        quarter_times_rhs<NC>(slot, slot + kQCols * kB, X + qq * kQCols * NC, r, h, acc);
+      }
+      __syncthreads();  // the slots are restaged by the next pass
     }
     if (h == 1) {
 #pragma unroll
@@ -591,7 +606,7 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   if (tid == 0 && i != withheld) st_release_i(flags + (size_t)b * nblk + i, 1);
 }
 
-constexpr int trsm_smem_bytes(int nc) { return kRing * kQFloats * (int)sizeof(float) + 3 * kB * nc * (int)sizeof(float2); }
+constexpr int trsm_smem_bytes(int nc, int ring) { return ring * kQFloats * (int)sizeof(float) + 3 * kB * nc * (int)sizeof(float2); }
 
 // x += r (the correction solved in place in r), then r = b for the residual.
 __global__ void ir_update_kernel(double2* __restrict__ X, double2* __restrict__ R, const double2* __restrict__ Bv,
@@ -664,11 +679,27 @@ __global__ void refine_check_kernel(const double* __restrict__ bn, const double*
 bool g_mixed_configured = false;
 int configure_mixed() {
   if (g_mixed_configured) return BEM_OK;
-  BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      trsm_smem_bytes(8)));
-  BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      trsm_smem_bytes(16)));
+  BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<8, kRingDeep>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, trsm_smem_bytes(8, kRingDeep)));
+  BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<16, kRingDeep>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, trsm_smem_bytes(16, kRingDeep)));
+  BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<8, kRingShallow>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, trsm_smem_bytes(8, kRingShallow)));
+  BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<16, kRingShallow>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      trsm_smem_bytes(16, kRingShallow)));
   g_mixed_configured = true;
+  return BEM_OK;
+}
+
+// Streaming multiprocessors of the current device (cached per device).
+int sm_count(int* out) {
+  static int counts[64] = {0};
+  int dev = 0;
+  BEM_CUDA_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(BEM_ERR_UNSUPPORTED, "device index out of range");
+  if (!counts[dev]) BEM_CUDA_CHECK(cudaDeviceGetAttribute(&counts[dev], cudaDevAttrMultiProcessorCount, dev));
+  *out = counts[dev];
   return BEM_OK;
 }
 
@@ -949,20 +980,26 @@ int clu_solve_enqueue(void* work_dev, int npad, int batch, void* B_dev, int64_t 
   const int nblk = npad / kB;
   int* ticket = w.flags + (size_t)batch * nblk;
   int launches = 0;
+  int sms = 0;
+  if ((st = sm_count(&sms))) return st;
+  // more block rows than SMs: two CTAs per SM with the shallow ring
+  const bool shallow = (long long)nblk * batch > sms;
   for (int c0 = 0; c0 < nrhs; c0 += kRhs) {
     const int nc = std::min(kRhs, nrhs - c0);
     double2* Bc = (double2*)B_dev + (size_t)c0 * ldb;
     for (int forward = 1; forward >= 0; --forward) {
       BEM_CUDA_CHECK(cudaMemsetAsync(w.flags, 0, sizeof(int) * ((size_t)batch * nblk + 1), s));
       TimedLaunch tl(kKCtrsm, s);
-      if (nc <= 8)
-        ctrsm_persistent_kernel<8><<<nblk * batch, 256, trsm_smem_bytes(8), s>>>(
-            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip, spin_limit,
-            withheld, mskip);
-      else
-        ctrsm_persistent_kernel<16><<<nblk * batch, 256, trsm_smem_bytes(16), s>>>(
-            W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip, spin_limit,
-            withheld, mskip);
+#define BEM_CTRSM(NC, R)                                                                                \
+  ctrsm_persistent_kernel<NC, R><<<nblk * batch, 256, trsm_smem_bytes(NC, R), s>>>(                     \
+      W, nblk, batch, w.inv, Bc, ldb, strideB, nc, forward, w.flags, ticket, err_dev, skip, spin_limit, \
+      withheld, mskip)
+      if (nc <= 8) {
+        if (shallow) BEM_CTRSM(8, kRingShallow); else BEM_CTRSM(8, kRingDeep);
+      } else {
+        if (shallow) BEM_CTRSM(16, kRingShallow); else BEM_CTRSM(16, kRingDeep);
+      }
+#undef BEM_CTRSM
       ++launches;
     }
   }
