@@ -106,6 +106,8 @@ _SIGNATURES = {
     "bem_assemble_wave_symmetric": ([ctypes.POINTER(AssemblyArgs), c_void_p, c_i64, c_void_p], c_int),
     "bem_assemble_wave_symmetric_batched": ([ctypes.POINTER(AssemblyArgs), c_void_p, c_i64, c_void_p, c_int, c_i64,
                                              c_i64, c_void_p], c_int),
+    "bem_assemble_wave_symmetric_batched_lu": ([ctypes.POINTER(AssemblyArgs), c_void_p, c_i64, c_void_p, c_int,
+                                                c_i64, c_i64, c_void_p, c_int, c_int, c_void_p], c_int),
     "bem_assemble_symmetric": ([ctypes.POINTER(AssemblyArgs), c_void_p], c_int),
     "bem_assemble_finite_depth": ([ctypes.POINTER(AssemblyArgs), c_double, c_int, c_void_p, c_int, c_void_p], c_int),
     "bem_assemble_wave_cached": ([ctypes.POINTER(AssemblyArgs), c_void_p, c_i64, c_void_p, c_int, c_i64, c_i64,
@@ -131,6 +133,7 @@ _SIGNATURES = {
                         c_void_p], c_int),
     "bem_clu_factor_grouped": ([c_void_p, c_i64, c_i64, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                 c_void_p, c_void_p], c_int),
+    "bem_clu_factor_planes": ([c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int),
     "bem_clu_solve": ([c_void_p, c_int, c_int, c_void_p, c_void_p, c_i64, c_i64, c_int, c_void_p, c_void_p], c_int),
     "bem_clu_solve_bounded": ([c_void_p, c_int, c_int, c_void_p, c_void_p, c_i64, c_i64, c_int, ctypes.c_longlong,
                                c_int, c_void_p, c_void_p], c_int),

@@ -663,6 +663,12 @@ constexpr int kSymBatch = 64;
 struct SymBatch {
   double k[kSymBatch];
   int64_t s_stride, k_stride;  // elements between the outputs of consecutive wavenumbers
+  // optional float32 copy of K in the planes of the mixed LU's workspace
+  // (real plane at w, imaginary plane w_im floats further; leading dimension
+  // w_ld, w_stride floats between wavenumbers): the LU then needs no
+  // conversion pass over K
+  float* w;
+  int64_t w_ld, w_stride, w_im;
 };
 
 // GENERAL: any collocation points (rows, a.n) against the panels of mesh2
@@ -682,6 +688,7 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
   const double k = kb.k[blockIdx.z];
   a.S_dev = reinterpret_cast<double2*>(a.S_dev) + blockIdx.z * kb.s_stride;
   a.K_dev = reinterpret_cast<double2*>(a.K_dev) + blockIdx.z * kb.k_stride;
+  float* Wre = kb.w ? kb.w + blockIdx.z * kb.w_stride : nullptr;
   __shared__ SymFace faces[kSymT];
   __shared__ double4 mir[kSymChunk][kSymT];  // (S_w re, S_w im, K_w re, K_w im) of entries (J, I)
   if (T.nr > 1 && T.nz > 1) {
@@ -790,6 +797,11 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
       if (a.diagonal_term && I == J) kre += (fabs(f.zc - a.free_surface) < kLit1em8) ? 1.0 : 0.5;
       S[(size_t)I + (size_t)a.lds * J] = make_double2(sre, sim);
       K[(size_t)I + (size_t)a.ldk * J] = make_double2(kre, kim);
+      if (Wre) {
+        const size_t w = (size_t)I + (size_t)kb.w_ld * J;
+        Wre[w] = (float)kre;
+        Wre[kb.w_im + w] = (float)kim;
+      }
       nan_seen |= isnan(sre) || isnan(sim) || isnan(kre) || isnan(kim);
     }
     if (!diag_tile) {
@@ -808,6 +820,11 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
           const double kre = kMinusOneOverFourPi * (rk.y + m.z), kim = kMinusOneOverFourPi * m.w;
           S[(size_t)J + (size_t)a.lds * Ic] = make_double2(sre, sim);
           K[(size_t)J + (size_t)a.ldk * Ic] = make_double2(kre, kim);
+          if (Wre) {
+            const size_t w = (size_t)J + (size_t)kb.w_ld * Ic;
+            Wre[w] = (float)kre;
+            Wre[kb.w_im + w] = (float)kim;
+          }
           nan_seen |= isnan(sre) || isnan(sim) || isnan(kre) || isnan(kim);
         }
       }
@@ -1160,9 +1177,13 @@ namespace bem {
 namespace {
 // Shared by the single- and multi-wavenumber entry points: checks, then one
 // launch per group of up to kSymBatch wavenumbers (grid z = wavenumber).
+// planes (optional): float32 copy of K into planes[0 .. nk) (real plane, the
+// imaginary plane planes_im floats further, leading dimension planes_ld,
+// planes_stride floats between wavenumbers).
 int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev, int64_t ld, const double* ks,
                           int nk, int64_t s_stride, int64_t k_stride, void* stream, const char* who,
-                          bool general = false, bool inplace = false) {
+                          bool general = false, bool inplace = false, float* planes = nullptr,
+                          int64_t planes_ld = 0, int64_t planes_stride = 0, int64_t planes_im = 0) {
   char msg[200];
   if (!args || !rankine_dev || !ks || nk <= 0) {
     std::snprintf(msg, sizeof(msg), "%s: null pointer or no wavenumber", who);
@@ -1230,6 +1251,10 @@ int wave_symmetric_launch(const bem_assembly_args* args, const void* rankine_dev
     for (int i = 0; i < cnt; ++i) kb.k[i] = ks[k0 + i];
     kb.s_stride = s_stride;
     kb.k_stride = k_stride;
+    kb.w = planes ? planes + (size_t)k0 * planes_stride : nullptr;
+    kb.w_ld = planes_ld;
+    kb.w_stride = planes_stride;
+    kb.w_im = planes_im;
     bem_assembly_args ak = a;
     ak.S_dev = reinterpret_cast<double2*>(a.S_dev) + (size_t)k0 * s_stride;
     ak.K_dev = reinterpret_cast<double2*>(a.K_dev) + (size_t)k0 * k_stride;
@@ -1276,6 +1301,24 @@ extern "C" int bem_assemble_wave_symmetric_batched(const bem_assembly_args* args
   using namespace bem;
   return wave_symmetric_launch(args, rankine_dev, ld, wavenumbers_host, nk, s_stride, k_stride, stream,
                                "bem_assemble_wave_symmetric_batched");
+}
+
+extern "C" int bem_assemble_wave_symmetric_batched_lu(const bem_assembly_args* args, const void* rankine_dev,
+                                                      int64_t ld, const double* wavenumbers_host, int nk,
+                                                      int64_t s_stride, int64_t k_stride, void* lu_work_dev,
+                                                      int npad, int first, void* stream) {
+  using namespace bem;
+  if (!args || !lu_work_dev || npad < args->n || npad % 128 || first < 0)
+    return set_error(BEM_ERR_INVALID_ARGUMENT,
+                     "bem_assemble_wave_symmetric_batched_lu: bad workspace arguments (npad a multiple of 128, "
+                     ">= n)");
+  float* re = nullptr;
+  int64_t pld = 0, pstride = 0, pim = 0;
+  int st = clu_planes(lu_work_dev, npad, &re, &pld, &pstride, &pim);
+  if (st) return st;
+  return wave_symmetric_launch(args, rankine_dev, ld, wavenumbers_host, nk, s_stride, k_stride, stream,
+                               "bem_assemble_wave_symmetric_batched_lu", false, false,
+                               re + (size_t)first * pstride, pld, pstride, pim);
 }
 
 extern "C" int bem_assemble_wave_cached(const bem_assembly_args* args, const void* rankine_dev, int64_t ld,

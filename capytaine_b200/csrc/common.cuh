@@ -88,6 +88,11 @@ int zlu_solve_enqueue(const void* A_dev, int n, int64_t lda, int64_t stride, int
                       cudaStream_t s, const int* skip, long long spin_limit, const int* mskip = nullptr);
 int* zlu_done_flag(void* work_dev, int n, int batch);
 
+// Float32 planes of the mixed LU's workspace (lu_mixed.cu): matrix b's real
+// plane at *re + b * stride, its imaginary plane im floats further, column-
+// major with leading dimension ld (= npad).
+int clu_planes(void* work_dev, int npad, float** re, int64_t* ld, int64_t* stride, int64_t* im);
+
 // Packed copy of a complex update's result (tc_gemm.cu), written by its
 // epilogue in the A operand layout of the next block step of the mixed LU:
 //   kPackRows: row i -> [Re C(i, 0..127) | Im C(i, 0..127)]  (n = 128)

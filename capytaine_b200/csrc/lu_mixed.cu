@@ -798,9 +798,36 @@ extern "C" int64_t bem_clu_workspace_bytes(int npad, int batch) {
 namespace bem {
 namespace {
 int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch, const int* act,
-                    int* piv_dev, int* info_dev, void* work_dev, int* err_dev, void* stream);
+                    int* piv_dev, int* info_dev, void* work_dev, int* err_dev, void* stream,
+                    bool planes_ready = false);
+
+// Identity on the padding of planes that already hold K (rows or columns n ..
+// npad - 1), the counterpart of convert_pad_kernel when the assembly wrote
+// the float32 planes itself.
+__global__ void pad_planes_kernel(int n, int npad, Planes W) {
+  const int b = blockIdx.z, c = blockIdx.y;
+  for (int r = (c < n ? n : 0) + blockIdx.x * blockDim.x + threadIdx.x; r < npad; r += gridDim.x * blockDim.x)
+    stp(W, b, r, c, make_float2(r == c ? 1.0f : 0.0f, 0.0f));
+}
+}  // namespace
+
+int clu_planes(void* work_dev, int npad, float** re, int64_t* ld, int64_t* stride, int64_t* im) {
+  if (!work_dev || npad <= 0 || npad % kB || (reinterpret_cast<uintptr_t>(work_dev) & 1023))
+    return set_error(BEM_ERR_INVALID_ARGUMENT, "mixed LU workspace: npad a multiple of 128, 1024-byte alignment");
+  // the planes come first in the workspace (carve)
+  *re = reinterpret_cast<float*>(work_dev);
+  *ld = npad;
+  *stride = 2 * (int64_t)npad * npad;
+  *im = (int64_t)npad * npad;
+  return BEM_OK;
 }
 }  // namespace bem
+
+extern "C" int bem_clu_factor_planes(int n, int npad, int batch, int* piv_dev, int* info_dev, void* work_dev,
+                                     int* err_dev, void* stream) {
+  return clu_factor_impl(nullptr, n, (int64_t)n * n, n, npad, batch, nullptr, piv_dev, info_dev, work_dev, err_dev,
+                         stream, true);
+}
 
 extern "C" int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
                               int* piv_dev, int* info_dev, void* work_dev, int* err_dev, void* stream) {
@@ -822,9 +849,9 @@ extern "C" int bem_clu_factor_grouped(const void* K_dev, int64_t ldk, int64_t st
 namespace bem {
 namespace {
 int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch, const int* act,
-                    int* piv_dev, int* info_dev, void* work_dev, int* err_dev, void* stream) {
-  if (!K_dev || !piv_dev || !info_dev || !work_dev || !err_dev || n <= 0 || npad < n || npad % kB || batch <= 0 ||
-      ldk < n)
+                    int* piv_dev, int* info_dev, void* work_dev, int* err_dev, void* stream, bool planes_ready) {
+  if ((!K_dev && !planes_ready) || !piv_dev || !info_dev || !work_dev || !err_dev || n <= 0 || npad < n ||
+      npad % kB || batch <= 0 || ldk < n)
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_clu_factor: bad arguments (npad multiple of 128, >= n)");
   if (reinterpret_cast<uintptr_t>(work_dev) & 1023)
     return set_error(BEM_ERR_INVALID_ARGUMENT, "bem_clu_factor: workspace must be 1024-byte aligned");
@@ -836,8 +863,13 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   const int nblk = npad / kB;
   int launches = 0;
   BEM_CUDA_CHECK(cudaMemsetAsync(info_dev, 0, sizeof(int) * batch, s));
-  convert_pad_kernel<<<dim3(ceil_div(npad, 256), npad, batch), 256, 0, s>>>((const double2*)K_dev, ldk, strideK, n,
-                                                                           npad, W);
+  if (planes_ready) {  // K is in the planes already: the identity padding only
+    if (npad > n)
+      pad_planes_kernel<<<dim3(ceil_div(npad, 256), npad, batch), 256, 0, s>>>(n, npad, W);
+  } else {
+    convert_pad_kernel<<<dim3(ceil_div(npad, 256), npad, batch), 256, 0, s>>>((const double2*)K_dev, ldk, strideK,
+                                                                             n, npad, W);
+  }
   ++launches;
   const size_t abuf = (size_t)batch * npad * 2 * kB, bbuf = (size_t)batch * 2 * npad * 2 * kB;
   // The updates and the panel product give each CTA an even share of up to

@@ -161,6 +161,7 @@ class _Factors:
     def __init__(self, n, batch, device, precision, alloc=None, lu=True):
         import torch
         self.n, self.batch, self.precision = n, batch, precision
+        self.planes_ready = False  # K already in the mixed LU's float32 planes (assemble_stage)
         lib = _lib.load()
         mk = _allocator(device, alloc)
         self.S = mk((batch, n * n), torch.complex128)
@@ -507,7 +508,7 @@ class B200Engine:
                 ev[0].record()
             ws.r.flags.zero_()
             self.assemble_stage(ws.f, mesh, wavenumbers(om, water_depth, g), nan_flag=ws.r.nan,
-                                water_depth=water_depth)
+                                water_depth=water_depth, planes=True)
             if ev:
                 ev[1].record()
             self.factor_stage(ws.f, nb, ws.r.err)
@@ -594,29 +595,39 @@ class B200Engine:
         return self.precision == "fp64" and self._linear_solver == "gmres"
 
     def assemble_stage(self, f: "_Factors", mesh, ks, *, nan_flag=None, reuse_rankine=True, first=0, lds=None,
-                       water_depth=np.inf):
+                       water_depth=np.inf, planes=False):
         """S and K of the mesh with itself at the wavenumbers ks into
         f[first:first+len(ks)] (one launch for all of them on the Rankine-reuse
         path when every wavenumber is finite and > 0; one per wavenumber in
-        finite depth)."""
+        finite depth).  planes (mixed engine, f's matrices are the mesh's own,
+        nothing padded afterwards): K also goes rounded to float32 into the LU
+        workspace where the sweep kernel can write it, and f.planes_ready says
+        whether every matrix of the batch got there (factor_stage then skips
+        the conversion pass)."""
         gf = self.green_function
         n = mesh.nb_faces
         lds = n if lds is None else lds
         ks = [float(k) for k in ks]
         adjoint = self.method == "indirect"  # K (adjoint double layer) or D
         precs = [self._wave_precision(mesh, k, water_depth) for k in ks]
+        planes = planes and self.precision == "mixed" and first == 0 and f.n == n
+        f.planes_ready = False
         if len(ks) > 1 and all(0.0 < k < np.inf for k in ks):
             # one sweep call per run of consecutive wavenumbers of the same precision
             i = 0
+            written = True
             while i < len(ks):
                 j = i
                 while j < len(ks) and precs[j] == precs[i]:
                     j += 1
-                gf.assemble_into(mesh, mesh, f.S[first + i], f.K[first + i], wavenumber=ks[i], lds=lds,
-                                 ldk=f.ldk, nan_flag=nan_flag, precision=precs[i], reuse_rankine=reuse_rankine,
-                                 sweep=(ks[i:j], f.S.shape[1], f.K.shape[1]), adjoint_double_layer=adjoint,
-                                 water_depth=water_depth)
+                lu_planes = (f.lu_work_ptr, f.npad, first + i) if planes else None
+                done = gf.assemble_into(mesh, mesh, f.S[first + i], f.K[first + i], wavenumber=ks[i], lds=lds,
+                                        ldk=f.ldk, nan_flag=nan_flag, precision=precs[i],
+                                        reuse_rankine=reuse_rankine, sweep=(ks[i:j], f.S.shape[1], f.K.shape[1]),
+                                        adjoint_double_layer=adjoint, water_depth=water_depth, lu_planes=lu_planes)
+                written = written and bool(done)
                 i = j
+            f.planes_ready = planes and written
             return
         for b, k in enumerate(ks):
             gf.assemble_into(mesh, mesh, f.S[first + b], f.K[first + b], wavenumber=k, lds=lds, ldk=f.ldk,
@@ -652,6 +663,10 @@ class B200Engine:
             act = (ctypes.c_int32 * nb)(*[int(min(a, npad)) for a in active])
             _lib.check(lib.bem_clu_factor_grouped(_vp(f.K), n, n * n, n, npad, nb, act, _vp(f.piv), _vp(f.info),
                                                   _vp(f.lu_work_ptr), _vp(err), stream))
+        elif self.precision == "mixed" and getattr(f, "planes_ready", False):
+            # the assembly wrote K into the workspace's float32 planes
+            _lib.check(lib.bem_clu_factor_planes(n, npad, nb, _vp(f.piv), _vp(f.info), _vp(f.lu_work_ptr),
+                                                 _vp(err), stream))
         elif self.precision == "mixed":
             _lib.check(lib.bem_clu_factor(_vp(f.K), n, n * n, n, npad, nb, _vp(f.piv), _vp(f.info),
                                           _vp(f.lu_work_ptr), _vp(err), stream))
@@ -662,6 +677,7 @@ class B200Engine:
             _lib.check(lib.bem_zpad_identity(_vp(f.LU), npad, npad * npad, nb, n, npad, stream))
             _lib.check(lib.bem_zlu_factor(_vp(f.LU), npad, npad, npad * npad, nb, _vp(f.piv), _vp(f.info),
                                           _vp(f.lu_work), stream))
+        f.planes_ready = False  # consumed
 
     def solve_stage(self, f: "_Factors", r: "_Rhs", body, om, heads, *, rho=1000.0, g=9.81, stats=None,
                     events=None, water_depth=np.inf):

@@ -348,7 +348,7 @@ class Delhommeau:
     def assemble_into(self, mesh1, mesh2, S, K, *, free_surface=0.0, water_depth=np.inf, wavenumber=1.0,
                       adjoint_double_layer=True, early_dot_product=True, diagonal_term_in_double_layer=True,
                       lds=None, ldk=None, k_plane_stride=None, precision=None, stream=None, nan_flag=None,
-                      reuse_rankine=True, sweep=None):
+                      reuse_rankine=True, sweep=None, lu_planes=None):
         """Write S and K into caller-owned device buffers (column-major with
         leading dimensions lds/ldk) through ``bem_assemble``.  For a mesh with
         itself the wavenumber-independent Rankine part is kept and reused
@@ -356,7 +356,9 @@ class Delhommeau:
         s_stride, k_stride): S and K of every wavenumber (finite, > 0; the
         variant is chosen with the first), the outputs of wavenumber i at
         S + i * s_stride and K + i * k_stride elements, in one launch per 64
-        wavenumbers on the Rankine-reuse path."""
+        wavenumbers on the Rankine-reuse path.  lu_planes = (workspace pointer,
+        npad, first matrix): on that path K is also written rounded to float32
+        into the planes of a mixed-LU workspace; returns True when it was."""
         import torch
         if free_surface == np.inf and water_depth != np.inf:
             raise ValueError("When setting free_surface=inf, the water depth should also be infinite")
@@ -433,13 +435,19 @@ class Delhommeau:
             if sweep is not None:
                 ks, s_stride, k_stride = sweep
                 kh = np.ascontiguousarray(np.asarray(ks, dtype=np.float64))
+                if lu_planes is not None:
+                    work, npad, first = lu_planes
+                    _lib.check(lib.bem_assemble_wave_symmetric_batched_lu(
+                        a, rank.data_ptr(), n, kh.ctypes.data_as(_lib.c_void_p), len(kh), int(s_stride),
+                        int(k_stride), _lib.c_void_p(int(work)), int(npad), int(first), _lib.stream_ptr(stream)))
+                    return True
                 _lib.check(lib.bem_assemble_wave_symmetric_batched(a, rank.data_ptr(), n,
                                                                    kh.ctypes.data_as(_lib.c_void_p), len(kh),
                                                                    int(s_stride), int(k_stride),
                                                                    _lib.stream_ptr(stream)))
-                return
+                return False
             _lib.check(lib.bem_assemble_wave_symmetric(a, rank.data_ptr(), n, _lib.stream_ptr(stream)))
-            return
+            return False
         if (self.symmetric_assembly and same_mesh and dm2.collocation_at_quadrature and all_wave
                 and sing in ("low_freq", "high_freq") and prec == "fp64" and dtype == _lib.BEM_DTYPE_C128
                 and early_dot_product and (ldk if ldk is not None else n) >= n):

@@ -174,6 +174,16 @@ int bem_assemble_wave_symmetric_batched(const bem_assembly_args* args, const voi
                                         const double* wavenumbers_host, int nk, int64_t s_stride, int64_t k_stride,
                                         void* stream);
 
+/* bem_assemble_wave_symmetric_batched that also writes K rounded to float32
+ * into the planes of a mixed-LU workspace (lu_work_dev of
+ * bem_clu_workspace_bytes(npad, ...), matrices first .. first + nk - 1), the
+ * way bem_clu_factor converts it; bem_clu_factor_planes then factors them
+ * without reading K again.  K and S are written as by the batched call.  No
+ * counterpart in the reference (matrices.f90:28-432 writes complex128 only). */
+int bem_assemble_wave_symmetric_batched_lu(const bem_assembly_args* args, const void* rankine_dev, int64_t ld,
+                                           const double* wavenumbers_host, int nk, int64_t s_stride,
+                                           int64_t k_stride, void* lu_work_dev, int npad, int first, void* stream);
+
 /* S and K of a mesh with itself at one wavenumber (finite, > 0) with no cached
  * Rankine part: bem_assemble_rankine_part into K_dev, then the wave term once
  * per unordered pair of faces added in place.  Same requirements as
@@ -343,6 +353,13 @@ int bem_clu_factor(const void* K_dev, int64_t ldk, int64_t strideK, int n, int n
 int bem_clu_factor_grouped(const void* K_dev, int64_t ldk, int64_t strideK, int n, int npad, int batch,
                            const int* active_host, int* piv_dev, int* info_dev, void* work_dev, int* err_dev,
                            void* stream);
+
+/* bem_clu_factor of matrices already in the workspace's float32 planes
+ * (written by bem_assemble_wave_symmetric_batched_lu): the identity padding
+ * beyond n, then the same factorisation, bit for bit.  Replaces the same
+ * zgetrf as bem_clu_factor (tools/block_circulant_matrices.py:374-385). */
+int bem_clu_factor_planes(int n, int npad, int batch, int* piv_dev, int* info_dev, void* work_dev, int* err_dev,
+                          void* stream);
 
 /* B <- (LU)^{-1} B with the float32 block factors; B complex128 (npad x nrhs, ldb); piv_dev reserved. */
 int bem_clu_solve(void* work_dev, int npad, int batch, const int* piv_dev, void* B_dev, int64_t ldb,

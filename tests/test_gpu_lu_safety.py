@@ -235,3 +235,35 @@ def test_grouped_factorisation_equals_the_padded_one():
     bad = (ctypes.c_int32 * batch)(128, 100, 128, 128)  # not a multiple of 128
     assert lib.bem_clu_factor_grouped(_vp(K), npad, npad * npad, npad, npad, batch, bad, _vp(piv), _vp(info),
                                       _vp(wptr), _vp(err), s) == _lib.BEM_ERR_INVALID_ARGUMENT
+
+
+def test_sweep_assembled_into_the_lu_planes_gives_the_same_factors(default_oracle_gf, tmp_path):
+    """The frequency-sweep assembly that also writes K rounded to float32
+    into the mixed LU's workspace (bem_assemble_wave_symmetric_batched_lu),
+    factored by bem_clu_factor_planes, gives S, K and the factors of the
+    plain sweep assembly followed by bem_clu_factor's conversion, bit for bit
+    (npad > n, so the identity padding is written too)."""
+    import torch
+    from capytaine_b200.engine import B200Engine, _Factors
+    from capytaine_b200.meshes import mesh_sphere
+    from test_gpu_mixed import _shared_table_gf
+    eng = B200Engine(green_function=_shared_table_gf(default_oracle_gf, tmp_path), precision="mixed")
+    mesh = mesh_sphere(radius=1.0, resolution=(10, 30)).immersed_part()
+    n = mesh.nb_faces
+    assert n % 128 != 0
+    ks = [0.3, 0.8, 1.7]
+    out = []
+    for planes in (True, False):
+        f = _Factors(n, len(ks), "cuda", "mixed")
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        f.lu_work.zero_()
+        eng.assemble_stage(f, mesh, ks, planes=planes)
+        assert f.planes_ready == planes
+        eng.factor_stage(f, len(ks), err)
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0 and not f.planes_ready
+        off = f.lu_work_ptr - f.lu_work.data_ptr()
+        w_bytes = len(ks) * 2 * f.npad * f.npad * 4
+        out.append((f.S.clone(), f.K.clone(), f.lu_work[off:off + w_bytes].clone(), f.info.clone()))
+    for a, b in zip(out[0], out[1]):
+        assert torch.equal(a, b)
