@@ -804,9 +804,12 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
 // Identity on the padding of planes that already hold K (rows or columns n ..
 // npad - 1), the counterpart of convert_pad_kernel when the assembly wrote
 // the float32 planes itself.
+// One warp per column (blockDim 32 x 8): columns below n only have their
+// rows n .. npad - 1 written, the columns from n on all of theirs.
 __global__ void pad_planes_kernel(int n, int npad, Planes W) {
-  const int b = blockIdx.z, c = blockIdx.y;
-  for (int r = (c < n ? n : 0) + blockIdx.x * blockDim.x + threadIdx.x; r < npad; r += gridDim.x * blockDim.x)
+  const int b = blockIdx.y, c = blockIdx.x * blockDim.y + threadIdx.y;
+  if (c >= npad) return;
+  for (int r = (c < n ? n : 0) + threadIdx.x; r < npad; r += blockDim.x)
     stp(W, b, r, c, make_float2(r == c ? 1.0f : 0.0f, 0.0f));
 }
 }  // namespace
@@ -865,7 +868,7 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   BEM_CUDA_CHECK(cudaMemsetAsync(info_dev, 0, sizeof(int) * batch, s));
   if (planes_ready) {  // K is in the planes already: the identity padding only
     if (npad > n)
-      pad_planes_kernel<<<dim3(ceil_div(npad, 256), npad, batch), 256, 0, s>>>(n, npad, W);
+      pad_planes_kernel<<<dim3(ceil_div(npad, 8), batch), dim3(32, 8), 0, s>>>(n, npad, W);
   } else {
     convert_pad_kernel<<<dim3(ceil_div(npad, 256), npad, batch), 256, 0, s>>>((const double2*)K_dev, ldk, strideK,
                                                                              n, npad, W);
