@@ -99,6 +99,8 @@ __global__ void convert_pad_kernel(const double2* __restrict__ K, int64_t ldk, i
 // column p_c).
 constexpr int kGjWarps = 8;
 constexpr int kGjSlots = kB / kGjWarps;  // columns per warp
+constexpr int kGjLd = kB + 1;            // column stride of the staged inverse (fewer bank conflicts)
+constexpr int kGjOutBytes = kB * kGjLd * (int)sizeof(float2);  // dynamic shared memory of the inverse
 
 // acc - a b in two fused multiply-adds per component.
 __device__ __forceinline__ float2 cfms(float2 acc, float2 a, float2 b) {
@@ -275,42 +277,58 @@ __global__ void __launch_bounds__(32 * kGjWarps, 1) clu_gj_kernel(Planes W, int 
   __syncthreads();
   if (tid < kB) sh.jinv[sh.piv_row[tid]] = tid;
   __syncthreads();
-  // A_kk^{-1}(jinv[r], piv_row[c]) = a(r, c) / pivot, also packed as the B
-  // operand of the split-TF32 product L21 = A21 A_kk^{-1} (three K-blocks of
-  // 256: hi, hi, lo; see clu_pack_kernel for the A side):
-  // row t: [Re X(:, t) | -Im X(:, t)] per block, row 128 + t: [Im X(:, t) | Re X(:, t)]
-  float2* out = inv + ((size_t)b * nblk + kk / kB) * kB * kB;
-  float* bo = binv + (size_t)b * (2 * kB) * kSplitK;
-  float* ao = ainv + (size_t)b * kB * 2 * kB;  // row r: [Re A_kk^{-1}(r, :) | Im A_kk^{-1}(r, :)]
+  // A_kk^{-1}(jinv[r], piv_row[c]) = a(r, c) / pivot: staged in shared memory
+  // at its place (column-major, column stride kGjLd), so that the three
+  // outputs below are written with coalesced stores (the permuted rows would
+  // scatter every store otherwise).
+  extern __shared__ float2 gj_out[];  // kB columns of kGjLd
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int r = lane + 32 * i;
     const int row = sh.jinv[r];
     const float2 sc = sh.rowscale[r];
 #pragma unroll
-    for (int m = 0; m < kGjSlots; ++m) {
-      const int col = sh.piv_row[w + kGjWarps * m];
-      const float2 v = fmul(a[i][m], sc);
-      out[row + (size_t)col * kB] = v;
-      ao[(size_t)row * 2 * kB + col] = v.x;
-      ao[(size_t)row * 2 * kB + kB + col] = v.y;
-      const float2 hi = make_float2(tf32_hi(v.x), tf32_hi(v.y));
-      const float2 lo = make_float2(v.x - hi.x, v.y - hi.y);
-      float* rr = bo + (size_t)col * kSplitK + row;
-      float* ri = bo + (size_t)(kB + col) * kSplitK + row;
-      rr[0] = hi.x;
-      rr[kB] = -hi.y;
-      rr[2 * kB] = hi.x;
-      rr[3 * kB] = -hi.y;
-      rr[4 * kB] = lo.x;
-      rr[5 * kB] = -lo.y;
-      ri[0] = hi.y;
-      ri[kB] = hi.x;
-      ri[2 * kB] = hi.y;
-      ri[3 * kB] = hi.x;
-      ri[4 * kB] = lo.y;
-      ri[5 * kB] = lo.x;
-    }
+    for (int m = 0; m < kGjSlots; ++m)
+      gj_out[(size_t)sh.piv_row[w + kGjWarps * m] * kGjLd + row] = fmul(a[i][m], sc);
+  }
+  __syncthreads();
+  // inv: column-major 128 x 128
+  float2* out = inv + ((size_t)b * nblk + kk / kB) * kB * kB;
+  for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
+    const int row = idx & (kB - 1), col = idx >> 7;
+    out[idx] = gj_out[col * kGjLd + row];
+  }
+  // the A operand of U' = A_kk^{-1} A12: row r = [Re A_kk^{-1}(r, :) | Im A_kk^{-1}(r, :)]
+  float* ao = ainv + (size_t)b * kB * 2 * kB;
+  for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
+    const int col = idx & (kB - 1), row = idx >> 7;
+    const float2 v = gj_out[col * kGjLd + row];
+    ao[(size_t)row * 2 * kB + col] = v.x;
+    ao[(size_t)row * 2 * kB + kB + col] = v.y;
+  }
+  // the B operand of the split-TF32 product L21 = A21 A_kk^{-1} (three
+  // K-blocks of 256: hi, hi, lo; see clu_pack_kernel for the A side):
+  // row t: [Re X(:, t) | -Im X(:, t)] per block, row 128 + t: [Im X(:, t) | Re X(:, t)]
+  float* bo = binv + (size_t)b * (2 * kB) * kSplitK;
+  for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
+    const int row = idx & (kB - 1), col = idx >> 7;
+    const float2 v = gj_out[col * kGjLd + row];
+    const float2 hi = make_float2(tf32_hi(v.x), tf32_hi(v.y));
+    const float2 lo = make_float2(v.x - hi.x, v.y - hi.y);
+    float* rr = bo + (size_t)col * kSplitK + row;
+    float* ri = bo + (size_t)(kB + col) * kSplitK + row;
+    rr[0] = hi.x;
+    rr[kB] = -hi.y;
+    rr[2 * kB] = hi.x;
+    rr[3 * kB] = -hi.y;
+    rr[4 * kB] = lo.x;
+    rr[5 * kB] = -lo.y;
+    ri[0] = hi.y;
+    ri[kB] = hi.x;
+    ri[2 * kB] = hi.y;
+    ri[3 * kB] = hi.x;
+    ri[4 * kB] = lo.y;
+    ri[5 * kB] = lo.x;
   }
 }
 
@@ -679,6 +697,7 @@ __global__ void refine_check_kernel(const double* __restrict__ bn, const double*
 bool g_mixed_configured = false;
 int configure_mixed() {
   if (g_mixed_configured) return BEM_OK;
+  BEM_CUDA_CHECK(cudaFuncSetAttribute(clu_gj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGjOutBytes));
   BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<8, kRingDeep>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, trsm_smem_bytes(8, kRingDeep)));
   BEM_CUDA_CHECK(cudaFuncSetAttribute(ctrsm_persistent_kernel<16, kRingDeep>,
@@ -889,7 +908,7 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   // block's parity).
   auto inverse = [&](int kk, cudaStream_t on) {
     TimedLaunch tl(kKCluGj, on);
-    clu_gj_kernel<<<batch, 32 * kGjWarps, 0, on>>>(W, kk, info_dev, w.inv, nblk, w.binv,
+    clu_gj_kernel<<<batch, 32 * kGjWarps, kGjOutBytes, on>>>(W, kk, info_dev, w.inv, nblk, w.binv,
                                          w.ainv + ((kk / kB) & 1) * ainv_buf);
     ++launches;
   };
