@@ -102,13 +102,15 @@ enum PackMode { kPackNone = 0, kPackRows = 1 };
 // (store = 1) on the tensor cores from packed operands; an optional second
 // operand pair adds K' depth in the same pass over C; limit_host: per-matrix
 // active sizes (grouped launches); pack: a packed copy of the result; lshape:
-// only the first tile row and column of the square block, corner excluded.
+// only the first tile row and column of the square block, corner excluded;
+// reserve_sms: SMs that a kernel beside this one holds (left out of the
+// launch's width).
 int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float* Bop, int64_t b_rows, int b_row0,
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store = 0, const float* Aop1 = nullptr,
                       const float* Bop1 = nullptr, int run = 0, long long wait_limit = 0,
                       const int* limit_host = nullptr, float* pack = nullptr, int pack_mode = kPackNone,
-                      int64_t pack_stride = 0, bool lshape = false);
+                      int64_t pack_stride = 0, bool lshape = false, int reserve_sms = 0);
 
 }  // namespace bem
 

@@ -936,11 +936,12 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   // C rows r0.. (m), complex columns c0.. (nc) -= L21 U12 of the block step whose
   // packed operands are in buffer buf, and of a second step (buffer buf2 >= 0)
   // in the same pass over C (depth 256); optionally a packed copy of the result.
-  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2, int run, bool lshape = false) -> int {
+  auto update = [&](int buf, int r0, int c0, int m, int nc, int buf2, int run, bool lshape = false,
+                    int reserve = 0) -> int {
     if (m <= 0 || nc <= 0) return BEM_OK;
     return cgemm_tf32_update(Aop[buf], npad, r0, Bop[buf], 2 * (int64_t)npad, 2 * c0, 2 * kB, W.re, W.im, npad,
                              W.stride, r0, c0, m, nc, batch, err_dev, s, 0, buf2 >= 0 ? Aop[buf2] : nullptr,
-                             buf2 >= 0 ? Bop[buf2] : nullptr, run, 0, act, nullptr, kPackNone, 0, lshape);
+                             buf2 >= 0 ? Bop[buf2] : nullptr, run, 0, act, nullptr, kPackNone, 0, lshape, reserve);
   };
   Lookahead* la = nullptr;
   if ((st = lookahead_for(s, &la))) return st;
@@ -992,7 +993,8 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
     // the SMs and HBM with the big update.)
     const bool big_step = (step & 1) && rest > 0;
     if (rest > 0) {
-      if ((st = update(cur, kn, kn, rest + kB, rest + kB, pend, 0, true))) return st;
+      // the inverse of block kn holds one SM per matrix meanwhile
+      if ((st = update(cur, kn, kn, rest + kB, rest + kB, pend, 0, true, batch))) return st;
       TimedLaunch tl(kKCluPanel, s);
       clu_pack_kernel<<<dim3(rest / kPT + rest / 32, batch), 256, 0, s>>>(W, npad, kn, rest / kPT, kn + kB, kn,
                                                                          Bop[nxt], w.a3);

@@ -486,7 +486,7 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
                       int kp, float* Cr, float* Ci, int64_t ldc, int64_t c_stride, int c_row0, int c_col0, int m,
                       int n, int batch, int* err, cudaStream_t stream, int store, const float* Aop1,
                       const float* Bop1, int run, long long wait_limit, const int* limit_host, float* pack,
-                      int pack_mode, int64_t pack_stride, bool lshape) {
+                      int pack_mode, int64_t pack_stride, bool lshape, int reserve_sms) {
   if (m <= 0 || n <= 0) return BEM_OK;
   if (lshape && (m != n || m <= kTM || pack_mode != kPackNone))
     return set_error(BEM_ERR_INVALID_ARGUMENT, "cgemm_tf32_update: an L-shaped update needs a square block of "
@@ -569,11 +569,14 @@ int cgemm_tf32_update(const float* Aop, int64_t a_rows, int a_row0, const float*
     if (ntiles == 0) continue;
     p.ntiles = (int)ntiles;
     // groups of up to one CTA per SM, each CTA with about `per` tiles (run, or
-    // up to 32 for the big updates so that other streams get SMs within a run)
+    // up to 32 for the big updates so that other streams get SMs within a run);
+    // reserve_sms SMs held by a kernel running beside this one are left out of
+    // the width, so that a group never waits for them with its share of tiles
     const long long per = run > 0 ? run : 32;
-    const long long waves = (ntiles + (long long)sms * per - 1) / ((long long)sms * per);
-    const long long width = std::min<long long>(sms, (ntiles + waves * (run > 0 ? run : 1) - 1) /
-                                                         (waves * (run > 0 ? run : 1)));
+    const long long avail = std::max(1, sms - std::min(std::max(0, reserve_sms), sms / 2));
+    const long long waves = (ntiles + avail * per - 1) / (avail * per);
+    const long long width = std::min<long long>(avail, (ntiles + waves * (run > 0 ? run : 1) - 1) /
+                                                           (waves * (run > 0 ? run : 1)));
     const long long ctas = waves * width;
     UpdateArgs q = p;
     q.waves = (int)waves;
@@ -604,5 +607,5 @@ extern "C" int bem_cgemm_tf32_update(const float* Aop_dev, int64_t a_rows, int a
     return bem::set_error(BEM_ERR_INVALID_ARGUMENT, "bem_cgemm_tf32_update: operands must be 16-byte aligned");
   return bem::cgemm_tf32_update(Aop_dev, a_rows, a_row0, Bop_dev, b_rows, b_row0, kp, Cr_dev, Ci_dev, ldc, c_stride,
                                 c_row0, c_col0, m, n, batch, err_dev, (cudaStream_t)stream, 0, nullptr, nullptr, 0, 0,
-                                nullptr, nullptr, bem::kPackNone, 0, false);
+                                nullptr, nullptr, bem::kPackNone, 0, false, 0);
 }
