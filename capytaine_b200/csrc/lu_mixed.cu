@@ -347,43 +347,67 @@ __global__ void __launch_bounds__(256) clu_pack_kernel(Planes W, int npad, int k
   const size_t kp = 2 * kB;
   const int t = blockIdx.x;
   if (t < nrest) {
-    // 128 x 64 of A12: B operand rows of the complex columns c0 .. c0+63
+    // 128 x 64 of A12: B operand rows of the complex columns c0 .. c0+63;
+    // thread (q, cc): rows 4 q .. 4 q + 3 of column cc (16-byte loads and stores)
     const int c0 = kk + kB + t * kPT;
     const int j0 = c0 & ~(kB - 1);
     float* Bb = Bop + (size_t)b * 2 * npad * kp;
-    for (int idx = tid; idx < kB * kPT; idx += blockDim.x) {
-      const int r = idx & (kB - 1), c = idx >> 7;
-      const float2 u = ldp(W, b, kk + r, c0 + c);
+    const float* re = W.re + (size_t)b * W.stride;
+    const float* im = W.im + (size_t)b * W.stride;
+    const int q = tid & 31;
+    for (int c = tid >> 5; c < kPT; c += 8) {
+      const size_t g = (size_t)(c0 + c) * W.ld + kk + 4 * q;
+      const float4 ur = *reinterpret_cast<const float4*>(re + g);
+      const float4 ui = *reinterpret_cast<const float4*>(im + g);
       const int jj = c0 - j0 + c;
-      float* rowR = Bb + (size_t)(2 * j0 + jj) * kp;
-      float* rowI = Bb + (size_t)(2 * j0 + kB + jj) * kp;
-      rowR[r] = u.x;
-      rowR[kB + r] = -u.y;
-      rowI[r] = u.y;
-      rowI[kB + r] = u.x;
+      float4* rowR = reinterpret_cast<float4*>(Bb + (size_t)(2 * j0 + jj) * kp);
+      float4* rowI = reinterpret_cast<float4*>(Bb + (size_t)(2 * j0 + kB + jj) * kp);
+      rowR[q] = ur;
+      rowR[kB / 4 + q] = make_float4(-ui.x, -ui.y, -ui.z, -ui.w);
+      rowI[q] = ui;
+      rowI[kB / 4 + q] = ur;
     }
     return;
   }
   const int r0 = row0 + (t - nrest) * 32;
-  const int lane = tid & 31, w = tid >> 5;
   const float* re = W.re + (size_t)b * W.stride;
   const float* im = W.im + (size_t)b * W.stride;
-  for (int c = w; c < kB; c += 8) {
-    const size_t g = (size_t)(col0 + c) * W.ld + r0 + lane;
-    tre[c][lane] = re[g];
-    tim[c][lane] = im[g];
+  {
+    // thread (q, c): rows 4 q .. 4 q + 3 of column c, 16-byte loads
+    const int q = tid & 7;
+    for (int c = tid >> 3; c < kB; c += 32) {
+      const size_t g = (size_t)(col0 + c) * W.ld + r0 + 4 * q;
+      const float4 vr = *reinterpret_cast<const float4*>(re + g);
+      const float4 vi = *reinterpret_cast<const float4*>(im + g);
+      tre[c][4 * q] = vr.x;
+      tre[c][4 * q + 1] = vr.y;
+      tre[c][4 * q + 2] = vr.z;
+      tre[c][4 * q + 3] = vr.w;
+      tim[c][4 * q] = vi.x;
+      tim[c][4 * q + 1] = vi.y;
+      tim[c][4 * q + 2] = vi.z;
+      tim[c][4 * q + 3] = vi.w;
+    }
   }
   __syncthreads();
-  const int c = tid & (kB - 1);
-  // split rows [hi | lo | hi], each [Re(128) | Im(128)], for the panel product
+  // split rows [hi | lo | hi], each [Re(128) | Im(128)], for the panel
+  // product; thread (q, i0): entries 4 q .. 4 q + 3 of rows i0, i0 + 4, ...
   float* dst = A3 + (size_t)b * npad * kSplitK + (size_t)r0 * kSplitK;
-  for (int i = 0; i < 32; ++i) {
-    const float x = (tid < kB) ? tre[c][i] : tim[c][i];
-    const float hi = tf32_hi(x);
-    float* row = dst + (size_t)i * kSplitK;
-    row[tid] = hi;
-    row[2 * kB + tid] = x - hi;
-    row[4 * kB + tid] = hi;
+  const int q = tid & 63;
+  const float(*src)[33] = q < 32 ? tre : tim;
+  const int cb = 4 * (q & 31);
+  for (int i = tid >> 6; i < 32; i += 4) {
+    float h[4], l[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const float x = src[cb + e][i];
+      h[e] = tf32_hi(x);
+      l[e] = x - h[e];
+    }
+    float4* row = reinterpret_cast<float4*>(dst + (size_t)i * kSplitK);
+    row[q] = make_float4(h[0], h[1], h[2], h[3]);
+    row[2 * kB / 4 + q] = make_float4(l[0], l[1], l[2], l[3]);
+    row[4 * kB / 4 + q] = make_float4(h[0], h[1], h[2], h[3]);
   }
 }
 
