@@ -87,7 +87,7 @@ __global__ void convert_pad_kernel(const double2* __restrict__ K, int64_t ldk, i
 
 // Gauss-Jordan inverse of a diagonal block: 8 warps, thread (warp w, lane l)
 // owns rows l + 32 a (a < 4) and columns w + 8 m (m < 16) of the 128 x 128
-// block in registers; column j = 8 JM + jw is slot JM of warp jw.
+// block in registers; column j = 8 m + w is slot m of warp w.
 // Pivoting is implicit: rows never move.  Step j picks the pivot of column j
 // among the rows not yet used as pivot rows (row p_j) and eliminates column j
 // from every other row with the unnormalised row p_j:
@@ -97,10 +97,19 @@ __global__ void convert_pad_kernel(const double2* __restrict__ K, int64_t ldk, i
 //   A^{-1}(j', p_c) = a(p_j', c) / pivot_j'
 // (row p_j' holds the j'-th pivot row, the slot of column c the inverse's
 // column p_c).
-constexpr int kGjWarps = 8;
+#ifndef BEM_GJ_WARPS
+#define BEM_GJ_WARPS 8
+#endif
+#ifndef BEM_GJ_DEPTH
+#define BEM_GJ_DEPTH 4
+#endif
+constexpr int kGjWarps = BEM_GJ_WARPS;
 constexpr int kGjSlots = kB / kGjWarps;  // columns per warp
+constexpr int kGjDepth = BEM_GJ_DEPTH;   // pivot columns published ahead of the slowest warp
+static_assert(kGjSlots <= 16 && kGjWarps * kGjSlots == kB, "a warp holds at most 16 columns of the block");
 constexpr int kGjLd = kB + 1;            // column stride of the staged inverse (fewer bank conflicts)
 constexpr int kGjOutBytes = kB * kGjLd * (int)sizeof(float2);  // dynamic shared memory of the inverse
+constexpr long long kGjWaitLimit = 1ll << 22;  // polls of a bounded wait (about a second)
 
 // acc - a b in two fused multiply-adds per component.
 __device__ __forceinline__ float2 cfms(float2 acc, float2 a, float2 b) {
@@ -111,30 +120,82 @@ __device__ __forceinline__ float2 cfms(float2 acc, float2 a, float2 b) {
   return acc;
 }
 
+__device__ __forceinline__ uint32_t gj_smem(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void gj_bar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(gj_smem(bar)), "r"(count));
+}
+__device__ __forceinline__ void gj_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(gj_smem(bar)) : "memory");
+}
+__device__ __forceinline__ bool gj_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(gj_smem(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 struct GjShared {
-  float2 colbuf[2][kB];             // pivot column of the step, by row (double buffered)
+  // full[s]: the column of buffer s is published (32 arrivals, the owner's
+  // lanes); empty[s]: every warp has read it (8 arrivals, one per warp).
+  uint64_t full[kGjDepth];
+  uint64_t empty[kGjDepth];
+  float2 colbuf[kGjDepth][kB];      // pivot column of step j in buffer j % kGjDepth, by row
   float2 xbuf[kGjWarps][kGjSlots];  // per warp: its entries of the pivot row
   float2 rowscale[kB];              // 1 / pivot of the step whose pivot row is this row
   int piv_row[kB];                  // pivot row of each step
   int jinv[kB];                     // step of each pivot row
   unsigned used[kB / 32];           // rows already used as pivot rows
-  int s_piv[2];
+  int s_piv[kGjDepth];              // pivot row of the column in each buffer
+  int abort;                        // a wait ran out: every warp leaves
 };
 
-// Pivot of column j (register slot M of this warp) among the unused rows:
-// publishes the column to colbuf[j & 1] and the pivot row to s_piv[j & 1],
-// marks the row used, then sets the column in registers to the unit vector of
-// the pivot row (the step's update turns it into the inverse's column); flags
-// an exactly zero pivot in info.
+// Bounded wait of a whole warp for phase `parity` of bar (every lane polls,
+// so that every lane acquires the published data); false for the whole warp
+// when a lane reached the limit or another warp gave up (the warp then leaves
+// its loop, with no lane left behind in a warp-synchronous call).
+__device__ __forceinline__ bool gj_wait(uint64_t* bar, uint32_t parity, GjShared& sh, int* __restrict__ err) {
+  bool ok = false, gave_up = false;
+  for (long long it = 0; it < kGjWaitLimit; ++it) {
+    if (gj_try_wait(bar, parity)) {
+      ok = true;
+      break;
+    }
+    if (*(volatile int*)&sh.abort) {
+      gave_up = true;
+      break;
+    }
+  }
+  if (!ok && !gave_up) {
+    *(volatile int*)&sh.abort = 1;
+    atomicExch(err, 1);
+  }
+  return __all_sync(0xffffffffu, ok);
+}
+
+// Column j (register slot M of this warp) after the update of step j - 1
+// (multipliers f, pivot-row entry um; f = 0 for column 0): pivot among the
+// unused rows, the column published to buffer j % kGjDepth with its pivot
+// row; flags an exactly zero pivot in info.  Returns the pivot row (the slot
+// becomes the unit vector of that row once the warp's own update of step
+// j - 1 is done).
 template <int M>
-__device__ __forceinline__ void gj_pivot(float2 (&a)[4][kGjSlots], int j, int kk, int b, int lane, GjShared& sh,
-                                         int* __restrict__ info) {
+__device__ __forceinline__ int gj_publish(const float2 (&a)[4][kGjSlots], const float2 (&f)[4], float2 um, int j,
+                                          int kk, int b, int lane, GjShared& sh, int* __restrict__ info) {
+  constexpr int S = M < kGjSlots ? M : 0;  // M >= kGjSlots: a case the switch never takes
+  float2 t[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) t[i] = cfms(a[i][S], f[i], um);
   float best = -1.0f;
   int bi = kB;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int r = lane + 32 * i;
-    const float av = fabs1(a[i][M]);
+    const float av = fabs1(t[i]);
     if (!((sh.used[i] >> lane) & 1u) && (av > best || (av == best && r < bi))) {
       best = av;
       bi = r;
@@ -154,94 +215,42 @@ __device__ __forceinline__ void gj_pivot(float2 (&a)[4][kGjSlots], int j, int kk
     for (int i = 3; i >= 0; --i)
       if (~sh.used[i]) bi = 32 * i + __ffs(~sh.used[i]) - 1;
   }
+  const int s = j % kGjDepth;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = lane + 32 * i;
-    sh.colbuf[j & 1][r] = a[i][M];
-    a[i][M] = make_float2(r == bi ? 1.0f : 0.0f, 0.0f);
-  }
+  for (int i = 0; i < 4; ++i) sh.colbuf[s][lane + 32 * i] = t[i];
   if (lane == 0) {
-    sh.s_piv[j & 1] = bi;
+    sh.s_piv[s] = bi;
     sh.piv_row[j] = bi;
     sh.used[bi >> 5] |= 1u << (bi & 31);
     if (!(best > 0.0f) && info[b] == 0) info[b] = kk + j + 1;
   }
+  gj_arrive(&sh.full[s]);  // release: this lane's writes above
+  return bi;
 }
 
-// Rank-one update of register slot M: a - f u (u the pivot row, read from the
-// warp's buffer).
 template <int M>
-__device__ __forceinline__ void gj_update(float2 (&a)[4][kGjSlots], const float2 (&f)[4], const float2* u) {
-  const float2 um = u[M];
+__device__ __forceinline__ void gj_unit(float2 (&a)[4][kGjSlots], int bi, int lane) {
+  constexpr int S = M < kGjSlots ? M : 0;  // M >= kGjSlots: a case the switch never takes
 #pragma unroll
-  for (int i = 0; i < 4; ++i) a[i][M] = cfms(a[i][M], f[i], um);
-}
-
-// One Gauss-Jordan column step, column j = 8 JM + jw (slot JM of warp jw,
-// known at compile time).  Only the pivot column crosses warps (shared memory,
-// double buffered, one barrier per column); the pivot row's entries of a
-// warp's columns go through the warp's buffer.
-template <int JM>
-__device__ __forceinline__ void gj_step(float2 (&a)[4][kGjSlots], int jw, int kk, int b, int lane, int w, int tid,
-                                        GjShared& sh, int* __restrict__ info) {
-  const int j = kGjWarps * JM + jw;
-  const int buf = j & 1;
-  __syncthreads();  // column j and its pivot row are published
-  const int p = sh.s_piv[buf];
-  const int lp = p & 31, sp = p >> 5;
-  float2* xw = sh.xbuf[w];
-  if (lane == lp) {
-    switch (sp) {  // one lane: a branch per register slot instead of selects
-#define BEM_GJ_ROWOUT(S) \
-  case S:                \
-    _Pragma("unroll") for (int m = 0; m < kGjSlots; ++m) xw[m] = a[S][m]; \
-    break;
-      BEM_GJ_ROWOUT(0) BEM_GJ_ROWOUT(1) BEM_GJ_ROWOUT(2) BEM_GJ_ROWOUT(3)
-#undef BEM_GJ_ROWOUT
-    }
-  }
-  const float2 piv = sh.colbuf[buf][p];
-  const float d = piv.x * piv.x + piv.y * piv.y;
-  const float rd = d > 0.0f ? 1.0f / d : 0.0f;
-  const float2 dinv = make_float2(piv.x * rd, -piv.y * rd);
-  if (tid == 0) sh.rowscale[p] = dinv;
-  float2 f[4];  // multipliers a_rj / pivot; 0 on the pivot row, which stays as it is
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const float2 c = sh.colbuf[buf][lane + 32 * i];
-    f[i] = (lane + 32 * i == p) ? make_float2(0.0f, 0.0f) : fmul(c, dinv);
-  }
-  __syncwarp();
-  const float2* u = xw;
-#define BEM_GJ_UPD(MM) gj_update<MM>(a, f, u);
-  BEM_GJ_UPD(0) BEM_GJ_UPD(1) BEM_GJ_UPD(2) BEM_GJ_UPD(3) BEM_GJ_UPD(4) BEM_GJ_UPD(5) BEM_GJ_UPD(6)
-  BEM_GJ_UPD(7) BEM_GJ_UPD(8) BEM_GJ_UPD(9) BEM_GJ_UPD(10) BEM_GJ_UPD(11) BEM_GJ_UPD(12) BEM_GJ_UPD(13)
-  BEM_GJ_UPD(14) BEM_GJ_UPD(15)
-#undef BEM_GJ_UPD
-  __syncwarp();  // the warp's reads of its buffer are done before the next step rewrites it
-  // the owner of column j + 1 (slot JM, or JM + 1 after the last warp) picks
-  // its pivot; one straight sequence of updates before it keeps the step's
-  // code small
-  if (w == ((j + 1) & (kGjWarps - 1))) {
-    if (jw < kGjWarps - 1)
-      gj_pivot<JM>(a, j + 1, kk, b, lane, sh, info);
-    else if constexpr (JM < kGjSlots - 1)
-      gj_pivot<JM + 1>(a, j + 1, kk, b, lane, sh, info);
-  }
+  for (int i = 0; i < 4; ++i) a[i][S] = make_float2(lane + 32 * i == bi ? 1.0f : 0.0f, 0.0f);
 }
 
 // Inverse of the diagonal block A_kk by Gauss-Jordan elimination with partial
-// pivoting among its rows (implicit, see above), the block in registers: per
-// column the owning warp picks the pivot and publishes the column, every warp
-// takes the pivot row's entries of its own columns and updates its entries;
-// one barrier per column.  Columns are visited slot by slot so that register
-// indices are compile-time constants.  Output: inv (128 x 128, column-major) =
-// A_kk^{-1}, and its packed copies for the panel product (binv) and the block
-// row of U' (ainv); info flags an exactly zero pivot.
+// pivoting among its rows (implicit, see above), the block in registers.  The
+// warps do not step together: the owner of column j + 1 updates that column
+// first, picks its pivot and publishes it (shared-memory buffers guarded by
+// mbarriers, kGjDepth columns deep) before its update of the other columns,
+// so that the pivot search of the next column overlaps the rank-one updates
+// of the other warps; every warp takes the pivot row's entries of its own
+// columns from its own lanes.  The step body is one loop over the columns
+// (register slots addressed through a switch only for the owner's column).
+// Output: inv (128 x 128, column-major) = A_kk^{-1}, and its packed copies for
+// the panel product (binv) and the block row of U' (ainv); info flags an
+// exactly zero pivot; err is set when a bounded wait runs out.
 __global__ void __launch_bounds__(32 * kGjWarps, 1) clu_gj_kernel(Planes W, int kk, int* __restrict__ info,
                                                                  float2* __restrict__ inv, int nblk,
                                                                  float* __restrict__ binv,
-                                                                 float* __restrict__ ainv) {
+                                                                 float* __restrict__ ainv, int* __restrict__ err) {
   __shared__ GjShared sh;
   const int b = blockIdx.x, tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
@@ -251,30 +260,89 @@ __global__ void __launch_bounds__(32 * kGjWarps, 1) clu_gj_kernel(Planes W, int 
 #pragma unroll
     for (int m = 0; m < kGjSlots; ++m) a[i][m] = ldp(W, b, kk + lane + 32 * i, kk + w + kGjWarps * m);
   if (tid < kB / 32) sh.used[tid] = 0u;
+  if (tid < kGjDepth) {
+    gj_bar_init(&sh.full[tid], 32);
+    gj_bar_init(&sh.empty[tid], kGjWarps);
+  }
+  if (tid == 0) sh.abort = 0;
   __syncthreads();
-  if (w == 0) gj_pivot<0>(a, 0, kk, b, lane, sh, info);  // column 0 (warp 0, slot 0)
-  // the 8 column steps of one slot stay a loop: one copy of the step's code
-  // is reused from the instruction cache
-#define BEM_GJ_SLOT(JM) \
-  _Pragma("unroll 1") for (int jw = 0; jw < kGjWarps; ++jw) gj_step<JM>(a, jw, kk, b, lane, w, tid, sh, info);
-  BEM_GJ_SLOT(0)
-  BEM_GJ_SLOT(1)
-  BEM_GJ_SLOT(2)
-  BEM_GJ_SLOT(3)
-  BEM_GJ_SLOT(4)
-  BEM_GJ_SLOT(5)
-  BEM_GJ_SLOT(6)
-  BEM_GJ_SLOT(7)
-  BEM_GJ_SLOT(8)
-  BEM_GJ_SLOT(9)
-  BEM_GJ_SLOT(10)
-  BEM_GJ_SLOT(11)
-  BEM_GJ_SLOT(12)
-  BEM_GJ_SLOT(13)
-  BEM_GJ_SLOT(14)
-  BEM_GJ_SLOT(15)
-#undef BEM_GJ_SLOT
+  float2 f[4];
+  if (w == 0) {  // column 0: slot 0 of warp 0, nothing to update yet
+#pragma unroll
+    for (int i = 0; i < 4; ++i) f[i] = make_float2(0.0f, 0.0f);
+    const int bi = gj_publish<0>(a, f, make_float2(0.0f, 0.0f), 0, kk, b, lane, sh, info);
+    gj_unit<0>(a, bi, lane);
+  }
+  float2* xw = sh.xbuf[w];
+#pragma unroll 1
+  for (int j = 0; j < kB; ++j) {
+    const int s = j % kGjDepth;
+    if (!gj_wait(&sh.full[s], (j / kGjDepth) & 1, sh, err)) break;
+    const int p = sh.s_piv[s];
+    const int lp = p & 31, sp = p >> 5;
+    if (lane == lp) {
+      switch (sp) {  // one lane: a branch per register slot instead of selects
+#define BEM_GJ_ROWOUT(S) \
+  case S:                \
+    _Pragma("unroll") for (int m = 0; m < kGjSlots; ++m) xw[m] = a[S][m]; \
+    break;
+        BEM_GJ_ROWOUT(0) BEM_GJ_ROWOUT(1) BEM_GJ_ROWOUT(2) BEM_GJ_ROWOUT(3)
+#undef BEM_GJ_ROWOUT
+      }
+    }
+    const float2 piv = sh.colbuf[s][p];
+    const float d = piv.x * piv.x + piv.y * piv.y;
+    const float rd = d > 0.0f ? 1.0f / d : 0.0f;
+    const float2 dinv = make_float2(piv.x * rd, -piv.y * rd);
+    if (tid == 0) sh.rowscale[p] = dinv;
+    // multipliers a_rj / pivot; 0 on the pivot row, which stays as it is
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float2 c = sh.colbuf[s][lane + 32 * i];
+      f[i] = (lane + 32 * i == p) ? make_float2(0.0f, 0.0f) : fmul(c, dinv);
+    }
+    __syncwarp();  // the pivot row is in the warp's buffer; the warp's reads of column j are done
+    if (lane == 0) gj_arrive(&sh.empty[s]);
+    const int nj = j + 1;
+    const bool owner = nj < kB && w == (nj & (kGjWarps - 1));
+    int bi = 0;
+    if (owner) {
+      // buffer nj % kGjDepth is free once every warp has read column nj - kGjDepth
+      if (nj >= kGjDepth && !gj_wait(&sh.empty[nj % kGjDepth], ((nj / kGjDepth) - 1) & 1, sh, err)) break;
+      switch (nj / kGjWarps) {
+#define BEM_GJ_PUB(M) \
+  case M:             \
+    bi = gj_publish<M>(a, f, xw[M < kGjSlots ? M : 0], nj, kk, b, lane, sh, info); \
+    break;
+        BEM_GJ_PUB(0) BEM_GJ_PUB(1) BEM_GJ_PUB(2) BEM_GJ_PUB(3) BEM_GJ_PUB(4) BEM_GJ_PUB(5) BEM_GJ_PUB(6)
+        BEM_GJ_PUB(7) BEM_GJ_PUB(8) BEM_GJ_PUB(9) BEM_GJ_PUB(10) BEM_GJ_PUB(11) BEM_GJ_PUB(12) BEM_GJ_PUB(13)
+        BEM_GJ_PUB(14) BEM_GJ_PUB(15)
+#undef BEM_GJ_PUB
+      }
+    }
+    // rank-one update of every column of the warp: a - f u (u the pivot row)
+#pragma unroll
+    for (int m = 0; m < kGjSlots; ++m) {
+      const float2 um = xw[m];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i][m] = cfms(a[i][m], f[i], um);
+    }
+    if (owner) {
+      switch (nj / kGjWarps) {
+#define BEM_GJ_UNIT(M) \
+  case M:              \
+    gj_unit<M>(a, bi, lane); \
+    break;
+        BEM_GJ_UNIT(0) BEM_GJ_UNIT(1) BEM_GJ_UNIT(2) BEM_GJ_UNIT(3) BEM_GJ_UNIT(4) BEM_GJ_UNIT(5) BEM_GJ_UNIT(6)
+        BEM_GJ_UNIT(7) BEM_GJ_UNIT(8) BEM_GJ_UNIT(9) BEM_GJ_UNIT(10) BEM_GJ_UNIT(11) BEM_GJ_UNIT(12)
+        BEM_GJ_UNIT(13) BEM_GJ_UNIT(14) BEM_GJ_UNIT(15)
+#undef BEM_GJ_UNIT
+      }
+    }
+    __syncwarp();  // the warp's reads of its buffer are done before the next step rewrites it
+  }
   __syncthreads();
+  if (sh.abort) return;
   if (tid < kB) sh.jinv[sh.piv_row[tid]] = tid;
   __syncthreads();
   // A_kk^{-1}(jinv[r], piv_row[c]) = a(r, c) / pivot: staged in shared memory
@@ -933,7 +1001,7 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   auto inverse = [&](int kk, cudaStream_t on) {
     TimedLaunch tl(kKCluGj, on);
     clu_gj_kernel<<<batch, 32 * kGjWarps, kGjOutBytes, on>>>(W, kk, info_dev, w.inv, nblk, w.binv,
-                                         w.ainv + ((kk / kB) & 1) * ainv_buf);
+                                         w.ainv + ((kk / kB) & 1) * ainv_buf, err_dev);
     ++launches;
   };
   // L21 = A21 A_kk^{-1} (split TF32: A_hi B_hi + A_lo B_hi + A_hi B_lo,
