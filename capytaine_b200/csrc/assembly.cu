@@ -536,20 +536,22 @@ __global__ void __launch_bounds__(kRows, 4) assemble_kernel(const bem_assembly_a
 }
 
 // Wave term of Green_wave.f90:162-271 at one point pair for a unit weight:
-// (g, gradient) with the arithmetic of wave_part<double> before its final
-// multiplication by k w.  Swapping the two points leaves g and the vertical
-// derivative unchanged and negates the horizontal derivatives exactly (they
-// are linear in x - xj), which the symmetric assembly below relies on.
-__device__ __forceinline__ void wave_core(const double x[3], const double xj[3], double k, const TabView& T,
+// (g, gradient) before the final multiplication by k w, from the horizontal
+// offset (dx, dy) of the two points, r = k |(dx, dy)| and z = k (x3 + xj3).
+// Swapping the two points leaves g and the vertical derivative unchanged and
+// negates the horizontal derivatives exactly (they are linear in (dx, dy)),
+// which the symmetric assembly below relies on.  The distances are plain
+// square roots and the gradient factors reciprocals (last-ulp differences from
+// the scaled norm and the divisions of wave_part; the stencil of the table is
+// chosen from r and z as there).
+__device__ __forceinline__ void wave_core(double dx, double dy, double r, double z, double k, const TabView& T,
                                           int sing, double& gre, double& gim, double dr[3], double di[3]) {
-  const double dx = x[0] - xj[0], dy = x[1] - xj[1];
-  const double r = k * norm2_2(dx, dy);
-  const double z = k * (x[2] + xj[2]);
-  const double r1 = hypot(r, z);
+  const double r1 = sqrt(r * r + z * z);
   double drdx1 = 0, drdx2 = 0;
   if (fabs(r) > 16 * kEpsilon) {
-    drdx1 = k * k * dx / r;
-    drdx2 = k * k * dy / r;
+    const double q = k * k / r;
+    drdx1 = q * dx;
+    drdx2 = q * dy;
   }
   const double dzdx3 = k;
   double I[5];
@@ -560,10 +562,10 @@ __device__ __forceinline__ void wave_core(const double x[3], const double xj[3],
   di[2] = dzdx3 * I[2];
   if (sing == kHighFreq) {
     gre = I[1];
-    const double r13 = r1 * r1 * r1;
-    dr[0] = drdx1 * I[3] - 2 * drdx1 * r / r13;
-    dr[1] = drdx2 * I[3] - 2 * drdx2 * r / r13;
-    dr[2] = dzdx3 * gre - 2 * dzdx3 * z / r13;
+    const double ir13 = 1 / (r1 * r1 * r1);
+    dr[0] = drdx1 * I[3] - 2 * drdx1 * r * ir13;
+    dr[1] = drdx2 * I[3] - 2 * drdx2 * r * ir13;
+    dr[2] = dzdx3 * gre - 2 * dzdx3 * z * ir13;
   } else {
     gre = I[0];
     dr[0] = drdx1 * I[3];
@@ -605,11 +607,8 @@ __device__ __forceinline__ void integrals_at_f32(double r, double z, const TabVi
   }
   asymptotic<float>((float)r, (float)z, out);
 }
-__device__ __forceinline__ void wave_core_f32(const double x[3], const double xj[3], double k, const TabView& T,
+__device__ __forceinline__ void wave_core_f32(double dx, double dy, double r, double z, double k, const TabView& T,
                                               int sing, double& gre, double& gim, double dr[3], double di[3]) {
-  const double dx = x[0] - xj[0], dy = x[1] - xj[1];
-  const double r = k * norm2_2(dx, dy);
-  const double z = k * (x[2] + xj[2]);
   const float rf = (float)r, zf = (float)z;
   const float r1 = sqrtf(rf * rf + zf * zf);
   float drdx1 = 0.f, drdx2 = 0.f;
@@ -741,12 +740,10 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
       const SymFace& f = faces[jj];
       const int J = J0 + jj;
       double gre, gim, dr[3], di[3];
-      bool self_fs = false;
-      {
-        const double rr = k * norm2_2(M[0] - f.x[0], M[1] - f.x[1]);
-        const double zz = k * (M[2] + f.x[2]);
-        self_fs = fabs(rr) < kLit1em10 && fabs(zz) < kLit1em10;
-      }
+      const double dx = M[0] - f.x[0], dy = M[1] - f.x[1];
+      const double rr = k * sqrt(dx * dx + dy * dy);
+      const double zz = k * (M[2] + f.x[2]);
+      const bool self_fs = fabs(rr) < kLit1em10 && fabs(zz) < kLit1em10;
       const size_t ridx = (size_t)I + (size_t)rank_ld * J;
       const double2 rk = INPLACE ? rank[ridx] : __ldg(rank + ridx);
       double sre, sim, kre, kim;
@@ -762,8 +759,8 @@ __global__ void __launch_bounds__(kSymT, 5) wave_symmetric_kernel(bem_assembly_a
         kre = kMinusOneOverFourPi * (rk.y + dn[2] * dz_re);
         kim = kMinusOneOverFourPi * (dn[2] * dz_im);
       } else {
-        if constexpr (F32) wave_core_f32(M, f.x, k, T, gf_sing, gre, gim, dr, di);
-        else wave_core(M, f.x, k, T, gf_sing, gre, gim, dr, di);
+        if constexpr (F32) wave_core_f32(dx, dy, rr, zz, k, T, gf_sing, gre, gim, dr, di);
+        else wave_core(dx, dy, rr, zz, k, T, gf_sing, gre, gim, dr, di);
         const double kwJ = k * f.w;
         double vr[3] = {kwJ * dr[0], kwJ * dr[1], kwJ * dr[2]};
         double vi[3] = {kwJ * di[0], kwJ * di[1], kwJ * di[2]};

@@ -145,7 +145,7 @@ struct GjShared {
   uint64_t full[kGjDepth];
   uint64_t empty[kGjDepth];
   float2 colbuf[kGjDepth][kB];      // pivot column of step j in buffer j % kGjDepth, by row
-  float2 xbuf[kGjWarps][kGjSlots];  // per warp: its entries of the pivot row
+  alignas(16) float2 xbuf[kGjWarps][kGjSlots];  // per warp: its entries of the pivot row
   float2 rowscale[kB];              // 1 / pivot of the step whose pivot row is this row
   int piv_row[kB];                  // pivot row of each step
   int jinv[kB];                     // step of each pivot row
@@ -190,26 +190,24 @@ __device__ __forceinline__ int gj_publish(const float2 (&a)[4][kGjSlots], const 
   float2 t[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) t[i] = cfms(a[i][S], f[i], um);
-  float best = -1.0f;
-  int bi = kB;
+  // this lane's candidate: the largest |t| among its unused rows (the first of
+  // equal ones, the smallest row), as an ordered key (the bits of the
+  // non-negative float plus one; 0: none, the used rows and NaN); then the
+  // largest key of the warp and, among equal keys, the smallest row
+  unsigned key = 0u;
+  int li = kB;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int r = lane + 32 * i;
     const float av = fabs1(t[i]);
-    if (!((sh.used[i] >> lane) & 1u) && (av > best || (av == best && r < bi))) {
-      best = av;
-      bi = r;
+    const unsigned kv = (((sh.used[i] >> lane) & 1u) || isnan(av)) ? 0u : __float_as_uint(av) + 1u;
+    if (kv > key) {
+      key = kv;
+      li = lane + 32 * i;
     }
   }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    const float ob = __shfl_xor_sync(0xffffffffu, best, off);
-    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-    if (ob > best || (ob == best && oi < bi)) {
-      best = ob;
-      bi = oi;
-    }
-  }
+  const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+  int bi = (int)__reduce_min_sync(0xffffffffu, key == kmax ? (unsigned)li : (unsigned)kB);
+  const float best = kmax ? __uint_as_float(kmax - 1u) : -1.0f;
   if (bi >= kB) {  // no comparable candidate (NaN): the first unused row
 #pragma unroll
     for (int i = 3; i >= 0; --i)
@@ -284,7 +282,8 @@ __global__ void __launch_bounds__(32 * kGjWarps, 1) clu_gj_kernel(Planes W, int 
       switch (sp) {  // one lane: a branch per register slot instead of selects
 #define BEM_GJ_ROWOUT(S) \
   case S:                \
-    _Pragma("unroll") for (int m = 0; m < kGjSlots; ++m) xw[m] = a[S][m]; \
+    _Pragma("unroll") for (int m = 0; m < kGjSlots; m += 2) \
+      reinterpret_cast<float4*>(xw)[m / 2] = make_float4(a[S][m].x, a[S][m].y, a[S][m + 1].x, a[S][m + 1].y); \
     break;
         BEM_GJ_ROWOUT(0) BEM_GJ_ROWOUT(1) BEM_GJ_ROWOUT(2) BEM_GJ_ROWOUT(3)
 #undef BEM_GJ_ROWOUT
@@ -292,7 +291,7 @@ __global__ void __launch_bounds__(32 * kGjWarps, 1) clu_gj_kernel(Planes W, int 
     }
     const float2 piv = sh.colbuf[s][p];
     const float d = piv.x * piv.x + piv.y * piv.y;
-    const float rd = d > 0.0f ? 1.0f / d : 0.0f;
+    const float rd = d > 0.0f ? __frcp_rn(d) : 0.0f;  // = 1.0f / d, correctly rounded
     const float2 dinv = make_float2(piv.x * rd, -piv.y * rd);
     if (tid == 0) sh.rowscale[p] = dinv;
     // multipliers a_rj / pivot; 0 on the pivot row, which stays as it is
@@ -320,10 +319,14 @@ __global__ void __launch_bounds__(32 * kGjWarps, 1) clu_gj_kernel(Planes W, int 
 #undef BEM_GJ_PUB
       }
     }
-    // rank-one update of every column of the warp: a - f u (u the pivot row)
+    // rank-one update of every column of the warp: a - f u (u the pivot row,
+    // read from the warp's buffer two entries per load)
+    float4 u4[kGjSlots / 2];
+#pragma unroll
+    for (int m = 0; m < kGjSlots / 2; ++m) u4[m] = reinterpret_cast<const float4*>(xw)[m];
 #pragma unroll
     for (int m = 0; m < kGjSlots; ++m) {
-      const float2 um = xw[m];
+      const float2 um = (m & 1) ? make_float2(u4[m / 2].z, u4[m / 2].w) : make_float2(u4[m / 2].x, u4[m / 2].y);
 #pragma unroll
       for (int i = 0; i < 4; ++i) a[i][m] = cfms(a[i][m], f[i], um);
     }
