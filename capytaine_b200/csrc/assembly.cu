@@ -220,13 +220,58 @@ struct TabView {
   const double* rinv;
   const double* zinv;
   double dz;
+  // set by tab_prologue on the device: the scaled grid's node index of r = 1,
+  // the slope of its linear part and 1 / dz (the float32 index estimates)
+  int index_of_1;
+  double r_slope, inv_dz;
 };
 __device__ __forceinline__ void tab_prologue(TabView& T) {
   if (T.nr > 1 && T.nz > 1) {
     T.rmax = __ldg(T.r_range + T.nr - 1);
     T.zlast = __ldg(T.z_range + T.nz - 1);
     T.dz = scaled_dz(T.zlast, T.nz);
+    T.index_of_1 = (int)lroundf((float)(T.nr * 81) / 676.0f);
+    T.r_slope = (double)(T.nr - T.index_of_1) / (T.rmax - 1);
+    T.inv_dz = 1 / T.dz;
   }
+}
+
+// f_nint(q) when q is more than `margin` away from every rounding boundary
+// (q an estimate of the float64 argument of the rounding, within margin of
+// it): then both round to the same node.  false: decide with the float64
+// expression.
+__device__ __forceinline__ bool nint_clear(double q, double margin, int& out) {
+  if (!(fabs(q) < 1.0e9)) return false;
+  const double fl = floor(q);
+  const double fr = q - fl;
+  if (fabs(fr - 0.5) <= margin) return false;
+  out = (int)fl + (fr > 0.5 ? 1 : 0);
+  return true;
+}
+// Delhommeau_integrals.f90:301-363 on the scaled grid from float32 logarithms
+// and precomputed slopes, falling back to the float64 expressions of
+// nearest_r_index / nearest_z_index within a margin of a rounding boundary
+// (log10f is within 2 ulp, i.e. 2e-6 absolute for |log10| <= 16; the margins
+// allow 1e-4): the same nodes as those, at a fraction of the float64 cost.
+__device__ __forceinline__ int nearest_r_index_fast(double r, const TabView& T) {
+  if (T.grid != kLegacyGrid && r >= kLit1em10) {
+    int i;
+    if (r < 1.0) {
+      const double q = ((double)log10f((float)r) / 10.0 + 1.0) * (double)(T.index_of_1 - 1) + 1;
+      if (nint_clear(q, 1e-5 * (double)(T.index_of_1 - 1), i)) return i;
+    } else {
+      if (nint_clear((r - 1) * T.r_slope + (double)T.index_of_1, 1e-9, i)) return i;
+    }
+  }
+  return nearest_r_index(r, T.nr, T.rmax, T.grid);
+}
+__device__ __forceinline__ int nearest_z_index_fast(double z, const TabView& T) {
+  if (T.grid != kLegacyGrid) {
+    int j;
+    const double q = ((double)log10f((float)fabs(z)) + 10) * T.inv_dz;
+    if (nint_clear(q, 1e-4 * T.inv_dz, j)) return j;
+  }
+  return nearest_z_index(z, T.nz, T.zlast, T.grid, T.dz);
 }
 // Lagrange weights of the three stencil nodes u[0..2] at x (node i's weight
 // prod_{k != i} (x - u_k) / (u_i - u_k)), the reciprocal denominators from inv
@@ -255,9 +300,9 @@ __device__ void integrals_at(double r, double z, const TabView& T, R out[5]) {
     return;
   }
   if (fabs(z) < fabs(T.zlast) && r < T.rmax) {
-    int i = nearest_r_index(r, T.nr, T.rmax, T.grid);
+    int i = nearest_r_index_fast(r, T);
     i = max(2, min(T.nr - 1, i));
-    int j = nearest_z_index(z, T.nz, T.zlast, T.grid, T.dz);
+    int j = nearest_z_index_fast(z, T);
     j = max(2, min(T.nz - 1, j));
     const int ic = i - 1, jc = j - 1;
     const double r1 = __ldg(T.r_range + ic - 1), r2 = __ldg(T.r_range + ic), r3 = __ldg(T.r_range + ic + 1);
@@ -543,10 +588,11 @@ __global__ void __launch_bounds__(kRows, 4) assemble_kernel(const bem_assembly_a
 // which the symmetric assembly below relies on.  The distances are plain
 // square roots and the gradient factors reciprocals (last-ulp differences from
 // the scaled norm and the divisions of wave_part; the stencil of the table is
-// chosen from r and z as there).
+// chosen from r and z as there).  r = z = 0 (a free-surface panel with
+// itself) never reaches it.
 __device__ __forceinline__ void wave_core(double dx, double dy, double r, double z, double k, const TabView& T,
                                           int sing, double& gre, double& gim, double dr[3], double di[3]) {
-  const double r1 = sqrt(r * r + z * z);
+  const double ir1 = rsqrt(r * r + z * z);  // 1 / |(r, z)|
   double drdx1 = 0, drdx2 = 0;
   if (fabs(r) > 16 * kEpsilon) {
     const double q = k * k / r;
@@ -562,7 +608,7 @@ __device__ __forceinline__ void wave_core(double dx, double dy, double r, double
   di[2] = dzdx3 * I[2];
   if (sing == kHighFreq) {
     gre = I[1];
-    const double ir13 = 1 / (r1 * r1 * r1);
+    const double ir13 = ir1 * ir1 * ir1;
     dr[0] = drdx1 * I[3] - 2 * drdx1 * r * ir13;
     dr[1] = drdx2 * I[3] - 2 * drdx2 * r * ir13;
     dr[2] = dzdx3 * gre - 2 * dzdx3 * z * ir13;
@@ -570,7 +616,7 @@ __device__ __forceinline__ void wave_core(double dx, double dy, double r, double
     gre = I[0];
     dr[0] = drdx1 * I[3];
     dr[1] = drdx2 * I[3];
-    dr[2] = (sing == kLowFreq) ? dzdx3 * (gre + 2 / r1) : dzdx3 * gre;
+    dr[2] = (sing == kLowFreq) ? dzdx3 * (gre + 2 * ir1) : dzdx3 * gre;
   }
 }
 
