@@ -875,7 +875,13 @@ def main():
             kernels[lib.bem_kernel_class_name(c).decode()] = {"class": c, "ms_total": tot.value,
                                                               "launches": int(cnt.value)}
     _lib.check(lib.bem_kernel_timer_enable(0))
-    st = engine.solve_frequencies(body, batches[0], sync_stats=True).stats
+    # stage times averaged over this rank's whole sweep (the stages' costs vary
+    # with the frequency: the wave term's table stencils and the refinement's
+    # iterations near the irregular frequencies)
+    nsweep = -(-len(my_omegas) // nb)
+    st = engine.solve_frequencies(body, my_omegas, batch=nb, sync_stats=True).stats
+    st = {k: (v / nsweep if k.endswith("_ms") else v) for k, v in st.items()}
+    st["batches_averaged"] = nsweep
     peaks, peak_src = measured_peaks()
     roofline = kernel_roofline(kernels, n, nb * args.steps, args.engine, peaks, peak_src)
 

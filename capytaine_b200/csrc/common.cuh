@@ -38,6 +38,19 @@ struct c64d {
 
 __host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+#ifdef __CUDACC__
+// x rounded to the nearest TF32 value (10 mantissa bits, ties away from zero,
+// the low 13 bits cleared).  The tensor cores read a float32 operand as TF32
+// by dropping those bits, which errs by up to 2^-10 and always towards zero;
+// operands stored rounded err by at most 2^-11 and without that bias, which
+// accumulates over the depth of a product otherwise.
+__device__ __forceinline__ float tf32_rn(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+#endif
+
 // Error recording shared by all entry points.
 int set_cuda_error(cudaError_t e, const char* where);
 int set_error(int code, const char* msg);

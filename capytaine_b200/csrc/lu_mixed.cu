@@ -38,14 +38,18 @@ constexpr int kRhs = 16;       // right-hand sides per solve launch
 constexpr int kOpBuffers = 3;  // packed operands of the current, previous and next block steps
 
 __device__ __forceinline__ float2 fmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
-__device__ __forceinline__ float2 ffms(float2 acc, float2 a, float2 b) {
-  return make_float2(acc.x - (a.x * b.x - a.y * b.y), acc.y - (a.x * b.y + a.y * b.x));
-}
-__device__ __forceinline__ float2 fdiv(float2 a, float2 b) {
-  const float d = b.x * b.x + b.y * b.y;
-  return make_float2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
-}
 __device__ __forceinline__ float fabs1(float2 a) { return fabsf(a.x) + fabsf(a.y); }
+// a b + c on a pair of floats in one instruction (fma.rn.f32x2: per element the
+// correctly rounded fused multiply-add of fmaf)
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n.reg .b64 ra, rb, rc, rd;\n"
+      "mov.b64 ra, {%2, %3};\nmov.b64 rb, {%4, %5};\nmov.b64 rc, {%6, %7};\n"
+      "fma.rn.f32x2 rd, ra, rb, rc;\nmov.b64 {%0, %1}, rd;\n}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
 
 struct Planes {
   float* re;
@@ -111,13 +115,13 @@ constexpr int kGjLd = kB + 1;            // column stride of the staged inverse 
 constexpr int kGjOutBytes = kB * kGjLd * (int)sizeof(float2);  // dynamic shared memory of the inverse
 constexpr long long kGjWaitLimit = 1ll << 22;  // polls of a bounded wait (about a second)
 
-// acc - a b in two fused multiply-adds per component.
-__device__ __forceinline__ float2 cfms(float2 acc, float2 a, float2 b) {
-  acc.x = fmaf(-a.x, b.x, acc.x);
-  acc.x = fmaf(a.y, b.y, acc.x);
-  acc.y = fmaf(-a.x, b.y, acc.y);
-  acc.y = fmaf(-a.y, b.x, acc.y);
-  return acc;
+// acc - a b in two fused multiply-adds per component, in this order:
+//   acc.x = fmaf(a.y, b.y, fmaf(-a.x, b.x, acc.x)),
+//   acc.y = fmaf(-a.y, b.x, fmaf(-a.x, b.y, acc.y)),
+// as two pair instructions: an = (-a.x, -a.x), ay = (a.y, -a.y) (once per
+// multiplier), b and bs = (b.y, b.x) (once per pivot-row entry).
+__device__ __forceinline__ float2 cfms2(float2 acc, float2 an, float2 ay, float2 b, float2 bs) {
+  return fma2(ay, bs, fma2(an, b, acc));
 }
 
 __device__ __forceinline__ uint32_t gj_smem(const void* p) {
@@ -189,7 +193,8 @@ __device__ __forceinline__ int gj_publish(const float2 (&a)[4][kGjSlots], const 
   constexpr int S = M < kGjSlots ? M : 0;  // M >= kGjSlots: a case the switch never takes
   float2 t[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) t[i] = cfms(a[i][S], f[i], um);
+  for (int i = 0; i < 4; ++i)
+    t[i] = cfms2(a[i][S], make_float2(-f[i].x, -f[i].x), make_float2(f[i].y, -f[i].y), um, make_float2(um.y, um.x));
   // this lane's candidate: the largest |t| among its unused rows (the first of
   // equal ones, the smallest row), as an ordered key (the bits of the
   // non-negative float plus one; 0: none, the used rows and NaN); then the
@@ -324,11 +329,18 @@ __global__ void __launch_bounds__(32 * kGjWarps, 1) clu_gj_kernel(Planes W, int 
     float4 u4[kGjSlots / 2];
 #pragma unroll
     for (int m = 0; m < kGjSlots / 2; ++m) u4[m] = reinterpret_cast<const float4*>(xw)[m];
+    float2 fn[4], fy[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      fn[i] = make_float2(-f[i].x, -f[i].x);
+      fy[i] = make_float2(f[i].y, -f[i].y);
+    }
 #pragma unroll
     for (int m = 0; m < kGjSlots; ++m) {
       const float2 um = (m & 1) ? make_float2(u4[m / 2].z, u4[m / 2].w) : make_float2(u4[m / 2].x, u4[m / 2].y);
+      const float2 us = make_float2(um.y, um.x);
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i][m] = cfms(a[i][m], f[i], um);
+      for (int i = 0; i < 4; ++i) a[i][m] = cfms2(a[i][m], fn[i], fy[i], um, us);
     }
     if (owner) {
       switch (nj / kGjWarps) {
@@ -374,8 +386,8 @@ __global__ void __launch_bounds__(32 * kGjWarps, 1) clu_gj_kernel(Planes W, int 
   for (int idx = tid; idx < kB * kB; idx += blockDim.x) {
     const int col = idx & (kB - 1), row = idx >> 7;
     const float2 v = gj_out[col * kGjLd + row];
-    ao[(size_t)row * 2 * kB + col] = v.x;
-    ao[(size_t)row * 2 * kB + kB + col] = v.y;
+    ao[(size_t)row * 2 * kB + col] = tf32_rn(v.x);
+    ao[(size_t)row * 2 * kB + kB + col] = tf32_rn(v.y);
   }
   // the B operand of the split-TF32 product L21 = A21 A_kk^{-1} (three
   // K-blocks of 256: hi, hi, lo; see clu_pack_kernel for the A side):
@@ -412,11 +424,11 @@ __global__ void __launch_bounds__(32 * kGjWarps, 1) clu_gj_kernel(Planes W, int 
 // Both through shared memory, so that reads and writes are coalesced.
 // Bop: [batch][2*npad][2*kB]; A3: [batch][npad][kSplitK].
 __global__ void __launch_bounds__(256) clu_pack_kernel(Planes W, int npad, int kk, int nrest, int row0, int col0,
-                                                       float* __restrict__ Bop, float* __restrict__ A3) {
+                                                       float* __restrict__ Bop, float* __restrict__ A3, int t0) {
   __shared__ float tre[kB][33], tim[kB][33];  // [column][row] of a 32 x 128 tile
   const int b = blockIdx.y, tid = threadIdx.x;
   const size_t kp = 2 * kB;
-  const int t = blockIdx.x;
+  const int t = blockIdx.x + t0;  // a launch may cover a range of the blocks only
   if (t < nrest) {
     // 128 x 64 of A12: B operand rows of the complex columns c0 .. c0+63;
     // thread (q, cc): rows 4 q .. 4 q + 3 of column cc (16-byte loads and stores)
@@ -428,8 +440,10 @@ __global__ void __launch_bounds__(256) clu_pack_kernel(Planes W, int npad, int k
     const int q = tid & 31;
     for (int c = tid >> 5; c < kPT; c += 8) {
       const size_t g = (size_t)(c0 + c) * W.ld + kk + 4 * q;
-      const float4 ur = *reinterpret_cast<const float4*>(re + g);
-      const float4 ui = *reinterpret_cast<const float4*>(im + g);
+      float4 ur = *reinterpret_cast<const float4*>(re + g);
+      float4 ui = *reinterpret_cast<const float4*>(im + g);
+      ur = make_float4(tf32_rn(ur.x), tf32_rn(ur.y), tf32_rn(ur.z), tf32_rn(ur.w));  // TF32 operands
+      ui = make_float4(tf32_rn(ui.x), tf32_rn(ui.y), tf32_rn(ui.z), tf32_rn(ui.w));
       const int jj = c0 - j0 + c;
       float4* rowR = reinterpret_cast<float4*>(Bb + (size_t)(2 * j0 + jj) * kp);
       float4* rowI = reinterpret_cast<float4*>(Bb + (size_t)(2 * j0 + kB + jj) * kp);
@@ -520,22 +534,35 @@ constexpr int kRingDeep = 5, kRingShallow = 2;
 constexpr int kQCols = 32;                   // columns of a quarter block
 constexpr int kQFloats = 2 * kQCols * kB;    // one slot: [plane][column][row]
 
+// acc += Re(A) y and acci += Im(A) y over the quarter's half h of columns for
+// row r (two pair instructions per entry and right-hand side, y = (Re, Im));
+// fold_rhs turns the two into the complex product A y.
 template <int NC>
 __device__ __forceinline__ void quarter_times_rhs(const float* __restrict__ Tre, const float* __restrict__ Tim,
                                                   const float2* __restrict__ Y, int r, int h,
-                                                  float2 (&acc)[NC]) {
+                                                  float2 (&acc)[NC], float2 (&acci)[NC]) {
 #pragma unroll 4
   for (int mm = 16 * h; mm < 16 * h + 16; ++mm) {
     const float ar = Tre[mm * kB + r], ai = Tim[mm * kB + r];
+    const float2 ar2 = make_float2(ar, ar), ai2 = make_float2(ai, ai);
     const float4* y4 = reinterpret_cast<const float4*>(Y + mm * NC);
 #pragma unroll
     for (int c2 = 0; c2 < NC / 2; ++c2) {
       const float4 y = y4[c2];
-      acc[2 * c2].x = fmaf(ar, y.x, fmaf(-ai, y.y, acc[2 * c2].x));
-      acc[2 * c2].y = fmaf(ar, y.y, fmaf(ai, y.x, acc[2 * c2].y));
-      acc[2 * c2 + 1].x = fmaf(ar, y.z, fmaf(-ai, y.w, acc[2 * c2 + 1].x));
-      acc[2 * c2 + 1].y = fmaf(ar, y.w, fmaf(ai, y.z, acc[2 * c2 + 1].y));
+      const float2 y0 = make_float2(y.x, y.y), y1 = make_float2(y.z, y.w);
+      acc[2 * c2] = fma2(ar2, y0, acc[2 * c2]);
+      acci[2 * c2] = fma2(ai2, y0, acci[2 * c2]);
+      acc[2 * c2 + 1] = fma2(ar2, y1, acc[2 * c2 + 1]);
+      acci[2 * c2 + 1] = fma2(ai2, y1, acci[2 * c2 + 1]);
     }
+  }
+}
+template <int NC>
+__device__ __forceinline__ void fold_rhs(float2 (&acc)[NC], float2 (&acci)[NC]) {
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    acc[c] = make_float2(acc[c].x - acci[c].y, acc[c].y + acci[c].x);
+    acci[c] = make_float2(0.0f, 0.0f);
   }
 }
 
@@ -546,7 +573,7 @@ __device__ __forceinline__ void cp_async_wait_group() {
 }
 
 template <int NC, int kRing>
-__global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nblk, int batch,
+__global__ void __launch_bounds__(256, kRing == kRingShallow ? 2 : 1) ctrsm_persistent_kernel(Planes W, int nblk, int batch,
                                                                const float2* __restrict__ inv, double2* B,
                                                                int64_t ldb, int64_t strideB, int nrhs, int forward,
                                                                int* flags, int* ticket, int* err, const int* skip,
@@ -587,9 +614,9 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
   const int ndep = forward ? i : (nblk - 1 - i);
   const float* Wre = W.re + (size_t)b * W.stride;
   const float* Wim = W.im + (size_t)b * W.stride;
-  float2 acc[NC];
+  float2 acc[NC], acci[NC];
 #pragma unroll
-  for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.0f, 0.0f);
+  for (int c = 0; c < NC; ++c) acc[c] = acci[c] = make_float2(0.0f, 0.0f);
   if (!forward) {
     // x_i = A_ii^{-1} b_i - sum_j U'_ij x_j with U' = A_ii^{-1} U: the product
     // with the diagonal inverse comes first, off the chain of dependencies,
@@ -609,10 +636,11 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
 #pragma unroll 1
       for (int qq = q0; qq < q0 + kDiagPass; ++qq) {
         const float* slot = ring + (qq - q0) * kQFloats;
-        quarter_times_rhs<NC>(slot, slot + kQCols * kB, X + qq * kQCols * NC, r, h, acc);
+        quarter_times_rhs<NC>(slot, slot + kQCols * kB, X + qq * kQCols * NC, r, h, acc, acci);
       }
       __syncthreads();  // the slots are restaged by the next pass
     }
+    fold_rhs<NC>(acc, acci);
     if (h == 1) {
 #pragma unroll
       for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
@@ -681,8 +709,9 @@ __global__ void __launch_bounds__(256) ctrsm_persistent_kernel(Planes W, int nbl
     cp_async_wait_group<kRing - 1>();  // this thread's copies of quarter q have landed
     __syncthreads();                   // everyone's copies, and Y
     const float* slot = ring + (q % kRing) * kQFloats;
-    quarter_times_rhs<NC>(slot, slot + kQCols * kB, Y + qq * kQCols * NC, r, h, acc);
+    quarter_times_rhs<NC>(slot, slot + kQCols * kB, Y + qq * kQCols * NC, r, h, acc, acci);
     if (qq == 3) {
+      fold_rhs<NC>(acc, acci);
       if (h == 1) {
 #pragma unroll
         for (int c = 0; c < NC; ++c) P[r * NC + c] = acc[c];
@@ -868,6 +897,7 @@ struct Lookahead {
   cudaStream_t upper = nullptr;
   cudaEvent_t diag = nullptr;
   cudaEvent_t strips = nullptr;
+  cudaEvent_t colpack = nullptr;
   cudaEvent_t panel = nullptr;
   cudaEvent_t upper_done[2] = {nullptr, nullptr};
 };
@@ -886,6 +916,7 @@ int lookahead_for(cudaStream_t caller, Lookahead** out) {
     BEM_CUDA_CHECK(cudaStreamCreateWithPriority(&fresh->upper, cudaStreamNonBlocking, least));
     BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->diag, cudaEventDisableTiming));
     BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->strips, cudaEventDisableTiming));
+    BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->colpack, cudaEventDisableTiming));
     BEM_CUDA_CHECK(cudaEventCreateWithFlags(&fresh->panel, cudaEventDisableTiming));
     for (auto& e : fresh->upper_done) BEM_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     la = std::move(fresh);
@@ -1059,7 +1090,7 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
   if (npad > kB) {
     const int m = npad - kB;
     TimedLaunch tl(kKCluPanel, s);
-    clu_pack_kernel<<<dim3(m / kPT + m / 32, batch), 256, 0, s>>>(W, npad, 0, m / kPT, kB, 0, Bop[0], w.a3);
+    clu_pack_kernel<<<dim3(m / kPT + m / 32, batch), 256, 0, s>>>(W, npad, 0, m / kPT, kB, 0, Bop[0], w.a3, 0);
     ++launches;
   }
   if ((st = panel(0, 0, s))) return st;
@@ -1090,15 +1121,24 @@ int clu_factor_impl(const void* K_dev, int64_t ldk, int64_t strideK, int n, int 
     if (rest > 0) {
       // the inverse of block kn holds one SM per matrix meanwhile
       if ((st = update(cur, kn, kn, rest + kB, rest + kB, pend, 0, true, batch))) return st;
+      // the block column's split copy first: the panel product starts on it
+      // while the block row is packed as the next step's B operand
       TimedLaunch tl(kKCluPanel, s);
-      clu_pack_kernel<<<dim3(rest / kPT + rest / 32, batch), 256, 0, s>>>(W, npad, kn, rest / kPT, kn + kB, kn,
-                                                                         Bop[nxt], w.a3);
-      ++launches;
+      clu_pack_kernel<<<dim3(rest / 32, batch), 256, 0, s>>>(W, npad, kn, rest / kPT, kn + kB, kn, Bop[nxt], w.a3,
+                                                            rest / kPT);
+      BEM_CUDA_CHECK(cudaEventRecord(la->colpack, s));
+      clu_pack_kernel<<<dim3(rest / kPT, batch), 256, 0, s>>>(W, npad, kn, rest / kPT, kn + kB, kn, Bop[nxt], w.a3,
+                                                             0);
+      launches += 2;
+    } else {
+      BEM_CUDA_CHECK(cudaEventRecord(la->colpack, s));
     }
     BEM_CUDA_CHECK(cudaEventRecord(la->strips, s));
-    BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->strips, 0));
+    BEM_CUDA_CHECK(cudaStreamWaitEvent(la->side, la->colpack, 0));
     if ((st = panel(kn, nxt, la->side))) return st;
     BEM_CUDA_CHECK(cudaEventRecord(la->panel, la->side));
+    // U' reads the block row's B operand and the inverse
+    BEM_CUDA_CHECK(cudaStreamWaitEvent(la->upper, la->strips, 0));
     BEM_CUDA_CHECK(cudaStreamWaitEvent(la->upper, la->panel, 0));
     if ((st = upper(kn, nxt, la->upper))) return st;
     BEM_CUDA_CHECK(cudaEventRecord(la->upper_done[(step + 1) & 1], la->upper));

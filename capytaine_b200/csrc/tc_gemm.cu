@@ -224,11 +224,13 @@ __device__ __forceinline__ bool mbar_wait_n(uint64_t* bar, uint32_t parity, int*
 }
 
 // Packed copy of 16 result values of one thread (row layout [Re | Im], 256
-// floats per row): off is the offset from the thread's pack pointer.
+// floats per row), rounded to TF32 (it is an operand of later products): off
+// is the offset from the thread's pack pointer.
 __device__ __forceinline__ void pack_chunk(float* pk, int off, const float (&v)[16]) {
   float4* d = reinterpret_cast<float4*>(pk + off);
 #pragma unroll
-  for (int j = 0; j < 4; ++j) d[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+  for (int j = 0; j < 4; ++j)
+    d[j] = make_float4(tf32_rn(v[4 * j]), tf32_rn(v[4 * j + 1]), tf32_rn(v[4 * j + 2]), tf32_rn(v[4 * j + 3]));
 }
 
 // Trailing update with double-buffered accumulators: a CTA (one per SM: 197 KB
