@@ -8,12 +8,19 @@
 // rotations, back substitution of the Hessenberg system at the end of each
 // restart cycle, the true residual b - A x checked after each cycle and the
 // inner tolerance adapted as SciPy does (gh-8400 rule).  With the float32 LU
-// factors of bem_clu_factor as M^-1 it is right-preconditioned GMRES,
-// A M^-1 u = b, x = M^-1 u, with float64 products: the Arnoldi residual is the
-// true residual, so a preconditioner that is poor in a few directions (K close
-// to singular near an irregular frequency) costs a few iterations, not the
-// convergence test.  This is GMRES-based iterative refinement of the
-// mixed-precision LU (capytaine calls SciPy's GMRES without a preconditioner).
+// factors of bem_clu_factor as M^-1 it is flexible GMRES (Saad, "A flexible
+// inner-outer preconditioned GMRES algorithm", SIAM J. Sci. Comput. 14, 1993):
+// each preconditioned vector z_k = M^-1 v_k is kept and the cycle ends with
+// x += Z y, so that A Z = V H holds for the vectors actually formed.  The
+// float32 substitutions make M^-1 slightly nonlinear (their rounding depends on
+// the vector), which matters when K is close to singular near an irregular
+// frequency: |M^-1| then reaches 1e5-1e6 and a second application M^-1 (V y)
+// at the end of a cycle no longer matches the products the Arnoldi process
+// saw.  With Z kept, the Arnoldi residual is the true residual (float64
+// products), so a preconditioner that is poor in a few directions costs a few
+// iterations, not the convergence test.  This is GMRES-based iterative
+// refinement of the mixed-precision LU (capytaine calls SciPy's GMRES without
+// a preconditioner).
 //
 // Every column of every matrix is an independent system ("system" below).  All
 // systems advance in lockstep: one matrix-vector product serves the current
@@ -349,24 +356,19 @@ __global__ void __launch_bounds__(kThreads) gmres_arnoldi_kernel(Layout L, int c
 }
 
 // End of a cycle: y = H^-1 S by back substitution (SciPy's pseudo-solve of
-// singular cases), x += V y; R = b for the residual.
-// With right preconditioning (Z != NULL) the combination z = V y goes to Z
-// (zero for systems that did not run) and x += M^-1 z follows.
-__global__ void __launch_bounds__(kThreads) gmres_update_kernel(Layout L, const double2* __restrict__ V,
+// singular cases), x += P y with P the basis the products were taken of (V
+// without a preconditioner, the kept Z = M^-1 V with one); R = b for the
+// residual.
+__global__ void __launch_bounds__(kThreads) gmres_update_kernel(Layout L, const double2* __restrict__ P,
                                                                 const double2* __restrict__ H,
                                                                 double2* __restrict__ Svec, const double2* __restrict__ Bv,
                                                                 double2* __restrict__ X, double2* __restrict__ R,
-                                                                double2* __restrict__ Z, const GmresSystem* sys,
-                                                                const Flags* flags) {
+                                                                const GmresSystem* sys, const Flags* flags) {
   __shared__ double2 y[kMaxRestart];
   if (flags->skip_all) return;
   const int s = blockIdx.x;
   const GmresSystem g = sys[s];
-  if (!g.ran || g.col_end < 0) {
-    if (Z)
-      for (int i = threadIdx.x; i < L.npad; i += blockDim.x) Z[L.vec_off(s) + i] = make_double2(0.0, 0.0);
-    return;
-  }
+  if (!g.ran || g.col_end < 0) return;
   const int col = g.col_end;
   if (threadIdx.x == 0) {
     const double2* h = H + (int64_t)s * L.m * (L.m + 1);  // h[c][r] at c*(m+1) + r
@@ -391,24 +393,10 @@ __global__ void __launch_bounds__(kThreads) gmres_update_kernel(Layout L, const 
   double2* x = X + L.x_off(s);
   const double2* b = Bv + L.x_off(s);
   double2* r = R + L.vec_off(s);
-  if (Z) {
-    double2* z = Z + L.vec_off(s);
-    for (int i = threadIdx.x; i < L.npad; i += blockDim.x) {
-      double2 zi = make_double2(0.0, 0.0);
-      for (int k = 0; k <= col; ++k) {
-        const double2 p = cmul(y[k], V[L.v_off(s, k) + i]);
-        zi.x += p.x;
-        zi.y += p.y;
-      }
-      z[i] = zi;
-      if (i < L.n) r[i] = b[i];
-    }
-    return;
-  }
   for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
     double2 xi = x[i];
     for (int k = 0; k <= col; ++k) {
-      const double2 p = cmul(y[k], V[L.v_off(s, k) + i]);
+      const double2 p = cmul(y[k], P[L.v_off(s, k) + i]);
       xi.x += p.x;
       xi.y += p.y;
     }
@@ -417,28 +405,15 @@ __global__ void __launch_bounds__(kThreads) gmres_update_kernel(Layout L, const 
   }
 }
 
-// x += z for the systems of the cycle (right preconditioning: z = M^-1 V y).
-__global__ void gmres_add_kernel(Layout L, const double2* __restrict__ Z, double2* __restrict__ X,
-                                 const GmresSystem* sys, const Flags* flags) {
-  if (flags->skip_all) return;
-  const int s = blockIdx.y;
-  if (!sys[s].ran || sys[s].col_end < 0) return;
-  const double2* z = Z + L.vec_off(s);
-  double2* x = X + L.x_off(s);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
-    const double2 zi = z[i], xi = x[i];
-    x[i] = make_double2(xi.x + zi.x, xi.y + zi.y);
-  }
-}
-
-// Z = v_col of the systems in the inner loop (right preconditioning: M^-1 v_col next).
+// z_col = v_col of the systems in the inner loop, into Z's slot col (same
+// layout as V), where M^-1 then solves in place (flexible GMRES keeps it).
 __global__ void gmres_gather_kernel(Layout L, const double2* __restrict__ V, int col, double2* __restrict__ Z,
                                     const GmresSystem* sys, const Flags* flags) {
   if (flags->skip_inner) return;
   const int s = blockIdx.y;
   if (!sys[s].active) return;
   const double2* v = V + L.v_off(s, col);
-  double2* z = Z + L.vec_off(s);
+  double2* z = Z + L.v_off(s, col);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.npad; i += gridDim.x * blockDim.x) z[i] = v[i];
 }
 
@@ -521,7 +496,7 @@ size_t carve_gmres(void* base, int n, int npad, int nrhs, int batch, int m, Gmre
   };
   const size_t oV = take(sizeof(double2) * nsys * (m + 1) * npad);
   const size_t oW = take(sizeof(double2) * nsys * npad);
-  const size_t oZ = take(sizeof(double2) * nsys * npad);
+  const size_t oZ = take(sizeof(double2) * nsys * (m + 1) * npad);  // kept M^-1 v_k (flexible GMRES)
   const size_t oR = take(sizeof(double2) * nsys * npad);
   const size_t oH = take(sizeof(double2) * nsys * m * (m + 1));
   const size_t oGs = take(sizeof(double2) * nsys * m);
@@ -585,7 +560,8 @@ extern "C" int bem_gmres_solve(const void* A_dev, int64_t lda, int64_t strideA, 
   BEM_CUDA_CHECK(cudaMemsetAsync(w.V, 0, sizeof(double2) * (size_t)nsys * (m + 1) * npad, s));
   BEM_CUDA_CHECK(cudaMemsetAsync(w.W, 0, sizeof(double2) * (size_t)nsys * npad, s));
   BEM_CUDA_CHECK(cudaMemsetAsync(w.R, 0, sizeof(double2) * (size_t)nsys * npad, s));
-  BEM_CUDA_CHECK(cudaMemsetAsync(w.Z, 0, sizeof(double2) * (size_t)nsys * npad, s));
+  if (precond_work_dev)
+    BEM_CUDA_CHECK(cudaMemsetAsync(w.Z, 0, sizeof(double2) * (size_t)nsys * (m + 1) * npad, s));
   BEM_CUDA_CHECK(cudaMemsetAsync(w.flags, 0, sizeof(Flags), s));
   for (int b = 0; b < batch; ++b)
     BEM_CUDA_CHECK(cudaMemset2DAsync((double2*)X_dev + (size_t)b * strideB, ldb * sizeof(double2), 0,
@@ -609,10 +585,11 @@ extern "C" int bem_gmres_solve(const void* A_dev, int64_t lda, int64_t strideA, 
         if (precond_work_dev) {
           gmres_gather_kernel<<<dim3(ceil_div(npad, 256), nsys), 256, 0, s>>>(L, w.V, col, w.Z, w.sys, w.flags);
           ++launches;
-          st = clu_solve_enqueue(precond_work_dev, npad, batch, w.Z, npad, strideW, nrhs, err_dev, s,
+          double2* zc = w.Z + (size_t)col * nrhs * npad;
+          st = clu_solve_enqueue(precond_work_dev, npad, batch, zc, npad, strideV, nrhs, err_dev, s,
                                  &w.flags->skip_inner);
           if (st) return st;
-          st = zgemm_ts_enqueue(n, n, nrhs, 1.0, 0.0, A_dev, lda, strideA, w.Z, npad, strideW, 0.0, 0.0, w.W, npad,
+          st = zgemm_ts_enqueue(n, n, nrhs, 1.0, 0.0, A_dev, lda, strideA, zc, ldv, strideV, 0.0, 0.0, w.W, npad,
                                 strideW, batch, w.ts, stream, &w.flags->skip_inner);
         } else {
           st = zgemm_ts_enqueue(n, n, nrhs, 1.0, 0.0, A_dev, lda, strideA, w.V + (size_t)col * nrhs * npad, ldv,
@@ -629,16 +606,9 @@ extern "C" int bem_gmres_solve(const void* A_dev, int64_t lda, int64_t strideA, 
         if (skip_inner) break;
       }
     }
-    gmres_update_kernel<<<nsys, kThreads, 0, s>>>(L, w.V, w.H, w.S, (const double2*)B_dev, (double2*)X_dev, w.R,
-                                                  precond_work_dev ? w.Z : nullptr, w.sys, w.flags);
+    gmres_update_kernel<<<nsys, kThreads, 0, s>>>(L, precond_work_dev ? w.Z : w.V, w.H, w.S,
+                                                  (const double2*)B_dev, (double2*)X_dev, w.R, w.sys, w.flags);
     ++launches;
-    if (precond_work_dev) {  // x += M^-1 (V y)
-      int st = clu_solve_enqueue(precond_work_dev, npad, batch, w.Z, npad, strideW, nrhs, err_dev, s,
-                                 &w.flags->skip_all);
-      if (st) return st;
-      gmres_add_kernel<<<dim3(ceil_div(n, 256), nsys), 256, 0, s>>>(L, w.Z, (double2*)X_dev, w.sys, w.flags);
-      ++launches;
-    }
     // r = b - A x
     int st = zgemm_ts_enqueue(n, n, nrhs, -1.0, 0.0, A_dev, lda, strideA, X_dev, ldb, strideB, 1.0, 0.0, w.R, npad,
                               strideW, batch, w.ts, stream, &w.flags->skip_all);
