@@ -395,8 +395,10 @@ int bem_refine_solve(const void* K_dev, int64_t ldk, int64_t strideK, int n, int
                      int* iters_out, double* resid_out, void* stream);
 
 /* ---- GMRES ------------------------------------------------------------------ */
-/* Workspace of bem_gmres_solve in bytes (Krylov bases, Hessenberg matrices,
- * rotations, per-system state, tall-GEMM partial sums); -1 for bad sizes. */
+/* Workspace of bem_gmres_solve in bytes (the Krylov basis V and the basis Z of
+ * preconditioned vectors, both restart + 1 vectors per system, Hessenberg
+ * matrices, rotations, per-system state, tall-GEMM partial sums); -1 for bad
+ * sizes. */
 int64_t bem_gmres_workspace_bytes(int n, int npad, int nrhs, int batch, int restart);
 
 /* Restarted GMRES, x0 = 0, for each of the nrhs columns of each of the `batch`
@@ -407,8 +409,10 @@ int64_t bem_gmres_workspace_bytes(int n, int npad, int nrhs, int batch, int rest
  * (capytaine/SciPy: 20), at most max_cycles restart cycles.
  * precond_work_dev: NULL for plain GMRES, or the factorisation of
  * bem_clu_factor (npad multiple of 128, err_dev required) used as the right
- * preconditioner M^-1 = (LU)^-1 (A M^-1 u = b, x = M^-1 u) with float32
- * factors and float64 products: GMRES-based iterative refinement of the
+ * preconditioner M^-1 = (LU)^-1 with float32 factors and float64 products, in
+ * the flexible form (z_k = M^-1 v_k kept, x += Z y at the end of a cycle, so
+ * that the rounding of the float32 substitutions cannot make the final update
+ * disagree with the Arnoldi products): GMRES-based iterative refinement of the
  * mixed-precision LU.  X (ldb,
  * strideB): rows < n written.  work_dev: bem_gmres_workspace_bytes, 256-byte
  * aligned.  iters_out: largest number of inner iterations over the systems;

@@ -163,8 +163,12 @@ def test_refinement_stops_and_gmres_recovers_near_a_singular_matrix():
     system): the float32 LU is wrong in that direction, the classical iteration
     x += (LU)^-1 r no longer contracts and stops early as non-converged; GMRES
     right-preconditioned by the same factors removes the outlier in a few
-    iterations.  The tolerance is 1e-8: with |x| ~ 1e7 |b| the float64 residual
-    b - K x cannot be resolved much below ~1e-10 |b|."""
+    iterations.  The factors are then close to singular themselves (|M^-1| of
+    order 1e5-1e6), where the float32 substitutions are measurably nonlinear:
+    the flexible form (M^-1 v_k kept for the update of x) converges in about 6
+    iterations, the plain form (M^-1 applied again to V y) took over 80.  The
+    tolerance is 1e-8: with |x| ~ 1e7 |b| the float64 residual b - K x cannot
+    be resolved much below ~1e-10 |b|."""
     import torch
     rng = np.random.default_rng(21)
     n, nrhs = 256, 3
