@@ -361,7 +361,7 @@ class B200Engine:
     BEMSolver(method=...) (bem/solver.py:172-207), for the device sweeps.
 
     refinement (precision "mixed"): "classical" (x += (LU)^-1 r) or "gmres"
-    (GMRES on the float64 K right-preconditioned by the float32 LU), both to
+    (flexible GMRES on the float64 K right-preconditioned by the float32 LU), both to
     refine_tol relative residual.  When the classical iteration stops
     contracting (K nearly singular, e.g. near an irregular frequency) the
     solve continues with the preconditioned GMRES (stats["escalated_to_gmres"]).
@@ -941,8 +941,8 @@ class B200Engine:
 
     def _refine(self, f, r, nb, Bc, Xc, Rc, nc, stats, stream):
         """Refined solve of nc columns (B, X, R column pointers, batch stride
-        npad * r.nrhs) with the float32 factors: classical refinement, or GMRES
-        right-preconditioned by the factors; the classical iteration continues
+        npad * r.nrhs) with the float32 factors: classical refinement, or flexible
+        GMRES right-preconditioned by the factors; the classical iteration continues
         with that GMRES when it stops contracting."""
         lib = _lib.load()
         n, npad, ld = f.n, f.npad, f.npad * r.nrhs
