@@ -201,3 +201,37 @@ def test_refinement_stops_and_gmres_recovers_near_a_singular_matrix():
     assert st == _lib.BEM_OK and res <= 1e-8 and it <= 20, (st, it, res, _lib.load().bem_last_error())
     for c in range(nrhs):
         assert np.linalg.norm(b[:, c] - A @ xs[0][:, c]) <= 2e-8 * np.linalg.norm(b[:, c])
+
+
+def test_flexible_gmres_over_short_restart_cycles():
+    """The preconditioned vectors are kept per restart cycle: with restart 2 a
+    K with one eigenvalue 1e-6 and a regular K, factored together by the
+    float32 LU and solved in one batched call, converge over several cycles,
+    every column to 1e-9 of its right-hand side (|x| reaches 1e6 |b| for the
+    first, so the float64 residual still resolves 1e-9)."""
+    import torch
+    rng = np.random.default_rng(8)
+    n, nrhs, npad = 256, 4, 256
+    mats = []
+    for lam0 in (1e-6 * (1 - 1j), None):
+        Q, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+        lam = rng.uniform(0.5, 1.5, n) * np.exp(1j * rng.uniform(-0.3, 0.3, n))
+        if lam0 is not None:
+            lam[0] = lam0
+        mats.append((Q * lam) @ Q.conj().T)
+    rhs = [rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs)) for _ in mats]
+    lib = _lib.load()
+    K = torch.stack([torch.as_tensor(np.ascontiguousarray(A.T)).reshape(-1) for A in mats]).cuda()
+    work = torch.empty(int(lib.bem_clu_workspace_bytes(npad, 2)) + 1024, dtype=torch.uint8, device="cuda")
+    wptr = (work.data_ptr() + 1023) // 1024 * 1024
+    piv = torch.empty((2, npad), dtype=torch.int32, device="cuda")
+    info = torch.zeros(2, dtype=torch.int32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.check(lib.bem_clu_factor(_vp(K), n, n * n, n, npad, 2, _vp(piv), _vp(info), _vp(wptr), _vp(err),
+                                  _lib.stream_ptr()))
+    xs, st, it, res, *_ = _gmres_device(mats, rhs, atol=0.0, rtol=1e-9, restart=2, precond=_vp(wptr), npad=npad)
+    assert st == _lib.BEM_OK and res <= 1e-9, (st, it, res, _lib.load().bem_last_error())
+    assert it > 2  # more than one cycle of 2
+    for A, b, x in zip(mats, rhs, xs):
+        for c in range(nrhs):
+            assert np.linalg.norm(b[:, c] - A @ x[:, c]) <= 2e-9 * np.linalg.norm(b[:, c])
