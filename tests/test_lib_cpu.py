@@ -286,6 +286,13 @@ def test_linear_algebra_arguments_checked_on_host(lib):
     assert lib.bem_gmres_solve(fake, 50, 10000, 100, 128, 1, fake, fake, 128, 128, 1, 0.0, 1e-5, 20, 5, None,
                                fake, fake, ctypes.byref(it), ctypes.byref(res), None) == bad  # lda < n
     assert lib.bem_gmres_workspace_bytes(100, 128, 1, 1, 20) > 0
+    # one more restart vector adds at least one complex128 column of npad rows
+    # per system to the Krylov basis V and one to the kept preconditioned
+    # basis Z of the flexible form
+    for nrhs, batch in ((1, 1), (7, 3)):
+        grow = (lib.bem_gmres_workspace_bytes(1000, 1024, nrhs, batch, 21)
+                - lib.bem_gmres_workspace_bytes(1000, 1024, nrhs, batch, 20))
+        assert grow >= 2 * 16 * 1024 * nrhs * batch
     # right-hand sides and forces: ldb < n, null outputs
     inf = float("inf")
     assert lib.bem_build_rhs(100, 1, fake, fake, 9.81, inf, 1, fake, 1, fake, fake, fake, None, fake, 99, 100 * 2,
